@@ -1,0 +1,375 @@
+"""
+CPU oracle of pyOCEAN's tracer hot path (TEST INFRASTRUCTURE ONLY).
+
+Only ``tests/``, ``__graft_entry__.smoke()`` (as the checker) and ``bench.py``'s CPU-baseline leg import this
+module.  The product package ``pyocean_b200`` never does: its path is the CUDA library, which fails loudly when it
+is missing.
+
+The arithmetic lives in ``pocean_oracle.c`` (one C function per Numba kernel of the reference, same expression
+order, no FMA contraction), loaded through ctypes.  This module restates the Python orchestration around those
+kernels with the reference's call signatures:
+
+* ``TracerAdvection`` — ``core/components/tracers.py:50-375`` (``advect_fct`` :208-254, the unlimited NumPy path
+  :256-301, ``advect`` :342-375, ``faces_h`` :166-176, ``upwind_faces_h`` :178-193, periodic pad/crop :80-102,
+  ``_open_inflow`` :65-78).
+* ``Periodic`` — ``core/model/periodic.py:31, 47-94`` (pad/crop with ``TRACER_HALO`` wrapped cells).
+* ``remap_column`` / ``remap_columns`` / ``reconstruct`` — ``core/vertical/remap.py:234-427``.
+
+Parity of this restatement with the reference is pinned by ``tests/test_oracle_golden.py`` against the vectors in
+``tests/golden/`` that ``tests/golden/make_golden.py`` generated by running the reference itself.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+from . import build as _build
+
+TRACER_HALO = 13                       # core/model/periodic.py:31
+PCM, PLM, PPM_H4 = 0, 1, 2             # core/vertical/remap.py:40
+SCHEMES = {"pcm": PCM, "plm": PLM, "ppm_h4": PPM_H4}
+
+_D = ctypes.POINTER(ctypes.c_double)
+_U8 = ctypes.POINTER(ctypes.c_uint8)
+_LIB = None
+
+
+def lib() -> ctypes.CDLL:
+    """The compiled oracle (built on first use if the shared object is missing)."""
+    global _LIB
+    if _LIB is None:
+        path = _build.LIB if os.path.exists(_build.LIB) else _build.build()
+        L = ctypes.CDLL(path)
+        i, d, v = ctypes.c_int, ctypes.c_double, ctypes.c_void_p
+        L.oracle_advect_faces_h.argtypes = [_D, _D, _D, _U8, _D, i, i, i, i, i, i, i, i, i, _D, _D]
+        L.oracle_advect_div.argtypes = [_D, _D, _D, _D, _U8, _D, i, i, i, i, i, i, i, i, i, i, _D]
+        L.oracle_rk_stage.argtypes = [_D, _D, _D, d, _D, _D, i, ctypes.c_int64, ctypes.c_int64, _D, _D]
+        L.oracle_fct_stage.argtypes = [_D, _D, _D, _D, d, d, d, _D, _D, i, i, i, i, _D, _D]
+        L.oracle_fct_fluxes.argtypes = [_D, _D, _D, _D, i, i, i, i, i, i, i, i, _D, _D, _D, _D, _D, _D, _D, _D,
+                                        _D, _D]
+        L.oracle_fct_coeff.argtypes = [_D, _D, _D, _D, _D, _U8, d, i, i, i, i, _D, _D]
+        L.oracle_fct_final.argtypes = [_D, _D, _D, _D, _D, _D, _D, d, _D, _D, i, i, i, i, _D]
+        L.oracle_advect_fct.argtypes = [_D, _D, _D, _D, _D, _U8, v, i, i, i, i, i, i, i, i, i, d, _D, v, v]
+        L.oracle_advect_fct.restype = i
+        L.oracle_remap_column.argtypes = [_D, _D, i, _D, i, i, _D, _D]
+        L.oracle_reconstruct.argtypes = [_D, _D, i, i, _D]
+        L.oracle_remap_columns.argtypes = [_D, _D, _D, i, i, i, i, i, _U8, _D]
+        L.oracle_num_threads.restype = i
+        L.oracle_set_threads.argtypes = [i]
+        _LIB = L
+    return _LIB
+
+
+def set_threads(n: int) -> None:
+    """OpenMP threads of the oracle's loops (results are identical for any count, as in the reference)."""
+    lib().oracle_set_threads(int(n))
+
+
+def num_threads() -> int:
+    return int(lib().oracle_num_threads())
+
+
+def _f64(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def _u8(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=bool).view(np.uint8)
+
+
+def _p(a: np.ndarray):
+    return a.ctypes.data_as(_D)
+
+
+def _pu8(a: np.ndarray):
+    return a.ctypes.data_as(_U8)
+
+
+# ------------------------------------------------------------------------------------------------ periodic
+class Periodic:
+    """Restatement of ``core/model/periodic.py:47-94``: which horizontal axes wrap, and the pad/crop halo."""
+
+    def __init__(self, axes=()) -> None:
+        if isinstance(axes, str):
+            axes = (axes,)
+        axes = tuple(axes or ())
+        bad = [a for a in axes if a not in ("x", "y")]
+        if bad:
+            raise ValueError(f"unknown periodic axes {bad}; use 'x', 'y' or both")
+        self.x, self.y = "x" in axes, "y" in axes
+        self.axes = tuple(a for a in ("x", "y") if a in axes)
+
+    def __bool__(self) -> bool:
+        return self.x or self.y
+
+    @staticmethod
+    def _index(n_cells: int, face: bool, halo: int) -> np.ndarray:
+        return np.arange(-halo, n_cells + halo + (1 if face else 0)) % n_cells
+
+    def pad(self, a, kind: str, halo: int) -> np.ndarray:
+        a = np.asarray(a)
+        if self.x:
+            face = kind in ("u", "q")
+            a = np.take(a, self._index(a.shape[-1] - face, face, halo), axis=-1)
+        if self.y:
+            face = kind in ("v", "q")
+            a = np.take(a, self._index(a.shape[-2] - face, face, halo), axis=-2)
+        return a
+
+    def crop(self, a: np.ndarray, kind: str, halo: int) -> np.ndarray:
+        if self.x:
+            a = a[..., halo:a.shape[-1] - halo]
+        if self.y:
+            a = a[..., halo:a.shape[-2] - halo, :]
+        return np.ascontiguousarray(a)
+
+
+NONE = Periodic()
+
+
+class OpenEdges:
+    """The part of the reference's open-boundary object that the tracer path reads: ``open`` (edge names)."""
+
+    def __init__(self, open_=()) -> None:
+        self.open = tuple(open_)
+
+
+# ------------------------------------------------------------------------------------------------ kernels
+def advect_faces_h(c, Qx, Qy, ok, ext, open_w, open_e, open_s, open_n, z_variant):
+    """``sigma_baroclinic.py:265-321``: WENO5 horizontal face fluxes (fx, fy) of the stack c."""
+    c = _f64(c)
+    nt, n, ny, nx = c.shape
+    Qx, Qy, ext = _f64(Qx), _f64(Qy), _f64(ext)
+    okc = _u8(np.broadcast_to(ok, c.shape[1:]))
+    fx = np.empty((nt, n, ny, nx + 1))
+    fy = np.empty((nt, n, ny + 1, nx))
+    lib().oracle_advect_faces_h(_p(c), _p(Qx), _p(Qy), _pu8(okc), _p(ext), nt, n, ny, nx, int(open_w), int(open_e),
+                                int(open_s), int(open_n), int(z_variant), _p(fx), _p(fy))
+    return fx, fy
+
+
+def advect_div(c, Qx, Qy, Fz, ok, ext, open_w, open_e, open_s, open_n, z_variant, vert):
+    """``sigma_baroclinic.py:324-364``: −∇·(Q c) with WENO5 faces in x, y and (``vert``) z."""
+    c = _f64(c)
+    nt, n, ny, nx = c.shape
+    out = np.empty_like(c)
+    okc = _u8(np.broadcast_to(ok, c.shape[1:]))
+    Qx, Qy, Fz, ext = _f64(Qx), _f64(Qy), _f64(Fz), _f64(ext)
+    lib().oracle_advect_div(_p(c), _p(Qx), _p(Qy), _p(Fz), _pu8(okc), _p(ext), nt, n, ny, nx, int(open_w),
+                            int(open_e), int(open_s), int(open_n), int(z_variant), int(vert), _p(out))
+    return out
+
+
+def fct_coefficients(c0, cL, V1, Ax, Ay, ok, dt):
+    """``sigma_baroclinic.py:407-449`` (``_fct_coeff_kernel``): Zalesak coefficients (Cx, Cy)."""
+    c0, cL, V1, Ax, Ay = _f64(c0), _f64(cL), _f64(V1), _f64(Ax), _f64(Ay)
+    nt, n, ny, nx = c0.shape
+    okc = _u8(np.broadcast_to(ok, c0.shape[1:]))
+    Cx, Cy = np.empty_like(Ax), np.empty_like(Ay)
+    lib().oracle_fct_coeff(_p(c0), _p(cL), _p(V1), _p(Ax), _p(Ay), _pu8(okc), float(dt), nt, n, ny, nx, _p(Cx),
+                           _p(Cy))
+    return Cx, Cy
+
+
+def _rk_stage(qa, qb, r, dt, V, C, stage):
+    """``sigma_baroclinic.py:856-875``: one SSP-RK3 stage with the ``safe`` rule."""
+    qa, qb, r, V, C = _f64(qa), _f64(qb), _f64(r), _f64(V), _f64(C)
+    q, c = np.empty_like(C), np.empty_like(C)
+    lib().oracle_rk_stage(_p(qa), _p(qb), _p(r), float(dt), _p(V), _p(C), int(stage), C.size, V.size, _p(q), _p(c))
+    return q, c
+
+
+# ------------------------------------------------------------------------------------------------ component
+class TracerAdvection:
+    """Restatement of ``core/components/tracers.py:50-375`` (WENO5 SSP-RK3 paths, FCT and unlimited)."""
+
+    def __init__(self, *, scheme: str = "weno5", time: str = "ssprk3", dt: float, ob=None) -> None:
+        self.tracer_scheme, self.tracer_time, self.dt = scheme, time, dt
+        self.ob = ob if ob is not None else OpenEdges()
+        self.per = NONE
+        self.record_open_flux = False
+        self.last_open_flux = None
+
+    # tracers.py:65-78
+    def _open_inflow(self, Fx, Fy):
+        opn = self.ob.open
+        out = np.zeros(Fx.shape[0])
+        for edge, F, sl, sgn in (("west", Fx, np.s_[..., 0], 1.0), ("east", Fx, np.s_[..., -1], -1.0),
+                                 ("south", Fy, np.s_[..., 0, :], 1.0), ("north", Fy, np.s_[..., -1, :], -1.0)):
+            if edge in opn:
+                out += sgn * F[sl].reshape(F.shape[0], -1).sum(axis=1)
+        return out
+
+    # tracers.py:80-102
+    def _periodic(self, method, C, V0, V1, Qx, Qy, Fz, ok, inflow, flux_face_i, **kw):
+        per, H = self.per, TRACER_HALO
+        pad = lambda a, kind: None if a is None else per.pad(a, kind, H)          # noqa: E731
+        fi = None if flux_face_i is None else flux_face_i + (H if per.x else 0)
+        args = [pad(C, "c"), pad(V0, "c"), pad(V1, "c"), pad(Qx, "u"), pad(Qy, "v")]
+        if Fz is not None:
+            args.append(pad(Fz, "c"))
+        args.append(pad(np.broadcast_to(ok, np.shape(C)[1:]), "c"))
+        self.per = NONE
+        try:
+            res = method(*args, inflow=pad(inflow, "c"), flux_face_i=fi, **kw)
+        finally:
+            self.per = per
+        if fi is None:
+            return per.crop(res, "c", H)
+        out, fx = res
+        if per.y:
+            fx = np.ascontiguousarray(fx[..., H:fx.shape[-1] - H])
+        return per.crop(out, "c", H), fx
+
+    def _open_flags(self):
+        o = self.ob.open
+        return "west" in o, "east" in o, "south" in o, "north" in o
+
+    # tracers.py:166-176
+    def faces_h(self, c, Qx, Qy, ok, ext=None, inflow=None):
+        c = _f64(c)
+        e = (c if inflow is None else inflow) if ext is None else ext
+        return advect_faces_h(c, Qx, Qy, ok, e, *self._open_flags(), self.tracer_scheme == "weno5")
+
+    # tracers.py:178-193
+    def upwind_faces_h(self, c, Qx, Qy, inflow=None):
+        ext = c if inflow is None else inflow
+        fx = np.zeros(c.shape[:3] + (c.shape[3] + 1,))
+        fy = np.zeros(c.shape[:2] + (c.shape[2] + 1, c.shape[3]))
+        fx[..., 1:-1] = Qx[None, ..., 1:-1] * np.where(Qx[None, ..., 1:-1] >= 0, c[..., :-1], c[..., 1:])
+        fy[..., 1:-1, :] = Qy[None, :, 1:-1, :] * np.where(Qy[None, :, 1:-1, :] >= 0, c[..., :-1, :], c[..., 1:, :])
+        opn = self.ob.open
+        if "west" in opn:
+            fx[..., 0] = Qx[None, ..., 0] * np.where(Qx[None, ..., 0] > 0, ext[..., 0], c[..., 0])
+        if "east" in opn:
+            fx[..., -1] = Qx[None, ..., -1] * np.where(Qx[None, ..., -1] < 0, ext[..., -1], c[..., -1])
+        if "south" in opn:
+            fy[..., 0, :] = Qy[None, :, 0, :] * np.where(Qy[None, :, 0, :] > 0, ext[..., 0, :], c[..., 0, :])
+        if "north" in opn:
+            fy[..., -1, :] = Qy[None, :, -1, :] * np.where(Qy[None, :, -1, :] < 0, ext[..., -1, :], c[..., -1, :])
+        return fx, fy
+
+    # tracers.py:153-164 (WENO5 schemes only: the fused compiled kernel)
+    def rhs(self, c, Qx, Qy, Fz, ok, centred=False, inflow=None):
+        if centred or not self.tracer_scheme.startswith("weno5"):
+            raise NotImplementedError("oracle: only the WENO5 upwind RHS (the compiled path) is restated")
+        c = _f64(c)
+        ext = c if inflow is None else inflow
+        return advect_div(c, Qx, Qy, Fz, ok, ext, *self._open_flags(), self.tracer_scheme == "weno5",
+                          bool(np.any(np.asarray(Fz) != 0.0)))
+
+    # tracers.py:208-254
+    def advect_fct(self, C, V0, V1, Qx, Qy, ok, unlimited=False, inflow=None, flux_face_i=None):
+        if self.per:
+            return self._periodic(self.advect_fct, C, V0, V1, Qx, Qy, None, ok, inflow, flux_face_i,
+                                  unlimited=unlimited)
+        if unlimited:
+            return self.advect_fct_numpy(C, V0, V1, Qx, Qy, ok, unlimited=True, inflow=inflow,
+                                         flux_face_i=flux_face_i)
+        dt = float(self.dt)
+        C_in = C
+        C = _f64(C)
+        own = inflow is None or (inflow is C_in and C is C_in)     # ``ext is C`` of the reference (identity)
+        Qx, Qy, V0, V1 = _f64(Qx), _f64(Qy), _f64(V0), _f64(V1)
+        nt, n, ny, nx = C.shape
+        okc = _u8(np.broadcast_to(ok, C.shape[1:]))
+        infl = None if own else _f64(inflow)
+        out = np.empty_like(C)
+        want = self.record_open_flux or flux_face_i is not None
+        Fx = np.empty((nt, n, ny, nx + 1)) if want else None
+        Fy = np.empty((nt, n, ny + 1, nx)) if want else None
+        w, e, s, nn = self._open_flags()
+        rc = lib().oracle_advect_fct(_p(C), _p(V0), _p(V1), _p(Qx), _p(Qy), _pu8(okc),
+                                     None if infl is None else infl.ctypes.data, nt, n, ny, nx, int(w), int(e),
+                                     int(s), int(nn), int(self.tracer_scheme == "weno5"), dt, _p(out),
+                                     None if Fx is None else Fx.ctypes.data, None if Fy is None else Fy.ctypes.data)
+        if rc != 0:
+            raise MemoryError("oracle_advect_fct: out of host memory")
+        if self.record_open_flux:
+            self.last_open_flux = self._open_inflow(Fx, Fy)
+        if flux_face_i is None:
+            return out
+        return out, np.ascontiguousarray(Fx[..., flux_face_i])
+
+    # tracers.py:256-301 (the unlimited branch; the limited branch is ``advect_fct``)
+    def advect_fct_numpy(self, C, V0, V1, Qx, Qy, ok, unlimited=False, inflow=None, flux_face_i=None):
+        if self.per:
+            return self._periodic(self.advect_fct_numpy, C, V0, V1, Qx, Qy, None, ok, inflow, flux_face_i,
+                                  unlimited=unlimited)
+        if not unlimited:
+            return self.advect_fct(C, V0, V1, Qx, Qy, ok, inflow=inflow, flux_face_i=flux_face_i)
+        dt = self.dt
+        C = np.asarray(C, float)
+        V0, V1, Qx, Qy = (np.asarray(a, float) for a in (V0, V1, Qx, Qy))
+        dV = V1 - V0
+        div = lambda fx, fy: fx[..., 1:] - fx[..., :-1] + fy[..., 1:, :] - fy[..., :-1, :]   # noqa: E731
+        safe = lambda q, v: np.where(v > 0, q / np.where(v > 0, v, 1.0), C)                  # noqa: E731
+        q0 = V0 * C
+        fx0, fy0 = self.faces_h(C, Qx, Qy, ok, inflow=inflow)
+        q1 = q0 - dt * div(fx0, fy0)
+        c1 = safe(q1, V0 + dV)
+        fx1, fy1 = self.faces_h(c1, Qx, Qy, ok, inflow=inflow)
+        q2 = 0.75 * q0 + 0.25 * (q1 - dt * div(fx1, fy1))
+        c2 = safe(q2, V0 + 0.5 * dV)
+        fx2, fy2 = self.faces_h(c2, Qx, Qy, ok, inflow=inflow)
+        FHx = (fx0 + fx1) / 6.0 + 2.0 * fx2 / 3.0
+        FHy = (fy0 + fy1) / 6.0 + 2.0 * fy2 / 3.0
+        out = safe(q0 - dt * div(FHx, FHy), V1)
+        i = flux_face_i
+        return out if i is None else (out, FHx[..., i])
+
+    # tracers.py:342-375 (SSP-RK3 with the fused WENO5 RHS)
+    def advect(self, C, V0, V1, Qx, Qy, Fz, ok, inflow=None, flux_face_i=None):
+        if self.per:
+            return self._periodic(self.advect, C, V0, V1, Qx, Qy, Fz, ok, inflow, flux_face_i)
+        if self.tracer_time != "ssprk3":
+            raise NotImplementedError("oracle: only the SSP-RK3 time stepping is restated")
+        dt = self.dt
+        C = _f64(C)
+        if np.shape(V0) != C.shape[1:] or np.shape(V1) != C.shape[1:]:
+            raise ValueError(f"_advect: volume shape {np.shape(V0)}/{np.shape(V1)} vs tracer layers {C.shape[1:]}")
+        V0, V1 = np.asarray(V0, float), np.asarray(V1, float)
+        dV = V1 - V0
+        Va, Vb = V0 + dV, V0 + 0.5 * dV
+        q0 = V0 * C
+        q1, c1 = _rk_stage(q0, q0, self.rhs(C, Qx, Qy, Fz, ok, inflow=inflow), dt, Va, C, 1)
+        q2, c2 = _rk_stage(q0, q1, self.rhs(c1, Qx, Qy, Fz, ok, inflow=inflow), dt, Vb, C, 2)
+        _, c3 = _rk_stage(q0, q2, self.rhs(c2, Qx, Qy, Fz, ok, inflow=inflow), dt, V1, C, 3)
+        if flux_face_i is None:
+            return c3
+        fx = lambda c: self.faces_h(c, Qx, Qy, ok, inflow=inflow)[0][..., flux_face_i]       # noqa: E731
+        return c3, (fx(C) + fx(c1)) / 6.0 + 2.0 * fx(c2) / 3.0
+
+
+# ------------------------------------------------------------------------------------------------ remap
+def reconstruct(h, u, scheme):
+    """``remap.py:234-294``: polynomial coefficients (n, 3) of one column."""
+    h, u = _f64(h), _f64(u)
+    coef = np.empty((h.size, 3))
+    lib().oracle_reconstruct(_p(h), _p(u), h.size, int(scheme), _p(coef))
+    return coef
+
+
+def remap_column(h_src, u_src, h_tgt, scheme, u_tgt=None):
+    """``remap.py:306-397``: conservative remap of one column; returns (and fills) u_tgt."""
+    h_src, u_src, h_tgt = _f64(h_src), _f64(u_src), _f64(h_tgt)
+    n0, n1 = h_src.size, h_tgt.size
+    out = np.empty(n1)
+    work = np.empty(10 * max(n0, n1) + 16)
+    lib().oracle_remap_column(_p(h_src), _p(u_src), n0, _p(h_tgt), n1, int(scheme), _p(out), _p(work))
+    if u_tgt is not None:
+        u_tgt[...] = out
+    return out
+
+
+def remap_columns(h_src, f_src, h_tgt, scheme, wet):
+    """``remap.py:418-427``: remap every wet column of f_src (N0, ny, nx) onto h_tgt (N1, ny, nx)."""
+    h_src, f_src, h_tgt = _f64(h_src), _f64(f_src), _f64(h_tgt)
+    n0, ny, nx = h_src.shape
+    n1 = h_tgt.shape[0]
+    out = np.empty(h_tgt.shape)
+    w = _u8(np.broadcast_to(wet, (ny, nx)))
+    lib().oracle_remap_columns(_p(h_src), _p(f_src), _p(h_tgt), n0, n1, ny, nx, int(scheme), _pu8(w), _p(out))
+    return out

@@ -1,0 +1,268 @@
+"""
+Generate the golden vectors of tests/golden/ by running the reference pyOCEAN code itself.
+
+Run in a container that has the reference checkout (read-only) at REFERENCE (default ``/root/reference``)::
+
+    python tests/golden/make_golden.py [REFERENCE]
+
+It imports the reference's own modules (``core.components.tracers``, ``core.dynamics.sigma_baroclinic``,
+``core.vertical.remap``) with a stub ``xarray`` (the hot-path modules use it only in annotations and helpers that
+are not called here), keeps Numba's cache and Python's bytecode out of the reference tree, feeds seeded synthetic
+inputs through the reference's public calls and stores inputs and outputs as compressed ``.npz`` files next to this
+script.  The tests never import the reference: they read these files.
+"""
+from __future__ import annotations
+
+import os
+import sys
+import types
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REFERENCE = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+
+os.environ.setdefault("NUMBA_CACHE_DIR", "/tmp/pocean_golden_numba_cache")
+os.environ["PYTHONDONTWRITEBYTECODE"] = "1"
+sys.dont_write_bytecode = True
+_xr = types.ModuleType("xarray")
+
+
+class _Placeholder:                                   # annotations only
+    pass
+
+
+_xr.Dataset = _xr.DataArray = _Placeholder
+sys.modules.setdefault("xarray", _xr)
+sys.path.insert(0, REFERENCE)
+
+import numpy as np                                     # noqa: E402
+
+from core.components.tracers import TracerAdvection    # noqa: E402
+from core.dynamics import sigma_baroclinic as sb       # noqa: E402
+from core.model import threads                         # noqa: E402
+from core.model.periodic import Periodic               # noqa: E402
+from core.vertical import remap as rm                  # noqa: E402
+
+
+class _OB:
+    def __init__(self, open_=()):
+        self.open = tuple(open_)
+
+
+def transports(rng, nt, n, ny, nx, dt, open_=(), land=0.1, thin=True, periodic=()):
+    """Seeded layer volumes and transports: V0, V1 = V0 − Δt ∇·Q, ok = active & V1 > 0 (as the ALE step)."""
+    h = rng.uniform(1.0, 5.0, (n, ny, nx))
+    if thin:
+        h[min(2, n - 1), ny // 2, nx // 2] = 1e-3
+    area = rng.uniform(0.9, 1.1, (ny, nx)) * 1e6
+    active = rng.random((ny, nx)) > land
+    V0 = area * h * active
+    hx = np.concatenate([h[..., :1], h], axis=-1)
+    hy = np.concatenate([h[:, :1], h], axis=1)
+    Qx = rng.uniform(-0.4, 0.4, (n, ny, nx + 1)) * 1e3 * hx
+    Qy = rng.uniform(-0.4, 0.4, (n, ny + 1, nx)) * 1e3 * hy
+    ax = np.zeros((ny, nx + 1), bool)
+    ax[:, 1:-1] = active[:, 1:] & active[:, :-1]
+    ay = np.zeros((ny + 1, nx), bool)
+    ay[1:-1] = active[1:] & active[:-1]
+    if "west" in open_:
+        ax[:, 0] = active[:, 0]
+    if "east" in open_:
+        ax[:, -1] = active[:, -1]
+    if "south" in open_:
+        ay[0] = active[0]
+    if "north" in open_:
+        ay[-1] = active[-1]
+    if "x" in periodic:
+        ax[:, 0] = ax[:, -1] = active[:, 0] & active[:, -1]
+    if "y" in periodic:
+        ay[0] = ay[-1] = active[0] & active[-1]
+    Qx *= ax
+    Qy *= ay
+    if "x" in periodic:
+        Qx[..., -1] = Qx[..., 0]
+    if "y" in periodic:
+        Qy[:, -1] = Qy[:, 0]
+    V1 = V0 - dt * (Qx[..., 1:] - Qx[..., :-1] + Qy[:, 1:] - Qy[:, :-1])
+    ok = active[None] & (V1 > 0)
+    return V0, V1, Qx, Qy, ok
+
+
+def fct_cases():
+    out = {}
+    specs = [
+        # name, nt, n, ny, nx, open, inflow, scheme, periodic, dt, extras
+        ("closed", 2, 4, 12, 14, (), False, "weno5", (), 30.0, {}),
+        ("open4_inflow", 2, 4, 12, 14, ("west", "east", "south", "north"), True, "weno5", (), 30.0, {}),
+        ("open3_noinflow", 2, 3, 10, 13, ("west", "east", "south"), False, "weno5", (), 30.0, {}),
+        ("js", 2, 4, 11, 12, ("west",), True, "weno5js", (), 30.0, {}),
+        ("periodic_x", 1, 5, 16, 16, (), False, "weno5", ("x",), 30.0, {}),
+        ("periodic_xy", 2, 3, 12, 10, (), False, "weno5", ("x", "y"), 30.0, {}),
+        ("periodic_x_open_sn", 1, 3, 12, 9, ("south", "north"), True, "weno5", ("x",), 30.0, {}),
+        ("tef_budget", 2, 3, 9, 11, ("west", "east", "north"), True, "weno5", (), 30.0,
+         {"flux_face_i": 4, "record": True}),
+        ("unlimited", 2, 3, 9, 11, ("west",), True, "weno5", (), 30.0, {"unlimited": True}),
+        ("unlimited_tef", 1, 3, 8, 10, (), False, "weno5", (), 30.0, {"unlimited": True, "flux_face_i": 3}),
+        ("tiny_1x1", 1, 2, 1, 1, (), False, "weno5", (), 30.0, {}),
+        ("thin_row", 1, 2, 1, 9, ("west", "east"), True, "weno5", (), 30.0, {}),
+    ]
+    for seed, (name, nt, n, ny, nx, open_, infl, scheme, per, dt, extras) in enumerate(specs):
+        rng = np.random.default_rng(100 + seed)
+        V0, V1, Qx, Qy, ok = transports(rng, nt, n, ny, nx, dt, open_, periodic=per)
+        T = 7.0 + rng.normal(0, 1, (n, ny, nx))
+        C = np.stack([T, T ** 2][:nt]) if nt <= 2 else rng.normal(0, 1, (nt, n, ny, nx))
+        inflow = np.stack([np.full(T.shape, 9.0), np.full(T.shape, 81.0)][:nt]) if infl else None
+        adv = TracerAdvection(scheme=scheme, time="ssprk3", dt=dt, ob=_OB(open_))
+        adv.per = Periodic(per)
+        adv.record_open_flux = bool(extras.get("record"))
+        res = adv.advect_fct(C, V0, V1, Qx, Qy, ok, unlimited=bool(extras.get("unlimited")), inflow=inflow,
+                             flux_face_i=extras.get("flux_face_i"))
+        rec = dict(C=C, V0=V0, V1=V1, Qx=Qx, Qy=Qy, ok=ok, dt=dt, scheme=scheme, open=np.array(open_, dtype="U5"),
+                   periodic=np.array(per, dtype="U1"), unlimited=bool(extras.get("unlimited")))
+        if inflow is not None:
+            rec["inflow"] = inflow
+        if "flux_face_i" in extras:
+            rec["flux_face_i"] = extras["flux_face_i"]
+            rec["out"], rec["fx_i"] = res
+        else:
+            rec["out"] = res
+        if adv.record_open_flux:
+            rec["open_flux"] = adv.last_open_flux
+        out[name] = rec
+    # the two-cell pulse at Courant 0.5 of tests/test_sigma_ale.py:1308-1325 (1-D, 4 layers, dx = 1 km)
+    nx, n, dt, dx = 60, 4, 30.0, 1000.0
+    h = np.full((n, 1, nx), 5.0)
+    V = h * dx * dx
+    Qx = np.zeros((n, 1, nx + 1))
+    Qx[:, :, 1:-1] = 0.5 * dx / dt * h[:, :, 1:] * dx
+    Qx[:, :, -2:] = 0.0
+    Qy = np.zeros((n, 2, nx))
+    V1 = V - dt * (Qx[..., 1:] - Qx[..., :-1])
+    ok = V1 > 0
+    T = np.where((np.arange(nx) >= 20) & (np.arange(nx) < 22), 1.0, 0.0)[None, None, :].repeat(n, 0)[None]
+    adv = TracerAdvection(scheme="weno5", time="ssprk3", dt=dt, ob=_OB())
+    out["pulse"] = dict(C=T, V0=V, V1=V1, Qx=Qx, Qy=Qy, ok=ok, dt=dt, scheme="weno5", open=np.array((), "U5"),
+                        periodic=np.array((), "U1"), unlimited=False, out=adv.advect_fct(T, V, V1, Qx, Qy, ok))
+    return out
+
+
+def rk3_cases():
+    out = {}
+    specs = [("open_vert", 2, 6, 9, 13, ("west", "east", "south"), True, "weno5", ()),
+             ("closed_js_vert", 1, 5, 8, 10, (), False, "weno5js", ()),
+             ("periodic_x_novert", 2, 4, 10, 12, (), False, "weno5", ("x",)),
+             ("tef", 1, 4, 7, 9, ("east",), False, "weno5", ())]
+    for seed, (name, nt, n, ny, nx, open_, vert, scheme, per) in enumerate(specs):
+        rng = np.random.default_rng(200 + seed)
+        dt = 10.0
+        V0, V1, Qx, Qy, ok = transports(rng, nt, n, ny, nx, dt, open_, periodic=per)
+        Fz = rng.normal(size=(n + 1, ny, nx)) * 1e2 if vert else np.zeros((n + 1, ny, nx))
+        Fz[0] = Fz[-1] = 0.0
+        C = rng.normal(10.0, 1.0, (nt, n, ny, nx))
+        adv = TracerAdvection(scheme=scheme, time="ssprk3", dt=dt, ob=_OB(open_))
+        adv.per = Periodic(per)
+        fi = 3 if name == "tef" else None
+        res = adv.advect(C, V0, V1, Qx, Qy, Fz, ok, inflow=None, flux_face_i=fi)
+        rec = dict(C=C, V0=V0, V1=V1, Qx=Qx, Qy=Qy, Fz=Fz, ok=ok, dt=dt, scheme=scheme,
+                   open=np.array(open_, dtype="U5"), periodic=np.array(per, dtype="U1"))
+        if fi is None:
+            rec["out"] = res
+        else:
+            rec["flux_face_i"] = fi
+            rec["out"], rec["fx_i"] = res
+        # the RHS alone (_advect_div) for the kernel-level check
+        rec["rhs"] = adv.rhs(C, Qx, Qy, Fz, ok) if not per else adv.rhs(C[..., :], Qx, Qy, Fz, ok)
+        out[name] = rec
+    return out
+
+
+def kernel_cases():
+    """Single kernels: faces_h and the FCT coefficients (tests/test_sigma_ale.py:1396-1429 inputs)."""
+    out = {}
+    rng = np.random.default_rng(3)
+    nt, n, ny, nx = 2, 3, 4, 5
+    c0 = rng.uniform(0, 1, (nt, n, ny, nx)); cL = rng.uniform(0, 1, (nt, n, ny, nx))
+    V1 = rng.uniform(0.5, 2, (n, ny, nx)) * 1e6
+    Ax = rng.normal(0, 1e4, (nt, n, ny, nx + 1)); Ax[..., [0, -1]] = 0
+    Ay = rng.normal(0, 1e4, (nt, n, ny + 1, nx)); Ay[..., [0, -1], :] = 0
+    ok = rng.uniform(0, 1, (n, ny, nx)) > 0.1
+    Cx, Cy = sb._fct_coeff_kernel(c0, cL, V1, Ax, Ay, ok, 30.0)
+    out["coeff"] = dict(c0=c0, cL=cL, V1=V1, Ax=Ax, Ay=Ay, ok=ok, dt=30.0, Cx=Cx, Cy=Cy)
+    rng = np.random.default_rng(11)
+    nt, n, ny, nx = 2, 3, 9, 11
+    c = rng.normal(10.0, 1.0, (nt, n, ny, nx))
+    Qx = rng.normal(size=(n, ny, nx + 1)); Qx[rng.random(Qx.shape) < 0.1] = 0.0
+    Qy = rng.normal(size=(n, ny + 1, nx)); Qy[rng.random(Qy.shape) < 0.1] = 0.0
+    ok = rng.random((n, ny, nx)) > 0.15
+    ext = rng.normal(12.0, 1.0, c.shape)
+    for z in (True, False):
+        fx, fy = sb._advect_faces_h(c, Qx, Qy, ok, ext, True, True, True, False, z)
+        out["faces_" + ("z" if z else "js")] = dict(c=c, Qx=Qx, Qy=Qy, ok=ok, ext=ext, fx=fx, fy=fy)
+    return out
+
+
+def remap_cases():
+    out = {}
+    rng = np.random.default_rng(5)
+    # many columns: random thicknesses with vanished layers at random places, n0 = n1 = 50
+    N, ny, nx = 50, 8, 25
+    h0 = np.where(rng.random((N, ny, nx)) < 0.3, rng.choice([0.0, 1e-10, 1e-3], (N, ny, nx)),
+                  rng.uniform(0.5, 50.0, (N, ny, nx)))
+    f = rng.normal(15, 3, (N, ny, nx))
+    h1 = rng.uniform(0.1, 2.0, (N, ny, nx))
+    h1 *= h0.sum(0) / h1.sum(0)
+    h1[:, 0, :5] = h0[:, 0, :5]                        # identity columns
+    h1[:, 1, :3] = 0.0                                 # vanished targets (whole column)
+    h1[3:9, 2, :] = 0.0                                # a band of vanished targets
+    h1[:, 2, :] *= h0[:, 2, :].sum(0) / np.where(h1[:, 2, :].sum(0) > 0, h1[:, 2, :].sum(0), 1.0)
+    h1[-1, 3, :4] += 1e-9                              # target thicker than source
+    h0[-1, 3, 4:8] += 1e-9                             # source thicker than target
+    h0[:, 4, :2] = 0.0                                 # dry-by-thickness columns (wet flag True)
+    wet = rng.random((ny, nx)) > 0.1
+    wet[4, :2] = True
+    out["cols"] = dict(h_src=h0, f_src=f, h_tgt=h1, wet=wet)
+    for name, scheme in (("pcm", rm.PCM), ("plm", rm.PLM), ("ppm_h4", rm.PPM_H4)):
+        out["cols"]["out_" + name] = rm.remap_columns(h0, f, h1, scheme, wet)
+    # n0 != n1 (with dry columns -> NaN), z*-like columns with many vanished bottom layers
+    N0, N1 = 30, 20
+    h0 = rng.uniform(0.0, 4.0, (N0, 6, 7)); h0[rng.random(h0.shape) < 0.2] = 0.0
+    h0[:22, 5, :] = 0.0
+    f = rng.normal(12, 2, (N0, 6, 7))
+    h1 = rng.uniform(0.1, 2.0, (N1, 6, 7)); h1 *= h0.sum(0) / h1.sum(0)
+    wet = np.ones((6, 7), bool); wet[0, 0] = False; wet[2, 3] = False
+    out["n0n1"] = dict(h_src=h0, f_src=f, h_tgt=h1, wet=wet)
+    for name, scheme in (("pcm", rm.PCM), ("plm", rm.PLM), ("ppm_h4", rm.PPM_H4)):
+        out["n0n1"]["out_" + name] = rm.remap_columns(h0, f, h1, scheme, wet)
+    # short columns (n = 1 … 5) in every scheme, single-column API
+    for n in (1, 2, 3, 4, 5):
+        hs = rng.uniform(0.2, 2.0, n); us = rng.normal(10, 2, n)
+        ht = rng.uniform(0.2, 2.0, n + 1); ht *= hs.sum() / ht.sum()
+        for name, scheme in (("pcm", rm.PCM), ("plm", rm.PLM), ("ppm_h4", rm.PPM_H4)):
+            u1 = np.empty(n + 1)
+            rm.remap_column(hs, us, ht, scheme, u1)
+            out[f"short{n}_{name}"] = dict(h_src=hs, f_src=us, h_tgt=ht, scheme=scheme, out=u1)
+    # reconstruction coefficients of a few columns
+    for name, scheme in (("plm", rm.PLM), ("ppm_h4", rm.PPM_H4)):
+        h = np.array([1.0, 0.7, 0.0, 1.3, 0.9, 1e-12, 1.1, 0.8, 1.2, 2.0])
+        u = rng.normal(10, 2, h.size)
+        coef = np.empty((h.size, 3))
+        rm.reconstruct(h, u, scheme, rm.H_NEGLECT, rm.H_NEGLECT_EDGE, coef)
+        out["coef_" + name] = dict(h=h, u=u, scheme=scheme, coef=coef)
+    return out
+
+
+def save(name, cases):
+    flat = {}
+    for case, rec in cases.items():
+        for k, v in rec.items():
+            flat[f"{case}/{k}"] = np.asarray(v)
+    path = os.path.join(HERE, name + ".npz")
+    np.savez_compressed(path, **flat)
+    print(f"{path}: {len(cases)} cases, {os.path.getsize(path) / 1e3:.0f} kB")
+
+
+if __name__ == "__main__":
+    threads.set_threads(1)
+    save("fct", fct_cases())
+    save("rk3", rk3_cases())
+    save("kernels", kernel_cases())
+    save("remap", remap_cases())

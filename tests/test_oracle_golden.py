@@ -1,0 +1,103 @@
+"""
+The CPU oracle (oracle/) against golden vectors produced by the reference itself (tests/golden/make_golden.py):
+bit-for-bit equality, since both evaluate the same FP64 expressions in the same order without FMA contraction.
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from conftest import case_open, case_periodic, load_golden
+from oracle import oracle as O
+
+FCT = load_golden("fct")
+RK3 = load_golden("rk3")
+KER = load_golden("kernels")
+REM = load_golden("remap")
+
+
+def _adv(rec, cls=O.TracerAdvection):
+    adv = cls(scheme=str(rec["scheme"]), time="ssprk3", dt=float(rec["dt"]), ob=O.OpenEdges(case_open(rec)))
+    adv.per = O.Periodic(case_periodic(rec))
+    return adv
+
+
+@pytest.mark.parametrize("case", sorted(FCT))
+def test_oracle_advect_fct_matches_reference_bitwise(case):
+    rec = FCT[case]
+    adv = _adv(rec)
+    adv.record_open_flux = "open_flux" in rec
+    fi = int(rec["flux_face_i"]) if "flux_face_i" in rec else None
+    res = adv.advect_fct(rec["C"], rec["V0"], rec["V1"], rec["Qx"], rec["Qy"], rec["ok"],
+                         unlimited=bool(rec["unlimited"]), inflow=rec.get("inflow"), flux_face_i=fi)
+    out, fx = (res if fi is not None else (res, None))
+    np.testing.assert_array_equal(out, rec["out"])
+    if fi is not None:
+        np.testing.assert_array_equal(fx, rec["fx_i"])
+    if "open_flux" in rec:
+        np.testing.assert_allclose(adv.last_open_flux, rec["open_flux"], rtol=1e-13, atol=0)
+
+
+@pytest.mark.parametrize("case", sorted(RK3))
+def test_oracle_rk3_matches_reference_bitwise(case):
+    rec = RK3[case]
+    adv = _adv(rec)
+    fi = int(rec["flux_face_i"]) if "flux_face_i" in rec else None
+    res = adv.advect(rec["C"], rec["V0"], rec["V1"], rec["Qx"], rec["Qy"], rec["Fz"], rec["ok"], flux_face_i=fi)
+    out, fx = (res if fi is not None else (res, None))
+    np.testing.assert_array_equal(out, rec["out"])
+    if fi is not None:
+        np.testing.assert_array_equal(fx, rec["fx_i"])
+    if not case_periodic(rec):
+        np.testing.assert_array_equal(adv.rhs(rec["C"], rec["Qx"], rec["Qy"], rec["Fz"], rec["ok"]), rec["rhs"])
+
+
+@pytest.mark.parametrize("variant", ["z", "js"])
+def test_oracle_faces_match_reference_bitwise(variant):
+    rec = KER["faces_" + variant]
+    fx, fy = O.advect_faces_h(rec["c"], rec["Qx"], rec["Qy"], rec["ok"], rec["ext"], True, True, True, False,
+                              variant == "z")
+    np.testing.assert_array_equal(fx, rec["fx"])
+    np.testing.assert_array_equal(fy, rec["fy"])
+
+
+def test_oracle_fct_coefficients_match_reference_bitwise():
+    rec = KER["coeff"]
+    Cx, Cy = O.fct_coefficients(rec["c0"], rec["cL"], rec["V1"], rec["Ax"], rec["Ay"], rec["ok"], float(rec["dt"]))
+    np.testing.assert_array_equal(Cx, rec["Cx"])
+    np.testing.assert_array_equal(Cy, rec["Cy"])
+
+
+@pytest.mark.parametrize("group", ["cols", "n0n1"])
+@pytest.mark.parametrize("scheme", ["pcm", "plm", "ppm_h4"])
+def test_oracle_remap_columns_match_reference_bitwise(group, scheme):
+    rec = REM[group]
+    out = O.remap_columns(rec["h_src"], rec["f_src"], rec["h_tgt"], O.SCHEMES[scheme], rec["wet"])
+    np.testing.assert_array_equal(out, rec["out_" + scheme])
+
+
+@pytest.mark.parametrize("case", sorted(c for c in REM if c.startswith("short")))
+def test_oracle_short_columns_match_reference_bitwise(case):
+    rec = REM[case]
+    out = O.remap_column(rec["h_src"], rec["f_src"], rec["h_tgt"], int(rec["scheme"]))
+    np.testing.assert_array_equal(out, rec["out"])
+
+
+@pytest.mark.parametrize("case", ["coef_plm", "coef_ppm_h4"])
+def test_oracle_reconstruction_matches_reference_bitwise(case):
+    rec = REM[case]
+    np.testing.assert_array_equal(O.reconstruct(rec["h"], rec["u"], int(rec["scheme"])), rec["coef"])
+
+
+def test_oracle_thread_count_does_not_change_results():
+    rec = FCT["open4_inflow"]
+    adv = _adv(rec)
+    n0 = O.num_threads()
+    try:
+        O.set_threads(1)
+        a = adv.advect_fct(rec["C"], rec["V0"], rec["V1"], rec["Qx"], rec["Qy"], rec["ok"], inflow=rec["inflow"])
+        O.set_threads(max(2, n0))
+        b = adv.advect_fct(rec["C"], rec["V0"], rec["V1"], rec["Qx"], rec["Qy"], rec["ok"], inflow=rec["inflow"])
+    finally:
+        O.set_threads(n0)
+    np.testing.assert_array_equal(a, b)
