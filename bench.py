@@ -1,0 +1,326 @@
+#!/usr/bin/env python
+"""
+Benchmark of the ALE tracer step on B200: advect_fct (SSP-RK3 WENO5-Z + Zalesak FCT) of a T/S stack followed by the
+PPM_H4 remap of both fields, on the 512 x 512 x 50 curvilinear basin (FP64, seeded synthetic data).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload basin|zstar_box]
+
+Metric: tracer cell-steps/s = nt * N * ny * nx * steps / time.  One "step" is one advect_fct + remap of the whole
+stack.  `value` is device-resident throughput (inputs already in HBM, CUDA events on the launching stream, max over
+ranks); `e2e` is the same step through the public drop-in API (TracerAdvection.advect_fct, remap_columns) with
+pinned host tensors, host<->device copies inside the timed region.  The stack (210 MB) and every geometry array
+(105 MB each) exceed the 126 MB L2, so no flush is needed between steps.
+
+Multi-GPU: the path does not shard (one domain per GPU, "replicas only"); under torchrun every rank runs its own
+replica and `value` sums the cell-steps of all ranks over the slowest rank's time.
+
+`--impl reference` times the reference's CPU implementation (the C restatement in oracle/, OpenMP on every host
+core; rank 0 only) on a bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="basin", choices=["basin", "zstar_box"])
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--cpu-seconds", type=float, default=12.0, help="budget of the CPU-baseline sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def make_workload(name: str):
+    from pyocean_b200 import workloads as W
+    return W.basin() if name == "basin" else W.zstar_box()
+
+
+def peaks() -> dict:
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return dict(hbm_gbs=float(d["hbm_gbs"]), source="measured")
+    return dict(hbm_gbs=6650.0, source="fallback")
+
+
+def cpu_model() -> str:
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+# ------------------------------------------------------------------------------------------------ CPU baseline
+def cpu_sample(w, budget_s: float) -> dict:
+    """The reference algorithm on the host (oracle/ C restatement, OpenMP over every core): whole steps of the same
+    workload until ~budget_s seconds have passed (at least one), timed with perf_counter."""
+    from oracle import oracle as O
+    ncores = os.cpu_count() or 1
+    O.set_threads(ncores)
+    adv = O.TracerAdvection(scheme=w.scheme, time="ssprk3", dt=w.dt, ob=O.OpenEdges(w.open))
+    adv.per = O.Periodic(w.periodic)
+    C = w.C
+    steps, t_total = 0, 0.0
+    while True:
+        t0 = time.perf_counter()
+        A = adv.advect_fct(C, w.V0, w.V1, w.Qx, w.Qy, w.ok)
+        C = np.stack([O.remap_columns(w.h_src, A[m], w.h_tgt, w.remap_scheme, w.wet) for m in range(A.shape[0])])
+        t_total += time.perf_counter() - t0
+        steps += 1
+        if t_total >= budget_s or steps >= 5:
+            break
+    value = w.tracer_cells * steps / t_total
+    return dict(value=value, unit="tracer cell-steps/s", cores=O.num_threads(), kind="port",
+                sample=f"{steps} full step(s) of {w.name} (advect_fct + remap of every tracer), "
+                       f"{t_total:.1f} s on {O.num_threads()} threads of {cpu_model()}",
+                seconds=t_total, steps=steps)
+
+
+# ------------------------------------------------------------------------------------------------ clocks
+class ClockSampler:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int) -> None:
+        self.gpu = gpu_index
+        self.proc = None
+
+    def start(self) -> None:
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return dict(sm_mhz=None, sm_max_mhz=None, reasons=["nvidia-smi unavailable"])
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=10)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+            out, _ = self.proc.communicate()
+        sm, smax, reasons, power = [], [], set(), []
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.strip().splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+                power.append(float(parts[3]))
+            except ValueError:
+                continue
+            for nm, flag in zip(names, parts[5:9]):
+                if flag.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return dict(sm_mhz=None, sm_max_mhz=None, reasons=["no samples"])
+        return dict(sm_mhz=statistics.median(sm), sm_max_mhz=max(smax), reasons=sorted(reasons),
+                    samples=len(sm), power_w_max=max(power) if power else None)
+
+
+# ------------------------------------------------------------------------------------------------ GPU arm
+def run_ours(args, rank: int, world: int, local_rank: int) -> dict | None:
+    import torch
+
+    from pyocean_b200 import _lib
+    from pyocean_b200.remap import remap_columns
+    from pyocean_b200.step import ALETracerStep
+    from pyocean_b200.tracers import OpenEdges, TracerAdvection
+    from pyocean_b200.periodic import Periodic
+    from pyocean_b200 import workloads as W
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    w = make_workload(args.workload)
+    nt, n, ny, nx = w.C.shape
+    flags = (_lib.PERIODIC_X if "x" in w.periodic else 0) | (_lib.PERIODIC_Y if "y" in w.periodic else 0)
+    g = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)                     # noqa: E731
+    C0, V0, V1, Qx, Qy = g(w.C), g(w.V0), g(w.V1), g(w.Qx), g(w.Qy)
+    ok = g(w.ok.view(np.uint8) if w.ok.dtype == np.bool_ else w.ok.astype(np.uint8))
+    wet = g(w.wet.astype(np.uint8))
+    hs, ht = g(w.h_src), g(w.h_tgt)
+    stepper = ALETracerStep(nt, n, ny, nx, w.dt, flags, w.remap_scheme, device=dev)
+    bufs = [C0.clone(), torch.empty_like(C0)]
+    stream = torch.cuda.current_stream(dev)
+
+    def one_step(i, ev=None):
+        src, dst = bufs[i % 2], bufs[(i + 1) % 2]
+        if ev is not None:
+            ev[0].record(stream)
+        a = stepper.advect(src, V0, V1, Qx, Qy, ok)
+        if ev is not None:
+            ev[1].record(stream)
+        stepper.remap(hs, a, ht, wet, dst)
+        if ev is not None:
+            ev[2].record(stream)
+
+    for i in range(args.warmup):
+        one_step(i)
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    evs = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(args.steps)]
+    t_start, t_end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    t_start.record(stream)
+    for i in range(args.steps):
+        one_step(args.warmup + i, evs[i])
+    t_end.record(stream)
+    torch.cuda.synchronize()
+    ms = t_start.elapsed_time(t_end)
+    if world > 1:
+        torch.distributed.barrier()
+    clk = clocks.stop()
+    adv_ms = [e[0].elapsed_time(e[1]) for e in evs]
+    rem_ms = [e[1].elapsed_time(e[2]) for e in evs]
+    # finite, conserved result (a cheap guard against timing a broken kernel)
+    res = bufs[(args.warmup + args.steps) % 2]
+    assert bool(torch.isfinite(res[:, :, w.wet]).all()), "non-finite tracer values after the timed steps"
+
+    if world > 1:
+        t = torch.tensor([ms], dtype=torch.float64, device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms = float(t.item())
+
+    # ---- end to end through the public API, pinned host tensors, copies inside the timed region
+    adv = TracerAdvection(scheme=w.scheme, time="ssprk3", dt=w.dt, ob=OpenEdges(w.open))
+    adv.per = Periodic(w.periodic)
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory()               # noqa: E731
+    hC, hV0, hV1, hQx, hQy, hok = pin(w.C), pin(w.V0), pin(w.V1), pin(w.Qx), pin(w.Qy), pin(w.ok)
+    hhs, hht, hwet = pin(w.h_src), pin(w.h_tgt), pin(w.wet)
+    h2d = sum(int(t.numel() * t.element_size()) for t in (hC, hV0, hV1, hQx, hQy, hok, hhs, hht, hwet))
+    h2d += int(hC.numel() * hC.element_size())            # the advected stack goes back in for the remap
+    d2h = 2 * int(hC.numel() * hC.element_size())
+    e2e_ms = float("nan")
+    if args.e2e_steps > 0:
+        for _ in range(1):                                 # warm-up of the API path (allocator, pinned pool)
+            A = adv.advect_fct(hC, hV0, hV1, hQx, hQy, hok)
+            remap_columns(hhs, A, hht, w.remap_scheme, hwet)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        hc = hC
+        for _ in range(args.e2e_steps):
+            A = adv.advect_fct(hc, hV0, hV1, hQx, hQy, hok)
+            hc = remap_columns(hhs, A, hht, w.remap_scheme, hwet)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        e2e_ms = e0.elapsed_time(e1) / args.e2e_steps
+    if world > 1:
+        t = torch.tensor([e2e_ms], dtype=torch.float64, device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+
+    cells = w.tracer_cells
+    value = cells * args.steps * world / (ms / 1e3)
+    ab = W.algorithmic_bytes(w)
+    pk = peaks()
+    adv_avg, rem_avg = float(np.mean(adv_ms)), float(np.mean(rem_ms))
+    adv_gbs = ab["advect"] / (adv_avg / 1e3) / 1e9
+    rem_gbs = ab["remap"] / (rem_avg / 1e3) / 1e9
+    dominant = ("advect_fct", adv_gbs, adv_avg, ab["advect"]) if adv_avg >= rem_avg else \
+        ("remap_columns", rem_gbs, rem_avg, ab["remap"])
+    line = {
+        "metric": "tracer cell-steps/s at 512^2x50 (advect_fct + PPM_H4 remap, FP64)",
+        "value": value,
+        "unit": "tracer cell-steps/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms / args.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic (seeded basin: Gaussian-bump bathymetry, 15% land, T/S stratification, eddy flow)",
+        "config": {"workload": w.name, "nt": nt, "nz": n, "ny": ny, "nx": nx, "remap": "ppm_h4",
+                   "limiter": "fct", "weno": "z", "l2": "inputs larger than L2 (210 MB stack, 105 MB per "
+                   "geometry array); no flush", "parallelism": f"replicas x{world}"},
+        "roofline": {"bound": "hbm", "kernel": dominant[0], "achieved": dominant[1], "peak": pk["hbm_gbs"],
+                     "unit": "GB/s", "frac": dominant[1] / pk["hbm_gbs"], "peak_source": pk["source"],
+                     "traffic": None, "algorithmic_bytes_per_launch": dominant[3],
+                     "avg_launch_ms": dominant[2],
+                     "parts": {"advect_fct": {"ms": adv_avg, "GB/s": adv_gbs, "bytes": ab["advect"]},
+                               "remap_columns": {"ms": rem_avg, "GB/s": rem_gbs, "bytes": ab["remap"]},
+                               "step": {"ms": ms / args.steps,
+                                        "GB/s": ab["step"] / (ms / args.steps / 1e3) / 1e9}}},
+        "e2e": {"value": cells * world / (e2e_ms / 1e3), "unit": "tracer cell-steps/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms,
+                "api": "TracerAdvection.advect_fct + remap_columns on pinned host tensors"},
+        "gpu_launches": stepper.launches_per_step * args.steps,
+        "clocks": clk,
+    }
+    return line
+
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        w = make_workload(args.workload)
+        s = cpu_sample(w, args.cpu_seconds)
+        line = {"metric": "tracer cell-steps/s at 512^2x50 (advect_fct + PPM_H4 remap, FP64)", "value": s["value"],
+                "unit": "tracer cell-steps/s", "n_gpus": 0, "steps": s["steps"], "warmup": 0,
+                "ms_per_step": 1e3 * s["seconds"] / s["steps"], "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64", "data": "synthetic (same seeded workload)", "impl": "reference",
+                "config": {"workload": w.name}, "cpu_baseline": {k: s[k] for k in
+                                                                 ("value", "unit", "cores", "kind", "sample")},
+                "e2e": {"value": s["value"], "unit": "tracer cell-steps/s", "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return
+    if world > 1:
+        import datetime
+
+        import torch
+        torch.cuda.set_device(local_rank)
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                             device_id=torch.device("cuda", local_rank))
+    line = run_ours(args, rank, world, local_rank)
+    if rank == 0:
+        if not args.no_cpu_baseline and world == 1:
+            s = cpu_sample(make_workload(args.workload), args.cpu_seconds)
+            line["cpu_baseline"] = {k: s[k] for k in ("value", "unit", "cores", "kind", "sample")}
+        print(json.dumps(line))
+    if world > 1:
+        import torch
+        torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,107 @@
+/*
+ * pocean_b200.h — C ABI of libpocean_b200.so, the B200 (sm_100a) implementation of pyOCEAN's baroclinic tracer
+ * hot path: SSP-RK3 WENO5-Z advection with Zalesak FCT, and the conservative ALE vertical remap.
+ *
+ * Conventions shared by every entry point:
+ *   - All array arguments are DEVICE pointers (cudaMalloc / torch CUDA tensors), C-contiguous, k = 0 at the bed:
+ *       tracer stacks (nt, nz, ny, nx) float64; layer geometry (nz, ny, nx) float64;
+ *       u-face arrays (nz, ny, nx+1); v-face arrays (nz, ny+1, nx); `ok` / `wet` one byte per cell (0 or 1).
+ *   - `stream` is a cudaStream_t passed as void* (NULL = the legacy default stream).  Calls are stream-ordered:
+ *     they enqueue kernels and return without synchronising; status codes report argument errors and launch
+ *     failures known at return time.
+ *   - Inputs are never written.  Outputs are fully written.
+ *   - The library allocates no device memory: scratch comes from the caller's `workspace`, sized by the matching
+ *     *_workspace_bytes() query.  A workspace may be reused by consecutive calls on the same stream; calls that
+ *     run concurrently need distinct workspaces.
+ *   - Return value: 0 on success, a POCEAN_E* code otherwise; pocean_last_error() gives the message (per thread).
+ */
+#ifndef POCEAN_B200_H
+#define POCEAN_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define POCEAN_OK 0
+#define POCEAN_EINVAL 1       /* bad sizes, null pointers, unknown flags or scheme */
+#define POCEAN_EWORKSPACE 2   /* workspace missing, misaligned or too small */
+#define POCEAN_ECUDA 3        /* a CUDA launch or API call failed */
+#define POCEAN_EDEVICE 4      /* the current device is not an sm_100 part */
+
+/* Flags of the advection entry points (bitwise OR). */
+#define POCEAN_OPEN_W 0x1u    /* open western edge (ob.open contains "west"), tracers.py:163 */
+#define POCEAN_OPEN_E 0x2u
+#define POCEAN_OPEN_S 0x4u
+#define POCEAN_OPEN_N 0x8u
+#define POCEAN_PERIODIC_X 0x10u /* periodic in x (core/model/periodic.py); u-face nx is u-face 0 */
+#define POCEAN_PERIODIC_Y 0x20u
+#define POCEAN_WENO_JS 0x40u  /* WENO5-JS weights (tracer_scheme != "weno5"); default WENO5-Z */
+#define POCEAN_FCT_UNLIMITED 0x80u /* advect_fct only: no limiter, C_out = the SSP-RK3 result (tracers.py:289-291) */
+
+/* Remap schemes (core/vertical/remap.py:40). */
+#define POCEAN_PCM 0
+#define POCEAN_PLM 1
+#define POCEAN_PPM_H4 2
+
+/* Message of the last failed call on this host thread ("" when none). */
+const char* pocean_last_error(void);
+
+/* Library version as MAJOR*10000 + MINOR*100 + PATCH. */
+int pocean_version(void);
+
+/*
+ * Workspace (bytes) that pocean_advect_fct_f64 needs for this shape.
+ */
+size_t pocean_advect_fct_workspace_bytes(int nt, int nz, int ny, int nx);
+
+/*
+ * One SSP-RK3 WENO5 advection step of the tracer stack C with Zalesak FCT, layer volumes linear from V0 to V1.
+ * Replaces TracerAdvection.advect_fct (core/components/tracers.py:208-254) and the Numba kernels it calls
+ * (_advect_faces_h, _fct_stage, _fct_fluxes, _fct_coeff_kernel, _fct_final in
+ * core/dynamics/sigma_baroclinic.py:265-321, 407-530).
+ *   inflow     (nt, nz, ny, nx) upstream values on open edges during inflow, or NULL: then stage 1 and the donor
+ *              flux use C, and stages 2 and 3 their own values (tracers.py:230-241).
+ *   C_out      (nt, nz, ny, nx) result.
+ *   face_i, fx_face  if fx_face != NULL: the step's effective flux F_L + C·A through u-face column face_i
+ *              (0 <= face_i <= nx), written as (nt, nz, ny) (tracers.py:251-254).
+ *   open_flux  if != NULL: (nt,) net inflow rate through the open edges, Σ_W F − Σ_E F + Σ_S F − Σ_N F of the
+ *              effective flux (tracers.py:65-78, 249-250).  Not defined for an open edge on a periodic axis.
+ */
+int pocean_advect_fct_f64(const double* C, const double* V0, const double* V1, const double* Qx,
+                          const double* Qy, const uint8_t* ok, const double* inflow, int nt, int nz, int ny,
+                          int nx, unsigned flags, double dt, double* C_out, int face_i, double* fx_face,
+                          double* open_flux, void* workspace, size_t workspace_bytes, void* stream);
+
+/*
+ * Workspace (bytes) that pocean_advect_rk3_f64 needs for this shape.
+ */
+size_t pocean_advect_rk3_workspace_bytes(int nt, int nz, int ny, int nx);
+
+/*
+ * One SSP-RK3 step without limiter, WENO5 faces in x, y and z (interface transports Fz (nz+1, ny, nx), or NULL
+ * for none).  Replaces TracerAdvection.advect (core/components/tracers.py:342-375) with _advect_div and _rk_stage
+ * (core/dynamics/sigma_baroclinic.py:324-364, 856-875).  fx_face: (nt, nz, ny) SSP-RK3 combination
+ * (F(c0) + F(c1))/6 + 2F(c2)/3 of the x-face fluxes through column face_i, or NULL.
+ */
+int pocean_advect_rk3_f64(const double* C, const double* V0, const double* V1, const double* Qx,
+                          const double* Qy, const double* Fz, const uint8_t* ok, const double* inflow, int nt,
+                          int nz, int ny, int nx, unsigned flags, double dt, double* C_out, int face_i,
+                          double* fx_face, void* workspace, size_t workspace_bytes, void* stream);
+
+/*
+ * Conservative remap of nfields stacked fields f_src (nfields, n0, ny, nx) from thicknesses h_src (n0, ny, nx)
+ * onto h_tgt (n1, ny, nx); out (nfields, n1, ny, nx).  wet (ny, nx): dry columns are copied when n0 == n1, else
+ * NaN.  scheme: POCEAN_PCM / POCEAN_PLM / POCEAN_PPM_H4.  Replaces core.vertical.remap.remap_columns
+ * (core/vertical/remap.py:400-427; one call per field there) and remap_column (:306-397).  Needs no workspace.
+ */
+int pocean_remap_columns_f64(const double* h_src, const double* f_src, const double* h_tgt, const uint8_t* wet,
+                             int n0, int n1, int ny, int nx, int nfields, int scheme, double* out, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* POCEAN_B200_H */

@@ -1,0 +1,66 @@
+"""ctypes binding of libpocean_b200.so (include/pocean_b200.h).
+
+The CUDA library is the only compute path of this package: there is no CPU fallback.  ``lib()`` raises a
+``RuntimeError`` naming the missing piece when the shared object has not been built or cannot be loaded.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libpocean_b200.so")
+
+# flags and codes of include/pocean_b200.h
+OPEN_W, OPEN_E, OPEN_S, OPEN_N = 0x1, 0x2, 0x4, 0x8
+PERIODIC_X, PERIODIC_Y = 0x10, 0x20
+WENO_JS = 0x40
+FCT_UNLIMITED = 0x80
+PCM, PLM, PPM_H4 = 0, 1, 2
+ERRORS = {1: "invalid argument", 2: "workspace", 3: "CUDA error", 4: "unsupported device"}
+
+# Every symbol the header declares, with its ctypes signature.
+_P, _I, _U, _D, _Z = ctypes.c_void_p, ctypes.c_int, ctypes.c_uint, ctypes.c_double, ctypes.c_size_t
+SIGNATURES: dict[str, tuple] = {
+    "pocean_last_error": (ctypes.c_char_p, []),
+    "pocean_version": (_I, []),
+    "pocean_advect_fct_workspace_bytes": (_Z, [_I, _I, _I, _I]),
+    "pocean_advect_fct_f64": (_I, [_P, _P, _P, _P, _P, _P, _P, _I, _I, _I, _I, _U, _D, _P, _I, _P, _P, _P, _Z,
+                                   _P]),
+    "pocean_advect_rk3_workspace_bytes": (_Z, [_I, _I, _I, _I]),
+    "pocean_advect_rk3_f64": (_I, [_P, _P, _P, _P, _P, _P, _P, _P, _I, _I, _I, _I, _U, _D, _P, _I, _P, _P, _Z,
+                                   _P]),
+    "pocean_remap_columns_f64": (_I, [_P, _P, _P, _P, _I, _I, _I, _I, _I, _I, _P, _P]),
+}
+
+_LIB: ctypes.CDLL | None = None
+
+
+class PoceanError(RuntimeError):
+    """A libpocean_b200 call returned an error status."""
+
+
+def lib() -> ctypes.CDLL:
+    """The loaded library with typed entry points; raises if it is missing."""
+    global _LIB
+    if _LIB is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is missing: build it with `python -m pyocean_b200.build` "
+                               "(or __graft_entry__.build()); this package has no CPU fallback")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _LIB = L
+    return _LIB
+
+
+def check(rc: int, what: str) -> None:
+    """Raise PoceanError (ValueError for argument errors) when a call returned a non-zero status."""
+    if rc == 0:
+        return
+    msg = lib().pocean_last_error().decode(errors="replace")
+    if rc == 1:
+        raise ValueError(f"{what}: {msg}")
+    raise PoceanError(f"{what}: {ERRORS.get(rc, rc)}: {msg}")

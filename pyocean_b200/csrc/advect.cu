@@ -1,0 +1,693 @@
+// FP64 tracer advection on B200: SSP-RK3 WENO5 with Zalesak FCT (TracerAdvection.advect_fct) and without limiter
+// (TracerAdvection.advect).
+//
+// Reference: core/components/tracers.py:208-254, 342-375 and the Numba kernels of
+// core/dynamics/sigma_baroclinic.py:265-364 (faces, RHS), 407-530 (FCT), 856-875 (RK stage).
+//
+// Design.  The reference runs 9 kernels over ~15 full-size temporaries per FCT step.  Here one step is 5 launches,
+// each a pass over (t, k) planes cut into 32 x 8 cell tiles:
+//   1. stage1   c tile + 3-cell halo -> shared memory; WENO5 x/y faces of the tile (each face once);
+//               q1 = q0 - dt div F0, c1 = safe(q1, Va); F0 kept on the faces (S).
+//   2. stage2   same on c1; q2 = 3/4 q0 + 1/4 (q1 - dt div F1), c2 = safe(q2, Vb); S = (F0 + F1)/6.
+//   3. flux3    F2 on c2; A = S + 2 F2/3 - F_L (donor flux F_L recomputed from C) written over S;
+//               c_L = safe(q0 - dt div F_L, V1) for the tile's cells.
+//   4. coeff    Zalesak R+ / R- per cell from the 7-point (x, y, k +- 1) bounds of C and c_L.
+//   5. final    face coefficients from R of both neighbours; C_out = safe(q0 - dt div(F_L + C A), V1).
+// q0 = V0 C, Va, Vb and F_L are recomputed where needed (one multiply/add each) instead of stored.  Periodic axes
+// wrap natively in every stencil (the reference pads by TRACER_HALO = 13 cells and crops; with the dependency
+// radius of the step, 10 cells, both give the same numbers).  The workspace holds 3 cell stacks and 2 face stacks,
+// reused across passes (q1 -> c_L, c1 -> R+, c2 -> R-, S -> A).
+//
+// Arithmetic: every expression in the reference's order, no FMA contraction (-fmad=false), IEEE division; the
+// results equal the reference's FP64 Numba path bit for bit.
+#include <cstdio>
+
+#include "common.cuh"
+#include "weno.cuh"
+
+namespace po {
+
+constexpr int TI = 32;          // tile width (i, contiguous in memory)
+constexpr int TJ = 8;           // tile height (j)
+constexpr int HALO = 3;         // WENO5 stencil radius
+constexpr int NTHREADS = TI * TJ;
+constexpr int SW = TI + 2 * HALO;   // shared tile row length
+constexpr int SH = TJ + 2 * HALO;   // shared tile rows
+
+struct Flags {
+    bool open_w, open_e, open_s, open_n, per_x, per_y, z;
+    __host__ __device__ explicit Flags(unsigned f)
+        : open_w(f & POCEAN_OPEN_W), open_e(f & POCEAN_OPEN_E), open_s(f & POCEAN_OPEN_S),
+          open_n(f & POCEAN_OPEN_N), per_x(f & POCEAN_PERIODIC_X), per_y(f & POCEAN_PERIODIC_Y),
+          z(!(f & POCEAN_WENO_JS)) {}
+};
+
+// Everything one FCT / RK3 step reads and writes.
+struct StepArgs {
+    Shape s;
+    unsigned flags;
+    double dt;
+    const double* __restrict__ C;
+    const double* __restrict__ V0;
+    const double* __restrict__ V1;
+    const double* __restrict__ Qx;
+    const double* __restrict__ Qy;
+    const double* __restrict__ Fz;      // RK3 only (nullable)
+    const uint8_t* __restrict__ ok;
+    const double* __restrict__ inflow;  // nullable
+    // workspace
+    double* q1;
+    double* c1;
+    double* q2;
+    double* c2;
+    double* Sx;
+    double* Sy;
+    double* tef0;                       // RK3 TEF column accumulators (nt, n, ny)
+    double* tef1;
+    // outputs
+    double* out;
+    int face_i;
+    double* fx_face;
+};
+
+// ---------------------------------------------------------------------------------------------------------------
+// Shared-memory tile of one (t, k) plane of a cell field with a HALO-cell border.  Out-of-domain cells (closed or
+// open edges) get value 0 and validity false, which is the reference's `0 <= i < n and ok[i]` rule; periodic axes
+// wrap.
+struct Tile {
+    double c[SH][SW];
+    uint8_t v[SH][SW];
+    double fx[TJ][TI + 1];      // x-face fluxes, face lf between local cells lf-1 and lf
+    double fy[TJ + 1][TI];      // y-face fluxes
+};
+
+__device__ __forceinline__ void load_tile(Tile& T, const double* __restrict__ cp, const uint8_t* __restrict__ okp,
+                                          const Shape& s, const Flags& fl, int j0, int i0)
+{
+    for (int idx = threadIdx.x; idx < SH * SW; idx += NTHREADS) {
+        const int lj = idx / SW, li = idx - lj * SW;
+        int gj = j0 + lj - HALO, gi = i0 + li - HALO;
+        bool in = true;
+        if (fl.per_x) gi = wrap(gi, s.nx); else in = in && (gi >= 0 && gi < s.nx);
+        if (fl.per_y) gj = wrap(gj, s.ny); else in = in && (gj >= 0 && gj < s.ny);
+        double val = 0.0;
+        uint8_t ok = 0;
+        if (in) {
+            const i64 o = (i64)gj * s.nx + gi;
+            val = cp[o];
+            ok = okp[o];
+        }
+        T.c[lj][li] = val;
+        T.v[lj][li] = ok;
+    }
+}
+
+// Upwind WENO5 value of a face from 6 consecutive tile cells w[0..5] (cells f-3 .. f+2 around face f).
+__device__ __forceinline__ double face_value(const double* w, const uint8_t* v, int step, double q, bool z)
+{
+    if (q >= 0.0)
+        return weno5_value(w[0], w[step], w[2 * step], w[3 * step], w[4 * step], v[0], v[step], v[2 * step],
+                           v[3 * step], v[4 * step], z);
+    return weno5_value(w[5 * step], w[4 * step], w[3 * step], w[2 * step], w[step], v[5 * step], v[4 * step],
+                       v[3 * step], v[2 * step], v[step], z);
+}
+
+// x-face flux Q c_face of global face gf (row gj) at tile position (lj, lf): WENO5 on interior faces, the upstream
+// value on open edges, 0 on closed edges (sigma_baroclinic.py:277-297).  `cg`/`eg`: the plane of c / ext.
+__device__ __forceinline__ double xface_flux(const Tile& T, int lj, int lf, int gj, int gf, int k, const Shape& s,
+                                             const Flags& fl, const double* __restrict__ Qx,
+                                             const double* __restrict__ cg, const double* __restrict__ eg)
+{
+    if (fl.per_x || (gf >= 1 && gf <= s.nx - 1)) {
+        const double q = Qx[s.qx(k, gj, gf == s.nx ? 0 : gf)];
+        if (q == 0.0) return 0.0;
+        return q * face_value(&T.c[lj + HALO][lf], &T.v[lj + HALO][lf], 1, q, fl.z);
+    }
+    const double q = Qx[s.qx(k, gj, gf)];
+    const i64 row = (i64)gj * s.nx;
+    if (gf == 0) return fl.open_w ? q * (q > 0.0 ? eg[row] : cg[row]) : 0.0;
+    return fl.open_e ? q * (q < 0.0 ? eg[row + s.nx - 1] : cg[row + s.nx - 1]) : 0.0;
+}
+
+__device__ __forceinline__ double yface_flux(const Tile& T, int lf, int li, int gf, int gi, int k, const Shape& s,
+                                             const Flags& fl, const double* __restrict__ Qy,
+                                             const double* __restrict__ cg, const double* __restrict__ eg)
+{
+    if (fl.per_y || (gf >= 1 && gf <= s.ny - 1)) {
+        const double q = Qy[s.qy(k, gf == s.ny ? 0 : gf, gi)];
+        if (q == 0.0) return 0.0;
+        return q * face_value(&T.c[lf][li + HALO], &T.v[lf][li + HALO], SW, q, fl.z);
+    }
+    const double q = Qy[s.qy(k, gf, gi)];
+    if (gf == 0) return fl.open_s ? q * (q > 0.0 ? eg[gi] : cg[gi]) : 0.0;
+    const i64 o = (i64)(s.ny - 1) * s.nx + gi;
+    return fl.open_n ? q * (q < 0.0 ? eg[o] : cg[o]) : 0.0;
+}
+
+// All x- and y-face fluxes of the tile into T.fx / T.fy.  Thread (tx, ty) computes the west face of its cell and
+// the south face; threads 0..TJ+TI-1 also compute the east faces of the last column and the north faces of the
+// last row.  Faces outside the domain are skipped.
+__device__ __forceinline__ void tile_faces(Tile& T, const Shape& s, const Flags& fl, int k, int j0, int i0,
+                                           const double* __restrict__ Qx, const double* __restrict__ Qy,
+                                           const double* __restrict__ cg, const double* __restrict__ eg)
+{
+    const int tx = threadIdx.x % TI, ty = threadIdx.x / TI;
+    const int gi = i0 + tx, gj = j0 + ty;
+    if (gj < s.ny && gi <= s.nx) T.fx[ty][tx] = xface_flux(T, ty, tx, gj, gi, k, s, fl, Qx, cg, eg);
+    if (gi < s.nx && gj <= s.ny) T.fy[ty][tx] = yface_flux(T, ty, tx, gj, gi, k, s, fl, Qy, cg, eg);
+    const int e = threadIdx.x;
+    if (e < TJ) {
+        const int r = j0 + e, f = i0 + TI;
+        if (r < s.ny && f <= s.nx) T.fx[e][TI] = xface_flux(T, e, TI, r, f, k, s, fl, Qx, cg, eg);
+    } else if (e < TJ + TI) {
+        const int c = e - TJ, f = j0 + TJ, col = i0 + c;
+        if (col < s.nx && f <= s.ny) T.fy[TJ][c] = yface_flux(T, TJ, c, f, col, k, s, fl, Qy, cg, eg);
+    }
+}
+
+// ---------------------------------------------------------------------------------------------------------------
+// FCT stages 1 and 2 (sigma_baroclinic.py:452-468 with tracers.py:233-240).
+template <int STAGE>
+__global__ void __launch_bounds__(NTHREADS) fct_stage_kernel(StepArgs a)
+{
+    __shared__ Tile T;
+    const Shape s = a.s;
+    const Flags fl(a.flags);
+    const int p = blockIdx.z, t = p / s.n, k = p - t * s.n;
+    const int i0 = blockIdx.x * TI, j0 = blockIdx.y * TJ;
+    const double* cin = STAGE == 1 ? a.C : a.c1;
+    const double* cp = cin + s.cell(t, k, 0, 0);
+    const double* ep = (a.inflow ? a.inflow : cin) + s.cell(t, k, 0, 0);
+    load_tile(T, cp, a.ok + s.geo(k, 0, 0), s, fl, j0, i0);
+    __syncthreads();
+    tile_faces(T, s, fl, k, j0, i0, a.Qx, a.Qy, cp, ep);
+    __syncthreads();
+
+    const int tx = threadIdx.x % TI, ty = threadIdx.x / TI;
+    const int gi = i0 + tx, gj = j0 + ty;
+    if (gi >= s.nx || gj >= s.ny) return;
+    // faces owned by this cell: west and south, plus east / north at the last column / row
+    {
+        const i64 w = s.ux(t, k, gj, gi), so = s.vy(t, k, gj, gi);
+        if (STAGE == 1) {
+            a.Sx[w] = T.fx[ty][tx];
+            a.Sy[so] = T.fy[ty][tx];
+            if (gi == s.nx - 1) a.Sx[w + 1] = T.fx[ty][tx + 1];
+            if (gj == s.ny - 1) a.Sy[so + s.nx] = T.fy[ty + 1][tx];
+        } else {
+            a.Sx[w] = (a.Sx[w] + T.fx[ty][tx]) / 6.0;
+            a.Sy[so] = (a.Sy[so] + T.fy[ty][tx]) / 6.0;
+            if (gi == s.nx - 1) a.Sx[w + 1] = (a.Sx[w + 1] + T.fx[ty][tx + 1]) / 6.0;
+            if (gj == s.ny - 1) a.Sy[so + s.nx] = (a.Sy[so + s.nx] + T.fy[ty + 1][tx]) / 6.0;
+        }
+    }
+    const double d = T.fx[ty][tx + 1] - T.fx[ty][tx] + T.fy[ty + 1][tx] - T.fy[ty][tx];
+    const i64 g = s.geo(k, gj, gi), ci = s.cell(t, k, gj, gi);
+    const double v0 = a.V0[g], v1 = a.V1[g], c0 = a.C[ci];
+    const double q0 = v0 * c0;
+    const double dv = v1 - v0;
+    double q, v;
+    if (STAGE == 1) {
+        q = 0.0 * q0 + 1.0 * (q0 - a.dt * d);
+        v = v0 + dv;
+        a.q1[ci] = q;
+        a.c1[ci] = v > 0.0 ? q / v : c0;
+    } else {
+        q = 0.75 * q0 + 0.25 * (a.q1[ci] - a.dt * d);
+        v = v0 + 0.5 * dv;
+        a.c2[ci] = v > 0.0 ? q / v : c0;
+    }
+}
+
+// Donor-cell flux F_L of x-face gf (sigma_baroclinic.py:486-494; periodic: every face interior, face nx = face 0).
+__device__ __forceinline__ double donor_x(const double* __restrict__ cp, const double* __restrict__ ep,
+                                          const double* __restrict__ Qx, const Shape& s, const Flags& fl, int k,
+                                          int j, int f)
+{
+    const i64 row = (i64)j * s.nx;
+    if (fl.per_x) {
+        const int ff = f == s.nx ? 0 : f;
+        const double q = Qx[s.qx(k, j, ff)];
+        return q * (q >= 0 ? cp[row + wrap(ff - 1, s.nx)] : cp[row + ff]);
+    }
+    const double q = Qx[s.qx(k, j, f)];
+    if (f >= 1 && f <= s.nx - 1) return q * (q >= 0 ? cp[row + f - 1] : cp[row + f]);
+    if (f == 0) return fl.open_w ? q * (q > 0 ? ep[row] : cp[row]) : 0.0;
+    return fl.open_e ? q * (q < 0 ? ep[row + s.nx - 1] : cp[row + s.nx - 1]) : 0.0;
+}
+
+__device__ __forceinline__ double donor_y(const double* __restrict__ cp, const double* __restrict__ ep,
+                                          const double* __restrict__ Qy, const Shape& s, const Flags& fl, int k,
+                                          int f, int i)
+{
+    if (fl.per_y) {
+        const int ff = f == s.ny ? 0 : f;
+        const double q = Qy[s.qy(k, ff, i)];
+        return q * (q >= 0 ? cp[(i64)wrap(ff - 1, s.ny) * s.nx + i] : cp[(i64)ff * s.nx + i]);
+    }
+    const double q = Qy[s.qy(k, f, i)];
+    if (f >= 1 && f <= s.ny - 1) return q * (q >= 0 ? cp[(i64)(f - 1) * s.nx + i] : cp[(i64)f * s.nx + i]);
+    if (f == 0) return fl.open_s ? q * (q > 0 ? ep[i] : cp[i]) : 0.0;
+    const i64 o = (i64)(s.ny - 1) * s.nx + i;
+    return fl.open_n ? q * (q < 0 ? ep[o] : cp[o]) : 0.0;
+}
+
+// Pass 3: F2, antidiffusive flux A = (F0 + F1)/6 + 2 F2/3 - F_L over S, and the low-order solution c_L
+// (sigma_baroclinic.py:471-511 and the _fct_stage call of tracers.py:246).
+__global__ void __launch_bounds__(NTHREADS) fct_flux3_kernel(StepArgs a)
+{
+    __shared__ Tile T;
+    const Shape s = a.s;
+    const Flags fl(a.flags);
+    const int p = blockIdx.z, t = p / s.n, k = p - t * s.n;
+    const int i0 = blockIdx.x * TI, j0 = blockIdx.y * TJ;
+    const double* c2p = a.c2 + s.cell(t, k, 0, 0);
+    const double* e2p = a.inflow ? a.inflow + s.cell(t, k, 0, 0) : c2p;
+    load_tile(T, c2p, a.ok + s.geo(k, 0, 0), s, fl, j0, i0);
+    __syncthreads();
+    tile_faces(T, s, fl, k, j0, i0, a.Qx, a.Qy, c2p, e2p);
+    __syncthreads();
+
+    const int tx = threadIdx.x % TI, ty = threadIdx.x / TI;
+    const int gi = i0 + tx, gj = j0 + ty;
+    if (gi >= s.nx || gj >= s.ny) return;
+    const double* Cp = a.C + s.cell(t, k, 0, 0);
+    const double* eL = a.inflow ? a.inflow + s.cell(t, k, 0, 0) : Cp;
+    const double flw = donor_x(Cp, eL, a.Qx, s, fl, k, gj, gi);
+    const double fle = donor_x(Cp, eL, a.Qx, s, fl, k, gj, gi + 1);
+    const double fls = donor_y(Cp, eL, a.Qy, s, fl, k, gj, gi);
+    const double fln = donor_y(Cp, eL, a.Qy, s, fl, k, gj + 1, gi);
+    {
+        const i64 w = s.ux(t, k, gj, gi), so = s.vy(t, k, gj, gi);
+        a.Sx[w] = (a.Sx[w] + 2.0 * T.fx[ty][tx] / 3.0) - flw;
+        a.Sy[so] = (a.Sy[so] + 2.0 * T.fy[ty][tx] / 3.0) - fls;
+        if (gi == s.nx - 1) a.Sx[w + 1] = (a.Sx[w + 1] + 2.0 * T.fx[ty][tx + 1] / 3.0) - fle;
+        if (gj == s.ny - 1) a.Sy[so + s.nx] = (a.Sy[so + s.nx] + 2.0 * T.fy[ty + 1][tx] / 3.0) - fln;
+    }
+    const double d = fle - flw + fln - fls;
+    const i64 g = s.geo(k, gj, gi), ci = s.cell(t, k, gj, gi);
+    const double v1 = a.V1[g], c0 = a.C[ci];
+    const double q0 = a.V0[g] * c0;
+    const double q = 0.0 * q0 + 1.0 * (q0 - a.dt * d);
+    a.q1[ci] = v1 > 0 ? q / v1 : c0;           // c_L, stored over q1
+}
+
+// Unlimited step (tracers.py:289-291, `unlimited=True`): C_out = safe(q0 - dt div F_H, V1) with the RK3 flux
+// F_H = (F0 + F1)/6 + 2 F2/3; S is read, not modified.
+__global__ void __launch_bounds__(NTHREADS) fct_unlimited_kernel(StepArgs a)
+{
+    __shared__ Tile T;
+    const Shape s = a.s;
+    const Flags fl(a.flags);
+    const int p = blockIdx.z, t = p / s.n, k = p - t * s.n;
+    const int i0 = blockIdx.x * TI, j0 = blockIdx.y * TJ;
+    const double* c2p = a.c2 + s.cell(t, k, 0, 0);
+    const double* e2p = a.inflow ? a.inflow + s.cell(t, k, 0, 0) : c2p;
+    load_tile(T, c2p, a.ok + s.geo(k, 0, 0), s, fl, j0, i0);
+    __syncthreads();
+    tile_faces(T, s, fl, k, j0, i0, a.Qx, a.Qy, c2p, e2p);
+    __syncthreads();
+
+    const int tx = threadIdx.x % TI, ty = threadIdx.x / TI;
+    const int gi = i0 + tx, gj = j0 + ty;
+    if (gi >= s.nx || gj >= s.ny) return;
+    const i64 w = s.ux(t, k, gj, gi), so = s.vy(t, k, gj, gi);
+    const double fw = a.Sx[w] + 2.0 * T.fx[ty][tx] / 3.0;
+    const double fe = a.Sx[w + 1] + 2.0 * T.fx[ty][tx + 1] / 3.0;
+    const double fs = a.Sy[so] + 2.0 * T.fy[ty][tx] / 3.0;
+    const double fn = a.Sy[so + s.nx] + 2.0 * T.fy[ty + 1][tx] / 3.0;
+    if (a.fx_face != nullptr && gi == (a.face_i == s.nx ? s.nx - 1 : a.face_i))
+        a.fx_face[((i64)t * s.n + k) * s.ny + gj] = a.face_i == s.nx ? fe : fw;
+    const double d = fe - fw + fn - fs;
+    const i64 g = s.geo(k, gj, gi), ci = s.cell(t, k, gj, gi);
+    const double v1 = a.V1[g], c0 = a.C[ci];
+    const double q = a.V0[g] * c0 - a.dt * d;
+    a.out[ci] = v1 > 0 ? q / v1 : c0;
+}
+
+// Pass 4: Zalesak R+ / R- (sigma_baroclinic.py:407-432): bounds over the cell, its x / y neighbours and the layers
+// k +- 1 (ok cells), P from the antidiffusive fluxes of the cell's faces, Q from V1 and c_L.
+__global__ void __launch_bounds__(256) fct_coeff_kernel(StepArgs a)
+{
+    const Shape s = a.s;
+    const Flags fl(a.flags);
+    const i64 total = (i64)s.nt * s.n * s.ny * s.nx;
+    const i64 ci = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (ci >= total) return;
+    const int i = (int)(ci % s.nx);
+    const int j = (int)((ci / s.nx) % s.ny);
+    const int k = (int)((ci / s.plane()) % s.n);
+    const int t = (int)(ci / ((i64)s.n * s.plane()));
+    const double* cL = a.q1;
+    double rin = 0.0, rout = 0.0;
+    if (a.ok[s.geo(k, j, i)]) {
+        double cmax = -INFINITY, cmin = INFINITY;
+        const int dk[7] = {0, 0, 0, 0, 0, -1, 1};
+        const int dj[7] = {0, 0, 0, -1, 1, 0, 0};
+        const int di[7] = {0, -1, 1, 0, 0, 0, 0};
+#pragma unroll
+        for (int m = 0; m < 7; ++m) {
+            int kk = k + dk[m], jj = j + dj[m], ii = i + di[m];
+            if (kk < 0 || kk >= s.n) continue;
+            if (fl.per_y) jj = wrap(jj, s.ny); else if (jj < 0 || jj >= s.ny) continue;
+            if (fl.per_x) ii = wrap(ii, s.nx); else if (ii < 0 || ii >= s.nx) continue;
+            if (!a.ok[s.geo(kk, jj, ii)]) continue;
+            const i64 o = s.cell(t, kk, jj, ii);
+            cmax = pmax(pmax(cmax, a.C[o]), cL[o]);
+            cmin = pmin(pmin(cmin, a.C[o]), cL[o]);
+        }
+        const i64 w = s.ux(t, k, j, i), so = s.vy(t, k, j, i);
+        const double axw = a.Sx[w], axe = a.Sx[w + 1], ays = a.Sy[so], ayn = a.Sy[so + s.nx];
+        const double p_in = a.dt * (pmax(axw, 0.0) - pmin(axe, 0.0) + pmax(ays, 0.0) - pmin(ayn, 0.0));
+        const double p_out = a.dt * (pmax(axe, 0.0) - pmin(axw, 0.0) + pmax(ayn, 0.0) - pmin(ays, 0.0));
+        const double v1 = a.V1[s.geo(k, j, i)];
+        const double q_in = pmax(v1 * (cmax - cL[ci]), 0.0);
+        const double q_out = pmax(v1 * (cL[ci] - cmin), 0.0);
+        rin = p_in > 0.0 ? pmin(1.0, q_in / p_in) : 0.0;
+        rout = p_out > 0.0 ? pmin(1.0, q_out / p_out) : 0.0;
+    }
+    a.c1[ci] = rin;            // R+ over c1
+    a.c2[ci] = rout;           // R- over c2
+}
+
+// Face coefficient C of x-face f of row j (sigma_baroclinic.py:435-442): min(R+ downstream, R- upstream) by the
+// sign of A; 0 on the domain edges unless periodic.
+__device__ __forceinline__ double coef_x(const StepArgs& a, const Shape& s, const Flags& fl, int t, int k, int j,
+                                         int f, double A)
+{
+    int l = f - 1, r = f;
+    if (fl.per_x) { l = wrap(l, s.nx); r = wrap(r, s.nx); }
+    else if (f < 1 || f > s.nx - 1) return 0.0;
+    const i64 ol = s.cell(t, k, j, l), orr = s.cell(t, k, j, r);
+    return A >= 0.0 ? pmin(a.c1[orr], a.c2[ol]) : pmin(a.c1[ol], a.c2[orr]);
+}
+
+__device__ __forceinline__ double coef_y(const StepArgs& a, const Shape& s, const Flags& fl, int t, int k, int f,
+                                         int i, double A)
+{
+    int l = f - 1, r = f;
+    if (fl.per_y) { l = wrap(l, s.ny); r = wrap(r, s.ny); }
+    else if (f < 1 || f > s.ny - 1) return 0.0;
+    const i64 ol = s.cell(t, k, l, i), orr = s.cell(t, k, r, i);
+    return A >= 0.0 ? pmin(a.c1[orr], a.c2[ol]) : pmin(a.c1[ol], a.c2[orr]);
+}
+
+// Pass 5: C_out = safe(q0 - dt div(F_L + C A), V1) (sigma_baroclinic.py:514-530); optional TEF column.
+__global__ void __launch_bounds__(256) fct_final_kernel(StepArgs a)
+{
+    const Shape s = a.s;
+    const Flags fl(a.flags);
+    const i64 total = (i64)s.nt * s.n * s.ny * s.nx;
+    const i64 ci = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (ci >= total) return;
+    const int i = (int)(ci % s.nx);
+    const int j = (int)((ci / s.nx) % s.ny);
+    const int k = (int)((ci / s.plane()) % s.n);
+    const int t = (int)(ci / ((i64)s.n * s.plane()));
+    const double* Cp = a.C + s.cell(t, k, 0, 0);
+    const double* eL = a.inflow ? a.inflow + s.cell(t, k, 0, 0) : Cp;
+    const i64 w = s.ux(t, k, j, i), so = s.vy(t, k, j, i);
+    const double axw = a.Sx[w], axe = a.Sx[w + 1], ays = a.Sy[so], ayn = a.Sy[so + s.nx];
+    const double fw = donor_x(Cp, eL, a.Qx, s, fl, k, j, i) + coef_x(a, s, fl, t, k, j, i, axw) * axw;
+    const double fe = donor_x(Cp, eL, a.Qx, s, fl, k, j, i + 1) + coef_x(a, s, fl, t, k, j, i + 1, axe) * axe;
+    const double fs = donor_y(Cp, eL, a.Qy, s, fl, k, j, i) + coef_y(a, s, fl, t, k, j, i, ays) * ays;
+    const double fn = donor_y(Cp, eL, a.Qy, s, fl, k, j + 1, i) + coef_y(a, s, fl, t, k, j + 1, i, ayn) * ayn;
+    const double d = fe - fw + fn - fs;
+    const i64 g = s.geo(k, j, i);
+    const double c0 = a.C[ci], v1 = a.V1[g];
+    const double q = a.V0[g] * c0 - a.dt * d;
+    a.out[ci] = v1 > 0 ? q / v1 : c0;
+}
+
+// Effective flux F_L + C A of the step through u-face column face_i, (nt, n, ny) (tracers.py:251-254).
+__global__ void fct_tef_kernel(StepArgs a)
+{
+    const Shape s = a.s;
+    const Flags fl(a.flags);
+    const i64 total = (i64)s.nt * s.n * s.ny;
+    const i64 r = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= total) return;
+    const int j = (int)(r % s.ny);
+    const int k = (int)((r / s.ny) % s.n);
+    const int t = (int)(r / ((i64)s.n * s.ny));
+    const double* Cp = a.C + s.cell(t, k, 0, 0);
+    const double* eL = a.inflow ? a.inflow + s.cell(t, k, 0, 0) : Cp;
+    const double A = a.Sx[s.ux(t, k, j, a.face_i)];
+    a.fx_face[r] = donor_x(Cp, eL, a.Qx, s, fl, k, j, a.face_i) + coef_x(a, s, fl, t, k, j, a.face_i, A) * A;
+}
+
+// Net inflow through the open edges per tracer (tracers.py:65-78): one block per tracer, a fixed-order reduction
+// so that the result does not change from run to run.
+__global__ void __launch_bounds__(256) fct_open_flux_kernel(StepArgs a, double* open_flux)
+{
+    __shared__ double red[256];
+    const Shape s = a.s;
+    const Flags fl(a.flags);
+    const int t = blockIdx.x;
+    double acc = 0.0;
+    const i64 nxe = (i64)s.n * s.ny, nye = (i64)s.n * s.nx;
+    for (i64 r = threadIdx.x; r < nxe; r += blockDim.x) {
+        const int j = (int)(r % s.ny), k = (int)(r / s.ny);
+        const double* Cp = a.C + s.cell(t, k, 0, 0);
+        const double* eL = a.inflow ? a.inflow + s.cell(t, k, 0, 0) : Cp;
+        if (fl.open_w) {
+            const double A = a.Sx[s.ux(t, k, j, 0)];
+            acc += donor_x(Cp, eL, a.Qx, s, fl, k, j, 0) + coef_x(a, s, fl, t, k, j, 0, A) * A;
+        }
+        if (fl.open_e) {
+            const double A = a.Sx[s.ux(t, k, j, s.nx)];
+            acc -= donor_x(Cp, eL, a.Qx, s, fl, k, j, s.nx) + coef_x(a, s, fl, t, k, j, s.nx, A) * A;
+        }
+    }
+    for (i64 r = threadIdx.x; r < nye; r += blockDim.x) {
+        const int i = (int)(r % s.nx), k = (int)(r / s.nx);
+        const double* Cp = a.C + s.cell(t, k, 0, 0);
+        const double* eL = a.inflow ? a.inflow + s.cell(t, k, 0, 0) : Cp;
+        if (fl.open_s) {
+            const double A = a.Sy[s.vy(t, k, 0, i)];
+            acc += donor_y(Cp, eL, a.Qy, s, fl, k, 0, i) + coef_y(a, s, fl, t, k, 0, i, A) * A;
+        }
+        if (fl.open_n) {
+            const double A = a.Sy[s.vy(t, k, s.ny, i)];
+            acc -= donor_y(Cp, eL, a.Qy, s, fl, k, s.ny, i) + coef_y(a, s, fl, t, k, s.ny, i, A) * A;
+        }
+    }
+    red[threadIdx.x] = acc;
+    __syncthreads();
+    for (int w = 128; w > 0; w >>= 1) {
+        if (threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) open_flux[t] = red[0];
+}
+
+// ---------------------------------------------------------------------------------------------------------------
+// SSP-RK3 without limiter (tracers.py:342-375): one launch per stage fuses the RHS of _advect_div (x, y and z
+// WENO5 faces) with the stage update of _rk_stage.
+
+// z-face flux through interface kf (between layers kf-1 and kf) of column (j, i): WENO5 in k on the layers of the
+// column, valid cells only, 0 on the bed and surface interfaces (sigma_baroclinic.py:335-353).
+__device__ __forceinline__ double zface_flux(const StepArgs& a, const Shape& s, const Flags& fl, const double* cin,
+                                             int t, int kf, int j, int i)
+{
+    if (a.Fz == nullptr || kf < 1 || kf > s.n - 1) return 0.0;
+    const double q = a.Fz[s.geo(kf, j, i)];
+    if (q == 0.0) return 0.0;
+    double w[6];
+    uint8_t v[6];
+#pragma unroll
+    for (int m = 0; m < 6; ++m) {
+        const int kk = kf - 3 + m;
+        const bool in = kk >= 0 && kk < s.n;
+        w[m] = in ? cin[s.cell(t, kk, j, i)] : 0.0;
+        v[m] = in ? a.ok[s.geo(kk, j, i)] : 0;
+    }
+    return q * face_value(w, v, 1, q, fl.z);
+}
+
+template <int STAGE>
+__global__ void __launch_bounds__(NTHREADS) rk3_stage_kernel(StepArgs a)
+{
+    __shared__ Tile T;
+    const Shape s = a.s;
+    const Flags fl(a.flags);
+    const int p = blockIdx.z, t = p / s.n, k = p - t * s.n;
+    const int i0 = blockIdx.x * TI, j0 = blockIdx.y * TJ;
+    const double* cin = STAGE == 1 ? a.C : (STAGE == 2 ? a.c1 : a.c2);
+    const double* cp = cin + s.cell(t, k, 0, 0);
+    const double* ep = (a.inflow ? a.inflow : cin) + s.cell(t, k, 0, 0);
+    load_tile(T, cp, a.ok + s.geo(k, 0, 0), s, fl, j0, i0);
+    __syncthreads();
+    tile_faces(T, s, fl, k, j0, i0, a.Qx, a.Qy, cp, ep);
+    __syncthreads();
+
+    const int tx = threadIdx.x % TI, ty = threadIdx.x / TI;
+    const int gi = i0 + tx, gj = j0 + ty;
+    if (gi >= s.nx || gj >= s.ny) return;
+    if (a.fx_face != nullptr && gi == (a.face_i == s.nx ? s.nx - 1 : a.face_i)) {
+        const int lf = a.face_i == s.nx ? tx + 1 : tx;
+        const double F = T.fx[ty][lf];
+        const i64 r = ((i64)t * s.n + k) * s.ny + gj;
+        if (STAGE == 1) a.tef0[r] = F;
+        else if (STAGE == 2) a.tef1[r] = F;
+        else a.fx_face[r] = (a.tef0[r] + a.tef1[r]) / 6.0 + 2.0 * F / 3.0;
+    }
+    const double fzb = zface_flux(a, s, fl, cin, t, k, gj, gi);
+    const double fzt = zface_flux(a, s, fl, cin, t, k + 1, gj, gi);
+    const double r = -(T.fx[ty][tx + 1] - T.fx[ty][tx] + T.fy[ty + 1][tx] - T.fy[ty][tx] + fzt - fzb);
+    const i64 g = s.geo(k, gj, gi), ci = s.cell(t, k, gj, gi);
+    const double v0 = a.V0[g], v1 = a.V1[g], c0 = a.C[ci];
+    const double q0 = v0 * c0, dv = v1 - v0;
+    double q, v;
+    if (STAGE == 1) {
+        q = q0 + a.dt * r;
+        v = v0 + dv;
+        a.q1[ci] = q;
+        a.c1[ci] = v > 0 ? q / v : c0;
+    } else if (STAGE == 2) {
+        q = 0.75 * q0 + 0.25 * (a.q1[ci] + a.dt * r);
+        v = v0 + 0.5 * dv;
+        a.q2[ci] = q;
+        a.c2[ci] = v > 0 ? q / v : c0;
+    } else {
+        q = q0 / 3.0 + 2.0 / 3.0 * (a.q2[ci] + a.dt * r);
+        a.out[ci] = v1 > 0 ? q / v1 : c0;
+    }
+}
+
+}  // namespace po
+
+// =================================================================================================================
+// C ABI
+using namespace po;
+
+static size_t align_up(size_t b) { return (b + 255) & ~(size_t)255; }
+
+static int check_shape(const char* fn, int nt, int nz, int ny, int nx)
+{
+    if (nt < 1 || nz < 1 || ny < 1 || nx < 1)
+        return pocean_fail(POCEAN_EINVAL, "%s: sizes must be >= 1 (nt=%d nz=%d ny=%d nx=%d)", fn, nt, nz, ny, nx);
+    if ((i64)nt * nz > 65535)
+        return pocean_fail(POCEAN_EINVAL, "%s: nt*nz = %lld exceeds 65535", fn, (long long)nt * nz);
+    return POCEAN_OK;
+}
+
+extern "C" size_t pocean_advect_fct_workspace_bytes(int nt, int nz, int ny, int nx)
+{
+    if (nt < 1 || nz < 1 || ny < 1 || nx < 1) return 0;
+    const size_t cells = (size_t)nt * nz * ny * nx * sizeof(double);
+    const size_t xf = (size_t)nt * nz * ny * (nx + 1) * sizeof(double);
+    const size_t yf = (size_t)nt * nz * (ny + 1) * nx * sizeof(double);
+    return 3 * align_up(cells) + align_up(xf) + align_up(yf);
+}
+
+extern "C" size_t pocean_advect_rk3_workspace_bytes(int nt, int nz, int ny, int nx)
+{
+    if (nt < 1 || nz < 1 || ny < 1 || nx < 1) return 0;
+    const size_t cells = (size_t)nt * nz * ny * nx * sizeof(double);
+    const size_t col = (size_t)nt * nz * ny * sizeof(double);
+    return 4 * align_up(cells) + 2 * align_up(col);
+}
+
+static int common_checks(const char* fn, const void* C, const void* V0, const void* V1, const void* Qx,
+                         const void* Qy, const void* ok, const void* out, int nt, int nz, int ny, int nx,
+                         unsigned flags, int face_i, const void* fx_face, void* ws, size_t ws_bytes, size_t need)
+{
+    int rc = check_shape(fn, nt, nz, ny, nx);
+    if (rc) return rc;
+    if (!C || !V0 || !V1 || !Qx || !Qy || !ok || !out)
+        return pocean_fail(POCEAN_EINVAL, "%s: null input or output pointer", fn);
+    if (flags & ~(unsigned)0xFF) return pocean_fail(POCEAN_EINVAL, "%s: unknown flag bits 0x%x", fn, flags);
+    if (fx_face && (face_i < 0 || face_i > nx))
+        return pocean_fail(POCEAN_EINVAL, "%s: face_i=%d outside 0..nx=%d", fn, face_i, nx);
+    if (!ws || ws_bytes < need)
+        return pocean_fail(POCEAN_EWORKSPACE, "%s: workspace of %zu bytes needed, %zu given", fn, need,
+                           ws ? ws_bytes : (size_t)0);
+    if (((uintptr_t)ws & 255) != 0) return pocean_fail(POCEAN_EWORKSPACE, "%s: workspace not 256-byte aligned", fn);
+    return pocean_check_device();
+}
+
+extern "C" int pocean_advect_fct_f64(const double* C, const double* V0, const double* V1, const double* Qx,
+                                     const double* Qy, const uint8_t* ok, const double* inflow, int nt, int nz,
+                                     int ny, int nx, unsigned flags, double dt, double* C_out, int face_i,
+                                     double* fx_face, double* open_flux, void* workspace, size_t workspace_bytes,
+                                     void* stream)
+{
+    const char* fn = "pocean_advect_fct_f64";
+    int rc = common_checks(fn, C, V0, V1, Qx, Qy, ok, C_out, nt, nz, ny, nx, flags, face_i, fx_face, workspace,
+                           workspace_bytes, pocean_advect_fct_workspace_bytes(nt, nz, ny, nx));
+    if (rc) return rc;
+    if ((flags & POCEAN_FCT_UNLIMITED) && open_flux)
+        return pocean_fail(POCEAN_EINVAL, "%s: open_flux is only defined for the limited step", fn);
+    if (open_flux && (((flags & POCEAN_PERIODIC_X) && (flags & (POCEAN_OPEN_W | POCEAN_OPEN_E))) ||
+                      ((flags & POCEAN_PERIODIC_Y) && (flags & (POCEAN_OPEN_S | POCEAN_OPEN_N)))))
+        return pocean_fail(POCEAN_EINVAL, "%s: open_flux is not defined for an open edge on a periodic axis", fn);
+    cudaStream_t st = (cudaStream_t)stream;
+    StepArgs a{};
+    a.s = Shape{nt, nz, ny, nx};
+    a.flags = flags;
+    a.dt = dt;
+    a.C = C; a.V0 = V0; a.V1 = V1; a.Qx = Qx; a.Qy = Qy; a.Fz = nullptr; a.ok = ok; a.inflow = inflow;
+    char* w = (char*)workspace;
+    const size_t cells = align_up((size_t)nt * nz * ny * nx * sizeof(double));
+    a.q1 = (double*)w; w += cells;
+    a.c1 = (double*)w; w += cells;
+    a.c2 = (double*)w; w += cells;
+    a.Sx = (double*)w; w += align_up((size_t)nt * nz * ny * (nx + 1) * sizeof(double));
+    a.Sy = (double*)w;
+    a.q2 = nullptr; a.tef0 = a.tef1 = nullptr;
+    a.out = C_out; a.face_i = face_i; a.fx_face = fx_face;
+
+    const dim3 grid(ceil_div(nx, TI), ceil_div(ny, TJ), nt * nz);
+    fct_stage_kernel<1><<<grid, NTHREADS, 0, st>>>(a);
+    fct_stage_kernel<2><<<grid, NTHREADS, 0, st>>>(a);
+    if (flags & POCEAN_FCT_UNLIMITED) {
+        if (open_flux) return pocean_fail(POCEAN_EINVAL, "%s: open_flux is only defined for the limited step", fn);
+        fct_unlimited_kernel<<<grid, NTHREADS, 0, st>>>(a);
+        return pocean_check_launch(fn);
+    }
+    fct_flux3_kernel<<<grid, NTHREADS, 0, st>>>(a);
+    const i64 total = (i64)nt * nz * ny * nx;
+    const unsigned nb = (unsigned)((total + 255) / 256);
+    fct_coeff_kernel<<<nb, 256, 0, st>>>(a);
+    fct_final_kernel<<<nb, 256, 0, st>>>(a);
+    if (fx_face) {
+        const i64 rows = (i64)nt * nz * ny;
+        fct_tef_kernel<<<(unsigned)((rows + 127) / 128), 128, 0, st>>>(a);
+    }
+    if (open_flux) fct_open_flux_kernel<<<nt, 256, 0, st>>>(a, open_flux);
+    return pocean_check_launch(fn);
+}
+
+extern "C" int pocean_advect_rk3_f64(const double* C, const double* V0, const double* V1, const double* Qx,
+                                     const double* Qy, const double* Fz, const uint8_t* ok, const double* inflow,
+                                     int nt, int nz, int ny, int nx, unsigned flags, double dt, double* C_out,
+                                     int face_i, double* fx_face, void* workspace, size_t workspace_bytes,
+                                     void* stream)
+{
+    const char* fn = "pocean_advect_rk3_f64";
+    int rc = common_checks(fn, C, V0, V1, Qx, Qy, ok, C_out, nt, nz, ny, nx, flags, face_i, fx_face, workspace,
+                           workspace_bytes, pocean_advect_rk3_workspace_bytes(nt, nz, ny, nx));
+    if (rc) return rc;
+    cudaStream_t st = (cudaStream_t)stream;
+    StepArgs a{};
+    a.s = Shape{nt, nz, ny, nx};
+    a.flags = flags;
+    a.dt = dt;
+    a.C = C; a.V0 = V0; a.V1 = V1; a.Qx = Qx; a.Qy = Qy; a.Fz = Fz; a.ok = ok; a.inflow = inflow;
+    char* w = (char*)workspace;
+    const size_t cells = align_up((size_t)nt * nz * ny * nx * sizeof(double));
+    a.q1 = (double*)w; w += cells;
+    a.c1 = (double*)w; w += cells;
+    a.q2 = (double*)w; w += cells;
+    a.c2 = (double*)w; w += cells;
+    a.tef0 = (double*)w; w += align_up((size_t)nt * nz * ny * sizeof(double));
+    a.tef1 = (double*)w;
+    a.Sx = a.Sy = nullptr;
+    a.out = C_out; a.face_i = face_i; a.fx_face = fx_face;
+    const dim3 grid(ceil_div(nx, TI), ceil_div(ny, TJ), nt * nz);
+    rk3_stage_kernel<1><<<grid, NTHREADS, 0, st>>>(a);
+    rk3_stage_kernel<2><<<grid, NTHREADS, 0, st>>>(a);
+    rk3_stage_kernel<3><<<grid, NTHREADS, 0, st>>>(a);
+    return pocean_check_launch(fn);
+}

@@ -1,0 +1,54 @@
+"""
+A resident ALE tracer step on one GPU: ``advect_fct`` of the stack followed by the remap of every member, with
+every buffer allocated once.
+
+This is the device-resident form of the reference's phases 7 and 8 (core/model/driver.py:888-985: the tracer
+advection of the stack, then ``ALECoordinate.regrid_remap`` remapping each stack member,
+core/components/vertical_coordinate.py:69-78).  All arrays are CUDA tensors; calls are stream-ordered and never
+synchronise, so a sequence of steps can be timed with events or captured in a CUDA graph.
+"""
+from __future__ import annotations
+
+import torch
+
+from . import _lib
+
+
+class ALETracerStep:
+    """advect_fct + PPM_H4 (or PCM / PLM) remap of a (nt, N, ny, nx) stack with preallocated buffers."""
+
+    def __init__(self, nt: int, n: int, ny: int, nx: int, dt: float, flags: int = 0, remap_scheme: int = 2,
+                 n_tgt: int | None = None, device=None) -> None:
+        self.nt, self.n, self.ny, self.nx = nt, n, ny, nx
+        self.n1 = n if n_tgt is None else n_tgt
+        self.dt, self.flags, self.remap_scheme = float(dt), int(flags), int(remap_scheme)
+        self.device = torch.device("cuda", torch.cuda.current_device()) if device is None else torch.device(device)
+        L = _lib.lib()
+        self.ws_bytes = L.pocean_advect_fct_workspace_bytes(nt, n, ny, nx)
+        self.ws = torch.empty(self.ws_bytes, dtype=torch.uint8, device=self.device)
+        self.adv_out = torch.empty((nt, n, ny, nx), dtype=torch.float64, device=self.device)
+        self.launches_per_step = 6      # 5 FCT passes + 1 remap
+
+    def stream(self) -> int:
+        return torch.cuda.current_stream(self.device).cuda_stream
+
+    def advect(self, C, V0, V1, Qx, Qy, ok, out=None, inflow=None) -> torch.Tensor:
+        out = self.adv_out if out is None else out
+        rc = _lib.lib().pocean_advect_fct_f64(C.data_ptr(), V0.data_ptr(), V1.data_ptr(), Qx.data_ptr(),
+                                              Qy.data_ptr(), ok.data_ptr(),
+                                              None if inflow is None else inflow.data_ptr(), self.nt, self.n,
+                                              self.ny, self.nx, self.flags, self.dt, out.data_ptr(), 0, None, None,
+                                              self.ws.data_ptr(), self.ws_bytes, self.stream())
+        _lib.check(rc, "advect_fct")
+        return out
+
+    def remap(self, h_src, f, h_tgt, wet, out) -> torch.Tensor:
+        rc = _lib.lib().pocean_remap_columns_f64(h_src.data_ptr(), f.data_ptr(), h_tgt.data_ptr(), wet.data_ptr(),
+                                                 self.n, self.n1, self.ny, self.nx, self.nt, self.remap_scheme,
+                                                 out.data_ptr(), self.stream())
+        _lib.check(rc, "remap_columns")
+        return out
+
+    def step(self, C, V0, V1, Qx, Qy, ok, h_src, h_tgt, wet, out) -> torch.Tensor:
+        """out = remap(advect_fct(C)); ``out`` must not alias ``C``."""
+        return self.remap(h_src, self.advect(C, V0, V1, Qx, Qy, ok), h_tgt, wet, out)

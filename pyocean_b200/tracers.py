@@ -1,0 +1,157 @@
+"""
+``TracerAdvection`` with the reference's interface (core/components/tracers.py:50-375), computed on the GPU.
+
+Drop-in use: construct it like the reference's component (``scheme``, ``time``, ``dt``, ``ob``), set ``per`` to the
+model's periodic axes, and call ``advect_fct`` (ALE step with Zalesak FCT) or ``advect`` (SSP-RK3 without limiter).
+Arrays are NumPy (copied to the GPU and back) or CUDA torch tensors (used in place, results stay on the device).
+Inputs are never modified; results are new arrays, as in the reference.
+
+What the reference offers and this class does not: the ``'pc'`` predictor-corrector time stepping and the
+non-WENO face schemes of ``advect`` (``upwind3`` / ``upwind1`` / centred faces) — both run the reference's NumPy
+path, not its compiled hot path — raise ``NotImplementedError``.  ``advect_fct`` uses WENO5-Z for
+``scheme='weno5'`` and WENO5-JS otherwise, exactly as the reference's fused path does (tracers.py:176).
+"""
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._device import Converter, shape_of
+from .periodic import NONE
+
+
+class OpenEdges:
+    """Minimal open-boundary descriptor: ``open`` is a tuple of edge names ('west', 'east', 'south', 'north')."""
+
+    def __init__(self, open_=()) -> None:
+        self.open = tuple(open_)
+
+
+class TracerAdvection:
+    """SSP-RK3 WENO5 tracer advection (with Zalesak FCT in ``advect_fct``) on frozen transports, on B200."""
+
+    name = "tracer_advection"
+    reads = ("T", "tr", "Qx", "Qy", "Fz")
+    writes = ("T", "tr")
+    per = NONE
+
+    def __init__(self, *, scheme: str, time: str, dt: float, ob=None) -> None:
+        self.tracer_scheme, self.tracer_time, self.dt = scheme, time, dt
+        self.ob = ob if ob is not None else OpenEdges()
+        self.record_open_flux = False
+        self.last_open_flux: np.ndarray | None = None
+
+    # ------------------------------------------------------------------------------------------------ helpers
+    def _flags(self) -> int:
+        opn = tuple(getattr(self.ob, "open", ()) or ())
+        f = 0
+        f |= _lib.OPEN_W if "west" in opn else 0
+        f |= _lib.OPEN_E if "east" in opn else 0
+        f |= _lib.OPEN_S if "south" in opn else 0
+        f |= _lib.OPEN_N if "north" in opn else 0
+        per = self.per
+        f |= _lib.PERIODIC_X if getattr(per, "x", False) else 0
+        f |= _lib.PERIODIC_Y if getattr(per, "y", False) else 0
+        f |= 0 if self.tracer_scheme == "weno5" else _lib.WENO_JS
+        return f
+
+    @staticmethod
+    def _shapes(C, Qx, Qy):
+        shp = shape_of(C)
+        if len(shp) != 4:
+            raise ValueError(f"tracer stack must be (ntr, N, ny, nx), got {shp}")
+        nt, n, ny, nx = shp
+        if shape_of(Qx) != (n, ny, nx + 1) or shape_of(Qy) != (n, ny + 1, nx):
+            raise ValueError(f"transports {shape_of(Qx)}/{shape_of(Qy)} do not match the stack {shp}")
+        return nt, n, ny, nx
+
+    # ------------------------------------------------------------------------------------------------ FCT
+    def advect_fct(self, C, V0, V1, Qx, Qy, ok, unlimited: bool = False, inflow=None, flux_face_i: int | None = None):
+        """
+        SSP-RK3 WENO5 step of the stack C (ntr, N, ny, nx) with Zalesak FCT (tracers.py:208-254).
+        ``unlimited``: the plain RK3 result (C = 1).  ``inflow``: exterior values used on open edges during
+        inflow (None: the stages' own values).  ``flux_face_i``: also return the step's effective flux through
+        u-face column i, (ntr, N, ny).  With ``record_open_flux`` the net inflow rate per stack member through the
+        open edges is left in ``last_open_flux`` (limited step only).
+        """
+        nt, n, ny, nx = self._shapes(C, Qx, Qy)
+        if shape_of(V0) != (n, ny, nx) or shape_of(V1) != (n, ny, nx):
+            raise ValueError(f"volume shape {shape_of(V0)}/{shape_of(V1)} vs tracer layers {(n, ny, nx)}")
+        cv = Converter(C, V0, V1, Qx, Qy, ok, inflow)
+        # tracers.py:230-231: an inflow stack that *is* C means "no exterior values" (each stage its own)
+        own = inflow is None or (inflow is C and (isinstance(C, torch.Tensor) or
+                                                  (isinstance(C, np.ndarray) and C.dtype == np.float64 and
+                                                   C.flags.c_contiguous)))
+        Cd = cv.f64(C)
+        V0d, V1d, Qxd, Qyd = cv.f64(V0), cv.f64(V1), cv.f64(Qx), cv.f64(Qy)
+        okd = cv.u8(ok, (n, ny, nx))
+        infl = None if own else cv.f64(inflow, (nt, n, ny, nx))
+        out = cv.empty((nt, n, ny, nx))
+        flags = self._flags() | (_lib.FCT_UNLIMITED if unlimited else 0)
+        fx = None
+        if flux_face_i is not None:
+            fi = int(flux_face_i)
+            if fi < 0:
+                fi += nx + 1
+            fx = cv.empty((nt, n, ny))
+        else:
+            fi = 0
+        record = self.record_open_flux and not unlimited
+        of = cv.empty((nt,)) if record else None
+        L = _lib.lib()
+        nbytes = L.pocean_advect_fct_workspace_bytes(nt, n, ny, nx)
+        ws = cv.workspace(nbytes)
+        rc = L.pocean_advect_fct_f64(Cd.data_ptr(), V0d.data_ptr(), V1d.data_ptr(), Qxd.data_ptr(), Qyd.data_ptr(),
+                                     okd.data_ptr(), None if infl is None else infl.data_ptr(), nt, n, ny, nx, flags,
+                                     float(self.dt), out.data_ptr(), fi, None if fx is None else fx.data_ptr(),
+                                     None if of is None else of.data_ptr(), ws.data_ptr(), nbytes, cv.stream())
+        _lib.check(rc, "advect_fct")
+        if record:
+            self.last_open_flux = of.cpu().numpy()
+        if flux_face_i is None:
+            return cv.out(out)
+        return cv.out(out), cv.out(fx)
+
+    # ------------------------------------------------------------------------------------------------ RK3
+    def advect(self, C, V0, V1, Qx, Qy, Fz, ok, inflow=None, flux_face_i: int | None = None):
+        """
+        SSP-RK3 flux-form advection of the stack C with frozen Qx, Qy, Fz (N+1, ny, nx); layer volumes linear from
+        V0 to V1 (tracers.py:342-375).  ``flux_face_i``: also return (F(c0) + F(c1))/6 + 2F(c2)/3 through u-face
+        column i.
+        """
+        if self.tracer_time == "pc":
+            raise NotImplementedError("tracer_time='pc' runs the reference's NumPy path; not implemented on GPU")
+        if not self.tracer_scheme.startswith("weno5"):
+            raise NotImplementedError(f"tracer_scheme={self.tracer_scheme!r}: only the WENO5 schemes are on GPU")
+        nt, n, ny, nx = self._shapes(C, Qx, Qy)
+        if shape_of(V0) != (n, ny, nx) or shape_of(V1) != (n, ny, nx):
+            raise ValueError(f"_advect: volume shape {shape_of(V0)}/{shape_of(V1)} vs tracer layers {(n, ny, nx)}")
+        if Fz is not None and shape_of(Fz) != (n + 1, ny, nx):
+            raise ValueError(f"Fz shape {shape_of(Fz)} vs {(n + 1, ny, nx)}")
+        cv = Converter(C, V0, V1, Qx, Qy, Fz, ok, inflow)
+        Cd = cv.f64(C)
+        V0d, V1d, Qxd, Qyd = cv.f64(V0), cv.f64(V1), cv.f64(Qx), cv.f64(Qy)
+        Fzd = None if Fz is None else cv.f64(Fz)
+        okd = cv.u8(ok, (n, ny, nx))
+        infl = None if inflow is None else cv.f64(inflow, (nt, n, ny, nx))
+        out = cv.empty((nt, n, ny, nx))
+        fx = None
+        fi = 0
+        if flux_face_i is not None:
+            fi = int(flux_face_i)
+            if fi < 0:
+                fi += nx + 1
+            fx = cv.empty((nt, n, ny))
+        L = _lib.lib()
+        nbytes = L.pocean_advect_rk3_workspace_bytes(nt, n, ny, nx)
+        ws = cv.workspace(nbytes)
+        rc = L.pocean_advect_rk3_f64(Cd.data_ptr(), V0d.data_ptr(), V1d.data_ptr(), Qxd.data_ptr(), Qyd.data_ptr(),
+                                     None if Fzd is None else Fzd.data_ptr(), okd.data_ptr(),
+                                     None if infl is None else infl.data_ptr(), nt, n, ny, nx, self._flags(),
+                                     float(self.dt), out.data_ptr(), fi, None if fx is None else fx.data_ptr(),
+                                     ws.data_ptr(), nbytes, cv.stream())
+        _lib.check(rc, "advect")
+        if flux_face_i is None:
+            return cv.out(out)
+        return cv.out(out), cv.out(fx)

@@ -1,0 +1,207 @@
+"""
+Seeded synthetic workloads with the shapes and value distributions of the benchmark configurations.
+
+No dataset is involved: every field is generated from ``numpy.random.default_rng(seed)``.
+
+* ``zstar_box`` — 64 x 64 x 20 z* C-grid, dx = dy = 1 km, 5 m layers, periodic in x, walls in y; one temperature
+  field (10 / 20 degC halves plus N(0, 0.01)); non-divergent flow from a random k^-3 streamfunction scaled to
+  0.5 m/s; dt at CFL 0.4; PPM_H4 remap each step from thicknesses perturbed by +-20 % back to the z* grid.
+* ``basin`` — 512 x 512 x 50 curvilinear basin (2 km spacing with a smooth +-5 % perturbation), Gaussian-bump
+  bathymetry in [50, 4000] m with ~15 % land, T (25 -> 4 degC) and S (34 -> 35 psu) linear in depth plus 1 degC
+  Gaussian eddies, geostrophic-like eddy flow up to 1 m/s, hybrid target grid, remap from thicknesses perturbed by
+  +-30 %.
+
+Transports come from a per-layer transport streamfunction on cell corners that vanishes on every corner touching
+land or a wall, so the discrete divergence of (Qx, Qy) is zero up to round-off and V1 = V0 - dt div Q stays
+positive wherever the column is wet.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+
+import numpy as np
+
+
+@dataclass
+class Workload:
+    name: str
+    C: np.ndarray          # (nt, N, ny, nx) tracer stack
+    V0: np.ndarray         # (N, ny, nx) layer volumes at the start of the step [m3]
+    V1: np.ndarray         # (N, ny, nx) layer volumes at the end of the step [m3]
+    Qx: np.ndarray         # (N, ny, nx+1) [m3 s-1]
+    Qy: np.ndarray         # (N, ny+1, nx)
+    ok: np.ndarray         # (N, ny, nx) bool
+    wet: np.ndarray        # (ny, nx) bool
+    h_tgt: np.ndarray      # (N, ny, nx) target thicknesses of the remap [m]
+    h_src: np.ndarray      # (N, ny, nx) source (Lagrangian) thicknesses of the remap [m]
+    dt: float
+    periodic: tuple = ()
+    open: tuple = ()
+    scheme: str = "weno5"
+    remap_scheme: int = 2
+    meta: dict = field(default_factory=dict)
+
+    @property
+    def shape(self) -> tuple:
+        return self.C.shape
+
+    @property
+    def tracer_cells(self) -> int:
+        return int(np.prod(self.C.shape))
+
+
+def _streamfunction_transports(psi_c: np.ndarray, h: np.ndarray, water: np.ndarray, periodic_x: bool):
+    """
+    Layer transports from a corner streamfunction psi_c (ny+1, nx+1) [m2 s-1] scaled by the corner thickness:
+    Qx = -(Psi[j+1, i] - Psi[j, i]), Qy = Psi[j, i+1] - Psi[j, i], Psi_k = psi * h_corner * mask.
+    A corner carries transport only if every cell around it is water (walls and land are closed).
+    """
+    n, ny, nx = h.shape
+    wp = np.pad(water, 1, constant_values=False)
+    hp = np.pad(h, ((0, 0), (1, 1), (1, 1)))
+    if periodic_x:
+        wp[1:-1, 0], wp[1:-1, -1] = water[:, -1], water[:, 0]
+        hp[:, 1:-1, 0], hp[:, 1:-1, -1] = h[:, :, -1], h[:, :, 0]
+    # cells around corner (j, i): (j-1, i-1), (j-1, i), (j, i-1), (j, i) -> padded (j, i), (j, i+1), (j+1, i), (j+1, i+1)
+    m = wp[:-1, :-1] & wp[:-1, 1:] & wp[1:, :-1] & wp[1:, 1:]
+    hc = 0.25 * (hp[:, :-1, :-1] + hp[:, :-1, 1:] + hp[:, 1:, :-1] + hp[:, 1:, 1:])
+    if periodic_x:
+        m[:, -1] = m[:, 0]
+        hc[:, :, -1] = hc[:, :, 0]
+    Psi = psi_c[None] * hc * m[None]
+    Qx = -(Psi[:, 1:, :] - Psi[:, :-1, :])          # (n, ny, nx+1)
+    Qy = Psi[:, :, 1:] - Psi[:, :, :-1]             # (n, ny+1, nx)
+    return Qx, Qy
+
+
+def _smooth_noise(rng, shape, scale: float) -> np.ndarray:
+    """Zero-mean field of unit max amplitude, smooth on ``scale`` cells (sum of random cosine modes)."""
+    ny, nx = shape
+    y, x = np.mgrid[0:ny, 0:nx]
+    out = np.zeros(shape)
+    for _ in range(12):
+        kx, ky = rng.normal(0, 1.0 / scale, 2)
+        out += np.cos(2 * np.pi * (kx * x + ky * y) + rng.uniform(0, 2 * np.pi))
+    return out / np.abs(out).max()
+
+
+def zstar_box(seed: int = 0, nx: int = 64, ny: int = 64, n: int = 20) -> Workload:
+    rng = np.random.default_rng(seed)
+    dx = dy = 1000.0
+    h0 = 5.0
+    h = np.full((n, ny, nx), h0)
+    area = dx * dy
+    # k^-3 streamfunction on corners: walls at j = 0 and j = ny (psi = 0), periodic in x
+    jc = np.arange(ny + 1)[:, None] / ny
+    ic = np.arange(nx + 1)[None, :] / nx
+    psi = np.zeros((ny + 1, nx + 1))
+    for m in range(1, 9):
+        for kk in range(-8, 9):
+            k = np.hypot(m / 2.0, kk)
+            if k == 0:
+                continue
+            psi += k ** -3 * np.sin(np.pi * m * jc) * np.cos(2 * np.pi * kk * ic + rng.uniform(0, 2 * np.pi))
+    psi[:, -1] = psi[:, 0]
+    water = np.ones((ny, nx), bool)
+    Qx, Qy = _streamfunction_transports(psi, h, water, periodic_x=True)
+    umax = max(np.abs(Qx).max() / (dy * h0), np.abs(Qy).max() / (dx * h0))
+    scale = 0.5 / umax
+    Qx *= scale
+    Qy *= scale
+    Qx[..., -1] = Qx[..., 0]
+    dt = 0.4 * dx / 0.5
+    V0 = area * h
+    div = Qx[..., 1:] - Qx[..., :-1] + Qy[:, 1:] - Qy[:, :-1]
+    V1 = V0 - dt * div
+    ok = V1 > 0
+    T = np.where(np.arange(nx)[None, None, :] < nx // 2, 10.0, 20.0) + rng.normal(0, 0.01, (n, ny, nx))
+    h_src = h * (1 + rng.uniform(-0.2, 0.2, h.shape))
+    h_src *= h.sum(0) / h_src.sum(0)
+    return Workload("zstar_box_64x64x20", T[None].copy(), V0, V1, Qx, Qy, ok, water, h.copy(), h_src, dt,
+                    periodic=("x",), meta=dict(dx=dx, dy=dy, cfl=0.4, umax=0.5))
+
+
+def hybrid_target(H: np.ndarray, n: int) -> np.ndarray:
+    """Hybrid target thicknesses (n, ny, nx), bed first: z-like 10 m layers near the surface where the depth allows,
+    stretched layers below, sigma in shallow water; zero thickness on land (H = 0)."""
+    ny, nx = H.shape
+    ntop = n // 2
+    top = np.minimum(10.0, H / n)                    # shallow water: sigma
+    rest = np.maximum(H - ntop * top, 0.0)
+    w = np.linspace(2.0, 1.0, n - ntop)              # thicker layers toward the bed
+    w /= w.sum()
+    h = np.empty((n, ny, nx))
+    h[: n - ntop] = w[:, None, None] * rest[None]
+    h[n - ntop:] = top[None]
+    return h
+
+
+def basin(seed: int = 0, nx: int = 512, ny: int = 512, n: int = 50, nt: int = 2) -> Workload:
+    rng = np.random.default_rng(seed)
+    dx = 2000.0 * (1 + 0.05 * _smooth_noise(rng, (ny, nx), 64.0))
+    dy = 2000.0 * (1 + 0.05 * _smooth_noise(rng, (ny, nx), 64.0))
+    area = dx * dy
+    # Gaussian-bump bathymetry in [50, 4000] m, land where it is shallowest (~15 %)
+    y, x = np.mgrid[0:ny, 0:nx]
+    bump = np.zeros((ny, nx))
+    for _ in range(40):
+        cx, cy = rng.uniform(0, nx), rng.uniform(0, ny)
+        r = rng.uniform(0.03, 0.15) * nx
+        bump += rng.uniform(-1, 1) * np.exp(-((x - cx) ** 2 + (y - cy) ** 2) / (2 * r * r))
+    bump = (bump - bump.min()) / (bump.max() - bump.min())
+    H = 50.0 + 3950.0 * bump
+    water = H > np.quantile(H, 0.15)
+    water[0, :] = water[-1, :] = water[:, 0] = water[:, -1] = False       # closed basin
+    H = np.where(water, H, 0.0)
+    h = hybrid_target(H, n)
+    # geostrophic-like eddies: streamfunction of Gaussian eddies on corners
+    yc, xc = np.mgrid[0:ny + 1, 0:nx + 1]
+    psi = np.zeros((ny + 1, nx + 1))
+    for _ in range(60):
+        cx, cy = rng.uniform(0, nx), rng.uniform(0, ny)
+        r = rng.uniform(8, 40)
+        psi += rng.uniform(-1, 1) * r * np.exp(-((xc - cx) ** 2 + (yc - cy) ** 2) / (2 * r * r))
+    dyf = np.concatenate([dy[:, :1], 0.5 * (dy[:, 1:] + dy[:, :-1]), dy[:, -1:]], axis=1)
+    dxf = np.concatenate([dx[:1], 0.5 * (dx[1:] + dx[:-1]), dx[-1:]], axis=0)
+    Qx, Qy = _streamfunction_transports(psi, h, water, periodic_x=False)
+    hx = np.concatenate([h[..., :1], 0.5 * (h[..., 1:] + h[..., :-1]), h[..., -1:]], axis=-1)
+    hy = np.concatenate([h[:, :1], 0.5 * (h[:, 1:] + h[:, :-1]), h[:, -1:]], axis=1)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        ux = np.where(hx > 0, np.abs(Qx) / (dyf[None] * hx), 0.0)
+        vy = np.where(hy > 0, np.abs(Qy) / (dxf[None] * hy), 0.0)
+    scale = 1.0 / max(ux.max(), vy.max())
+    Qx *= scale
+    Qy *= scale
+    dt = 0.4 * 2000.0 * 0.95 / 1.0
+    V0 = area[None] * h
+    div = Qx[..., 1:] - Qx[..., :-1] + Qy[:, 1:] - Qy[:, :-1]
+    V1 = V0 - dt * div
+    ok = water[None] & (V1 > 0)
+    # T 25 -> 4 degC and S 34 -> 35 psu linear in depth (bed first), plus 1 degC Gaussian eddies on T
+    zc = np.cumsum(h, axis=0) - 0.5 * h                  # height of the cell centre above the bed
+    depth = H[None] - zc
+    frac = np.where(H[None] > 0, np.clip(depth / 4000.0, 0, 1), 0.0)
+    eddy = np.zeros((ny, nx))
+    for _ in range(30):
+        cx, cy = rng.uniform(0, nx), rng.uniform(0, ny)
+        r = rng.uniform(5, 30)
+        eddy += rng.choice([-1.0, 1.0]) * np.exp(-((x - cx) ** 2 + (y - cy) ** 2) / (2 * r * r))
+    T = 25.0 - 21.0 * frac + np.clip(eddy, -1, 1)[None]
+    S = 34.0 + 1.0 * frac
+    stack = [T, S] + [rng.uniform(0, 1, T.shape) for _ in range(max(0, nt - 2))]
+    C = np.stack(stack[:nt])
+    h_src = h * (1 + rng.uniform(-0.3, 0.3, h.shape))
+    col = h_src.sum(0)
+    h_src *= np.where(col > 0, h.sum(0) / np.where(col > 0, col, 1.0), 0.0)[None]
+    return Workload(f"basin_{nx}x{ny}x{n}_nt{nt}", C, V0, V1, Qx, Qy, ok, water, h, h_src, dt,
+                    meta=dict(land_frac=float(1 - water.mean()), umax=1.0))
+
+
+def algorithmic_bytes(w: Workload) -> dict:
+    """Compulsory HBM bytes of one step (each input read once, each output written once): advect_fct reads C, V0,
+    V1, Qx, Qy, ok and writes C_out; the remap reads h_src, h_tgt, wet, the stack and writes it."""
+    nt, n, ny, nx = w.C.shape
+    cells = n * ny * nx
+    adv = cells * (16 * nt + 8 + 8 + 1) + 8 * n * ny * (nx + 1) + 8 * n * (ny + 1) * nx
+    rem = cells * (16 + 16 * nt) + ny * nx
+    return dict(advect=adv, remap=rem, step=adv + rem)

@@ -1,0 +1,72 @@
+"""The C ABI (include/pocean_b200.h) without a GPU: the library loads, exports every declared symbol, sizes its
+workspaces and rejects bad arguments before touching a device."""
+from __future__ import annotations
+
+import ctypes
+import os
+import re
+
+import pytest
+
+from conftest import ROOT
+from pyocean_b200 import _lib
+
+HEADER = os.path.join(ROOT, "include", "pocean_b200.h")
+
+
+def declared_functions() -> list[str]:
+    text = open(HEADER).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(pocean_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_symbol():
+    L = _lib.lib()
+    names = declared_functions()
+    assert "pocean_advect_fct_f64" in names and "pocean_remap_columns_f64" in names
+    for name in names:
+        assert hasattr(L, name), name
+        assert name in _lib.SIGNATURES, f"{name} has no ctypes signature in pyocean_b200._lib"
+
+
+def test_version_and_workspace_sizes():
+    L = _lib.lib()
+    assert L.pocean_version() >= 100
+    nt, n, ny, nx = 2, 50, 512, 512
+    cells = nt * n * ny * nx * 8
+    fct = L.pocean_advect_fct_workspace_bytes(nt, n, ny, nx)
+    assert 5 * cells <= fct <= 5 * cells + 4 * nt * n * (ny + nx) * 8 + 5 * 256
+    assert L.pocean_advect_fct_workspace_bytes(0, n, ny, nx) == 0
+    assert L.pocean_advect_rk3_workspace_bytes(nt, n, ny, nx) >= 4 * cells
+
+
+def _fct_call(**over):
+    L = _lib.lib()
+    args = dict(C=1, V0=1, V1=1, Qx=1, Qy=1, ok=1, inflow=None, nt=1, nz=2, ny=3, nx=4, flags=0, dt=1.0, out=1,
+                face_i=0, fx=None, of=None, ws=256, wsb=1 << 20, stream=None)
+    args.update(over)
+    return L.pocean_advect_fct_f64(*args.values())
+
+
+def test_argument_errors_are_reported_before_any_device_work():
+    L = _lib.lib()
+    assert _fct_call(nx=0) == 1
+    assert b"sizes" in L.pocean_last_error()
+    assert _fct_call(C=None) == 1
+    assert _fct_call(flags=0x100) == 1
+    assert _fct_call(fx=8, face_i=5) == 1                       # face_i > nx
+    assert _fct_call(ws=None) == 2
+    assert _fct_call(wsb=16) == 2
+    assert _fct_call(ws=264) == 2                               # misaligned workspace
+    assert L.pocean_remap_columns_f64(1, 1, 1, 1, 300, 10, 2, 2, 1, 2, 1, None) == 1
+    assert L.pocean_remap_columns_f64(1, 1, 1, 1, 10, 10, 2, 2, 1, 7, 1, None) == 1
+    with pytest.raises(ValueError):
+        _lib.check(1, "x")
+
+
+def test_package_has_no_cpu_fallback(monkeypatch):
+    # the product path refuses to run without the CUDA library instead of computing on the host
+    monkeypatch.setattr(_lib, "_LIB", None)
+    monkeypatch.setattr(_lib, "LIB_PATH", os.path.join(ROOT, "does-not-exist.so"))
+    with pytest.raises(RuntimeError, match="no CPU fallback"):
+        _lib.lib()
