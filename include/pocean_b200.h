@@ -76,6 +76,22 @@ int pocean_advect_fct_f64(const double* C, const double* V0, const double* V1, c
                           double* open_flux, void* workspace, size_t workspace_bytes, void* stream);
 
 /*
+ * The same FCT step as pocean_advect_fct_f64 for callers that cannot allocate device memory (a host model that
+ * reaches the GPU only through this ABI with no device allocator of its own, or one whose device memory belongs
+ * to a pool that forbids side allocations).  No counterpart in the reference: it is an addition of this library.
+ * It allocates nothing; its scratch is a fixed array of POCEAN_NOALLOC_SCRATCH_BYTES inside the library, held by
+ * every GPU that loads it until the process exits.  Shapes whose pocean_advect_fct_workspace_bytes() exceeds that
+ * size are rejected with POCEAN_EINVAL.  The first call on a device looks up the array's address; make it before
+ * any stream capture.  All calls on a device share the array: calls that overlap on the GPU race, so order them
+ * on one stream.
+ */
+#define POCEAN_NOALLOC_SCRATCH_BYTES (64u << 20)
+int pocean_advect_fct_f64_noalloc(const double* C, const double* V0, const double* V1, const double* Qx,
+                                  const double* Qy, const uint8_t* ok, const double* inflow, int nt, int nz, int ny,
+                                  int nx, unsigned flags, double dt, double* C_out, int face_i, double* fx_face,
+                                  double* open_flux, void* stream);
+
+/*
  * Workspace (bytes) that pocean_advect_rk3_f64 needs for this shape.
  */
 size_t pocean_advect_rk3_workspace_bytes(int nt, int nz, int ny, int nx);
