@@ -4,19 +4,23 @@
 // Reference: core/components/tracers.py:208-254, 342-375 and the Numba kernels of
 // core/dynamics/sigma_baroclinic.py:265-364 (faces, RHS), 407-530 (FCT), 856-875 (RK stage).
 //
-// Design.  The reference runs 9 kernels over ~15 full-size temporaries per FCT step.  Here one step is 5 launches,
-// each a pass over (t, k) planes cut into 32 x 8 cell tiles:
-//   1. stage1   c tile + 3-cell halo -> shared memory; WENO5 x/y faces of the tile (each face once);
-//               q1 = q0 - dt div F0, c1 = safe(q1, Va); F0 kept on the faces (S).
-//   2. stage2   same on c1; q2 = 3/4 q0 + 1/4 (q1 - dt div F1), c2 = safe(q2, Vb); S = (F0 + F1)/6.
-//   3. flux3    F2 on c2; A = S + 2 F2/3 - F_L (donor flux F_L recomputed from C) written over S;
-//               c_L = safe(q0 - dt div F_L, V1) for the tile's cells.
-//   4. coeff    Zalesak R+ / R- per cell from the 7-point (x, y, k +- 1) bounds of C and c_L.
-//   5. final    face coefficients from R of both neighbours; C_out = safe(q0 - dt div(F_L + C A), V1).
-// q0 = V0 C, Va, Vb and F_L are recomputed where needed (one multiply/add each) instead of stored.  Periodic axes
-// wrap natively in every stencil (the reference pads by TRACER_HALO = 13 cells and crops; with the dependency
-// radius of the step, 10 cells, both give the same numbers).  The workspace holds 3 cell stacks and 2 face stacks,
-// reused across passes (q1 -> c_L, c1 -> R+, c2 -> R-, S -> A).
+// Design.  The reference runs 9 kernels over ~15 full-size temporaries per FCT step.  Here one step is 5 launches:
+//   1-3. WENO5 passes (fct_strip.cuh): warps march in j along 31-cell strips of a (t, k) plane; each face is
+//        computed once per stage (32/31 per cell in x, 1 + 1/SEG in y) from a register window (y) and a per-warp
+//        shared-memory row ring (x), without block barriers.
+//        1: F0, c1 = safe(q0 - dt div F0, Va); F0 kept on the faces (S).
+//        2: F1, q1 recomputed from the kept F0 (never stored), c2 = safe(3/4 q0 + 1/4 (q1 - dt div F1), Vb);
+//           T = (F0 + F1)/6.
+//        3: F2, antidiffusive flux A = T + 2 F2/3 - F_L over S (donor flux F_L from C), c_L = safe(q0 - dt div F_L,
+//           V1).
+//   4. coeff  Zalesak R+ / R- per cell from the 7-point (x, y, k +- 1) bounds of C and c_L (tracers looped per
+//             thread: the stencil geometry is read once).
+//   5. final  face coefficients from R of both neighbours; C_out = safe(q0 - dt div(F_L + C A), V1).
+// q0 = V0 C, Va, Vb, q1 and F_L are recomputed where needed instead of stored.  Planes run k-major (the tracers
+// of one layer follow each other) so a layer's geometry is re-read from L2.  Periodic axes wrap natively in every
+// stencil (the reference pads by TRACER_HALO = 13 cells and crops; with the dependency radius of the step, 10
+// cells, both give the same numbers).  Workspace: 3 cell stacks (c1 -> R+, c2 -> R-, c_L) and 4 face stacks
+// (S: F0 -> A, T: (F0 + F1)/6).
 //
 // Arithmetic: every expression in the reference's order, no FMA contraction (-fmad=false), IEEE division; the
 // results equal the reference's FP64 Numba path bit for bit.
@@ -60,8 +64,10 @@ struct StepArgs {
     double* c1;
     double* q2;
     double* c2;
-    double* Sx;
+    double* Sx;                         // FCT: F0, then the antidiffusive flux A
     double* Sy;
+    double* Tx;                         // FCT: (F0 + F1)/6
+    double* Ty;
     double* tef0;                       // RK3 TEF column accumulators (nt, n, ny)
     double* tef1;
     // outputs
@@ -102,26 +108,19 @@ __device__ __forceinline__ void load_tile(Tile& T, const double* __restrict__ cp
     }
 }
 
-// Upwind WENO5 value of a face from 6 consecutive tile cells w[0..5] (cells f-3 .. f+2 around face f).
-__device__ __forceinline__ double face_value(const double* w, const uint8_t* v, int step, double q, bool z)
-{
-    if (q >= 0.0)
-        return weno5_value(w[0], w[step], w[2 * step], w[3 * step], w[4 * step], v[0], v[step], v[2 * step],
-                           v[3 * step], v[4 * step], z);
-    return weno5_value(w[5 * step], w[4 * step], w[3 * step], w[2 * step], w[step], v[5 * step], v[4 * step],
-                       v[3 * step], v[2 * step], v[step], z);
-}
-
 // x-face flux Q c_face of global face gf (row gj) at tile position (lj, lf): WENO5 on interior faces, the upstream
 // value on open edges, 0 on closed edges (sigma_baroclinic.py:277-297).  `cg`/`eg`: the plane of c / ext.
-__device__ __forceinline__ double xface_flux(const Tile& T, int lj, int lf, int gj, int gf, int k, const Shape& s,
-                                             const Flags& fl, const double* __restrict__ Qx,
+typedef double TileC[SW];      // one row of a shared halo tile of values
+typedef uint8_t TileV[SW];     // one row of validity flags
+
+__device__ __forceinline__ double xface_flux(const TileC* tc, const TileV* tv, int lj, int lf, int gj, int gf, int k,
+                                             const Shape& s, const Flags& fl, const double* __restrict__ Qx,
                                              const double* __restrict__ cg, const double* __restrict__ eg)
 {
     if (fl.per_x || (gf >= 1 && gf <= s.nx - 1)) {
         const double q = Qx[s.qx(k, gj, gf == s.nx ? 0 : gf)];
         if (q == 0.0) return 0.0;
-        return q * face_value(&T.c[lj + HALO][lf], &T.v[lj + HALO][lf], 1, q, fl.z);
+        return q * upwind_face_value(&tc[lj + HALO][lf], &tv[lj + HALO][lf], 1, q, fl.z);
     }
     const double q = Qx[s.qx(k, gj, gf)];
     const i64 row = (i64)gj * s.nx;
@@ -129,14 +128,14 @@ __device__ __forceinline__ double xface_flux(const Tile& T, int lj, int lf, int 
     return fl.open_e ? q * (q < 0.0 ? eg[row + s.nx - 1] : cg[row + s.nx - 1]) : 0.0;
 }
 
-__device__ __forceinline__ double yface_flux(const Tile& T, int lf, int li, int gf, int gi, int k, const Shape& s,
-                                             const Flags& fl, const double* __restrict__ Qy,
+__device__ __forceinline__ double yface_flux(const TileC* tc, const TileV* tv, int lf, int li, int gf, int gi, int k,
+                                             const Shape& s, const Flags& fl, const double* __restrict__ Qy,
                                              const double* __restrict__ cg, const double* __restrict__ eg)
 {
     if (fl.per_y || (gf >= 1 && gf <= s.ny - 1)) {
         const double q = Qy[s.qy(k, gf == s.ny ? 0 : gf, gi)];
         if (q == 0.0) return 0.0;
-        return q * face_value(&T.c[lf][li + HALO], &T.v[lf][li + HALO], SW, q, fl.z);
+        return q * upwind_face_value(&tc[lf][li + HALO], &tv[lf][li + HALO], SW, q, fl.z);
     }
     const double q = Qy[s.qy(k, gf, gi)];
     if (gf == 0) return fl.open_s ? q * (q > 0.0 ? eg[gi] : cg[gi]) : 0.0;
@@ -147,78 +146,33 @@ __device__ __forceinline__ double yface_flux(const Tile& T, int lf, int li, int 
 // All x- and y-face fluxes of the tile into T.fx / T.fy.  Thread (tx, ty) computes the west face of its cell and
 // the south face; threads 0..TJ+TI-1 also compute the east faces of the last column and the north faces of the
 // last row.  Faces outside the domain are skipped.
-__device__ __forceinline__ void tile_faces(Tile& T, const Shape& s, const Flags& fl, int k, int j0, int i0,
+__device__ __forceinline__ void tile_faces(const TileC* tc, const TileV* tv, double (*fx)[TI + 1],
+                                           double (*fy)[TI], const Shape& s, const Flags& fl, int k, int j0, int i0,
                                            const double* __restrict__ Qx, const double* __restrict__ Qy,
                                            const double* __restrict__ cg, const double* __restrict__ eg)
 {
     const int tx = threadIdx.x % TI, ty = threadIdx.x / TI;
     const int gi = i0 + tx, gj = j0 + ty;
-    if (gj < s.ny && gi <= s.nx) T.fx[ty][tx] = xface_flux(T, ty, tx, gj, gi, k, s, fl, Qx, cg, eg);
-    if (gi < s.nx && gj <= s.ny) T.fy[ty][tx] = yface_flux(T, ty, tx, gj, gi, k, s, fl, Qy, cg, eg);
+    if (gj < s.ny && gi <= s.nx) fx[ty][tx] = xface_flux(tc, tv, ty, tx, gj, gi, k, s, fl, Qx, cg, eg);
+    if (gi < s.nx && gj <= s.ny) fy[ty][tx] = yface_flux(tc, tv, ty, tx, gj, gi, k, s, fl, Qy, cg, eg);
     const int e = threadIdx.x;
     if (e < TJ) {
         const int r = j0 + e, f = i0 + TI;
-        if (r < s.ny && f <= s.nx) T.fx[e][TI] = xface_flux(T, e, TI, r, f, k, s, fl, Qx, cg, eg);
+        if (r < s.ny && f <= s.nx) fx[e][TI] = xface_flux(tc, tv, e, TI, r, f, k, s, fl, Qx, cg, eg);
     } else if (e < TJ + TI) {
         const int c = e - TJ, f = j0 + TJ, col = i0 + c;
-        if (col < s.nx && f <= s.ny) T.fy[TJ][c] = yface_flux(T, TJ, c, f, col, k, s, fl, Qy, cg, eg);
+        if (col < s.nx && f <= s.ny) fy[TJ][c] = yface_flux(tc, tv, TJ, c, f, col, k, s, fl, Qy, cg, eg);
     }
+}
+
+__device__ __forceinline__ void tile_faces(Tile& T, const Shape& s, const Flags& fl, int k, int j0, int i0,
+                                           const double* __restrict__ Qx, const double* __restrict__ Qy,
+                                           const double* __restrict__ cg, const double* __restrict__ eg)
+{
+    tile_faces(T.c, T.v, T.fx, T.fy, s, fl, k, j0, i0, Qx, Qy, cg, eg);
 }
 
 // ---------------------------------------------------------------------------------------------------------------
-// FCT stages 1 and 2 (sigma_baroclinic.py:452-468 with tracers.py:233-240).
-template <int STAGE>
-__global__ void __launch_bounds__(NTHREADS) fct_stage_kernel(StepArgs a)
-{
-    __shared__ Tile T;
-    const Shape s = a.s;
-    const Flags fl(a.flags);
-    const int p = blockIdx.z, t = p / s.n, k = p - t * s.n;
-    const int i0 = blockIdx.x * TI, j0 = blockIdx.y * TJ;
-    const double* cin = STAGE == 1 ? a.C : a.c1;
-    const double* cp = cin + s.cell(t, k, 0, 0);
-    const double* ep = (a.inflow ? a.inflow : cin) + s.cell(t, k, 0, 0);
-    load_tile(T, cp, a.ok + s.geo(k, 0, 0), s, fl, j0, i0);
-    __syncthreads();
-    tile_faces(T, s, fl, k, j0, i0, a.Qx, a.Qy, cp, ep);
-    __syncthreads();
-
-    const int tx = threadIdx.x % TI, ty = threadIdx.x / TI;
-    const int gi = i0 + tx, gj = j0 + ty;
-    if (gi >= s.nx || gj >= s.ny) return;
-    // faces owned by this cell: west and south, plus east / north at the last column / row
-    {
-        const i64 w = s.ux(t, k, gj, gi), so = s.vy(t, k, gj, gi);
-        if (STAGE == 1) {
-            a.Sx[w] = T.fx[ty][tx];
-            a.Sy[so] = T.fy[ty][tx];
-            if (gi == s.nx - 1) a.Sx[w + 1] = T.fx[ty][tx + 1];
-            if (gj == s.ny - 1) a.Sy[so + s.nx] = T.fy[ty + 1][tx];
-        } else {
-            a.Sx[w] = (a.Sx[w] + T.fx[ty][tx]) / 6.0;
-            a.Sy[so] = (a.Sy[so] + T.fy[ty][tx]) / 6.0;
-            if (gi == s.nx - 1) a.Sx[w + 1] = (a.Sx[w + 1] + T.fx[ty][tx + 1]) / 6.0;
-            if (gj == s.ny - 1) a.Sy[so + s.nx] = (a.Sy[so + s.nx] + T.fy[ty + 1][tx]) / 6.0;
-        }
-    }
-    const double d = T.fx[ty][tx + 1] - T.fx[ty][tx] + T.fy[ty + 1][tx] - T.fy[ty][tx];
-    const i64 g = s.geo(k, gj, gi), ci = s.cell(t, k, gj, gi);
-    const double v0 = a.V0[g], v1 = a.V1[g], c0 = a.C[ci];
-    const double q0 = v0 * c0;
-    const double dv = v1 - v0;
-    double q, v;
-    if (STAGE == 1) {
-        q = 0.0 * q0 + 1.0 * (q0 - a.dt * d);
-        v = v0 + dv;
-        a.q1[ci] = q;
-        a.c1[ci] = v > 0.0 ? q / v : c0;
-    } else {
-        q = 0.75 * q0 + 0.25 * (a.q1[ci] - a.dt * d);
-        v = v0 + 0.5 * dv;
-        a.c2[ci] = v > 0.0 ? q / v : c0;
-    }
-}
-
 // Donor-cell flux F_L of x-face gf (sigma_baroclinic.py:486-494; periodic: every face interior, face nx = face 0).
 __device__ __forceinline__ double donor_x(const double* __restrict__ cp, const double* __restrict__ ep,
                                           const double* __restrict__ Qx, const Shape& s, const Flags& fl, int k,
@@ -252,45 +206,11 @@ __device__ __forceinline__ double donor_y(const double* __restrict__ cp, const d
     return fl.open_n ? q * (q < 0 ? ep[o] : cp[o]) : 0.0;
 }
 
-// Pass 3: F2, antidiffusive flux A = (F0 + F1)/6 + 2 F2/3 - F_L over S, and the low-order solution c_L
-// (sigma_baroclinic.py:471-511 and the _fct_stage call of tracers.py:246).
-__global__ void __launch_bounds__(NTHREADS) fct_flux3_kernel(StepArgs a)
-{
-    __shared__ Tile T;
-    const Shape s = a.s;
-    const Flags fl(a.flags);
-    const int p = blockIdx.z, t = p / s.n, k = p - t * s.n;
-    const int i0 = blockIdx.x * TI, j0 = blockIdx.y * TJ;
-    const double* c2p = a.c2 + s.cell(t, k, 0, 0);
-    const double* e2p = a.inflow ? a.inflow + s.cell(t, k, 0, 0) : c2p;
-    load_tile(T, c2p, a.ok + s.geo(k, 0, 0), s, fl, j0, i0);
-    __syncthreads();
-    tile_faces(T, s, fl, k, j0, i0, a.Qx, a.Qy, c2p, e2p);
-    __syncthreads();
+}  // namespace po
 
-    const int tx = threadIdx.x % TI, ty = threadIdx.x / TI;
-    const int gi = i0 + tx, gj = j0 + ty;
-    if (gi >= s.nx || gj >= s.ny) return;
-    const double* Cp = a.C + s.cell(t, k, 0, 0);
-    const double* eL = a.inflow ? a.inflow + s.cell(t, k, 0, 0) : Cp;
-    const double flw = donor_x(Cp, eL, a.Qx, s, fl, k, gj, gi);
-    const double fle = donor_x(Cp, eL, a.Qx, s, fl, k, gj, gi + 1);
-    const double fls = donor_y(Cp, eL, a.Qy, s, fl, k, gj, gi);
-    const double fln = donor_y(Cp, eL, a.Qy, s, fl, k, gj + 1, gi);
-    {
-        const i64 w = s.ux(t, k, gj, gi), so = s.vy(t, k, gj, gi);
-        a.Sx[w] = (a.Sx[w] + 2.0 * T.fx[ty][tx] / 3.0) - flw;
-        a.Sy[so] = (a.Sy[so] + 2.0 * T.fy[ty][tx] / 3.0) - fls;
-        if (gi == s.nx - 1) a.Sx[w + 1] = (a.Sx[w + 1] + 2.0 * T.fx[ty][tx + 1] / 3.0) - fle;
-        if (gj == s.ny - 1) a.Sy[so + s.nx] = (a.Sy[so + s.nx] + 2.0 * T.fy[ty + 1][tx] / 3.0) - fln;
-    }
-    const double d = fle - flw + fln - fls;
-    const i64 g = s.geo(k, gj, gi), ci = s.cell(t, k, gj, gi);
-    const double v1 = a.V1[g], c0 = a.C[ci];
-    const double q0 = a.V0[g] * c0;
-    const double q = 0.0 * q0 + 1.0 * (q0 - a.dt * d);
-    a.q1[ci] = v1 > 0 ? q / v1 : c0;           // c_L, stored over q1
-}
+#include "fct_strip.cuh"
+
+namespace po {
 
 // Unlimited step (tracers.py:289-291, `unlimited=True`): C_out = safe(q0 - dt div F_H, V1) with the RK3 flux
 // F_H = (F0 + F1)/6 + 2 F2/3; S is read, not modified.
@@ -312,10 +232,10 @@ __global__ void __launch_bounds__(NTHREADS) fct_unlimited_kernel(StepArgs a)
     const int gi = i0 + tx, gj = j0 + ty;
     if (gi >= s.nx || gj >= s.ny) return;
     const i64 w = s.ux(t, k, gj, gi), so = s.vy(t, k, gj, gi);
-    const double fw = a.Sx[w] + 2.0 * T.fx[ty][tx] / 3.0;
-    const double fe = a.Sx[w + 1] + 2.0 * T.fx[ty][tx + 1] / 3.0;
-    const double fs = a.Sy[so] + 2.0 * T.fy[ty][tx] / 3.0;
-    const double fn = a.Sy[so + s.nx] + 2.0 * T.fy[ty + 1][tx] / 3.0;
+    const double fw = a.Tx[w] + div3_exact(2.0 * T.fx[ty][tx]);
+    const double fe = a.Tx[w + 1] + div3_exact(2.0 * T.fx[ty][tx + 1]);
+    const double fs = a.Ty[so] + div3_exact(2.0 * T.fy[ty][tx]);
+    const double fn = a.Ty[so + s.nx] + div3_exact(2.0 * T.fy[ty + 1][tx]);
     if (a.fx_face != nullptr && gi == (a.face_i == s.nx ? s.nx - 1 : a.face_i))
         a.fx_face[((i64)t * s.n + k) * s.ny + gj] = a.face_i == s.nx ? fe : fw;
     const double d = fe - fw + fn - fs;
@@ -327,47 +247,55 @@ __global__ void __launch_bounds__(NTHREADS) fct_unlimited_kernel(StepArgs a)
 
 // Pass 4: Zalesak R+ / R- (sigma_baroclinic.py:407-432): bounds over the cell, its x / y neighbours and the layers
 // k +- 1 (ok cells), P from the antidiffusive fluxes of the cell's faces, Q from V1 and c_L.
-__global__ void __launch_bounds__(256) fct_coeff_kernel(StepArgs a)
+__global__ void __launch_bounds__(NTHREADS) fct_coeff_kernel(StepArgs a)
 {
     const Shape s = a.s;
     const Flags fl(a.flags);
-    const i64 total = (i64)s.nt * s.n * s.ny * s.nx;
-    const i64 ci = (i64)blockIdx.x * blockDim.x + threadIdx.x;
-    if (ci >= total) return;
-    const int i = (int)(ci % s.nx);
-    const int j = (int)((ci / s.nx) % s.ny);
-    const int k = (int)((ci / s.plane()) % s.n);
-    const int t = (int)(ci / ((i64)s.n * s.plane()));
+    const int i = blockIdx.x * TI + threadIdx.x % TI, j = blockIdx.y * TJ + threadIdx.x / TI;
+    const int k = blockIdx.z;
+    if (i >= s.nx || j >= s.ny) return;
     const double* cL = a.q1;
-    double rin = 0.0, rout = 0.0;
-    if (a.ok[s.geo(k, j, i)]) {
-        double cmax = -INFINITY, cmin = INFINITY;
-        const int dk[7] = {0, 0, 0, 0, 0, -1, 1};
-        const int dj[7] = {0, 0, 0, -1, 1, 0, 0};
-        const int di[7] = {0, -1, 1, 0, 0, 0, 0};
+    // the 7-point stencil of the bounds: cell, x / y neighbours, layers k -+ 1 (ok cells only); its geometry is
+    // the same for every tracer
+    const int dk[7] = {0, 0, 0, 0, 0, -1, 1};
+    const int dj[7] = {0, 0, 0, -1, 1, 0, 0};
+    const int di[7] = {0, -1, 1, 0, 0, 0, 0};
+    const bool self_ok = a.ok[s.geo(k, j, i)];
+    int nb[7];
 #pragma unroll
-        for (int m = 0; m < 7; ++m) {
-            int kk = k + dk[m], jj = j + dj[m], ii = i + di[m];
-            if (kk < 0 || kk >= s.n) continue;
-            if (fl.per_y) jj = wrap(jj, s.ny); else if (jj < 0 || jj >= s.ny) continue;
-            if (fl.per_x) ii = wrap(ii, s.nx); else if (ii < 0 || ii >= s.nx) continue;
-            if (!a.ok[s.geo(kk, jj, ii)]) continue;
-            const i64 o = s.cell(t, kk, jj, ii);
-            cmax = pmax(pmax(cmax, a.C[o]), cL[o]);
-            cmin = pmin(pmin(cmin, a.C[o]), cL[o]);
-        }
-        const i64 w = s.ux(t, k, j, i), so = s.vy(t, k, j, i);
-        const double axw = a.Sx[w], axe = a.Sx[w + 1], ays = a.Sy[so], ayn = a.Sy[so + s.nx];
-        const double p_in = a.dt * (pmax(axw, 0.0) - pmin(axe, 0.0) + pmax(ays, 0.0) - pmin(ayn, 0.0));
-        const double p_out = a.dt * (pmax(axe, 0.0) - pmin(axw, 0.0) + pmax(ayn, 0.0) - pmin(ays, 0.0));
-        const double v1 = a.V1[s.geo(k, j, i)];
-        const double q_in = pmax(v1 * (cmax - cL[ci]), 0.0);
-        const double q_out = pmax(v1 * (cL[ci] - cmin), 0.0);
-        rin = p_in > 0.0 ? pmin(1.0, q_in / p_in) : 0.0;
-        rout = p_out > 0.0 ? pmin(1.0, q_out / p_out) : 0.0;
+    for (int m = 0; m < 7; ++m) {
+        int kk = k + dk[m], jj = j + dj[m], ii = i + di[m];
+        bool in = kk >= 0 && kk < s.n;
+        if (fl.per_y) jj = wrap(jj, s.ny); else in = in && jj >= 0 && jj < s.ny;
+        if (fl.per_x) ii = wrap(ii, s.nx); else in = in && ii >= 0 && ii < s.nx;
+        nb[m] = (in && a.ok[s.geo(in ? kk : 0, in ? jj : 0, in ? ii : 0)]) ? (int)(((i64)kk * s.ny + jj) * s.nx + ii) : -1;
     }
-    a.c1[ci] = rin;            // R+ over c1
-    a.c2[ci] = rout;           // R- over c2
+    const double v1 = a.V1[s.geo(k, j, i)];
+    const i64 tstride = (i64)s.n * s.plane();
+    for (int t = 0; t < s.nt; ++t) {
+        const i64 ci = s.cell(t, k, j, i);
+        double rin = 0.0, rout = 0.0;
+        if (self_ok) {
+            double cmax = -INFINITY, cmin = INFINITY;
+#pragma unroll
+            for (int m = 0; m < 7; ++m) {
+                if (nb[m] < 0) continue;
+                const i64 o = (i64)t * tstride + nb[m];
+                cmax = pmax(pmax(cmax, a.C[o]), cL[o]);
+                cmin = pmin(pmin(cmin, a.C[o]), cL[o]);
+            }
+            const i64 w = s.ux(t, k, j, i), so = s.vy(t, k, j, i);
+            const double axw = a.Sx[w], axe = a.Sx[w + 1], ays = a.Sy[so], ayn = a.Sy[so + s.nx];
+            const double p_in = a.dt * (pmax(axw, 0.0) - pmin(axe, 0.0) + pmax(ays, 0.0) - pmin(ayn, 0.0));
+            const double p_out = a.dt * (pmax(axe, 0.0) - pmin(axw, 0.0) + pmax(ayn, 0.0) - pmin(ays, 0.0));
+            const double q_in = pmax(v1 * (cmax - cL[ci]), 0.0);
+            const double q_out = pmax(v1 * (cL[ci] - cmin), 0.0);
+            rin = p_in > 0.0 ? pmin(1.0, q_in / p_in) : 0.0;
+            rout = p_out > 0.0 ? pmin(1.0, q_out / p_out) : 0.0;
+        }
+        a.c1[ci] = rin;            // R+ over c1
+        a.c2[ci] = rout;           // R- over c2
+    }
 }
 
 // Face coefficient C of x-face f of row j (sigma_baroclinic.py:435-442): min(R+ downstream, R- upstream) by the
@@ -392,31 +320,32 @@ __device__ __forceinline__ double coef_y(const StepArgs& a, const Shape& s, cons
     return A >= 0.0 ? pmin(a.c1[orr], a.c2[ol]) : pmin(a.c1[ol], a.c2[orr]);
 }
 
-// Pass 5: C_out = safe(q0 - dt div(F_L + C A), V1) (sigma_baroclinic.py:514-530); optional TEF column.
-__global__ void __launch_bounds__(256) fct_final_kernel(StepArgs a)
+// Pass 5: C_out = safe(q0 - dt div(F_L + C A), V1) (sigma_baroclinic.py:514-530).  One thread per column cell
+// (k, j, i) loops over the tracers, so the geometry is read once and the tracers' loads are independent.
+__global__ void __launch_bounds__(NTHREADS) fct_final_kernel(StepArgs a)
 {
     const Shape s = a.s;
     const Flags fl(a.flags);
-    const i64 total = (i64)s.nt * s.n * s.ny * s.nx;
-    const i64 ci = (i64)blockIdx.x * blockDim.x + threadIdx.x;
-    if (ci >= total) return;
-    const int i = (int)(ci % s.nx);
-    const int j = (int)((ci / s.nx) % s.ny);
-    const int k = (int)((ci / s.plane()) % s.n);
-    const int t = (int)(ci / ((i64)s.n * s.plane()));
-    const double* Cp = a.C + s.cell(t, k, 0, 0);
-    const double* eL = a.inflow ? a.inflow + s.cell(t, k, 0, 0) : Cp;
-    const i64 w = s.ux(t, k, j, i), so = s.vy(t, k, j, i);
-    const double axw = a.Sx[w], axe = a.Sx[w + 1], ays = a.Sy[so], ayn = a.Sy[so + s.nx];
-    const double fw = donor_x(Cp, eL, a.Qx, s, fl, k, j, i) + coef_x(a, s, fl, t, k, j, i, axw) * axw;
-    const double fe = donor_x(Cp, eL, a.Qx, s, fl, k, j, i + 1) + coef_x(a, s, fl, t, k, j, i + 1, axe) * axe;
-    const double fs = donor_y(Cp, eL, a.Qy, s, fl, k, j, i) + coef_y(a, s, fl, t, k, j, i, ays) * ays;
-    const double fn = donor_y(Cp, eL, a.Qy, s, fl, k, j + 1, i) + coef_y(a, s, fl, t, k, j + 1, i, ayn) * ayn;
-    const double d = fe - fw + fn - fs;
+    const int i = blockIdx.x * TI + threadIdx.x % TI, j = blockIdx.y * TJ + threadIdx.x / TI;
+    const int k = blockIdx.z;
+    if (i >= s.nx || j >= s.ny) return;
     const i64 g = s.geo(k, j, i);
-    const double c0 = a.C[ci], v1 = a.V1[g];
-    const double q = a.V0[g] * c0 - a.dt * d;
-    a.out[ci] = v1 > 0 ? q / v1 : c0;
+    const double v0 = __ldg(a.V0 + g), v1 = __ldg(a.V1 + g);
+    for (int t = 0; t < s.nt; ++t) {
+        const i64 ci = s.cell(t, k, j, i);
+        const double* Cp = a.C + s.cell(t, k, 0, 0);
+        const double* eL = a.inflow ? a.inflow + s.cell(t, k, 0, 0) : Cp;
+        const i64 w = s.ux(t, k, j, i), so = s.vy(t, k, j, i);
+        const double axw = a.Sx[w], axe = a.Sx[w + 1], ays = a.Sy[so], ayn = a.Sy[so + s.nx];
+        const double fw = donor_x(Cp, eL, a.Qx, s, fl, k, j, i) + coef_x(a, s, fl, t, k, j, i, axw) * axw;
+        const double fe = donor_x(Cp, eL, a.Qx, s, fl, k, j, i + 1) + coef_x(a, s, fl, t, k, j, i + 1, axe) * axe;
+        const double fs = donor_y(Cp, eL, a.Qy, s, fl, k, j, i) + coef_y(a, s, fl, t, k, j, i, ays) * ays;
+        const double fn = donor_y(Cp, eL, a.Qy, s, fl, k, j + 1, i) + coef_y(a, s, fl, t, k, j + 1, i, ayn) * ayn;
+        const double d = fe - fw + fn - fs;
+        const double c0 = a.C[ci];
+        const double q = v0 * c0 - a.dt * d;
+        a.out[ci] = v1 > 0 ? q / v1 : c0;
+    }
 }
 
 // Effective flux F_L + C A of the step through u-face column face_i, (nt, n, ny) (tracers.py:251-254).
@@ -502,7 +431,7 @@ __device__ __forceinline__ double zface_flux(const StepArgs& a, const Shape& s, 
         w[m] = in ? cin[s.cell(t, kk, j, i)] : 0.0;
         v[m] = in ? a.ok[s.geo(kk, j, i)] : 0;
     }
-    return q * face_value(w, v, 1, q, fl.z);
+    return q * upwind_face_value(w, v, 1, q, fl.z);
 }
 
 template <int STAGE>
@@ -530,7 +459,7 @@ __global__ void __launch_bounds__(NTHREADS) rk3_stage_kernel(StepArgs a)
         const i64 r = ((i64)t * s.n + k) * s.ny + gj;
         if (STAGE == 1) a.tef0[r] = F;
         else if (STAGE == 2) a.tef1[r] = F;
-        else a.fx_face[r] = (a.tef0[r] + a.tef1[r]) / 6.0 + 2.0 * F / 3.0;
+        else a.fx_face[r] = div6_exact(a.tef0[r] + a.tef1[r]) + div3_exact(2.0 * F);
     }
     const double fzb = zface_flux(a, s, fl, cin, t, k, gj, gi);
     const double fzt = zface_flux(a, s, fl, cin, t, k + 1, gj, gi);
@@ -550,7 +479,7 @@ __global__ void __launch_bounds__(NTHREADS) rk3_stage_kernel(StepArgs a)
         a.q2[ci] = q;
         a.c2[ci] = v > 0 ? q / v : c0;
     } else {
-        q = q0 / 3.0 + 2.0 / 3.0 * (a.q2[ci] + a.dt * r);
+        q = div3_exact(q0) + 2.0 / 3.0 * (a.q2[ci] + a.dt * r);
         a.out[ci] = v1 > 0 ? q / v1 : c0;
     }
 }
@@ -569,6 +498,8 @@ static int check_shape(const char* fn, int nt, int nz, int ny, int nx)
         return pocean_fail(POCEAN_EINVAL, "%s: sizes must be >= 1 (nt=%d nz=%d ny=%d nx=%d)", fn, nt, nz, ny, nx);
     if ((i64)nt * nz > 65535)
         return pocean_fail(POCEAN_EINVAL, "%s: nt*nz = %lld exceeds 65535", fn, (long long)nt * nz);
+    if ((i64)nz * (ny + 1) * (nx + 1) >= (1ll << 31))
+        return pocean_fail(POCEAN_EINVAL, "%s: one field of %d x %d x %d cells exceeds 2^31 entries", fn, nz, ny, nx);
     return POCEAN_OK;
 }
 
@@ -578,7 +509,7 @@ extern "C" size_t pocean_advect_fct_workspace_bytes(int nt, int nz, int ny, int 
     const size_t cells = (size_t)nt * nz * ny * nx * sizeof(double);
     const size_t xf = (size_t)nt * nz * ny * (nx + 1) * sizeof(double);
     const size_t yf = (size_t)nt * nz * (ny + 1) * nx * sizeof(double);
-    return 3 * align_up(cells) + align_up(xf) + align_up(yf);
+    return 3 * align_up(cells) + 2 * (align_up(xf) + align_up(yf));
 }
 
 extern "C" size_t pocean_advect_rk3_workspace_bytes(int nt, int nz, int ny, int nx)
@@ -633,24 +564,28 @@ extern "C" int pocean_advect_fct_f64(const double* C, const double* V0, const do
     a.q1 = (double*)w; w += cells;
     a.c1 = (double*)w; w += cells;
     a.c2 = (double*)w; w += cells;
-    a.Sx = (double*)w; w += align_up((size_t)nt * nz * ny * (nx + 1) * sizeof(double));
-    a.Sy = (double*)w;
+    const size_t xf = align_up((size_t)nt * nz * ny * (nx + 1) * sizeof(double));
+    const size_t yf = align_up((size_t)nt * nz * (ny + 1) * nx * sizeof(double));
+    a.Sx = (double*)w; w += xf;
+    a.Sy = (double*)w; w += yf;
+    a.Tx = (double*)w; w += xf;
+    a.Ty = (double*)w;
     a.q2 = nullptr; a.tef0 = a.tef1 = nullptr;
     a.out = C_out; a.face_i = face_i; a.fx_face = fx_face;
 
     const dim3 grid(ceil_div(nx, TI), ceil_div(ny, TJ), nt * nz);
-    fct_stage_kernel<1><<<grid, NTHREADS, 0, st>>>(a);
-    fct_stage_kernel<2><<<grid, NTHREADS, 0, st>>>(a);
+    const int nstrips = ceil_div(nx, STRIP);
+    const dim3 sgrid(ceil_div(nstrips, SWARPS), ceil_div(ny, SEG), nt * nz);
+    fct_strip_kernel<1><<<sgrid, SWARPS * 32, 0, st>>>(a);
+    fct_strip_kernel<2><<<sgrid, SWARPS * 32, 0, st>>>(a);
     if (flags & POCEAN_FCT_UNLIMITED) {
         if (open_flux) return pocean_fail(POCEAN_EINVAL, "%s: open_flux is only defined for the limited step", fn);
         fct_unlimited_kernel<<<grid, NTHREADS, 0, st>>>(a);
         return pocean_check_launch(fn);
     }
-    fct_flux3_kernel<<<grid, NTHREADS, 0, st>>>(a);
-    const i64 total = (i64)nt * nz * ny * nx;
-    const unsigned nb = (unsigned)((total + 255) / 256);
-    fct_coeff_kernel<<<nb, 256, 0, st>>>(a);
-    fct_final_kernel<<<nb, 256, 0, st>>>(a);
+    fct_strip_kernel<3><<<sgrid, SWARPS * 32, 0, st>>>(a);
+    fct_coeff_kernel<<<dim3(ceil_div(nx, TI), ceil_div(ny, TJ), nz), NTHREADS, 0, st>>>(a);
+    fct_final_kernel<<<dim3(ceil_div(nx, TI), ceil_div(ny, TJ), nz), NTHREADS, 0, st>>>(a);
     if (fx_face) {
         const i64 rows = (i64)nt * nz * ny;
         fct_tef_kernel<<<(unsigned)((rows + 127) / 128), 128, 0, st>>>(a);
@@ -683,7 +618,7 @@ extern "C" int pocean_advect_rk3_f64(const double* C, const double* V0, const do
     a.c2 = (double*)w; w += cells;
     a.tef0 = (double*)w; w += align_up((size_t)nt * nz * ny * sizeof(double));
     a.tef1 = (double*)w;
-    a.Sx = a.Sy = nullptr;
+    a.Sx = a.Sy = a.Tx = a.Ty = nullptr;
     a.out = C_out; a.face_i = face_i; a.fx_face = fx_face;
     const dim3 grid(ceil_div(nx, TI), ceil_div(ny, TJ), nt * nz);
     rk3_stage_kernel<1><<<grid, NTHREADS, 0, st>>>(a);

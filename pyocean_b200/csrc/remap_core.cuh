@@ -8,14 +8,16 @@
 //                        overlaps (two passes over those targets: the first finds the thickest piece, the second
 //                        accumulates the others and gives the thickest the residual, remap.py:359-366).  No column
 //                        array is stored; finished targets are written as the sweep passes them.
-//   remap_column_general the reference's array formulation (column arrays in thread-local memory), used for the
-//                        columns the sweep cannot take in one pass: a target thickness that is negative or NaN.
-// Both evaluate every expression in the reference's order; compiled without FMA contraction they give the
+// The sweep needs non-negative target thicknesses (a vanished target then sits in the cell that passes it); the
+// kernel sends a column with a negative or NaN target thickness to the reference's array formulation instead.
+// Every expression is evaluated in the reference's order; compiled without FMA contraction the results are the
 // reference's numbers bit for bit.
 #pragma once
 
 #include <math.h>
 #include <stdint.h>
+
+#include "exactdiv.cuh"
 
 #ifdef __CUDACC__
 #define PO_HD __host__ __device__ __forceinline__
@@ -44,11 +46,14 @@ PO_HD int effective_scheme(int n_active, int scheme)          // remap.py:46-53
     return scheme;
 }
 
-PO_HD double plm_slope(double h_l, double h_c, double h_r, double u_l, double u_c, double u_r)   // remap.py:59-80
+// Thickness factor h_c / (h_l + 2 h_c + h_r + h_neglect) of the PLM slope, shared by every field of a column.
+PO_HD double plm_ratio(double h_l, double h_c, double h_r) { return h_c / (h_l + 2.0 * h_c + h_r + H_NEGLECT); }
+
+PO_HD double plm_slope(double ratio, double u_l, double u_c, double u_r)   // remap.py:59-80
 {
     const double sigma_r = u_r - u_c;
     const double sigma_l = u_c - u_l;
-    const double sigma_c = 2.0 * (u_r - u_l) * (h_c / (h_l + 2.0 * h_c + h_r + H_NEGLECT));
+    const double sigma_c = 2.0 * (u_r - u_l) * ratio;
     const double u_min = pmin(pmin(u_l, u_c), u_r);
     const double u_max = pmax(pmax(u_l, u_c), u_r);
     double slope = 0.0;
@@ -173,13 +178,28 @@ PO_HD double h4_edge(const H4Weights& w, double u0, double u1, double u2, double
     return (et1 + (et2 + et3)) / w.den;
 }
 
-// Limited slope of bound_edges for cell k with neighbours km1 / kp1 (remap.py:203-213).
-PO_HD double bound_slope(double h_m, double h_c, double h_p, double u_m, double u_c, double u_p)
+// Thickness part of bound_edges' slope for cell k with neighbours km1 / kp1 (remap.py:205-207): whether the slope
+// is formed at all, and h_k / ((h_km1 + h_kp1) + 2 h_k); shared by every field of a column.
+struct BoundRatio {
+    bool active;
+    double ratio;
+};
+
+PO_HD BoundRatio bound_ratio(double h_m, double h_c, double h_p)
+{
+    BoundRatio b;
+    b.active = (h_m + h_p) + 2.0 * h_c > 0.0;
+    b.ratio = b.active ? h_c / ((h_m + h_p) + 2.0 * h_c) : 0.0;
+    return b;
+}
+
+// Limited slope of bound_edges for cell k (remap.py:203-213).
+PO_HD double bound_slope(const BoundRatio& br, double u_m, double u_c, double u_p)
 {
     double slope_x_h = 0.0;
-    if ((h_m + h_p) + 2.0 * h_c > 0.0) {
+    if (br.active) {
         const double sl = u_c - u_m;
-        const double sc = (u_p - u_m) * (h_c / ((h_m + h_p) + 2.0 * h_c));
+        const double sc = (u_p - u_m) * br.ratio;
         const double sr = u_p - u_c;
         if (sl * sr > 0.0) {
             const double m = pmin(pmin(fabs(sl), fabs(sc)), fabs(sr));
@@ -241,13 +261,16 @@ PO_HD double average(double c0, double c1, double c2, double xa, double xb)     
         const double x = 0.5 * (xa + xb);
         return c0 + x * (c1 + x * c2);
     }
-    return c0 + 0.5 * c1 * (xa + xb) + c2 * (xa * xa + xa * xb + xb * xb) / 3.0;
+    return c0 + 0.5 * c1 * (xa + xb) + div3_exact(c2 * (xa * xa + xa * xb + xb * xb));
 }
 
 // ------------------------------------------------------------------------------------------------------------
 // One-pass column remap.  IO: hs(k), ht(k), f(m, k) loads and put(m, k, v) stores; NF fields share the
-// thickness work.  Preconditions: the column is wet, has at least one active source cell, and every target
-// thickness is >= 0 (the caller routes other columns to remap_column_general).
+// thickness work.  Preconditions: the column is wet, has n_active >= 1 source cells with h > 0 (the last one is
+// `last`), and every target thickness is >= 0 (the caller sends other columns to the general algorithm).
+//
+// Window: slot s holds source cell i - 2 + s (s = 0..5) while cell i is processed; out-of-range slots hold 0 and
+// are never read by the formulas (each use is guarded by its cell range).
 template <int NF, class IO>
 PO_HDT void remap_column_stream(IO& io, int n0, int n1, int scheme, int n_active, int last)
 {
@@ -255,113 +278,109 @@ PO_HDT void remap_column_stream(IO& io, int n0, int n1, int scheme, int n_active
     const bool plm = sch == PLM && n0 >= 3;
     const bool ppm = sch == PPM_H4 && n0 >= 4;
 
-    // window: slot s holds cell i - 2 + s (s = 0..5) of the current step i
     double wh[6];
     double wu[NF][6];
+#pragma unroll
     for (int s = 0; s < 6; ++s) {
         const int k = s - 2;
         const bool in = k >= 0 && k < n0;
         wh[s] = in ? io.hs(k) : 0.0;
+#pragma unroll
         for (int m = 0; m < NF; ++m) wu[m][s] = in ? io.f(m, k) : 0.0;
     }
-    // PLM state: raw slope of cells i-1, i, i+1 and monotonized slope of cells i, i+1 (zeros at the ends)
-    double slp_m1[NF], slp_0[NF], slp_p1[NF], mslp_0[NF], mslp_p1[NF];
-    // PPM state: bounded/checked left edge of cell i, bound slopes of cells i and i+1, raw edge of interface i+1
-    double el_i[NF], sl_i[NF], top_in[NF], top_out[NF];
-    for (int m = 0; m < NF; ++m) {
-        slp_m1[m] = slp_0[m] = slp_p1[m] = mslp_0[m] = mslp_p1[m] = 0.0;
-        el_i[m] = sl_i[m] = top_in[m] = top_out[m] = 0.0;
-    }
+    // PLM: raw slopes of cells i, i+1 and the monotonized slope of cell i (remap.py:248-262; zero at both ends).
+    // PPM: checked left edge of cell i, bound slope of cell i, raw edge of interface i+1, and the top end values.
+    double st_a[NF], st_b[NF], st_c[NF], top_in[NF], top_out[NF];
+#pragma unroll
+    for (int m = 0; m < NF; ++m) st_a[m] = st_b[m] = st_c[m] = top_in[m] = top_out[m] = 0.0;
+    BoundRatio br_i{false, 0.0};
     if (plm) {
-        // slopes of cells 0 (zero), 1; monotonized slope of cell 0 is zero
+        const double r1 = plm_ratio(wh[2], wh[3], wh[4]);          // slope of cell 1 (cells 0, 1, 2)
+#pragma unroll
         for (int m = 0; m < NF; ++m) {
-            slp_0[m] = 0.0;
-            slp_p1[m] = n0 - 1 > 1 ? plm_slope(wh[2], wh[3], wh[4], wu[m][2], wu[m][3], wu[m][4]) : 0.0;
-            mslp_0[m] = 0.0;
+            st_a[m] = 0.0;                                           // slp[0]
+            st_b[m] = plm_slope(r1, wu[m][2], wu[m][3], wu[m][4]);   // slp[1] (n0 >= 3)
+            st_c[m] = 0.0;                                           // mslp[0]
         }
     }
     if (ppm) {
-        // end values: bottom from cells 0..3, top from cells n0-1..n0-4 (thicknesses floored at h_neglect_edge)
         double hb[4], ht4[4];
+#pragma unroll
         for (int q = 0; q < 4; ++q) {
             hb[q] = pmax(H_NEGLECT_EDGE, io.hs(q));
             ht4[q] = pmax(H_NEGLECT_EDGE, io.hs(n0 - 1 - q));
         }
+        br_i = bound_ratio(wh[2], wh[2], wh[3]);                      // cell 0: km1 = 0, kp1 = 1
+#pragma unroll
         for (int m = 0; m < NF; ++m) {
             double e00, e01;
             end_values(hb[0], hb[1], hb[2], hb[3], io.f(m, 0), io.f(m, 1), io.f(m, 2), io.f(m, 3), e00, e01);
             end_values(ht4[0], ht4[1], ht4[2], ht4[3], io.f(m, n0 - 1), io.f(m, n0 - 2), io.f(m, n0 - 3),
                        io.f(m, n0 - 4), top_out[m], top_in[m]);
-            // cell 0: km1 = 0, kp1 = 1
-            const double s0 = bound_slope(wh[2], wh[2], wh[3], wu[m][2], wu[m][2], wu[m][3]);
-            sl_i[m] = s0;
-            el_i[m] = bound_edge(e00, wu[m][2], wu[m][2], s0, -1.0);
-            // raw edge of interface 1 kept in slp_p1 (reused as the PPM "next raw edge")
-            slp_p1[m] = e01;
+            const double s0 = bound_slope(br_i, wu[m][2], wu[m][2], wu[m][3]);
+            st_b[m] = s0;                                                     // bound slope of cell 0
+            st_a[m] = bound_edge(e00, wu[m][2], wu[m][2], s0, -1.0);          // left edge of cell 0 (interface 0)
+            st_c[m] = e01;                                                    // raw edge of interface 1
         }
     }
 
-    // target sweep state
+    // target sweep state: current target j with edges t_lo = t_edge[j], t_hi = t_edge[j+1]; acc = its content
     int j = 0;
-    double t_lo = 0.0, t_hi = io.ht(0);   // t_edge[j], t_edge[j+1]
-    double acc[NF];
-    for (int m = 0; m < NF; ++m) acc[m] = 0.0;
-    bool last_target_reached = n1 == 1;   // target n1-1 reached (its vanished value then comes from that cell)
-    double last_target_val[NF];
-    bool last_val_set = false;
+    double t_lo = 0.0, t_hi = 0.0 + io.ht(0);
+    double acc[NF], last_val[NF];
+#pragma unroll
+    for (int m = 0; m < NF; ++m) acc[m] = last_val[m] = 0.0;
+    bool last_reached = n1 == 1;      // target n1-1 reached: a vanished last target takes that cell's polynomial
+    bool last_set = false;
     double a = 0.0;
 
     for (int i = 0; i < n0; ++i) {
-        // ---- coefficients of cell i (window slots: 1 = i-1, 2 = i, 3 = i+1, 4 = i+2, 5 = i+3)
+        // ---- polynomial of cell i (slots: 1 = i-1, 2 = i, 3 = i+1, 4 = i+2, 5 = i+3)
         double c0[NF], c1[NF], c2[NF];
+#pragma unroll
         for (int m = 0; m < NF; ++m) { c0[m] = wu[m][2]; c1[m] = 0.0; c2[m] = 0.0; }
         if (plm) {
+            const bool have_p2 = i + 2 <= n0 - 2;                        // slope of cell i+2 is formed
+            const double r2 = have_p2 ? plm_ratio(wh[3], wh[4], wh[5]) : 0.0;
+            const bool have_m1 = i + 1 >= 1 && i + 1 <= n0 - 2;          // monotonized slope of cell i+1
+#pragma unroll
             for (int m = 0; m < NF; ++m) {
-                // slope of cell i+2 and monotonized slope of cell i+1
-                const double slp_p2 = (i + 2 <= n0 - 2) ? plm_slope(wh[3], wh[4], wh[5], wu[m][3], wu[m][4], wu[m][5])
-                                                         : 0.0;
-                mslp_p1[m] = (i + 1 >= 1 && i + 1 <= n0 - 2)
-                                 ? plm_monotonized(wu[m][2], wu[m][3], wu[m][4], slp_0[m], slp_p1[m], slp_p2)
-                                 : 0.0;
-                if (i >= 1 && i <= n0 - 2)
-                    plm_coef(wu[m][2], wu[m][3], mslp_0[m], mslp_p1[m], slp_p1[m], c0[m], c1[m]);
-                slp_m1[m] = slp_0[m];
-                slp_0[m] = slp_p1[m];
-                slp_p1[m] = slp_p2;
-                mslp_0[m] = mslp_p1[m];
+                const double slp_p2 = have_p2 ? plm_slope(r2, wu[m][3], wu[m][4], wu[m][5]) : 0.0;
+                const double mslp_p1 = have_m1 ? plm_monotonized(wu[m][2], wu[m][3], wu[m][4], st_a[m], st_b[m],
+                                                                 slp_p2)
+                                               : 0.0;
+                if (i >= 1 && i <= n0 - 2) plm_coef(wu[m][2], wu[m][3], st_c[m], mslp_p1, st_b[m], c0[m], c1[m]);
+                st_a[m] = st_b[m];
+                st_b[m] = slp_p2;
+                st_c[m] = mslp_p1;
             }
         } else if (ppm) {
-            // raw edge of interface i+2 (stencil cells i..i+3): interior H4, or the top end values
-            H4Weights w{};
-            const bool interior = i + 2 >= 2 && i + 2 <= n0 - 2;
-            if (interior) w = h4_weights(wh[2], wh[3], wh[4], wh[5]);
+            const bool interior = i + 2 <= n0 - 2;                        // interface i+2 from cells i..i+3
+            const H4Weights w = interior ? h4_weights(wh[2], wh[3], wh[4], wh[5]) : H4Weights{0, 0, 0, 0, 1};
+            const bool has_next = i + 1 <= n0 - 1;                        // cell i+1 exists
+            const bool next_has_p = i + 2 <= n0 - 1;                      // cell i+1 has a cell above it
+            const BoundRatio br_n = has_next ? bound_ratio(wh[2], wh[3], next_has_p ? wh[4] : wh[3])
+                                             : BoundRatio{false, 0.0};
+#pragma unroll
             for (int m = 0; m < NF; ++m) {
-                // raw edges: interface i (left of i) is already in el_i (bounded), interface i+1 raw in slp_p1
-                const double e_ip1 = slp_p1[m];
+                const double e_ip1 = st_c[m];
                 double e_ip2 = 0.0;
-                if (i + 2 <= n0) {
-                    if (interior) e_ip2 = h4_edge(w, wu[m][2], wu[m][3], wu[m][4], wu[m][5]);
-                    else if (i + 2 == n0 - 1) e_ip2 = top_in[m];
-                    else e_ip2 = top_out[m];
-                }
-                // bound slope of cell i+1 (km1 = i, kp1 = min(i+2, n0-1))
-                double sl_ip1 = 0.0;
-                if (i + 1 <= n0 - 1) {
-                    const int sp = i + 2 <= n0 - 1 ? 4 : 3;
-                    sl_ip1 = bound_slope(wh[2], wh[3], wh[sp], wu[m][2], wu[m][3], wu[m][sp]);
-                }
-                // right edge of cell i (kp1 = min(i+1, n0-1)) and left edge of cell i+1 (km1 = i), then the check
-                const int rp = i + 1 <= n0 - 1 ? 3 : 2;
-                double er = bound_edge(e_ip1, wu[m][rp], wu[m][2], sl_i[m], 1.0);
+                if (interior) e_ip2 = h4_edge(w, wu[m][2], wu[m][3], wu[m][4], wu[m][5]);
+                else if (i + 2 == n0 - 1) e_ip2 = top_in[m];
+                else if (i + 2 == n0) e_ip2 = top_out[m];
+                const double u_n = next_has_p ? wu[m][4] : wu[m][3];
+                const double sl_n = has_next ? bound_slope(br_n, wu[m][2], wu[m][3], u_n) : 0.0;
+                const double u_r = has_next ? wu[m][3] : wu[m][2];        // kp1 of cell i
+                double er = bound_edge(e_ip1, u_r, wu[m][2], st_b[m], 1.0);
                 double el_next = 0.0;
-                if (i + 1 <= n0 - 1) {
-                    el_next = bound_edge(e_ip1, wu[m][2], wu[m][3], sl_ip1, -1.0);
+                if (has_next) {
+                    el_next = bound_edge(e_ip1, wu[m][2], wu[m][3], sl_n, -1.0);
                     check_pair(er, el_next, wu[m][2], wu[m][3]);
                 }
-                if (i >= 1 && i <= n0 - 2) ppm_coef(wu[m][1], wu[m][2], wu[m][3], el_i[m], er, c0[m], c1[m], c2[m]);
-                el_i[m] = el_next;
-                sl_i[m] = sl_ip1;
-                slp_p1[m] = e_ip2;
+                if (i >= 1 && i <= n0 - 2) ppm_coef(wu[m][1], wu[m][2], wu[m][3], st_a[m], er, c0[m], c1[m], c2[m]);
+                st_a[m] = el_next;
+                st_b[m] = sl_n;
+                st_c[m] = e_ip2;
             }
         }
 
@@ -369,16 +388,17 @@ PO_HDT void remap_column_stream(IO& io, int n0, int n1, int scheme, int n_active
         const double hi = wh[2];
         if (hi > 0.0) {
             const double b = a + hi;
-            // pass 1: targets touched, thickest piece (first maximum)
-            int jj = j;
+            // pass 1: which targets the cell reaches, and the first thickest piece
+            int jj = j, jthick = -1;
             double tl = t_lo, th = t_hi, thick = -1.0;
-            int jthick = -1;
             while (true) {
                 const double lo = pmax(a, tl);
                 const double hi_t = jj < n1 - 1 ? th : pmax(th, b);
-                const double up = pmin(b, hi_t);
-                const double L = up - lo;
-                if (L > 0.0 && L > thick) { thick = L; jthick = jj; }
+                const double L = pmin(b, hi_t) - lo;
+                if (L > 0.0 && L > thick) {
+                    thick = L;
+                    jthick = jj;
+                }
                 if (hi_t <= b && jj < n1 - 1) {
                     ++jj;
                     tl = th;
@@ -388,26 +408,29 @@ PO_HDT void remap_column_stream(IO& io, int n0, int n1, int scheme, int n_active
                 }
             }
             const int j_end = jj;
-            // pass 2: pieces, the residual of the thickest, finished targets written as they are passed
+            // pass 2: pieces in target order; every piece but the thickest is summed, the thickest gets the
+            // residual u h - sum (Hallberg); targets the sweep leaves behind are final and written
             double s[NF], base_thick[NF];
-            for (int m = 0; m < NF; ++m) { s[m] = 0.0; base_thick[m] = 0.0; }
+#pragma unroll
+            for (int m = 0; m < NF; ++m) s[m] = base_thick[m] = 0.0;
             jj = j;
             tl = t_lo;
             th = t_hi;
-            double h_jj = th - tl;   // placeholder; the target thickness is reloaded below
-            (void)h_jj;
             while (true) {
                 const double lo = pmax(a, tl);
                 const double hi_t = jj < n1 - 1 ? th : pmax(th, b);
                 const double up = pmin(b, hi_t);
                 const double L = up - lo;
                 double content[NF];
+#pragma unroll
                 for (int m = 0; m < NF; ++m) content[m] = jj == j ? acc[m] : 0.0;
                 if (L > 0.0) {
-                    const double xa = (lo - a) / hi, xb = (up - a) / hi;
                     if (jj == jthick) {
+#pragma unroll
                         for (int m = 0; m < NF; ++m) base_thick[m] = content[m];
                     } else {
+                        const double xa = (lo - a) / hi, xb = (up - a) / hi;
+#pragma unroll
                         for (int m = 0; m < NF; ++m) {
                             const double piece = L * average(c0[m], c1[m], c2[m], xa, xb);
                             s[m] += piece;
@@ -415,80 +438,199 @@ PO_HDT void remap_column_stream(IO& io, int n0, int n1, int scheme, int n_active
                         }
                     }
                 }
-                if (jj < j_end) {
+                if (jj == j_end) {
                     if (jj != jthick) {
-                        const double hgt = io.ht(jj);
-                        for (int m = 0; m < NF; ++m) {
-                            double val;
-                            if (hgt > 0.0) {
-                                val = content[m] / hgt;
-                            } else {           // vanished target: value of this cell's polynomial at its position
-                                const double xi = (tl - a) / hi;
-                                val = c0[m] + xi * (c1[m] + xi * c2[m]);
-                            }
-                            io.put(m, jj, val);
-                        }
-                    }
-                    ++jj;
-                    tl = th;
-                    th = th + io.ht(jj);
-                } else {
-                    if (jj != jthick)
+#pragma unroll
                         for (int m = 0; m < NF; ++m) acc[m] = content[m];
+                    }
                     break;
                 }
-            }
-            if (jthick >= 0) {
-                for (int m = 0; m < NF; ++m) {
-                    const double piece = wu[m][2] * hi - s[m];
-                    const double cth = base_thick[m] + piece;
-                    if (jthick < j_end) {
-                        const double hgt = io.ht(jthick);
-                        io.put(m, jthick, hgt > 0.0 ? cth / hgt : cth);   // hgt > 0: a piece needs a thickness
-                    } else {
-                        acc[m] = cth;
+                if (jj != jthick) {
+                    const double hgt = io.ht(jj);
+                    if (hgt > 0.0) {
+#pragma unroll
+                        for (int m = 0; m < NF; ++m) io.put(m, jj, content[m] / hgt);
+                    } else {                                   // vanished target: this cell's value at its position
+                        const double xi = (tl - a) / hi;
+#pragma unroll
+                        for (int m = 0; m < NF; ++m) io.put(m, jj, c0[m] + xi * (c1[m] + xi * c2[m]));
                     }
                 }
+                ++jj;
+                tl = th;
+                th = th + io.ht(jj);
             }
-            // the last target, reached for the first time in this cell, takes this cell's polynomial if vanished
-            if (!last_target_reached && j_end == n1 - 1) last_target_reached = true;
-            if (last_target_reached && !last_val_set) {
-                // x = t_edge[n1-1] = tl at the end of pass 2 when j_end == n1-1
+            if (jthick >= 0) {
+                const double hgt = jthick < j_end ? io.ht(jthick) : 0.0;
+#pragma unroll
+                for (int m = 0; m < NF; ++m) {
+                    const double cth = base_thick[m] + (wu[m][2] * hi - s[m]);
+                    if (jthick < j_end) io.put(m, jthick, cth / hgt);     // a piece implies a positive thickness
+                    else acc[m] = cth;
+                }
+            }
+            if (j_end == n1 - 1) last_reached = true;
+            if (last_reached && !last_set) {                       // x = t_edge[n1-1] = tl when j_end = n1-1
                 const double xi = (tl - a) / hi;
-                for (int m = 0; m < NF; ++m) last_target_val[m] = c0[m] + xi * (c1[m] + xi * c2[m]);
-                last_val_set = true;
+#pragma unroll
+                for (int m = 0; m < NF; ++m) last_val[m] = c0[m] + xi * (c1[m] + xi * c2[m]);
+                last_set = true;
             }
             j = j_end;
             t_lo = tl;
             t_hi = th;
             a = b;
         }
-        // ---- slide the window by one cell
+        // ---- slide the window
+#pragma unroll
         for (int s = 0; s < 5; ++s) {
             wh[s] = wh[s + 1];
+#pragma unroll
             for (int m = 0; m < NF; ++m) wu[m][s] = wu[m][s + 1];
         }
-        const int knew = i + 4;
-        const bool in = knew < n0;
-        wh[5] = in ? io.hs(knew) : 0.0;
-        for (int m = 0; m < NF; ++m) wu[m][5] = in ? io.f(m, knew) : 0.0;
+        const bool in = i + 4 < n0;
+        wh[5] = in ? io.hs(i + 4) : 0.0;
+#pragma unroll
+        for (int m = 0; m < NF; ++m) wu[m][5] = in ? io.f(m, i + 4) : 0.0;
     }
 
-    // targets from the current one to the top: the current one holds its accumulated content; the ones above it
-    // were never reached (content 0, or the last source value when vanished)
+    // the current target keeps its content; targets above it were never reached: content 0, or (vanished) the
+    // value of the last source cell, except a vanished last target reached by some cell (remap.py:382-397)
     for (int jj = j; jj < n1; ++jj) {
         const double hgt = io.ht(jj);
+#pragma unroll
         for (int m = 0; m < NF; ++m) {
             double val;
-            if (hgt > 0.0) {
-                val = (jj == j ? acc[m] : 0.0) / hgt;
-            } else if (jj == n1 - 1 && last_val_set) {
-                val = last_target_val[m];
-            } else {
-                val = io.f(m, last);
-            }
+            if (hgt > 0.0) val = (jj == j ? acc[m] : 0.0) / hgt;
+            else if (jj == n1 - 1 && last_set) val = last_val[m];
+            else val = io.f(m, last);
             io.put(m, jj, val);
         }
+    }
+}
+
+// Column with no active source cell (remap.py:375-381): copied when n0 == n1, else every target takes the mean.
+template <int NF, class IO>
+PO_HDT void remap_column_dry(IO& io, int n0, int n1)
+{
+#pragma unroll
+    for (int m = 0; m < NF; ++m) {
+        if (n0 == n1) {
+            for (int k = 0; k < n1; ++k) io.put(m, k, io.f(m, k));
+        } else {
+            double mean = 0.0;
+            for (int k = 0; k < n0; ++k) mean += io.f(m, k) / n0;
+            for (int k = 0; k < n1; ++k) io.put(m, k, mean);
+        }
+    }
+}
+
+// ------------------------------------------------------------------------------------------------------------
+// The reference's array formulation of remap_column (remap.py:306-397) for one field, with the column held in
+// thread-local arrays of NMAX entries (n0, n1 <= NMAX).  Used for the columns outside the one-pass sweep's domain
+// (a negative or NaN target thickness); same arithmetic, same results.
+template <int NMAX, class IO>
+PO_HDT void remap_column_general(IO& io, int m, int n0, int n1, int scheme)
+{
+    double h[NMAX], u[NMAX], c0[NMAX], c1[NMAX], c2[NMAX], e0[NMAX], e1[NMAX];
+    double t_edge[NMAX + 1], content[NMAX], piece[NMAX + 1];
+    int piece_j[NMAX + 1];
+    int n_active = 0;
+    for (int k = 0; k < n0; ++k) {
+        h[k] = io.hs(k);
+        u[k] = io.f(m, k);
+        if (h[k] > 0.0) ++n_active;
+    }
+    const int sch = effective_scheme(n_active, scheme);
+    for (int k = 0; k < n0; ++k) { c0[k] = u[k]; c1[k] = 0.0; c2[k] = 0.0; }
+    if (sch == PLM && n0 >= 3) {                           // remap.py:248-262 (e0 = slp, e1 = mslp)
+        e0[0] = e0[n0 - 1] = e1[0] = e1[n0 - 1] = 0.0;
+        for (int k = 1; k < n0 - 1; ++k) e0[k] = plm_slope(plm_ratio(h[k - 1], h[k], h[k + 1]), u[k - 1], u[k], u[k + 1]);
+        for (int k = 1; k < n0 - 1; ++k) e1[k] = plm_monotonized(u[k - 1], u[k], u[k + 1], e0[k - 1], e0[k], e0[k + 1]);
+        for (int k = 1; k < n0 - 1; ++k) plm_coef(u[k], u[k + 1], e1[k], e1[k + 1], e0[k + 1], c0[k], c1[k]);
+    } else if (sch == PPM_H4 && n0 >= 4) {                 // remap.py:263-294 (e0 = left edges, e1 = right edges)
+        for (int i = 2; i < n0 - 1; ++i) {
+            e0[i] = h4_edge(h4_weights(h[i - 2], h[i - 1], h[i], h[i + 1]), u[i - 2], u[i - 1], u[i], u[i + 1]);
+            e1[i - 1] = e0[i];
+        }
+        end_values(pmax(H_NEGLECT_EDGE, h[0]), pmax(H_NEGLECT_EDGE, h[1]), pmax(H_NEGLECT_EDGE, h[2]),
+                   pmax(H_NEGLECT_EDGE, h[3]), u[0], u[1], u[2], u[3], e0[0], e1[0]);
+        e0[1] = e1[0];
+        end_values(pmax(H_NEGLECT_EDGE, h[n0 - 1]), pmax(H_NEGLECT_EDGE, h[n0 - 2]), pmax(H_NEGLECT_EDGE, h[n0 - 3]),
+                   pmax(H_NEGLECT_EDGE, h[n0 - 4]), u[n0 - 1], u[n0 - 2], u[n0 - 3], u[n0 - 4], e1[n0 - 1],
+                   e0[n0 - 1]);
+        e1[n0 - 2] = e0[n0 - 1];
+        for (int k = 0; k < n0; ++k) {
+            const int km1 = k > 0 ? k - 1 : 0, kp1 = k < n0 - 1 ? k + 1 : n0 - 1;
+            const double sl = bound_slope(bound_ratio(h[km1], h[k], h[kp1]), u[km1], u[k], u[kp1]);
+            e0[k] = bound_edge(e0[k], u[km1], u[k], sl, -1.0);
+            e1[k] = bound_edge(e1[k], u[kp1], u[k], sl, 1.0);
+        }
+        for (int k = 0; k < n0 - 1; ++k) check_pair(e1[k], e0[k + 1], u[k], u[k + 1]);
+        for (int k = 1; k < n0 - 1; ++k) ppm_coef(u[k - 1], u[k], u[k + 1], e0[k], e1[k], c0[k], c1[k], c2[k]);
+    }
+    t_edge[0] = 0.0;
+    for (int j = 0; j < n1; ++j) {
+        t_edge[j + 1] = t_edge[j] + io.ht(j);
+        content[j] = 0.0;
+    }
+    double a = 0.0;
+    int j = 0, last = -1;
+    for (int i = 0; i < n0; ++i) {
+        const double hi = h[i];
+        if (hi <= 0.0) continue;
+        last = i;
+        const double b = a + hi;
+        int npc = 0, ithick = 0;
+        double thick = -1.0;
+        while (j < n1) {
+            const double lo = pmax(a, t_edge[j]);
+            const double hi_t = j < n1 - 1 ? t_edge[j + 1] : pmax(t_edge[n1], b);
+            const double up = pmin(b, hi_t);
+            const double L = up - lo;
+            if (L > 0.0) {
+                piece[npc] = L * average(c0[i], c1[i], c2[i], (lo - a) / hi, (up - a) / hi);
+                piece_j[npc] = j;
+                if (L > thick) { thick = L; ithick = npc; }
+                ++npc;
+            }
+            if (hi_t <= b && j < n1 - 1) ++j;
+            else break;
+        }
+        if (npc > 0) {
+            double s = 0.0;
+            for (int q = 0; q < npc; ++q) if (q != ithick) s += piece[q];
+            piece[ithick] = u[i] * hi - s;
+            for (int q = 0; q < npc; ++q) content[piece_j[q]] += piece[q];
+        }
+        a = b;
+    }
+    if (last < 0) {
+        double mean = 0.0;
+        for (int i = 0; i < n0; ++i) mean += u[i] / n0;
+        for (int jj = 0; jj < n1; ++jj) io.put(m, jj, n0 == n1 ? u[jj] : mean);
+        return;
+    }
+    for (int jj = 0; jj < n1; ++jj) {
+        const double ht = io.ht(jj);
+        double val;
+        if (ht > 0.0) {
+            val = content[jj] / ht;
+        } else {
+            const double x = t_edge[jj];
+            double aa = 0.0;
+            val = u[last];
+            for (int i = 0; i < n0; ++i) {
+                if (h[i] <= 0.0) continue;
+                if (x <= aa + h[i]) {
+                    const double xi = (x - aa) / h[i];
+                    val = c0[i] + xi * (c1[i] + xi * c2[i]);
+                    break;
+                }
+                aa += h[i];
+            }
+        }
+        io.put(m, jj, val);
     }
 }
 

@@ -35,7 +35,8 @@ def test_version_and_workspace_sizes():
     nt, n, ny, nx = 2, 50, 512, 512
     cells = nt * n * ny * nx * 8
     fct = L.pocean_advect_fct_workspace_bytes(nt, n, ny, nx)
-    assert 5 * cells <= fct <= 5 * cells + 4 * nt * n * (ny + nx) * 8 + 5 * 256
+    # 3 cell stacks and 4 face stacks (u- and v-faces, twice)
+    assert 7 * cells <= fct <= 7 * cells + 4 * nt * n * (ny + nx) * 8 + 7 * 256
     assert L.pocean_advect_fct_workspace_bytes(0, n, ny, nx) == 0
     assert L.pocean_advect_rk3_workspace_bytes(nt, n, ny, nx) >= 4 * cells
 
