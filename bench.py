@@ -213,6 +213,27 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> dict | None:
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         ms = float(t.item())
 
+    # ---- the mixed-precision form of the same step (FP32 WENO weights, FP64 limiter / bookkeeping / remap)
+    mixed_stepper = ALETracerStep(nt, n, ny, nx, w.dt, flags, w.remap_scheme, device=dev, mixed=True)
+    stepper = mixed_stepper
+    for i in range(args.warmup):
+        one_step(i)
+    torch.cuda.synchronize()
+    m0, m1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    mevs = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(args.steps)]
+    m0.record(stream)
+    for i in range(args.steps):
+        one_step(args.warmup + i, mevs[i])
+    m1.record(stream)
+    torch.cuda.synchronize()
+    mixed_ms = m0.elapsed_time(m1)
+    mixed_adv = float(np.mean([e[0].elapsed_time(e[1]) for e in mevs]))
+    if world > 1:
+        t = torch.tensor([mixed_ms], dtype=torch.float64, device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        mixed_ms = float(t.item())
+    del mixed_stepper
+
     # ---- end to end through the public API, pinned host tensors, copies inside the timed region
     adv = TracerAdvection(scheme=w.scheme, time="ssprk3", dt=w.dt, ob=OpenEdges(w.open))
     adv.per = Periodic(w.periodic)
@@ -278,6 +299,10 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> dict | None:
         "e2e": {"value": cells * world / (e2e_ms / 1e3), "unit": "tracer cell-steps/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms,
                 "api": "TracerAdvection.advect_fct + remap_columns on pinned host tensors"},
+        "mixed": {"value": cells * args.steps * world / (mixed_ms / 1e3), "ms_per_step": mixed_ms / args.steps,
+                  "advect_fct_ms": mixed_adv, "speedup_vs_f64": ms / mixed_ms,
+                  "what": "pocean_advect_fct_mixed (FP32 WENO5 weights and face values, FP64 fluxes, limiter and "
+                          "bookkeeping) + FP64 PPM_H4 remap, same workload"},
         "gpu_launches": stepper.launches_per_step * args.steps,
         "clocks": clk,
     }

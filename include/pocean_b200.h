@@ -76,6 +76,19 @@ int pocean_advect_fct_f64(const double* C, const double* V0, const double* V1, c
                           double* open_flux, void* workspace, size_t workspace_bytes, void* stream);
 
 /*
+ * The FCT step of pocean_advect_fct_f64 with mixed precision: the WENO5 smoothness indicators, nonlinear weights
+ * and face values are computed in FP32 (on the stencil's differences from the upwind cell, normalised), while the
+ * fluxes, the Zalesak limiter, the donor-cell bookkeeping and every stage update stay in FP64, so tracer content is
+ * conserved to FP64 round-off.  Same arguments and workspace as pocean_advect_fct_f64.  Replaces the same
+ * reference function (core/components/tracers.py:208-254) at reduced precision of the high-order face values;
+ * its error against the FP64 path is measured, not bit-exact.
+ */
+int pocean_advect_fct_mixed(const double* C, const double* V0, const double* V1, const double* Qx,
+                            const double* Qy, const uint8_t* ok, const double* inflow, int nt, int nz, int ny,
+                            int nx, unsigned flags, double dt, double* C_out, int face_i, double* fx_face,
+                            double* open_flux, void* workspace, size_t workspace_bytes, void* stream);
+
+/*
  * The same FCT step as pocean_advect_fct_f64 for callers that cannot allocate device memory (a host model that
  * reaches the GPU only through this ABI with no device allocator of its own, or one whose device memory belongs
  * to a pool that forbids side allocations).  No counterpart in the reference: it is an addition of this library.

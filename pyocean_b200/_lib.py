@@ -27,6 +27,8 @@ SIGNATURES: dict[str, tuple] = {
     "pocean_advect_fct_workspace_bytes": (_Z, [_I, _I, _I, _I]),
     "pocean_advect_fct_f64": (_I, [_P, _P, _P, _P, _P, _P, _P, _I, _I, _I, _I, _U, _D, _P, _I, _P, _P, _P, _Z,
                                    _P]),
+    "pocean_advect_fct_mixed": (_I, [_P, _P, _P, _P, _P, _P, _P, _I, _I, _I, _I, _U, _D, _P, _I, _P, _P, _P, _Z,
+                                     _P]),
     "pocean_advect_fct_f64_noalloc": (_I, [_P, _P, _P, _P, _P, _P, _P, _I, _I, _I, _I, _U, _D, _P, _I, _P, _P,
                                            _P]),
     "pocean_advect_rk3_workspace_bytes": (_Z, [_I, _I, _I, _I]),

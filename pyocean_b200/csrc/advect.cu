@@ -276,16 +276,23 @@ __global__ void __launch_bounds__(NTHREADS) fct_coeff_kernel(StepArgs a)
         const i64 ci = s.cell(t, k, j, i);
         double rin = 0.0, rout = 0.0;
         if (self_ok) {
+            // every load of the tracer first (independent, in flight together), then the bounds in stencil order
+            double vc[7], vl[7];
+#pragma unroll
+            for (int m = 0; m < 7; ++m) {
+                const i64 o = (i64)t * tstride + (nb[m] >= 0 ? nb[m] : nb[0]);
+                vc[m] = __ldg(a.C + o);
+                vl[m] = cL[o];
+            }
+            const i64 w = s.ux(t, k, j, i), so = s.vy(t, k, j, i);
+            const double axw = a.Sx[w], axe = a.Sx[w + 1], ays = a.Sy[so], ayn = a.Sy[so + s.nx];
             double cmax = -INFINITY, cmin = INFINITY;
 #pragma unroll
             for (int m = 0; m < 7; ++m) {
                 if (nb[m] < 0) continue;
-                const i64 o = (i64)t * tstride + nb[m];
-                cmax = pmax(pmax(cmax, a.C[o]), cL[o]);
-                cmin = pmin(pmin(cmin, a.C[o]), cL[o]);
+                cmax = pmax(pmax(cmax, vc[m]), vl[m]);
+                cmin = pmin(pmin(cmin, vc[m]), vl[m]);
             }
-            const i64 w = s.ux(t, k, j, i), so = s.vy(t, k, j, i);
-            const double axw = a.Sx[w], axe = a.Sx[w + 1], ays = a.Sy[so], ayn = a.Sy[so + s.nx];
             const double p_in = a.dt * (pmax(axw, 0.0) - pmin(axe, 0.0) + pmax(ays, 0.0) - pmin(ayn, 0.0));
             const double p_out = a.dt * (pmax(axe, 0.0) - pmin(axw, 0.0) + pmax(ayn, 0.0) - pmin(ays, 0.0));
             const double q_in = pmax(v1 * (cmax - cL[ci]), 0.0);
@@ -321,7 +328,27 @@ __device__ __forceinline__ double coef_y(const StepArgs& a, const Shape& s, cons
 }
 
 // Pass 5: C_out = safe(q0 - dt div(F_L + C A), V1) (sigma_baroclinic.py:514-530).  One thread per column cell
-// (k, j, i) loops over the tracers, so the geometry is read once and the tracers' loads are independent.
+// (k, j, i) loops over the tracers, so the geometry is read once; every value a tracer needs (C, R+ and R- at the
+// cell and its four neighbours, A on the four faces) is loaded before any is used, so the loads of a thread are
+// independent and in flight together.
+
+// Effective flux F_L + C A through one face from its preloaded neighbourhood: `interior` faces take the donor value
+// and the limited antidiffusive flux; domain-edge faces (closed, or open with the upstream rule) carry no
+// antidiffusive part (C = 0 there).
+__device__ __forceinline__ double face_flux(bool interior, bool open, bool inflow_side_pos, double q, double A,
+                                            double c_l, double c_r, double rin_l, double rin_r, double rout_l,
+                                            double rout_r, double ext, double c_edge)
+{
+    if (interior) {
+        const double fl = q * (q >= 0 ? c_l : c_r);
+        const double cf = A >= 0.0 ? pmin(rin_r, rout_l) : pmin(rin_l, rout_r);
+        return fl + cf * A;
+    }
+    // edge: inflow when q > 0 on the west/south edge (inflow_side_pos) or q < 0 on the east/north edge
+    const double fl = open ? q * ((inflow_side_pos ? q > 0 : q < 0) ? ext : c_edge) : 0.0;
+    return fl + 0.0 * A;
+}
+
 __global__ void __launch_bounds__(NTHREADS) fct_final_kernel(StepArgs a)
 {
     const Shape s = a.s;
@@ -329,22 +356,42 @@ __global__ void __launch_bounds__(NTHREADS) fct_final_kernel(StepArgs a)
     const int i = blockIdx.x * TI + threadIdx.x % TI, j = blockIdx.y * TJ + threadIdx.x / TI;
     const int k = blockIdx.z;
     if (i >= s.nx || j >= s.ny) return;
+    // neighbours (wrapped on periodic axes, -1 outside the domain) and which faces are interior
+    const int iw = fl.per_x ? wrap(i - 1, s.nx) : i - 1, ie = fl.per_x ? wrap(i + 1, s.nx) : (i + 1 < s.nx ? i + 1 : -1);
+    const int js = fl.per_y ? wrap(j - 1, s.ny) : j - 1, jn = fl.per_y ? wrap(j + 1, s.ny) : (j + 1 < s.ny ? j + 1 : -1);
+    const bool in_w = fl.per_x || i >= 1, in_e = fl.per_x || i + 1 <= s.nx - 1;
+    const bool in_s = fl.per_y || j >= 1, in_n = fl.per_y || j + 1 <= s.ny - 1;
     const i64 g = s.geo(k, j, i);
     const double v0 = __ldg(a.V0 + g), v1 = __ldg(a.V1 + g);
+    const double qw = __ldg(a.Qx + s.qx(k, j, i));
+    const double qe = __ldg(a.Qx + s.qx(k, j, (fl.per_x && i + 1 == s.nx) ? 0 : i + 1));
+    const double qs = __ldg(a.Qy + s.qy(k, j, i));
+    const double qn = __ldg(a.Qy + s.qy(k, (fl.per_y && j + 1 == s.ny) ? 0 : j + 1, i));
+    const i64 row = (i64)j * s.nx;
+    const i64 o_c = row + i, o_w = row + (iw >= 0 ? iw : i), o_e = row + (ie >= 0 ? ie : i);
+    const i64 o_s = (i64)(js >= 0 ? js : j) * s.nx + i, o_n = (i64)(jn >= 0 ? jn : j) * s.nx + i;
     for (int t = 0; t < s.nt; ++t) {
-        const i64 ci = s.cell(t, k, j, i);
-        const double* Cp = a.C + s.cell(t, k, 0, 0);
-        const double* eL = a.inflow ? a.inflow + s.cell(t, k, 0, 0) : Cp;
+        const i64 pc = s.cell(t, k, 0, 0);
+        const double* C = a.C + pc;
+        const double* Rp = a.c1 + pc;
+        const double* Rm = a.c2 + pc;
+        const double c0 = __ldg(C + o_c), cw = __ldg(C + o_w), ce = __ldg(C + o_e), cs = __ldg(C + o_s),
+                     cn = __ldg(C + o_n);
+        const double rp0 = Rp[o_c], rpw = Rp[o_w], rpe = Rp[o_e], rps = Rp[o_s], rpn = Rp[o_n];
+        const double rm0 = Rm[o_c], rmw = Rm[o_w], rme = Rm[o_e], rms = Rm[o_s], rmn = Rm[o_n];
         const i64 w = s.ux(t, k, j, i), so = s.vy(t, k, j, i);
-        const double axw = a.Sx[w], axe = a.Sx[w + 1], ays = a.Sy[so], ayn = a.Sy[so + s.nx];
-        const double fw = donor_x(Cp, eL, a.Qx, s, fl, k, j, i) + coef_x(a, s, fl, t, k, j, i, axw) * axw;
-        const double fe = donor_x(Cp, eL, a.Qx, s, fl, k, j, i + 1) + coef_x(a, s, fl, t, k, j, i + 1, axe) * axe;
-        const double fs = donor_y(Cp, eL, a.Qy, s, fl, k, j, i) + coef_y(a, s, fl, t, k, j, i, ays) * ays;
-        const double fn = donor_y(Cp, eL, a.Qy, s, fl, k, j + 1, i) + coef_y(a, s, fl, t, k, j + 1, i, ayn) * ayn;
+        const double aw = a.Sx[w], ae = a.Sx[w + 1], as = a.Sy[so], an = a.Sy[so + s.nx];
+        double ext_c = c0;
+        if (a.inflow && ((!in_w && fl.open_w) || (!in_e && fl.open_e) || (!in_s && fl.open_s) ||
+                         (!in_n && fl.open_n)))
+            ext_c = __ldg(a.inflow + pc + o_c);
+        const double fw = face_flux(in_w, fl.open_w, true, qw, aw, cw, c0, rpw, rp0, rmw, rm0, ext_c, c0);
+        const double fe = face_flux(in_e, fl.open_e, false, qe, ae, c0, ce, rp0, rpe, rm0, rme, ext_c, c0);
+        const double fs = face_flux(in_s, fl.open_s, true, qs, as, cs, c0, rps, rp0, rms, rm0, ext_c, c0);
+        const double fn = face_flux(in_n, fl.open_n, false, qn, an, c0, cn, rp0, rpn, rm0, rmn, ext_c, c0);
         const double d = fe - fw + fn - fs;
-        const double c0 = a.C[ci];
         const double q = v0 * c0 - a.dt * d;
-        a.out[ci] = v1 > 0 ? q / v1 : c0;
+        a.out[pc + o_c] = v1 > 0 ? q / v1 : c0;
     }
 }
 
@@ -538,13 +585,20 @@ static int common_checks(const char* fn, const void* C, const void* V0, const vo
     return pocean_check_device();
 }
 
-extern "C" int pocean_advect_fct_f64(const double* C, const double* V0, const double* V1, const double* Qx,
-                                     const double* Qy, const uint8_t* ok, const double* inflow, int nt, int nz,
-                                     int ny, int nx, unsigned flags, double dt, double* C_out, int face_i,
-                                     double* fx_face, double* open_flux, void* workspace, size_t workspace_bytes,
-                                     void* stream)
+template <bool ZV, bool MIX>
+static void launch_strips(const StepArgs& a, int stage, dim3 grid, int nstrips, int nsegs, cudaStream_t st)
 {
-    const char* fn = "pocean_advect_fct_f64";
+    if (stage == 1) fct_strip_kernel<1, ZV, MIX><<<grid, SWARPS * 32, 0, st>>>(a, nstrips, nsegs);
+    else if (stage == 2) fct_strip_kernel<2, ZV, MIX><<<grid, SWARPS * 32, 0, st>>>(a, nstrips, nsegs);
+    else fct_strip_kernel<3, ZV, MIX><<<grid, SWARPS * 32, 0, st>>>(a, nstrips, nsegs);
+}
+
+// The FCT step with FP64 (mixed = false) or FP32-weight (mixed = true) WENO faces; everything else FP64.
+static int advect_fct_impl(const char* fn, bool mixed, const double* C, const double* V0, const double* V1,
+                           const double* Qx, const double* Qy, const uint8_t* ok, const double* inflow, int nt,
+                           int nz, int ny, int nx, unsigned flags, double dt, double* C_out, int face_i,
+                           double* fx_face, double* open_flux, void* workspace, size_t workspace_bytes, void* stream)
+{
     int rc = common_checks(fn, C, V0, V1, Qx, Qy, ok, C_out, nt, nz, ny, nx, flags, face_i, fx_face, workspace,
                            workspace_bytes, pocean_advect_fct_workspace_bytes(nt, nz, ny, nx));
     if (rc) return rc;
@@ -574,16 +628,22 @@ extern "C" int pocean_advect_fct_f64(const double* C, const double* V0, const do
     a.out = C_out; a.face_i = face_i; a.fx_face = fx_face;
 
     const dim3 grid(ceil_div(nx, TI), ceil_div(ny, TJ), nt * nz);
-    const int nstrips = ceil_div(nx, STRIP);
-    const dim3 sgrid(ceil_div(nstrips, SWARPS), ceil_div(ny, SEG), nt * nz);
-    fct_strip_kernel<1><<<sgrid, SWARPS * 32, 0, st>>>(a);
-    fct_strip_kernel<2><<<sgrid, SWARPS * 32, 0, st>>>(a);
+    const int nstrips = ceil_div(nx, STRIP), nsegs = ceil_div(ny, SEG);
+    const dim3 sgrid(ceil_div(nstrips * nsegs, SWARPS), nt * nz);
+    const bool zv = !(flags & POCEAN_WENO_JS);
+    auto strips = [&](int stage) {
+        if (zv && !mixed) launch_strips<true, false>(a, stage, sgrid, nstrips, nsegs, st);
+        else if (!zv && !mixed) launch_strips<false, false>(a, stage, sgrid, nstrips, nsegs, st);
+        else if (zv) launch_strips<true, true>(a, stage, sgrid, nstrips, nsegs, st);
+        else launch_strips<false, true>(a, stage, sgrid, nstrips, nsegs, st);
+    };
+    strips(1);
+    strips(2);
     if (flags & POCEAN_FCT_UNLIMITED) {
-        if (open_flux) return pocean_fail(POCEAN_EINVAL, "%s: open_flux is only defined for the limited step", fn);
         fct_unlimited_kernel<<<grid, NTHREADS, 0, st>>>(a);
         return pocean_check_launch(fn);
     }
-    fct_strip_kernel<3><<<sgrid, SWARPS * 32, 0, st>>>(a);
+    strips(3);
     fct_coeff_kernel<<<dim3(ceil_div(nx, TI), ceil_div(ny, TJ), nz), NTHREADS, 0, st>>>(a);
     fct_final_kernel<<<dim3(ceil_div(nx, TI), ceil_div(ny, TJ), nz), NTHREADS, 0, st>>>(a);
     if (fx_face) {
@@ -592,6 +652,26 @@ extern "C" int pocean_advect_fct_f64(const double* C, const double* V0, const do
     }
     if (open_flux) fct_open_flux_kernel<<<nt, 256, 0, st>>>(a, open_flux);
     return pocean_check_launch(fn);
+}
+
+extern "C" int pocean_advect_fct_f64(const double* C, const double* V0, const double* V1, const double* Qx,
+                                     const double* Qy, const uint8_t* ok, const double* inflow, int nt, int nz,
+                                     int ny, int nx, unsigned flags, double dt, double* C_out, int face_i,
+                                     double* fx_face, double* open_flux, void* workspace, size_t workspace_bytes,
+                                     void* stream)
+{
+    return advect_fct_impl("pocean_advect_fct_f64", false, C, V0, V1, Qx, Qy, ok, inflow, nt, nz, ny, nx, flags, dt,
+                           C_out, face_i, fx_face, open_flux, workspace, workspace_bytes, stream);
+}
+
+extern "C" int pocean_advect_fct_mixed(const double* C, const double* V0, const double* V1, const double* Qx,
+                                       const double* Qy, const uint8_t* ok, const double* inflow, int nt, int nz,
+                                       int ny, int nx, unsigned flags, double dt, double* C_out, int face_i,
+                                       double* fx_face, double* open_flux, void* workspace, size_t workspace_bytes,
+                                       void* stream)
+{
+    return advect_fct_impl("pocean_advect_fct_mixed", true, C, V0, V1, Qx, Qy, ok, inflow, nt, nz, ny, nx, flags,
+                           dt, C_out, face_i, fx_face, open_flux, workspace, workspace_bytes, stream);
 }
 
 extern "C" int pocean_advect_rk3_f64(const double* C, const double* V0, const double* V1, const double* Qx,

@@ -1,39 +1,29 @@
 // Warp-strip marching for the three WENO5 passes of the FCT step (included by advect.cu).
 //
 // Each warp owns one strip of 31 cells along i (lanes 0..30; lane 31 computes the strip's 32nd x-face, which is
-// the east face of lane 30's cell) and a segment of SEG rows of one (t, k) plane, and marches in j:
-//   * y-faces: every lane keeps the 6-cell y-stencil of its column in registers and slides it by one row a step,
-//     so a y-face costs one new load;
-//   * x-faces: the row being finished is staged in a small per-warp ring in shared memory (columns i0-3 .. i0+33,
-//     read by the warp's own lanes after __syncwarp), one x-face per lane;
-//   * row j+3 is loaded (coalesced) while row j is computed, and the cell update of row j-1 uses the x-faces of the
-//     previous step (the east face from lane+1 by shuffle) and the y-faces of the previous and current steps.
-// There is no block-level barrier: warps march independently.  Faces per cell: 32/31 x-faces and 32/31 +
-// 1/SEG y-faces, against 2 + 1/32 + 1/8 for 32 x 8 tiles.  The arithmetic is the reference's (weno.cuh).
+// the east face of lane 30's cell) and a segment of SEG rows of one (t, k) plane, and marches in j.  Rows of the
+// input field (columns i0-3 .. i0+33 with their validity bytes) pass through a per-warp ring of RING rows in
+// shared memory: the row j+4 is loaded (coalesced) into registers while row j is computed and written to the ring
+// one step later, so the ring holds rows j-3 .. j+3.  A lane's y-stencil is its ring column, its x-stencil six
+// neighbouring ring entries of row j; both need only __syncwarp, never a block barrier, and the warp keeps just
+// the in-flight row and the faces of the previous step in registers (a register budget that lets 32 warps share
+// an SM, which the FP64 dependency chains of WENO5 need).  The cell update of row j-1 uses the x-faces of the
+// previous step (the east one from lane+1 by shuffle) and the y-faces of the previous and current steps.
+// Faces per cell: 32/31 in x and 32/31 (1 + 1/SEG) in y.  The arithmetic is the reference's (weno.cuh).
 #pragma once
 
 namespace po {
 
 constexpr int STRIP = 31;            // cells per warp along i
-constexpr int SEG = 32;              // rows per warp segment
+constexpr int SEG = 64;              // rows per warp segment
 constexpr int SWARPS = 4;            // warps per CTA (independent)
-constexpr int RXW = 37;              // ring row: columns i0-3 .. i0+33
-constexpr int RING = 4;              // ring rows
+constexpr int RXW = 40;              // ring row pitch (37 used: columns i0-3 .. i0+33)
+constexpr int RING = 8;              // ring rows (rows j-3 .. j+3 plus the one being refilled)
 
 struct StripSmem {
-    double row[SWARPS][RING][RXW + 3];
-    uint8_t val[SWARPS][RING][RXW + 3];
+    double row[SWARPS][RING][RXW];
+    uint8_t val[SWARPS][RING][RXW];
 };
-
-// Upwind WENO5 face value from register stencils (cells f-3 .. f+2 in w0..w5, validity bits in vb bits 0..5).
-__device__ __forceinline__ double upwind_face_reg(double w0, double w1, double w2, double w3, double w4, double w5,
-                                                  unsigned vb, double q, bool z)
-{
-    const bool pos = q >= 0.0;
-    const bool b0 = vb & 1u, b1 = vb & 2u, b2 = vb & 4u, b3 = vb & 8u, b4 = vb & 16u, b5 = vb & 32u;
-    return weno5_value(pos ? w0 : w5, pos ? w1 : w4, pos ? w2 : w3, pos ? w3 : w2, pos ? w4 : w1,
-                       pos ? b0 : b5, pos ? b1 : b4, pos ? b2 : b3, pos ? b3 : b2, pos ? b4 : b1, z);
-}
 
 // Global row index of row r (periodic wrap, or -1 outside a closed/open domain).
 __device__ __forceinline__ int row_of(int r, const Shape& s, const Flags& fl)
@@ -42,26 +32,37 @@ __device__ __forceinline__ int row_of(int r, const Shape& s, const Flags& fl)
     return (r >= 0 && r < s.ny) ? r : -1;
 }
 
-template <int STAGE>
-__global__ void __launch_bounds__(SWARPS * 32) fct_strip_kernel(StepArgs a)
+template <int STAGE, bool ZV, bool MIX>
+__global__ void __launch_bounds__(SWARPS * 32, STAGE == 3 ? 8 : 5) fct_strip_kernel(StepArgs a, int nstrips, int nsegs)
 {
     __shared__ StripSmem SM;
     const Shape s = a.s;
     const Flags fl(a.flags);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int strip = blockIdx.x * SWARPS + warp;
+    const int pair = blockIdx.x * SWARPS + warp;               // (segment, strip) pairs, strip fastest
+    if (pair >= nstrips * nsegs) return;                       // whole warp leaves together
+    const int seg = pair / nstrips, strip = pair - seg * nstrips;
     const int i0 = strip * STRIP;
-    if (i0 >= s.nx) return;                                   // whole warp leaves together
-    const int jA = blockIdx.y * SEG;
+    const int jA = seg * SEG;
     const int jB = min(jA + SEG, s.ny);                        // cells jA..jB-1; y-faces jA..jB
-    const int p = blockIdx.z, k = p / s.nt, t = p - k * s.nt;   // k-major: the tracers of a layer in a row
+    const int p = blockIdx.y, k = p / s.nt, t = p - k * s.nt;   // k-major: the tracers of a layer in a row
 
-    const double* cin = STAGE == 1 ? a.C : (STAGE == 2 ? a.c1 : a.c2);
-    const double* cp = cin + s.cell(t, k, 0, 0);
-    const double* ep = (a.inflow ? a.inflow : cin) + s.cell(t, k, 0, 0);
-    const uint8_t* okp = a.ok + s.geo(k, 0, 0);
-    const double* qxp = a.Qx + s.qx(k, 0, 0);
-    const double* qyp = a.Qy + s.qy(k, 0, 0);
+    const i64 pc = s.cell(t, k, 0, 0);
+    const i64 pg = s.geo(k, 0, 0);
+    // plane base pointers: every per-step address below is a 32-bit offset from one of them
+    const double* __restrict__ cin = (STAGE == 1 ? a.C : (STAGE == 2 ? a.c1 : a.c2)) + pc;
+    const uint8_t* __restrict__ okk = a.ok + pg;
+    const double* __restrict__ qxk = a.Qx + s.qx(k, 0, 0);
+    const double* __restrict__ qyk = a.Qy + s.qy(k, 0, 0);
+    const double* __restrict__ v0k = a.V0 + pg;
+    const double* __restrict__ v1k = a.V1 + pg;
+    const double* __restrict__ ck = a.C + pc;
+    const double* __restrict__ ek = a.inflow ? a.inflow + pc : cin;
+    double* __restrict__ sxk = a.Sx + s.ux(t, k, 0, 0);
+    double* __restrict__ syk = a.Sy + s.vy(t, k, 0, 0);
+    double* __restrict__ txk = a.Tx + s.ux(t, k, 0, 0);
+    double* __restrict__ tyk = a.Ty + s.vy(t, k, 0, 0);
+    const int nx1 = s.nx + 1;
     double* ring = &SM.row[warp][0][0];
     uint8_t* ringv = &SM.val[warp][0][0];
 
@@ -74,160 +75,193 @@ __global__ void __launch_bounds__(SWARPS * 32) fct_strip_kernel(StepArgs a)
         const int hc = i0 - 3 + hslot;
         hcol = fl.per_x ? wrap(hc, s.nx) : ((hc >= 0 && hc < s.nx) ? hc : -1);
     }
-    // x-face of this lane: face f = ci (between cells ci-1 and ci)
-    const bool has_x = ci <= s.nx;
+    const bool has_x = ci <= s.nx;                              // x-face ci exists
     const bool x_interior = fl.per_x || (ci >= 1 && ci <= s.nx - 1);
     const int qx_col = (fl.per_x && ci == s.nx) ? 0 : ci;
-    // y-faces of this lane's column exist for ci < nx
-    const bool has_col = ci < s.nx;
+    const bool has_col = ci < s.nx;                             // column ci exists (its y-faces, its cells)
     const bool cell_lane = lane < STRIP && has_col;
 
     auto load_row = [&](int r, double& mv, uint8_t& mo, double& hv, uint8_t& ho) {
         const int g = row_of(r, s, fl);
         mv = 0.0; mo = 0; hv = 0.0; ho = 0;
         if (g >= 0) {
-            const i64 base = (i64)g * s.nx;
-            if (mcol >= 0) { mv = __ldg(cp + base + mcol); mo = __ldg(okp + base + mcol); }
-            if (hcol >= 0) { hv = __ldg(cp + base + hcol); ho = __ldg(okp + base + hcol); }
+            const int base = g * s.nx;
+            if (mcol >= 0) { mv = __ldg(cin + base + mcol); mo = __ldg(okk + base + mcol); }
+            if (hcol >= 0) { hv = __ldg(cin + base + hcol); ho = __ldg(okk + base + hcol); }
         }
     };
+    auto slot_of = [&](int r) { return (r - jA + 8 * RING) % RING; };
     auto put_ring = [&](int r, double mv, uint8_t mo, double hv, uint8_t ho) {
-        const int slot = ((r % RING) + RING) % RING;
-        ring[slot * (RXW + 3) + lane + 3] = mv;
-        ringv[slot * (RXW + 3) + lane + 3] = mo;
+        const int sl = slot_of(r);
+        ring[sl * RXW + lane + 3] = mv;
+        ringv[sl * RXW + lane + 3] = mo;
         if (hslot >= 0) {
-            ring[slot * (RXW + 3) + hslot] = hv;
-            ringv[slot * (RXW + 3) + hslot] = ho;
+            ring[sl * RXW + hslot] = hv;
+            ringv[sl * RXW + hslot] = ho;
         }
     };
 
-    // prologue: y-window rows jA-3 .. jA+1 (slots 1..5 before the first shift), ring rows jA, jA+1, incoming jA+2
-    double w0 = 0.0, w1, w2, w3, w4, w5;
-    unsigned vb = 0;
-    {
-        double mv[5], hv[5];
-        uint8_t mo[5], ho[5];
-#pragma unroll
-        for (int r = 0; r < 5; ++r) load_row(jA - 3 + r, mv[r], mo[r], hv[r], ho[r]);
-        w1 = mv[0]; w2 = mv[1]; w3 = mv[2]; w4 = mv[3]; w5 = mv[4];
-        vb = ((unsigned)mo[0] << 1) | ((unsigned)mo[1] << 2) | ((unsigned)mo[2] << 3) | ((unsigned)mo[3] << 4) |
-             ((unsigned)mo[4] << 5);
-        put_ring(jA, mv[3], mo[3], hv[3], ho[3]);
-        put_ring(jA + 1, mv[4], mo[4], hv[4], ho[4]);
-    }
+    // prologue: rows jA-3 .. jA+2 into the ring, row jA+3 in flight
     double in_mv, in_hv;
     uint8_t in_mo, in_ho;
-    load_row(jA + 2, in_mv, in_mo, in_hv, in_ho);
-    // x- and y-face transports of the first step
-    double qx_next = (has_x && jA < s.ny) ? __ldg(qxp + (i64)jA * (s.nx + 1) + qx_col) : 0.0;
-    const int qy_row0 = (fl.per_y && jA == s.ny) ? 0 : jA;
-    double qy_next = has_col ? __ldg(qyp + (i64)qy_row0 * s.nx + ci) : 0.0;
+#pragma unroll 1
+    for (int r = jA - 3; r <= jA + 2; ++r) {
+        load_row(r, in_mv, in_mo, in_hv, in_ho);
+        put_ring(r, in_mv, in_mo, in_hv, in_ho);
+    }
+    load_row(jA + 3, in_mv, in_mo, in_hv, in_ho);
 
-    // stage 2 recomputes q1 = q0 - dt div F0 from the F0 faces kept by stage 1 (the same arithmetic as the stored
-    // value), so q1 is never stored; F0 of this lane's x-face of row j and y-face j are loaded one step ahead
-    const double* f0x = a.Sx + s.ux(t, k, 0, 0);
-    const double* f0y = a.Sy + s.vy(t, k, 0, 0);
-    auto load_f0 = [&](int j, double& x, double& y) {
-        x = (STAGE == 2 && has_x && j < s.ny) ? f0x[(i64)j * (s.nx + 1) + ci] : 0.0;
-        y = (STAGE == 2 && has_col && j <= s.ny) ? f0y[(i64)j * s.nx + ci] : 0.0;
+    // C, V0, V1 of this lane's cell are loaded one row ahead of the cell update; pass 3 also forms the donor fluxes
+    // F_L of its faces from these values (left neighbour by shuffle, the row below from the previous step)
+    const int lcol = fl.per_x ? wrap(i0 - 1, s.nx) : i0 - 1;  // lane 0's left neighbour column
+    auto crow_at = [&](int r) -> double {
+        const int g = row_of(r, s, fl);
+        return (g >= 0 && mcol >= 0) ? __ldg(ck + g * s.nx + mcol) : 0.0;   // periodic: column nx is column 0
     };
-    double f0x_next, f0y_next;
-    load_f0(jA, f0x_next, f0y_next);
+    double c_prev = STAGE == 3 ? crow_at(jA - 1) : 0.0;     // C of row j-1 (pass 3: the cell below face j)
+    double v0_prev = 0.0, v1_prev = 0.0;
+    double flx_prev = 0.0, fly_prev = 0.0;
 
+    // stage 2 recomputes q1 = q0 - dt div F0 from the F0 faces kept by stage 1 (the same arithmetic as the value
+    // stage 1 formed), so q1 is never stored
     double fx_prev = 0.0, fy_prev = 0.0, f0x_prev = 0.0, f0y_prev = 0.0;
+#pragma unroll 1
     for (int j = jA; j <= jB; ++j) {
-        // 1. slide the y-window: rows j-3 .. j+2
-        w0 = w1; w1 = w2; w2 = w3; w3 = w4; w4 = w5; w5 = in_mv;
-        vb = (vb >> 1) | ((unsigned)in_mo << 5);
-        // 2. stage row j+2 in the ring
-        put_ring(j + 2, in_mv, in_mo, in_hv, in_ho);
-        // 3. loads for the next step
-        const double qx_cur = qx_next, qy_cur = qy_next;
-        const double f0x_cur = f0x_next, f0y_cur = f0y_next;
-        if (j + 1 <= jB) {
-            load_f0(j + 1, f0x_next, f0y_next);
-            load_row(j + 3, in_mv, in_mo, in_hv, in_ho);
-            const int jn = j + 1;
-            qx_next = (has_x && jn < s.ny) ? __ldg(qxp + (i64)jn * (s.nx + 1) + qx_col) : 0.0;
-            const int qyr = (fl.per_y && jn == s.ny) ? 0 : jn;
-            qy_next = (has_col && jn <= s.ny) ? __ldg(qyp + (i64)qyr * s.nx + ci) : 0.0;
-        }
         __syncwarp();
-        // 4. x-face of row j (west face of column ci)
+        // face transports of this step (and F0 in stage 2)
+        const double qx = (j < jB && has_x) ? __ldg(qxk + j * nx1 + qx_col) : 0.0;
+        const double qy = has_col ? __ldg(qyk + ((fl.per_y && j == s.ny) ? 0 : j) * s.nx + ci) : 0.0;
+        double f0x = 0.0, f0y = 0.0;
+        if (STAGE == 2) {
+            f0x = (j < jB && has_x) ? sxk[j * nx1 + ci] : 0.0;
+            f0y = has_col ? syk[j * s.nx + ci] : 0.0;
+        }
+        // C, V0, V1 of row j (used by the update of row j at the next step, and by pass 3's donor fluxes now)
+        const double crow = (STAGE == 3 || j < jB) ? crow_at(j) : 0.0;
+        const bool row_in = j < jB && has_col;
+        const double v0row = row_in ? __ldg(v0k + j * s.nx + ci) : 0.0;
+        const double v1row = row_in ? __ldg(v1k + j * s.nx + ci) : 0.0;
+        double flx = 0.0, fly = 0.0;
+        if (STAGE == 3) {
+            // donor flux of x-face (j, ci) (sigma_baroclinic.py:486-494): left cell by shuffle (lane 0 loads it)
+            double cleft = __shfl_up_sync(0xffffffffu, crow, 1);
+            if (lane == 0) cleft = (lcol >= 0 && j < jB) ? __ldg(ck + j * s.nx + lcol) : 0.0;
+            if (j < jB && has_x) {
+                if (x_interior) {
+                    flx = qx * (qx >= 0 ? cleft : crow);
+                } else if (ci == 0) {
+                    flx = fl.open_w ? qx * (qx > 0 ? __ldg(a.inflow ? a.inflow + pc + j * s.nx : ck + j * s.nx) : crow)
+                                    : 0.0;
+                } else {
+                    flx = fl.open_e ? qx * (qx < 0 ? __ldg((a.inflow ? a.inflow + pc : ck) + j * s.nx + s.nx - 1)
+                                                   : cleft)
+                                    : 0.0;
+                }
+            }
+            // donor flux of y-face (j, ci) (:498-507): the cell below from the previous step
+            if (has_col) {
+                if (fl.per_y || (j >= 1 && j <= s.ny - 1)) {
+                    fly = qy * (qy >= 0 ? c_prev : crow);
+                } else if (j == 0) {
+                    fly = fl.open_s ? qy * (qy > 0 ? __ldg((a.inflow ? a.inflow + pc : ck) + ci) : crow) : 0.0;
+                } else {
+                    fly = fl.open_n ? qy * (qy < 0 ? __ldg((a.inflow ? a.inflow + pc : ck) + (s.ny - 1) * s.nx + ci)
+                                                   : c_prev)
+                                    : 0.0;
+                }
+            }
+        }
+        // x-face of row j (west face of column ci)
         double fx = 0.0;
         if (j < jB && has_x) {
             if (x_interior) {
-                if (qx_cur != 0.0) {
-                    const int slot = j % RING;
-                    fx = qx_cur * upwind_face_value(ring + slot * (RXW + 3) + lane, ringv + slot * (RXW + 3) + lane,
-                                                    1, qx_cur, fl.z);
+                if (qx != 0.0) {
+                    const int sl = slot_of(j);
+                    fx = qx * upwind_face<MIX>(ring + sl * RXW + lane, ringv + sl * RXW + lane, 1, qx, ZV);
                 }
             } else {
-                const i64 row = (i64)j * s.nx;
-                if (ci == 0) fx = fl.open_w ? qx_cur * (qx_cur > 0.0 ? ep[row] : cp[row]) : 0.0;
-                else fx = fl.open_e ? qx_cur * (qx_cur < 0.0 ? ep[row + s.nx - 1] : cp[row + s.nx - 1]) : 0.0;
+                const int row = j * s.nx;
+                if (ci == 0) fx = fl.open_w ? qx * (qx > 0.0 ? ek[row] : cin[row]) : 0.0;
+                else fx = fl.open_e ? qx * (qx < 0.0 ? ek[row + s.nx - 1] : cin[row + s.nx - 1]) : 0.0;
             }
         }
-        // 5. y-face j of this column
+        // y-face j of this column: cells j-3 .. j+2 are ring rows
         double fy = 0.0;
         if (has_col) {
             if (fl.per_y || (j >= 1 && j <= s.ny - 1)) {
-                if (qy_cur != 0.0) fy = qy_cur * upwind_face_reg(w0, w1, w2, w3, w4, w5, vb, qy_cur, fl.z);
-            } else if (j == 0) {
-                fy = fl.open_s ? qy_cur * (qy_cur > 0.0 ? ep[ci] : cp[ci]) : 0.0;
+                if (qy != 0.0) {
+                    const int s0 = slot_of(j - 3);
+                    double w[6];
+                    uint8_t v[6];
+#pragma unroll
+                    for (int m = 0; m < 6; ++m) {
+                        const int sl = (s0 + m) & (RING - 1);
+                        w[m] = ring[sl * RXW + lane + 3];
+                        v[m] = ringv[sl * RXW + lane + 3];
+                    }
+                    fy = qy * upwind_face<MIX>(w, v, 1, qy, ZV);
+                }
             } else {
-                const i64 o = (i64)(s.ny - 1) * s.nx + ci;
-                fy = fl.open_n ? qy_cur * (qy_cur < 0.0 ? ep[o] : cp[o]) : 0.0;
+                if (j == 0) {
+                    fy = fl.open_s ? qy * (qy > 0.0 ? ek[ci] : cin[ci]) : 0.0;
+                } else {
+                    const int o = (s.ny - 1) * s.nx + ci;
+                    fy = fl.open_n ? qy * (qy < 0.0 ? ek[o] : cin[o]) : 0.0;
+                }
             }
         }
-        // 6. cell update of row j-1 with faces: west fx_prev, east = lane+1's fx_prev, south fy_prev, north fy
+        // row j+3 enters the ring (its slot held row j-5, read for the last time two steps ago), row j+4 in flight
+        put_ring(j + 3, in_mv, in_mo, in_hv, in_ho);
+        if (j + 1 <= jB) load_row(j + 4, in_mv, in_mo, in_hv, in_ho);
+
+        // cell update of row j-1: west fx_prev, east = lane+1's fx_prev, south fy_prev, north fy
         const double fx_east = __shfl_down_sync(0xffffffffu, fx_prev, 1);
-        const double f0_east = __shfl_down_sync(0xffffffffu, f0x_prev, 1);
+        const double f0_east = STAGE == 2 ? __shfl_down_sync(0xffffffffu, f0x_prev, 1) : 0.0;
+        const double fl_east = STAGE == 3 ? __shfl_down_sync(0xffffffffu, flx_prev, 1) : 0.0;
         if (j > jA && cell_lane) {
             const int jc = j - 1;
-            const i64 w = s.ux(t, k, jc, ci), so = s.vy(t, k, jc, ci);
-            const i64 g = s.geo(k, jc, ci), cc = s.cell(t, k, jc, ci);
-            const double v0 = __ldg(a.V0 + g), v1 = __ldg(a.V1 + g), c0 = __ldg(a.C + cc);
+            const int w = jc * nx1 + ci, so = jc * s.nx + ci, cc = jc * s.nx + ci;
+            const double v0 = v0_prev, v1 = v1_prev, c0 = c_prev;
             const double d = fx_east - fx_prev + fy - fy_prev;
             const double q0 = v0 * c0;
             if (STAGE == 1) {
-                a.Sx[w] = fx_prev;
-                a.Sy[so] = fy_prev;
-                if (ci == s.nx - 1) a.Sx[w + 1] = fx_east;
-                if (jc == s.ny - 1) a.Sy[so + s.nx] = fy;
+                sxk[w] = fx_prev;
+                syk[so] = fy_prev;
+                if (ci == s.nx - 1) sxk[w + 1] = fx_east;
+                if (jc == s.ny - 1) syk[so + s.nx] = fy;
                 const double q = 0.0 * q0 + 1.0 * (q0 - a.dt * d);
                 const double v = v0 + (v1 - v0);
-                a.c1[cc] = v > 0.0 ? q / v : c0;
+                a.c1[pc + cc] = v > 0.0 ? q / v : c0;
             } else if (STAGE == 2) {
-                a.Tx[w] = div6_exact(f0x_prev + fx_prev);
-                a.Ty[so] = div6_exact(f0y_prev + fy_prev);
-                if (ci == s.nx - 1) a.Tx[w + 1] = div6_exact(f0_east + fx_east);
-                if (jc == s.ny - 1) a.Ty[so + s.nx] = div6_exact(f0y_cur + fy);
-                const double d0 = f0_east - f0x_prev + f0y_cur - f0y_prev;
+                txk[w] = div6_exact(f0x_prev + fx_prev);
+                tyk[so] = div6_exact(f0y_prev + fy_prev);
+                if (ci == s.nx - 1) txk[w + 1] = div6_exact(f0_east + fx_east);
+                if (jc == s.ny - 1) tyk[so + s.nx] = div6_exact(f0y + fy);
+                const double d0 = f0_east - f0x_prev + f0y - f0y_prev;
                 const double q1 = 0.0 * q0 + 1.0 * (q0 - a.dt * d0);
                 const double q = 0.75 * q0 + 0.25 * (q1 - a.dt * d);
                 const double v = v0 + 0.5 * (v1 - v0);
-                a.c2[cc] = v > 0.0 ? q / v : c0;
+                a.c2[pc + cc] = v > 0.0 ? q / v : c0;
             } else {
-                const double* Cp = a.C + s.cell(t, k, 0, 0);
-                const double* eL = a.inflow ? a.inflow + s.cell(t, k, 0, 0) : Cp;
-                const double flw = donor_x(Cp, eL, a.Qx, s, fl, k, jc, ci);
-                const double fle = donor_x(Cp, eL, a.Qx, s, fl, k, jc, ci + 1);
-                const double fls = donor_y(Cp, eL, a.Qy, s, fl, k, jc, ci);
-                const double fln = donor_y(Cp, eL, a.Qy, s, fl, k, jc + 1, ci);
-                a.Sx[w] = (a.Tx[w] + div3_exact(2.0 * fx_prev)) - flw;
-                a.Sy[so] = (a.Ty[so] + div3_exact(2.0 * fy_prev)) - fls;
-                if (ci == s.nx - 1) a.Sx[w + 1] = (a.Tx[w + 1] + div3_exact(2.0 * fx_east)) - fle;
-                if (jc == s.ny - 1) a.Sy[so + s.nx] = (a.Ty[so + s.nx] + div3_exact(2.0 * fy)) - fln;
+                const double flw = flx_prev, fle = fl_east, fls = fly_prev, fln = fly;
+                sxk[w] = (txk[w] + div3_exact(2.0 * fx_prev)) - flw;
+                syk[so] = (tyk[so] + div3_exact(2.0 * fy_prev)) - fls;
+                if (ci == s.nx - 1) sxk[w + 1] = (txk[w + 1] + div3_exact(2.0 * fx_east)) - fle;
+                if (jc == s.ny - 1) syk[so + s.nx] = (tyk[so + s.nx] + div3_exact(2.0 * fy)) - fln;
                 const double dl = fle - flw + fln - fls;
                 const double q = 0.0 * q0 + 1.0 * (q0 - a.dt * dl);
-                a.q1[cc] = v1 > 0 ? q / v1 : c0;               // c_L
+                a.q1[pc + cc] = v1 > 0 ? q / v1 : c0;          // c_L
             }
         }
-        f0x_prev = f0x_cur;
-        f0y_prev = f0y_cur;
+        c_prev = crow;
+        v0_prev = v0row;
+        v1_prev = v1row;
+        flx_prev = flx;
+        fly_prev = fly;
         fx_prev = fx;
         fy_prev = fy;
+        f0x_prev = f0x;
+        f0y_prev = f0y;
     }
 }
 

@@ -66,4 +66,89 @@ __device__ __forceinline__ double upwind_face_value(const double* w, const uint8
                        pos ? b0 : b5, pos ? b1 : b4, pos ? b2 : b3, pos ? b3 : b2, pos ? b4 : b1, z);
 }
 
+// ---------------------------------------------------------------------------------------------------------------
+// Mixed-precision WENO5 face value: the smoothness indicators, the nonlinear weights and the weighted candidate
+// run in FP32 on the differences of the stencil from the upwind cell (formed in FP64, then rounded), normalised by
+// their largest magnitude s; the result is added back to the FP64 upwind value: face = v3 + s * w(d/s).  Every
+// quantity of the scheme is a function of these differences (q_r - v3 and beta_r are linear / quadratic forms in
+// them), so the FP32 rounding acts on the local variation only (relative face error ~1e-7 of s, not of v3).  The
+// normalisation keeps beta_r in [0, 40] so FP32 cannot overflow; WENO5-Z's epsilon, 1e-40 in FP64, becomes 1e-30 on
+// the normalised scale (both are negligible against any non-zero beta_r, and both give the same limit when a
+// beta_r vanishes).  Stencils whose variation is outside what the FP32 forms represent safely (s below 1e-30 or,
+// for the absolute-epsilon forms WENO5-JS and WENO3, above 1e8) keep the FP64 arithmetic of weno5_value.
+
+__device__ __forceinline__ double weno5_value_mixed(double v1, double v2, double v3, double v4, double v5,
+                                                    bool k1, bool k2, bool k3, bool k4, bool k5, bool z_variant)
+{
+    if (k1 && k2 && k3 && k4 && k5) {
+        const float e1 = (float)(v1 - v3), e2 = (float)(v2 - v3), e4 = (float)(v4 - v3), e5 = (float)(v5 - v3);
+        const float sc = fmaxf(fmaxf(fabsf(e1), fabsf(e2)), fmaxf(fabsf(e4), fabsf(e5)));
+        if (sc == 0.f) {
+            if (v1 == v3 && v2 == v3 && v4 == v3 && v5 == v3) return v3;      // flat: every candidate is v3
+            return weno5_value(v1, v2, v3, v4, v5, k1, k2, k3, k4, k5, z_variant);
+        }
+        if (!(sc > 1e-30f) || (!z_variant && sc > 1e8f))
+            return weno5_value(v1, v2, v3, v4, v5, k1, k2, k3, k4, k5, z_variant);
+        const float inv = 1.f / sc;
+        const float d1 = e1 * inv, d2 = e2 * inv, d4 = e4 * inv, d5 = e5 * inv;
+        const float c1312 = 13.f / 12.f;
+        float t = fmaf(-2.f, d2, d1), u = fmaf(-4.f, d2, d1);
+        const float b0 = fmaf(c1312 * t, t, 0.25f * u * u);
+        t = d2 + d4;
+        u = d2 - d4;
+        const float b1 = fmaf(c1312 * t, t, 0.25f * u * u);
+        t = fmaf(-2.f, d4, d5);
+        u = fmaf(-4.f, d4, d5);
+        const float b2 = fmaf(c1312 * t, t, 0.25f * u * u);
+        const float tau = fabsf(b2 - b0);
+        float a0, a1, a2;
+        if (z_variant) {
+            a0 = 0.1f * (1.f + __fdividef(tau, 1e-30f + b0));
+            a1 = 0.6f * (1.f + __fdividef(tau, 1e-30f + b1));
+            a2 = 0.3f * (1.f + __fdividef(tau, 1e-30f + b2));
+        } else {
+            // JS weights use an absolute epsilon (1e-6): un-normalise beta (s <= 1e8 keeps the squares finite)
+            const float s2 = sc * sc;
+            const float g0 = fmaf(s2, b0, 1e-6f), g1 = fmaf(s2, b1, 1e-6f), g2 = fmaf(s2, b2, 1e-6f);
+            a0 = __fdividef(0.1f, g0 * g0);
+            a1 = __fdividef(0.6f, g1 * g1);
+            a2 = __fdividef(0.3f, g2 * g2);
+        }
+        // 6 (q_r - v3) / s
+        const float p0 = fmaf(2.f, d1, -7.f * d2), p1 = fmaf(2.f, d4, -d2), p2 = fmaf(5.f, d4, -d5);
+        const float num = fmaf(a0, p0, fmaf(a1, p1, a2 * p2));
+        const float den = 6.f * (a0 + a1 + a2);
+        return v3 + (double)(sc * __fdividef(num, den));
+    }
+    if (k2 && k3 && k4) {
+        // WENO3 (absolute eps 1e-6): candidates v3 - e2/2 and v3 + e4/2
+        const float d2 = (float)(v2 - v3), d4 = (float)(v4 - v3);
+        if (!(fmaxf(fabsf(d2), fabsf(d4)) <= 1e8f)) return weno5_value(v1, v2, v3, v4, v5, k1, k2, k3, k4, k5, z_variant);
+        const float g0 = fmaf(d2, d2, 1e-6f), g1 = fmaf(d4, d4, 1e-6f);
+        const float w0 = __fdividef(1.f / 3.f, g0 * g0), w1 = __fdividef(2.f / 3.f, g1 * g1);
+        const float corr = __fdividef(fmaf(w1, 0.5f * d4, -w0 * 0.5f * d2), w0 + w1);
+        return v3 + (double)corr;
+    }
+    return v3;
+}
+
+template <bool MIX>
+__device__ __forceinline__ double weno5_face(double v1, double v2, double v3, double v4, double v5, bool k1, bool k2,
+                                             bool k3, bool k4, bool k5, bool z)
+{
+    if (MIX) return weno5_value_mixed(v1, v2, v3, v4, v5, k1, k2, k3, k4, k5, z);
+    return weno5_value(v1, v2, v3, v4, v5, k1, k2, k3, k4, k5, z);
+}
+
+// Upwind face value with the arithmetic selected at compile time (MIX: FP32 weights).
+template <bool MIX>
+__device__ __forceinline__ double upwind_face(const double* w, const uint8_t* v, int step, double q, bool z)
+{
+    const bool pos = q >= 0.0;
+    const double w0 = w[0], w1 = w[step], w2 = w[2 * step], w3 = w[3 * step], w4 = w[4 * step], w5 = w[5 * step];
+    const bool b0 = v[0], b1 = v[step], b2 = v[2 * step], b3 = v[3 * step], b4 = v[4 * step], b5 = v[5 * step];
+    return weno5_face<MIX>(pos ? w0 : w5, pos ? w1 : w4, pos ? w2 : w3, pos ? w3 : w2, pos ? w4 : w1,
+                           pos ? b0 : b5, pos ? b1 : b4, pos ? b2 : b3, pos ? b3 : b2, pos ? b4 : b1, z);
+}
+
 }  // namespace po

@@ -18,10 +18,11 @@ class ALETracerStep:
     """advect_fct + PPM_H4 (or PCM / PLM) remap of a (nt, N, ny, nx) stack with preallocated buffers."""
 
     def __init__(self, nt: int, n: int, ny: int, nx: int, dt: float, flags: int = 0, remap_scheme: int = 2,
-                 n_tgt: int | None = None, device=None) -> None:
+                 n_tgt: int | None = None, device=None, mixed: bool = False) -> None:
         self.nt, self.n, self.ny, self.nx = nt, n, ny, nx
         self.n1 = n if n_tgt is None else n_tgt
         self.dt, self.flags, self.remap_scheme = float(dt), int(flags), int(remap_scheme)
+        self.mixed = bool(mixed)
         self.device = torch.device("cuda", torch.cuda.current_device()) if device is None else torch.device(device)
         L = _lib.lib()
         self.ws_bytes = L.pocean_advect_fct_workspace_bytes(nt, n, ny, nx)
@@ -34,7 +35,9 @@ class ALETracerStep:
 
     def advect(self, C, V0, V1, Qx, Qy, ok, out=None, inflow=None) -> torch.Tensor:
         out = self.adv_out if out is None else out
-        rc = _lib.lib().pocean_advect_fct_f64(C.data_ptr(), V0.data_ptr(), V1.data_ptr(), Qx.data_ptr(),
+        L = _lib.lib()
+        fn = L.pocean_advect_fct_mixed if self.mixed else L.pocean_advect_fct_f64
+        rc = fn(C.data_ptr(), V0.data_ptr(), V1.data_ptr(), Qx.data_ptr(),
                                               Qy.data_ptr(), ok.data_ptr(),
                                               None if inflow is None else inflow.data_ptr(), self.nt, self.n,
                                               self.ny, self.nx, self.flags, self.dt, out.data_ptr(), 0, None, None,

@@ -36,8 +36,13 @@ class TracerAdvection:
     writes = ("T", "tr")
     per = NONE
 
-    def __init__(self, *, scheme: str, time: str, dt: float, ob=None) -> None:
+    def __init__(self, *, scheme: str, time: str, dt: float, ob=None, precision: str = "f64") -> None:
+        """``precision``: "f64" (the reference's arithmetic, bit for bit) or "mixed" (WENO5 weights and face values
+        in FP32, everything else in FP64; ``advect_fct`` only)."""
+        if precision not in ("f64", "mixed"):
+            raise ValueError(f"precision must be 'f64' or 'mixed', got {precision!r}")
         self.tracer_scheme, self.tracer_time, self.dt = scheme, time, dt
+        self.precision = precision
         self.ob = ob if ob is not None else OpenEdges()
         self.record_open_flux = False
         self.last_open_flux: np.ndarray | None = None
@@ -102,7 +107,8 @@ class TracerAdvection:
         L = _lib.lib()
         nbytes = L.pocean_advect_fct_workspace_bytes(nt, n, ny, nx)
         ws = cv.workspace(nbytes)
-        rc = L.pocean_advect_fct_f64(Cd.data_ptr(), V0d.data_ptr(), V1d.data_ptr(), Qxd.data_ptr(), Qyd.data_ptr(),
+        fn = L.pocean_advect_fct_mixed if self.precision == "mixed" else L.pocean_advect_fct_f64
+        rc = fn(Cd.data_ptr(), V0d.data_ptr(), V1d.data_ptr(), Qxd.data_ptr(), Qyd.data_ptr(),
                                      okd.data_ptr(), None if infl is None else infl.data_ptr(), nt, n, ny, nx, flags,
                                      float(self.dt), out.data_ptr(), fi, None if fx is None else fx.data_ptr(),
                                      None if of is None else of.data_ptr(), ws.data_ptr(), nbytes, cv.stream())
@@ -122,6 +128,8 @@ class TracerAdvection:
         """
         if self.tracer_time == "pc":
             raise NotImplementedError("tracer_time='pc' runs the reference's NumPy path; not implemented on GPU")
+        if self.precision != "f64":
+            raise NotImplementedError("advect (no limiter) is available in FP64 only")
         if not self.tracer_scheme.startswith("weno5"):
             raise NotImplementedError(f"tracer_scheme={self.tracer_scheme!r}: only the WENO5 schemes are on GPU")
         nt, n, ny, nx = self._shapes(C, Qx, Qy)

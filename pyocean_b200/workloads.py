@@ -136,7 +136,10 @@ def hybrid_target(H: np.ndarray, n: int) -> np.ndarray:
     return h
 
 
-def basin(seed: int = 0, nx: int = 512, ny: int = 512, n: int = 50, nt: int = 2) -> Workload:
+def basin(seed: int = 0, nx: int = 512, ny: int = 512, n: int = 50, nt: int = 2, passive: str = "uniform") -> Workload:
+    """The curvilinear basin.  Tracers: T, S, then nt - 2 passive ones — uniform noise in [0, 1] (``passive=
+    "uniform"``) or sharp top-hat patches of 1 in a field of 0 (``passive="tophat"``, the limiter stress test of
+    the 1024 x 1024 x 75 mixed-precision configuration)."""
     rng = np.random.default_rng(seed)
     dx = 2000.0 * (1 + 0.05 * _smooth_noise(rng, (ny, nx), 64.0))
     dy = 2000.0 * (1 + 0.05 * _smooth_noise(rng, (ny, nx), 64.0))
@@ -188,7 +191,21 @@ def basin(seed: int = 0, nx: int = 512, ny: int = 512, n: int = 50, nt: int = 2)
         eddy += rng.choice([-1.0, 1.0]) * np.exp(-((x - cx) ** 2 + (y - cy) ** 2) / (2 * r * r))
     T = 25.0 - 21.0 * frac + np.clip(eddy, -1, 1)[None]
     S = 34.0 + 1.0 * frac
-    stack = [T, S] + [rng.uniform(0, 1, T.shape) for _ in range(max(0, nt - 2))]
+    extra = []
+    for _ in range(max(0, nt - 2)):
+        if passive == "tophat":
+            f = np.zeros((ny, nx))
+            for _ in range(6):
+                cx, cy = rng.uniform(0.1, 0.9) * nx, rng.uniform(0.1, 0.9) * ny
+                r = rng.uniform(0.03, 0.1) * nx
+                f[(x - cx) ** 2 + (y - cy) ** 2 < r * r] = 1.0
+            k0, k1 = sorted(rng.integers(0, n, 2))
+            g = np.zeros((n, ny, nx))
+            g[k0:k1 + 1] = f
+            extra.append(g)
+        else:
+            extra.append(rng.uniform(0, 1, T.shape))
+    stack = [T, S] + extra
     C = np.stack(stack[:nt])
     h_src = h * (1 + rng.uniform(-0.3, 0.3, h.shape))
     col = h_src.sum(0)
