@@ -129,6 +129,51 @@ int pocean_advect_rk3_f64(const double* C, const double* V0, const double* V1, c
 int pocean_remap_columns_f64(const double* h_src, const double* f_src, const double* h_tgt, const uint8_t* wet,
                              int n0, int n1, int ny, int nx, int nfields, int scheme, double* out, void* stream);
 
+/*
+ * Batched steps of many independent domains (no counterpart in the reference, which advances one model at a time):
+ * one ALE tracer step = advect_fct of the stack C then the remap of the advected stack C_adv onto the target grid,
+ * into C_next.  Every pass is one launch over all domains; pocean_batch_step only enqueues kernels, so a sequence
+ * of steps can be captured in a CUDA graph.  Parity 0 reads C and writes C_next, parity 1 reads C_next and writes C
+ * (C is written: it is the ping-pong partner).  Results of each domain equal pocean_advect_fct_f64 (or _mixed)
+ * followed by pocean_remap_columns_f64 on that domain alone.
+ */
+typedef struct pocean_domain {
+    const double* C;          /* (nt, nz, ny, nx) stack at parity 0 */
+    const double* V0;         /* (nz, ny, nx) */
+    const double* V1;
+    const double* Qx;         /* (nz, ny, nx+1) */
+    const double* Qy;         /* (nz, ny+1, nx) */
+    const uint8_t* ok;        /* (nz, ny, nx) */
+    const double* inflow;     /* (nt, nz, ny, nx) or NULL */
+    int nt, nz, ny, nx;
+    unsigned flags;           /* POCEAN_OPEN_*, POCEAN_PERIODIC_*, POCEAN_WENO_JS (the same variant for all) */
+    double dt;
+    double* C_adv;            /* (nt, nz, ny, nx) advected stack */
+    void* workspace;          /* pocean_advect_fct_workspace_bytes(nt, nz, ny, nx) bytes, 256-byte aligned */
+    size_t workspace_bytes;
+    const double* h_src;      /* (nz, ny, nx) source thicknesses of the remap */
+    const double* h_tgt;      /* (nz, ny, nx) target thicknesses */
+    const uint8_t* wet;       /* (ny, nx) */
+    int remap_scheme;         /* POCEAN_PCM / POCEAN_PLM / POCEAN_PPM_H4 */
+    double* C_next;           /* (nt, nz, ny, nx) remapped stack */
+} pocean_domain;
+
+typedef struct pocean_batch pocean_batch;   /* host-side plan of a batch */
+
+/* Device bytes of the batch plan for ndom domains (descriptors of both parities and the CTA-offset tables). */
+size_t pocean_batch_device_bytes(int ndom);
+
+/* Validates the domains and writes the plan into device_buf (synchronous copy; call outside stream capture).
+ * seglen: rows per warp segment of the WENO passes (a tuning parameter; results do not depend on it). */
+int pocean_batch_create(const pocean_domain* domains, int ndom, int seglen, void* device_buf, size_t device_bytes,
+                        pocean_batch** out);
+
+/* Enqueues one step of every domain.  remap_nf: fields per remap thread (1 or 2, a tuning parameter); mixed: FP32
+ * WENO weights (pocean_advect_fct_mixed) instead of FP64. */
+int pocean_batch_step(const pocean_batch* b, int parity, int remap_nf, int mixed, void* stream);
+
+void pocean_batch_destroy(pocean_batch* b);
+
 #ifdef __cplusplus
 }
 #endif

@@ -35,6 +35,10 @@ SIGNATURES: dict[str, tuple] = {
     "pocean_advect_rk3_f64": (_I, [_P, _P, _P, _P, _P, _P, _P, _P, _I, _I, _I, _I, _U, _D, _P, _I, _P, _P, _Z,
                                    _P]),
     "pocean_remap_columns_f64": (_I, [_P, _P, _P, _P, _I, _I, _I, _I, _I, _I, _P, _P]),
+    "pocean_batch_device_bytes": (_Z, [_I]),
+    "pocean_batch_create": (_I, [_P, _I, _I, _P, _Z, ctypes.POINTER(_P)]),
+    "pocean_batch_step": (_I, [_P, _I, _I, _I, _P]),
+    "pocean_batch_destroy": (None, [_P]),
 }
 
 _LIB: ctypes.CDLL | None = None

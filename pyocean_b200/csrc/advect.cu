@@ -27,6 +27,7 @@
 #include <cstdio>
 
 #include "common.cuh"
+#include "fct_args.cuh"
 #include "weno.cuh"
 
 namespace po {
@@ -37,44 +38,6 @@ constexpr int HALO = 3;         // WENO5 stencil radius
 constexpr int NTHREADS = TI * TJ;
 constexpr int SW = TI + 2 * HALO;   // shared tile row length
 constexpr int SH = TJ + 2 * HALO;   // shared tile rows
-
-struct Flags {
-    bool open_w, open_e, open_s, open_n, per_x, per_y, z;
-    __host__ __device__ explicit Flags(unsigned f)
-        : open_w(f & POCEAN_OPEN_W), open_e(f & POCEAN_OPEN_E), open_s(f & POCEAN_OPEN_S),
-          open_n(f & POCEAN_OPEN_N), per_x(f & POCEAN_PERIODIC_X), per_y(f & POCEAN_PERIODIC_Y),
-          z(!(f & POCEAN_WENO_JS)) {}
-};
-
-// Everything one FCT / RK3 step reads and writes.
-struct StepArgs {
-    Shape s;
-    unsigned flags;
-    double dt;
-    const double* __restrict__ C;
-    const double* __restrict__ V0;
-    const double* __restrict__ V1;
-    const double* __restrict__ Qx;
-    const double* __restrict__ Qy;
-    const double* __restrict__ Fz;      // RK3 only (nullable)
-    const uint8_t* __restrict__ ok;
-    const double* __restrict__ inflow;  // nullable
-    // workspace
-    double* q1;
-    double* c1;
-    double* q2;
-    double* c2;
-    double* Sx;                         // FCT: F0, then the antidiffusive flux A
-    double* Sy;
-    double* Tx;                         // FCT: (F0 + F1)/6
-    double* Ty;
-    double* tef0;                       // RK3 TEF column accumulators (nt, n, ny)
-    double* tef1;
-    // outputs
-    double* out;
-    int face_i;
-    double* fx_face;
-};
 
 // ---------------------------------------------------------------------------------------------------------------
 // Shared-memory tile of one (t, k) plane of a cell field with a HALO-cell border.  Out-of-domain cells (closed or
@@ -247,12 +210,10 @@ __global__ void __launch_bounds__(NTHREADS) fct_unlimited_kernel(StepArgs a)
 
 // Pass 4: Zalesak R+ / R- (sigma_baroclinic.py:407-432): bounds over the cell, its x / y neighbours and the layers
 // k +- 1 (ok cells), P from the antidiffusive fluxes of the cell's faces, Q from V1 and c_L.
-__global__ void __launch_bounds__(NTHREADS) fct_coeff_kernel(StepArgs a)
+__device__ __forceinline__ void coeff_body(const StepArgs& a, int i, int j, int k)
 {
     const Shape s = a.s;
     const Flags fl(a.flags);
-    const int i = blockIdx.x * TI + threadIdx.x % TI, j = blockIdx.y * TJ + threadIdx.x / TI;
-    const int k = blockIdx.z;
     if (i >= s.nx || j >= s.ny) return;
     const double* cL = a.q1;
     // the 7-point stencil of the bounds: cell, x / y neighbours, layers k -+ 1 (ok cells only); its geometry is
@@ -349,12 +310,10 @@ __device__ __forceinline__ double face_flux(bool interior, bool open, bool inflo
     return fl + 0.0 * A;
 }
 
-__global__ void __launch_bounds__(NTHREADS) fct_final_kernel(StepArgs a)
+__device__ __forceinline__ void final_body(const StepArgs& a, int i, int j, int k)
 {
     const Shape s = a.s;
     const Flags fl(a.flags);
-    const int i = blockIdx.x * TI + threadIdx.x % TI, j = blockIdx.y * TJ + threadIdx.x / TI;
-    const int k = blockIdx.z;
     if (i >= s.nx || j >= s.ny) return;
     // neighbours (wrapped on periodic axes, -1 outside the domain) and which faces are interior
     const int iw = fl.per_x ? wrap(i - 1, s.nx) : i - 1, ie = fl.per_x ? wrap(i + 1, s.nx) : (i + 1 < s.nx ? i + 1 : -1);
@@ -393,6 +352,50 @@ __global__ void __launch_bounds__(NTHREADS) fct_final_kernel(StepArgs a)
         const double q = v0 * c0 - a.dt * d;
         a.out[pc + o_c] = v1 > 0 ? q / v1 : c0;
     }
+}
+
+// Single-domain launches of passes 4 and 5: a 32 x 8 tile of one layer per CTA.
+__global__ void __launch_bounds__(NTHREADS) fct_coeff_kernel(StepArgs a)
+{
+    coeff_body(a, blockIdx.x * TI + threadIdx.x % TI, blockIdx.y * TJ + threadIdx.x / TI, blockIdx.z);
+}
+
+__global__ void __launch_bounds__(NTHREADS) fct_final_kernel(StepArgs a)
+{
+    final_body(a, blockIdx.x * TI + threadIdx.x % TI, blockIdx.y * TJ + threadIdx.x / TI, blockIdx.z);
+}
+
+// Batched launches of passes 4 and 5: domain d owns CTAs off[d] .. off[d+1]-1, one 32 x 8 tile of one layer each.
+__device__ __forceinline__ void batched_tile(const BatchDomain* __restrict__ doms, const int* __restrict__ off,
+                                             int ndom, int& d, int& i, int& j, int& k)
+{
+    d = find_domain(off, ndom, blockIdx.x);
+    const Shape s = doms[d].a.s;
+    const int tx = ceil_div(s.nx, TI), ty = ceil_div(s.ny, TJ);
+    int local = blockIdx.x - __ldg(off + d);
+    k = local / (tx * ty);
+    local -= k * tx * ty;
+    const int by = local / tx, bx = local - by * tx;
+    i = bx * TI + threadIdx.x % TI;
+    j = by * TJ + threadIdx.x / TI;
+}
+
+__global__ void __launch_bounds__(NTHREADS) fct_coeff_batched(const BatchDomain* __restrict__ doms,
+                                                               const int* __restrict__ off, int ndom)
+{
+    int d, i, j, k;
+    batched_tile(doms, off, ndom, d, i, j, k);
+    const StepArgs a = doms[d].a;
+    coeff_body(a, i, j, k);
+}
+
+__global__ void __launch_bounds__(NTHREADS) fct_final_batched(const BatchDomain* __restrict__ doms,
+                                                               const int* __restrict__ off, int ndom)
+{
+    int d, i, j, k;
+    batched_tile(doms, off, ndom, d, i, j, k);
+    const StepArgs a = doms[d].a;
+    final_body(a, i, j, k);
 }
 
 // Effective flux F_L + C A of the step through u-face column face_i, (nt, n, ny) (tracers.py:251-254).
@@ -539,6 +542,24 @@ using namespace po;
 
 static size_t align_up(size_t b) { return (b + 255) & ~(size_t)255; }
 
+// The FCT workspace of shape a.s cut into its buffers (layout of pocean_advect_fct_workspace_bytes).
+void po::carve_fct_workspace(StepArgs& a, void* workspace)
+{
+    const Shape& s = a.s;
+    char* w = (char*)workspace;
+    const size_t cells = align_up((size_t)s.nt * s.n * s.ny * s.nx * sizeof(double));
+    a.q1 = (double*)w; w += cells;
+    a.c1 = (double*)w; w += cells;
+    a.c2 = (double*)w; w += cells;
+    const size_t xf = align_up((size_t)s.nt * s.n * s.ny * (s.nx + 1) * sizeof(double));
+    const size_t yf = align_up((size_t)s.nt * s.n * (s.ny + 1) * s.nx * sizeof(double));
+    a.Sx = (double*)w; w += xf;
+    a.Sy = (double*)w; w += yf;
+    a.Tx = (double*)w; w += xf;
+    a.Ty = (double*)w;
+    a.q2 = nullptr; a.tef0 = a.tef1 = nullptr;
+}
+
 static int check_shape(const char* fn, int nt, int nz, int ny, int nx)
 {
     if (nt < 1 || nz < 1 || ny < 1 || nx < 1)
@@ -588,9 +609,9 @@ static int common_checks(const char* fn, const void* C, const void* V0, const vo
 template <bool ZV, bool MIX>
 static void launch_strips(const StepArgs& a, int stage, dim3 grid, int nstrips, int nsegs, cudaStream_t st)
 {
-    if (stage == 1) fct_strip_kernel<1, ZV, MIX><<<grid, SWARPS * 32, 0, st>>>(a, nstrips, nsegs);
-    else if (stage == 2) fct_strip_kernel<2, ZV, MIX><<<grid, SWARPS * 32, 0, st>>>(a, nstrips, nsegs);
-    else fct_strip_kernel<3, ZV, MIX><<<grid, SWARPS * 32, 0, st>>>(a, nstrips, nsegs);
+    if (stage == 1) fct_strip_kernel<1, ZV, MIX><<<grid, SWARPS * 32, 0, st>>>(a, SEG, nstrips, nsegs);
+    else if (stage == 2) fct_strip_kernel<2, ZV, MIX><<<grid, SWARPS * 32, 0, st>>>(a, SEG, nstrips, nsegs);
+    else fct_strip_kernel<3, ZV, MIX><<<grid, SWARPS * 32, 0, st>>>(a, SEG, nstrips, nsegs);
 }
 
 // The FCT step with FP64 (mixed = false) or FP32-weight (mixed = true) WENO faces; everything else FP64.
@@ -613,18 +634,7 @@ static int advect_fct_impl(const char* fn, bool mixed, const double* C, const do
     a.flags = flags;
     a.dt = dt;
     a.C = C; a.V0 = V0; a.V1 = V1; a.Qx = Qx; a.Qy = Qy; a.Fz = nullptr; a.ok = ok; a.inflow = inflow;
-    char* w = (char*)workspace;
-    const size_t cells = align_up((size_t)nt * nz * ny * nx * sizeof(double));
-    a.q1 = (double*)w; w += cells;
-    a.c1 = (double*)w; w += cells;
-    a.c2 = (double*)w; w += cells;
-    const size_t xf = align_up((size_t)nt * nz * ny * (nx + 1) * sizeof(double));
-    const size_t yf = align_up((size_t)nt * nz * (ny + 1) * nx * sizeof(double));
-    a.Sx = (double*)w; w += xf;
-    a.Sy = (double*)w; w += yf;
-    a.Tx = (double*)w; w += xf;
-    a.Ty = (double*)w;
-    a.q2 = nullptr; a.tef0 = a.tef1 = nullptr;
+    carve_fct_workspace(a, workspace);
     a.out = C_out; a.face_i = face_i; a.fx_face = fx_face;
 
     const dim3 grid(ceil_div(nx, TI), ceil_div(ny, TJ), nt * nz);
@@ -653,6 +663,46 @@ static int advect_fct_impl(const char* fn, bool mixed, const double* C, const do
     if (open_flux) fct_open_flux_kernel<<<nt, 256, 0, st>>>(a, open_flux);
     return pocean_check_launch(fn);
 }
+
+namespace po {
+
+// The FCT passes of every domain of a batch, one launch per pass (off_host: the CTA offsets also held on the device).
+template <bool ZV, bool MIX>
+static void fct_batched_impl(const BatchDomain* doms, const int* off_dev, const int* off_host, int ndom,
+                             cudaStream_t st)
+{
+    const int* so = off_dev + BP_STRIP * (ndom + 1);
+    const int* to = off_dev + BP_TILE * (ndom + 1);
+    const unsigned ns = (unsigned)off_host[BP_STRIP * (ndom + 1) + ndom];
+    const unsigned nt = (unsigned)off_host[BP_TILE * (ndom + 1) + ndom];
+    fct_strip_batched<1, ZV, MIX><<<ns, SWARPS * 32, 0, st>>>(doms, so, ndom);
+    fct_strip_batched<2, ZV, MIX><<<ns, SWARPS * 32, 0, st>>>(doms, so, ndom);
+    fct_strip_batched<3, ZV, MIX><<<ns, SWARPS * 32, 0, st>>>(doms, so, ndom);
+    fct_coeff_batched<<<nt, NTHREADS, 0, st>>>(doms, to, ndom);
+    fct_final_batched<<<nt, NTHREADS, 0, st>>>(doms, to, ndom);
+}
+
+void fct_batched_launch(const BatchDomain* doms, const int* off_dev, const int* off_host, int ndom, bool zv,
+                        bool mixed, cudaStream_t st)
+{
+    if (zv && !mixed) fct_batched_impl<true, false>(doms, off_dev, off_host, ndom, st);
+    else if (!zv && !mixed) fct_batched_impl<false, false>(doms, off_dev, off_host, ndom, st);
+    else if (zv) fct_batched_impl<true, true>(doms, off_dev, off_host, ndom, st);
+    else fct_batched_impl<false, true>(doms, off_dev, off_host, ndom, st);
+}
+
+// CTAs of each batched FCT pass for one domain (strip pairs per plane x planes; tiles x layers).
+void fct_batched_ctas(const Shape& s, int seglen, int& strip_ctas, int& tile_ctas, int& nstrips, int& nsegs)
+{
+    nstrips = ceil_div(s.nx, STRIP);
+    nsegs = ceil_div(s.ny, seglen);
+    strip_ctas = ceil_div(nstrips * nsegs, SWARPS) * s.nt * s.n;
+    tile_ctas = ceil_div(s.nx, TI) * ceil_div(s.ny, TJ) * s.n;
+}
+
+}  // namespace po
+
+using namespace po;
 
 extern "C" int pocean_advect_fct_f64(const double* C, const double* V0, const double* V1, const double* Qx,
                                      const double* Qy, const uint8_t* ok, const double* inflow, int nt, int nz,

@@ -15,7 +15,7 @@
 namespace po {
 
 constexpr int STRIP = 31;            // cells per warp along i
-constexpr int SEG = 64;              // rows per warp segment
+constexpr int SEG = 64;              // default rows per warp segment (a launch parameter)
 constexpr int SWARPS = 4;            // warps per CTA (independent)
 constexpr int RXW = 40;              // ring row pitch (37 used: columns i0-3 .. i0+33)
 constexpr int RING = 8;              // ring rows (rows j-3 .. j+3 plus the one being refilled)
@@ -32,20 +32,18 @@ __device__ __forceinline__ int row_of(int r, const Shape& s, const Flags& fl)
     return (r >= 0 && r < s.ny) ? r : -1;
 }
 
+// One warp's work: (segment, strip) pair `pair` of plane p (k-major) of the domain described by `a`.
 template <int STAGE, bool ZV, bool MIX>
-__global__ void __launch_bounds__(SWARPS * 32, STAGE == 3 ? 8 : 5) fct_strip_kernel(StepArgs a, int nstrips, int nsegs)
+__device__ __forceinline__ void strip_body(const StepArgs& a, StripSmem& SM, int seglen, int nstrips, int pair, int p)
 {
-    __shared__ StripSmem SM;
     const Shape s = a.s;
     const Flags fl(a.flags);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int pair = blockIdx.x * SWARPS + warp;               // (segment, strip) pairs, strip fastest
-    if (pair >= nstrips * nsegs) return;                       // whole warp leaves together
     const int seg = pair / nstrips, strip = pair - seg * nstrips;
     const int i0 = strip * STRIP;
-    const int jA = seg * SEG;
-    const int jB = min(jA + SEG, s.ny);                        // cells jA..jB-1; y-faces jA..jB
-    const int p = blockIdx.y, k = p / s.nt, t = p - k * s.nt;   // k-major: the tracers of a layer in a row
+    const int jA = seg * seglen;
+    const int jB = min(jA + seglen, s.ny);                     // cells jA..jB-1; y-faces jA..jB
+    const int k = p / s.nt, t = p - k * s.nt;                  // k-major: the tracers of a layer in a row
 
     const i64 pc = s.cell(t, k, 0, 0);
     const i64 pg = s.geo(k, 0, 0);
@@ -263,6 +261,36 @@ __global__ void __launch_bounds__(SWARPS * 32, STAGE == 3 ? 8 : 5) fct_strip_ker
         f0x_prev = f0x;
         f0y_prev = f0y;
     }
+}
+
+// Single-domain launch: blockIdx.x covers the (segment, strip) pairs SWARPS at a time, blockIdx.y the planes.
+template <int STAGE, bool ZV, bool MIX>
+__global__ void __launch_bounds__(SWARPS * 32, STAGE == 3 ? 8 : 5)
+    fct_strip_kernel(StepArgs a, int seglen, int nstrips, int nsegs)
+{
+    __shared__ StripSmem SM;
+    const int pair = blockIdx.x * SWARPS + (threadIdx.x >> 5);
+    if (pair >= nstrips * nsegs) return;                       // whole warp leaves together
+    strip_body<STAGE, ZV, MIX>(a, SM, seglen, nstrips, pair, blockIdx.y);
+}
+
+// Batched launch over many domains: domain d owns CTAs off[d] .. off[d+1]-1, each a block of SWARPS pairs of one
+// of its planes.
+template <int STAGE, bool ZV, bool MIX>
+__global__ void __launch_bounds__(SWARPS * 32, STAGE == 3 ? 8 : 5)
+    fct_strip_batched(const BatchDomain* __restrict__ doms, const int* __restrict__ off, int ndom)
+{
+    __shared__ StripSmem SM;
+    const int d = find_domain(off, ndom, blockIdx.x);
+    const BatchDomain& D = doms[d];
+    const int local = blockIdx.x - __ldg(off + d);
+    const int npairs = D.nstrips * D.nsegs;
+    const int per_plane = (npairs + SWARPS - 1) / SWARPS;
+    const int p = local / per_plane;
+    const int pair = (local - p * per_plane) * SWARPS + (threadIdx.x >> 5);
+    if (pair >= npairs) return;
+    const StepArgs a = D.a;
+    strip_body<STAGE, ZV, MIX>(a, SM, D.seglen, D.nstrips, pair, p);
 }
 
 }  // namespace po

@@ -15,6 +15,7 @@
 #include <cmath>
 
 #include "common.cuh"
+#include "fct_args.cuh"
 #include "remap_core.cuh"
 
 namespace po {
@@ -37,16 +38,13 @@ struct ColumnIO {
     __device__ __forceinline__ void put(int m, int k, double v) { o[m][k * plane] = v; }
 };
 
+// One column c of NF fields m0 .. m0+NF-1: f_src (nfields, n0, plane) -> out (nfields, n1, plane).
 template <int NF>
-__global__ void __launch_bounds__(128) remap_stream_kernel(const double* __restrict__ h_src,
-                                                           const double* __restrict__ f_src,
-                                                           const double* __restrict__ h_tgt,
-                                                           const uint8_t* __restrict__ wet, int n0, int n1, i64 plane,
-                                                           int field0, int scheme, double* __restrict__ out)
+__device__ __forceinline__ void remap_stream_body(const double* __restrict__ h_src, const double* __restrict__ f_src,
+                                                  const double* __restrict__ h_tgt, const uint8_t* __restrict__ wet,
+                                                  int n0, int n1, i64 plane, int m0, int scheme,
+                                                  double* __restrict__ out, i64 c)
 {
-    const i64 c = (i64)blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= plane) return;
-    const int m0 = field0 + (int)blockIdx.y * NF;
     ColumnIO<NF> io;
     io.h = h_src + c;
     io.t = h_tgt + c;
@@ -77,14 +75,10 @@ __global__ void __launch_bounds__(128) remap_stream_kernel(const double* __restr
 }
 
 template <int NMAX>
-__global__ void __launch_bounds__(128) remap_general_kernel(const double* __restrict__ h_src,
-                                                            const double* __restrict__ f_src,
-                                                            const double* __restrict__ h_tgt, int n0, int n1,
-                                                            i64 plane, int scheme, double* __restrict__ out)
+__device__ __forceinline__ void remap_general_body(const double* __restrict__ h_src, const double* __restrict__ f_src,
+                                                   const double* __restrict__ h_tgt, int n0, int n1, i64 plane,
+                                                   int m, int scheme, double* __restrict__ out, i64 c)
 {
-    const i64 c = (i64)blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= plane) return;
-    const int m = blockIdx.y;
     double* o = out + (i64)m * n1 * plane + c;
     if (__double_as_longlong(o[0]) != kRedo) return;
     ColumnIO<1> io;
@@ -96,7 +90,83 @@ __global__ void __launch_bounds__(128) remap_general_kernel(const double* __rest
     rc::remap_column_general<NMAX>(io, 0, n0, n1, scheme);
 }
 
+template <int NF>
+__global__ void __launch_bounds__(128) remap_stream_kernel(const double* __restrict__ h_src,
+                                                           const double* __restrict__ f_src,
+                                                           const double* __restrict__ h_tgt,
+                                                           const uint8_t* __restrict__ wet, int n0, int n1, i64 plane,
+                                                           int field0, int scheme, double* __restrict__ out)
+{
+    const i64 c = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= plane) return;
+    remap_stream_body<NF>(h_src, f_src, h_tgt, wet, n0, n1, plane, field0 + (int)blockIdx.y * NF, scheme, out, c);
+}
+
+template <int NMAX>
+__global__ void __launch_bounds__(128) remap_general_kernel(const double* __restrict__ h_src,
+                                                            const double* __restrict__ f_src,
+                                                            const double* __restrict__ h_tgt, int n0, int n1,
+                                                            i64 plane, int scheme, double* __restrict__ out)
+{
+    const i64 c = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= plane) return;
+    remap_general_body<NMAX>(h_src, f_src, h_tgt, n0, n1, plane, blockIdx.y, scheme, out, c);
+}
+
+// Batched remap of every domain's advected stack (D.a.out -> D.rout).  Mode: NF = 2 over field pairs (group g =
+// fields 2g, 2g+1), or NF = 1 over single fields starting at `first` (the odd field left by the pairs, or all).
+template <int NF>
+__global__ void __launch_bounds__(128) remap_stream_batched(const BatchDomain* __restrict__ doms,
+                                                            const int* __restrict__ off, int ndom, int odd_only)
+{
+    const int d = find_domain(off, ndom, blockIdx.x);
+    const BatchDomain& D = doms[d];
+    const Shape s = D.a.s;
+    const i64 plane = (i64)s.ny * s.nx;
+    const int cblocks = (int)((plane + 127) / 128);
+    const int local = blockIdx.x - __ldg(off + d);
+    const int g = local / cblocks;
+    const i64 c = (i64)(local - g * cblocks) * 128 + threadIdx.x;
+    if (c >= plane) return;
+    const int m0 = NF == 2 ? 2 * g : (odd_only ? s.nt - 1 : g);
+    remap_stream_body<NF>(D.h_src, D.a.out, D.h_tgt, D.wet, s.n, s.n, plane, m0, D.remap_scheme, D.rout, c);
+}
+
+template <int NMAX>
+__global__ void __launch_bounds__(128) remap_general_batched(const BatchDomain* __restrict__ doms,
+                                                             const int* __restrict__ off, int ndom)
+{
+    const int d = find_domain(off, ndom, blockIdx.x);
+    const BatchDomain& D = doms[d];
+    const Shape s = D.a.s;
+    const i64 plane = (i64)s.ny * s.nx;
+    const int cblocks = (int)((plane + 127) / 128);
+    const int local = blockIdx.x - __ldg(off + d);
+    const int m = local / cblocks;
+    const i64 c = (i64)(local - m * cblocks) * 128 + threadIdx.x;
+    if (c >= plane) return;
+    remap_general_body<NMAX>(D.h_src, D.a.out, D.h_tgt, s.n, s.n, plane, m, D.remap_scheme, D.rout, c);
+}
+
 }  // namespace remap
+
+// nf_mode 2: field pairs (+ the odd field); nf_mode 1: every field on its own.  nmax: the batch's deepest column.
+void remap_batched_launch(const BatchDomain* doms, const int* off_dev, const int* off_host, int ndom, int nf_mode,
+                          int nmax, cudaStream_t st)
+{
+    auto total = [&](int pass) { return (unsigned)off_host[pass * (ndom + 1) + ndom]; };
+    auto offs = [&](int pass) { return off_dev + pass * (ndom + 1); };
+    if (nf_mode == 2) {
+        if (total(BP_RPAIR)) remap::remap_stream_batched<2><<<total(BP_RPAIR), 128, 0, st>>>(doms, offs(BP_RPAIR), ndom, 0);
+        if (total(BP_RREM)) remap::remap_stream_batched<1><<<total(BP_RREM), 128, 0, st>>>(doms, offs(BP_RREM), ndom, 1);
+    } else {
+        remap::remap_stream_batched<1><<<total(BP_RALL), 128, 0, st>>>(doms, offs(BP_RALL), ndom, 0);
+    }
+    if (nmax <= 64) remap::remap_general_batched<64><<<total(BP_RGEN), 128, 0, st>>>(doms, offs(BP_RGEN), ndom);
+    else if (nmax <= 128) remap::remap_general_batched<128><<<total(BP_RGEN), 128, 0, st>>>(doms, offs(BP_RGEN), ndom);
+    else remap::remap_general_batched<256><<<total(BP_RGEN), 128, 0, st>>>(doms, offs(BP_RGEN), ndom);
+}
+
 }  // namespace po
 
 using namespace po;

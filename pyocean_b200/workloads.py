@@ -85,25 +85,27 @@ def _smooth_noise(rng, shape, scale: float) -> np.ndarray:
     return out / np.abs(out).max()
 
 
-def zstar_box(seed: int = 0, nx: int = 64, ny: int = 64, n: int = 20) -> Workload:
+def zstar_box(seed: int = 0, nx: int = 64, ny: int = 64, n: int = 20, nt: int = 1) -> Workload:
+    """The z* box; ``nt`` tracers, each 10 / 20 degC halves in x plus its own N(0, 0.01) noise."""
     rng = np.random.default_rng(seed)
     dx = dy = 1000.0
     h0 = 5.0
     h = np.full((n, ny, nx), h0)
     area = dx * dy
-    # k^-3 streamfunction on corners: walls at j = 0 and j = ny (psi = 0), periodic in x
-    jc = np.arange(ny + 1)[:, None] / ny
-    ic = np.arange(nx + 1)[None, :] / nx
-    psi = np.zeros((ny + 1, nx + 1))
-    for m in range(1, 9):
-        for kk in range(-8, 9):
-            k = np.hypot(m / 2.0, kk)
-            if k == 0:
-                continue
-            psi += k ** -3 * np.sin(np.pi * m * jc) * np.cos(2 * np.pi * kk * ic + rng.uniform(0, 2 * np.pi))
+    # k^-3 streamfunction on corners: walls at j = 0 and j = ny (psi = 0), periodic in x.  Mode (m, kk) is
+    # k^-3 sin(pi m y) cos(2 pi kk x + phase), k = hypot(m / 2, kk); summed as an outer product over m.
+    m = np.arange(1, 9)[:, None]
+    kk = np.arange(-8, 9)[None, :]
+    phase = rng.uniform(0, 2 * np.pi, (8, 17))
+    amp = np.hypot(m / 2.0, kk) ** -3
+    ic = np.arange(nx + 1) / nx
+    jc = np.arange(ny + 1) / ny
+    gx = np.einsum("mk,mki->mi", amp, np.cos(2 * np.pi * kk[..., None] * ic[None, None] + phase[..., None]))
+    psi = np.sin(np.pi * m * jc[None]).T @ gx
     psi[:, -1] = psi[:, 0]
     water = np.ones((ny, nx), bool)
-    Qx, Qy = _streamfunction_transports(psi, h, water, periodic_x=True)
+    # uniform layers: every layer carries the same transport, computed once and repeated
+    Qx, Qy = _streamfunction_transports(psi, h[:1], water, periodic_x=True)
     umax = max(np.abs(Qx).max() / (dy * h0), np.abs(Qy).max() / (dx * h0))
     scale = 0.5 / umax
     Qx *= scale
@@ -114,11 +116,38 @@ def zstar_box(seed: int = 0, nx: int = 64, ny: int = 64, n: int = 20) -> Workloa
     div = Qx[..., 1:] - Qx[..., :-1] + Qy[:, 1:] - Qy[:, :-1]
     V1 = V0 - dt * div
     ok = V1 > 0
-    T = np.where(np.arange(nx)[None, None, :] < nx // 2, 10.0, 20.0) + rng.normal(0, 0.01, (n, ny, nx))
+    Qx, Qy = np.repeat(Qx, n, axis=0), np.repeat(Qy, n, axis=0)
+    halves = np.where(np.arange(nx)[None, None, :] < nx // 2, 10.0, 20.0)
+    C = np.stack([halves + rng.normal(0, 0.01, (n, ny, nx)) for _ in range(nt)])
     h_src = h * (1 + rng.uniform(-0.2, 0.2, h.shape))
     h_src *= h.sum(0) / h_src.sum(0)
-    return Workload("zstar_box_64x64x20", T[None].copy(), V0, V1, Qx, Qy, ok, water, h.copy(), h_src, dt,
-                    periodic=("x",), meta=dict(dx=dx, dy=dy, cfl=0.4, umax=0.5))
+    return Workload(f"zstar_box_{nx}x{ny}x{n}" + (f"_nt{nt}" if nt != 1 else ""), C, V0, V1, Qx, Qy, ok, water,
+                    h.copy(), h_src, dt, periodic=("x",), meta=dict(dx=dx, dy=dy, cfl=0.4, umax=0.5))
+
+
+def uneven_domain_sizes(seed: int = 0, ndom: int = 64, lo: int = 96, hi: int = 384, nzs=(30, 50, 75),
+                        nt: int = 1) -> list:
+    """(seed, nx, ny, nz, nt) of ``ndom`` independent z* boxes: nx, ny log-uniform in [lo, hi], nz drawn from
+    ``nzs``, domain d seeded with seed * 1000 + d (the batched uneven-domains configuration: 64 domains, 96..384,
+    nz in {30, 50, 75})."""
+    rng = np.random.default_rng(seed)
+    sizes = np.exp(rng.uniform(np.log(lo), np.log(hi), (ndom, 2))).round().astype(int)
+    nz = rng.choice(np.asarray(nzs), ndom)
+    return [(seed * 1000 + d, int(sizes[d, 0]), int(sizes[d, 1]), int(nz[d]), nt) for d in range(ndom)]
+
+
+def uneven_domains(seed: int = 0, ndom: int = 64, lo: int = 96, hi: int = 384, nzs=(30, 50, 75), nt: int = 1,
+                   threads: int = 8):
+    """Iterator over the ``ndom`` z* boxes of ``uneven_domain_sizes`` (generated ``threads`` at a time), so
+    that a caller moving each to the GPU holds only a few on the host at once."""
+    from concurrent.futures import ThreadPoolExecutor
+    specs = uneven_domain_sizes(seed, ndom, lo, hi, nzs, nt)
+    with ThreadPoolExecutor(max(1, threads)) as ex:
+        for i in range(0, len(specs), max(1, threads)):
+            futs = [ex.submit(lambda a: zstar_box(seed=a[0], nx=a[1], ny=a[2], n=a[3], nt=a[4]), sp)
+                    for sp in specs[i:i + max(1, threads)]]
+            for f in futs:
+                yield f.result()
 
 
 def hybrid_target(H: np.ndarray, n: int) -> np.ndarray:

@@ -71,3 +71,35 @@ def test_package_has_no_cpu_fallback(monkeypatch):
     monkeypatch.setattr(_lib, "LIB_PATH", os.path.join(ROOT, "does-not-exist.so"))
     with pytest.raises(RuntimeError, match="no CPU fallback"):
         _lib.lib()
+
+
+def test_batch_domain_struct_layout_matches_ctypes(tmp_path):
+    # the ctypes mirror of pocean_domain must agree with the C compiler's layout field by field
+    import subprocess
+    from pyocean_b200.batch import _Domain
+    names = [f[0] for f in _Domain._fields_]
+    src = tmp_path / "layout.c"
+    body = "".join(f'    printf("%s %zu\\n", "{n}", offsetof(pocean_domain, {n}));\n' for n in names)
+    src.write_text('#include <stdio.h>\n#include <stddef.h>\n#include "pocean_b200.h"\nint main(void) {\n'
+                   f'    printf("sizeof %zu\\n", sizeof(pocean_domain));\n{body}    return 0;\n}}\n')
+    exe = tmp_path / "layout"
+    subprocess.check_call(["gcc", "-std=c99", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)])
+    got = dict(line.split() for line in subprocess.check_output([str(exe)], text=True).splitlines())
+    assert int(got["sizeof"]) == ctypes.sizeof(_Domain)
+    for n in names:
+        assert int(got[n]) == getattr(_Domain, n).offset, n
+
+
+def test_batch_argument_errors():
+    L = _lib.lib()
+    assert L.pocean_batch_device_bytes(0) == 0
+    assert L.pocean_batch_device_bytes(64) > L.pocean_batch_device_bytes(1) > 0
+    h = ctypes.c_void_p()
+    assert L.pocean_batch_create(8, 1, 64, 256, 1 << 20, None) == 1            # no output handle
+    assert L.pocean_batch_create(None, 1, 64, 256, 1 << 20, ctypes.byref(h)) == 1
+    assert L.pocean_batch_create(8, 0, 64, 256, 1 << 20, ctypes.byref(h)) == 1
+    assert L.pocean_batch_create(8, 1, 2, 256, 1 << 20, ctypes.byref(h)) == 1   # segment length
+    assert L.pocean_batch_create(8, 1, 64, 256, 16, ctypes.byref(h)) == 2      # plan buffer too small
+    assert L.pocean_batch_create(8, 1, 64, 264, 1 << 20, ctypes.byref(h)) == 2  # misaligned
+    assert h.value is None
+    assert L.pocean_batch_step(None, 0, 2, 0, None) == 1
