@@ -43,12 +43,26 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="budget of the CPU-baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--batched-steps", type=int, default=50,
+                    help="steps of the 64-uneven-domains batch report (0: skip)")
+    ap.add_argument("--serve-jobs", type=int, default=200, help="jobs of the served-stream report (0: skip)")
+    ap.add_argument("--serve-rate", type=float, default=15.0, help="Poisson arrival rate of the served stream [1/s]")
     return ap.parse_args()
 
 
 def make_workload(name: str):
     from pyocean_b200 import workloads as W
     return W.basin() if name == "basin" else W.zstar_box()
+
+
+# From one ncu capture of a step of this workload (all seven kernels; the profile summary
+# profiles/fct_and_remap_kernels_basin_512x512x50.md gives the command): DRAM bytes read + written per call, and
+# FP64 thread instructions (DFMA + DMUL + DADD) per call.
+NCU_PER_CALL = {
+    "basin_512x512x50_nt2": {"advect_fct": {"dram_bytes": 8232481032, "fp64_inst": 18667451893},
+                             "remap_columns": {"dram_bytes": 713337152, "fp64_inst": 2839950659}},
+}
+FP64_LANES_PER_SM, SMS = 64, 148
 
 
 def peaks() -> dict:
@@ -272,6 +286,16 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> dict | None:
     rem_gbs = ab["remap"] / (rem_avg / 1e3) / 1e9
     dominant = ("advect_fct", adv_gbs, adv_avg, ab["advect"]) if adv_avg >= rem_avg else \
         ("remap_columns", rem_gbs, rem_avg, ab["remap"])
+    ncu = NCU_PER_CALL.get(w.name, {})
+    sm_hz = (clk.get("sm_mhz") or 1965.0) * 1e6
+    fp64_rate = FP64_LANES_PER_SM * SMS * sm_hz                  # FP64 thread instructions per second at this clock
+
+    def fp64_part(name, ms):
+        if name not in ncu:
+            return None
+        t_min = ncu[name]["fp64_inst"] / fp64_rate
+        return {"fp64_inst_per_call": ncu[name]["fp64_inst"], "issue_bound_ms": 1e3 * t_min,
+                "frac": t_min / (ms / 1e3)}
     line = {
         "metric": "tracer cell-steps/s at 512^2x50 (advect_fct + PPM_H4 remap, FP64)",
         "value": value,
@@ -290,8 +314,13 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> dict | None:
                    "geometry array); no flush", "parallelism": f"replicas x{world}"},
         "roofline": {"bound": "hbm", "kernel": dominant[0], "achieved": dominant[1], "peak": pk["hbm_gbs"],
                      "unit": "GB/s", "frac": dominant[1] / pk["hbm_gbs"], "peak_source": pk["source"],
-                     "traffic": None, "algorithmic_bytes_per_launch": dominant[3],
+                     "traffic": ncu.get(dominant[0], {}).get("dram_bytes"),
+                     "traffic_note": "ncu dram__bytes_read.sum + dram__bytes_write.sum summed over the call's kernels",
+                     "algorithmic_bytes_per_launch": dominant[3],
                      "avg_launch_ms": dominant[2],
+                     "fp64_issue_bound": {"advect_fct": fp64_part("advect_fct", adv_avg),
+                                          "remap_columns": fp64_part("remap_columns", rem_avg),
+                                          "peak": "64 FP64 lanes x 148 SMs x median SM clock under load"},
                      "parts": {"advect_fct": {"ms": adv_avg, "GB/s": adv_gbs, "bytes": ab["advect"]},
                                "remap_columns": {"ms": rem_avg, "GB/s": rem_gbs, "bytes": ab["remap"]},
                                "step": {"ms": ms / args.steps,
@@ -337,6 +366,16 @@ def main():
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
                                              device_id=torch.device("cuda", local_rank))
     line = run_ours(args, rank, world, local_rank)
+    import torch
+    torch.cuda.empty_cache()
+    if args.batched_steps > 0:
+        from pyocean_b200.batch_report import batched_report
+        line["batched"] = batched_report(steps=args.batched_steps)
+        torch.cuda.empty_cache()
+    if args.serve_jobs > 0:
+        from pyocean_b200.serve import serve_report
+        line["served"] = serve_report(n_jobs=args.serve_jobs, rate=args.serve_rate)
+        torch.cuda.empty_cache()
     if rank == 0:
         if not args.no_cpu_baseline and world == 1:
             s = cpu_sample(make_workload(args.workload), args.cpu_seconds)

@@ -85,27 +85,37 @@ class Domain:
                    workspace=torch.empty(nbytes, dtype=torch.uint8, device=dev), flags=int(flags), dt=float(dt),
                    remap_scheme=int(remap_scheme), inflow=None if inflow is None else inflow.contiguous())
 
-    def as_struct(self) -> _Domain:
+    def as_struct(self, swapped: bool = False) -> _Domain:
+        """The C descriptor; ``swapped``: the current state is in C_next (parity 0 of the plan reads C_next)."""
         nt, n, ny, nx = self.shape
         p = lambda t: None if t is None else t.data_ptr()                              # noqa: E731
-        return _Domain(p(self.C), p(self.V0), p(self.V1), p(self.Qx), p(self.Qy), p(self.ok), p(self.inflow),
+        cur, nxt = (self.C_next, self.C) if swapped else (self.C, self.C_next)
+        return _Domain(p(cur), p(self.V0), p(self.V1), p(self.Qx), p(self.Qy), p(self.ok), p(self.inflow),
                        nt, n, ny, nx, self.flags, self.dt, p(self.C_adv), p(self.workspace), self.workspace.numel(),
-                       p(self.h_src), p(self.h_tgt), p(self.wet), self.remap_scheme, p(self.C_next))
+                       p(self.h_src), p(self.h_tgt), p(self.wet), self.remap_scheme, p(nxt))
 
 
 class _Plan:
-    """A ``pocean_batch`` plan and the device buffer holding its descriptors."""
+    """A ``pocean_batch`` plan and the device buffer holding its descriptors (``buf``: reuse a buffer of an earlier
+    plan — the new descriptors are written in stream order, after the steps already enqueued)."""
 
-    def __init__(self, structs, seglen: int, device) -> None:
+    def __init__(self, structs, seglen: int, device, buf: torch.Tensor | None = None, stream: int | None = None) -> None:
         L = _lib.lib()
         n = len(structs)
-        self.buf = torch.empty(L.pocean_batch_device_bytes(n), dtype=torch.uint8, device=device)
+        need = L.pocean_batch_device_bytes(n)
+        if buf is None or buf.numel() < need:
+            buf = torch.empty(need, dtype=torch.uint8, device=device)
+        self.buf = buf
         arr = (_Domain * n)(*structs)
         h = ctypes.c_void_p()
+        st = torch.cuda.current_stream(device).cuda_stream if stream is None else stream
         _lib.check(L.pocean_batch_create(ctypes.cast(arr, ctypes.c_void_p), n, seglen, self.buf.data_ptr(),
-                                         self.buf.numel(), ctypes.byref(h)), "batch_create")
+                                         self.buf.numel(), ctypes.byref(h), st), "batch_create")
         self.handle = h
         self.seglen = seglen
+
+    def step(self, parity: int, remap_nf: int, mixed: bool, stream: int) -> None:
+        _lib.check(_lib.lib().pocean_batch_step(self.handle, parity, remap_nf, int(mixed), stream), "batch_step")
 
     def __del__(self) -> None:
         h = getattr(self, "handle", None)
@@ -160,10 +170,8 @@ class DomainBatch:
         return d.C if self.parity == 0 else d.C_next
 
     def step(self, steps: int = 1) -> None:
-        L = _lib.lib()
         for _ in range(steps):
-            _lib.check(L.pocean_batch_step(self.plan.handle, self.parity, self.remap_nf, int(self.mixed),
-                                           self.stream()), "batch_step")
+            self.plan.step(self.parity, self.remap_nf, self.mixed, self.stream())
             self.parity ^= 1
 
     def capture(self, steps: int) -> torch.cuda.CUDAGraph:
