@@ -163,10 +163,13 @@ typedef struct pocean_batch pocean_batch;   /* host-side plan of a batch */
 /* Device bytes of the batch plan for ndom domains (descriptors of both parities and the CTA-offset tables). */
 size_t pocean_batch_device_bytes(int ndom);
 
-/* Validates the domains and writes the plan into device_buf (synchronous copy; call outside stream capture).
- * seglen: rows per warp segment of the WENO passes (a tuning parameter; results do not depend on it). */
+/* Validates the domains and writes the plan into device_buf with copies ordered on `stream` (after the steps
+ * already enqueued there, which may still be reading an earlier plan in the same buffer); `domains` may be released
+ * on return.  Not capturable: call outside stream capture.  seglen: rows per warp segment of the WENO passes (a
+ * tuning parameter; results do not depend on it).  A plan only refers to the domains' buffers; steps enqueued with
+ * it must be ordered after the plan's copies (same stream, or an event). */
 int pocean_batch_create(const pocean_domain* domains, int ndom, int seglen, void* device_buf, size_t device_bytes,
-                        pocean_batch** out);
+                        pocean_batch** out, void* stream);
 
 /* Enqueues one step of every domain.  remap_nf: fields per remap thread (1 or 2, a tuning parameter); mixed: FP32
  * WENO weights (pocean_advect_fct_mixed) instead of FP64. */

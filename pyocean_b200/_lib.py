@@ -36,7 +36,7 @@ SIGNATURES: dict[str, tuple] = {
                                    _P]),
     "pocean_remap_columns_f64": (_I, [_P, _P, _P, _P, _I, _I, _I, _I, _I, _I, _P, _P]),
     "pocean_batch_device_bytes": (_Z, [_I]),
-    "pocean_batch_create": (_I, [_P, _I, _I, _P, _Z, ctypes.POINTER(_P)]),
+    "pocean_batch_create": (_I, [_P, _I, _I, _P, _Z, ctypes.POINTER(_P), _P]),
     "pocean_batch_step": (_I, [_P, _I, _I, _I, _P]),
     "pocean_batch_destroy": (None, [_P]),
 }

@@ -29,7 +29,7 @@ extern "C" size_t pocean_batch_device_bytes(int ndom)
 }
 
 extern "C" int pocean_batch_create(const pocean_domain* domains, int ndom, int seglen, void* device_buf,
-                                   size_t device_bytes, pocean_batch** out)
+                                   size_t device_bytes, pocean_batch** out, void* stream)
 {
     const char* fn = "pocean_batch_create";
     if (!out) return pocean_fail(POCEAN_EINVAL, "%s: null output handle", fn);
@@ -101,9 +101,13 @@ extern "C" int pocean_batch_create(const pocean_domain* domains, int ndom, int s
     b->dev_doms = (BatchDomain*)device_buf;
     b->dev_off = (int*)((char*)device_buf + (((size_t)2 * ndom * sizeof(BatchDomain) + 255) & ~(size_t)255));
     b->host_off = off;
-    cudaError_t e = cudaMemcpy(b->dev_doms, host.data(), host.size() * sizeof(BatchDomain), cudaMemcpyHostToDevice);
+    // Pageable sources: each copy is staged before the call returns, so the host vectors may go; on the device
+    // the copies are ordered after the work already on `stream` (which may still read an older plan here).
+    cudaStream_t st = (cudaStream_t)stream;
+    cudaError_t e = cudaMemcpyAsync(b->dev_doms, host.data(), host.size() * sizeof(BatchDomain),
+                                    cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess)
-        e = cudaMemcpy(b->dev_off, off.data(), off.size() * sizeof(int), cudaMemcpyHostToDevice);
+        e = cudaMemcpyAsync(b->dev_off, off.data(), off.size() * sizeof(int), cudaMemcpyHostToDevice, st);
     if (e != cudaSuccess) {
         delete b;
         return pocean_fail(POCEAN_ECUDA, "%s: %s", fn, cudaGetErrorString(e));

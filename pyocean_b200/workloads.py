@@ -251,3 +251,47 @@ def algorithmic_bytes(w: Workload) -> dict:
     adv = cells * (16 * nt + 8 + 8 + 1) + 8 * n * ny * (nx + 1) + 8 * n * (ny + 1) * nx
     rem = cells * (16 + 16 * nt) + ny * nx
     return dict(advect=adv, remap=rem, step=adv + rem)
+
+
+def zstar_box_device(seed: int, nx: int, ny: int, n: int, nt: int, device) -> dict:
+    """The z* box of ``zstar_box`` generated on the GPU with torch's CUDA generator (same construction, another
+    random stream): the inputs of a served job, built where they are used.  Returns device tensors C, V0, V1, Qx,
+    Qy, ok (uint8), h_src, h_tgt, wet (uint8) and the scalars dt, flags (periodic in x), remap_scheme."""
+    import torch
+    f64 = dict(dtype=torch.float64, device=device)
+    gen = torch.Generator(device=device)
+    gen.manual_seed(int(seed))
+    dx = dy = 1000.0
+    h0 = 5.0
+    m = torch.arange(1, 9, **f64)[:, None]
+    kk = torch.arange(-8, 9, **f64)[None, :]
+    phase = torch.rand((8, 17), generator=gen, **f64) * (2 * np.pi)
+    amp = torch.hypot(m / 2.0, kk) ** -3
+    ic = torch.arange(nx + 1, **f64) / nx
+    jc = torch.arange(ny + 1, **f64) / ny
+    gx = torch.einsum("mk,mki->mi", amp, torch.cos(2 * np.pi * kk[..., None] * ic[None, None] + phase[..., None]))
+    psi = torch.sin(np.pi * m * jc[None]).T @ gx
+    psi[:, -1] = psi[:, 0]
+    # all water, walls at j = 0 and j = ny: corners on the walls carry no transport; uniform h0 layers
+    Psi = psi * h0
+    Psi[0] = 0.0
+    Psi[-1] = 0.0
+    Qx = -(Psi[1:] - Psi[:-1])                         # (ny, nx+1)
+    Qy = Psi[:, 1:] - Psi[:, :-1]                      # (ny+1, nx)
+    umax = max(float(Qx.abs().max()) / (dy * h0), float(Qy.abs().max()) / (dx * h0))
+    Qx *= 0.5 / umax
+    Qy *= 0.5 / umax
+    Qx[:, -1] = Qx[:, 0]
+    dt = 0.4 * dx / 0.5
+    V0 = torch.full((n, ny, nx), dx * dy * h0, **f64)
+    div = Qx[:, 1:] - Qx[:, :-1] + Qy[1:] - Qy[:-1]
+    V1 = V0 - dt * div[None]
+    ok = (V1 > 0).to(torch.uint8)
+    halves = torch.where(torch.arange(nx, device=device) < nx // 2, 10.0, 20.0).to(torch.float64)
+    C = halves + 0.01 * torch.randn((nt, n, ny, nx), generator=gen, **f64)
+    h = torch.full((n, ny, nx), h0, **f64)
+    h_src = h * (1 + 0.4 * (torch.rand((n, ny, nx), generator=gen, **f64) - 0.5))
+    h_src *= h.sum(0) / h_src.sum(0)
+    return dict(C=C, V0=V0, V1=V1, Qx=Qx[None].expand(n, -1, -1).contiguous(),
+                Qy=Qy[None].expand(n, -1, -1).contiguous(), ok=ok, h_src=h_src, h_tgt=h,
+                wet=torch.ones((ny, nx), dtype=torch.uint8, device=device), dt=dt, flags=0x10, remap_scheme=2)
