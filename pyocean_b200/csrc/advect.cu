@@ -36,6 +36,23 @@ constexpr int TI = 32;          // tile width (i, contiguous in memory)
 constexpr int TJ = 8;           // tile height (j)
 constexpr int HALO = 3;         // WENO5 stencil radius
 constexpr int NTHREADS = TI * TJ;
+
+// Launch bounds of the coefficient and final passes; POCEAN_*_CTAS (resident CTAs per SM) sets their register
+// budget when defined, else ptxas chooses.  The final pass is fitted to 3 CTAs (24 warps) per SM: 3 % faster than
+// ptxas's choice (112 registers, 2 CTAs) and than 2 or 4 CTAs, measured at 512 x 512 x 50.
+#ifndef POCEAN_FINAL_CTAS
+#define POCEAN_FINAL_CTAS 3
+#endif
+#ifdef POCEAN_COEFF_CTAS
+#define COEFF_BOUNDS __launch_bounds__(NTHREADS, POCEAN_COEFF_CTAS)
+#else
+#define COEFF_BOUNDS __launch_bounds__(NTHREADS)
+#endif
+#ifdef POCEAN_FINAL_CTAS
+#define FINAL_BOUNDS __launch_bounds__(NTHREADS, POCEAN_FINAL_CTAS)
+#else
+#define FINAL_BOUNDS __launch_bounds__(NTHREADS)
+#endif
 constexpr int SW = TI + 2 * HALO;   // shared tile row length
 constexpr int SH = TJ + 2 * HALO;   // shared tile rows
 
@@ -355,12 +372,12 @@ __device__ __forceinline__ void final_body(const StepArgs& a, int i, int j, int 
 }
 
 // Single-domain launches of passes 4 and 5: a 32 x 8 tile of one layer per CTA.
-__global__ void __launch_bounds__(NTHREADS) fct_coeff_kernel(StepArgs a)
+__global__ void COEFF_BOUNDS fct_coeff_kernel(StepArgs a)
 {
     coeff_body(a, blockIdx.x * TI + threadIdx.x % TI, blockIdx.y * TJ + threadIdx.x / TI, blockIdx.z);
 }
 
-__global__ void __launch_bounds__(NTHREADS) fct_final_kernel(StepArgs a)
+__global__ void FINAL_BOUNDS fct_final_kernel(StepArgs a)
 {
     final_body(a, blockIdx.x * TI + threadIdx.x % TI, blockIdx.y * TJ + threadIdx.x / TI, blockIdx.z);
 }
@@ -380,7 +397,7 @@ __device__ __forceinline__ void batched_tile(const BatchDomain* __restrict__ dom
     j = by * TJ + threadIdx.x / TI;
 }
 
-__global__ void __launch_bounds__(NTHREADS) fct_coeff_batched(const BatchDomain* __restrict__ doms,
+__global__ void COEFF_BOUNDS fct_coeff_batched(const BatchDomain* __restrict__ doms,
                                                                const int* __restrict__ off, int ndom)
 {
     int d, i, j, k;
@@ -389,7 +406,7 @@ __global__ void __launch_bounds__(NTHREADS) fct_coeff_batched(const BatchDomain*
     coeff_body(a, i, j, k);
 }
 
-__global__ void __launch_bounds__(NTHREADS) fct_final_batched(const BatchDomain* __restrict__ doms,
+__global__ void FINAL_BOUNDS fct_final_batched(const BatchDomain* __restrict__ doms,
                                                                const int* __restrict__ off, int ndom)
 {
     int d, i, j, k;

@@ -20,6 +20,14 @@ constexpr int SWARPS = 4;            // warps per CTA (independent)
 constexpr int RXW = 40;              // ring row pitch (37 used: columns i0-3 .. i0+33)
 constexpr int RING = 8;              // ring rows (rows j-3 .. j+3 plus the one being refilled)
 
+// Resident CTAs per SM the register allocation is fitted to, per pass (stages 1 and 2 / stage 3).
+#ifndef POCEAN_STRIP_CTAS_12
+#define POCEAN_STRIP_CTAS_12 5
+#endif
+#ifndef POCEAN_STRIP_CTAS_3
+#define POCEAN_STRIP_CTAS_3 8
+#endif
+
 struct StripSmem {
     double row[SWARPS][RING][RXW];
     uint8_t val[SWARPS][RING][RXW];
@@ -265,7 +273,7 @@ __device__ __forceinline__ void strip_body(const StepArgs& a, StripSmem& SM, int
 
 // Single-domain launch: blockIdx.x covers the (segment, strip) pairs SWARPS at a time, blockIdx.y the planes.
 template <int STAGE, bool ZV, bool MIX>
-__global__ void __launch_bounds__(SWARPS * 32, STAGE == 3 ? 8 : 5)
+__global__ void __launch_bounds__(SWARPS * 32, STAGE == 3 ? POCEAN_STRIP_CTAS_3 : POCEAN_STRIP_CTAS_12)
     fct_strip_kernel(StepArgs a, int seglen, int nstrips, int nsegs)
 {
     __shared__ StripSmem SM;
@@ -277,7 +285,7 @@ __global__ void __launch_bounds__(SWARPS * 32, STAGE == 3 ? 8 : 5)
 // Batched launch over many domains: domain d owns CTAs off[d] .. off[d+1]-1, each a block of SWARPS pairs of one
 // of its planes.
 template <int STAGE, bool ZV, bool MIX>
-__global__ void __launch_bounds__(SWARPS * 32, STAGE == 3 ? 8 : 5)
+__global__ void __launch_bounds__(SWARPS * 32, STAGE == 3 ? POCEAN_STRIP_CTAS_3 : POCEAN_STRIP_CTAS_12)
     fct_strip_batched(const BatchDomain* __restrict__ doms, const int* __restrict__ off, int ndom)
 {
     __shared__ StripSmem SM;
