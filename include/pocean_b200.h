@@ -130,6 +130,47 @@ int pocean_remap_columns_f64(const double* h_src, const double* f_src, const dou
                              int n0, int n1, int ny, int nx, int nfields, int scheme, double* out, void* stream);
 
 /*
+ * The neighbours of the tracer step.
+ *
+ * Regrid + remap (ALECoordinate.regrid_remap, core/components/vertical_coordinate.py:69-78, with the z* and sigma
+ * rules of core/vertical/regrid.py:44-98, 309-395): per column wet = active & (H + eta > 0) & (sum_k h_src > 0)
+ * (H with NaN read as 0, numpy.nan_to_num), h_new = the rule's layer thicknesses where wet, else h_src; then the
+ * nfields stacked fields f_src (nfields, nz, ny, nx) are remapped from h_src onto h_new into out, as
+ * remap_columns(h_src, f, h_new, scheme, wet) does for each field (a regrid launch, then the remap launches of
+ * pocean_remap_columns_f64).  rule POCEAN_REGRID_ZSTAR: coord = dz_top (nz, surface first);
+ * POCEAN_REGRID_SIGMA: coord = dsigma (nz, bed first).  h_min: the rules' minimum thickness (the reference's
+ * default is 1e-3 m).  wet (ny, nx) bytes out.  nfields = 0: the regrid alone.  bad_columns (device int, may be
+ * NULL): incremented for every wet column that breaks the rule's precondition (z*: H > 0), for which the reference
+ * raises ValueError; those columns' outputs are undefined.
+ */
+#define POCEAN_REGRID_ZSTAR 0
+#define POCEAN_REGRID_SIGMA 1
+int pocean_regrid_remap_f64(int rule, const double* H, const double* eta, const double* h_src, const uint8_t* active,
+                            const double* coord, double h_min, const double* f_src, int nz, int ny, int nx,
+                            int nfields, int scheme, double* h_new, uint8_t* wet, double* out, int* bad_columns,
+                            void* stream);
+
+/* Face fractions w_k = hf_k / sum_k hf_k (1/nz where the sum is not positive) of hf (nz, ny, nx); replaces
+ * core/vertical/ale.py:883-902 (face_fractions / _fractions_kernel). */
+int pocean_face_fractions_f64(const double* hf, int nz, int ny, int nx, double* w, void* stream);
+
+/* Velocity remap in fraction space (ALECoordinate.remap_faces, vertical_coordinate.py:142-153): each face column of
+ * the nfields stacked fields vel (nfields, nz, ny, nx) goes from thicknesses w_src S to w_tgt S, S = sum_k hf_src
+ * (1 where not positive, those columns copied), w_src = face_fractions(hf_src), w_tgt = the given fractions or
+ * face_fractions(hf_tgt) when w_tgt is NULL.  The fractions are formed in the kernel. */
+int pocean_remap_faces_f64(const double* vel, const double* hf_src, const double* hf_tgt, const double* w_tgt,
+                           int nz, int ny, int nx, int nfields, int scheme, double* out, void* stream);
+
+/* ALE horizontal diffusion (sigma_baroclinic.py:533-561 `_diffuse_ale_kernel`, as TracerAdvection.diffuse_h calls
+ * it, core/components/tracers.py:421-447) of nt stacked fields T / Tw (nt, nz, ny, nx) sharing h, V (nz, ny, nx),
+ * act (ny, nx), cx = L_u / dx_u and okx (ny, nx+1), cy and oky (ny+1, nx).  flags: POCEAN_PERIODIC_X / _Y (the wrap
+ * faces read as the reference's halo-1 pad/crop reads them: face 0).  h is used as given (the reference passes
+ * where(act, nan_to_num(h), 0)). */
+int pocean_diffuse_ale_f64(const double* T, const double* Tw, const double* h, const uint8_t* act, const double* cx,
+                           const double* cy, const uint8_t* okx, const uint8_t* oky, const double* V, int nt, int nz,
+                           int ny, int nx, unsigned flags, double kh, double dt, double* out, void* stream);
+
+/*
  * Batched steps of many independent domains (no counterpart in the reference, which advances one model at a time):
  * one ALE tracer step = advect_fct of the stack C then the remap of the advected stack C_adv onto the target grid,
  * into C_next.  Every pass is one launch over all domains; pocean_batch_step only enqueues kernels, so a sequence

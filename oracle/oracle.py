@@ -14,6 +14,12 @@ kernels with the reference's call signatures:
   ``_open_inflow`` :65-78).
 * ``Periodic`` — ``core/model/periodic.py:31, 47-94`` (pad/crop with ``TRACER_HALO`` wrapped cells).
 * ``remap_column`` / ``remap_columns`` / ``reconstruct`` — ``core/vertical/remap.py:234-427``.
+* ``regrid`` / ``regrid_remap`` — the z* and sigma rules of ``core/vertical/regrid.py:44-98, 309-395`` as
+  ``ALECoordinate.regrid_remap`` uses them (``core/components/vertical_coordinate.py:69-111``).
+* ``diffuse_ale`` — ``_diffuse_ale_kernel`` (``core/dynamics/sigma_baroclinic.py:533-561``) with the pad/crop of
+  ``TracerAdvection.diffuse_h`` (``core/components/tracers.py:421-447``).
+* ``face_fractions`` / ``remap_faces`` — ``core/vertical/ale.py:883-902`` and
+  ``ALECoordinate.remap_faces`` (``vertical_coordinate.py:142-153``).
 
 Parity of this restatement with the reference is pinned by ``tests/test_oracle_golden.py`` against the vectors in
 ``tests/golden/`` that ``tests/golden/make_golden.py`` generated by running the reference itself.
@@ -56,6 +62,10 @@ def lib() -> ctypes.CDLL:
         L.oracle_remap_column.argtypes = [_D, _D, i, _D, i, i, _D, _D]
         L.oracle_reconstruct.argtypes = [_D, _D, i, i, _D]
         L.oracle_remap_columns.argtypes = [_D, _D, _D, i, i, i, i, i, _U8, _D]
+        L.oracle_regrid.argtypes = [i, _D, _D, _D, _U8, _D, d, i, i, i, _D, _U8]
+        L.oracle_regrid.restype = i
+        L.oracle_diffuse_ale.argtypes = [_D, _D, _D, _U8, _D, _D, _U8, _U8, _D, d, d, i, i, i, _D]
+        L.oracle_face_fractions.argtypes = [_D, i, i, i, _D]
         L.oracle_num_threads.restype = i
         L.oracle_set_threads.argtypes = [i]
         _LIB = L
@@ -373,3 +383,72 @@ def remap_columns(h_src, f_src, h_tgt, scheme, wet):
     w = _u8(np.broadcast_to(wet, (ny, nx)))
     lib().oracle_remap_columns(_p(h_src), _p(f_src), _p(h_tgt), n0, n1, ny, nx, int(scheme), _pu8(w), _p(out))
     return out
+
+
+# ---------------------------------------------------------------------------------------------------- neighbours
+H_MIN = 1e-3                           # core/vertical/regrid.py:41
+RULES = {"zstar": 0, "sigma": 1}
+
+
+def regrid(rule: str, H, eta, h_src, active, coord, h_min: float = H_MIN):
+    """z* / sigma target thicknesses of ``ALECoordinate.regrid_remap`` (vertical_coordinate.py:69-78, 96-111):
+    returns (h_new, wet, bad) with bad = wet columns that break the rule's precondition."""
+    h_src = _f64(h_src)
+    n, ny, nx = h_src.shape
+    h_new = np.empty_like(h_src)
+    wet = np.empty((ny, nx), np.uint8)
+    bad = lib().oracle_regrid(RULES[rule], _p(_f64(H)), _p(_f64(eta)), _p(h_src),
+                              _pu8(_u8(np.broadcast_to(active, (ny, nx)))), _p(_f64(coord)), float(h_min), n, ny,
+                              nx, _p(h_new), _pu8(wet))
+    return h_new, wet.view(bool), int(bad)
+
+
+def regrid_remap(rule: str, H, eta, h_src, active, fields, coord, scheme: int, h_min: float = H_MIN):
+    """(h_new, [remap_columns(h_src, f, h_new, scheme, wet) for f in fields]) as ``ALECoordinate.regrid_remap``
+    with the z* or sigma rule; ValueError where the reference's ``regrid_columns`` raises (z* and H <= 0)."""
+    h_new, wet, bad = regrid(rule, H, eta, h_src, active, coord, h_min)
+    if bad:
+        raise ValueError("z* needs H > 0 in every wet column (cells that can dry: sigma, or hybrid with d_hybrid > 0)")
+    return h_new, [remap_columns(h_src, f, h_new, scheme, wet) for f in fields]
+
+
+def diffuse_ale(T, Tw, h, act, cx, cy, okx, oky, V, kh: float, dt: float, per=None):
+    """``_diffuse_ale_kernel`` on one field (N, ny, nx); periodic axes by pad/crop with halo 1 as
+    ``TracerAdvection.diffuse_h`` (tracers.py:436-447).  ``h`` is passed as the kernel receives it."""
+    per = per or NONE
+
+    def run(T, Tw, h, act, cx, cy, okx, oky, V):
+        T, Tw, h, V = _f64(T), _f64(Tw), _f64(h), _f64(V)
+        n, ny, nx = T.shape
+        out = np.empty_like(T)
+        lib().oracle_diffuse_ale(_p(T), _p(Tw), _p(h), _pu8(_u8(act)), _p(_f64(cx)), _p(_f64(cy)),
+                                 _pu8(_u8(okx)), _pu8(_u8(oky)), _p(V), float(kh), float(dt), n, ny, nx, _p(out))
+        return out
+
+    args = (T, Tw, h, act, cx, cy, okx, oky, V)
+    if per:
+        kinds = ("c", "c", "c", "c", "u", "v", "u", "v", "c")
+        return per.crop(run(*(per.pad(a, k, 1) for a, k in zip(args, kinds))), "c", 1)
+    return run(*args)
+
+
+def face_fractions(hf) -> np.ndarray:
+    """``_fractions_kernel`` (ale.py:883-892) on (N, a, b)."""
+    hf = _f64(hf)
+    n, a, b = hf.shape
+    w = np.empty_like(hf)
+    lib().oracle_face_fractions(_p(hf), n, a, b, _p(w))
+    return w
+
+
+def remap_faces(vel, hf_src, hf_tgt, scheme: int, w_tgt=None):
+    """``ALECoordinate.remap_faces`` (vertical_coordinate.py:142-153): the velocity remap in fraction space,
+    thicknesses w_src S -> w_tgt S with the column total S of hf_src (summed k = 0 .. N-1)."""
+    hf_src = _f64(hf_src)
+    tot = np.zeros(hf_src.shape[1:])
+    for k in range(hf_src.shape[0]):
+        tot = tot + hf_src[k]
+    wet = tot > 0
+    S = np.where(wet, tot, 1.0)[None]
+    w_tgt = face_fractions(hf_tgt) if w_tgt is None else _f64(w_tgt)
+    return remap_columns(face_fractions(hf_src) * S, vel, w_tgt * S, scheme, wet)

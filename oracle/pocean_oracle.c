@@ -20,6 +20,7 @@
  *   core/components/tracers.py         TracerAdvection.advect_fct :208-254 (orchestration in oracle.py)
  *   core/vertical/remap.py             remap_column :306-397 and its helpers :46-303, _remap_columns :400-415
  */
+#include <float.h>
 #include <math.h>
 #include <stdint.h>
 #include <stdlib.h>
@@ -745,6 +746,136 @@ int oracle_advect_fct(const double* C, const double* V0, const double* V1, const
     if (Fy_eff) for (i64 p = 0; p < NY; ++p) Fy_eff[p] = FLy[p] + Cy[p] * Ay[p];
     free(mem);
     return 0;
+}
+
+/* ============================================================================================================
+ * Neighbours of the path: the z* / sigma regrid that produces the remap target, the ALE horizontal diffusion and the
+ * face fractions of the velocity remap.
+ * ========================================================================================================== */
+
+/* core/vertical/regrid.py:87-98 `enforce_min_thickness` (zw bed first, n+1 interfaces). */
+static void enforce_min_thickness(double* zw, int n, double h_min)
+{
+    const double hm = pmin(h_min, (zw[n] - zw[0]) / n);
+    for (int j = n - 1; j > 0; --j)
+        if (zw[j] > zw[j + 1] - hm) zw[j] = zw[j + 1] - hm;
+    for (int j = 1; j < n; ++j)
+        if (zw[j] < zw[j - 1] + hm) zw[j] = zw[j - 1] + hm;
+}
+
+/* regrid.py:44-61 `zstar_column`: interfaces bed first; dz_top surface first; e holds n+1 doubles. */
+static void zstar_column(double H, double eta, const double* dz_top, int n, double h_min, double* e, double* zw)
+{
+    const double D = H + eta;
+    const double hm = pmin(h_min, D / n);
+    const double s = D / H;
+    e[0] = eta;
+    for (int k = 0; k < n; ++k) e[k + 1] = e[k] - s * dz_top[k];
+    e[n] = -H;
+    for (int k = n - 1; k >= 0; --k)
+        if (e[k] < e[k + 1] + hm) e[k] = e[k + 1] + hm;
+    for (int j = 0; j <= n; ++j) zw[j] = e[n - j];
+}
+
+/* regrid.py:63-78 `sigma_column`: fractions dsigma bed first. */
+static void sigma_column(double H, double eta, const double* dsigma, int n, double h_min, double* zw)
+{
+    const double D = H + eta;
+    zw[0] = -H;
+    for (int j = 0; j < n; ++j) zw[j + 1] = zw[j] + D * dsigma[j];
+    zw[n] = eta;
+    enforce_min_thickness(zw, n, h_min);
+}
+
+static double nan_to_num(double x)
+{
+    if (isnan(x)) return 0.0;
+    if (isinf(x)) return x > 0 ? DBL_MAX : -DBL_MAX;
+    return x;
+}
+
+/*
+ * ALECoordinate.regrid_remap's regrid half for the z* (rule 0) and sigma (rule 1) rules
+ * (core/components/vertical_coordinate.py:69-78, 96-111; regrid.py:309-395): per column
+ * wet = active & (H + eta > 0) & (sum_k h_src > 0) with H = nan_to_num(H) and the sum taken k = 0 .. n-1;
+ * h_new = diff(zw) where wet, else h_src.  coord: dz_top (surface first, z*) or dsigma (bed first, sigma).
+ * Returns the number of wet columns that break the rule's precondition (z*: H > 0), which the reference
+ * raises for.
+ */
+int oracle_regrid(int rule, const double* Hin, const double* eta, const double* h_src, const uint8_t* active,
+                  const double* coord, double h_min, int n, int ny, int nx, double* h_new, uint8_t* wet)
+{
+    const i64 plane = (i64)ny * nx;
+    int bad = 0;
+#pragma omp parallel for reduction(+ : bad)
+    for (i64 c = 0; c < plane; ++c) {
+        const double H = nan_to_num(Hin[c]);
+        double tot = 0.0;
+        for (int k = 0; k < n; ++k) tot += h_src[k * plane + c];
+        const int w = active[c] && (H + eta[c] > 0) && (tot > 0);
+        wet[c] = (uint8_t)w;
+        if (!w) {
+            for (int k = 0; k < n; ++k) h_new[k * plane + c] = h_src[k * plane + c];
+            continue;
+        }
+        double* zw = (double*)malloc(2 * (size_t)(n + 1) * sizeof(double));
+        if (rule == 0) {
+            if (!(H > 0)) ++bad;
+            zstar_column(H, eta[c], coord, n, h_min, zw + n + 1, zw);
+        } else {
+            sigma_column(H, eta[c], coord, n, h_min, zw);
+        }
+        for (int k = 0; k < n; ++k) h_new[k * plane + c] = zw[k + 1] - zw[k];
+        free(zw);
+    }
+    return bad;
+}
+
+/* sigma_baroclinic.py:533-561 `_diffuse_ale_kernel` on one field (n, ny, nx); faces (ny, nx+1) / (ny+1, nx). */
+void oracle_diffuse_ale(const double* T, const double* Tw, const double* h, const uint8_t* act, const double* cx,
+                        const double* cy, const uint8_t* okx, const uint8_t* oky, const double* V, double kh,
+                        double dt, int n, int ny, int nx, double* out)
+{
+#pragma omp parallel for
+    for (int p = 0; p < n * ny; ++p) {
+        const int k = p / ny, j = p % ny;
+        const i64 r = ((i64)k * ny + j) * nx;
+        for (int i = 0; i < nx; ++i) {
+            double fw = 0.0, fe = 0.0, fs = 0.0, fn = 0.0;
+            const i64 ux = (i64)j * (nx + 1) + i, vy = (i64)j * nx + i, a = (i64)j * nx + i;
+            if (0 < i && okx[ux]) {
+                const double hu = (act[a - 1] && act[a]) ? pmin(h[r + i - 1], h[r + i]) : 0.0;
+                fw = -kh * cx[ux] * hu * (Tw[r + i] - Tw[r + i - 1]);
+            }
+            if (i < nx - 1 && okx[ux + 1]) {
+                const double hu = (act[a] && act[a + 1]) ? pmin(h[r + i], h[r + i + 1]) : 0.0;
+                fe = -kh * cx[ux + 1] * hu * (Tw[r + i + 1] - Tw[r + i]);
+            }
+            if (0 < j && oky[vy]) {
+                const double hv = (act[a - nx] && act[a]) ? pmin(h[r + i - nx], h[r + i]) : 0.0;
+                fs = -kh * cy[vy] * hv * (Tw[r + i] - Tw[r + i - nx]);
+            }
+            if (j < ny - 1 && oky[vy + nx]) {
+                const double hv = (act[a] && act[a + nx]) ? pmin(h[r + i], h[r + i + nx]) : 0.0;
+                fn = -kh * cy[vy + nx] * hv * (Tw[r + i + nx] - Tw[r + i]);
+            }
+            const double div = fe - fw + fn - fs;
+            out[r + i] = V[r + i] > 0.0 ? T[r + i] - dt * div / V[r + i] : T[r + i];
+        }
+    }
+}
+
+/* core/vertical/ale.py:883-892 `_fractions_kernel`: w_k = hf_k / sum_k hf_k (sequential sum), 1/n where the sum
+ * is not positive; hf (n, a, b). */
+void oracle_face_fractions(const double* hf, int n, int a, int b, double* w)
+{
+    const i64 plane = (i64)a * b;
+#pragma omp parallel for
+    for (i64 c = 0; c < plane; ++c) {
+        double tot = 0.0;
+        for (int k = 0; k < n; ++k) tot += hf[k * plane + c];
+        for (int k = 0; k < n; ++k) w[k * plane + c] = tot > 0.0 ? hf[k * plane + c] / tot : 1.0 / n;
+    }
 }
 
 /* Threads available to the OpenMP loops (for reporting the CPU baseline's core count). */

@@ -17,6 +17,7 @@ PERIODIC_X, PERIODIC_Y = 0x10, 0x20
 WENO_JS = 0x40
 FCT_UNLIMITED = 0x80
 PCM, PLM, PPM_H4 = 0, 1, 2
+REGRID_ZSTAR, REGRID_SIGMA = 0, 1
 ERRORS = {1: "invalid argument", 2: "workspace", 3: "CUDA error", 4: "unsupported device"}
 
 # Every symbol the header declares, with its ctypes signature.
@@ -35,6 +36,10 @@ SIGNATURES: dict[str, tuple] = {
     "pocean_advect_rk3_f64": (_I, [_P, _P, _P, _P, _P, _P, _P, _P, _I, _I, _I, _I, _U, _D, _P, _I, _P, _P, _Z,
                                    _P]),
     "pocean_remap_columns_f64": (_I, [_P, _P, _P, _P, _I, _I, _I, _I, _I, _I, _P, _P]),
+    "pocean_regrid_remap_f64": (_I, [_I, _P, _P, _P, _P, _P, _D, _P, _I, _I, _I, _I, _I, _P, _P, _P, _P, _P]),
+    "pocean_face_fractions_f64": (_I, [_P, _I, _I, _I, _P, _P]),
+    "pocean_remap_faces_f64": (_I, [_P, _P, _P, _P, _I, _I, _I, _I, _I, _P, _P]),
+    "pocean_diffuse_ale_f64": (_I, [_P, _P, _P, _P, _P, _P, _P, _P, _P, _I, _I, _I, _I, _U, _D, _D, _P, _P]),
     "pocean_batch_device_bytes": (_Z, [_I]),
     "pocean_batch_create": (_I, [_P, _I, _I, _P, _Z, ctypes.POINTER(_P), _P]),
     "pocean_batch_step": (_I, [_P, _I, _I, _I, _P]),

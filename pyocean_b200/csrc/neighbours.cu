@@ -1,0 +1,353 @@
+// The kernels either side of the tracer step: the z* / sigma regrid that produces the remap target (with the remap
+// in the same call); the velocity remap in fraction space with its face fractions; the ALE horizontal diffusion.
+//
+// Reference: core/vertical/regrid.py:44-98 (zstar_column, sigma_column, enforce_min_thickness) and :309-395
+// (regrid_columns), core/components/vertical_coordinate.py:69-111, 142-153 (ALECoordinate.regrid_remap / regrid /
+// remap_faces), core/vertical/ale.py:883-902 (_fractions_kernel), core/dynamics/sigma_baroclinic.py:533-561
+// (_diffuse_ale_kernel) with the periodic pad/crop of core/components/tracers.py:436-447.
+//
+// Every expression keeps the reference's order (compiled with -fmad=false), so results are bit-identical.
+#include <cfloat>
+#include <cmath>
+
+#include "common.cuh"
+#include "remap_io.cuh"
+
+namespace po {
+namespace nb {
+
+__device__ __forceinline__ double nan_to_num(double x)          // numpy.nan_to_num
+{
+    if (isnan(x)) return 0.0;
+    if (isinf(x)) return x > 0.0 ? DBL_MAX : -DBL_MAX;
+    return x;
+}
+
+// regrid.py:44-61 `zstar_column` into e (surface first, n+1 heights); the bed-first interfaces are e[n - j].
+__device__ __forceinline__ void zstar_heights(double H, double eta, const double* __restrict__ dz_top, int n,
+                                              double h_min, double* e)
+{
+    const double D = H + eta;
+    const double hm = pmin(h_min, D / n);
+    const double s = D / H;
+    e[0] = eta;
+    for (int k = 0; k < n; ++k) e[k + 1] = e[k] - s * __ldg(dz_top + k);
+    e[n] = -H;
+    for (int k = n - 1; k >= 0; --k)
+        if (e[k] < e[k + 1] + hm) e[k] = e[k + 1] + hm;
+}
+
+// regrid.py:63-78 `sigma_column` with `enforce_min_thickness` (:87-98) into zw (bed first, n+1 heights).
+__device__ __forceinline__ void sigma_heights(double H, double eta, const double* __restrict__ dsigma, int n,
+                                              double h_min, double* zw)
+{
+    const double D = H + eta;
+    zw[0] = -H;
+    for (int j = 0; j < n; ++j) zw[j + 1] = zw[j] + D * __ldg(dsigma + j);
+    zw[n] = eta;
+    const double hm = pmin(h_min, (zw[n] - zw[0]) / n);
+    for (int j = n - 1; j > 0; --j)
+        if (zw[j] > zw[j + 1] - hm) zw[j] = zw[j + 1] - hm;
+    for (int j = 1; j < n; ++j)
+        if (zw[j] < zw[j - 1] + hm) zw[j] = zw[j - 1] + hm;
+}
+
+// One thread per column: wet = active & (H + eta > 0) & (sum_k h_src > 0) and h_new (the rule's thicknesses where
+// wet, else h_src).  The remap that follows is the ordinary column remap with h_new as the target: a single kernel
+// that remapped from the heights it had just built was measured 6-8 % slower at 512 x 512 x 50 (the remap is
+// latency-bound and the regrid's registers and column array cost it occupancy), so the two stay separate launches.
+template <int NMAX>
+__global__ void __launch_bounds__(128) regrid_kernel(int rule, const double* __restrict__ Hin,
+                                                     const double* __restrict__ eta, const double* __restrict__ h_src,
+                                                     const uint8_t* __restrict__ active,
+                                                     const double* __restrict__ coord, double h_min, int n, i64 plane,
+                                                     double* __restrict__ h_new, uint8_t* __restrict__ wet_out,
+                                                     int* __restrict__ bad)
+{
+    const i64 c = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= plane) return;
+    const double H = nan_to_num(__ldg(Hin + c));
+    double tot = 0.0;                                          // h_src.sum(axis=0), k = 0 .. n-1
+    for (int k = 0; k < n; ++k) tot += __ldg(h_src + k * plane + c);
+    const double et = __ldg(eta + c);
+    const bool wet = __ldg(active + c) != 0 && H + et > 0.0 && tot > 0.0;
+    wet_out[c] = wet;
+    if (!wet) {
+        for (int k = 0; k < n; ++k) h_new[k * plane + c] = __ldg(h_src + k * plane + c);
+        return;
+    }
+    double z[NMAX + 1];
+    if (rule == 0) {
+        if (!(H > 0.0) && bad) atomicAdd(bad, 1);
+        zstar_heights(H, et, coord, n, h_min, z);
+        for (int k = 0; k < n; ++k) h_new[k * plane + c] = z[n - k - 1] - z[n - k];   // zw[k] = e[n - k]
+    } else {
+        sigma_heights(H, et, coord, n, h_min, z);
+        for (int k = 0; k < n; ++k) h_new[k * plane + c] = z[k + 1] - z[k];
+    }
+}
+
+// Column IO of the velocity remap in fraction space (vertical_coordinate.py:142-153): source thickness
+// w_src,k S and target w_tgt,k S, with w = hf / sum(hf) (1/n where the sum is not positive, ale.py:883-892) and S the
+// source column total (1 where it is not positive); the fractions are formed on the fly, never stored.
+template <int NF>
+struct FractionIO {
+    const double* __restrict__ hfs;
+    const double* __restrict__ hft;
+    const double* __restrict__ wt;             // given target fractions, or null
+    const double* __restrict__ u[NF];
+    double* __restrict__ o[NF];
+    i64 plane;
+    int n;
+    double tot_s, tot_t, S;
+    __device__ __forceinline__ double hs(int k) const
+    {
+        const double w = tot_s > 0.0 ? __ldg(hfs + k * plane) / tot_s : 1.0 / n;
+        return w * S;
+    }
+    __device__ __forceinline__ double ht(int k) const
+    {
+        const double w = wt ? __ldg(wt + k * plane) : (tot_t > 0.0 ? __ldg(hft + k * plane) / tot_t : 1.0 / n);
+        return w * S;
+    }
+    __device__ __forceinline__ double f(int m, int k) const { return __ldg(u[m] + k * plane); }
+    __device__ __forceinline__ void put(int m, int k, double v) { o[m][k * plane] = v; }
+};
+
+template <int NF>
+__device__ __forceinline__ void fraction_io(FractionIO<NF>& io, const double* hf_src, const double* hf_tgt,
+                                            const double* w_tgt, int n, i64 plane, i64 c)
+{
+    io.hfs = hf_src + c;
+    io.hft = hf_tgt ? hf_tgt + c : nullptr;
+    io.wt = w_tgt ? w_tgt + c : nullptr;
+    io.plane = plane;
+    io.n = n;
+    double ts = 0.0, tt = 0.0;
+    for (int k = 0; k < n; ++k) ts += __ldg(io.hfs + k * plane);
+    if (!w_tgt)
+        for (int k = 0; k < n; ++k) tt += __ldg(io.hft + k * plane);
+    io.tot_s = ts;
+    io.tot_t = tt;
+    io.S = ts > 0.0 ? ts : 1.0;
+}
+
+// One thread per face column and field group (NF fields from NF * blockIdx.y).
+template <int NF>
+__global__ void __launch_bounds__(128) remap_faces_kernel(const double* __restrict__ vel,
+                                                          const double* __restrict__ hf_src,
+                                                          const double* __restrict__ hf_tgt,
+                                                          const double* __restrict__ w_tgt, int n, i64 plane,
+                                                          int field0, int scheme, double* __restrict__ out)
+{
+    const i64 c = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= plane) return;
+    FractionIO<NF> io;
+    fraction_io(io, hf_src, hf_tgt, w_tgt, n, plane, c);
+    const int m0 = field0 + NF * (int)blockIdx.y;
+#pragma unroll
+    for (int m = 0; m < NF; ++m) {
+        io.u[m] = vel + (i64)(m0 + m) * n * plane + c;
+        io.o[m] = out + (i64)(m0 + m) * n * plane + c;
+    }
+    remap::remap_column_io<NF>(io, io.tot_s > 0.0, n, n, scheme);
+}
+
+// The general algorithm for the sentinel columns of the velocity remap.
+template <int NMAX>
+__global__ void __launch_bounds__(128) remap_faces_general_kernel(const double* __restrict__ vel,
+                                                                  const double* __restrict__ hf_src,
+                                                                  const double* __restrict__ hf_tgt,
+                                                                  const double* __restrict__ w_tgt, int n,
+                                                                  i64 plane, int scheme, double* __restrict__ out)
+{
+    const i64 c = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= plane) return;
+    double* o = out + (i64)blockIdx.y * n * plane + c;
+    if (__double_as_longlong(o[0]) != remap::kRedo) return;
+    FractionIO<1> io;
+    fraction_io(io, hf_src, hf_tgt, w_tgt, n, plane, c);
+    io.u[0] = vel + (i64)blockIdx.y * n * plane + c;
+    io.o[0] = o;
+    rc::remap_column_general<NMAX>(io, 0, n, n, scheme);
+}
+
+// ale.py:883-892 `_fractions_kernel`.
+__global__ void __launch_bounds__(128) face_fractions_kernel(const double* __restrict__ hf, int n, i64 plane,
+                                                             double* __restrict__ w)
+{
+    const i64 c = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= plane) return;
+    double tot = 0.0;
+    for (int k = 0; k < n; ++k) tot += __ldg(hf + k * plane + c);
+    for (int k = 0; k < n; ++k) w[k * plane + c] = tot > 0.0 ? __ldg(hf + k * plane + c) / tot : 1.0 / n;
+}
+
+// sigma_baroclinic.py:533-561 `_diffuse_ale_kernel` for nt stacked fields sharing the geometry; periodic axes
+// natively (the wrap face of cells 0 and n-1 is face 0, as the reference's halo-1 pad/crop reads it).  One thread
+// per (j, i) column and DKL consecutive layers: the column's masks and metrics are read once for its layers;
+// consecutive threads take consecutive i.  Every index is valid whether or not its face exists, so each layer's
+// loads are issued together and the masks applied afterwards.
+constexpr int DTI = 32, DTJ = 4, DKL = 4;
+
+__global__ void __launch_bounds__(DTI * DTJ) diffuse_ale_kernel(const double* __restrict__ T,
+                                                                const double* __restrict__ Tw,
+                                                                const double* __restrict__ h,
+                                                                const uint8_t* __restrict__ act,
+                                                                const double* __restrict__ cx,
+                                                                const double* __restrict__ cy,
+                                                                const uint8_t* __restrict__ okx,
+                                                                const uint8_t* __restrict__ oky,
+                                                                const double* __restrict__ V, int nt, int n, int ny,
+                                                                int nx, bool per_x, bool per_y, double kh, double dt,
+                                                                double* __restrict__ out)
+{
+    const int i = blockIdx.x * DTI + threadIdx.x % DTI;
+    const int j = blockIdx.y * DTJ + threadIdx.x / DTI;
+    if (i >= nx || j >= ny) return;
+    const int k0 = blockIdx.z * DKL, k1 = min(k0 + DKL, n);
+    const i64 plane = (i64)ny * nx;
+    const i64 a = (i64)j * nx + i;
+    const bool has_w = (i > 0 || per_x), has_e = (i < nx - 1 || per_x);
+    const bool has_s = (j > 0 || per_y), has_n = (j < ny - 1 || per_y);
+    const int iw = i > 0 ? i - 1 : nx - 1, ie = i < nx - 1 ? i + 1 : 0;
+    const int js = j > 0 ? j - 1 : ny - 1, jn = j < ny - 1 ? j + 1 : 0;
+    const i64 fw_i = (i64)j * (nx + 1) + i, fe_i = (i64)j * (nx + 1) + ie;
+    const i64 fs_i = (i64)j * nx + i, fn_i = (i64)jn * nx + i;
+    const i64 aw = (i64)j * nx + iw, ae = (i64)j * nx + ie, as = (i64)js * nx + i, an = (i64)jn * nx + i;
+    const bool ow = has_w && __ldg(okx + fw_i), oe = has_e && __ldg(okx + fe_i);
+    const bool os = has_s && __ldg(oky + fs_i), on = has_n && __ldg(oky + fn_i);
+    const bool ac = __ldg(act + a) != 0;
+    const bool bw = __ldg(act + aw) && ac, be = ac && __ldg(act + ae);
+    const bool bs = __ldg(act + as) && ac, bn = ac && __ldg(act + an);
+    const double cxw = __ldg(cx + fw_i), cxe = __ldg(cx + fe_i), cys = __ldg(cy + fs_i), cyn = __ldg(cy + fn_i);
+#pragma unroll 2
+    for (int k = k0; k < k1; ++k) {
+        const i64 hk = (i64)k * plane;
+        const double hc = __ldg(h + hk + a), hw = __ldg(h + hk + aw), he = __ldg(h + hk + ae),
+                     hs = __ldg(h + hk + as), hn = __ldg(h + hk + an);
+        const double v = __ldg(V + hk + a);
+        const double hu_w = bw ? pmin(hw, hc) : 0.0;
+        const double hu_e = be ? pmin(hc, he) : 0.0;
+        const double hv_s = bs ? pmin(hs, hc) : 0.0;
+        const double hv_n = bn ? pmin(hc, hn) : 0.0;
+        for (int t = 0; t < nt; ++t) {
+            const i64 to = (i64)t * n * plane + hk;
+            const double* tw = Tw + to;
+            const double twc = __ldg(tw + a), tww = __ldg(tw + aw), twe = __ldg(tw + ae), tws = __ldg(tw + as),
+                         twn = __ldg(tw + an);
+            const double tc = __ldg(T + to + a);
+            const double fw = ow ? -kh * cxw * hu_w * (twc - tww) : 0.0;
+            const double fe = oe ? -kh * cxe * hu_e * (twe - twc) : 0.0;
+            const double fs = os ? -kh * cys * hv_s * (twc - tws) : 0.0;
+            const double fn = on ? -kh * cyn * hv_n * (twn - twc) : 0.0;
+            const double div = fe - fw + fn - fs;
+            out[to + a] = v > 0.0 ? tc - dt * div / v : tc;
+        }
+    }
+}
+
+}  // namespace nb
+}  // namespace po
+
+using namespace po;
+
+extern "C" int pocean_regrid_remap_f64(int rule, const double* H, const double* eta, const double* h_src,
+                                       const uint8_t* active, const double* coord, double h_min,
+                                       const double* f_src, int nz, int ny, int nx, int nfields, int scheme,
+                                       double* h_new, uint8_t* wet, double* out, int* bad_columns, void* stream)
+{
+    const char* fn = "pocean_regrid_remap_f64";
+    if (rule != POCEAN_REGRID_ZSTAR && rule != POCEAN_REGRID_SIGMA)
+        return pocean_fail(POCEAN_EINVAL, "%s: unknown rule %d (z* = 0, sigma = 1)", fn, rule);
+    if (nz < 1 || ny < 1 || nx < 1 || nfields < 0)
+        return pocean_fail(POCEAN_EINVAL, "%s: bad sizes nz=%d ny=%d nx=%d nfields=%d", fn, nz, ny, nx, nfields);
+    if (nz > 256) return pocean_fail(POCEAN_EINVAL, "%s: at most 256 layers per column (nz=%d)", fn, nz);
+    if (nfields > 65535) return pocean_fail(POCEAN_EINVAL, "%s: nfields=%d exceeds 65535", fn, nfields);
+    if (nfields > 0 && (scheme < POCEAN_PCM || scheme > POCEAN_PPM_H4))
+        return pocean_fail(POCEAN_EINVAL, "%s: unknown scheme %d", fn, scheme);
+    if (!H || !eta || !h_src || !active || !coord || !h_new || !wet || (nfields > 0 && (!f_src || !out)))
+        return pocean_fail(POCEAN_EINVAL, "%s: null pointer", fn);
+    int rc = pocean_check_device();
+    if (rc) return rc;
+    cudaStream_t st = (cudaStream_t)stream;
+    const i64 plane = (i64)ny * nx;
+    const unsigned gx = (unsigned)((plane + 127) / 128);
+    if (nz <= 64)
+        nb::regrid_kernel<64><<<gx, 128, 0, st>>>(rule, H, eta, h_src, active, coord, h_min, nz, plane, h_new, wet,
+                                                  bad_columns);
+    else if (nz <= 128)
+        nb::regrid_kernel<128><<<gx, 128, 0, st>>>(rule, H, eta, h_src, active, coord, h_min, nz, plane, h_new, wet,
+                                                   bad_columns);
+    else
+        nb::regrid_kernel<256><<<gx, 128, 0, st>>>(rule, H, eta, h_src, active, coord, h_min, nz, plane, h_new, wet,
+                                                   bad_columns);
+    rc = pocean_check_launch(fn);
+    if (rc || nfields == 0) return rc;
+    return pocean_remap_columns_f64(h_src, f_src, h_new, wet, nz, nz, ny, nx, nfields, scheme, out, stream);
+}
+
+extern "C" int pocean_face_fractions_f64(const double* hf, int nz, int ny, int nx, double* w, void* stream)
+{
+    const char* fn = "pocean_face_fractions_f64";
+    if (nz < 1 || ny < 1 || nx < 1) return pocean_fail(POCEAN_EINVAL, "%s: bad sizes", fn);
+    if (!hf || !w) return pocean_fail(POCEAN_EINVAL, "%s: null pointer", fn);
+    int rc = pocean_check_device();
+    if (rc) return rc;
+    const i64 plane = (i64)ny * nx;
+    nb::face_fractions_kernel<<<(unsigned)((plane + 127) / 128), 128, 0, (cudaStream_t)stream>>>(hf, nz, plane, w);
+    return pocean_check_launch(fn);
+}
+
+extern "C" int pocean_remap_faces_f64(const double* vel, const double* hf_src, const double* hf_tgt,
+                                      const double* w_tgt, int nz, int ny, int nx, int nfields, int scheme,
+                                      double* out, void* stream)
+{
+    const char* fn = "pocean_remap_faces_f64";
+    if (nz < 1 || ny < 1 || nx < 1 || nfields < 1) return pocean_fail(POCEAN_EINVAL, "%s: bad sizes", fn);
+    if (nz > 256) return pocean_fail(POCEAN_EINVAL, "%s: at most 256 layers per column (nz=%d)", fn, nz);
+    if (nfields > 65535) return pocean_fail(POCEAN_EINVAL, "%s: nfields=%d exceeds 65535", fn, nfields);
+    if (scheme < POCEAN_PCM || scheme > POCEAN_PPM_H4) return pocean_fail(POCEAN_EINVAL, "%s: unknown scheme", fn);
+    if (!vel || !hf_src || (!hf_tgt && !w_tgt) || !out) return pocean_fail(POCEAN_EINVAL, "%s: null pointer", fn);
+    int rc = pocean_check_device();
+    if (rc) return rc;
+    cudaStream_t st = (cudaStream_t)stream;
+    const i64 plane = (i64)ny * nx;
+    const unsigned gx = (unsigned)((plane + 127) / 128);
+    if (nfields / 2 > 0)
+        nb::remap_faces_kernel<2><<<dim3(gx, nfields / 2), 128, 0, st>>>(vel, hf_src, hf_tgt, w_tgt, nz, plane, 0,
+                                                                          scheme, out);
+    if (nfields & 1)
+        nb::remap_faces_kernel<1><<<dim3(gx, 1), 128, 0, st>>>(vel, hf_src, hf_tgt, w_tgt, nz, plane, nfields - 1,
+                                                                scheme, out);
+    const dim3 g2(gx, (unsigned)nfields);
+    if (nz <= 64)
+        nb::remap_faces_general_kernel<64><<<g2, 128, 0, st>>>(vel, hf_src, hf_tgt, w_tgt, nz, plane, scheme, out);
+    else if (nz <= 128)
+        nb::remap_faces_general_kernel<128><<<g2, 128, 0, st>>>(vel, hf_src, hf_tgt, w_tgt, nz, plane, scheme, out);
+    else
+        nb::remap_faces_general_kernel<256><<<g2, 128, 0, st>>>(vel, hf_src, hf_tgt, w_tgt, nz, plane, scheme, out);
+    return pocean_check_launch(fn);
+}
+
+extern "C" int pocean_diffuse_ale_f64(const double* T, const double* Tw, const double* h, const uint8_t* act,
+                                      const double* cx, const double* cy, const uint8_t* okx, const uint8_t* oky,
+                                      const double* V, int nt, int nz, int ny, int nx, unsigned flags, double kh,
+                                      double dt, double* out, void* stream)
+{
+    const char* fn = "pocean_diffuse_ale_f64";
+    if (nt < 1 || nz < 1 || ny < 1 || nx < 1 || nz > 65535)
+        return pocean_fail(POCEAN_EINVAL, "%s: bad sizes nt=%d nz=%d ny=%d nx=%d", fn, nt, nz, ny, nx);
+    if (flags & ~(unsigned)(POCEAN_PERIODIC_X | POCEAN_PERIODIC_Y))
+        return pocean_fail(POCEAN_EINVAL, "%s: only the periodic flags apply (0x%x)", fn, flags);
+    if (!T || !Tw || !h || !act || !cx || !cy || !okx || !oky || !V || !out)
+        return pocean_fail(POCEAN_EINVAL, "%s: null pointer", fn);
+    int rc = pocean_check_device();
+    if (rc) return rc;
+    const dim3 grid((unsigned)((nx + nb::DTI - 1) / nb::DTI), (unsigned)((ny + nb::DTJ - 1) / nb::DTJ),
+                    (unsigned)((nz + nb::DKL - 1) / nb::DKL));
+    nb::diffuse_ale_kernel<<<grid, nb::DTI * nb::DTJ, 0, (cudaStream_t)stream>>>(
+        T, Tw, h, act, cx, cy, okx, oky, V, nt, nz, ny, nx, (flags & POCEAN_PERIODIC_X) != 0,
+        (flags & POCEAN_PERIODIC_Y) != 0, kh, dt, out);
+    return pocean_check_launch(fn);
+}

@@ -17,38 +17,17 @@
 #include "common.cuh"
 #include "fct_args.cuh"
 #include "remap_core.cuh"
+#include "remap_io.cuh"
 
-// Launch bounds of the streaming remap; POCEAN_REMAP_CTAS (resident CTAs per SM) sets its register budget when
-// defined, else ptxas chooses.  Fitted to 5 CTAs (20 warps) per SM: 10 % faster than ptxas's choice (128
+// Launch bounds of the streaming remap; POCEAN_REMAP_CTAS (resident CTAs per SM) sets its register budget.  Fitted to 5 CTAs (20 warps) per SM: 10 % faster than ptxas's choice (128
 // registers with spills, 4 CTAs), 6 % faster than 6 CTAs, measured at 512 x 512 x 50 with two fields.
 #ifndef POCEAN_REMAP_CTAS
 #define POCEAN_REMAP_CTAS 5
 #endif
-#ifdef POCEAN_REMAP_CTAS
 #define REMAP_BOUNDS __launch_bounds__(128, POCEAN_REMAP_CTAS)
-#else
-#define REMAP_BOUNDS __launch_bounds__(128)
-#endif
 
 namespace po {
 namespace remap {
-
-// Bit pattern left in out[field, 0, column] for a column that the general algorithm must finish (a NaN payload
-// that no arithmetic here produces; a coincidental match only costs a recomputation with the exact algorithm).
-constexpr long long kRedo = 0x7FF40000C0DE0001ll;
-
-template <int NF>
-struct ColumnIO {
-    const double* __restrict__ h;
-    const double* __restrict__ t;
-    const double* __restrict__ u[NF];
-    double* __restrict__ o[NF];
-    i64 plane;
-    __device__ __forceinline__ double hs(int k) const { return __ldg(h + k * plane); }
-    __device__ __forceinline__ double ht(int k) const { return __ldg(t + k * plane); }
-    __device__ __forceinline__ double f(int m, int k) const { return __ldg(u[m] + k * plane); }
-    __device__ __forceinline__ void put(int m, int k, double v) { o[m][k * plane] = v; }
-};
 
 // One column c of NF fields m0 .. m0+NF-1: f_src (nfields, n0, plane) -> out (nfields, n1, plane).
 template <int NF>
@@ -66,24 +45,7 @@ __device__ __forceinline__ void remap_stream_body(const double* __restrict__ h_s
         io.u[m] = f_src + (i64)(m0 + m) * n0 * plane + c;
         io.o[m] = out + (i64)(m0 + m) * n1 * plane + c;
     }
-    if (!wet[c]) {                                   // remap.py:405-408
-#pragma unroll
-        for (int m = 0; m < NF; ++m)
-            for (int k = 0; k < n1; ++k) io.put(m, k, n0 == n1 ? io.f(m, k) : nan(""));
-        return;
-    }
-    int n_active = 0, last = -1;
-    for (int k = 0; k < n0; ++k)
-        if (io.hs(k) > 0.0) { ++n_active; last = k; }
-    bool regular = true;
-    for (int k = 0; k < n1; ++k) regular = regular && io.ht(k) >= 0.0;
-    if (!regular) {
-#pragma unroll
-        for (int m = 0; m < NF; ++m) io.put(m, 0, __longlong_as_double(kRedo));
-        return;
-    }
-    if (n_active == 0) rc::remap_column_dry<NF>(io, n0, n1);
-    else rc::remap_column_stream<NF>(io, n0, n1, scheme, n_active, last);
+    remap_column_io<NF>(io, wet[c] != 0, n0, n1, scheme);
 }
 
 template <int NMAX>
@@ -179,6 +141,19 @@ void remap_batched_launch(const BatchDomain* doms, const int* off_dev, const int
     else remap::remap_general_batched<256><<<total(BP_RGEN), 128, 0, st>>>(doms, offs(BP_RGEN), ndom);
 }
 
+void remap_general_launch(const double* h_src, const double* f_src, const double* h_tgt, int n0, int n1, i64 plane,
+                          int nfields, int scheme, double* out, cudaStream_t st)
+{
+    const dim3 g2((unsigned)((plane + 127) / 128), (unsigned)nfields);
+    const int nm = n0 > n1 ? n0 : n1;
+    if (nm <= 64)
+        remap::remap_general_kernel<64><<<g2, 128, 0, st>>>(h_src, f_src, h_tgt, n0, n1, plane, scheme, out);
+    else if (nm <= 128)
+        remap::remap_general_kernel<128><<<g2, 128, 0, st>>>(h_src, f_src, h_tgt, n0, n1, plane, scheme, out);
+    else
+        remap::remap_general_kernel<256><<<g2, 128, 0, st>>>(h_src, f_src, h_tgt, n0, n1, plane, scheme, out);
+}
+
 }  // namespace po
 
 using namespace po;
@@ -209,13 +184,6 @@ extern "C" int pocean_remap_columns_f64(const double* h_src, const double* f_src
     if (nfields & 1)
         remap::remap_stream_kernel<1><<<dim3(gx, 1), 128, 0, st>>>(h_src, f_src, h_tgt, wet, n0, n1, plane,
                                                                    nfields - 1, scheme, out);
-    const dim3 g2(gx, (unsigned)nfields);
-    const int nm = n0 > n1 ? n0 : n1;
-    if (nm <= 64)
-        remap::remap_general_kernel<64><<<g2, 128, 0, st>>>(h_src, f_src, h_tgt, n0, n1, plane, scheme, out);
-    else if (nm <= 128)
-        remap::remap_general_kernel<128><<<g2, 128, 0, st>>>(h_src, f_src, h_tgt, n0, n1, plane, scheme, out);
-    else
-        remap::remap_general_kernel<256><<<g2, 128, 0, st>>>(h_src, f_src, h_tgt, n0, n1, plane, scheme, out);
+    remap_general_launch(h_src, f_src, h_tgt, n0, n1, plane, nfields, scheme, out, st);
     return pocean_check_launch(fn);
 }

@@ -1,0 +1,122 @@
+"""
+Timing of the neighbours of the tracer step at the benchmark size (512 x 512 x 50 basin, T and S):
+
+* the z* regrid + PPM_H4 remap of both tracers in one call (``pocean_regrid_remap_f64``), and the regrid alone;
+* the ALE horizontal diffusion of the T/S stack, with its compulsory HBM bytes (T, Tw in and out per tracer; h, V
+  per cell; the 2-D masks and metrics once) against the measured HBM peak;
+* the velocity remap in fraction space of the u-faces (512 x 513 x 50).
+
+    python -m pyocean_b200.neighbours_report
+"""
+from __future__ import annotations
+
+import json
+import os
+
+import numpy as np
+import torch
+
+from . import _lib
+from . import workloads as W
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _hbm_peak() -> float:
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"])
+    return 6650.0
+
+
+def _time(fn, reps: int = 20, warm: int = 3) -> float:
+    for _ in range(warm):
+        fn()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(reps):
+        fn()
+    e1.record()
+    e1.synchronize()
+    return e0.elapsed_time(e1) / reps
+
+
+def neighbours_report(device=None) -> dict:
+    dev = torch.device("cuda", torch.cuda.current_device()) if device is None else torch.device(device)
+    L = _lib.lib()
+    w = W.basin()
+    nt, n, ny, nx = w.C.shape
+    plane = ny * nx
+    g = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)                       # noqa: E731
+    st = lambda: torch.cuda.current_stream(dev).cuda_stream                                # noqa: E731
+    H = w.h_tgt.sum(0)
+    Hd, etad = g(np.where(w.wet, H, np.nan)), g(np.zeros((ny, nx)))
+    hs, C = g(w.h_src), g(w.C)
+    act = g(w.wet.astype(np.uint8))
+    dz = g(np.full(n, 4000.0 / n))
+    h_new, wet = torch.empty_like(hs), torch.empty((ny, nx), dtype=torch.uint8, device=dev)
+    out, out2 = torch.empty_like(C), torch.empty_like(C)
+
+    def fused():
+        _lib.check(L.pocean_regrid_remap_f64(0, Hd.data_ptr(), etad.data_ptr(), hs.data_ptr(), act.data_ptr(),
+                                             dz.data_ptr(), 1e-3, C.data_ptr(), n, ny, nx, nt, 2, h_new.data_ptr(),
+                                             wet.data_ptr(), out.data_ptr(), None, st()), "regrid_remap")
+
+    def separate():
+        _lib.check(L.pocean_regrid_remap_f64(0, Hd.data_ptr(), etad.data_ptr(), hs.data_ptr(), act.data_ptr(),
+                                             dz.data_ptr(), 1e-3, None, n, ny, nx, 0, 2, h_new.data_ptr(),
+                                             wet.data_ptr(), None, None, st()), "regrid")
+        _lib.check(L.pocean_remap_columns_f64(hs.data_ptr(), C.data_ptr(), h_new.data_ptr(), wet.data_ptr(), n, n,
+                                              ny, nx, nt, 2, out2.data_ptr(), st()), "remap_columns")
+
+    def regrid_only():
+        _lib.check(L.pocean_regrid_remap_f64(0, Hd.data_ptr(), etad.data_ptr(), hs.data_ptr(), act.data_ptr(),
+                                             dz.data_ptr(), 1e-3, None, n, ny, nx, 0, 2, h_new.data_ptr(),
+                                             wet.data_ptr(), None, None, st()), "regrid")
+
+    t_fused, t_sep, t_regrid = _time(fused), _time(separate), _time(regrid_only)
+    torch.cuda.synchronize()
+    same = bool(torch.equal(out, out2))
+
+    # diffusion of the stack
+    rng = np.random.default_rng(1)
+    h = g(np.where(w.wet[None], w.h_tgt, 0.0))
+    V = g(w.V0)
+    cx, cy = g(rng.uniform(0.5, 2.0, (ny, nx + 1))), g(rng.uniform(0.5, 2.0, (ny + 1, nx)))
+    okx = g((rng.random((ny, nx + 1)) > 0.05).astype(np.uint8))
+    oky = g((rng.random((ny + 1, nx)) > 0.05).astype(np.uint8))
+    Tw = C - 10.0
+    dout = torch.empty_like(C)
+
+    def diffuse():
+        _lib.check(L.pocean_diffuse_ale_f64(C.data_ptr(), Tw.data_ptr(), h.data_ptr(), act.data_ptr(), cx.data_ptr(),
+                                            cy.data_ptr(), okx.data_ptr(), oky.data_ptr(), V.data_ptr(), nt, n, ny,
+                                            nx, 0, 100.0, 600.0, dout.data_ptr(), st()), "diffuse_ale")
+
+    t_diff = _time(diffuse)
+    diff_bytes = n * plane * (24 * nt + 16) + plane * (1 + 2 * 9)
+    # velocity remap of the u-faces
+    nf = nx + 1
+    hu_src = g(np.abs(rng.normal(5.0, 2.0, (n, ny, nf))))
+    hu_tgt = g(np.abs(rng.normal(5.0, 2.0, (n, ny, nf))))
+    vel = g(rng.normal(0.0, 0.3, (n, ny, nf)))
+    vout = torch.empty_like(vel)
+
+    def faces():
+        _lib.check(L.pocean_remap_faces_f64(vel.data_ptr(), hu_src.data_ptr(), hu_tgt.data_ptr(), None, n, ny, nf, 1,
+                                            2, vout.data_ptr(), st()), "remap_faces")
+
+    t_faces = _time(faces)
+    peak = _hbm_peak()
+    return dict(workload=w.name,
+                regrid_remap_zstar=dict(call_ms=t_fused, regrid_ms=t_regrid, regrid_then_remap_columns_ms=t_sep,
+                                        equal=same, fields=nt),
+                diffuse_ale=dict(ms=t_diff, algorithmic_bytes=diff_bytes, gbs=diff_bytes / t_diff / 1e6,
+                                 frac_of_measured_hbm=diff_bytes / t_diff / 1e6 / peak, fields=nt),
+                remap_faces_u=dict(ms=t_faces, faces=n * ny * nf))
+
+
+if __name__ == "__main__":
+    print(json.dumps(neighbours_report()))

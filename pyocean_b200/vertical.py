@@ -1,0 +1,143 @@
+"""
+The vertical-coordinate neighbours of the tracer step, with the reference's interface, computed on the GPU.
+
+``ALECoordinate`` mirrors the part of ``core.components.vertical_coordinate.ALECoordinate`` that the ALE tracer
+step calls (vertical_coordinate.py:69-111, 142-153): ``regrid_remap`` (regrid to the z* or sigma target, then the
+conservative remap of every field — one fused kernel: the target grid is built in the remap kernel and written once),
+``regrid`` and ``remap_faces`` (the velocity remap in fraction space).  ``face_fractions`` is
+``core.vertical.ale.face_fractions``.  Arrays are NumPy (copied in and out) or CUDA torch tensors (results stay on
+the device).  The hybrid (HYCOM1) rule is not on the GPU: ``NotImplementedError``.
+"""
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._device import Converter, shape_of
+
+H_MIN = 1e-3                                    # core/vertical/regrid.py:41
+RULES = {"zstar": _lib.REGRID_ZSTAR, "sigma": _lib.REGRID_SIGMA}
+
+
+class ALECoordinate:
+    """z* / sigma regrid + remap and the velocity remap of an ALE vertical coordinate, on B200.
+
+    ``H`` (ny, nx) depth [m] (NaN on land reads as 0), ``active`` (ny, nx) water mask, ``regrid_rule`` 'zstar' or
+    'sigma', ``regrid_params`` with ``dz_top`` (z*, surface first) or ``dsigma`` (sigma, bed first) and optional
+    ``h_min``, ``remap_code`` 0 / 1 / 2 (PCM / PLM / PPM_H4) — the attributes of the reference's component."""
+
+    def __init__(self, H, active, regrid_rule: str, regrid_params: dict, remap_code: int = _lib.PPM_H4) -> None:
+        if regrid_rule not in ("zstar", "sigma", "hybrid"):
+            raise ValueError(f"unknown rule {regrid_rule!r}; use 'zstar', 'sigma' or 'hybrid'")
+        self.H, self.active = H, active
+        self.regrid_rule, self.regrid_params, self.remap_code = regrid_rule, dict(regrid_params), int(remap_code)
+
+    @classmethod
+    def like(cls, ref) -> "ALECoordinate":
+        """The GPU coordinate of a reference ALECoordinate instance (reads H, active, rule, params, remap code)."""
+        return cls(ref.H, ref.active, ref.regrid_rule, ref.regrid_params, ref.remap_code)
+
+    def _coord(self, n: int) -> np.ndarray:
+        if self.regrid_rule == "hybrid":
+            raise NotImplementedError("the hybrid (HYCOM1) regrid rule is not on the GPU")
+        key = "dz_top" if self.regrid_rule == "zstar" else "dsigma"
+        if key not in self.regrid_params:
+            raise ValueError(f"regrid_columns({self.regrid_rule!r}) needs params[{key!r}]")
+        coord = np.ascontiguousarray(self.regrid_params[key], dtype=np.float64)
+        if coord.shape != (n,):
+            raise ValueError(f"{key} must have one entry per layer ({n}), got {coord.shape}")
+        return coord
+
+    def regrid_remap(self, eta, h_src, fields, T=None, S=None):
+        """(h_new, [remap_columns(h_src, f, h_new, remap_code, wet) for f in fields]) with the rule's target grid
+        (vertical_coordinate.py:69-78); ``fields`` a list of (N, ny, nx) arrays or one (nf, N, ny, nx) stack."""
+        stacked = not isinstance(fields, (list, tuple))
+        h_new, outs = self._run(eta, h_src, fields if stacked else list(fields))
+        return h_new, (outs if stacked else list(outs))
+
+    def regrid(self, eta, h, T=None, wet=None, S=None):
+        """New layer thicknesses of the rule where wet (active, D > 0, water in the column), else h
+        (vertical_coordinate.py:96-111; ``wet`` is always the reference's default mask)."""
+        if wet is not None:
+            raise NotImplementedError("regrid with a caller-given wet mask; the GPU regrid derives it as the "
+                                      "reference's default")
+        return self._run(eta, h, None)[0]
+
+    def _run(self, eta, h_src, fields):
+        n, ny, nx = shape_of(h_src)
+        coord = self._coord(n)
+        if fields is None:
+            arrays = ()
+        elif isinstance(fields, list):
+            arrays = tuple(fields)
+        else:
+            arrays = (fields,)
+        cv = Converter(h_src, eta, self.H, *arrays)
+        hsd = cv.f64(h_src)
+        Hd = cv.f64(self.H, (ny, nx))
+        ed = cv.f64(eta, (ny, nx))
+        act = cv.u8(self.active, (ny, nx))
+        cd = cv.f64(coord)
+        if fields is None:
+            nf, fd = 0, None
+        elif isinstance(fields, list):
+            nf = len(fields)
+            fd = torch.stack([cv.f64(f, (n, ny, nx)) for f in fields]) if nf else None
+        else:
+            fd = cv.f64(fields)
+            nf = fd.shape[0]
+        h_new = cv.empty((n, ny, nx))
+        wet = torch.empty((ny, nx), dtype=torch.uint8, device=cv.device)
+        out = cv.empty((nf, n, ny, nx)) if nf else None
+        bad = torch.zeros(1, dtype=torch.int32, device=cv.device)
+        rc = _lib.lib().pocean_regrid_remap_f64(RULES[self.regrid_rule], Hd.data_ptr(), ed.data_ptr(),
+                                                hsd.data_ptr(), act.data_ptr(), cd.data_ptr(),
+                                                float(self.regrid_params.get("h_min", H_MIN)),
+                                                None if fd is None else fd.data_ptr(), n, ny, nx, nf,
+                                                self.remap_code, h_new.data_ptr(), wet.data_ptr(),
+                                                None if out is None else out.data_ptr(), bad.data_ptr(), cv.stream())
+        _lib.check(rc, "regrid_remap")
+        if int(bad.item()):
+            raise ValueError("z* needs H > 0 in every wet column (cells that can dry: sigma, or hybrid with "
+                             "d_hybrid > 0)")
+        if out is None:
+            return cv.out(h_new), None
+        if isinstance(fields, list):
+            return cv.out(h_new), [cv.out(out[m]) for m in range(nf)]
+        return cv.out(h_new), cv.out(out)
+
+    def remap_faces(self, vel, hf_src, hf_tgt, w_tgt=None):
+        """Face velocities remapped from the face layers hf_src to hf_tgt in fraction space (Σ w u conserved,
+        vertical_coordinate.py:142-153).  ``vel`` (N, ny, nf) or a stack (m, N, ny, nf)."""
+        return remap_faces(vel, hf_src, hf_tgt, self.remap_code, w_tgt)
+
+
+def remap_faces(vel, hf_src, hf_tgt, scheme: int, w_tgt=None):
+    vs, hs = shape_of(vel), shape_of(hf_src)
+    if len(hs) != 3 or vs[-3:] != hs or len(vs) not in (3, 4) or shape_of(hf_tgt) != hs:
+        raise ValueError(f"face arrays must share (N, ny, nf): vel {vs}, hf_src {hs}, hf_tgt {shape_of(hf_tgt)}")
+    n, ny, nf = hs
+    m = vs[0] if len(vs) == 4 else 1
+    cv = Converter(vel, hf_src, hf_tgt, w_tgt)
+    vd, hsd, htd = cv.f64(vel), cv.f64(hf_src), cv.f64(hf_tgt)
+    wd = None if w_tgt is None else cv.f64(w_tgt, hs)
+    out = cv.empty(vs)
+    rc = _lib.lib().pocean_remap_faces_f64(vd.data_ptr(), hsd.data_ptr(), htd.data_ptr(),
+                                           None if wd is None else wd.data_ptr(), n, ny, nf, m, int(scheme),
+                                           out.data_ptr(), cv.stream())
+    _lib.check(rc, "remap_faces")
+    return cv.out(out)
+
+
+def face_fractions(hf):
+    """w_k = h_k,f / Σ_k h_k,f, uniform 1/N on faces with no water (core/vertical/ale.py:895-902)."""
+    if len(shape_of(hf)) != 3:
+        raise ValueError("face_fractions expects (N, ny, nf) face thicknesses")
+    n, ny, nf = shape_of(hf)
+    cv = Converter(hf)
+    hd = cv.f64(hf)
+    w = cv.empty((n, ny, nf))
+    _lib.check(_lib.lib().pocean_face_fractions_f64(hd.data_ptr(), n, ny, nf, w.data_ptr(), cv.stream()),
+               "face_fractions")
+    return cv.out(w)

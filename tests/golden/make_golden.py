@@ -41,6 +41,9 @@ from core.dynamics import sigma_baroclinic as sb       # noqa: E402
 from core.model import threads                         # noqa: E402
 from core.model.periodic import Periodic               # noqa: E402
 from core.vertical import remap as rm                  # noqa: E402
+from core.vertical import regrid as rg                 # noqa: E402
+from core.vertical.ale import face_fractions           # noqa: E402
+from core.components.vertical_coordinate import ALECoordinate   # noqa: E402
 
 
 class _OB:
@@ -250,6 +253,122 @@ def remap_cases():
     return out
 
 
+class _Vertical:
+    """The attributes of an ALECoordinate that regrid_remap / regrid / remap_faces read, with the reference's own
+    methods (core/components/vertical_coordinate.py:69-153)."""
+    regrid_remap = ALECoordinate.regrid_remap
+    regrid = ALECoordinate.regrid
+    regrid_density = ALECoordinate.regrid_density
+    remap_faces = ALECoordinate.remap_faces
+
+    def __init__(self, H, active, rule, params, remap_code):
+        self.H, self.active, self.regrid_rule = H, active, rule
+        self.regrid_params, self.remap_code = params, remap_code
+
+
+def neighbour_cases():
+    """The z*/sigma regrid + remap, the ALE diffusion kernel and the velocity remap in fraction space."""
+    out = {}
+    rng = np.random.default_rng(21)
+    n, ny, nx = 12, 7, 9
+    H = rng.uniform(20.0, 400.0, (ny, nx))
+    H[0, :3] = rng.uniform(0.5, 3.0, 3)                       # shallower than the nominal levels: collapsed layers
+    H[1, 0] = np.nan                                         # land depth NaN (nan_to_num -> 0, not wet)
+    active = rng.random((ny, nx)) > 0.1
+    active[1, 0] = True
+    eta = rng.uniform(-1.0, 1.0, (ny, nx))
+    eta[1, 0] = -0.5                                         # the NaN-depth column is dry (D <= 0)
+    h_src = rng.uniform(0.5, 40.0, (n, ny, nx))
+    h_src[rng.random(h_src.shape) < 0.1] = 0.0
+    h_src[:, 2, 2] = 0.0                                     # no water: not wet
+    T = rng.normal(12.0, 3.0, (n, ny, nx))
+    S = rng.normal(35.0, 0.3, (n, ny, nx))
+    dz_top = np.linspace(2.0, 30.0, n)                       # nominal z* levels, surface first
+    dsigma = rng.uniform(0.5, 1.5, n)
+    dsigma /= dsigma.sum()
+    for rule, params in (("zstar", {"dz_top": dz_top}), ("sigma", {"dsigma": dsigma}),
+                         ("zstar_hmin", {"dz_top": dz_top, "h_min": 0.25})):
+        Hc = H.copy()
+        if rule == "sigma":
+            Hc[3, 4] = -0.5                                   # flooded land: sigma at any depth (D > 0 with eta)
+        etac = eta.copy()
+        etac[3, 4] = 1.0
+        r = rule.split("_")[0]
+        vc = _Vertical(Hc, active, r, params, rm.PPM_H4)
+        h_new, (T1, S1) = vc.regrid_remap(etac, h_src, [T, S], T, S)
+        coord = params["dz_top"] if r == "zstar" else params["dsigma"]
+        out["regrid_" + rule] = dict(rule=r, H=Hc, eta=etac, h_src=h_src, active=active, coord=coord,
+                                     h_min=params.get("h_min", rg.H_MIN), T=T, S=S, h_new=h_new, T1=T1, S1=S1)
+    # z* with a wet column of H <= 0: the reference raises ValueError
+    Hb = H.copy()
+    Hb[4, 4] = 0.0
+    eb = eta.copy()
+    eb[4, 4] = 0.5
+    try:
+        _Vertical(Hb, active | True, "zstar", {"dz_top": dz_top}, rm.PPM_H4).regrid_remap(eb, h_src, [T], T)
+        raised = False
+    except ValueError:
+        raised = True
+    assert raised
+    out["regrid_zstar_bad"] = dict(rule="zstar", H=Hb, eta=eb, h_src=h_src, active=active | True, coord=dz_top,
+                                   h_min=rg.H_MIN, T=T, raises=True)
+
+    # ALE diffusion kernel (tracers.py:436-447): closed, periodic x, periodic x and y
+    n, ny, nx = 4, 9, 11
+    for name, axes in (("closed", ()), ("per_x", ("x",)), ("per_xy", ("x", "y"))):
+        Tf = rng.normal(15.0, 2.0, (n, ny, nx))
+        Tw = Tf - rng.normal(14.0, 0.5, (n, 1, 1))
+        act = rng.random((ny, nx)) > 0.1
+        h = np.where(act[None], rng.uniform(0.0, 20.0, (n, ny, nx)), 0.0)
+        h[1, 3, 3] = 0.0
+        cx = rng.uniform(0.5, 2.0, (ny, nx + 1))
+        cy = rng.uniform(0.5, 2.0, (ny + 1, nx))
+        okx = rng.random((ny, nx + 1)) > 0.1
+        oky = rng.random((ny + 1, nx)) > 0.1
+        if "x" in axes:
+            cx[:, -1] = cx[:, 0]
+            okx[:, -1] = okx[:, 0]
+        if "y" in axes:
+            cy[-1] = cy[0]
+            oky[-1] = oky[0]
+        V = np.where(act[None], rng.uniform(1e5, 1e7, (n, ny, nx)), 0.0)
+        kh, dt = 50.0, 300.0
+
+        def run(T, Tw, h, act, cx, cy, okx, oky, V):
+            o = np.empty(np.shape(T))
+            c = np.ascontiguousarray
+            sb._diffuse_ale_kernel(c(T, dtype=float), c(Tw, dtype=float), c(h, dtype=float), c(act),
+                                   c(cx, dtype=float), c(cy, dtype=float), c(okx), c(oky), c(V, dtype=float), kh, dt,
+                                   o)
+            return o
+        args = (Tf, Tw, h, act, cx, cy, okx, oky, V)
+        if axes:
+            res = Periodic(axes).apply(run, args, ("c", "c", "c", "c", "u", "v", "u", "v", "c"), "c", 1)
+        else:
+            res = run(*args)
+        out["diffuse_" + name] = dict(T=Tf, Tw=Tw, h=h, act=act, cx=cx, cy=cy, okx=okx, oky=oky, V=V, kh=kh,
+                                      dt=dt, periodic=np.array(axes, dtype=str), out=res)
+
+    # velocity remap in fraction space and the fractions themselves (u-faces (N, ny, nx+1))
+    n, ny, nxf = 10, 6, 9
+    vel = rng.normal(0.0, 0.3, (n, ny, nxf))
+    hf_src = rng.uniform(0.0, 8.0, (n, ny, nxf))
+    hf_src[rng.random(hf_src.shape) < 0.15] = 0.0
+    hf_src[:, 0, 0] = 0.0                                    # a face without water
+    hf_tgt = rng.uniform(0.1, 6.0, (n, ny, nxf))
+    hf_tgt[:4, 1, :] = 0.0
+    for code, name in ((rm.PPM_H4, "ppm_h4"), (rm.PLM, "plm")):
+        vc = _Vertical(None, None, "zstar", {}, code)
+        out["faces_" + name] = dict(vel=vel, hf_src=hf_src, hf_tgt=hf_tgt, scheme=code,
+                                    out=vc.remap_faces(vel, hf_src, hf_tgt))
+    w_given = face_fractions(hf_tgt)
+    out["faces_wgiven"] = dict(vel=vel, hf_src=hf_src, hf_tgt=hf_tgt, w_tgt=w_given, scheme=rm.PPM_H4,
+                               out=_Vertical(None, None, "zstar", {}, rm.PPM_H4).remap_faces(vel, hf_src, hf_tgt,
+                                                                                              w_given))
+    out["fractions"] = dict(hf=hf_src, w=face_fractions(hf_src))
+    return out
+
+
 def save(name, cases):
     flat = {}
     for case, rec in cases.items():
@@ -262,7 +381,8 @@ def save(name, cases):
 
 if __name__ == "__main__":
     threads.set_threads(1)
-    save("fct", fct_cases())
-    save("rk3", rk3_cases())
-    save("kernels", kernel_cases())
-    save("remap", remap_cases())
+    which = sys.argv[2:] or ["fct", "rk3", "kernels", "remap", "neighbours"]
+    makers = {"fct": fct_cases, "rk3": rk3_cases, "kernels": kernel_cases, "remap": remap_cases,
+              "neighbours": neighbour_cases}
+    for name in which:
+        save(name, makers[name]())

@@ -103,3 +103,17 @@ def test_batch_argument_errors():
     assert L.pocean_batch_create(8, 1, 64, 264, 1 << 20, ctypes.byref(h), None) == 2  # misaligned
     assert h.value is None
     assert L.pocean_batch_step(None, 0, 2, 0, None) == 1
+
+
+def test_neighbour_argument_errors():
+    L = _lib.lib()
+    # unknown rule, too many layers, null pointers, bad scheme
+    assert L.pocean_regrid_remap_f64(2, 8, 8, 8, 8, 8, 1e-3, 8, 4, 3, 3, 1, 2, 8, 8, 8, None, None) == 1
+    assert L.pocean_regrid_remap_f64(0, 8, 8, 8, 8, 8, 1e-3, 8, 300, 3, 3, 1, 2, 8, 8, 8, None, None) == 1
+    assert L.pocean_regrid_remap_f64(0, 8, 8, 8, 8, None, 1e-3, 8, 4, 3, 3, 1, 2, 8, 8, 8, None, None) == 1
+    assert L.pocean_regrid_remap_f64(0, 8, 8, 8, 8, 8, 1e-3, 8, 4, 3, 3, 1, 9, 8, 8, 8, None, None) == 1
+    assert L.pocean_face_fractions_f64(None, 4, 3, 3, 8, None) == 1
+    assert L.pocean_remap_faces_f64(8, 8, None, None, 4, 3, 3, 1, 2, 8, None) == 1
+    assert L.pocean_remap_faces_f64(8, 8, 8, None, 4, 3, 3, 0, 2, 8, None) == 1
+    assert L.pocean_diffuse_ale_f64(8, 8, 8, 8, 8, 8, 8, 8, 8, 1, 2, 3, 4, 0x1, 1.0, 1.0, 8, None) == 1   # open flag
+    assert L.pocean_diffuse_ale_f64(8, 8, 8, 8, 8, 8, 8, 8, None, 1, 2, 3, 4, 0, 1.0, 1.0, 8, None) == 1

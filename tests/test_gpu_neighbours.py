@@ -1,0 +1,112 @@
+"""The neighbours of the tracer step on the GPU: z* / sigma regrid fused with the remap, the velocity remap in
+fraction space, the face fractions and the ALE diffusion — bit for bit against the reference's golden vectors and
+the oracle, plus full-size cases against the oracle."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+import torch
+
+from conftest import case_periodic, load_golden
+from oracle import oracle as O
+from pyocean_b200 import ALECoordinate, Periodic, diffuse_ale, face_fractions, remap_faces
+from pyocean_b200 import workloads as W
+
+pytestmark = pytest.mark.gpu
+NB = load_golden("neighbours")
+
+
+def _vc(rec):
+    key = "dz_top" if str(rec["rule"]) == "zstar" else "dsigma"
+    return ALECoordinate(rec["H"], rec["active"], str(rec["rule"]), {key: rec["coord"], "h_min": float(rec["h_min"])},
+                         2)
+
+
+@pytest.mark.parametrize("case", ["regrid_zstar", "regrid_sigma", "regrid_zstar_hmin"])
+def test_regrid_remap_matches_reference_bitwise(case):
+    rec = NB[case]
+    h_new, (T1, S1) = _vc(rec).regrid_remap(rec["eta"], rec["h_src"], [rec["T"], rec["S"]], rec["T"], rec["S"])
+    np.testing.assert_array_equal(h_new, rec["h_new"])
+    np.testing.assert_array_equal(T1, rec["T1"])
+    np.testing.assert_array_equal(S1, rec["S1"])
+
+
+@pytest.mark.parametrize("case", ["regrid_zstar", "regrid_sigma"])
+def test_regrid_alone_and_three_fields(case):
+    rec = NB[case]
+    vc = _vc(rec)
+    np.testing.assert_array_equal(vc.regrid(rec["eta"], rec["h_src"], rec["T"]), rec["h_new"])
+    U = rec["T"] * 0.5 + 1.0
+    _, outs = vc.regrid_remap(rec["eta"], rec["h_src"], [rec["T"], rec["S"], U])   # a pair and an odd field
+    wet = rec["active"] & (np.nan_to_num(rec["H"]) + rec["eta"] > 0) & (rec["h_src"].sum(0) > 0)
+    np.testing.assert_array_equal(outs[2], O.remap_columns(rec["h_src"], U, rec["h_new"], 2, wet))
+
+
+def test_zstar_regrid_raises_like_the_reference():
+    rec = NB["regrid_zstar_bad"]
+    with pytest.raises(ValueError, match="z\\* needs H > 0"):
+        _vc(rec).regrid_remap(rec["eta"], rec["h_src"], [rec["T"]], rec["T"])
+
+
+@pytest.mark.parametrize("case", ["faces_ppm_h4", "faces_plm", "faces_wgiven"])
+def test_velocity_remap_matches_reference_bitwise(case):
+    rec = NB[case]
+    out = remap_faces(rec["vel"], rec["hf_src"], rec["hf_tgt"], int(rec["scheme"]), rec.get("w_tgt"))
+    np.testing.assert_array_equal(out, rec["out"])
+
+
+def test_face_fractions_match_reference_bitwise():
+    rec = NB["fractions"]
+    np.testing.assert_array_equal(face_fractions(rec["hf"]), rec["w"])
+
+
+@pytest.mark.parametrize("case", ["diffuse_closed", "diffuse_per_x", "diffuse_per_xy"])
+def test_diffusion_matches_reference_bitwise(case):
+    rec = NB[case]
+    per = Periodic(case_periodic(rec))
+    out = diffuse_ale(rec["T"], rec["Tw"], rec["h"], rec["act"], rec["cx"], rec["cy"], rec["okx"], rec["oky"],
+                      rec["V"], float(rec["kh"]), float(rec["dt"]), per)
+    np.testing.assert_array_equal(out, rec["out"])
+
+
+def test_diffusion_stack_equals_fields_one_by_one():
+    rec = NB["diffuse_per_x"]
+    per = Periodic(("x",))
+    T2 = np.stack([rec["T"], rec["T"] * 1.5])
+    Tw2 = np.stack([rec["Tw"], rec["Tw"] - 3.0])
+    out = diffuse_ale(T2, Tw2, rec["h"], rec["act"], rec["cx"], rec["cy"], rec["okx"], rec["oky"], rec["V"],
+                      float(rec["kh"]), float(rec["dt"]), per)
+    for m in range(2):
+        one = O.diffuse_ale(T2[m], Tw2[m], rec["h"], rec["act"], rec["cx"], rec["cy"], rec["okx"], rec["oky"],
+                            rec["V"], float(rec["kh"]), float(rec["dt"]), O.Periodic(("x",)))
+        np.testing.assert_array_equal(out[m], one)
+
+
+def test_full_size_regrid_remap_and_diffusion_against_oracle():
+    # the basin's bathymetry with z* and sigma targets, both tracers; the diffusion of T on the same grid
+    w = W.basin(seed=2, nx=256, ny=192, n=30)
+    rng = np.random.default_rng(9)
+    H = w.h_tgt.sum(0)
+    H = np.where(w.wet, H, np.nan)
+    eta = rng.uniform(-0.5, 0.5, H.shape)
+    dz = np.linspace(5.0, 300.0, 30)
+    for rule, params in (("zstar", {"dz_top": dz}), ("sigma", {"dsigma": np.full(30, 1 / 30)})):
+        vc = ALECoordinate(H, w.wet, rule, params, 2)
+        dev = torch.device("cuda", 0)
+        g = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)                   # noqa: E731
+        h_new, outs = vc.regrid_remap(g(eta), g(w.h_src), g(w.C))
+        coord = params["dz_top"] if rule == "zstar" else params["dsigma"]
+        ref_h, ref = O.regrid_remap(rule, H, eta, w.h_src, w.wet, [w.C[0], w.C[1]], coord, 2)
+        assert torch.equal(h_new.cpu(), torch.from_numpy(ref_h))
+        for m in range(2):
+            np.testing.assert_array_equal(outs[m].cpu().numpy(), ref[m])
+    n, ny, nx = w.V0.shape
+    act = w.wet
+    h = np.where(act[None], w.h_tgt, 0.0)
+    cx = rng.uniform(0.5, 2.0, (ny, nx + 1))
+    cy = rng.uniform(0.5, 2.0, (ny + 1, nx))
+    okx = rng.random((ny, nx + 1)) > 0.05
+    oky = rng.random((ny + 1, nx)) > 0.05
+    Tw = w.C[0] - 10.0
+    out = diffuse_ale(w.C[0], Tw, h, act, cx, cy, okx, oky, w.V0, 100.0, 600.0)
+    np.testing.assert_array_equal(out, O.diffuse_ale(w.C[0], Tw, h, act, cx, cy, okx, oky, w.V0, 100.0, 600.0))

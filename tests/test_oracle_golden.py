@@ -101,3 +101,43 @@ def test_oracle_thread_count_does_not_change_results():
     finally:
         O.set_threads(n0)
     np.testing.assert_array_equal(a, b)
+
+
+NB = load_golden("neighbours")
+
+
+@pytest.mark.parametrize("case", ["regrid_zstar", "regrid_sigma", "regrid_zstar_hmin"])
+def test_oracle_regrid_remap_matches_reference_bitwise(case):
+    rec = NB[case]
+    h_new, (T1, S1) = O.regrid_remap(str(rec["rule"]), rec["H"], rec["eta"], rec["h_src"], rec["active"],
+                                     [rec["T"], rec["S"]], rec["coord"], O.PPM_H4, float(rec["h_min"]))
+    np.testing.assert_array_equal(h_new, rec["h_new"])
+    np.testing.assert_array_equal(T1, rec["T1"])
+    np.testing.assert_array_equal(S1, rec["S1"])
+
+
+def test_oracle_zstar_regrid_refuses_a_wet_column_without_depth():
+    rec = NB["regrid_zstar_bad"]
+    with pytest.raises(ValueError, match="z\\* needs H > 0"):
+        O.regrid_remap("zstar", rec["H"], rec["eta"], rec["h_src"], rec["active"], [rec["T"]], rec["coord"],
+                       O.PPM_H4, float(rec["h_min"]))
+
+
+@pytest.mark.parametrize("case", ["diffuse_closed", "diffuse_per_x", "diffuse_per_xy"])
+def test_oracle_diffusion_matches_reference_bitwise(case):
+    rec = NB[case]
+    out = O.diffuse_ale(rec["T"], rec["Tw"], rec["h"], rec["act"], rec["cx"], rec["cy"], rec["okx"], rec["oky"],
+                        rec["V"], float(rec["kh"]), float(rec["dt"]), O.Periodic(case_periodic(rec)))
+    np.testing.assert_array_equal(out, rec["out"])
+
+
+@pytest.mark.parametrize("case", ["faces_ppm_h4", "faces_plm", "faces_wgiven"])
+def test_oracle_velocity_remap_matches_reference_bitwise(case):
+    rec = NB[case]
+    out = O.remap_faces(rec["vel"], rec["hf_src"], rec["hf_tgt"], int(rec["scheme"]), rec.get("w_tgt"))
+    np.testing.assert_array_equal(out, rec["out"])
+
+
+def test_oracle_face_fractions_match_reference_bitwise():
+    rec = NB["fractions"]
+    np.testing.assert_array_equal(O.face_fractions(rec["hf"]), rec["w"])
