@@ -20,6 +20,9 @@ kernels with the reference's call signatures:
   ``TracerAdvection.diffuse_h`` (``core/components/tracers.py:421-447``).
 * ``face_fractions`` / ``remap_faces`` — ``core/vertical/ale.py:883-902`` and
   ``ALECoordinate.remap_faces`` (``vertical_coordinate.py:142-153``).
+* The producers of the step's inputs (``core/vertical/ale.py``): ``face_transport_thickness`` (:177-231),
+  ``transport_velocity`` (:789-825), ``ppm_edges_x`` / ``ppm_transport_x`` (:582-764), ``limit_outflow`` with
+  ``_give_back`` (:300-441) and ``lagrangian_thickness`` (:278-294).
 
 Parity of this restatement with the reference is pinned by ``tests/test_oracle_golden.py`` against the vectors in
 ``tests/golden/`` that ``tests/golden/make_golden.py`` generated by running the reference itself.
@@ -66,6 +69,17 @@ def lib() -> ctypes.CDLL:
         L.oracle_regrid.restype = i
         L.oracle_diffuse_ale.argtypes = [_D, _D, _D, _U8, _D, _D, _U8, _U8, _D, d, d, i, i, i, _D]
         L.oracle_face_fractions.argtypes = [_D, i, i, i, _D]
+        L.oracle_ftt.argtypes = [_D, _D, _U8, i, i, i, i, _D, _D]
+        L.oracle_transport_velocity.argtypes = [_D, _D, _U8, _D, _D, _D, d, d, i, i, i, _D, _D]
+        L.oracle_ppm_edges.argtypes = [_D, _U8, d, i, i, i, _D, _D]
+        L.oracle_ppm_transport.argtypes = [_D, _D, _D, _D, _D, _D, _D, _D, _U8, d, _D, i, i, i, i, _D]
+        L.oracle_ppm_transport.restype = i
+        L.oracle_outflow_exceeds.argtypes = [_D, _D, _D, _D, d, _U8, d, i, i, i]
+        L.oracle_outflow_exceeds.restype = i
+        L.oracle_limit_outflow.argtypes = [_D, _D, _D, _D, d, _U8, d, i, i, i, i, i, i, ctypes.POINTER(i)]
+        L.oracle_limit_outflow.restype = i
+        L.oracle_lagrangian_thickness.argtypes = [_D, _D, d, _D, d, i, i, i, _D]
+        L.oracle_lagrangian_thickness.restype = ctypes.c_longlong
         L.oracle_num_threads.restype = i
         L.oracle_set_threads.argtypes = [i]
         _LIB = L
@@ -452,3 +466,87 @@ def remap_faces(vel, hf_src, hf_tgt, scheme: int, w_tgt=None):
     S = np.where(wet, tot, 1.0)[None]
     w_tgt = face_fractions(hf_tgt) if w_tgt is None else _f64(w_tgt)
     return remap_columns(face_fractions(hf_src) * S, vel, w_tgt * S, scheme, wet)
+
+
+# ---------------------------------------------------------------------------------------------------- producers
+H_PPM_MIN = 2e-10                      # core/vertical/ale.py:297
+
+
+def face_transport_thickness(h, H, active, clip: bool):
+    """``_ftt_kernel`` (ale.py:177-210): (q_e, q_w) on the u-faces."""
+    h = _f64(h)
+    n, ny, nx = h.shape
+    q_e, q_w = np.empty((n, ny, nx + 1)), np.empty((n, ny, nx + 1))
+    lib().oracle_ftt(_p(h), _p(_f64(H)), _pu8(_u8(active)), int(bool(clip)), n, ny, nx, _p(q_e), _p(q_w))
+    return q_e, q_w
+
+
+def transport_velocity(u_new, u_old, last_wet, w, L, D, theta: float, theta_bc: float | None = None):
+    """``_transport_velocity_kernel`` (ale.py:789-808): (u^theta, Q_bt)."""
+    u_new = _f64(u_new)
+    n, a, b = u_new.shape
+    ut, Qb = np.empty((n, a, b)), np.empty((a, b))
+    tb = theta if theta_bc is None else theta_bc
+    lib().oracle_transport_velocity(_p(u_new), _p(_f64(u_old)), _pu8(_u8(last_wet)), _p(_f64(w)), _p(_f64(L)),
+                                    _p(_f64(D)), float(theta), float(tb), n, a, b, _p(ut), _p(Qb))
+    return ut, Qb
+
+
+def _masked(h, active):
+    return np.ascontiguousarray(np.where(np.asarray(active, bool)[None], np.nan_to_num(np.asarray(h, float)), 0.0))
+
+
+def ppm_edges_x(h, active, h_min: float = H_PPM_MIN):
+    """``_ppm_edges_kernel`` (ale.py:582-626) on where(active, nan_to_num(h), 0)."""
+    hc = _masked(h, active)
+    n, ny, nx = hc.shape
+    h_w, h_e = np.empty_like(hc), np.empty_like(hc)
+    lib().oracle_ppm_edges(_p(hc), _pu8(_u8(active)), float(h_min), n, ny, nx, _p(h_w), _p(h_e))
+    return h_w, h_e
+
+
+def ppm_transport_x(h, ut, L, Q_bt, q_e, q_w, active, dt: float, dx_t, max_iter: int = 20):
+    """``ppm_transport_x`` (ale.py:743-764): PPM layer fluxes with the barotropic correction (u-faces)."""
+    hc = _masked(h, active)
+    n, ny, nx = hc.shape
+    h_w, h_e = ppm_edges_x(hc, active)
+    out = np.empty((n, ny, nx + 1))
+    lib().oracle_ppm_transport(_p(hc), _p(h_w), _p(h_e), _p(_f64(ut)), _p(_f64(L)), _p(_f64(Q_bt)), _p(_f64(q_e)),
+                               _p(_f64(q_w)), _pu8(_u8(active)), float(dt), _p(_f64(dx_t)), int(max_iter), n, ny, nx,
+                               _p(out))
+    return out
+
+
+def limit_outflow(h, Qx, Qy, area, dt: float, active, h_floor: float = H_PPM_MIN, max_pass: int = 50,
+                  periodic=(False, False)):
+    """``limit_outflow`` (ale.py:331-395): (Qx, Qy, n_limited); the inputs themselves when nothing exceeds;
+    RuntimeError where the reference raises."""
+    h, Qx, Qy, area = _f64(h), _f64(Qx), _f64(Qy), _f64(area)
+    n, ny, nx = h.shape
+    act = _u8(active)
+    if not lib().oracle_outflow_exceeds(_p(h), _p(Qx), _p(Qy), _p(area), float(dt), _pu8(act), float(h_floor), n,
+                                        ny, nx):
+        return Qx, Qy, 0
+    Qx, Qy = Qx.copy(), Qy.copy()
+    nl = ctypes.c_int(0)
+    st = lib().oracle_limit_outflow(_p(h), _p(Qx), _p(Qy), _p(area), float(dt), _pu8(act), float(h_floor),
+                                    int(max_pass), int(bool(periodic[0])), int(bool(periodic[1])), n, ny, nx,
+                                    ctypes.byref(nl))
+    if st >= 2:
+        raise RuntimeError("limit_outflow: " + ("barotropic CFL" if st == 2 else "flow out of a dry donor column"))
+    return Qx, Qy, int(nl.value)
+
+
+def lagrangian_thickness(h, divq, dt: float, area, tol: float = 1e-9):
+    """``lagrangian_thickness`` (ale.py:278-294)."""
+    h = _f64(h)
+    n, ny, nx = h.shape
+    out = np.empty_like(h)
+    bad = lib().oracle_lagrangian_thickness(_p(h), _p(_f64(divq)), float(dt), _p(_f64(area)), float(tol), n, ny, nx,
+                                            _p(out))
+    if bad >= 0:
+        k, j, i = np.unravel_index(int(bad), h.shape)
+        v = h[k, j, i] - dt * _f64(divq)[k, j, i] / (area[j, i] if area[j, i] > 0 else 1.0)
+        raise RuntimeError(f"layer {k} of cell (j={j}, i={i}) emptied in the Lagrangian step: h† = {v:.3e} m "
+                           f"(reduce dt)")
+    return out

@@ -878,6 +878,479 @@ void oracle_face_fractions(const double* hf, int n, int a, int b, double* w)
     }
 }
 
+/* ============================================================================================================
+ * Producers of the step's inputs (core/vertical/ale.py): face transport thicknesses, transport velocity, PPM layer
+ * transport with the barotropic correction, the outflow limiter and the Lagrangian thickness.
+ * ========================================================================================================== */
+
+/* ale.py:177-210 `_ftt_kernel`: q_e, q_w (n, ny, nx+1) from h (n, ny, nx), H (ny, nx). */
+void oracle_ftt(const double* h, const double* H, const uint8_t* active, int clip, int n, int ny, int nx,
+                double* q_e, double* q_w)
+{
+    const int nf = nx + 1;
+    const i64 pc = (i64)ny * nx, pf = (i64)ny * nf;
+#pragma omp parallel for
+    for (int j = 0; j < ny; ++j)
+        for (int f = 0; f < nf; ++f) {
+            const int iw = f > 0 ? f - 1 : 0, ie = f < nx ? f : nx - 1;
+            const i64 o = (i64)j * nf + f;
+            if (!(active[j * nx + iw] && active[j * nx + ie])) {
+                for (int k = 0; k < n; ++k) q_e[k * pf + o] = q_w[k * pf + o] = 0.0;
+                continue;
+            }
+            if (clip) {
+                const double Hw0 = H[j * nx + iw], He0 = H[j * nx + ie];
+                const double Hw = Hw0 == Hw0 ? Hw0 : 0.0, He = He0 == He0 ? He0 : 0.0;
+                const double z_bed = pmax(-Hw, -He);
+                double cw = 0.0, ce = 0.0;
+                for (int k = 0; k < n; ++k) {
+                    const double a = h[k * pc + j * nx + iw], b = h[k * pc + j * nx + ie];
+                    const double hw = a == a ? a : 0.0, he = b == b ? b : 0.0;
+                    cw += hw;
+                    ce += he;
+                    q_e[k * pf + o] = pmin(hw, pmax(0.0, (-Hw + cw) - z_bed));
+                    q_w[k * pf + o] = pmin(he, pmax(0.0, (-He + ce) - z_bed));
+                }
+            } else {
+                for (int k = 0; k < n; ++k) {
+                    const double a = h[k * pc + j * nx + iw], b = h[k * pc + j * nx + ie];
+                    q_e[k * pf + o] = a == a ? a : 0.0;
+                    q_w[k * pf + o] = b == b ? b : 0.0;
+                }
+            }
+        }
+}
+
+/* ale.py:789-808 `_transport_velocity_kernel` on (n, a, b) face arrays. */
+void oracle_transport_velocity(const double* u_new, const double* u_old, const uint8_t* last_wet, const double* w,
+                               const double* L, const double* D, double theta, double theta_bc, int n, int a, int b,
+                               double* ut, double* Qb)
+{
+    const i64 plane = (i64)a * b;
+#pragma omp parallel for
+    for (i64 c = 0; c < plane; ++c) {
+        double m1 = 0.0, m0 = 0.0;
+        for (int k = 0; k < n; ++k) {
+            const double un = last_wet[c] ? u_old[k * plane + c] : 0.0;
+            m1 += w[k * plane + c] * u_new[k * plane + c];
+            m0 += w[k * plane + c] * un;
+        }
+        const double d = (theta - theta_bc) * (m1 - m0);
+        double s = 0.0;
+        for (int k = 0; k < n; ++k) {
+            const double un = last_wet[c] ? u_old[k * plane + c] : 0.0;
+            const double x = theta_bc * u_new[k * plane + c] + (1 - theta_bc) * un + d;
+            ut[k * plane + c] = x;
+            s += w[k * plane + c] * x;
+        }
+        Qb[c] = L[c] * D[c] * s;
+    }
+}
+
+/* ale.py:582-626 `_ppm_edges_kernel` (h already masked: where(active, nan_to_num(h), 0)). */
+void oracle_ppm_edges(const double* h, const uint8_t* active, double h_min, int n, int ny, int nx, double* h_w,
+                      double* h_e)
+{
+    const i64 pc = (i64)ny * nx;
+#pragma omp parallel for
+    for (int j = 0; j < ny; ++j) {
+        double* slp = (double*)malloc((size_t)nx * sizeof(double));
+        for (int k = 0; k < n; ++k) {
+            const double* hr = h + k * pc + (i64)j * nx;
+            const uint8_t* ar = active + (i64)j * nx;
+            for (int i = 0; i < nx; ++i) {
+                const double m = ar[i] ? 1.0 : 0.0;
+                const double mw = i > 0 ? (ar[i - 1] ? 1.0 : 0.0) : 0.0;
+                const double me = i < nx - 1 ? (ar[i + 1] ? 1.0 : 0.0) : 0.0;
+                const double hc = hr[i];
+                const double hm1 = i > 0 ? mw * hr[i - 1] + (1.0 - mw) * hc : hc;
+                const double hp1 = i < nx - 1 ? me * hr[i + 1] + (1.0 - me) * hc : hc;
+                double sl = 0.5 * (hp1 - hm1);
+                const double dmx = pmax(pmax(hp1, hm1), hc) - hc;
+                const double dmn = hc - pmin(pmin(hp1, hm1), hc);
+                const double a = pmin(fabs(sl), 2.0 * pmin(dmx, dmn));
+                sl = sl > 0.0 ? a : (sl < 0.0 ? -a : 0.0);
+                slp[i] = mw * me * m > 0.0 ? sl : 0.0;
+            }
+            for (int i = 0; i < nx; ++i) {
+                const double mw = i > 0 ? (ar[i - 1] ? 1.0 : 0.0) : 0.0;
+                const double me = i < nx - 1 ? (ar[i + 1] ? 1.0 : 0.0) : 0.0;
+                const double hc = hr[i];
+                const double hm1 = i > 0 ? mw * hr[i - 1] + (1.0 - mw) * hc : hc;
+                const double hp1 = i < nx - 1 ? me * hr[i + 1] + (1.0 - me) * hc : hc;
+                const double sw = i > 0 ? slp[i - 1] : 0.0, se = i < nx - 1 ? slp[i + 1] : 0.0;
+                const double hw = 0.5 * (hm1 + hc) + (sw - slp[i]) / 6.0;
+                const double he = 0.5 * (hp1 + hc) + (slp[i] - se) / 6.0;
+                const double curv = 3.0 * ((hw + he) - 2.0 * hc);
+                const double dh = he - hw;
+                const int inside = curv > 0.0 && fabs(dh) < curv;
+                const i64 o = k * pc + (i64)j * nx + i;
+                if (inside && hc <= h_min) {
+                    h_w[o] = hc;
+                    h_e[o] = hc;
+                    continue;
+                }
+                double sc = 1.0;
+                if (inside) {
+                    const double num = 12.0 * curv * (hc - h_min);
+                    const double den = curv * curv + 3.0 * dh * dh;
+                    if (num < den) sc = num / den;
+                }
+                h_w[o] = hc + sc * (hw - hc);
+                h_e[o] = hc + sc * (he - hc);
+            }
+        }
+        free(slp);
+    }
+}
+
+/* ale.py:629-647 `_face_flux`: (F, dF/du) of layer k at u-face (j, f). */
+static void face_flux(int k, int j, int f, double u, const double* h, const double* h_w, const double* h_e,
+                      const double* dx, const double* q_e, const double* q_w, double L_f, double dt, int ny, int nx,
+                      double* F, double* dF)
+{
+    const int iw = f > 0 ? f - 1 : 0, ie = f < nx ? f : nx - 1;
+    const i64 pc = (i64)ny * nx, pf = (i64)ny * (nx + 1);
+    double c, hu, ww, ee, curv3, dh, edge, q;
+    if (u >= 0.0) {
+        c = pmin(fabs(u) * dt / dx[j * nx + iw], 1.0);
+        const i64 o = k * pc + (i64)j * nx + iw;
+        hu = h[o]; ww = h_w[o]; ee = h_e[o];
+        curv3 = (ww + ee) - 2.0 * hu; dh = ww - ee; edge = ee; q = q_e[k * pf + (i64)j * (nx + 1) + f];
+    } else {
+        c = pmin(fabs(u) * dt / dx[j * nx + ie], 1.0);
+        const i64 o = k * pc + (i64)j * nx + ie;
+        hu = h[o]; ww = h_w[o]; ee = h_e[o];
+        curv3 = (ww + ee) - 2.0 * hu; dh = ee - ww; edge = ww; q = q_w[k * pf + (i64)j * (nx + 1) + f];
+    }
+    double mean = edge + c * (0.5 * dh + curv3 * (c - 1.5));
+    double marg = edge + c * (dh + 3.0 * curv3 * (c - 1.0));
+    if (q < hu) {
+        mean = pmin(mean, q);
+        marg = pmin(marg, q);
+    }
+    *F = L_f * u * pmax(mean, 0.0);
+    *dF = L_f * pmax(marg, 0.0);
+}
+
+/* ale.py:650-740 `_ppm_transport_kernel`; h masked, h_w / h_e its edges; out (n, ny, nx+1).  Returns the number of
+ * Newton iterations taken. */
+int oracle_ppm_transport(const double* h, const double* h_w, const double* h_e, const double* ut, const double* L,
+                         const double* Q_bt, const double* q_e, const double* q_w, const uint8_t* active, double dt,
+                         const double* dx, int max_iter, int n, int ny, int nx, double* out)
+{
+    const int nf = nx + 1;
+    const i64 pf = (i64)ny * nf;
+    double* du = (double*)calloc((size_t)pf, sizeof(double));
+    double* lo = (double*)malloc((size_t)pf * sizeof(double));
+    double* hi = (double*)malloc((size_t)pf * sizeof(double));
+    double* err = (double*)malloc((size_t)pf * sizeof(double));
+    double* dsum = (double*)malloc((size_t)pf * sizeof(double));
+#pragma omp parallel for
+    for (int j = 0; j < ny; ++j)
+        for (int f = 0; f < nf; ++f) {
+            const i64 o = (i64)j * nf + f;
+            const int iw = f > 0 ? f - 1 : 0, ie = f < nx ? f : nx - 1;
+            const double limw = 0.5 * dx[j * nx + iw] / dt, lime = 0.5 * dx[j * nx + ie] / dt;
+            double mnw = INFINITY, mxe = -INFINITY;
+            for (int k = 0; k < n; ++k) {
+                mnw = pmin(mnw, limw - ut[k * pf + o]);
+                mxe = pmax(mxe, -(lime + ut[k * pf + o]));
+            }
+            hi[o] = pmax(pmin(limw, mnw), 0.0);
+            lo[o] = pmin(pmax(-lime, mxe), 0.0);
+            double s = 0.0, sd = 0.0;
+            if (active[j * nx + iw] && active[j * nx + ie])
+                for (int k = 0; k < n; ++k) {
+                    double F, dF;
+                    face_flux(k, j, f, ut[k * pf + o], h, h_w, h_e, dx, q_e, q_w, L[o], dt, ny, nx, &F, &dF);
+                    s += F;
+                    sd += dF;
+                }
+            err[o] = s - Q_bt[o];
+            dsum[o] = sd;
+        }
+    int it = 0;
+    for (; it < max_iter;) {
+#pragma omp parallel for
+        for (int j = 0; j < ny; ++j)
+            for (int f = 0; f < nf; ++f) {
+                const i64 o = (i64)j * nf + f;
+                const double e = err[o], d = du[o];
+                if (e > 0.0) hi[o] = d;
+                if (e < 0.0) lo[o] = d;
+                const double step = dsum[o] > 0.0 ? -e / dsum[o] : 0.0;
+                double nw = d + step;
+                if (step > 0.0 && nw >= hi[o]) nw = 0.5 * (d + hi[o]);
+                if (step < 0.0 && nw <= lo[o]) nw = 0.5 * (d + lo[o]);
+                du[o] = nw;
+                const int iw = f > 0 ? f - 1 : 0, ie = f < nx ? f : nx - 1;
+                double s = 0.0, sd = 0.0;
+                if (active[j * nx + iw] && active[j * nx + ie])
+                    for (int k = 0; k < n; ++k) {
+                        double F, dF;
+                        face_flux(k, j, f, ut[k * pf + o] + nw, h, h_w, h_e, dx, q_e, q_w, L[o], dt, ny, nx, &F, &dF);
+                        s += F;
+                        sd += dF;
+                    }
+                err[o] = s - Q_bt[o];
+                dsum[o] = sd;
+            }
+        ++it;
+        int done = 1;
+        for (i64 o = 0; o < pf; ++o)
+            if (fabs(err[o]) > 1e-12 * pmax(fabs(Q_bt[o]), 1.0)) done = 0;
+        if (done) break;
+    }
+#pragma omp parallel for
+    for (int j = 0; j < ny; ++j) {
+        double* Fk = (double*)malloc((size_t)n * sizeof(double));
+        for (int f = 0; f < nf; ++f) {
+            const i64 o = (i64)j * nf + f;
+            const int iw = f > 0 ? f - 1 : 0, ie = f < nx ? f : nx - 1;
+            if (!(active[j * nx + iw] && active[j * nx + ie])) {
+                for (int k = 0; k < n; ++k) out[k * pf + o] = 0.0;
+                continue;
+            }
+            double s = 0.0;
+            for (int k = 0; k < n; ++k) {
+                double F, dF;
+                face_flux(k, j, f, ut[k * pf + o] + du[o], h, h_w, h_e, dx, q_e, q_w, L[o], dt, ny, nx, &F, &dF);
+                Fk[k] = F;
+                s += Fk[k];
+            }
+            const double R = Q_bt[o] - s;
+            double te = 0.0, tw = 0.0;
+            for (int k = 0; k < n; ++k) {
+                te += q_e[k * pf + o];
+                tw += q_w[k * pf + o];
+            }
+            int use_e = R >= 0.0;
+            double tot = use_e ? te : tw;
+            if (tot <= 0.0) {
+                use_e = !use_e;
+                tot = use_e ? te : tw;
+            }
+            const double den = tot > 0.0 ? tot : 1.0;
+            for (int k = 0; k < n; ++k)
+                out[k * pf + o] = Fk[k] + R * (use_e ? q_e[k * pf + o] : q_w[k * pf + o]) / den;
+        }
+        free(Fk);
+    }
+    free(du); free(lo); free(hi); free(err); free(dsum);
+    return it;
+}
+
+/* Outflow of a cell-layer through its four faces, ale.py:300-303. */
+static inline double outflow_at(const double* Qx, const double* Qy, int k, int j, int i, int ny, int nx)
+{
+    const i64 ox = (i64)k * ny * (nx + 1) + (i64)j * (nx + 1) + i, oy = (i64)k * (ny + 1) * nx + (i64)j * nx + i;
+    return pmax(Qx[ox + 1], 0.0) - pmin(Qx[ox], 0.0) + pmax(Qy[oy + nx], 0.0) - pmin(Qy[oy], 0.0);
+}
+
+/* ale.py:306-321 `_exceeds_kernel`. */
+int oracle_outflow_exceeds(const double* h, const double* Qx, const double* Qy, const double* area, double dt,
+                           const uint8_t* active, double h_floor, int n, int ny, int nx)
+{
+    int hit = 0;
+    for (int k = 0; k < n && !hit; ++k)
+        for (int j = 0; j < ny && !hit; ++j)
+            for (int i = 0; i < nx; ++i) {
+                if (!active[j * nx + i]) continue;
+                const double o = outflow_at(Qx, Qy, k, j, i, ny, nx);
+                if (o > pmax(h[(i64)k * ny * nx + (i64)j * nx + i] - h_floor, 0.0) * area[j * nx + i] / dt) {
+                    hit = 1;
+                    break;
+                }
+            }
+    return hit;
+}
+
+static inline double sgn(double x) { return x > 0.0 ? 1.0 : (x < 0.0 ? -1.0 : (x == 0.0 ? 0.0 : x)); }
+
+/*
+ * One face column of the give-back (ale.py:398-441 `_give_back`) for face (j, f) of one axis: nq layers of Q with
+ * stride sq, the donor cells' room (lo / hi side) and whole content (full) with stride sc.  lo_ok / hi_ok: the
+ * donor exists (otherwise the edge value, 0).  Returns 1 if the face must carry flow out of a dry donor column.
+ */
+static int give_back_face(double* Q, i64 sq, int nq, double delta, const double* room_lo, const double* room_hi,
+                          const double* full_lo, const double* full_hi, i64 sc, int lo_ok, int hi_ok)
+{
+    const double s = sgn(delta);
+    double tot = 0.0;
+    for (int k = 0; k < nq; ++k) {
+        const double rl = pmax(lo_ok ? room_lo[k * sc] : 0.0, 0.0), rh = pmax(hi_ok ? room_hi[k * sc] : 0.0, 0.0);
+        const double q = Q[k * sq];
+        const int same = sgn(q) == s && q != 0.0 && s != 0.0;
+        tot += same ? (s > 0 ? rl : rh) : 0.0;
+    }
+    const double need = fabs(delta);
+    const double give = need < tot ? need : tot;                    /* np.minimum */
+    const double X = tot > 0 ? give / (tot > 0 ? tot : 1.0) : 0.0;
+    for (int k = 0; k < nq; ++k) {
+        const double rl = pmax(lo_ok ? room_lo[k * sc] : 0.0, 0.0), rh = pmax(hi_ok ? room_hi[k * sc] : 0.0, 0.0);
+        const double q = Q[k * sq];
+        const int same = sgn(q) == s && q != 0.0 && s != 0.0;
+        const double rm = same ? (s > 0 ? rl : rh) : 0.0;
+        Q[k * sq] = q + s * rm * X;
+    }
+    double rest = need - give;
+    double cap = 0.0;
+    for (int k = 0; k < nq; ++k) {
+        const double q = Q[k * sq];
+        const int opp = sgn(q) == -s && s != 0.0;
+        cap += opp ? fabs(q) : 0.0;
+    }
+    const double mrc = rest < cap ? rest : cap;
+    const double frac = cap > 0 ? mrc / (cap > 0 ? cap : 1.0) : 0.0;
+    for (int k = 0; k < nq; ++k) {
+        const double q = Q[k * sq];
+        const int opp = sgn(q) == -s && s != 0.0;
+        Q[k * sq] = q - (opp ? q * frac : 0.0);
+    }
+    rest = rest - mrc;
+    const double rp = rest > 0 ? 1.0 : 0.0;
+    double ftot = 0.0;
+    for (int k = 0; k < nq; ++k) {
+        const double fl = lo_ok ? full_lo[k * sc] : 0.0, fh = hi_ok ? full_hi[k * sc] : 0.0;
+        ftot += (s > 0 ? fl : fh) * rp;
+    }
+    if (rest > 0 && ftot <= 0) return 1;
+    const double Y = ftot > 0 ? rest / (ftot > 0 ? ftot : 1.0) : 0.0;
+    for (int k = 0; k < nq; ++k) {
+        const double fl = lo_ok ? full_lo[k * sc] : 0.0, fh = hi_ok ? full_hi[k * sc] : 0.0;
+        const double fm = (s > 0 ? fl : fh) * rp;
+        Q[k * sq] = Q[k * sq] + s * fm * Y;
+    }
+    return 0;
+}
+
+/*
+ * ale.py:331-395 `limit_outflow` after its fast check found a cell to limit; Qx, Qy are limited in place.
+ * Returns 0 (limited), 1 (accepted with the reference's warning), 2 (raises: barotropic CFL), 3 (raises: a face must
+ * carry flow out of a dry donor column); *n_lim the count of limited cell-layers over the passes.
+ */
+int oracle_limit_outflow(const double* h, double* Qx, double* Qy, const double* area, double dt,
+                         const uint8_t* active, double h_floor, int max_pass, int per_x, int per_y, int n, int ny,
+                         int nx, int* n_lim)
+{
+    const i64 pc = (i64)ny * nx, px = (i64)ny * (nx + 1), py = (i64)(ny + 1) * nx;
+    double* room0 = (double*)malloc((size_t)(n * pc) * sizeof(double));
+    double* room = (double*)malloc((size_t)(n * pc) * sizeof(double));
+    double* r = (double*)malloc((size_t)(n * pc) * sizeof(double));
+    uint8_t* over = (uint8_t*)malloc((size_t)(n * pc));
+    double* Qn = (double*)malloc((size_t)(n * (px > py ? px : py)) * sizeof(double));
+    for (int k = 0; k < n; ++k)
+        for (i64 c = 0; c < pc; ++c) {
+            const double A = active[c] ? area[c] : 0.0;
+            room0[k * pc + c] = pmax(h[k * pc + c] - h_floor, 0.0) * A / dt;
+        }
+    int status = -1, cnt = 0, any = 0;
+    for (int k = 0; k < n; ++k)
+        for (int j = 0; j < ny; ++j)
+            for (int i = 0; i < nx; ++i) {
+                const i64 o = k * pc + (i64)j * nx + i;
+                over[o] = active[j * nx + i] && outflow_at(Qx, Qy, k, j, i, ny, nx) > room0[o];
+            }
+    for (int pass = 0; pass < max_pass && status < 0; ++pass) {
+        for (i64 o = 0; o < n * pc; ++o) cnt += over[o];
+        for (int k = 0; k < n; ++k)
+            for (int j = 0; j < ny; ++j)
+                for (int i = 0; i < nx; ++i) {
+                    const i64 o = k * pc + (i64)j * nx + i;
+                    const double O = outflow_at(Qx, Qy, k, j, i, ny, nx);
+                    r[o] = over[o] ? room0[o] / (O > 0 ? O : 1.0) : 1.0;
+                }
+        for (int ax = 0; ax < 2 && status < 0; ++ax) {
+            /* ax 0: x faces (j, f), f = 0 .. nx; ax 1: y faces (f, i), f = 0 .. ny */
+            const int wrap = ax == 0 ? per_x : per_y;
+            double* Q = ax == 0 ? Qx : Qy;
+            const int na = ax == 0 ? ny : nx, nc = ax == 0 ? nx : ny;  /* columns across, cells along the axis */
+            const i64 pq = ax == 0 ? px : py;
+            double* delta = (double*)malloc((size_t)(na * (nc + 1)) * sizeof(double));
+            for (int a = 0; a < na; ++a)
+                for (int f = 0; f <= nc; ++f) {
+                    double d = 0.0;
+                    for (int k = 0; k < n; ++k) {
+                        const i64 oq = ax == 0 ? k * pq + (i64)a * (nx + 1) + f : k * pq + (i64)f * nx + a;
+                        const int lo_c = f > 0 ? f - 1 : (wrap ? nc - 1 : -1), hi_c = f < nc ? f : (wrap ? 0 : -1);
+                        const double rlo = lo_c < 0 ? 1.0 : r[k * pc + (ax == 0 ? (i64)a * nx + lo_c : (i64)lo_c * nx + a)];
+                        const double rhi = hi_c < 0 ? 1.0 : r[k * pc + (ax == 0 ? (i64)a * nx + hi_c : (i64)hi_c * nx + a)];
+                        const double q = Q[oq];
+                        const double nw = q > 0 ? q * rlo : (q < 0 ? q * rhi : q);
+                        d += q - nw;
+                        Qn[oq] = nw;
+                    }
+                    delta[a * (nc + 1) + f] = d;
+                }
+            for (i64 o = 0; o < n * pq; ++o) Q[o] = Qn[o];
+            for (int k = 0; k < n; ++k)
+                for (int j = 0; j < ny; ++j)
+                    for (int i = 0; i < nx; ++i) {
+                        const i64 o = k * pc + (i64)j * nx + i;
+                        room[o] = room0[o] - outflow_at(Qx, Qy, k, j, i, ny, nx);
+                    }
+            for (int a = 0; a < na && status < 0; ++a)
+                for (int f = 0; f <= nc; ++f) {
+                    const int lo_c = f > 0 ? f - 1 : (wrap ? nc - 1 : -1), hi_c = f < nc ? f : (wrap ? 0 : -1);
+                    const i64 clo = lo_c < 0 ? 0 : (ax == 0 ? (i64)a * nx + lo_c : (i64)lo_c * nx + a);
+                    const i64 chi = hi_c < 0 ? 0 : (ax == 0 ? (i64)a * nx + hi_c : (i64)hi_c * nx + a);
+                    const i64 oq = ax == 0 ? (i64)a * (nx + 1) + f : (i64)f * nx + a;
+                    if (give_back_face(Q + oq, pq, n, delta[a * (nc + 1) + f], room + clo, room + chi, room0 + clo,
+                                       room0 + chi, pc, lo_c >= 0, hi_c >= 0)) {
+                        status = 3;
+                        break;
+                    }
+                }
+            free(delta);
+        }
+        if (status >= 0) break;
+        any = 0;
+        for (int k = 0; k < n; ++k)
+            for (int j = 0; j < ny; ++j)
+                for (int i = 0; i < nx; ++i) {
+                    const i64 o = k * pc + (i64)j * nx + i;
+                    over[o] = active[j * nx + i] && outflow_at(Qx, Qy, k, j, i, ny, nx) > room0[o] * (1.0 + 1e-12);
+                    any |= over[o];
+                }
+        if (!any) status = 0;
+    }
+    if (status < 0) {
+        double mn = INFINITY;
+        for (int k = 0; k < n; ++k)
+            for (int j = 0; j < ny; ++j)
+                for (int i = 0; i < nx; ++i) {
+                    const i64 c = (i64)j * nx + i;
+                    const i64 ox = (i64)k * px + (i64)j * (nx + 1) + i, oy = (i64)k * py + (i64)j * nx + i;
+                    const double div = Qx[ox + 1] - Qx[ox] + Qy[oy + nx] - Qy[oy];
+                    const double A = active[c] ? area[c] : 0.0;
+                    const double hd = active[c] ? h[k * pc + c] - dt * div / (A > 0 ? A : 1.0) : 0.0;
+                    mn = hd < mn ? hd : mn;
+                }
+        status = mn >= -h_floor ? 1 : 2;
+    }
+    *n_lim = cnt;
+    free(room0); free(room); free(r); free(over); free(Qn);
+    return status;
+}
+
+/* ale.py:278-294 `lagrangian_thickness`: out = max(h - dt divq / A, 0); returns the flat index of the first
+ * cell-layer below -tol (the reference raises there), or -1. */
+long long oracle_lagrangian_thickness(const double* h, const double* divq, double dt, const double* area, double tol,
+                                      int n, int ny, int nx, double* out)
+{
+    const i64 pc = (i64)ny * nx;
+    long long bad = -1;
+    for (int k = 0; k < n; ++k)
+        for (i64 c = 0; c < pc; ++c) {
+            const i64 o = k * pc + c;
+            const double v = h[o] - dt * divq[o] / (area[c] > 0 ? area[c] : 1.0);
+            if (v < -tol && bad < 0) bad = o;
+            out[o] = (v >= 0.0 || isnan(v)) ? v : 0.0;                /* np.maximum(v, 0.0) */
+        }
+    return bad;
+}
+
 /* Threads available to the OpenMP loops (for reporting the CPU baseline's core count). */
 #ifdef _OPENMP
 #include <omp.h>

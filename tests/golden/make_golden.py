@@ -42,6 +42,7 @@ from core.model import threads                         # noqa: E402
 from core.model.periodic import Periodic               # noqa: E402
 from core.vertical import remap as rm                  # noqa: E402
 from core.vertical import regrid as rg                 # noqa: E402
+from core.vertical import ale                          # noqa: E402
 from core.vertical.ale import face_fractions           # noqa: E402
 from core.components.vertical_coordinate import ALECoordinate   # noqa: E402
 
@@ -369,6 +370,94 @@ def neighbour_cases():
     return out
 
 
+def _producer_state(rng, n, ny, nx, land=0.12):
+    """A basin of layers for the producer cases: depth, active mask, layer thicknesses (bed first, z*-like with a
+    shallow shelf), face lengths, metrics and a velocity field."""
+    H = rng.uniform(30.0, 300.0, (ny, nx))
+    H[:, : nx // 4] = rng.uniform(5.0, 20.0, (ny, nx // 4))            # shelf: thin / vanished bed layers
+    active = rng.random((ny, nx)) > land
+    h = np.empty((n, ny, nx))
+    for k in range(n):
+        h[k] = H / n * rng.uniform(0.6, 1.4, (ny, nx))
+    h[0, :, : nx // 4] = 0.0                                           # vanished bed layer on the shelf
+    h[:, ~active] = np.nan
+    dx = rng.uniform(900.0, 1100.0, (ny, nx))
+    Lu = rng.uniform(900.0, 1100.0, (ny, nx + 1))
+    return H, active, h, dx, Lu
+
+
+def producer_cases():
+    """The producers of the step's inputs: face transport thicknesses, transport velocity, PPM layer transport
+    with its barotropic correction, the outflow limiter (fast and limiting paths) and the Lagrangian thickness."""
+    out = {}
+    rng = np.random.default_rng(33)
+    n, ny, nx = 6, 9, 14
+    H, active, h, dx, Lu = _producer_state(rng, n, ny, nx)
+    for clip in (True, False):
+        q_e, q_w = ale.face_transport_thickness(h, H, active, clip)
+        out["ftt_" + ("clip" if clip else "noclip")] = dict(h=h, H=H, active=active, clip=clip, q_e=q_e, q_w=q_w)
+    q_e, q_w = ale.face_transport_thickness(h, H, active, True)
+    # transport velocity (fractions of the face layers, half the faces wet in the last step)
+    u_new = rng.normal(0.0, 0.4, (n, ny, nx + 1))
+    u_old = rng.normal(0.0, 0.4, (n, ny, nx + 1))
+    last_wet = rng.random((ny, nx + 1)) > 0.2
+    w = face_fractions(0.5 * (q_e + q_w))
+    D = rng.uniform(5.0, 300.0, (ny, nx + 1))
+    ut, Qb = ale.transport_velocity(u_new, u_old, last_wet, w, Lu, D, 0.6, 0.5)
+    out["tvel"] = dict(u_new=u_new, u_old=u_old, last_wet=last_wet, w=w, L=Lu, D=D, theta=0.6, theta_bc=0.5, ut=ut,
+                       Qb=Qb)
+    # PPM edges and layer transport (Courant up to ~0.4, a barotropic target that needs correcting)
+    dt = 600.0
+    hc = np.where(active[None], np.nan_to_num(h), 0.0)
+    h_w, h_e = ale.ppm_edges_x(hc, active)
+    out["ppm_edges"] = dict(h=h, active=active, h_w=h_w, h_e=h_e)
+    Q_bt = Qb * rng.uniform(0.8, 1.2, Qb.shape)
+    for it in (20, 1):
+        Qx = ale.ppm_transport_x(h, ut, Lu, Q_bt, q_e, q_w, active, dt, dx, it)
+        out[f"ppm_transport_it{it}"] = dict(h=h, ut=ut, L=Lu, Q_bt=Q_bt, q_e=q_e, q_w=q_w, active=active, dt=dt,
+                                            dx=dx, max_iter=it, Qx=Qx)
+    # outflow limiter: a calm case (nothing to limit) and one with strong outflow from thin layers
+    area = dx * rng.uniform(900.0, 1100.0, (ny, nx))
+    hz = np.where(active[None], np.nan_to_num(h), 0.0)
+    for name, amp in (("calm", 0.02), ("limited", 0.2), ("heavy", 0.3), ("strong", 3.0)):
+        Qx = rng.normal(0.0, 1.0, (n, ny, nx + 1)) * amp * 1e3 * np.concatenate([hz[..., :1], hz], axis=-1)
+        Qy = rng.normal(0.0, 1.0, (n, ny + 1, nx)) * amp * 1e3 * np.concatenate([hz[:, :1], hz], axis=1)
+        fx = np.zeros((ny, nx + 1), bool)
+        fx[:, 1:-1] = active[:, 1:] & active[:, :-1]
+        fy = np.zeros((ny + 1, nx), bool)
+        fy[1:-1] = active[1:] & active[:-1]
+        Qx *= fx
+        Qy *= fy
+        for per in ((False, False), (True, False)):
+            Qxp, Qyp = Qx.copy(), Qy.copy()
+            if per[0]:                                         # flow through the wrap face (cells nx-1 and 0)
+                wrapf = active[:, 0] & active[:, -1]
+                wq = rng.normal(0.0, 1.0, (n, ny)) * amp * 1e3 * np.minimum(hz[..., 0], hz[..., -1]) * wrapf
+                Qxp[..., 0] = Qxp[..., -1] = wq
+            try:
+                Lx, Ly, nl = ale.limit_outflow(hz, Qxp, Qyp, area, dt, active, periodic=per)
+                status = "ok"
+            except RuntimeError:
+                Lx, Ly, nl, status = Qxp, Qyp, -1, "raised"
+            out[f"limit_{name}" + ("_perx" if per[0] else "")] = dict(
+                h=hz, Qx=Qxp, Qy=Qyp, area=area, dt=dt, active=active, periodic=np.array(per), Qx_out=Lx,
+                Qy_out=Ly, n_limited=nl, status=status)
+    # Lagrangian thickness of the limited fluxes (where the limiter finished), and a step too long for the outflow
+    Aw = np.where(active, area, 0.0)
+    for name in ("limit_calm", "limit_limited", "limit_strong"):
+        rec = out[name]
+        div = rec["Qx_out"][..., 1:] - rec["Qx_out"][..., :-1] + rec["Qy_out"][:, 1:] - rec["Qy_out"][:, :-1]
+        try:
+            out["lagrangian_" + name[6:]] = dict(h=hz, divq=div, dt=dt, area=Aw,
+                                                  h_dag=ale.lagrangian_thickness(hz, div, dt, Aw), raises=False)
+        except RuntimeError:
+            out["lagrangian_" + name[6:]] = dict(h=hz, divq=div, dt=dt, area=Aw, raises=True)
+    for k, v in out.items():
+        if k.startswith(("limit", "lagr")):
+            print(k, v.get("status"), v.get("n_limited"), v.get("raises"))
+    return out
+
+
 def save(name, cases):
     flat = {}
     for case, rec in cases.items():
@@ -381,8 +470,8 @@ def save(name, cases):
 
 if __name__ == "__main__":
     threads.set_threads(1)
-    which = sys.argv[2:] or ["fct", "rk3", "kernels", "remap", "neighbours"]
+    which = sys.argv[2:] or ["fct", "rk3", "kernels", "remap", "neighbours", "producers"]
     makers = {"fct": fct_cases, "rk3": rk3_cases, "kernels": kernel_cases, "remap": remap_cases,
-              "neighbours": neighbour_cases}
+              "neighbours": neighbour_cases, "producers": producer_cases}
     for name in which:
         save(name, makers[name]())

@@ -141,3 +141,63 @@ def test_oracle_velocity_remap_matches_reference_bitwise(case):
 def test_oracle_face_fractions_match_reference_bitwise():
     rec = NB["fractions"]
     np.testing.assert_array_equal(O.face_fractions(rec["hf"]), rec["w"])
+
+
+PR = load_golden("producers")
+
+
+@pytest.mark.parametrize("case", ["ftt_clip", "ftt_noclip"])
+def test_oracle_face_transport_thickness_matches_reference_bitwise(case):
+    rec = PR[case]
+    q_e, q_w = O.face_transport_thickness(rec["h"], rec["H"], rec["active"], bool(rec["clip"]))
+    np.testing.assert_array_equal(q_e, rec["q_e"])
+    np.testing.assert_array_equal(q_w, rec["q_w"])
+
+
+def test_oracle_transport_velocity_matches_reference_bitwise():
+    rec = PR["tvel"]
+    ut, Qb = O.transport_velocity(rec["u_new"], rec["u_old"], rec["last_wet"], rec["w"], rec["L"], rec["D"],
+                                  float(rec["theta"]), float(rec["theta_bc"]))
+    np.testing.assert_array_equal(ut, rec["ut"])
+    np.testing.assert_array_equal(Qb, rec["Qb"])
+
+
+def test_oracle_ppm_edges_match_reference_bitwise():
+    rec = PR["ppm_edges"]
+    h_w, h_e = O.ppm_edges_x(rec["h"], rec["active"])
+    np.testing.assert_array_equal(h_w, rec["h_w"])
+    np.testing.assert_array_equal(h_e, rec["h_e"])
+
+
+@pytest.mark.parametrize("case", ["ppm_transport_it20", "ppm_transport_it1"])
+def test_oracle_ppm_transport_matches_reference_bitwise(case):
+    rec = PR[case]
+    out = O.ppm_transport_x(rec["h"], rec["ut"], rec["L"], rec["Q_bt"], rec["q_e"], rec["q_w"], rec["active"],
+                            float(rec["dt"]), rec["dx"], int(rec["max_iter"]))
+    np.testing.assert_array_equal(out, rec["Qx"])
+
+
+@pytest.mark.parametrize("case", sorted(c for c in PR if c.startswith("limit_")))
+def test_oracle_limit_outflow_matches_reference_bitwise(case):
+    rec = PR[case]
+    args = (rec["h"], rec["Qx"], rec["Qy"], rec["area"], float(rec["dt"]), rec["active"])
+    per = tuple(bool(x) for x in rec["periodic"])
+    if str(rec["status"]) == "raised":
+        with pytest.raises(RuntimeError):
+            O.limit_outflow(*args, periodic=per)
+        return
+    Qx, Qy, nl = O.limit_outflow(*args, periodic=per)
+    assert nl == int(rec["n_limited"])
+    np.testing.assert_array_equal(Qx, rec["Qx_out"])
+    np.testing.assert_array_equal(Qy, rec["Qy_out"])
+
+
+@pytest.mark.parametrize("case", ["lagrangian_calm", "lagrangian_limited", "lagrangian_strong"])
+def test_oracle_lagrangian_thickness_matches_reference_bitwise(case):
+    rec = PR[case]
+    args = (rec["h"], rec["divq"], float(rec["dt"]), rec["area"])
+    if bool(rec["raises"]):
+        with pytest.raises(RuntimeError, match="emptied in the Lagrangian step"):
+            O.lagrangian_thickness(*args)
+        return
+    np.testing.assert_array_equal(O.lagrangian_thickness(*args), rec["h_dag"])
