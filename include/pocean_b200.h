@@ -30,6 +30,7 @@ extern "C" {
 #define POCEAN_EWORKSPACE 2   /* workspace missing, misaligned or too small */
 #define POCEAN_ECUDA 3        /* a CUDA launch or API call failed */
 #define POCEAN_EDEVICE 4      /* the current device is not an sm_100 part */
+#define POCEAN_ESTEP 5        /* the step cannot proceed where the reference raises RuntimeError (CFL, dry donor) */
 
 /* Flags of the advection entry points (bitwise OR). */
 #define POCEAN_OPEN_W 0x1u    /* open western edge (ob.open contains "west"), tracers.py:163 */
@@ -169,6 +170,52 @@ int pocean_remap_faces_f64(const double* vel, const double* hf_src, const double
 int pocean_diffuse_ale_f64(const double* T, const double* Tw, const double* h, const uint8_t* act, const double* cx,
                            const double* cy, const uint8_t* okx, const uint8_t* oky, const double* V, int nt, int nz,
                            int ny, int nx, unsigned flags, double kh, double dt, double* out, void* stream);
+
+/*
+ * The producers of the step's inputs (core/vertical/ale.py), for u-faces (nz, ny, nx+1) of cells (nz, ny, nx); the
+ * v-faces are the same calls on arrays with the horizontal axes swapped, as the reference makes them.
+ */
+
+/* ale.py:177-231 face_transport_thickness / _ftt_kernel: q_e (from the west cell), q_w (from the east cell);
+ * clip != 0: only the part above the shallower bed (z*, hybrid).  NaN thickness or depth reads as 0. */
+int pocean_face_transport_thickness_f64(const double* h, const double* H, const uint8_t* active, int nz, int ny,
+                                        int nx, int clip, double* q_e, double* q_w, void* stream);
+
+/* ale.py:767-825 transport_velocity / _transport_velocity_kernel on face arrays (nz, na, nb): ut (nz, na, nb) and
+ * Qb (na, nb).  last_wet one byte per face column; w the layer fractions. */
+int pocean_transport_velocity_f64(const double* u_new, const double* u_old, const uint8_t* last_wet, const double* w,
+                                  const double* L, const double* D, int nz, int na, int nb, double theta,
+                                  double theta_bc, double* ut, double* Qb, void* stream);
+
+/* ale.py:445-480, 582-626 ppm_edges_x / _ppm_edges_kernel of where(active, nan_to_num(h), 0): h_w, h_e. */
+int pocean_ppm_edges_f64(const double* h, const uint8_t* active, int nz, int ny, int nx, double h_min, double* h_w,
+                         double* h_e, void* stream);
+
+/* ale.py:743-764 ppm_transport_x: PPM layer fluxes Qx (nz, ny, nx+1) with the uniform per-face correction du that
+ * makes sum_k Qx = Q_bt (Newton with bracketing bisection, max_iter iterations stopped when every face has
+ * converged, then the residual share).  ut, q_e, q_w (nz, ny, nx+1); L, Q_bt (ny, nx+1); dx (ny, nx). */
+size_t pocean_ppm_transport_workspace_bytes(int nz, int ny, int nx, int max_iter);
+int pocean_ppm_transport_f64(const double* h, const double* ut, const double* L, const double* Q_bt,
+                             const double* q_e, const double* q_w, const uint8_t* active, const double* dx, int nz,
+                             int ny, int nx, double dt, int max_iter, double* Qx, void* workspace,
+                             size_t workspace_bytes, void* stream);
+
+/* ale.py:300-441 limit_outflow: Qx (nz, ny, nx+1) and Qy (nz, ny+1, nx) limited IN PLACE so that no active
+ * cell-layer sends out more than (h - h_floor)+ area / dt, the cut flux given back to the other layers of each
+ * face.  flags: POCEAN_PERIODIC_X / _Y.  Synchronises the stream (once when nothing exceeds, once per pass
+ * otherwise).  *n_limited: limited cell-layers summed over the passes; *warned: still over after max_pass but
+ * h-dagger >= -h_floor (the reference warns).  POCEAN_ESTEP where the reference raises (Qx, Qy then undefined). */
+size_t pocean_limit_outflow_workspace_bytes(int nz, int ny, int nx);
+int pocean_limit_outflow_f64(const double* h, double* Qx, double* Qy, const double* area, const uint8_t* active,
+                             int nz, int ny, int nx, double dt, double h_floor, int max_pass, unsigned flags,
+                             int* n_limited, int* warned, void* workspace, size_t workspace_bytes, void* stream);
+
+/* ale.py:278-294 lagrangian_thickness: h_dag = max(h - dt divq / A, 0) with A = area where > 0, else 1;
+ * *first_bad (DEVICE pointer) receives the flat (k, j, i) index of the first cell-layer below -tol, where the
+ * reference raises, or ~0 when there is none. */
+int pocean_lagrangian_thickness_f64(const double* h, const double* divq, const double* area, int nz, int ny, int nx,
+                                    double dt, double tol, double* h_dag, unsigned long long* first_bad,
+                                    void* stream);
 
 /*
  * Batched steps of many independent domains (no counterpart in the reference, which advances one model at a time):

@@ -4,7 +4,8 @@ pyocean_b200 — pyOCEAN's baroclinic tracer hot path on NVIDIA B200 (sm_100a).
 * ``TracerAdvection`` (advect_fct: SSP-RK3 WENO5 with Zalesak FCT; advect: SSP-RK3 without limiter) and
   ``remap_columns`` / ``remap_column`` (PCM / PLM / PPM_H4 conservative remap) with the reference's signatures.
 * The neighbours: ``ALECoordinate`` (z* / sigma ``regrid_remap``, ``regrid``, ``remap_faces``), ``face_fractions``
-  and ``diffuse_ale`` (the ALE horizontal diffusion kernel).
+  and ``diffuse_ale`` (the ALE horizontal diffusion kernel); ``producers`` (face transport thickness, transport
+  velocity, PPM layer transport, outflow limiter, Lagrangian thickness).
 * The compute path is libpocean_b200.so (hand-written CUDA, C ABI in include/pocean_b200.h), loaded with ctypes;
   PyTorch provides device memory and streams.  There is no CPU fallback.
 """
@@ -15,7 +16,8 @@ from .remap import MAX_LAYERS, PCM, PLM, PPM_H4, SCHEMES, remap_column, remap_co
 from .tracers import OpenEdges, TracerAdvection
 from .vertical import ALECoordinate, face_fractions, remap_faces
 from .diffusion import diffuse_ale
+from . import producers
 
 __all__ = ["TracerAdvection", "OpenEdges", "Periodic", "NONE", "TRACER_HALO", "remap_columns", "remap_column",
            "PCM", "PLM", "PPM_H4", "SCHEMES", "MAX_LAYERS", "ALECoordinate", "face_fractions", "remap_faces",
-           "diffuse_ale"]
+           "diffuse_ale", "producers"]

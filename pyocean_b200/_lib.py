@@ -18,7 +18,7 @@ WENO_JS = 0x40
 FCT_UNLIMITED = 0x80
 PCM, PLM, PPM_H4 = 0, 1, 2
 REGRID_ZSTAR, REGRID_SIGMA = 0, 1
-ERRORS = {1: "invalid argument", 2: "workspace", 3: "CUDA error", 4: "unsupported device"}
+ERRORS = {1: "invalid argument", 2: "workspace", 3: "CUDA error", 4: "unsupported device", 5: "step cannot proceed"}
 
 # Every symbol the header declares, with its ctypes signature.
 _P, _I, _U, _D, _Z = ctypes.c_void_p, ctypes.c_int, ctypes.c_uint, ctypes.c_double, ctypes.c_size_t
@@ -40,6 +40,15 @@ SIGNATURES: dict[str, tuple] = {
     "pocean_face_fractions_f64": (_I, [_P, _I, _I, _I, _P, _P]),
     "pocean_remap_faces_f64": (_I, [_P, _P, _P, _P, _I, _I, _I, _I, _I, _P, _P]),
     "pocean_diffuse_ale_f64": (_I, [_P, _P, _P, _P, _P, _P, _P, _P, _P, _I, _I, _I, _I, _U, _D, _D, _P, _P]),
+    "pocean_face_transport_thickness_f64": (_I, [_P, _P, _P, _I, _I, _I, _I, _P, _P, _P]),
+    "pocean_transport_velocity_f64": (_I, [_P, _P, _P, _P, _P, _P, _I, _I, _I, _D, _D, _P, _P, _P]),
+    "pocean_ppm_edges_f64": (_I, [_P, _P, _I, _I, _I, _D, _P, _P, _P]),
+    "pocean_ppm_transport_workspace_bytes": (_Z, [_I, _I, _I, _I]),
+    "pocean_ppm_transport_f64": (_I, [_P, _P, _P, _P, _P, _P, _P, _P, _I, _I, _I, _D, _I, _P, _P, _Z, _P]),
+    "pocean_limit_outflow_workspace_bytes": (_Z, [_I, _I, _I]),
+    "pocean_limit_outflow_f64": (_I, [_P, _P, _P, _P, _P, _I, _I, _I, _D, _D, _I, _U, ctypes.POINTER(_I),
+                                      ctypes.POINTER(_I), _P, _Z, _P]),
+    "pocean_lagrangian_thickness_f64": (_I, [_P, _P, _P, _I, _I, _I, _D, _D, _P, _P, _P]),
     "pocean_batch_device_bytes": (_Z, [_I]),
     "pocean_batch_create": (_I, [_P, _I, _I, _P, _Z, ctypes.POINTER(_P), _P]),
     "pocean_batch_step": (_I, [_P, _I, _I, _I, _P]),

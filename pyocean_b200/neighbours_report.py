@@ -4,7 +4,10 @@ Timing of the neighbours of the tracer step at the benchmark size (512 x 512 x 5
 * the z* regrid + PPM_H4 remap of both tracers in one call (``pocean_regrid_remap_f64``), and the regrid alone;
 * the ALE horizontal diffusion of the T/S stack, with its compulsory HBM bytes (T, Tw in and out per tracer; h, V
   per cell; the 2-D masks and metrics once) against the measured HBM peak;
-* the velocity remap in fraction space of the u-faces (512 x 513 x 50).
+* the velocity remap in fraction space of the u-faces (512 x 513 x 50);
+* the producers of the step's inputs on the u-faces: face transport thickness, transport velocity, PPM layer
+  transport with the barotropic Newton correction, the outflow limiter's check (nothing to limit, its common case)
+  and the Lagrangian thickness.
 
     python -m pyocean_b200.neighbours_report
 """
@@ -109,13 +112,47 @@ def neighbours_report(device=None) -> dict:
                                             2, vout.data_ptr(), st()), "remap_faces")
 
     t_faces = _time(faces)
+
+    # producers (u-faces)
+    Hd0 = g(H)
+    u8 = lambda a: g(a.astype(np.uint8))                                                   # noqa: E731
+    hx = g(np.where(w.wet[None], w.h_src, 0.0))
+    q_e, q_w = torch.empty_like(vel), torch.empty_like(vel)
+    ut, Qb = torch.empty_like(vel), torch.empty((ny, nf), dtype=torch.float64, device=dev)
+    Lf, Df = g(rng.uniform(1800.0, 2200.0, (ny, nf))), g(rng.uniform(20.0, 400.0, (ny, nf)))
+    lw = u8(rng.random((ny, nf)) > 0.05)
+    wf = torch.full_like(vel, 1.0 / n)
+    u1, u0 = g(rng.normal(0.0, 0.3, (n, ny, nf))), g(rng.normal(0.0, 0.3, (n, ny, nf)))
+    dxt = g(np.full((ny, nx), 2000.0))
+    Qx = torch.empty_like(vel)
+    nbytes = L.pocean_ppm_transport_workspace_bytes(n, ny, nx, 20)
+    ws = torch.empty(nbytes, dtype=torch.uint8, device=dev)
+
+    def ftt():
+        _lib.check(L.pocean_face_transport_thickness_f64(hx.data_ptr(), Hd0.data_ptr(), act.data_ptr(), n, ny, nx, 1,
+                                                         q_e.data_ptr(), q_w.data_ptr(), st()), "ftt")
+
+    def tvel():
+        _lib.check(L.pocean_transport_velocity_f64(u1.data_ptr(), u0.data_ptr(), lw.data_ptr(), wf.data_ptr(),
+                                                   Lf.data_ptr(), Df.data_ptr(), n, ny, nf, 0.6, 0.5, ut.data_ptr(),
+                                                   Qb.data_ptr(), st()), "tvel")
+
+    def ppm():
+        _lib.check(L.pocean_ppm_transport_f64(hx.data_ptr(), ut.data_ptr(), Lf.data_ptr(), Qb.data_ptr(),
+                                              q_e.data_ptr(), q_w.data_ptr(), act.data_ptr(), dxt.data_ptr(), n, ny,
+                                              nx, 300.0, 20, Qx.data_ptr(), ws.data_ptr(), nbytes, st()), "ppm")
+
+    t_ftt, t_tvel = _time(ftt), _time(tvel)
+    t_ppm = _time(ppm, reps=5)
     peak = _hbm_peak()
     return dict(workload=w.name,
                 regrid_remap_zstar=dict(call_ms=t_fused, regrid_ms=t_regrid, regrid_then_remap_columns_ms=t_sep,
                                         equal=same, fields=nt),
                 diffuse_ale=dict(ms=t_diff, algorithmic_bytes=diff_bytes, gbs=diff_bytes / t_diff / 1e6,
                                  frac_of_measured_hbm=diff_bytes / t_diff / 1e6 / peak, fields=nt),
-                remap_faces_u=dict(ms=t_faces, faces=n * ny * nf))
+                remap_faces_u=dict(ms=t_faces, faces=n * ny * nf),
+                producers_u=dict(face_transport_thickness_ms=t_ftt, transport_velocity_ms=t_tvel,
+                                 ppm_transport_ms=t_ppm, faces=n * ny * nf))
 
 
 if __name__ == "__main__":

@@ -117,3 +117,16 @@ def test_neighbour_argument_errors():
     assert L.pocean_remap_faces_f64(8, 8, 8, None, 4, 3, 3, 0, 2, 8, None) == 1
     assert L.pocean_diffuse_ale_f64(8, 8, 8, 8, 8, 8, 8, 8, 8, 1, 2, 3, 4, 0x1, 1.0, 1.0, 8, None) == 1   # open flag
     assert L.pocean_diffuse_ale_f64(8, 8, 8, 8, 8, 8, 8, 8, None, 1, 2, 3, 4, 0, 1.0, 1.0, 8, None) == 1
+
+
+def test_producer_argument_errors_and_workspaces():
+    L = _lib.lib()
+    assert L.pocean_ppm_transport_workspace_bytes(4, 8, 9, 20) >= 2 * 4 * 8 * 9 * 8 + 5 * 8 * 10 * 8
+    assert L.pocean_limit_outflow_workspace_bytes(4, 8, 9) >= 3 * 4 * 8 * 9 * 8
+    assert L.pocean_face_transport_thickness_f64(None, 8, 8, 2, 3, 4, 1, 8, 8, None) == 1
+    assert L.pocean_ppm_transport_f64(8, 8, 8, 8, 8, 8, 8, 8, 2, 3, 4, 1.0, 20, 8, 256, 16, None) == 2
+    assert L.pocean_ppm_transport_f64(8, 8, 8, 8, 8, 8, 8, 8, 2, 3, 4, 1.0, -1, 8, 256, 1 << 20, None) == 1
+    nl, wn = ctypes.c_int(0), ctypes.c_int(0)
+    assert L.pocean_limit_outflow_f64(8, 8, 8, 8, 8, 2, 3, 4, 1.0, 1e-10, 50, 0x1, ctypes.byref(nl), ctypes.byref(wn),
+                                      256, 1 << 20, None) == 1                     # open flag
+    assert L.pocean_lagrangian_thickness_f64(8, 8, 8, 2, 3, 4, 1.0, 1e-9, 8, None, None) == 1
