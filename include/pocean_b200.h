@@ -253,10 +253,10 @@ size_t pocean_batch_device_bytes(int ndom);
 
 /* Validates the domains and writes the plan into device_buf with copies ordered on `stream` (after the steps
  * already enqueued there, which may still be reading an earlier plan in the same buffer); `domains` may be released
- * on return.  Not capturable: call outside stream capture.  seglen: rows per warp segment of the WENO passes (a
- * tuning parameter; results do not depend on it).  A plan only refers to the domains' buffers; steps enqueued with
- * it must be ordered after the plan's copies (same stream, or an event). */
-int pocean_batch_create(const pocean_domain* domains, int ndom, int seglen, void* device_buf, size_t device_bytes,
+ * on return.  Not capturable: call outside stream capture.  tile_rows: 4, 8 or 16, the height of the 32-wide cell
+ * tiles of the WENO face and stage passes (a tuning parameter; results do not depend on it).  A plan only refers to
+ * the domains' buffers; steps enqueued with it must be ordered after the plan's copies (same stream, or an event). */
+int pocean_batch_create(const pocean_domain* domains, int ndom, int tile_rows, void* device_buf, size_t device_bytes,
                         pocean_batch** out, void* stream);
 
 /* Enqueues one step of every domain.  remap_nf: fields per remap thread (1 or 2, a tuning parameter); mixed: FP32

@@ -2,7 +2,7 @@
 Batched ALE tracer steps of many independent, unevenly sized domains on one GPU.
 
 One step of every domain is ``advect_fct`` of its stack followed by the remap of every stack member onto its target
-grid (the reference's phases 7 and 8, core/model/driver.py:888-985, run once per domain).  Instead of 7-8 kernel
+grid (the reference's phases 7 and 8, core/model/driver.py:888-985, run once per domain).  Instead of 10-11 kernel
 launches per domain and step, each pass of the step is ONE launch over all domains: the CTAs of a launch are split
 into per-domain ranges by a CTA-offset table and every CTA finds its domain by binary search, so small domains share
 the GPU instead of each leaving most of the 148 SMs idle.  A step sequence only enqueues kernels and is captured in
@@ -99,7 +99,8 @@ class _Plan:
     """A ``pocean_batch`` plan and the device buffer holding its descriptors (``buf``: reuse a buffer of an earlier
     plan — the new descriptors are written in stream order, after the steps already enqueued)."""
 
-    def __init__(self, structs, seglen: int, device, buf: torch.Tensor | None = None, stream: int | None = None) -> None:
+    def __init__(self, structs, tile_rows: int, device, buf: torch.Tensor | None = None,
+                 stream: int | None = None) -> None:
         L = _lib.lib()
         n = len(structs)
         need = L.pocean_batch_device_bytes(n)
@@ -109,10 +110,10 @@ class _Plan:
         arr = (_Domain * n)(*structs)
         h = ctypes.c_void_p()
         st = torch.cuda.current_stream(device).cuda_stream if stream is None else stream
-        _lib.check(L.pocean_batch_create(ctypes.cast(arr, ctypes.c_void_p), n, seglen, self.buf.data_ptr(),
+        _lib.check(L.pocean_batch_create(ctypes.cast(arr, ctypes.c_void_p), n, tile_rows, self.buf.data_ptr(),
                                          self.buf.numel(), ctypes.byref(h), st), "batch_create")
         self.handle = h
-        self.seglen = seglen
+        self.tile_rows = tile_rows
 
     def step(self, parity: int, remap_nf: int, mixed: bool, stream: int) -> None:
         _lib.check(_lib.lib().pocean_batch_step(self.handle, parity, remap_nf, int(mixed), stream), "batch_step")
@@ -127,10 +128,10 @@ class _Plan:
 class DomainBatch:
     """Many independent domains stepped together: every pass of a step is one launch over all of them."""
 
-    SEGLENS = (16, 32, 64, 128)
+    TILE_ROWS = (4, 8, 16)
     REMAP_NF = (1, 2)
 
-    def __init__(self, domains: Iterable[Domain], seglen: int = 64, remap_nf: int = 2, mixed: bool = False) -> None:
+    def __init__(self, domains: Iterable[Domain], tile_rows: int = 8, remap_nf: int = 2, mixed: bool = False) -> None:
         self.domains = list(domains)
         if not self.domains:
             raise ValueError("a batch needs at least one domain")
@@ -140,21 +141,21 @@ class DomainBatch:
         self.parity = 0
         self._structs = [d.as_struct() for d in self.domains]
         self._plans: dict[int, _Plan] = {}
-        self.plan = self._plan(seglen)
+        self.plan = self._plan(tile_rows)
 
     @property
     def launches_per_step(self) -> int:
-        """3 WENO passes, the limiter coefficients, the final update, then the remap: one pass over field pairs
-        and one over the odd fields (or one over all fields) and the general-column fixup."""
+        """3 face and 3 cell passes, the limiter coefficients, the final update, then the remap: one pass over
+        field pairs and one over the odd fields (or one over all fields) and the general-column fixup."""
         nts = [d.shape[0] for d in self.domains]
         if self.remap_nf == 2:
-            return 5 + any(n >= 2 for n in nts) + any(n % 2 for n in nts) + 1
-        return 5 + 2
+            return 8 + any(n >= 2 for n in nts) + any(n % 2 for n in nts) + 1
+        return 8 + 2
 
-    def _plan(self, seglen: int) -> _Plan:
-        if seglen not in self._plans:
-            self._plans[seglen] = _Plan(self._structs, seglen, self.device)
-        return self._plans[seglen]
+    def _plan(self, tile_rows: int) -> _Plan:
+        if tile_rows not in self._plans:
+            self._plans[tile_rows] = _Plan(self._structs, tile_rows, self.device)
+        return self._plans[tile_rows]
 
     @property
     def cells(self) -> int:
@@ -190,16 +191,16 @@ class DomainBatch:
         self.parity = p0
         return g
 
-    def autotune(self, steps: int = 2, seglens: Sequence[int] | None = None,
+    def autotune(self, steps: int = 2, tile_rows: Sequence[int] | None = None,
                  nfs: Sequence[int] | None = None) -> dict:
-        """Times every (seglen, remap_nf) on the batch itself and keeps the fastest.  The state is saved before
-        and restored after, so tuning does not advance the domains."""
-        seglens = tuple(seglens or self.SEGLENS)
+        """Times every (tile rows of the stage passes, remap fields per thread) on the batch itself and keeps the
+        fastest.  The state is saved before and restored after, so tuning does not advance the domains."""
+        rows = tuple(tile_rows or self.TILE_ROWS)
         nfs = tuple(nfs or self.REMAP_NF)
         saved = [self.state(i).clone() for i in range(len(self.domains))]
         p0 = self.parity
         times = {}
-        for sl in seglens:
+        for sl in rows:
             self.plan = self._plan(sl)
             for nf in nfs:
                 self.remap_nf = nf
@@ -217,13 +218,14 @@ class DomainBatch:
         self.parity = p0
         for i, s in enumerate(saved):
             self.state(i).copy_(s)
-        return dict(seglen=best[0], remap_nf=best[1], ms_per_step={f"{k[0]}/{k[1]}": v for k, v in times.items()})
+        return dict(tile_rows=best[0], remap_nf=best[1],
+                    ms_per_step={f"{k[0]}/{k[1]}": v for k, v in times.items()})
 
 
 def sequential_launches(domains: Sequence[Domain]) -> int:
-    """Kernel launches of one ``sequential_step``: 5 FCT passes, then per domain the remap of field pairs (if any),
+    """Kernel launches of one ``sequential_step``: 8 FCT passes, then per domain the remap of field pairs (if any),
     of the odd field (if any) and the general-column fixup."""
-    return sum(5 + (d.shape[0] >= 2) + (d.shape[0] % 2) + 1 for d in domains)
+    return sum(8 + (d.shape[0] >= 2) + (d.shape[0] % 2) + 1 for d in domains)
 
 
 def sequential_step(domains: Sequence[Domain], parity: int, mixed: bool = False, stream: int | None = None) -> None:

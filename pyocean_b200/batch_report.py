@@ -78,7 +78,7 @@ def batched_report(steps: int = 50, seed: int = 0, ndom: int = 64, device=None, 
 
     # batched mixed precision
     restore()
-    mb = DomainBatch(doms, seglen=tune["seglen"], remap_nf=tune["remap_nf"], mixed=True)
+    mb = DomainBatch(doms, tile_rows=tune["tile_rows"], remap_nf=tune["remap_nf"], mixed=True)
     gm = mb.capture(steps)
     restore()
     mix_ms = _timed(gm.replay, stream)

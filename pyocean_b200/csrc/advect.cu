@@ -4,23 +4,24 @@
 // Reference: core/components/tracers.py:208-254, 342-375 and the Numba kernels of
 // core/dynamics/sigma_baroclinic.py:265-364 (faces, RHS), 407-530 (FCT), 856-875 (RK stage).
 //
-// Design.  The reference runs 9 kernels over ~15 full-size temporaries per FCT step.  Here one step is 5 launches:
-//   1-3. WENO5 passes (fct_strip.cuh): warps march in j along 31-cell strips of a (t, k) plane; each face is
-//        computed once per stage (32/31 per cell in x, 1 + 1/SEG in y) from a register window (y) and a per-warp
-//        shared-memory row ring (x), without block barriers.
-//        1: F0, c1 = safe(q0 - dt div F0, Va); F0 kept on the faces (S).
-//        2: F1, q1 recomputed from the kept F0 (never stored), c2 = safe(3/4 q0 + 1/4 (q1 - dt div F1), Vb);
-//           T = (F0 + F1)/6.
-//        3: F2, antidiffusive flux A = T + 2 F2/3 - F_L over S (donor flux F_L from C), c_L = safe(q0 - dt div F_L,
-//           V1).
-//   4. coeff  Zalesak R+ / R- per cell from the 7-point (x, y, k +- 1) bounds of C and c_L (tracers looped per
+// Design.  The reference runs 9 kernels over ~15 full-size temporaries per FCT step.  Here one step is 8 launches:
+//   1-6. for each RK stage s a face pass and a cell pass (fct_split.cuh): one thread per cell computes the west x-
+//        face and the south y-face of its cell from global memory (L1 serves the overlapping stencils; no shared
+//        memory, no barrier, high occupancy, two independent WENO5 chains per thread), then a streaming pass updates
+//        the cells from the stored faces.
+//        1: S <- F0;  c1 = safe(q0 - dt div F0, Va).
+//        2: T <- F1;  q1 recomputed from F0, c2 = safe(3/4 q0 + 1/4 (q1 - dt div F1), Vb).
+//        3: S <- A = ((F0 + F1)/6 + 2 F2/3) - F_L, T <- F_L (donor flux of C);  c_L = safe(q0 - dt div F_L, V1).
+//   7. coeff  Zalesak R+ / R- per cell from the 7-point (x, y, k +- 1) bounds of C and c_L (tracers looped per
 //             thread: the stencil geometry is read once).
-//   5. final  face coefficients from R of both neighbours; C_out = safe(q0 - dt div(F_L + C A), V1).
-// q0 = V0 C, Va, Vb, q1 and F_L are recomputed where needed instead of stored.  Planes run k-major (the tracers
-// of one layer follow each other) so a layer's geometry is re-read from L2.  Periodic axes wrap natively in every
-// stencil (the reference pads by TRACER_HALO = 13 cells and crops; with the dependency radius of the step, 10
-// cells, both give the same numbers).  Workspace: 3 cell stacks (c1 -> R+, c2 -> R-, c_L) and 4 face stacks
-// (S: F0 -> A, T: (F0 + F1)/6).
+//   8. final  face coefficients from R of both neighbours; C_out = safe(q0 - dt div(F_L + C A), V1).
+// q0 = V0 C, Va, Vb and q1 are recomputed where needed instead of stored.  Planes run k-major (the tracers of one
+// layer follow each other) so a layer's geometry is re-read from L2.  Periodic axes wrap natively in every stencil
+// (the reference pads by TRACER_HALO = 13 cells and crops; with the dependency radius of the step, 10 cells, both
+// give the same numbers).  Workspace: 3 cell stacks (c1 -> R+, c2 -> R-, c_L) and 4 face stacks (S, T).
+// An earlier form marched warps along 31-cell strips with a shared-memory row ring and did each stage in one pass;
+// the split form is 14 % faster at 512 x 512 x 50 (the passes are bound by instruction issue and latency, and the
+// simple face threads run at twice the occupancy).
 //
 // Arithmetic: every expression in the reference's order, no FMA contraction (-fmad=false), IEEE division; the
 // results equal the reference's FP64 Numba path bit for bit.
@@ -188,7 +189,7 @@ __device__ __forceinline__ double donor_y(const double* __restrict__ cp, const d
 
 }  // namespace po
 
-#include "fct_strip.cuh"
+#include "fct_split.cuh"
 
 namespace po {
 
@@ -212,10 +213,11 @@ __global__ void __launch_bounds__(NTHREADS) fct_unlimited_kernel(StepArgs a)
     const int gi = i0 + tx, gj = j0 + ty;
     if (gi >= s.nx || gj >= s.ny) return;
     const i64 w = s.ux(t, k, gj, gi), so = s.vy(t, k, gj, gi);
-    const double fw = a.Tx[w] + div3_exact(2.0 * T.fx[ty][tx]);
-    const double fe = a.Tx[w + 1] + div3_exact(2.0 * T.fx[ty][tx + 1]);
-    const double fs = a.Ty[so] + div3_exact(2.0 * T.fy[ty][tx]);
-    const double fn = a.Ty[so + s.nx] + div3_exact(2.0 * T.fy[ty + 1][tx]);
+    // S holds F0 and T holds F1: (F0 + F1)/6 formed here
+    const double fw = div6_exact(a.Sx[w] + a.Tx[w]) + div3_exact(2.0 * T.fx[ty][tx]);
+    const double fe = div6_exact(a.Sx[w + 1] + a.Tx[w + 1]) + div3_exact(2.0 * T.fx[ty][tx + 1]);
+    const double fs = div6_exact(a.Sy[so] + a.Ty[so]) + div3_exact(2.0 * T.fy[ty][tx]);
+    const double fn = div6_exact(a.Sy[so + s.nx] + a.Ty[so + s.nx]) + div3_exact(2.0 * T.fy[ty + 1][tx]);
     if (a.fx_face != nullptr && gi == (a.face_i == s.nx ? s.nx - 1 : a.face_i))
         a.fx_face[((i64)t * s.n + k) * s.ny + gj] = a.face_i == s.nx ? fe : fw;
     const double d = fe - fw + fn - fs;
@@ -624,11 +626,20 @@ static int common_checks(const char* fn, const void* C, const void* V0, const vo
 }
 
 template <bool ZV, bool MIX>
-static void launch_strips(const StepArgs& a, int stage, dim3 grid, int nstrips, int nsegs, cudaStream_t st)
+static void launch_split(const StepArgs& a, int stage, cudaStream_t st)
 {
-    if (stage == 1) fct_strip_kernel<1, ZV, MIX><<<grid, SWARPS * 32, 0, st>>>(a, SEG, nstrips, nsegs);
-    else if (stage == 2) fct_strip_kernel<2, ZV, MIX><<<grid, SWARPS * 32, 0, st>>>(a, SEG, nstrips, nsegs);
-    else fct_strip_kernel<3, ZV, MIX><<<grid, SWARPS * 32, 0, st>>>(a, SEG, nstrips, nsegs);
+    const Shape& s = a.s;
+    const dim3 grid(ceil_div(s.nx, TI), ceil_div(s.ny, TJ), s.nt * s.n);
+    if (stage == 1) {
+        fct_faces_kernel<1, ZV, MIX, TJ><<<grid, TI * TJ, 0, st>>>(a);
+        fct_update_kernel<1, TJ><<<grid, TI * TJ, 0, st>>>(a);
+    } else if (stage == 2) {
+        fct_faces_kernel<2, ZV, MIX, TJ><<<grid, TI * TJ, 0, st>>>(a);
+        fct_update_kernel<2, TJ><<<grid, TI * TJ, 0, st>>>(a);
+    } else {
+        fct_faces_kernel<3, ZV, MIX, TJ><<<grid, TI * TJ, 0, st>>>(a);
+        fct_update_kernel<3, TJ><<<grid, TI * TJ, 0, st>>>(a);
+    }
 }
 
 // The FCT step with FP64 (mixed = false) or FP32-weight (mixed = true) WENO faces; everything else FP64.
@@ -655,22 +666,20 @@ static int advect_fct_impl(const char* fn, bool mixed, const double* C, const do
     a.out = C_out; a.face_i = face_i; a.fx_face = fx_face;
 
     const dim3 grid(ceil_div(nx, TI), ceil_div(ny, TJ), nt * nz);
-    const int nstrips = ceil_div(nx, STRIP), nsegs = ceil_div(ny, SEG);
-    const dim3 sgrid(ceil_div(nstrips * nsegs, SWARPS), nt * nz);
     const bool zv = !(flags & POCEAN_WENO_JS);
-    auto strips = [&](int stage) {
-        if (zv && !mixed) launch_strips<true, false>(a, stage, sgrid, nstrips, nsegs, st);
-        else if (!zv && !mixed) launch_strips<false, false>(a, stage, sgrid, nstrips, nsegs, st);
-        else if (zv) launch_strips<true, true>(a, stage, sgrid, nstrips, nsegs, st);
-        else launch_strips<false, true>(a, stage, sgrid, nstrips, nsegs, st);
+    auto stage_passes = [&](int stage) {
+        if (zv && !mixed) launch_split<true, false>(a, stage, st);
+        else if (!zv && !mixed) launch_split<false, false>(a, stage, st);
+        else if (zv) launch_split<true, true>(a, stage, st);
+        else launch_split<false, true>(a, stage, st);
     };
-    strips(1);
-    strips(2);
+    stage_passes(1);
+    stage_passes(2);
     if (flags & POCEAN_FCT_UNLIMITED) {
         fct_unlimited_kernel<<<grid, NTHREADS, 0, st>>>(a);
         return pocean_check_launch(fn);
     }
-    strips(3);
+    stage_passes(3);
     fct_coeff_kernel<<<dim3(ceil_div(nx, TI), ceil_div(ny, TJ), nz), NTHREADS, 0, st>>>(a);
     fct_final_kernel<<<dim3(ceil_div(nx, TI), ceil_div(ny, TJ), nz), NTHREADS, 0, st>>>(a);
     if (fx_face) {
@@ -684,36 +693,47 @@ static int advect_fct_impl(const char* fn, bool mixed, const double* C, const do
 namespace po {
 
 // The FCT passes of every domain of a batch, one launch per pass (off_host: the CTA offsets also held on the device).
+template <bool ZV, bool MIX, int TJR>
+static void fct_batched_stages(const BatchDomain* doms, const int* po, unsigned np, int ndom, cudaStream_t st)
+{
+    fct_faces_batched<1, ZV, MIX, TJR><<<np, TI * TJR, 0, st>>>(doms, po, ndom);
+    fct_update_batched<1, TJR><<<np, TI * TJR, 0, st>>>(doms, po, ndom);
+    fct_faces_batched<2, ZV, MIX, TJR><<<np, TI * TJR, 0, st>>>(doms, po, ndom);
+    fct_update_batched<2, TJR><<<np, TI * TJR, 0, st>>>(doms, po, ndom);
+    fct_faces_batched<3, ZV, MIX, TJR><<<np, TI * TJR, 0, st>>>(doms, po, ndom);
+    fct_update_batched<3, TJR><<<np, TI * TJR, 0, st>>>(doms, po, ndom);
+}
+
+// The FCT passes of every domain of a batch, one launch per pass (off_host: the CTA offsets also held on the device).
 template <bool ZV, bool MIX>
-static void fct_batched_impl(const BatchDomain* doms, const int* off_dev, const int* off_host, int ndom,
+static void fct_batched_impl(const BatchDomain* doms, const int* off_dev, const int* off_host, int ndom, int tile_rows,
                              cudaStream_t st)
 {
-    const int* so = off_dev + BP_STRIP * (ndom + 1);
+    const int* po = off_dev + BP_PTILE * (ndom + 1);
     const int* to = off_dev + BP_TILE * (ndom + 1);
-    const unsigned ns = (unsigned)off_host[BP_STRIP * (ndom + 1) + ndom];
+    const unsigned np = (unsigned)off_host[BP_PTILE * (ndom + 1) + ndom];
     const unsigned nt = (unsigned)off_host[BP_TILE * (ndom + 1) + ndom];
-    fct_strip_batched<1, ZV, MIX><<<ns, SWARPS * 32, 0, st>>>(doms, so, ndom);
-    fct_strip_batched<2, ZV, MIX><<<ns, SWARPS * 32, 0, st>>>(doms, so, ndom);
-    fct_strip_batched<3, ZV, MIX><<<ns, SWARPS * 32, 0, st>>>(doms, so, ndom);
+    if (tile_rows == 4) fct_batched_stages<ZV, MIX, 4>(doms, po, np, ndom, st);
+    else if (tile_rows == 16) fct_batched_stages<ZV, MIX, 16>(doms, po, np, ndom, st);
+    else fct_batched_stages<ZV, MIX, 8>(doms, po, np, ndom, st);
     fct_coeff_batched<<<nt, NTHREADS, 0, st>>>(doms, to, ndom);
     fct_final_batched<<<nt, NTHREADS, 0, st>>>(doms, to, ndom);
 }
 
 void fct_batched_launch(const BatchDomain* doms, const int* off_dev, const int* off_host, int ndom, bool zv,
-                        bool mixed, cudaStream_t st)
+                        bool mixed, int tile_rows, cudaStream_t st)
 {
-    if (zv && !mixed) fct_batched_impl<true, false>(doms, off_dev, off_host, ndom, st);
-    else if (!zv && !mixed) fct_batched_impl<false, false>(doms, off_dev, off_host, ndom, st);
-    else if (zv) fct_batched_impl<true, true>(doms, off_dev, off_host, ndom, st);
-    else fct_batched_impl<false, true>(doms, off_dev, off_host, ndom, st);
+    if (zv && !mixed) fct_batched_impl<true, false>(doms, off_dev, off_host, ndom, tile_rows, st);
+    else if (!zv && !mixed) fct_batched_impl<false, false>(doms, off_dev, off_host, ndom, tile_rows, st);
+    else if (zv) fct_batched_impl<true, true>(doms, off_dev, off_host, ndom, tile_rows, st);
+    else fct_batched_impl<false, true>(doms, off_dev, off_host, ndom, tile_rows, st);
 }
 
-// CTAs of each batched FCT pass for one domain (strip pairs per plane x planes; tiles x layers).
-void fct_batched_ctas(const Shape& s, int seglen, int& strip_ctas, int& tile_ctas, int& nstrips, int& nsegs)
+// CTAs of each batched FCT pass for one domain: 32 x tile_rows tiles x planes (stage passes); 32 x 8 tiles x
+// layers (coefficient and final passes).
+void fct_batched_ctas(const Shape& s, int tile_rows, int& plane_ctas, int& tile_ctas)
 {
-    nstrips = ceil_div(s.nx, STRIP);
-    nsegs = ceil_div(s.ny, seglen);
-    strip_ctas = ceil_div(nstrips * nsegs, SWARPS) * s.nt * s.n;
+    plane_ctas = ceil_div(s.nx, TI) * ceil_div(s.ny, tile_rows) * s.nt * s.n;
     tile_ctas = ceil_div(s.nx, TI) * ceil_div(s.ny, TJ) * s.n;
 }
 

@@ -1,6 +1,6 @@
 // Batched ALE tracer steps of many independent domains: every pass of the FCT advection and the remap is one launch
 // over all domains (domain d owns a contiguous range of the launch's CTAs, found by binary search of a CTA-offset
-// table), so a batch of uneven domains costs 7-8 launches per step instead of 7-8 per domain, and the step
+// table), so a batch of uneven domains costs 10-11 launches per step instead of 10-11 per domain, and the step
 // sequence can be captured in one CUDA graph.  The batch plan (descriptors of both ping-pong parities and the
 // offset tables) lives in a caller-provided device buffer; the library allocates no device memory.
 #include <cstdlib>
@@ -14,6 +14,7 @@ using namespace po;
 
 struct pocean_batch {
     int ndom;
+    int tile_rows;                     // rows of the 32-wide tiles of the stage passes
     int nmax;                          // deepest column of the batch
     bool zv;                           // WENO5-Z (else JS) for every domain
     BatchDomain* dev_doms;             // 2 * ndom descriptors: parity 0 then parity 1
@@ -28,14 +29,15 @@ extern "C" size_t pocean_batch_device_bytes(int ndom)
     return d + (size_t)BP_COUNT * (ndom + 1) * sizeof(int);
 }
 
-extern "C" int pocean_batch_create(const pocean_domain* domains, int ndom, int seglen, void* device_buf,
+extern "C" int pocean_batch_create(const pocean_domain* domains, int ndom, int tile_rows, void* device_buf,
                                    size_t device_bytes, pocean_batch** out, void* stream)
 {
     const char* fn = "pocean_batch_create";
     if (!out) return pocean_fail(POCEAN_EINVAL, "%s: null output handle", fn);
     *out = nullptr;
     if (ndom < 1 || !domains) return pocean_fail(POCEAN_EINVAL, "%s: no domains", fn);
-    if (seglen < 4 || seglen > 4096) return pocean_fail(POCEAN_EINVAL, "%s: segment length %d outside 4..4096", fn, seglen);
+    if (tile_rows != 4 && tile_rows != 8 && tile_rows != 16)
+        return pocean_fail(POCEAN_EINVAL, "%s: tile rows %d (4, 8 or 16)", fn, tile_rows);
     if (!device_buf || device_bytes < pocean_batch_device_bytes(ndom) || ((uintptr_t)device_buf & 255))
         return pocean_fail(POCEAN_EWORKSPACE, "%s: device buffer of %zu bytes (256-byte aligned) needed", fn,
                            pocean_batch_device_bytes(ndom));
@@ -78,9 +80,8 @@ extern "C" int pocean_batch_create(const pocean_domain* domains, int ndom, int s
             B.a.out = D.C_adv;
             B.h_src = D.h_src; B.h_tgt = D.h_tgt; B.wet = D.wet; B.remap_scheme = D.remap_scheme;
             B.rout = parity == 0 ? D.C_next : const_cast<double*>(D.C);
-            int sc, tc, ns, ng;
-            fct_batched_ctas(B.a.s, seglen, sc, tc, ns, ng);
-            B.seglen = seglen; B.nstrips = ns; B.nsegs = ng;
+            int sc, tc;
+            fct_batched_ctas(B.a.s, tile_rows, sc, tc);
             if (parity == 0) {
                 const long long cb = ((long long)D.ny * D.nx + 127) / 128;
                 const long long n_pass[BP_COUNT] = {sc, tc, cb * (D.nt / 2), cb * (D.nt % 2), cb * D.nt, cb * D.nt};
@@ -96,6 +97,7 @@ extern "C" int pocean_batch_create(const pocean_domain* domains, int ndom, int s
     for (int q = 0; q < BP_COUNT; ++q) off[(size_t)q * (ndom + 1) + ndom] = (int)tot[q];
     pocean_batch* b = new pocean_batch;
     b->ndom = ndom;
+    b->tile_rows = tile_rows;
     b->nmax = nmax;
     b->zv = zv;
     b->dev_doms = (BatchDomain*)device_buf;
@@ -124,7 +126,7 @@ extern "C" int pocean_batch_step(const pocean_batch* b, int parity, int remap_nf
     if (remap_nf != 1 && remap_nf != 2) return pocean_fail(POCEAN_EINVAL, "%s: remap_nf must be 1 or 2", fn);
     cudaStream_t st = (cudaStream_t)stream;
     const BatchDomain* doms = b->dev_doms + (size_t)parity * b->ndom;
-    fct_batched_launch(doms, b->dev_off, b->host_off.data(), b->ndom, b->zv, mixed != 0, st);
+    fct_batched_launch(doms, b->dev_off, b->host_off.data(), b->ndom, b->zv, mixed != 0, b->tile_rows, st);
     remap_batched_launch(doms, b->dev_off, b->host_off.data(), b->ndom, remap_nf, b->nmax, st);
     return pocean_check_launch(fn);
 }

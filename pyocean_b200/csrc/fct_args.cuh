@@ -52,11 +52,11 @@ struct BatchDomain {
     const double* h_tgt;
     const uint8_t* wet;
     double* rout;
-    int seglen, nstrips, nsegs, remap_scheme;
+    int remap_scheme;
 };
 
 // CTA offsets of every batched pass: domain d owns CTAs off[d] .. off[d+1]-1 of the launch (ndom + 1 entries each).
-enum BatchPass { BP_STRIP = 0, BP_TILE = 1, BP_RPAIR = 2, BP_RREM = 3, BP_RALL = 4, BP_RGEN = 5, BP_COUNT = 6 };
+enum BatchPass { BP_PTILE = 0, BP_TILE = 1, BP_RPAIR = 2, BP_RREM = 3, BP_RALL = 4, BP_RGEN = 5, BP_COUNT = 6 };
 
 // The domain whose CTA range holds CTA b (binary search of off[0..ndom]).
 __device__ __forceinline__ int find_domain(const int* __restrict__ off, int ndom, int b)
@@ -75,8 +75,8 @@ void carve_fct_workspace(StepArgs& a, void* workspace);
 
 // Host launchers of the batched passes (advect.cu, remap.cu).
 void fct_batched_launch(const BatchDomain* doms, const int* off_dev, const int* off_host, int ndom, bool zv,
-                        bool mixed, cudaStream_t st);
-void fct_batched_ctas(const Shape& s, int seglen, int& strip_ctas, int& tile_ctas, int& nstrips, int& nsegs);
+                        bool mixed, int tile_rows, cudaStream_t st);
+void fct_batched_ctas(const Shape& s, int tile_rows, int& plane_ctas, int& tile_ctas);
 void remap_batched_launch(const BatchDomain* doms, const int* off_dev, const int* off_host, int ndom, int nf_mode,
                           int nmax, cudaStream_t st);
 

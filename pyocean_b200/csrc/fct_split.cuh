@@ -1,0 +1,294 @@
+// The three WENO passes of the FCT step split into a face pass and a cell pass each (included by advect.cu).
+//
+// Face pass of stage s: one thread per cell (t, k, j, i) computes the west x-face and the south y-face of its cell
+// (the last column / row also the east / north domain face) straight from global memory (the six-cell stencils
+// overlap between neighbouring threads and are served by L1), with no shared memory and no barrier, so the pass runs
+// at high occupancy and the two independent WENO5 chains of a thread overlap.  Cell pass of stage s: the stage
+// update from the stored faces.  Faces per stage are stored once:
+//   stage 1: S <- F0;  stage 2: T <- F1;  stage 3: S <- A = ((F0 + F1)/6 + 2 F2/3) - F_L and T <- F_L,
+// with (F0 + F1)/6 and 2 F2/3 formed by the same exact divisions as the reference.  The arithmetic of every face and
+// update is the reference's (weno.cuh; sigma_baroclinic.py:265-321, 452-511), so results equal the reference's bit
+// for bit.  Addresses are formed once per thread as plane pointers with 32-bit offsets; interior stencils (all six
+// cells inside the domain, the common case) load with fixed offsets, edge and periodic stencils take a guarded path.
+#pragma once
+
+namespace po {
+
+// The stage's input field (stages 1: C; 2: c1; 3: c2).
+template <int STAGE>
+__device__ __forceinline__ const double* stage_field(const StepArgs& a)
+{
+    return STAGE == 1 ? a.C : (STAGE == 2 ? a.c1 : a.c2);
+}
+
+// Six cells f-3 .. f+2 of a line with element stride ST (compile-time 1 for rows) or st (columns): values and the
+// reference's validity `0 <= g < n and ok[g]` (periodic lines wrap).
+template <int ST>
+__device__ __forceinline__ void line6(const double* __restrict__ c, const uint8_t* __restrict__ ok, int st, int n,
+                                      bool per, int f, double* w, bool* v)
+{
+    const int stride = ST > 0 ? ST : st;
+    if (f >= 3 && f + 2 < n) {
+        const double* pc = c + (f - 3) * stride;
+        const uint8_t* po = ok + (f - 3) * stride;
+#pragma unroll
+        for (int m = 0; m < 6; ++m) {
+            w[m] = __ldg(pc);
+            v[m] = __ldg(po) != 0;
+            pc += stride;
+            po += stride;
+        }
+        return;
+    }
+#pragma unroll
+    for (int m = 0; m < 6; ++m) {
+        int g = f - 3 + m;
+        bool in = true;
+        if (per) g = wrap(g, n); else in = g >= 0 && g < n;
+        w[m] = in ? __ldg(c + g * stride) : 0.0;
+        v[m] = in && __ldg(ok + (in ? g : 0) * stride) != 0;
+    }
+}
+
+// Q times the upwind face value of the stencil (the reference's _wval on the upwind ordering, sigma_baroclinic.py
+// :204-233, 277-297).
+template <bool MIX>
+__device__ __forceinline__ double weno_flux(const double* w, const bool* v, double q, bool z)
+{
+    const bool pos = q >= 0.0;
+    return q * weno5_face<MIX>(pos ? w[0] : w[5], pos ? w[1] : w[4], pos ? w[2] : w[3], pos ? w[3] : w[2],
+                               pos ? w[4] : w[1], pos ? v[0] : v[5], pos ? v[1] : v[4], pos ? v[2] : v[3],
+                               pos ? v[3] : v[2], pos ? v[4] : v[1], z);
+}
+
+// One plane (t, k) of the step as pointers; element offsets below are 32-bit.
+struct FacePlane {
+    const double* __restrict__ c;     // stage field
+    const double* __restrict__ e;     // exterior on open edges (inflow, else the stage field)
+    const double* __restrict__ c0;    // C (donor flux of stage 3)
+    const double* __restrict__ e0;    // exterior of C
+    const uint8_t* __restrict__ ok;
+    const double* __restrict__ qx;
+    const double* __restrict__ qy;
+    double* sx;
+    double* sy;
+    double* tx;
+    double* ty;
+};
+
+// Flux F through x-face f of row j (WENO5 on interior faces, 0 where Q = 0; open edges upstream with the exterior
+// on inflow; closed edges 0) and, for stage 3, the donor flux FL of C through the same face
+// (sigma_baroclinic.py:277-297, 486-494).
+template <bool ZV, bool MIX, bool DONOR>
+__device__ __forceinline__ void x_face(const FacePlane& P, const Shape& s, const Flags& fl, int j, int f, double& F,
+                                       double& FL)
+{
+    const int row = j * s.nx;
+    const bool interior = fl.per_x || (f >= 1 && f <= s.nx - 1);
+    const double q = __ldg(P.qx + j * (s.nx + 1) + ((fl.per_x && f == s.nx) ? 0 : f));
+    F = 0.0;
+    FL = 0.0;
+    if (interior) {
+        if (q != 0.0) {
+            double w[6];
+            bool v[6];
+            line6<1>(P.c + row, P.ok + row, 1, s.nx, fl.per_x, f, w, v);
+            F = weno_flux<MIX>(w, v, q, ZV);
+        }
+        if (DONOR) {
+            const int ff = f == s.nx ? 0 : f;
+            const int fm = ff >= 1 ? ff - 1 : s.nx - 1;          // f >= 1 unless periodic
+            FL = q * (q >= 0 ? __ldg(P.c0 + row + fm) : __ldg(P.c0 + row + ff));
+        }
+        return;
+    }
+    if (f == 0) {
+        if (fl.open_w) {
+            F = q * (q > 0.0 ? P.e[row] : P.c[row]);
+            if (DONOR) FL = q * (q > 0 ? __ldg(P.e0 + row) : __ldg(P.c0 + row));
+        }
+    } else if (fl.open_e) {
+        F = q * (q < 0.0 ? P.e[row + s.nx - 1] : P.c[row + s.nx - 1]);
+        if (DONOR) FL = q * (q < 0 ? __ldg(P.e0 + row + s.nx - 1) : __ldg(P.c0 + row + s.nx - 1));
+    }
+}
+
+template <bool ZV, bool MIX, bool DONOR>
+__device__ __forceinline__ void y_face(const FacePlane& P, const Shape& s, const Flags& fl, int f, int i, double& F,
+                                       double& FL)
+{
+    const bool interior = fl.per_y || (f >= 1 && f <= s.ny - 1);
+    const double q = __ldg(P.qy + ((fl.per_y && f == s.ny) ? 0 : f) * s.nx + i);
+    F = 0.0;
+    FL = 0.0;
+    if (interior) {
+        if (q != 0.0) {
+            double w[6];
+            bool v[6];
+            line6<0>(P.c + i, P.ok + i, s.nx, s.ny, fl.per_y, f, w, v);
+            F = weno_flux<MIX>(w, v, q, ZV);
+        }
+        if (DONOR) {
+            const int ff = f == s.ny ? 0 : f;
+            const int fm = ff >= 1 ? ff - 1 : s.ny - 1;
+            FL = q * (q >= 0 ? __ldg(P.c0 + fm * s.nx + i) : __ldg(P.c0 + ff * s.nx + i));
+        }
+        return;
+    }
+    if (f == 0) {
+        if (fl.open_s) {
+            F = q * (q > 0.0 ? P.e[i] : P.c[i]);
+            if (DONOR) FL = q * (q > 0 ? __ldg(P.e0 + i) : __ldg(P.c0 + i));
+        }
+    } else if (fl.open_n) {
+        const int o = (s.ny - 1) * s.nx + i;
+        F = q * (q < 0.0 ? P.e[o] : P.c[o]);
+        if (DONOR) FL = q * (q < 0 ? __ldg(P.e0 + o) : __ldg(P.c0 + o));
+    }
+}
+
+// Store the stage's quantity of one face (S, T: the face arrays of this plane; s0, t0: their old values, read
+// before the face computation so the loads overlap it).
+template <int STAGE>
+__device__ __forceinline__ void put_face(double* S, double* T, int fo, double F, double FL, double s0, double t0)
+{
+    if (STAGE == 1) {
+        S[fo] = F;
+    } else if (STAGE == 2) {
+        T[fo] = F;
+    } else {
+        S[fo] = (div6_exact(s0 + t0) + div3_exact(2.0 * F)) - FL;
+        T[fo] = FL;
+    }
+}
+
+// Face pass of stage STAGE for cell (t, k, j, i); blocks are 32 x TJR cells of one (t, k) plane, planes k-major (the
+// tracers of a layer in a row share the layer's transports in L2).
+template <int STAGE, bool ZV, bool MIX>
+__device__ __forceinline__ void faces_body(const StepArgs& a, int t, int k, int i, int j)
+{
+    const Shape s = a.s;
+    const Flags fl(a.flags);
+    if (i >= s.nx || j >= s.ny) return;
+    const i64 pc = s.cell(t, k, 0, 0);
+    FacePlane P;
+    P.c = stage_field<STAGE>(a) + pc;
+    P.e = a.inflow ? a.inflow + pc : P.c;
+    P.c0 = a.C + pc;
+    P.e0 = a.inflow ? a.inflow + pc : P.c0;
+    P.ok = a.ok + s.geo(k, 0, 0);
+    P.qx = a.Qx + s.qx(k, 0, 0);
+    P.qy = a.Qy + s.qy(k, 0, 0);
+    P.sx = a.Sx + s.ux(t, k, 0, 0);
+    P.sy = a.Sy + s.vy(t, k, 0, 0);
+    P.tx = a.Tx + s.ux(t, k, 0, 0);
+    P.ty = a.Ty + s.vy(t, k, 0, 0);
+    const int fxo = j * (s.nx + 1) + i, fyo = j * s.nx + i;
+    const bool last_x = i == s.nx - 1, last_y = j == s.ny - 1;
+    double sxw = 0.0, txw = 0.0, sys = 0.0, tys = 0.0, sxe = 0.0, txe = 0.0, syn = 0.0, tyn = 0.0;
+    if (STAGE == 3) {
+        sxw = P.sx[fxo]; txw = P.tx[fxo];
+        sys = P.sy[fyo]; tys = P.ty[fyo];
+        if (last_x) { sxe = P.sx[fxo + 1]; txe = P.tx[fxo + 1]; }
+        if (last_y) { syn = P.sy[fyo + s.nx]; tyn = P.ty[fyo + s.nx]; }
+    }
+    double fw, lw, fs, ls;
+    x_face<ZV, MIX, STAGE == 3>(P, s, fl, j, i, fw, lw);
+    y_face<ZV, MIX, STAGE == 3>(P, s, fl, j, i, fs, ls);
+    put_face<STAGE>(P.sx, P.tx, fxo, fw, lw, sxw, txw);
+    put_face<STAGE>(P.sy, P.ty, fyo, fs, ls, sys, tys);
+    if (last_x) {
+        double fe, le;
+        x_face<ZV, MIX, STAGE == 3>(P, s, fl, j, s.nx, fe, le);
+        put_face<STAGE>(P.sx, P.tx, fxo + 1, fe, le, sxe, txe);
+    }
+    if (last_y) {
+        double fn, ln;
+        y_face<ZV, MIX, STAGE == 3>(P, s, fl, s.ny, i, fn, ln);
+        put_face<STAGE>(P.sy, P.ty, fyo + s.nx, fn, ln, syn, tyn);
+    }
+}
+
+template <int STAGE, bool ZV, bool MIX, int TJR>
+__global__ void __launch_bounds__(TI * TJR) fct_faces_kernel(StepArgs a)
+{
+    const int p = blockIdx.z, k = p / a.s.nt, t = p - k * a.s.nt;
+    faces_body<STAGE, ZV, MIX>(a, t, k, blockIdx.x * TI + threadIdx.x % TI, blockIdx.y * TJR + threadIdx.x / TI);
+}
+
+// Domain, plane and cell of a thread of a batched stage pass: domain d owns CTAs off[d] .. off[d+1]-1, each one
+// 32 x TJR tile of one (t, k) plane (k-major).
+template <int TJR>
+__device__ __forceinline__ int batched_plane_tile(const BatchDomain* __restrict__ doms, const int* __restrict__ off,
+                                                  int ndom, int& t, int& k, int& i, int& j)
+{
+    const int d = find_domain(off, ndom, blockIdx.x);
+    const Shape s = doms[d].a.s;
+    const int tx = ceil_div(s.nx, TI), ty = ceil_div(s.ny, TJR);
+    int local = blockIdx.x - __ldg(off + d);
+    const int p = local / (tx * ty);
+    local -= p * tx * ty;
+    k = p / s.nt;
+    t = p - k * s.nt;
+    const int by = local / tx, bx = local - by * tx;
+    i = bx * TI + threadIdx.x % TI;
+    j = by * TJR + threadIdx.x / TI;
+    return d;
+}
+
+template <int STAGE, bool ZV, bool MIX, int TJR>
+__global__ void __launch_bounds__(TI * TJR) fct_faces_batched(const BatchDomain* __restrict__ doms,
+                                                              const int* __restrict__ off, int ndom)
+{
+    int t, k, i, j;
+    const int d = batched_plane_tile<TJR>(doms, off, ndom, t, k, i, j);
+    const StepArgs a = doms[d].a;
+    faces_body<STAGE, ZV, MIX>(a, t, k, i, j);
+}
+
+// Cell pass of stage STAGE (sigma_baroclinic.py:452-468 `_fct_stage`; stage 3: c_L of `_fct_fluxes` :509-511).
+template <int STAGE>
+__device__ __forceinline__ void update_body(const StepArgs& a, int t, int k, int i, int j)
+{
+    const Shape s = a.s;
+    if (i >= s.nx || j >= s.ny) return;
+    const i64 w = s.ux(t, k, j, i), so = s.vy(t, k, j, i), g = s.geo(k, j, i), cc = s.cell(t, k, j, i);
+    const double v0 = __ldg(a.V0 + g), v1 = __ldg(a.V1 + g), c0 = __ldg(a.C + cc);
+    const double q0 = v0 * c0;
+    if (STAGE == 1) {
+        const double d = a.Sx[w + 1] - a.Sx[w] + a.Sy[so + s.nx] - a.Sy[so];
+        const double q = 0.0 * q0 + 1.0 * (q0 - a.dt * d);
+        const double v = v0 + (v1 - v0);
+        a.c1[cc] = v > 0.0 ? q / v : c0;
+    } else if (STAGE == 2) {
+        const double d0 = a.Sx[w + 1] - a.Sx[w] + a.Sy[so + s.nx] - a.Sy[so];
+        const double d = a.Tx[w + 1] - a.Tx[w] + a.Ty[so + s.nx] - a.Ty[so];
+        const double q1 = 0.0 * q0 + 1.0 * (q0 - a.dt * d0);
+        const double q = 0.75 * q0 + 0.25 * (q1 - a.dt * d);
+        const double v = v0 + 0.5 * (v1 - v0);
+        a.c2[cc] = v > 0.0 ? q / v : c0;
+    } else {
+        const double dl = a.Tx[w + 1] - a.Tx[w] + a.Ty[so + s.nx] - a.Ty[so];
+        const double q = 0.0 * q0 + 1.0 * (q0 - a.dt * dl);
+        a.q1[cc] = v1 > 0 ? q / v1 : c0;            // c_L
+    }
+}
+
+template <int STAGE, int TJR>
+__global__ void __launch_bounds__(TI * TJR) fct_update_kernel(StepArgs a)
+{
+    const int p = blockIdx.z, k = p / a.s.nt, t = p - k * a.s.nt;
+    update_body<STAGE>(a, t, k, blockIdx.x * TI + threadIdx.x % TI, blockIdx.y * TJR + threadIdx.x / TI);
+}
+
+template <int STAGE, int TJR>
+__global__ void __launch_bounds__(TI * TJR) fct_update_batched(const BatchDomain* __restrict__ doms,
+                                                               const int* __restrict__ off, int ndom)
+{
+    int t, k, i, j;
+    const int d = batched_plane_tile<TJR>(doms, off, ndom, t, k, i, j);
+    const StepArgs a = doms[d].a;
+    update_body<STAGE>(a, t, k, i, j);
+}
+
+}  // namespace po

@@ -91,7 +91,7 @@ class Server:
 
     def __init__(self, device=None, mixed: bool = True, batched: bool = True, max_slots: int = 256,
                  hbm_budget: int | None = None, max_ahead: int = 3, max_steps_per_iter: int = 4,
-                 seglen: int = 64, remap_nf: int = 2, keep_results: bool = False) -> None:
+                 tile_rows: int = 8, remap_nf: int = 2, keep_results: bool = False) -> None:
         self.device = torch.device("cuda", torch.cuda.current_device()) if device is None else torch.device(device)
         self.mixed, self.batched = bool(mixed), bool(batched)
         self.max_slots = 1 if not batched else int(max_slots)
@@ -100,7 +100,7 @@ class Server:
             hbm_budget = int(0.6 * free)
         self.hbm_budget = int(hbm_budget)
         self.max_ahead, self.kmax = int(max_ahead), int(max_steps_per_iter)
-        self.seglen, self.remap_nf = int(seglen), int(remap_nf)
+        self.tile_rows, self.remap_nf = int(tile_rows), int(remap_nf)
         self.keep_results = bool(keep_results)
 
     def run(self, jobs: list[Job], clock=time.perf_counter) -> dict:
@@ -150,7 +150,7 @@ class Server:
             k = min(self.kmax, min(j.steps - j.done_steps for j in active))
             if self.batched:
                 if changed or plan is None:
-                    plan = _Plan([j.dom.as_struct(swapped=bool(j.flip)) for j in active], self.seglen, dev,
+                    plan = _Plan([j.dom.as_struct(swapped=bool(j.flip)) for j in active], self.tile_rows, dev,
                                  buf=plan_buf, stream=stream.cuda_stream)
                     parity = 0
                 for _ in range(k):
@@ -161,7 +161,7 @@ class Server:
                 for j in active:
                     for s in range(k):
                         sequential_step([j.dom], j.flip ^ (s & 1), mixed=self.mixed, stream=stream.cuda_stream)
-                launches += k * sum(5 + (j.nt >= 2) + (j.nt % 2) + 1 for j in active)
+                launches += k * sum(8 + (j.nt >= 2) + (j.nt % 2) + 1 for j in active)
             iters += 1
             occupancy.append(len(active))
             done = []
@@ -200,8 +200,8 @@ class Server:
 
     def _launches(self, active) -> int:
         if self.remap_nf == 2:
-            return 5 + any(j.nt >= 2 for j in active) + any(j.nt % 2 for j in active) + 1
-        return 7
+            return 8 + any(j.nt >= 2 for j in active) + any(j.nt % 2 for j in active) + 1
+        return 10
 
     def _retire(self, j: Job, stream) -> None:
         """Marks the job done on the device and releases its buffers (stream-ordered: the caching allocator hands

@@ -95,12 +95,12 @@ def test_batch_argument_errors():
     assert L.pocean_batch_device_bytes(0) == 0
     assert L.pocean_batch_device_bytes(64) > L.pocean_batch_device_bytes(1) > 0
     h = ctypes.c_void_p()
-    assert L.pocean_batch_create(8, 1, 64, 256, 1 << 20, None, None) == 1            # no output handle
-    assert L.pocean_batch_create(None, 1, 64, 256, 1 << 20, ctypes.byref(h), None) == 1
-    assert L.pocean_batch_create(8, 0, 64, 256, 1 << 20, ctypes.byref(h), None) == 1
-    assert L.pocean_batch_create(8, 1, 2, 256, 1 << 20, ctypes.byref(h), None) == 1   # segment length
-    assert L.pocean_batch_create(8, 1, 64, 256, 16, ctypes.byref(h), None) == 2      # plan buffer too small
-    assert L.pocean_batch_create(8, 1, 64, 264, 1 << 20, ctypes.byref(h), None) == 2  # misaligned
+    assert L.pocean_batch_create(8, 1, 8, 256, 1 << 20, None, None) == 1             # no output handle
+    assert L.pocean_batch_create(None, 1, 8, 256, 1 << 20, ctypes.byref(h), None) == 1
+    assert L.pocean_batch_create(8, 0, 8, 256, 1 << 20, ctypes.byref(h), None) == 1
+    assert L.pocean_batch_create(8, 1, 5, 256, 1 << 20, ctypes.byref(h), None) == 1   # tile rows
+    assert L.pocean_batch_create(8, 1, 8, 256, 16, ctypes.byref(h), None) == 2       # plan buffer too small
+    assert L.pocean_batch_create(8, 1, 8, 264, 1 << 20, ctypes.byref(h), None) == 2   # misaligned
     assert h.value is None
     assert L.pocean_batch_step(None, 0, 2, 0, None) == 1
 

@@ -59,9 +59,9 @@ def expected(dev):
     return [_alone(d, STEPS) for d in _domains(dev)]
 
 
-@pytest.mark.parametrize("seglen,nf", [(16, 1), (32, 2), (64, 2), (128, 1)])
-def test_batched_equals_each_domain_alone(dev, expected, seglen, nf):
-    b = DomainBatch(_domains(dev), seglen=seglen, remap_nf=nf)
+@pytest.mark.parametrize("tile_rows,nf", [(4, 1), (8, 2), (16, 2), (16, 1)])
+def test_batched_equals_each_domain_alone(dev, expected, tile_rows, nf):
+    b = DomainBatch(_domains(dev), tile_rows=tile_rows, remap_nf=nf)
     b.step(STEPS)
     torch.cuda.synchronize()
     for i, ref in enumerate(expected):
@@ -93,8 +93,8 @@ def test_mixed_batch_equals_mixed_alone(dev):
 def test_autotune_keeps_state_and_results(dev, expected):
     b = DomainBatch(_domains(dev))
     before = [b.state(i).clone() for i in range(len(b.domains))]
-    cfg = b.autotune(steps=1, seglens=(16, 64), nfs=(1, 2))
-    assert cfg["seglen"] in (16, 64) and cfg["remap_nf"] in (1, 2) and len(cfg["ms_per_step"]) == 4
+    cfg = b.autotune(steps=1, tile_rows=(4, 16), nfs=(1, 2))
+    assert cfg["tile_rows"] in (4, 16) and cfg["remap_nf"] in (1, 2) and len(cfg["ms_per_step"]) == 4
     for i, s in enumerate(before):
         assert torch.equal(b.state(i), s)
     b.step(STEPS)
@@ -114,7 +114,7 @@ def test_js_batch_equals_js_alone(dev):
     ds = _domains(dev)
     for d in ds:
         d.flags |= _lib.WENO_JS
-    b = DomainBatch(ds, seglen=32)
+    b = DomainBatch(ds, tile_rows=4)
     b.step(2)
     torch.cuda.synchronize()
     for i, d in enumerate(_domains(dev)):
