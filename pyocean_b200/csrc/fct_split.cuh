@@ -6,7 +6,8 @@
 // at high occupancy and the two independent WENO5 chains of a thread overlap.  Cell pass of stage s: the stage
 // update from the stored faces.  Faces per stage are stored once:
 //   stage 1: S <- F0;  stage 2: T <- F1;  stage 3: S <- A = ((F0 + F1)/6 + 2 F2/3) - F_L and T <- F_L,
-// with (F0 + F1)/6 and 2 F2/3 formed by the same exact divisions as the reference.  The arithmetic of every face and
+// with (F0 + F1)/6 and 2 F2/3 formed by the same exact divisions as the reference (storing F_L was measured 3 %
+// faster than recomputing it in the stage-3 cell pass).  The arithmetic of every face and
 // update is the reference's (weno.cuh; sigma_baroclinic.py:265-321, 452-511), so results equal the reference's bit
 // for bit.  Addresses are formed once per thread as plane pointers with 32-bit offsets; interior stencils (all six
 // cells inside the domain, the common case) load with fixed offsets, edge and periodic stencils take a guarded path.
@@ -209,8 +210,15 @@ __device__ __forceinline__ void faces_body(const StepArgs& a, int t, int k, int 
     }
 }
 
+// Register budget of the face passes: ptxas's own choice for TI * TJR threads (a minimum-blocks bound of 1 lets it
+// take up to 255 registers and is slower); POCEAN_FACES_MINB sets the resident blocks per SM when defined.
+#ifdef POCEAN_FACES_MINB
+#define FACES_BOUNDS(n) __launch_bounds__(n, POCEAN_FACES_MINB)
+#else
+#define FACES_BOUNDS(n) __launch_bounds__(n)
+#endif
 template <int STAGE, bool ZV, bool MIX, int TJR>
-__global__ void __launch_bounds__(TI * TJR) fct_faces_kernel(StepArgs a)
+__global__ void FACES_BOUNDS(TI * TJR) fct_faces_kernel(StepArgs a)
 {
     const int p = blockIdx.z, k = p / a.s.nt, t = p - k * a.s.nt;
     faces_body<STAGE, ZV, MIX>(a, t, k, blockIdx.x * TI + threadIdx.x % TI, blockIdx.y * TJR + threadIdx.x / TI);
