@@ -625,20 +625,26 @@ static int common_checks(const char* fn, const void* C, const void* V0, const vo
     return pocean_check_device();
 }
 
+// Rows of the 32-wide cell tiles of the single-domain stage passes.
+#ifndef POCEAN_FACE_ROWS
+#define POCEAN_FACE_ROWS 8
+#endif
+
 template <bool ZV, bool MIX>
 static void launch_split(const StepArgs& a, int stage, cudaStream_t st)
 {
+    constexpr int R = POCEAN_FACE_ROWS;
     const Shape& s = a.s;
-    const dim3 grid(ceil_div(s.nx, TI), ceil_div(s.ny, TJ), s.nt * s.n);
+    const dim3 grid(ceil_div(s.nx, TI), ceil_div(s.ny, R), s.nt * s.n);
     if (stage == 1) {
-        fct_faces_kernel<1, ZV, MIX, TJ><<<grid, TI * TJ, 0, st>>>(a);
-        fct_update_kernel<1, TJ><<<grid, TI * TJ, 0, st>>>(a);
+        fct_faces_kernel<1, ZV, MIX, R><<<grid, TI * R, 0, st>>>(a);
+        fct_update_kernel<1, R><<<grid, TI * R, 0, st>>>(a);
     } else if (stage == 2) {
-        fct_faces_kernel<2, ZV, MIX, TJ><<<grid, TI * TJ, 0, st>>>(a);
-        fct_update_kernel<2, TJ><<<grid, TI * TJ, 0, st>>>(a);
+        fct_faces_kernel<2, ZV, MIX, R><<<grid, TI * R, 0, st>>>(a);
+        fct_update_kernel<2, R><<<grid, TI * R, 0, st>>>(a);
     } else {
-        fct_faces_kernel<3, ZV, MIX, TJ><<<grid, TI * TJ, 0, st>>>(a);
-        fct_update_kernel<3, TJ><<<grid, TI * TJ, 0, st>>>(a);
+        fct_faces3_kernel<ZV, MIX, R><<<grid, TI * R, 0, st>>>(a);
+        fct_update_kernel<3, R><<<grid, TI * R, 0, st>>>(a);
     }
 }
 
@@ -700,7 +706,7 @@ static void fct_batched_stages(const BatchDomain* doms, const int* po, unsigned 
     fct_update_batched<1, TJR><<<np, TI * TJR, 0, st>>>(doms, po, ndom);
     fct_faces_batched<2, ZV, MIX, TJR><<<np, TI * TJR, 0, st>>>(doms, po, ndom);
     fct_update_batched<2, TJR><<<np, TI * TJR, 0, st>>>(doms, po, ndom);
-    fct_faces_batched<3, ZV, MIX, TJR><<<np, TI * TJR, 0, st>>>(doms, po, ndom);
+    fct_faces3_batched<ZV, MIX, TJR><<<np, TI * TJR, 0, st>>>(doms, po, ndom);
     fct_update_batched<3, TJR><<<np, TI * TJR, 0, st>>>(doms, po, ndom);
 }
 

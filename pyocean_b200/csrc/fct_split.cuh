@@ -210,18 +210,34 @@ __device__ __forceinline__ void faces_body(const StepArgs& a, int t, int k, int 
     }
 }
 
-// Register budget of the face passes: ptxas's own choice for TI * TJR threads (a minimum-blocks bound of 1 lets it
-// take up to 255 registers and is slower); POCEAN_FACES_MINB sets the resident blocks per SM when defined.
-#ifdef POCEAN_FACES_MINB
-#define FACES_BOUNDS(n) __launch_bounds__(n, POCEAN_FACES_MINB)
-#else
-#define FACES_BOUNDS(n) __launch_bounds__(n)
+// Register budget of the face passes, as resident 256-thread blocks per SM (scaled for other block sizes): stages
+// 1-2 at 6 (42 registers), stage 3 at 5 (51 registers).  Measured at 512 x 512 x 50: 8.5 % faster than ptxas's
+// own choice (58 / 80 registers), whose lower occupancy left the FP64 chains and the stencil loads exposed.
+#ifndef POCEAN_FACES12_MINB
+#define POCEAN_FACES12_MINB 6
 #endif
+#ifndef POCEAN_FACES3_MINB
+#define POCEAN_FACES3_MINB 5
+#endif
+#define FACES12_BOUNDS(n) __launch_bounds__(n, POCEAN_FACES12_MINB * 256 / (n))
+#define FACES3_BOUNDS(n) __launch_bounds__(n, POCEAN_FACES3_MINB * 256 / (n))
 template <int STAGE, bool ZV, bool MIX, int TJR>
-__global__ void FACES_BOUNDS(TI * TJR) fct_faces_kernel(StepArgs a)
+__device__ __forceinline__ void faces_plane(const StepArgs& a)
 {
     const int p = blockIdx.z, k = p / a.s.nt, t = p - k * a.s.nt;
     faces_body<STAGE, ZV, MIX>(a, t, k, blockIdx.x * TI + threadIdx.x % TI, blockIdx.y * TJR + threadIdx.x / TI);
+}
+
+template <int STAGE, bool ZV, bool MIX, int TJR>
+__global__ void FACES12_BOUNDS(TI * TJR) fct_faces_kernel(StepArgs a)
+{
+    faces_plane<STAGE, ZV, MIX, TJR>(a);
+}
+
+template <bool ZV, bool MIX, int TJR>
+__global__ void FACES3_BOUNDS(TI * TJR) fct_faces3_kernel(StepArgs a)
+{
+    faces_plane<3, ZV, MIX, TJR>(a);
 }
 
 // Domain, plane and cell of a thread of a batched stage pass: domain d owns CTAs off[d] .. off[d+1]-1, each one
@@ -245,13 +261,27 @@ __device__ __forceinline__ int batched_plane_tile(const BatchDomain* __restrict_
 }
 
 template <int STAGE, bool ZV, bool MIX, int TJR>
-__global__ void __launch_bounds__(TI * TJR) fct_faces_batched(const BatchDomain* __restrict__ doms,
-                                                              const int* __restrict__ off, int ndom)
+__device__ __forceinline__ void faces_batched_body(const BatchDomain* __restrict__ doms, const int* __restrict__ off,
+                                                   int ndom)
 {
     int t, k, i, j;
     const int d = batched_plane_tile<TJR>(doms, off, ndom, t, k, i, j);
     const StepArgs a = doms[d].a;
     faces_body<STAGE, ZV, MIX>(a, t, k, i, j);
+}
+
+template <int STAGE, bool ZV, bool MIX, int TJR>
+__global__ void FACES12_BOUNDS(TI * TJR) fct_faces_batched(const BatchDomain* __restrict__ doms,
+                                                           const int* __restrict__ off, int ndom)
+{
+    faces_batched_body<STAGE, ZV, MIX, TJR>(doms, off, ndom);
+}
+
+template <bool ZV, bool MIX, int TJR>
+__global__ void FACES3_BOUNDS(TI * TJR) fct_faces3_batched(const BatchDomain* __restrict__ doms,
+                                                           const int* __restrict__ off, int ndom)
+{
+    faces_batched_body<3, ZV, MIX, TJR>(doms, off, ndom);
 }
 
 // Cell pass of stage STAGE (sigma_baroclinic.py:452-468 `_fct_stage`; stage 3: c_L of `_fct_fluxes` :509-511).
