@@ -404,7 +404,8 @@ __global__ void COEFF_BOUNDS fct_coeff_batched(const BatchDomain* __restrict__ d
 {
     int d, i, j, k;
     batched_tile(doms, off, ndom, d, i, j, k);
-    const StepArgs a = doms[d].a;
+    __shared__ StepArgs sh;
+    const StepArgs& a = block_args(doms, d, sh);
     coeff_body(a, i, j, k);
 }
 
@@ -413,7 +414,8 @@ __global__ void FINAL_BOUNDS fct_final_batched(const BatchDomain* __restrict__ d
 {
     int d, i, j, k;
     batched_tile(doms, off, ndom, d, i, j, k);
-    const StepArgs a = doms[d].a;
+    __shared__ StepArgs sh;
+    const StepArgs& a = block_args(doms, d, sh);
     final_body(a, i, j, k);
 }
 

@@ -70,6 +70,20 @@ __device__ __forceinline__ int find_domain(const int* __restrict__ off, int ndom
     return lo;
 }
 
+// The argument block of the block's domain, copied once into shared memory (every thread of a batched CTA works on
+// the same domain; reading the block from there is cheaper than a per-thread copy of ~200 bytes).  Call before any
+// thread returns: it contains a block barrier.
+__device__ __forceinline__ const StepArgs& block_args(const BatchDomain* __restrict__ doms, int d, StepArgs& sh)
+{
+    static_assert(sizeof(StepArgs) % sizeof(unsigned long long) == 0, "StepArgs is copied in 8-byte words");
+    constexpr int W = sizeof(StepArgs) / sizeof(unsigned long long);
+    const unsigned long long* src = reinterpret_cast<const unsigned long long*>(&doms[d].a);
+    unsigned long long* dst = reinterpret_cast<unsigned long long*>(&sh);
+    for (int w = threadIdx.x; w < W; w += blockDim.x) dst[w] = __ldg(src + w);
+    __syncthreads();
+    return sh;
+}
+
 // The FCT workspace cut into a's buffers (advect.cu).
 void carve_fct_workspace(StepArgs& a, void* workspace);
 

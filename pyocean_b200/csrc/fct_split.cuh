@@ -266,7 +266,8 @@ __device__ __forceinline__ void faces_batched_body(const BatchDomain* __restrict
 {
     int t, k, i, j;
     const int d = batched_plane_tile<TJR>(doms, off, ndom, t, k, i, j);
-    const StepArgs a = doms[d].a;
+    __shared__ StepArgs sh;
+    const StepArgs& a = block_args(doms, d, sh);
     faces_body<STAGE, ZV, MIX>(a, t, k, i, j);
 }
 
@@ -325,7 +326,8 @@ __global__ void __launch_bounds__(TI * TJR) fct_update_batched(const BatchDomain
 {
     int t, k, i, j;
     const int d = batched_plane_tile<TJR>(doms, off, ndom, t, k, i, j);
-    const StepArgs a = doms[d].a;
+    __shared__ StepArgs sh;
+    const StepArgs& a = block_args(doms, d, sh);
     update_body<STAGE>(a, t, k, i, j);
 }
 
