@@ -15,7 +15,8 @@ kernels with the reference's call signatures:
 * ``Periodic`` — ``core/model/periodic.py:31, 47-94`` (pad/crop with ``TRACER_HALO`` wrapped cells).
 * ``remap_column`` / ``remap_columns`` / ``reconstruct`` — ``core/vertical/remap.py:234-427``.
 * ``regrid`` / ``regrid_remap`` — the z* and sigma rules of ``core/vertical/regrid.py:44-98, 309-395`` as
-  ``ALECoordinate.regrid_remap`` uses them (``core/components/vertical_coordinate.py:69-111``).
+  ``ALECoordinate.regrid_remap`` uses them (``core/components/vertical_coordinate.py:69-111``); ``regrid_hybrid``
+  the hybrid (HYCOM1) rule of ``core/vertical/regrid.py:100-289, 309-342``.
 * ``diffuse_ale`` — ``_diffuse_ale_kernel`` (``core/dynamics/sigma_baroclinic.py:533-561``) with the pad/crop of
   ``TracerAdvection.diffuse_h`` (``core/components/tracers.py:421-447``).
 * ``face_fractions`` / ``remap_faces`` — ``core/vertical/ale.py:883-902`` and
@@ -67,6 +68,8 @@ def lib() -> ctypes.CDLL:
         L.oracle_remap_columns.argtypes = [_D, _D, _D, i, i, i, i, i, _U8, _D]
         L.oracle_regrid.argtypes = [i, _D, _D, _D, _U8, _D, d, i, i, i, _D, _U8]
         L.oracle_regrid.restype = i
+        L.oracle_regrid_hybrid.argtypes = [_D, _D, _D, _U8, _D, _D, _D, _D, _D, d, d, d, i, i, i, i, _D, _U8]
+        L.oracle_regrid_hybrid.restype = i
         L.oracle_diffuse_ale.argtypes = [_D, _D, _D, _U8, _D, _D, _U8, _U8, _D, d, d, i, i, i, _D]
         L.oracle_face_fractions.argtypes = [_D, i, i, i, _D]
         L.oracle_ftt.argtypes = [_D, _D, _U8, i, i, i, i, _D, _D]
@@ -414,6 +417,24 @@ def regrid(rule: str, H, eta, h_src, active, coord, h_min: float = H_MIN):
     bad = lib().oracle_regrid(RULES[rule], _p(_f64(H)), _p(_f64(eta)), _p(h_src),
                               _pu8(_u8(np.broadcast_to(active, (ny, nx)))), _p(_f64(coord)), float(h_min), n, ny,
                               nx, _p(h_new), _pu8(wet))
+    return h_new, wet.view(bool), int(bad)
+
+
+def regrid_hybrid(H, eta, h_src, active, rho, params: dict):
+    """The hybrid rule of ``_regrid_columns`` (regrid.py:309-342) as ``ALECoordinate.regrid`` uses it (n_out = the
+    source layer count): (h_new, wet, bad)."""
+    h_src = _f64(h_src)
+    n, ny, nx = h_src.shape
+    f = lambda key, default: _f64(params.get(key, default))                        # noqa: E731
+    h_new = np.empty_like(h_src)
+    wet = np.empty((ny, nx), np.uint8)
+    bad = lib().oracle_regrid_hybrid(_p(_f64(H)), _p(_f64(eta)), _p(h_src),
+                                     _pu8(_u8(np.broadcast_to(active, (ny, nx)))), _p(_f64(rho)),
+                                     _p(f("rho_target", np.zeros(n + 1))), _p(f("dz_top", np.ones(n))),
+                                     _p(f("max_h_top", np.full(n, np.inf))), _p(f("dsigma", np.full(n, 1.0 / n))),
+                                     float(params.get("d_sigma", 0.0)), float(params.get("d_hybrid", 0.0)),
+                                     float(params.get("h_min", H_MIN)), int(bool(params.get("keep_isopycnal", True))),
+                                     n, ny, nx, _p(h_new), _pu8(wet))
     return h_new, wet.view(bool), int(bad)
 
 

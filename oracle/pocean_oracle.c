@@ -831,6 +831,219 @@ int oracle_regrid(int rule, const double* Hin, const double* eta, const double* 
     return bad;
 }
 
+/* regrid.py:100-154 `_p1m_h2_positions`: depths (0 at the surface) of the m+1 target interface densities in a
+ * column of n layers (h, rho surface first); e holds 2n doubles, xg n+1. */
+static void p1m_h2_positions(const double* h, const double* rho, int n, const double* targets, int m, double* x,
+                             double* e, double* xg)
+{
+    e[0] = rho[0];
+    e[2 * (n - 1) + 1] = rho[n - 1];
+    for (int k = 1; k < n; ++k) {
+        if (h[k - 1] + h[k] == 0.0) e[2 * k] = 0.5 * (rho[k - 1] + rho[k]);
+        else e[2 * k] = (rho[k - 1] * h[k] + rho[k] * h[k - 1]) / (h[k - 1] + h[k]);
+        e[2 * (k - 1) + 1] = e[2 * k];
+    }
+    bound_edges(h, rho, n, e);
+    for (int k = 0; k < n - 1; ++k)
+        if (e[2 * k + 1] != e[2 * (k + 1)]) {
+            const double a = 0.5 * (e[2 * k + 1] + e[2 * (k + 1)]);
+            e[2 * k + 1] = a;
+            e[2 * (k + 1)] = a;
+        }
+    xg[0] = 0.0;
+    for (int k = 0; k < n; ++k) xg[k + 1] = xg[k] + h[k];
+    for (int k = 0; k <= m; ++k) x[k] = m == n ? xg[k] : xg[n] * k / m;
+    for (int kk = 1; kk < m; ++kk) {
+        const double t = targets[kk];
+        if (t <= e[0]) {
+            x[kk] = xg[0];
+            continue;
+        }
+        int found = 0;
+        for (int k = 1; k < n; ++k)
+            if (t >= e[2 * (k - 1) + 1] && t <= e[2 * k]) {
+                x[kk] = xg[k];
+                found = 1;
+                break;
+            }
+        if (found) continue;
+        if (t >= e[2 * (n - 1) + 1]) {
+            x[kk] = xg[n];
+            continue;
+        }
+        for (int k = 0; k < n; ++k)
+            if (e[2 * k] < t && t < e[2 * k + 1]) {
+                const double xi = (t - e[2 * k]) / (e[2 * k + 1] - e[2 * k]);
+                x[kk] = xg[k] + pmin(pmax(xi, 0.0), 1.0) * h[k];
+                break;
+            }
+    }
+}
+
+/* regrid.py:158-201 `_keep_consistent` (x: n+1 depths, overwritten); xg n+1, ok / kept scratch. */
+static void keep_consistent(const double* h, const double* rho, int n, const double* targets, double h_mass, double* x,
+                            double* xg, uint8_t* ok, uint8_t* kept)
+{
+    for (int j = 0; j < n; ++j) ok[j] = h[j] < h_mass || (targets[j] <= rho[j] && rho[j] <= targets[j + 1]);
+    xg[0] = 0.0;
+    for (int j = 0; j < n; ++j) xg[j + 1] = xg[j] + h[j];
+    for (int j = 0; j <= n; ++j) kept[j] = 0;
+    kept[0] = kept[n] = 1;
+    for (int j = 1; j < n; ++j) {
+        const int straddle = h[j - 1] >= h_mass && h[j] >= h_mass && rho[j - 1] <= targets[j] && targets[j] <= rho[j];
+        if ((ok[j - 1] && ok[j]) || straddle) {
+            x[j] = xg[j];
+            kept[j] = 1;
+        }
+    }
+    double lo = xg[0];
+    for (int j = 1; j < n; ++j) {
+        if (kept[j]) lo = x[j];
+        else if (x[j] < lo) x[j] = lo;
+    }
+    double hi = xg[n];
+    for (int j = n - 1; j > 0; --j) {
+        if (kept[j]) hi = x[j];
+        else if (x[j] > hi) x[j] = hi;
+    }
+}
+
+/* regrid.py:204-252 `hycom1_column` with n == m (target grid = source layer count); zw bed first (n+1).
+ * work: >= 8n+8 doubles, bwork >= 2n+2 bytes. */
+static void hycom1_column(double H, double eta, const double* h_bed, const double* rho_bed, const double* rho_target,
+                          const double* dz_top, const double* max_h_top, double h_min, int keep, int n, double* zw,
+                          double* work, uint8_t* bwork)
+{
+    const int m = n;
+    const double D = H + eta;
+    double* h_top = work;
+    double* rho_own = h_top + n;
+    double* rho = rho_own + n;
+    double* x = rho + n;                 /* m+1 */
+    double* e = x + m + 1;               /* 2n */
+    double* xg = e + 2 * n;              /* n+1 */
+    for (int k = 0; k < n; ++k) {
+        h_top[k] = h_bed[n - 1 - k];
+        rho_own[k] = rho_bed[n - 1 - k];
+        rho[k] = rho_own[k];
+    }
+    const double h_mass = 2.0 * h_min;
+    double last = -1.0;
+    for (int k = 0; k < n; ++k) {
+        if (h_top[k] >= h_mass) last = rho[k];
+        else if (last >= 0.0) rho[k] = last;
+    }
+    int k0 = 0;
+    for (k0 = 0; k0 < n; ++k0)
+        if (h_top[k0] >= h_mass) break;
+    if (k0 == n) k0 = n - 1;             /* the loop variable's last value when nothing breaks */
+    if (k0 > 0 && h_top[k0] >= h_mass)
+        for (int kk = 0; kk < k0; ++kk) rho[kk] = rho[k0];
+    for (int k = n - 2; k >= 0; --k) rho[k] = pmin(rho[k], rho[k + 1]);
+    p1m_h2_positions(h_top, rho, n, rho_target, m, x, e, xg);
+    if (keep) keep_consistent(h_top, rho_own, n, rho_target, 2.0 * h_min, x, xg, bwork, bwork + n + 1);
+    const double s = D / H;
+    double nominal = 0.0;
+    for (int k = 1; k <= m; ++k) {
+        nominal += dz_top[k - 1] * s;
+        x[k] = pmin(pmax(x[k], nominal), D);
+    }
+    for (int k = 1; k < m; ++k) x[k] = pmin(x[k], x[k - 1] + max_h_top[k - 1]);
+    for (int k = 1; k <= m; ++k) x[k] = pmax(x[k], x[k - 1]);
+    x[m] = D;
+    for (int j = 0; j <= m; ++j) zw[j] = eta - x[m - j];
+    zw[0] = -H;
+    zw[m] = eta;
+    enforce_min_thickness(zw, m, h_min);
+}
+
+/* regrid.py:255-260 `transition_weight`. */
+static double transition_weight(double D, double d_sigma, double d_hybrid)
+{
+    if (d_hybrid <= d_sigma) return D > d_sigma ? 1.0 : 0.0;
+    return pmin(pmax((D - d_sigma) / (d_hybrid - d_sigma), 0.0), 1.0);
+}
+
+/* regrid.py:263-289 `window_shallow_sigma` into zw (zw_hyb may alias nothing). */
+static void window_shallow_sigma(const double* zw_hyb, const double* zw_sig, const double* zw_zs, double H, double D,
+                                 double d_sigma, double d_hybrid, double h_min, int n, double* zw)
+{
+    const double q = transition_weight(D, d_sigma, d_hybrid);
+    if (q >= 1.0) {
+        for (int j = 0; j <= n; ++j) zw[j] = zw_hyb[j];
+        return;
+    }
+    for (int j = 0; j <= n; ++j) {
+        const double lo = q * (-H) + (1.0 - q) * zw_sig[j];
+        const double hi = q * zw_zs[j] + (1.0 - q) * zw_sig[j];
+        zw[j] = pmin(pmax(zw_hyb[j], lo), hi);
+    }
+    zw[0] = -H;
+    zw[n] = zw_sig[n];
+    enforce_min_thickness(zw, n, h_min);
+}
+
+/*
+ * The hybrid rule of `_regrid_columns` (regrid.py:309-342, code 2) as ALECoordinate.regrid uses it: per column the
+ * wet mask as oracle_regrid, then sigma where the shallow-sigma weight is 0 (or H <= 0 with a sigma zone),
+ * else hycom1_column, windowed towards sigma where 0 < q < 1.  rho (n, ny, nx) bed first; rho_target (n+1) surface
+ * first; dz_top, max_h_top (n) surface first; dsigma (n) bed first.  Returns the number of wet columns that break
+ * the rule's preconditions (H <= 0 without a sigma zone, or a non-finite density), for which the reference raises.
+ */
+int oracle_regrid_hybrid(const double* Hin, const double* eta, const double* h_src, const uint8_t* active,
+                         const double* rho, const double* rho_target, const double* dz_top, const double* max_h_top,
+                         const double* dsigma, double d_sigma, double d_hybrid, double h_min, int keep, int n, int ny,
+                         int nx, double* h_new, uint8_t* wet)
+{
+    const i64 plane = (i64)ny * nx;
+    int bad = 0;
+#pragma omp parallel for reduction(+ : bad)
+    for (i64 c = 0; c < plane; ++c) {
+        const double H = nan_to_num(Hin[c]);
+        double tot = 0.0;
+        for (int k = 0; k < n; ++k) tot += h_src[k * plane + c];
+        const int w = active[c] && (H + eta[c] > 0) && (tot > 0);
+        wet[c] = (uint8_t)w;
+        if (!w) {
+            for (int k = 0; k < n; ++k) h_new[k * plane + c] = h_src[k * plane + c];
+            continue;
+        }
+        double* buf = (double*)malloc((size_t)(16 * n + 32) * sizeof(double));
+        uint8_t* bwork = (uint8_t*)malloc((size_t)(2 * n + 4));
+        double* hb = buf;                      /* n */
+        double* rb = hb + n;                   /* n */
+        double* col = rb + n;                  /* n+1 */
+        double* sig = col + n + 1;             /* n+1 */
+        double* zs = sig + n + 1;              /* n+1 */
+        double* hyb = zs + n + 1;              /* n+1 */
+        double* work = hyb + n + 1;            /* 8n+8 */
+        int finite = 1;
+        for (int k = 0; k < n; ++k) {
+            hb[k] = h_src[k * plane + c];
+            rb[k] = rho[k * plane + c];
+            finite = finite && isfinite(rb[k]);
+        }
+        if (!finite || (d_hybrid <= 0.0 && !(H > 0))) ++bad;
+        const double q = d_hybrid > 0.0 ? transition_weight(H + eta[c], d_sigma, d_hybrid) : 1.0;
+        const double qq = (d_hybrid > 0.0 && H <= 0.0) ? 0.0 : q;
+        if (qq <= 0.0) {
+            sigma_column(H, eta[c], dsigma, n, h_min, col);
+        } else {
+            hycom1_column(H, eta[c], hb, rb, rho_target, dz_top, max_h_top, h_min, keep, n, col, work, bwork);
+            if (qq < 1.0) {
+                sigma_column(H, eta[c], dsigma, n, h_min, sig);
+                zstar_column(H, eta[c], dz_top, n, h_min, work, zs);
+                for (int j = 0; j <= n; ++j) hyb[j] = col[j];
+                window_shallow_sigma(hyb, sig, zs, H, H + eta[c], d_sigma, d_hybrid, h_min, n, col);
+            }
+        }
+        for (int k = 0; k < n; ++k) h_new[k * plane + c] = col[k + 1] - col[k];
+        free(buf);
+        free(bwork);
+    }
+    return bad;
+}
+
 /* sigma_baroclinic.py:533-561 `_diffuse_ale_kernel` on one field (n, ny, nx); faces (ny, nx+1) / (ny+1, nx). */
 void oracle_diffuse_ale(const double* T, const double* Tw, const double* h, const uint8_t* act, const double* cx,
                         const double* cy, const uint8_t* okx, const uint8_t* oky, const double* V, double kh,

@@ -268,7 +268,7 @@ class _Vertical:
 
 
 def neighbour_cases():
-    """The z*/sigma regrid + remap, the ALE diffusion kernel and the velocity remap in fraction space."""
+    """The z*/sigma/hybrid regrid + remap, the ALE diffusion kernel and the velocity remap in fraction space."""
     out = {}
     rng = np.random.default_rng(21)
     n, ny, nx = 12, 7, 9
@@ -313,6 +313,34 @@ def neighbour_cases():
     assert raised
     out["regrid_zstar_bad"] = dict(rule="zstar", H=Hb, eta=eb, h_src=h_src, active=active | True, coord=dz_top,
                                    h_min=rg.H_MIN, T=T, raises=True)
+
+    # the hybrid (HYCOM1) rule with a linear equation of state: isopycnal targets, a z* floor, a maximum top
+    # thickness, and (second case) a shallow sigma zone with flooded land
+    class _EOS:
+        linear = True
+
+        @staticmethod
+        def density(T, S):
+            return 1027.0 * (1.0 - 2e-4 * (T - 10.0) + 7.6e-4 * (S - 35.0))
+
+    rho_col = _EOS.density(T, S)
+    rho_t = rg.target_densities(rho_col[::-1, 3, 3], n, n_light=2)
+    base = {"dz_top": dz_top, "rho_target": rho_t, "max_h_top": np.full(n, 80.0), "h_min": 0.05}
+    for name, extra in (("hybrid", {}), ("hybrid_window", {"dsigma": dsigma, "d_sigma": 5.0, "d_hybrid": 60.0}),
+                        ("hybrid_nokeep", {"keep_isopycnal": False})):
+        params = dict(base, **extra)
+        Hc, etac = H.copy(), eta.copy()
+        if "d_hybrid" in extra:
+            Hc[3, 4], etac[3, 4] = -0.5, 1.0                          # flooded land: sigma at any depth
+        vc = _Vertical(Hc, active, "hybrid", params, rm.PPM_H4)
+        vc.eos = _EOS
+        h_new, (T1, S1) = vc.regrid_remap(etac, h_src, [T, S], T, S)
+        out["regrid_" + name] = dict(rule="hybrid", H=Hc, eta=etac, h_src=h_src, active=active, rho=rho_col,
+                                     rho_target=rho_t, dz_top=dz_top, max_h_top=params["max_h_top"],
+                                     dsigma=params.get("dsigma", np.full(n, 1.0 / n)),
+                                     d_sigma=params.get("d_sigma", 0.0), d_hybrid=params.get("d_hybrid", 0.0),
+                                     h_min=params["h_min"], keep=params.get("keep_isopycnal", True), T=T, S=S,
+                                     h_new=h_new, T1=T1, S1=S1)
 
     # ALE diffusion kernel (tracers.py:436-447): closed, periodic x, periodic x and y
     n, ny, nx = 4, 9, 11

@@ -123,6 +123,19 @@ def test_oracle_zstar_regrid_refuses_a_wet_column_without_depth():
                        O.PPM_H4, float(rec["h_min"]))
 
 
+@pytest.mark.parametrize("case", ["regrid_hybrid", "regrid_hybrid_window", "regrid_hybrid_nokeep"])
+def test_oracle_hybrid_regrid_remap_matches_reference_bitwise(case):
+    rec = NB[case]
+    params = {k: rec[k] for k in ("dz_top", "rho_target", "max_h_top", "dsigma")}
+    params.update(d_sigma=float(rec["d_sigma"]), d_hybrid=float(rec["d_hybrid"]), h_min=float(rec["h_min"]),
+                  keep_isopycnal=bool(rec["keep"]))
+    h_new, wet, bad = O.regrid_hybrid(rec["H"], rec["eta"], rec["h_src"], rec["active"], rec["rho"], params)
+    assert bad == 0
+    np.testing.assert_array_equal(h_new, rec["h_new"])
+    for f, ref in (("T", "T1"), ("S", "S1")):
+        np.testing.assert_array_equal(O.remap_columns(rec["h_src"], rec[f], h_new, O.PPM_H4, wet), rec[ref])
+
+
 @pytest.mark.parametrize("case", ["diffuse_closed", "diffuse_per_x", "diffuse_per_xy"])
 def test_oracle_diffusion_matches_reference_bitwise(case):
     rec = NB[case]
