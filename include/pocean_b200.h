@@ -151,6 +151,25 @@ int pocean_regrid_remap_f64(int rule, const double* H, const double* eta, const 
                             int nfields, int scheme, double* h_new, uint8_t* wet, double* out, int* bad_columns,
                             void* stream);
 
+/*
+ * Regrid with the hybrid (HYCOM1) rule + remap (ALECoordinate.regrid_remap with rule 'hybrid',
+ * core/vertical/regrid.py:100-289 and the code-2 branch of :309-342): per wet column (the mask of
+ * pocean_regrid_remap_f64) the interfaces follow the target densities rho_target (nz+1, surface first) through the
+ * P1M/H2 positions of the layer densities rho (nz, ny, nx, bed first), kept where layers already sit in their
+ * density class (keep != 0, the default `keep_isopycnal`), floored at the z* grid dz_top (nz, surface first) and
+ * capped at max_h_top (nz; +inf = no cap); with d_hybrid > 0 the columns shallower than d_hybrid are windowed
+ * towards sigma (dsigma, nz, bed first) and fully sigma below d_sigma or where H <= 0.  Then the nfields stacked
+ * fields are remapped onto h_new as pocean_regrid_remap_f64 does.  bad_columns (device int, may be NULL) counts the
+ * wet columns with a non-finite density, or with H <= 0 when d_hybrid <= 0, for which the reference raises
+ * ValueError.  nz <= 256.  The reference's finer-source initial regrid (n_out != nz) is not provided.
+ */
+int pocean_regrid_hybrid_remap_f64(const double* H, const double* eta, const double* h_src, const uint8_t* active,
+                                   const double* rho, const double* rho_target, const double* dz_top,
+                                   const double* max_h_top, const double* dsigma, double d_sigma, double d_hybrid,
+                                   double h_min, int keep, const double* f_src, int nz, int ny, int nx, int nfields,
+                                   int scheme, double* h_new, uint8_t* wet, double* out, int* bad_columns,
+                                   void* stream);
+
 /* Face fractions w_k = hf_k / sum_k hf_k (1/nz where the sum is not positive) of hf (nz, ny, nx); replaces
  * core/vertical/ale.py:883-902 (face_fractions / _fractions_kernel). */
 int pocean_face_fractions_f64(const double* hf, int nz, int ny, int nx, double* w, void* stream);

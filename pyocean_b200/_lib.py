@@ -37,6 +37,8 @@ SIGNATURES: dict[str, tuple] = {
                                    _P]),
     "pocean_remap_columns_f64": (_I, [_P, _P, _P, _P, _I, _I, _I, _I, _I, _I, _P, _P]),
     "pocean_regrid_remap_f64": (_I, [_I, _P, _P, _P, _P, _P, _D, _P, _I, _I, _I, _I, _I, _P, _P, _P, _P, _P]),
+    "pocean_regrid_hybrid_remap_f64": (_I, [_P, _P, _P, _P, _P, _P, _P, _P, _P, _D, _D, _D, _I, _P, _I, _I, _I, _I,
+                                            _I, _P, _P, _P, _P, _P]),
     "pocean_face_fractions_f64": (_I, [_P, _I, _I, _I, _P, _P]),
     "pocean_remap_faces_f64": (_I, [_P, _P, _P, _P, _I, _I, _I, _I, _I, _P, _P]),
     "pocean_diffuse_ale_f64": (_I, [_P, _P, _P, _P, _P, _P, _P, _P, _P, _I, _I, _I, _I, _U, _D, _D, _P, _P]),

@@ -1,8 +1,10 @@
-// The kernels either side of the tracer step: the z* / sigma regrid that produces the remap target (with the remap
-// in the same call); the velocity remap in fraction space with its face fractions; the ALE horizontal diffusion.
+// The kernels either side of the tracer step: the z* / sigma / hybrid regrid that produces the remap target (with the
+// remap in the same call); the velocity remap in fraction space with its face fractions; the ALE horizontal
+// diffusion.
 //
-// Reference: core/vertical/regrid.py:44-98 (zstar_column, sigma_column, enforce_min_thickness) and :309-395
-// (regrid_columns), core/components/vertical_coordinate.py:69-111, 142-153 (ALECoordinate.regrid_remap / regrid /
+// Reference: core/vertical/regrid.py:44-98 (zstar_column, sigma_column, enforce_min_thickness), :100-289
+// (the hybrid rule: _p1m_h2_positions, _keep_consistent, hycom1_column, transition_weight, window_shallow_sigma)
+// and :309-395 (regrid_columns), core/vertical/remap.py:199-220 (_bound_edges), core/components/vertical_coordinate.py:69-111, 142-153 (ALECoordinate.regrid_remap / regrid /
 // remap_faces), core/vertical/ale.py:883-902 (_fractions_kernel), core/dynamics/sigma_baroclinic.py:533-561
 // (_diffuse_ale_kernel) with the periodic pad/crop of core/components/tracers.py:436-447.
 //
@@ -85,6 +87,234 @@ __global__ void __launch_bounds__(128) regrid_kernel(int rule, const double* __r
         sigma_heights(H, et, coord, n, h_min, z);
         for (int k = 0; k < n; ++k) h_new[k * plane + c] = z[k + 1] - z[k];
     }
+}
+
+// ---------------------------------------------------------------------------------------------------------------
+// The hybrid (HYCOM1) rule (regrid.py:100-289, 309-342) per column, with NMAX-sized thread-local arrays.
+
+// remap.py:199-220 `_bound_edges` on a column (e: left / right edge pairs).
+__device__ __forceinline__ void bound_edges_col(const double* h, const double* u, int n, double* e)
+{
+    for (int k = 0; k < n; ++k) {
+        const int km1 = k - 1 > 0 ? k - 1 : 0;
+        const int kp1 = k + 1 < n - 1 ? k + 1 : n - 1;
+        double slope_x_h = 0.0;
+        if ((h[km1] + h[kp1]) + 2.0 * h[k] > 0.0) {
+            const double sl = u[k] - u[km1];
+            const double sc = (u[kp1] - u[km1]) * (h[k] / ((h[km1] + h[kp1]) + 2.0 * h[k]));
+            const double sr = u[kp1] - u[k];
+            if (sl * sr > 0.0) {
+                const double m = pmin(pmin(fabs(sl), fabs(sc)), fabs(sr));
+                slope_x_h = sc >= 0.0 ? m : -m;
+            }
+        }
+        const double sg = slope_x_h >= 0.0 ? 1.0 : -1.0;
+        double el = e[2 * k], er = e[2 * k + 1];
+        if ((u[km1] - el) * (el - u[k]) < 0.0) el = u[k] - sg * pmin(fabs(slope_x_h), fabs(el - u[k]));
+        if ((u[kp1] - er) * (er - u[k]) < 0.0) er = u[k] + sg * pmin(fabs(slope_x_h), fabs(er - u[k]));
+        e[2 * k] = pmax(pmin(el, pmax(u[km1], u[k])), pmin(u[km1], u[k]));
+        e[2 * k + 1] = pmax(pmin(er, pmax(u[kp1], u[k])), pmin(u[kp1], u[k]));
+    }
+}
+
+// regrid.py:100-154 `_p1m_h2_positions` (m == n): depths of the target interface densities.
+__device__ __forceinline__ void p1m_h2_positions(const double* h, const double* rho, int n,
+                                                 const double* __restrict__ targets, double* x, double* e, double* xg)
+{
+    e[0] = rho[0];
+    e[2 * (n - 1) + 1] = rho[n - 1];
+    for (int k = 1; k < n; ++k) {
+        if (h[k - 1] + h[k] == 0.0) e[2 * k] = 0.5 * (rho[k - 1] + rho[k]);
+        else e[2 * k] = (rho[k - 1] * h[k] + rho[k] * h[k - 1]) / (h[k - 1] + h[k]);
+        e[2 * (k - 1) + 1] = e[2 * k];
+    }
+    bound_edges_col(h, rho, n, e);
+    for (int k = 0; k < n - 1; ++k)
+        if (e[2 * k + 1] != e[2 * (k + 1)]) {
+            const double a = 0.5 * (e[2 * k + 1] + e[2 * (k + 1)]);
+            e[2 * k + 1] = a;
+            e[2 * (k + 1)] = a;
+        }
+    xg[0] = 0.0;
+    for (int k = 0; k < n; ++k) xg[k + 1] = xg[k] + h[k];
+    for (int k = 0; k <= n; ++k) x[k] = xg[k];
+    for (int kk = 1; kk < n; ++kk) {
+        const double t = __ldg(targets + kk);
+        if (t <= e[0]) {
+            x[kk] = xg[0];
+            continue;
+        }
+        bool found = false;
+        for (int k = 1; k < n; ++k)
+            if (t >= e[2 * (k - 1) + 1] && t <= e[2 * k]) {
+                x[kk] = xg[k];
+                found = true;
+                break;
+            }
+        if (found) continue;
+        if (t >= e[2 * (n - 1) + 1]) {
+            x[kk] = xg[n];
+            continue;
+        }
+        for (int k = 0; k < n; ++k)
+            if (e[2 * k] < t && t < e[2 * k + 1]) {
+                const double xi = (t - e[2 * k]) / (e[2 * k + 1] - e[2 * k]);
+                x[kk] = xg[k] + pmin(pmax(xi, 0.0), 1.0) * h[k];
+                break;
+            }
+    }
+}
+
+// regrid.py:158-201 `_keep_consistent`: interfaces between layers already in their density class stay put.
+template <int NMAX>
+__device__ __forceinline__ void keep_consistent(const double* h, const double* rho, int n,
+                                                const double* __restrict__ targets, double h_mass, double* x,
+                                                double* xg)
+{
+    bool ok[NMAX], kept[NMAX + 1];
+    for (int j = 0; j < n; ++j) {
+        const double r = rho[j];
+        ok[j] = h[j] < h_mass || (__ldg(targets + j) <= r && r <= __ldg(targets + j + 1));
+    }
+    xg[0] = 0.0;
+    for (int j = 0; j < n; ++j) xg[j + 1] = xg[j] + h[j];
+    for (int j = 0; j <= n; ++j) kept[j] = false;
+    kept[0] = kept[n] = true;
+    for (int j = 1; j < n; ++j) {
+        const bool straddle = h[j - 1] >= h_mass && h[j] >= h_mass && rho[j - 1] <= __ldg(targets + j) &&
+                              __ldg(targets + j) <= rho[j];
+        if ((ok[j - 1] && ok[j]) || straddle) {
+            x[j] = xg[j];
+            kept[j] = true;
+        }
+    }
+    double lo = xg[0];
+    for (int j = 1; j < n; ++j) {
+        if (kept[j]) lo = x[j];
+        else if (x[j] < lo) x[j] = lo;
+    }
+    double hi = xg[n];
+    for (int j = n - 1; j > 0; --j) {
+        if (kept[j]) hi = x[j];
+        else if (x[j] > hi) x[j] = hi;
+    }
+}
+
+// regrid.py:87-98 `enforce_min_thickness` on bed-first interfaces.
+__device__ __forceinline__ void enforce_min_thickness(double* zw, int n, double h_min)
+{
+    const double hm = pmin(h_min, (zw[n] - zw[0]) / n);
+    for (int j = n - 1; j > 0; --j)
+        if (zw[j] > zw[j + 1] - hm) zw[j] = zw[j + 1] - hm;
+    for (int j = 1; j < n; ++j)
+        if (zw[j] < zw[j - 1] + hm) zw[j] = zw[j - 1] + hm;
+}
+
+struct HybridParams {
+    const double* rho_target;      // n+1, surface first
+    const double* dz_top;          // n, surface first
+    const double* max_h_top;       // n
+    const double* dsigma;          // n, bed first
+    double d_sigma, d_hybrid, h_min;
+    int keep;
+};
+
+// regrid.py:204-252 `hycom1_column` (m == n) into zw (bed first).
+template <int NMAX>
+__device__ __forceinline__ void hycom1_column(double H, double eta, const double* h_src, const double* rho_src,
+                                              i64 plane, int n, const HybridParams& P, double* zw)
+{
+    double h_top[NMAX], rho_own[NMAX], rho[NMAX], x[NMAX + 1], e[2 * NMAX], xg[NMAX + 1];
+    const double D = H + eta;
+    for (int k = 0; k < n; ++k) {
+        h_top[k] = __ldg(h_src + (i64)(n - 1 - k) * plane);
+        rho_own[k] = __ldg(rho_src + (i64)(n - 1 - k) * plane);
+        rho[k] = rho_own[k];
+    }
+    const double h_mass = 2.0 * P.h_min;
+    double last = -1.0;                       // massless layers take the density of the massive layer above
+    for (int k = 0; k < n; ++k) {
+        if (h_top[k] >= h_mass) last = rho[k];
+        else if (last >= 0.0) rho[k] = last;
+    }
+    int k0 = 0;
+    while (k0 < n && !(h_top[k0] >= h_mass)) ++k0;
+    if (k0 == n) k0 = n - 1;                  // the reference loop variable's last value when nothing breaks
+    if (k0 > 0 && h_top[k0] >= h_mass)
+        for (int kk = 0; kk < k0; ++kk) rho[kk] = rho[k0];
+    for (int k = n - 2; k >= 0; --k) rho[k] = pmin(rho[k], rho[k + 1]);
+    p1m_h2_positions(h_top, rho, n, P.rho_target, x, e, xg);
+    if (P.keep) keep_consistent<NMAX>(h_top, rho_own, n, P.rho_target, 2.0 * P.h_min, x, xg);
+    const double s = D / H;
+    double nominal = 0.0;
+    for (int k = 1; k <= n; ++k) {
+        nominal += __ldg(P.dz_top + k - 1) * s;
+        x[k] = pmin(pmax(x[k], nominal), D);
+    }
+    for (int k = 1; k < n; ++k) x[k] = pmin(x[k], x[k - 1] + __ldg(P.max_h_top + k - 1));
+    for (int k = 1; k <= n; ++k) x[k] = pmax(x[k], x[k - 1]);
+    x[n] = D;
+    for (int j = 0; j <= n; ++j) zw[j] = eta - x[n - j];
+    zw[0] = -H;
+    zw[n] = eta;
+    enforce_min_thickness(zw, n, P.h_min);
+}
+
+// regrid.py:255-260 `transition_weight`.
+__device__ __forceinline__ double transition_weight(double D, double d_sigma, double d_hybrid)
+{
+    if (d_hybrid <= d_sigma) return D > d_sigma ? 1.0 : 0.0;
+    return pmin(pmax((D - d_sigma) / (d_hybrid - d_sigma), 0.0), 1.0);
+}
+
+// One thread per column: the hybrid rule of `_regrid_columns` (code 2) with the wet mask and h_new of
+// regrid_kernel.  bad counts wet columns with H <= 0 and no sigma zone, or a non-finite density.
+template <int NMAX>
+__global__ void __launch_bounds__(128) regrid_hybrid_kernel(const double* __restrict__ Hin,
+                                                            const double* __restrict__ eta,
+                                                            const double* __restrict__ h_src,
+                                                            const uint8_t* __restrict__ active,
+                                                            const double* __restrict__ rho, HybridParams P, int n,
+                                                            i64 plane, double* __restrict__ h_new,
+                                                            uint8_t* __restrict__ wet_out, int* __restrict__ bad)
+{
+    const i64 c = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= plane) return;
+    const double H = nan_to_num(__ldg(Hin + c));
+    double tot = 0.0;
+    for (int k = 0; k < n; ++k) tot += __ldg(h_src + k * plane + c);
+    const double et = __ldg(eta + c);
+    const bool wet = __ldg(active + c) != 0 && H + et > 0.0 && tot > 0.0;
+    wet_out[c] = wet;
+    if (!wet) {
+        for (int k = 0; k < n; ++k) h_new[k * plane + c] = __ldg(h_src + k * plane + c);
+        return;
+    }
+    bool finite = true;
+    for (int k = 0; k < n; ++k) finite = finite && isfinite(__ldg(rho + k * plane + c));
+    if ((!finite || (P.d_hybrid <= 0.0 && !(H > 0.0))) && bad) atomicAdd(bad, 1);
+    double col[NMAX + 1];
+    const double q = P.d_hybrid > 0.0 ? transition_weight(H + et, P.d_sigma, P.d_hybrid) : 1.0;
+    const double qq = (P.d_hybrid > 0.0 && H <= 0.0) ? 0.0 : q;     // flooded land: sigma at any depth
+    if (qq <= 0.0) {
+        sigma_heights(H, et, P.dsigma, n, P.h_min, col);
+    } else {
+        hycom1_column<NMAX>(H, et, h_src + c, rho + c, plane, n, P, col);
+        if (qq < 1.0) {                               // regrid.py:263-289 `window_shallow_sigma`
+            double sig[NMAX + 1], zs[NMAX + 1];
+            sigma_heights(H, et, P.dsigma, n, P.h_min, sig);
+            zstar_heights(H, et, P.dz_top, n, P.h_min, zs);   // surface first: bed-first interface j is zs[n - j]
+            for (int j = 0; j <= n; ++j) {
+                const double lo = qq * (-H) + (1.0 - qq) * sig[j];
+                const double hi = qq * zs[n - j] + (1.0 - qq) * sig[j];
+                col[j] = pmin(pmax(col[j], lo), hi);
+            }
+            col[0] = -H;
+            col[n] = sig[n];
+            enforce_min_thickness(col, n, P.h_min);
+        }
+    }
+    for (int k = 0; k < n; ++k) h_new[k * plane + c] = col[k + 1] - col[k];
 }
 
 // Column IO of the velocity remap in fraction space (vertical_coordinate.py:142-153): source thickness
@@ -282,6 +512,44 @@ extern "C" int pocean_regrid_remap_f64(int rule, const double* H, const double* 
     else
         nb::regrid_kernel<256><<<gx, 128, 0, st>>>(rule, H, eta, h_src, active, coord, h_min, nz, plane, h_new, wet,
                                                    bad_columns);
+    rc = pocean_check_launch(fn);
+    if (rc || nfields == 0) return rc;
+    return pocean_remap_columns_f64(h_src, f_src, h_new, wet, nz, nz, ny, nx, nfields, scheme, out, stream);
+}
+
+extern "C" int pocean_regrid_hybrid_remap_f64(const double* H, const double* eta, const double* h_src,
+                                              const uint8_t* active, const double* rho, const double* rho_target,
+                                              const double* dz_top, const double* max_h_top, const double* dsigma,
+                                              double d_sigma, double d_hybrid, double h_min, int keep,
+                                              const double* f_src, int nz, int ny, int nx, int nfields, int scheme,
+                                              double* h_new, uint8_t* wet, double* out, int* bad_columns,
+                                              void* stream)
+{
+    const char* fn = "pocean_regrid_hybrid_remap_f64";
+    if (nz < 1 || ny < 1 || nx < 1 || nfields < 0)
+        return pocean_fail(POCEAN_EINVAL, "%s: bad sizes nz=%d ny=%d nx=%d nfields=%d", fn, nz, ny, nx, nfields);
+    if (nz > 256) return pocean_fail(POCEAN_EINVAL, "%s: at most 256 layers per column (nz=%d)", fn, nz);
+    if (nfields > 65535) return pocean_fail(POCEAN_EINVAL, "%s: nfields=%d exceeds 65535", fn, nfields);
+    if (nfields > 0 && (scheme < POCEAN_PCM || scheme > POCEAN_PPM_H4))
+        return pocean_fail(POCEAN_EINVAL, "%s: unknown scheme %d", fn, scheme);
+    if (!H || !eta || !h_src || !active || !rho || !rho_target || !dz_top || !max_h_top || !dsigma || !h_new ||
+        !wet || (nfields > 0 && (!f_src || !out)))
+        return pocean_fail(POCEAN_EINVAL, "%s: null pointer", fn);
+    int rc = pocean_check_device();
+    if (rc) return rc;
+    cudaStream_t st = (cudaStream_t)stream;
+    const i64 plane = (i64)ny * nx;
+    const unsigned gx = (unsigned)((plane + 127) / 128);
+    const nb::HybridParams P{rho_target, dz_top, max_h_top, dsigma, d_sigma, d_hybrid, h_min, keep};
+    if (nz <= 64)
+        nb::regrid_hybrid_kernel<64><<<gx, 128, 0, st>>>(H, eta, h_src, active, rho, P, nz, plane, h_new, wet,
+                                                         bad_columns);
+    else if (nz <= 128)
+        nb::regrid_hybrid_kernel<128><<<gx, 128, 0, st>>>(H, eta, h_src, active, rho, P, nz, plane, h_new, wet,
+                                                          bad_columns);
+    else
+        nb::regrid_hybrid_kernel<256><<<gx, 128, 0, st>>>(H, eta, h_src, active, rho, P, nz, plane, h_new, wet,
+                                                          bad_columns);
     rc = pocean_check_launch(fn);
     if (rc || nfields == 0) return rc;
     return pocean_remap_columns_f64(h_src, f_src, h_new, wet, nz, nz, ny, nx, nfields, scheme, out, stream);

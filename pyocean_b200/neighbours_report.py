@@ -2,6 +2,7 @@
 Timing of the neighbours of the tracer step at the benchmark size (512 x 512 x 50 basin, T and S):
 
 * the z* regrid + PPM_H4 remap of both tracers in one call (``pocean_regrid_remap_f64``), and the regrid alone;
+* the same with the hybrid (HYCOM1) rule on a stratified column (``pocean_regrid_hybrid_remap_f64``);
 * the ALE horizontal diffusion of the T/S stack, with its compulsory HBM bytes (T, Tw in and out per tracer; h, V
   per cell; the 2-D masks and metrics once) against the measured HBM peak;
 * the velocity remap in fraction space of the u-faces (512 x 513 x 50);
@@ -83,6 +84,27 @@ def neighbours_report(device=None) -> dict:
     torch.cuda.synchronize()
     same = bool(torch.equal(out, out2))
 
+    # hybrid rule: densities of a stratified column (linear EOS), isopycnal targets over their range, a z* floor and
+    # a shallow sigma window
+    rng = np.random.default_rng(3)
+    zmid = np.cumsum(w.h_src, axis=0) - 0.5 * w.h_src
+    T = 4.0 + 16.0 * zmid / np.maximum(w.h_src.sum(0), 1.0) + rng.normal(0.0, 0.3, w.h_src.shape)
+    rho_np = 1027.0 * (1.0 - 2e-4 * (T - 10.0))
+    lo, hi = float(rho_np[:, w.wet].min()), float(rho_np[:, w.wet].max())
+    rho = g(rho_np)
+    rho_t = g(np.r_[lo - 0.02, lo - 0.01, np.linspace(lo, hi, n - 1)])
+    dzh, mht, dsg = g(np.linspace(2.0, 120.0, n)), g(np.full(n, 400.0)), g(np.full(n, 1.0 / n))
+
+    def hybrid(nf):
+        _lib.check(L.pocean_regrid_hybrid_remap_f64(Hd.data_ptr(), etad.data_ptr(), hs.data_ptr(), act.data_ptr(),
+                                                    rho.data_ptr(), rho_t.data_ptr(), dzh.data_ptr(), mht.data_ptr(),
+                                                    dsg.data_ptr(), 10.0, 150.0, 1e-2, 1,
+                                                    C.data_ptr() if nf else None, n, ny, nx, nf, 2,
+                                                    h_new.data_ptr(), wet.data_ptr(),
+                                                    out.data_ptr() if nf else None, None, st()), "regrid_hybrid")
+
+    t_hyb, t_hyb_regrid = _time(lambda: hybrid(nt), reps=10), _time(lambda: hybrid(0), reps=10)
+
     # diffusion of the stack
     rng = np.random.default_rng(1)
     h = g(np.where(w.wet[None], w.h_tgt, 0.0))
@@ -148,6 +170,7 @@ def neighbours_report(device=None) -> dict:
     return dict(workload=w.name,
                 regrid_remap_zstar=dict(call_ms=t_fused, regrid_ms=t_regrid, regrid_then_remap_columns_ms=t_sep,
                                         equal=same, fields=nt),
+                regrid_remap_hybrid=dict(call_ms=t_hyb, regrid_ms=t_hyb_regrid, fields=nt),
                 diffuse_ale=dict(ms=t_diff, algorithmic_bytes=diff_bytes, gbs=diff_bytes / t_diff / 1e6,
                                  frac_of_measured_hbm=diff_bytes / t_diff / 1e6 / peak, fields=nt),
                 remap_faces_u=dict(ms=t_faces, faces=n * ny * nf),

@@ -3,10 +3,12 @@ The vertical-coordinate neighbours of the tracer step, with the reference's inte
 
 ``ALECoordinate`` mirrors the part of ``core.components.vertical_coordinate.ALECoordinate`` that the ALE tracer
 step calls (vertical_coordinate.py:69-111, 142-153): ``regrid_remap`` (regrid to the z* or sigma target, then the
-conservative remap of every field — one fused kernel: the target grid is built in the remap kernel and written once),
-``regrid`` and ``remap_faces`` (the velocity remap in fraction space).  ``face_fractions`` is
+conservative remap of every field: a regrid launch writes the target thicknesses, the column remap follows),
+``regrid`` and ``remap_faces`` (the velocity remap in fraction space), for the rules 'zstar', 'sigma' and 'hybrid'
+(HYCOM1 with isopycnal targets, a z* floor and an optional shallow sigma window).  ``face_fractions`` is
 ``core.vertical.ale.face_fractions``.  Arrays are NumPy (copied in and out) or CUDA torch tensors (results stay on
-the device).  The hybrid (HYCOM1) rule is not on the GPU: ``NotImplementedError``.
+the device).  The hybrid rule's layer densities come from the model's equation of state (``eos``, the reference's
+EOS component, outside this path) or are given directly (``rho=``).
 """
 from __future__ import annotations
 
@@ -18,67 +20,92 @@ from ._device import Converter, shape_of
 
 H_MIN = 1e-3                                    # core/vertical/regrid.py:41
 RULES = {"zstar": _lib.REGRID_ZSTAR, "sigma": _lib.REGRID_SIGMA}
+P_REF = 2e7                                     # vertical_coordinate.py:37, reference pressure of the hybrid density
 
 
 class ALECoordinate:
     """z* / sigma regrid + remap and the velocity remap of an ALE vertical coordinate, on B200.
 
-    ``H`` (ny, nx) depth [m] (NaN on land reads as 0), ``active`` (ny, nx) water mask, ``regrid_rule`` 'zstar' or
-    'sigma', ``regrid_params`` with ``dz_top`` (z*, surface first) or ``dsigma`` (sigma, bed first) and optional
-    ``h_min``, ``remap_code`` 0 / 1 / 2 (PCM / PLM / PPM_H4) — the attributes of the reference's component."""
+    ``H`` (ny, nx) depth [m] (NaN on land reads as 0), ``active`` (ny, nx) water mask, ``regrid_rule`` 'zstar',
+    'sigma' or 'hybrid', ``regrid_params`` as ``core.vertical.regrid.regrid_columns`` takes them (``dz_top``
+    surface first, ``dsigma`` bed first, ``rho_target`` surface first, ``max_h_top``, ``d_sigma``, ``d_hybrid``,
+    ``h_min``, ``keep_isopycnal``), ``remap_code`` 0 / 1 / 2 (PCM / PLM / PPM_H4), and for 'hybrid' the equation of
+    state ``eos`` (``linear``, ``density(T, S)``, ``potential_density(T, S, p_ref)``) with ``p_ref`` — the attributes
+    of the reference's component."""
 
-    def __init__(self, H, active, regrid_rule: str, regrid_params: dict, remap_code: int = _lib.PPM_H4) -> None:
+    def __init__(self, H, active, regrid_rule: str, regrid_params: dict, remap_code: int = _lib.PPM_H4, eos=None,
+                 p_ref: float = P_REF) -> None:
         if regrid_rule not in ("zstar", "sigma", "hybrid"):
             raise ValueError(f"unknown rule {regrid_rule!r}; use 'zstar', 'sigma' or 'hybrid'")
         self.H, self.active = H, active
         self.regrid_rule, self.regrid_params, self.remap_code = regrid_rule, dict(regrid_params), int(remap_code)
+        self.eos, self.p_ref = eos, float(p_ref)
 
     @classmethod
     def like(cls, ref) -> "ALECoordinate":
-        """The GPU coordinate of a reference ALECoordinate instance (reads H, active, rule, params, remap code)."""
-        return cls(ref.H, ref.active, ref.regrid_rule, ref.regrid_params, ref.remap_code)
+        """The GPU coordinate of a reference ALECoordinate instance (reads H, active, rule, params, remap code, eos)."""
+        return cls(ref.H, ref.active, ref.regrid_rule, ref.regrid_params, ref.remap_code, getattr(ref, "eos", None),
+                   getattr(ref, "p_ref", P_REF))
 
-    def _coord(self, n: int) -> np.ndarray:
-        if self.regrid_rule == "hybrid":
-            raise NotImplementedError("the hybrid (HYCOM1) regrid rule is not on the GPU")
-        key = "dz_top" if self.regrid_rule == "zstar" else "dsigma"
-        if key not in self.regrid_params:
+    def _param(self, key: str, n: int, default=None) -> np.ndarray:
+        if key not in self.regrid_params and default is None:
             raise ValueError(f"regrid_columns({self.regrid_rule!r}) needs params[{key!r}]")
-        coord = np.ascontiguousarray(self.regrid_params[key], dtype=np.float64)
-        if coord.shape != (n,):
-            raise ValueError(f"{key} must have one entry per layer ({n}), got {coord.shape}")
-        return coord
+        v = np.ascontiguousarray(self.regrid_params.get(key, default), dtype=np.float64)
+        if v.shape != (n,):
+            raise ValueError(f"{key} must have {n} entries, got {v.shape}")
+        return v
 
-    def regrid_remap(self, eta, h_src, fields, T=None, S=None):
+    def regrid_density(self, T, S=None):
+        """Layer density the hybrid rule follows (vertical_coordinate.py:80-94): the equation of state's density for
+        a linear EOS, the potential density at ``p_ref`` otherwise; computed by the given ``eos``."""
+        if self.eos is None:
+            raise ValueError("the hybrid rule needs the layer densities: give eos= or rho=")
+        if self.eos.linear:
+            return self.eos.density(T, S)
+        return self.eos.potential_density(T, S, self.p_ref)
+
+    def regrid_remap(self, eta, h_src, fields, T=None, S=None, rho=None):
         """(h_new, [remap_columns(h_src, f, h_new, remap_code, wet) for f in fields]) with the rule's target grid
-        (vertical_coordinate.py:69-78); ``fields`` a list of (N, ny, nx) arrays or one (nf, N, ny, nx) stack."""
+        (vertical_coordinate.py:69-78); ``fields`` a list of (N, ny, nx) arrays or one (nf, N, ny, nx) stack.
+        'hybrid': the densities ``rho`` (N, ny, nx, bed first), else ``regrid_density(T, S)``."""
         stacked = not isinstance(fields, (list, tuple))
-        h_new, outs = self._run(eta, h_src, fields if stacked else list(fields))
+        h_new, outs = self._run(eta, h_src, fields if stacked else list(fields), T, S, rho)
         return h_new, (outs if stacked else list(outs))
 
-    def regrid(self, eta, h, T=None, wet=None, S=None):
+    def regrid(self, eta, h, T=None, wet=None, S=None, rho=None):
         """New layer thicknesses of the rule where wet (active, D > 0, water in the column), else h
         (vertical_coordinate.py:96-111; ``wet`` is always the reference's default mask)."""
         if wet is not None:
             raise NotImplementedError("regrid with a caller-given wet mask; the GPU regrid derives it as the "
                                       "reference's default")
-        return self._run(eta, h, None)[0]
+        return self._run(eta, h, None, T, S, rho)[0]
 
-    def _run(self, eta, h_src, fields):
+    def _run(self, eta, h_src, fields, T=None, S=None, rho=None):
         n, ny, nx = shape_of(h_src)
-        coord = self._coord(n)
+        hybrid = self.regrid_rule == "hybrid"
+        if hybrid:
+            d_hybrid = float(self.regrid_params.get("d_hybrid", 0.0))
+            coords = (self._param("rho_target", n + 1), self._param("dz_top", n),
+                      self._param("max_h_top", n, np.full(n, np.inf)),
+                      self._param("dsigma", n, None if d_hybrid > 0.0 else np.full(n, 1.0 / n)))
+            if rho is None:
+                if T is None:
+                    raise ValueError("regrid_columns('hybrid') needs the layer densities rho")
+                rho = self.regrid_density(T, S)
+        else:
+            coords = (self._param("dz_top" if self.regrid_rule == "zstar" else "dsigma", n),)
         if fields is None:
             arrays = ()
         elif isinstance(fields, list):
             arrays = tuple(fields)
         else:
             arrays = (fields,)
-        cv = Converter(h_src, eta, self.H, *arrays)
+        cv = Converter(h_src, eta, self.H, *arrays, *((rho,) if hybrid else ()))
         hsd = cv.f64(h_src)
         Hd = cv.f64(self.H, (ny, nx))
         ed = cv.f64(eta, (ny, nx))
         act = cv.u8(self.active, (ny, nx))
-        cd = cv.f64(coord)
+        cds = [cv.f64(c) for c in coords]
         if fields is None:
             nf, fd = 0, None
         elif isinstance(fields, list):
@@ -91,14 +118,23 @@ class ALECoordinate:
         wet = torch.empty((ny, nx), dtype=torch.uint8, device=cv.device)
         out = cv.empty((nf, n, ny, nx)) if nf else None
         bad = torch.zeros(1, dtype=torch.int32, device=cv.device)
-        rc = _lib.lib().pocean_regrid_remap_f64(RULES[self.regrid_rule], Hd.data_ptr(), ed.data_ptr(),
-                                                hsd.data_ptr(), act.data_ptr(), cd.data_ptr(),
-                                                float(self.regrid_params.get("h_min", H_MIN)),
-                                                None if fd is None else fd.data_ptr(), n, ny, nx, nf,
-                                                self.remap_code, h_new.data_ptr(), wet.data_ptr(),
-                                                None if out is None else out.data_ptr(), bad.data_ptr(), cv.stream())
+        h_min = float(self.regrid_params.get("h_min", H_MIN))
+        tail = (None if fd is None else fd.data_ptr(), n, ny, nx, nf, self.remap_code, h_new.data_ptr(),
+                wet.data_ptr(), None if out is None else out.data_ptr(), bad.data_ptr(), cv.stream())
+        if hybrid:
+            rd = cv.f64(rho, (n, ny, nx))
+            rc = _lib.lib().pocean_regrid_hybrid_remap_f64(
+                Hd.data_ptr(), ed.data_ptr(), hsd.data_ptr(), act.data_ptr(), rd.data_ptr(),
+                *(c.data_ptr() for c in cds), float(self.regrid_params.get("d_sigma", 0.0)), d_hybrid, h_min,
+                int(bool(self.regrid_params.get("keep_isopycnal", True))), *tail)
+        else:
+            rc = _lib.lib().pocean_regrid_remap_f64(RULES[self.regrid_rule], Hd.data_ptr(), ed.data_ptr(),
+                                                    hsd.data_ptr(), act.data_ptr(), cds[0].data_ptr(), h_min, *tail)
         _lib.check(rc, "regrid_remap")
         if int(bad.item()):
+            if hybrid:
+                raise ValueError("hybrid needs finite densities in wet columns and H > 0 unless it has a shallow "
+                                 "sigma zone (d_hybrid > 0)")
             raise ValueError("z* needs H > 0 in every wet column (cells that can dry: sigma, or hybrid with "
                              "d_hybrid > 0)")
         if out is None:

@@ -112,6 +112,10 @@ def test_neighbour_argument_errors():
     assert L.pocean_regrid_remap_f64(0, 8, 8, 8, 8, 8, 1e-3, 8, 300, 3, 3, 1, 2, 8, 8, 8, None, None) == 1
     assert L.pocean_regrid_remap_f64(0, 8, 8, 8, 8, None, 1e-3, 8, 4, 3, 3, 1, 2, 8, 8, 8, None, None) == 1
     assert L.pocean_regrid_remap_f64(0, 8, 8, 8, 8, 8, 1e-3, 8, 4, 3, 3, 1, 9, 8, 8, 8, None, None) == 1
+    # hybrid: too many layers, null density, bad scheme
+    hyb = lambda nz, rho, scheme: L.pocean_regrid_hybrid_remap_f64(                      # noqa: E731
+        8, 8, 8, 8, rho, 8, 8, 8, 8, 0.0, 0.0, 1e-3, 1, 8, nz, 3, 3, 1, scheme, 8, 8, 8, None, None)
+    assert hyb(300, 8, 2) == 1 and hyb(4, None, 2) == 1 and hyb(4, 8, 7) == 1
     assert L.pocean_face_fractions_f64(None, 4, 3, 3, 8, None) == 1
     assert L.pocean_remap_faces_f64(8, 8, None, None, 4, 3, 3, 1, 2, 8, None) == 1
     assert L.pocean_remap_faces_f64(8, 8, 8, None, 4, 3, 3, 0, 2, 8, None) == 1

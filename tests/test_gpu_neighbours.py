@@ -1,4 +1,4 @@
-"""The neighbours of the tracer step on the GPU: z* / sigma regrid fused with the remap, the velocity remap in
+"""The neighbours of the tracer step on the GPU: z* / sigma / hybrid regrid with the remap, the velocity remap in
 fraction space, the face fractions and the ALE diffusion — bit for bit against the reference's golden vectors and
 the oracle, plus full-size cases against the oracle."""
 from __future__ import annotations
@@ -46,6 +46,80 @@ def test_zstar_regrid_raises_like_the_reference():
     rec = NB["regrid_zstar_bad"]
     with pytest.raises(ValueError, match="z\\* needs H > 0"):
         _vc(rec).regrid_remap(rec["eta"], rec["h_src"], [rec["T"]], rec["T"])
+
+
+class _LinearEOS:
+    """The linear equation of state the hybrid golden cases were made with."""
+    linear = True
+
+    @staticmethod
+    def density(T, S):
+        return 1027.0 * (1.0 - 2e-4 * (T - 10.0) + 7.6e-4 * (S - 35.0))
+
+
+def _hybrid_params(rec) -> dict:
+    return {"dz_top": rec["dz_top"], "rho_target": rec["rho_target"], "max_h_top": rec["max_h_top"],
+            "dsigma": rec["dsigma"], "d_sigma": float(rec["d_sigma"]), "d_hybrid": float(rec["d_hybrid"]),
+            "h_min": float(rec["h_min"]), "keep_isopycnal": bool(rec["keep"])}
+
+
+@pytest.mark.parametrize("case", ["regrid_hybrid", "regrid_hybrid_window", "regrid_hybrid_nokeep"])
+def test_hybrid_regrid_remap_matches_reference_bitwise(case):
+    rec = NB[case]
+    vc = ALECoordinate(rec["H"], rec["active"], "hybrid", _hybrid_params(rec), 2, eos=_LinearEOS)
+    h_new, (T1, S1) = vc.regrid_remap(rec["eta"], rec["h_src"], [rec["T"], rec["S"]], rec["T"], rec["S"])
+    np.testing.assert_array_equal(h_new, rec["h_new"])
+    np.testing.assert_array_equal(T1, rec["T1"])
+    np.testing.assert_array_equal(S1, rec["S1"])
+    # the densities given directly, regrid alone
+    np.testing.assert_array_equal(vc.regrid(rec["eta"], rec["h_src"], rho=rec["rho"]), rec["h_new"])
+
+
+def test_hybrid_regrid_raises_like_the_reference():
+    rec = NB["regrid_hybrid"]
+    params = _hybrid_params(rec)
+    H = rec["H"].copy()
+    H[2, 3] = 0.0                                      # a wet column with H <= 0 and no sigma zone
+    eta = rec["eta"].copy()
+    eta[2, 3] = 0.5
+    act = np.ones_like(rec["active"])
+    with pytest.raises(ValueError, match="hybrid needs"):
+        ALECoordinate(H, act, "hybrid", params, 2).regrid_remap(eta, rec["h_src"], [rec["T"]], rho=rec["rho"])
+    rho = rec["rho"].copy()
+    rho[1, 3, 3] = np.nan                              # non-finite density in a wet column
+    with pytest.raises(ValueError, match="hybrid needs"):
+        ALECoordinate(rec["H"], act, "hybrid", params, 2).regrid(rec["eta"], rec["h_src"], rho=rho)
+    with pytest.raises(ValueError, match="rho_target"):
+        ALECoordinate(rec["H"], rec["active"], "hybrid", {"dz_top": rec["dz_top"]}, 2).regrid(
+            rec["eta"], rec["h_src"], rho=rec["rho"])
+
+
+def test_full_size_hybrid_regrid_remap_against_oracle():
+    # a stratified basin: isopycnal targets over the density range, a z* floor, a shallow sigma window
+    w = W.basin(seed=4, nx=192, ny=160, n=40)
+    rng = np.random.default_rng(21)
+    n = 40
+    H = np.where(w.wet, w.h_tgt.sum(0), np.nan)
+    eta = rng.uniform(-0.5, 0.5, H.shape)
+    z = np.cumsum(w.h_src, axis=0) - 0.5 * w.h_src                   # layer mid heights above the bed
+    T = 4.0 + 16.0 * z / np.maximum(w.h_src.sum(0), 1.0) + rng.normal(0.0, 0.3, w.h_src.shape)
+    S = 35.0 + rng.normal(0.0, 0.2, w.h_src.shape)
+    rho = _LinearEOS.density(T, S)
+    lo, hi = float(rho[:, w.wet].min()), float(rho[:, w.wet].max())
+    rho_t = np.r_[lo - 0.02, lo - 0.01, np.linspace(lo, hi, n - 1)]
+    params = {"dz_top": np.linspace(2.0, 120.0, n), "rho_target": rho_t, "max_h_top": np.full(n, 400.0),
+              "dsigma": np.full(n, 1.0 / n), "d_sigma": 10.0, "d_hybrid": 150.0, "h_min": 0.01}
+    dev = torch.device("cuda", 0)
+    g = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)                       # noqa: E731
+    for keep in (True, False):
+        p = dict(params, keep_isopycnal=keep)
+        vc = ALECoordinate(H, w.wet, "hybrid", p, 2, eos=_LinearEOS)
+        h_new, outs = vc.regrid_remap(g(eta), g(w.h_src), [g(T), g(S)], g(T), g(S))
+        ref_h, wet, bad = O.regrid_hybrid(H, eta, w.h_src, w.wet, rho, p)
+        assert bad == 0
+        assert torch.equal(h_new.cpu(), torch.from_numpy(ref_h))
+        for m, f in enumerate((T, S)):
+            np.testing.assert_array_equal(outs[m].cpu().numpy(), O.remap_columns(w.h_src, f, ref_h, 2, wet))
 
 
 @pytest.mark.parametrize("case", ["faces_ppm_h4", "faces_plm", "faces_wgiven"])
