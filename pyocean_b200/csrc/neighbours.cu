@@ -90,115 +90,19 @@ __global__ void __launch_bounds__(128) regrid_kernel(int rule, const double* __r
 }
 
 // ---------------------------------------------------------------------------------------------------------------
-// The hybrid (HYCOM1) rule (regrid.py:100-289, 309-342) per column, with NMAX-sized thread-local arrays.
-
-// remap.py:199-220 `_bound_edges` on a column (e: left / right edge pairs).
-__device__ __forceinline__ void bound_edges_col(const double* h, const double* u, int n, double* e)
-{
-    for (int k = 0; k < n; ++k) {
-        const int km1 = k - 1 > 0 ? k - 1 : 0;
-        const int kp1 = k + 1 < n - 1 ? k + 1 : n - 1;
-        double slope_x_h = 0.0;
-        if ((h[km1] + h[kp1]) + 2.0 * h[k] > 0.0) {
-            const double sl = u[k] - u[km1];
-            const double sc = (u[kp1] - u[km1]) * (h[k] / ((h[km1] + h[kp1]) + 2.0 * h[k]));
-            const double sr = u[kp1] - u[k];
-            if (sl * sr > 0.0) {
-                const double m = pmin(pmin(fabs(sl), fabs(sc)), fabs(sr));
-                slope_x_h = sc >= 0.0 ? m : -m;
-            }
-        }
-        const double sg = slope_x_h >= 0.0 ? 1.0 : -1.0;
-        double el = e[2 * k], er = e[2 * k + 1];
-        if ((u[km1] - el) * (el - u[k]) < 0.0) el = u[k] - sg * pmin(fabs(slope_x_h), fabs(el - u[k]));
-        if ((u[kp1] - er) * (er - u[k]) < 0.0) er = u[k] + sg * pmin(fabs(slope_x_h), fabs(er - u[k]));
-        e[2 * k] = pmax(pmin(el, pmax(u[km1], u[k])), pmin(u[km1], u[k]));
-        e[2 * k + 1] = pmax(pmin(er, pmax(u[kp1], u[k])), pmin(u[kp1], u[k]));
-    }
-}
-
-// regrid.py:100-154 `_p1m_h2_positions` (m == n): depths of the target interface densities.
-__device__ __forceinline__ void p1m_h2_positions(const double* h, const double* rho, int n,
-                                                 const double* __restrict__ targets, double* x, double* e, double* xg)
-{
-    e[0] = rho[0];
-    e[2 * (n - 1) + 1] = rho[n - 1];
-    for (int k = 1; k < n; ++k) {
-        if (h[k - 1] + h[k] == 0.0) e[2 * k] = 0.5 * (rho[k - 1] + rho[k]);
-        else e[2 * k] = (rho[k - 1] * h[k] + rho[k] * h[k - 1]) / (h[k - 1] + h[k]);
-        e[2 * (k - 1) + 1] = e[2 * k];
-    }
-    bound_edges_col(h, rho, n, e);
-    for (int k = 0; k < n - 1; ++k)
-        if (e[2 * k + 1] != e[2 * (k + 1)]) {
-            const double a = 0.5 * (e[2 * k + 1] + e[2 * (k + 1)]);
-            e[2 * k + 1] = a;
-            e[2 * (k + 1)] = a;
-        }
-    xg[0] = 0.0;
-    for (int k = 0; k < n; ++k) xg[k + 1] = xg[k] + h[k];
-    for (int k = 0; k <= n; ++k) x[k] = xg[k];
-    for (int kk = 1; kk < n; ++kk) {
-        const double t = __ldg(targets + kk);
-        if (t <= e[0]) {
-            x[kk] = xg[0];
-            continue;
-        }
-        bool found = false;
-        for (int k = 1; k < n; ++k)
-            if (t >= e[2 * (k - 1) + 1] && t <= e[2 * k]) {
-                x[kk] = xg[k];
-                found = true;
-                break;
-            }
-        if (found) continue;
-        if (t >= e[2 * (n - 1) + 1]) {
-            x[kk] = xg[n];
-            continue;
-        }
-        for (int k = 0; k < n; ++k)
-            if (e[2 * k] < t && t < e[2 * k + 1]) {
-                const double xi = (t - e[2 * k]) / (e[2 * k + 1] - e[2 * k]);
-                x[kk] = xg[k] + pmin(pmax(xi, 0.0), 1.0) * h[k];
-                break;
-            }
-    }
-}
-
-// regrid.py:158-201 `_keep_consistent`: interfaces between layers already in their density class stay put.
-template <int NMAX>
-__device__ __forceinline__ void keep_consistent(const double* h, const double* rho, int n,
-                                                const double* __restrict__ targets, double h_mass, double* x,
-                                                double* xg)
-{
-    bool ok[NMAX], kept[NMAX + 1];
-    for (int j = 0; j < n; ++j) {
-        const double r = rho[j];
-        ok[j] = h[j] < h_mass || (__ldg(targets + j) <= r && r <= __ldg(targets + j + 1));
-    }
-    xg[0] = 0.0;
-    for (int j = 0; j < n; ++j) xg[j + 1] = xg[j] + h[j];
-    for (int j = 0; j <= n; ++j) kept[j] = false;
-    kept[0] = kept[n] = true;
-    for (int j = 1; j < n; ++j) {
-        const bool straddle = h[j - 1] >= h_mass && h[j] >= h_mass && rho[j - 1] <= __ldg(targets + j) &&
-                              __ldg(targets + j) <= rho[j];
-        if ((ok[j - 1] && ok[j]) || straddle) {
-            x[j] = xg[j];
-            kept[j] = true;
-        }
-    }
-    double lo = xg[0];
-    for (int j = 1; j < n; ++j) {
-        if (kept[j]) lo = x[j];
-        else if (x[j] < lo) x[j] = lo;
-    }
-    double hi = xg[n];
-    for (int j = n - 1; j > 0; --j) {
-        if (kept[j]) hi = x[j];
-        else if (x[j] > hi) x[j] = hi;
-    }
-}
+// The hybrid (HYCOM1) rule (regrid.py:100-289, 309-342), one thread per column.
+//
+// The reference builds 2n edge densities per column and, for each of the n-1 target densities, scans them in order
+// for the first match (a point hit on an interface, else the layer whose edges bracket it).  Here the column keeps
+// only the n+1 interface densities I: after the reference's running minimum the layer densities are nondecreasing
+// downwards, each bounded edge lies between its layer's and its neighbour's density (the bound of `_bound_edges`),
+// and the two edges meeting at an interface are equal after the averaging step (their mean, computed as
+// 0.5 * (a + b), stays between the same two densities), so I is nondecreasing and the first match is found by a
+// binary search, bit for bit the same position.  The per-thread state is four (n+1)-arrays (interface densities,
+// positions, cumulative thickness, the modified densities, later reused for the windowed grids) plus a bitmask of
+// the kept interfaces; the thicknesses and the columns' own densities are re-read from global memory (coalesced
+// across the warp's columns).  Non-finite densities make I unordered: the search stays in bounds and the column is
+// reported as bad, as the reference raises for it.
 
 // regrid.py:87-98 `enforce_min_thickness` on bed-first interfaces.
 __device__ __forceinline__ void enforce_min_thickness(double* zw, int n, double h_min)
@@ -219,32 +123,151 @@ struct HybridParams {
     int keep;
 };
 
-// regrid.py:204-252 `hycom1_column` (m == n) into zw (bed first).
-template <int NMAX>
-__device__ __forceinline__ void hycom1_column(double H, double eta, const double* h_src, const double* rho_src,
-                                              i64 plane, int n, const HybridParams& P, double* zw)
+// One column's thickness and own density, surface first (k = 0 is the top layer).
+struct HybridColumn {
+    const double* h;               // h_src + c
+    const double* r;               // rho + c
+    i64 plane;
+    int n;
+    __device__ __forceinline__ double th(int k) const { return __ldg(h + (i64)(n - 1 - k) * plane); }
+    __device__ __forceinline__ double rho(int k) const { return __ldg(r + (i64)(n - 1 - k) * plane); }
+};
+
+// The weighted edge density between top-first layers k-1 and k (regrid.py:112-117).
+__device__ __forceinline__ double edge_weighted(double h0, double h1, double r0, double r1)
 {
-    double h_top[NMAX], rho_own[NMAX], rho[NMAX], x[NMAX + 1], e[2 * NMAX], xg[NMAX + 1];
-    const double D = H + eta;
+    if (h0 + h1 == 0.0) return 0.5 * (r0 + r1);
+    return (r0 * h1 + r1 * h0) / (h0 + h1);
+}
+
+// regrid.py:100-154 `_p1m_h2_positions` with m == n.  u: the modified densities; I out: interface densities;
+// G out: cumulative thickness from the surface; x out: the interface depths.
+__device__ __forceinline__ void p1m_h2_positions(const HybridColumn& col, const double* u,
+                                                 const double* __restrict__ targets, double* I, double* G, double* x)
+{
+    const int n = col.n;
+    double hm = col.th(0), hc = hm;                   // sliding h[k-1], h[k], h[k+1]
+    double hp = n > 1 ? col.th(1) : hc;
+    double wl = u[0];                                 // left edge of layer k before bounding
+    double er_prev = 0.0;
+    G[0] = 0.0;
     for (int k = 0; k < n; ++k) {
-        h_top[k] = __ldg(h_src + (i64)(n - 1 - k) * plane);
-        rho_own[k] = __ldg(rho_src + (i64)(n - 1 - k) * plane);
-        rho[k] = rho_own[k];
+        const int km1 = k - 1 > 0 ? k - 1 : 0;
+        const int kp1 = k + 1 < n - 1 ? k + 1 : n - 1;
+        const double um = u[km1], uc = u[k], up = u[kp1];
+        const double wr = k == n - 1 ? u[n - 1] : edge_weighted(hc, hp, uc, up);
+        // remap.py:199-220 `_bound_edges` for layer k
+        double slope_x_h = 0.0;
+        if ((hm + hp) + 2.0 * hc > 0.0) {
+            const double sl = uc - um;
+            const double sc = (up - um) * (hc / ((hm + hp) + 2.0 * hc));
+            const double sr = up - uc;
+            if (sl * sr > 0.0) {
+                const double m = pmin(pmin(fabs(sl), fabs(sc)), fabs(sr));
+                slope_x_h = sc >= 0.0 ? m : -m;
+            }
+        }
+        const double sg = slope_x_h >= 0.0 ? 1.0 : -1.0;
+        double el = wl, er = wr;
+        if ((um - el) * (el - uc) < 0.0) el = uc - sg * pmin(fabs(slope_x_h), fabs(el - uc));
+        if ((up - er) * (er - uc) < 0.0) er = uc + sg * pmin(fabs(slope_x_h), fabs(er - uc));
+        el = pmax(pmin(el, pmax(um, uc)), pmin(um, uc));
+        er = pmax(pmin(er, pmax(up, uc)), pmin(up, uc));
+        // regrid.py:120-124: the two edges meeting at interface k are replaced by their mean where they differ
+        I[k] = k == 0 ? el : (er_prev != el ? 0.5 * (er_prev + el) : er_prev);
+        er_prev = er;
+        G[k + 1] = G[k] + hc;
+        wl = wr;
+        hm = hc;
+        hc = hp;
+        hp = k + 2 < n ? col.th(k + 2) : hc;
     }
+    I[n] = er_prev;
+    for (int k = 0; k <= n; ++k) x[k] = G[k];
+    for (int kk = 1; kk < n; ++kk) {
+        const double t = __ldg(targets + kk);
+        int lo = 0, len = n + 1;                      // p = first index with I[p] >= t (n + 1 if none)
+        while (len > 0) {
+            const int half = len >> 1;
+            if (!(I[lo + half] >= t)) {
+                lo += half + 1;
+                len -= half + 1;
+            } else {
+                len = half;
+            }
+        }
+        const int p = lo;
+        if (t <= I[0]) x[kk] = G[0];
+        else if (p >= 1 && p <= n - 1 && I[p] == t) x[kk] = G[p];
+        else if (t >= I[n]) x[kk] = G[n];
+        else if (p >= 1 && p <= n && I[p - 1] < t && t < I[p]) {
+            const double xi = (t - I[p - 1]) / (I[p] - I[p - 1]);
+            x[kk] = G[p - 1] + pmin(pmax(xi, 0.0), 1.0) * col.th(p - 1);
+        }
+    }
+}
+
+// regrid.py:158-201 `_keep_consistent`: interfaces between layers already in their density class stay put.
+template <int NMAX>
+__device__ __forceinline__ void keep_consistent(const HybridColumn& col, const double* __restrict__ targets,
+                                                double h_mass, const double* G, double* x)
+{
+    const int n = col.n;
+    uint32_t kept[(NMAX + 32) / 32];
+    for (int w = 0; w <= n / 32; ++w) kept[w] = 0u;
+    double h0 = col.th(0), r0 = col.rho(0);
+    bool ok0 = h0 < h_mass || (__ldg(targets) <= r0 && r0 <= __ldg(targets + 1));
+    for (int j = 1; j < n; ++j) {
+        const double h1 = col.th(j), r1 = col.rho(j);
+        const double tj = __ldg(targets + j);
+        const bool ok1 = h1 < h_mass || (tj <= r1 && r1 <= __ldg(targets + j + 1));
+        const bool straddle = h0 >= h_mass && h1 >= h_mass && r0 <= tj && tj <= r1;
+        if ((ok0 && ok1) || straddle) {
+            x[j] = G[j];
+            kept[j >> 5] |= 1u << (j & 31);
+        }
+        h0 = h1;
+        r0 = r1;
+        ok0 = ok1;
+    }
+    double lo = G[0];
+    for (int j = 1; j < n; ++j) {
+        if ((kept[j >> 5] >> (j & 31)) & 1u) lo = x[j];
+        else if (x[j] < lo) x[j] = lo;
+    }
+    double hi = G[n];
+    for (int j = n - 1; j > 0; --j) {
+        if ((kept[j >> 5] >> (j & 31)) & 1u) hi = x[j];
+        else if (x[j] > hi) x[j] = hi;
+    }
+}
+
+// regrid.py:204-252 `hycom1_column` (m == n) into zw (bed first); A, B, G scratch of n+1 each.
+template <int NMAX>
+__device__ __forceinline__ void hycom1_column(double H, double eta, const HybridColumn& col, const HybridParams& P,
+                                              double* zw, double* A, double* B, double* G)
+{
+    const int n = col.n;
+    const double D = H + eta;
     const double h_mass = 2.0 * P.h_min;
     double last = -1.0;                       // massless layers take the density of the massive layer above
+    int k0 = -1;                              // the first massive layer
     for (int k = 0; k < n; ++k) {
-        if (h_top[k] >= h_mass) last = rho[k];
-        else if (last >= 0.0) rho[k] = last;
+        double r = col.rho(k);
+        if (col.th(k) >= h_mass) {
+            last = r;
+            if (k0 < 0) k0 = k;
+        } else if (last >= 0.0) {
+            r = last;
+        }
+        A[k] = r;
     }
-    int k0 = 0;
-    while (k0 < n && !(h_top[k0] >= h_mass)) ++k0;
-    if (k0 == n) k0 = n - 1;                  // the reference loop variable's last value when nothing breaks
-    if (k0 > 0 && h_top[k0] >= h_mass)
-        for (int kk = 0; kk < k0; ++kk) rho[kk] = rho[k0];
-    for (int k = n - 2; k >= 0; --k) rho[k] = pmin(rho[k], rho[k + 1]);
-    p1m_h2_positions(h_top, rho, n, P.rho_target, x, e, xg);
-    if (P.keep) keep_consistent<NMAX>(h_top, rho_own, n, P.rho_target, 2.0 * P.h_min, x, xg);
+    if (k0 > 0)                               // massless top layers take the first massive layer's density
+        for (int kk = 0; kk < k0; ++kk) A[kk] = A[k0];
+    for (int k = n - 2; k >= 0; --k) A[k] = pmin(A[k], A[k + 1]);
+    double* x = zw;                           // depths in zw's storage, reversed into A below
+    p1m_h2_positions(col, A, P.rho_target, B, G, x);
+    if (P.keep) keep_consistent<NMAX>(col, P.rho_target, 2.0 * P.h_min, G, x);
     const double s = D / H;
     double nominal = 0.0;
     for (int k = 1; k <= n; ++k) {
@@ -254,10 +277,11 @@ __device__ __forceinline__ void hycom1_column(double H, double eta, const double
     for (int k = 1; k < n; ++k) x[k] = pmin(x[k], x[k - 1] + __ldg(P.max_h_top + k - 1));
     for (int k = 1; k <= n; ++k) x[k] = pmax(x[k], x[k - 1]);
     x[n] = D;
-    for (int j = 0; j <= n; ++j) zw[j] = eta - x[n - j];
-    zw[0] = -H;
-    zw[n] = eta;
-    enforce_min_thickness(zw, n, P.h_min);
+    for (int j = 0; j <= n; ++j) A[j] = eta - x[n - j];
+    A[0] = -H;
+    A[n] = eta;
+    enforce_min_thickness(A, n, P.h_min);
+    for (int j = 0; j <= n; ++j) zw[j] = A[j];
 }
 
 // regrid.py:255-260 `transition_weight`.
@@ -293,15 +317,17 @@ __global__ void __launch_bounds__(128) regrid_hybrid_kernel(const double* __rest
     bool finite = true;
     for (int k = 0; k < n; ++k) finite = finite && isfinite(__ldg(rho + k * plane + c));
     if ((!finite || (P.d_hybrid <= 0.0 && !(H > 0.0))) && bad) atomicAdd(bad, 1);
-    double col[NMAX + 1];
+    double col[NMAX + 1], A[NMAX + 1], B[NMAX + 1], G[NMAX + 1];
     const double q = P.d_hybrid > 0.0 ? transition_weight(H + et, P.d_sigma, P.d_hybrid) : 1.0;
     const double qq = (P.d_hybrid > 0.0 && H <= 0.0) ? 0.0 : q;     // flooded land: sigma at any depth
     if (qq <= 0.0) {
         sigma_heights(H, et, P.dsigma, n, P.h_min, col);
     } else {
-        hycom1_column<NMAX>(H, et, h_src + c, rho + c, plane, n, P, col);
+        const HybridColumn hc{h_src + c, rho + c, plane, n};
+        hycom1_column<NMAX>(H, et, hc, P, col, A, B, G);
         if (qq < 1.0) {                               // regrid.py:263-289 `window_shallow_sigma`
-            double sig[NMAX + 1], zs[NMAX + 1];
+            double* sig = A;
+            double* zs = B;
             sigma_heights(H, et, P.dsigma, n, P.h_min, sig);
             zstar_heights(H, et, P.dz_top, n, P.h_min, zs);   // surface first: bed-first interface j is zs[n - j]
             for (int j = 0; j <= n; ++j) {

@@ -85,7 +85,7 @@ def neighbours_report(device=None) -> dict:
     same = bool(torch.equal(out, out2))
 
     # hybrid rule: densities of a stratified column (linear EOS), isopycnal targets over their range, a z* floor and
-    # a shallow sigma window
+    # a sigma window over the shallower part of the basin (1300-1700 m)
     rng = np.random.default_rng(3)
     zmid = np.cumsum(w.h_src, axis=0) - 0.5 * w.h_src
     T = 4.0 + 16.0 * zmid / np.maximum(w.h_src.sum(0), 1.0) + rng.normal(0.0, 0.3, w.h_src.shape)
@@ -98,7 +98,7 @@ def neighbours_report(device=None) -> dict:
     def hybrid(nf):
         _lib.check(L.pocean_regrid_hybrid_remap_f64(Hd.data_ptr(), etad.data_ptr(), hs.data_ptr(), act.data_ptr(),
                                                     rho.data_ptr(), rho_t.data_ptr(), dzh.data_ptr(), mht.data_ptr(),
-                                                    dsg.data_ptr(), 10.0, 150.0, 1e-2, 1,
+                                                    dsg.data_ptr(), 1300.0, 1700.0, 1e-2, 1,
                                                     C.data_ptr() if nf else None, n, ny, nx, nf, 2,
                                                     h_new.data_ptr(), wet.data_ptr(),
                                                     out.data_ptr() if nf else None, None, st()), "regrid_hybrid")

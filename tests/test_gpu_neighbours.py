@@ -95,31 +95,34 @@ def test_hybrid_regrid_raises_like_the_reference():
 
 
 def test_full_size_hybrid_regrid_remap_against_oracle():
-    # a stratified basin: isopycnal targets over the density range, a z* floor, a shallow sigma window
+    # a stratified basin with density inversions and massless layers: isopycnal targets over the density range, a
+    # z* floor, a shallow sigma window
     w = W.basin(seed=4, nx=192, ny=160, n=40)
     rng = np.random.default_rng(21)
     n = 40
     H = np.where(w.wet, w.h_tgt.sum(0), np.nan)
     eta = rng.uniform(-0.5, 0.5, H.shape)
-    z = np.cumsum(w.h_src, axis=0) - 0.5 * w.h_src                   # layer mid heights above the bed
-    T = 4.0 + 16.0 * z / np.maximum(w.h_src.sum(0), 1.0) + rng.normal(0.0, 0.3, w.h_src.shape)
-    S = 35.0 + rng.normal(0.0, 0.2, w.h_src.shape)
+    hs = w.h_src.copy()
+    hs[rng.random(hs.shape) < 0.1] = 0.0
+    z = np.cumsum(hs, axis=0) - 0.5 * hs                             # layer mid heights above the bed
+    T = 4.0 + 16.0 * z / np.maximum(hs.sum(0), 1.0) + rng.normal(0.0, 0.3, hs.shape)
+    S = 35.0 + rng.normal(0.0, 0.2, hs.shape)
     rho = _LinearEOS.density(T, S)
     lo, hi = float(rho[:, w.wet].min()), float(rho[:, w.wet].max())
     rho_t = np.r_[lo - 0.02, lo - 0.01, np.linspace(lo, hi, n - 1)]
     params = {"dz_top": np.linspace(2.0, 120.0, n), "rho_target": rho_t, "max_h_top": np.full(n, 400.0),
-              "dsigma": np.full(n, 1.0 / n), "d_sigma": 10.0, "d_hybrid": 150.0, "h_min": 0.01}
+              "dsigma": np.full(n, 1.0 / n), "d_sigma": 1300.0, "d_hybrid": 1700.0, "h_min": 0.01}
     dev = torch.device("cuda", 0)
     g = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)                       # noqa: E731
     for keep in (True, False):
         p = dict(params, keep_isopycnal=keep)
         vc = ALECoordinate(H, w.wet, "hybrid", p, 2, eos=_LinearEOS)
-        h_new, outs = vc.regrid_remap(g(eta), g(w.h_src), [g(T), g(S)], g(T), g(S))
-        ref_h, wet, bad = O.regrid_hybrid(H, eta, w.h_src, w.wet, rho, p)
+        h_new, outs = vc.regrid_remap(g(eta), g(hs), [g(T), g(S)], g(T), g(S))
+        ref_h, wet, bad = O.regrid_hybrid(H, eta, hs, w.wet, rho, p)
         assert bad == 0
         assert torch.equal(h_new.cpu(), torch.from_numpy(ref_h))
         for m, f in enumerate((T, S)):
-            np.testing.assert_array_equal(outs[m].cpu().numpy(), O.remap_columns(w.h_src, f, ref_h, 2, wet))
+            np.testing.assert_array_equal(outs[m].cpu().numpy(), O.remap_columns(hs, f, ref_h, 2, wet))
 
 
 @pytest.mark.parametrize("case", ["faces_ppm_h4", "faces_plm", "faces_wgiven"])
