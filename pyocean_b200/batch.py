@@ -145,12 +145,12 @@ class DomainBatch:
 
     @property
     def launches_per_step(self) -> int:
-        """3 face and 3 cell passes, the limiter coefficients, the final update, then the remap: one pass over
+        """3 face and 2 cell passes, the limiter coefficients, the final update, then the remap: one pass over
         field pairs and one over the odd fields (or one over all fields) and the general-column fixup."""
         nts = [d.shape[0] for d in self.domains]
         if self.remap_nf == 2:
-            return 8 + any(n >= 2 for n in nts) + any(n % 2 for n in nts) + 1
-        return 8 + 2
+            return 7 + any(n >= 2 for n in nts) + any(n % 2 for n in nts) + 1
+        return 7 + 2
 
     def _plan(self, tile_rows: int) -> _Plan:
         if tile_rows not in self._plans:
@@ -223,9 +223,9 @@ class DomainBatch:
 
 
 def sequential_launches(domains: Sequence[Domain]) -> int:
-    """Kernel launches of one ``sequential_step``: 8 FCT passes, then per domain the remap of field pairs (if any),
+    """Kernel launches of one ``sequential_step``: 7 FCT passes, then per domain the remap of field pairs (if any),
     of the odd field (if any) and the general-column fixup."""
-    return sum(8 + (d.shape[0] >= 2) + (d.shape[0] % 2) + 1 for d in domains)
+    return sum(7 + (d.shape[0] >= 2) + (d.shape[0] % 2) + 1 for d in domains)
 
 
 def sequential_step(domains: Sequence[Domain], parity: int, mixed: bool = False, stream: int | None = None) -> None:

@@ -4,17 +4,18 @@
 // Reference: core/components/tracers.py:208-254, 342-375 and the Numba kernels of
 // core/dynamics/sigma_baroclinic.py:265-364 (faces, RHS), 407-530 (FCT), 856-875 (RK stage).
 //
-// Design.  The reference runs 9 kernels over ~15 full-size temporaries per FCT step.  Here one step is 8 launches:
-//   1-6. for each RK stage s a face pass and a cell pass (fct_split.cuh): one thread per cell computes the west x-
-//        face and the south y-face of its cell from global memory (L1 serves the overlapping stencils; no shared
-//        memory, no barrier, high occupancy, two independent WENO5 chains per thread), then a streaming pass updates
-//        the cells from the stored faces.
+// Design.  The reference runs 9 kernels over ~15 full-size temporaries per FCT step.  Here one step is 7 launches:
+//   1-5. for RK stages 1 and 2 a face pass and a cell pass, for stage 3 a face pass (fct_split.cuh): one thread per
+//        cell computes the west x-face and the south y-face of its cell from global memory (L1 serves the
+//        overlapping stencils; no shared memory, no barrier, high occupancy, two independent WENO5 chains per
+//        thread), then a streaming pass updates the cells from the stored faces.
 //        1: S <- F0;  c1 = safe(q0 - dt div F0, Va).
 //        2: T <- F1;  q1 recomputed from F0, c2 = safe(3/4 q0 + 1/4 (q1 - dt div F1), Vb).
-//        3: S <- A = ((F0 + F1)/6 + 2 F2/3) - F_L, T <- F_L (donor flux of C);  c_L = safe(q0 - dt div F_L, V1).
-//   7. coeff  Zalesak R+ / R- per cell from the 7-point (x, y, k +- 1) bounds of C and c_L (tracers looped per
+//        3: S <- A = ((F0 + F1)/6 + 2 F2/3) - F_L, and c_L = safe(q0 - dt div F_L, V1) from the donor fluxes F_L
+//           of the cell's four faces (recomputed, never stored).
+//   6. coeff  Zalesak R+ / R- per cell from the 7-point (x, y, k +- 1) bounds of C and c_L (tracers looped per
 //             thread: the stencil geometry is read once).
-//   8. final  face coefficients from R of both neighbours; C_out = safe(q0 - dt div(F_L + C A), V1).
+//   7. final  face coefficients from R of both neighbours; C_out = safe(q0 - dt div(F_L + C A), V1).
 // q0 = V0 C, Va, Vb and q1 are recomputed where needed instead of stored.  Planes run k-major (the tracers of one
 // layer follow each other) so a layer's geometry is re-read from L2.  Periodic axes wrap natively in every stencil
 // (the reference pads by TRACER_HALO = 13 cells and crops; with the dependency radius of the step, 10 cells, both
@@ -646,7 +647,6 @@ static void launch_split(const StepArgs& a, int stage, cudaStream_t st)
         fct_update_kernel<2, R><<<grid, TI * R, 0, st>>>(a);
     } else {
         fct_faces3_kernel<ZV, MIX, R><<<grid, TI * R, 0, st>>>(a);
-        fct_update_kernel<3, R><<<grid, TI * R, 0, st>>>(a);
     }
 }
 
@@ -709,7 +709,6 @@ static void fct_batched_stages(const BatchDomain* doms, const int* po, unsigned 
     fct_faces_batched<2, ZV, MIX, TJR><<<np, TI * TJR, 0, st>>>(doms, po, ndom);
     fct_update_batched<2, TJR><<<np, TI * TJR, 0, st>>>(doms, po, ndom);
     fct_faces3_batched<ZV, MIX, TJR><<<np, TI * TJR, 0, st>>>(doms, po, ndom);
-    fct_update_batched<3, TJR><<<np, TI * TJR, 0, st>>>(doms, po, ndom);
 }
 
 // The FCT passes of every domain of a batch, one launch per pass (off_host: the CTA offsets also held on the device).

@@ -5,9 +5,10 @@
 // overlap between neighbouring threads and are served by L1), with no shared memory and no barrier, so the pass runs
 // at high occupancy and the two independent WENO5 chains of a thread overlap.  Cell pass of stage s: the stage
 // update from the stored faces.  Faces per stage are stored once:
-//   stage 1: S <- F0;  stage 2: T <- F1;  stage 3: S <- A = ((F0 + F1)/6 + 2 F2/3) - F_L and T <- F_L,
-// with (F0 + F1)/6 and 2 F2/3 formed by the same exact divisions as the reference (storing F_L was measured 3 %
-// faster than recomputing it in the stage-3 cell pass).  The arithmetic of every face and
+//   stage 1: S <- F0;  stage 2: T <- F1;  stage 3: S <- A = ((F0 + F1)/6 + 2 F2/3) - F_L,
+// with (F0 + F1)/6 and 2 F2/3 formed by the same exact divisions as the reference.  Stage 3 has no cell pass: its
+// face pass also forms the donor-cell solution c_L of its cell, recomputing the cheap donor fluxes F_L of the
+// cell's east and north faces, so F_L is never stored.  The arithmetic of every face and
 // update is the reference's (weno.cuh; sigma_baroclinic.py:265-321, 452-511), so results equal the reference's bit
 // for bit.  Addresses are formed once per thread as plane pointers with 32-bit offsets; interior stencils (all six
 // cells inside the domain, the common case) load with fixed offsets, edge and periodic stencils take a guarded path.
@@ -159,7 +160,6 @@ __device__ __forceinline__ void put_face(double* S, double* T, int fo, double F,
         T[fo] = F;
     } else {
         S[fo] = (div6_exact(s0 + t0) + div3_exact(2.0 * F)) - FL;
-        T[fo] = FL;
     }
 }
 
@@ -193,20 +193,33 @@ __device__ __forceinline__ void faces_body(const StepArgs& a, int t, int k, int 
         if (last_x) { sxe = P.sx[fxo + 1]; txe = P.tx[fxo + 1]; }
         if (last_y) { syn = P.sy[fyo + s.nx]; tyn = P.ty[fyo + s.nx]; }
     }
-    double fw, lw, fs, ls;
+    double fw, lw, fs, ls, le = 0.0, ln = 0.0;
     x_face<ZV, MIX, STAGE == 3>(P, s, fl, j, i, fw, lw);
     y_face<ZV, MIX, STAGE == 3>(P, s, fl, j, i, fs, ls);
     put_face<STAGE>(P.sx, P.tx, fxo, fw, lw, sxw, txw);
     put_face<STAGE>(P.sy, P.ty, fyo, fs, ls, sys, tys);
     if (last_x) {
-        double fe, le;
+        double fe;
         x_face<ZV, MIX, STAGE == 3>(P, s, fl, j, s.nx, fe, le);
         put_face<STAGE>(P.sx, P.tx, fxo + 1, fe, le, sxe, txe);
     }
     if (last_y) {
-        double fn, ln;
+        double fn;
         y_face<ZV, MIX, STAGE == 3>(P, s, fl, s.ny, i, fn, ln);
         put_face<STAGE>(P.sy, P.ty, fyo + s.nx, fn, ln, syn, tyn);
+    }
+    if (STAGE == 3) {
+        // c_L = safe(q0 - dt div F_L, V1) of this cell (sigma_baroclinic.py:509-511): the donor fluxes of its east
+        // and north faces are recomputed here (they are its neighbours' west and south faces), so F_L is never
+        // stored and no separate cell pass runs
+        if (!last_x) le = donor_x(P.c0, P.e0, a.Qx, s, fl, k, j, i + 1);
+        if (!last_y) ln = donor_y(P.c0, P.e0, a.Qy, s, fl, k, j + 1, i);
+        const double dl = le - lw + ln - ls;
+        const i64 g = s.geo(k, j, i);
+        const double v0 = __ldg(a.V0 + g), v1 = __ldg(a.V1 + g), c0 = __ldg(P.c0 + j * s.nx + i);
+        const double q0 = v0 * c0;
+        const double q = 0.0 * q0 + 1.0 * (q0 - a.dt * dl);
+        a.q1[pc + j * s.nx + i] = v1 > 0 ? q / v1 : c0;
     }
 }
 
@@ -285,7 +298,8 @@ __global__ void FACES3_BOUNDS(TI * TJR) fct_faces3_batched(const BatchDomain* __
     faces_batched_body<3, ZV, MIX, TJR>(doms, off, ndom);
 }
 
-// Cell pass of stage STAGE (sigma_baroclinic.py:452-468 `_fct_stage`; stage 3: c_L of `_fct_fluxes` :509-511).
+// Cell pass of stage STAGE = 1, 2 (sigma_baroclinic.py:452-468 `_fct_stage`); stage 3 has none (its face pass
+// writes c_L).
 template <int STAGE>
 __device__ __forceinline__ void update_body(const StepArgs& a, int t, int k, int i, int j)
 {
@@ -306,10 +320,6 @@ __device__ __forceinline__ void update_body(const StepArgs& a, int t, int k, int
         const double q = 0.75 * q0 + 0.25 * (q1 - a.dt * d);
         const double v = v0 + 0.5 * (v1 - v0);
         a.c2[cc] = v > 0.0 ? q / v : c0;
-    } else {
-        const double dl = a.Tx[w + 1] - a.Tx[w] + a.Ty[so + s.nx] - a.Ty[so];
-        const double q = 0.0 * q0 + 1.0 * (q0 - a.dt * dl);
-        a.q1[cc] = v1 > 0 ? q / v1 : c0;            // c_L
     }
 }
 

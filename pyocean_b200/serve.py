@@ -161,7 +161,7 @@ class Server:
                 for j in active:
                     for s in range(k):
                         sequential_step([j.dom], j.flip ^ (s & 1), mixed=self.mixed, stream=stream.cuda_stream)
-                launches += k * sum(8 + (j.nt >= 2) + (j.nt % 2) + 1 for j in active)
+                launches += k * sum(7 + (j.nt >= 2) + (j.nt % 2) + 1 for j in active)
             iters += 1
             occupancy.append(len(active))
             done = []
@@ -200,8 +200,8 @@ class Server:
 
     def _launches(self, active) -> int:
         if self.remap_nf == 2:
-            return 8 + any(j.nt >= 2 for j in active) + any(j.nt % 2 for j in active) + 1
-        return 10
+            return 7 + any(j.nt >= 2 for j in active) + any(j.nt % 2 for j in active) + 1
+        return 9
 
     def _retire(self, j: Job, stream) -> None:
         """Marks the job done on the device and releases its buffers (stream-ordered: the caching allocator hands

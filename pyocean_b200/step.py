@@ -28,9 +28,9 @@ class ALETracerStep:
         self.ws_bytes = L.pocean_advect_fct_workspace_bytes(nt, n, ny, nx)
         self.ws = torch.empty(self.ws_bytes, dtype=torch.uint8, device=self.device)
         self.adv_out = torch.empty((nt, n, ny, nx), dtype=torch.float64, device=self.device)
-        # 8 FCT passes (3 x face + cell, coefficients, final); the remap: field pairs (nt >= 2), the odd field
-        # (nt odd), the general-column fixup
-        self.launches_per_step = 8 + (nt >= 2) + (nt % 2) + 1
+        # 7 FCT passes (face + cell for stages 1 and 2, the stage-3 face pass, coefficients, final); the remap:
+        # field pairs (nt >= 2), the odd field (nt odd), the general-column fixup
+        self.launches_per_step = 7 + (nt >= 2) + (nt % 2) + 1
 
     def stream(self) -> int:
         return torch.cuda.current_stream(self.device).cuda_stream
