@@ -212,25 +212,34 @@ __device__ __forceinline__ void faces_body(const StepArgs& a, int t, int k, int 
         // c_L = safe(q0 - dt div F_L, V1) of this cell (sigma_baroclinic.py:509-511): the donor fluxes of its east
         // and north faces are recomputed here (they are its neighbours' west and south faces), so F_L is never
         // stored and no separate cell pass runs
-        if (!last_x) le = donor_x(P.c0, P.e0, a.Qx, s, fl, k, j, i + 1);
-        if (!last_y) ln = donor_y(P.c0, P.e0, a.Qy, s, fl, k, j + 1, i);
+        // faces i + 1 <= nx - 1 and j + 1 <= ny - 1 are interior on any axis (periodic or not)
+        const double c0 = __ldg(P.c0 + fyo);
+        if (!last_x) {
+            const double q = __ldg(P.qx + fxo + 1);
+            le = q * (q >= 0 ? c0 : __ldg(P.c0 + fyo + 1));
+        }
+        if (!last_y) {
+            const double q = __ldg(P.qy + fyo + s.nx);
+            ln = q * (q >= 0 ? c0 : __ldg(P.c0 + fyo + s.nx));
+        }
         const double dl = le - lw + ln - ls;
         const i64 g = s.geo(k, j, i);
-        const double v0 = __ldg(a.V0 + g), v1 = __ldg(a.V1 + g), c0 = __ldg(P.c0 + j * s.nx + i);
+        const double v0 = __ldg(a.V0 + g), v1 = __ldg(a.V1 + g);
         const double q0 = v0 * c0;
         const double q = 0.0 * q0 + 1.0 * (q0 - a.dt * dl);
         a.q1[pc + j * s.nx + i] = v1 > 0 ? q / v1 : c0;
     }
 }
 
-// Register budget of the face passes, as resident 256-thread blocks per SM (scaled for other block sizes): stages
-// 1-2 at 6 (42 registers), stage 3 at 5 (51 registers).  Measured at 512 x 512 x 50: 8.5 % faster than ptxas's
-// own choice (58 / 80 registers), whose lower occupancy left the FP64 chains and the stencil loads exposed.
+// Register budget of the face passes, as resident 256-thread blocks per SM (scaled for other block sizes): 6 for
+// all three stages (40 registers; stage 3 spills a few values to L1).  Measured at 512 x 512 x 50: 8.5 % faster
+// than ptxas's own choice (58 / 80 registers), whose lower occupancy left the FP64 chains and the stencil loads
+// exposed; for stage 3, 6 is 0.6 % faster than 5 and 5 than 4.
 #ifndef POCEAN_FACES12_MINB
 #define POCEAN_FACES12_MINB 6
 #endif
 #ifndef POCEAN_FACES3_MINB
-#define POCEAN_FACES3_MINB 5
+#define POCEAN_FACES3_MINB 6
 #endif
 #define FACES12_BOUNDS(n) __launch_bounds__(n, POCEAN_FACES12_MINB * 256 / (n))
 #define FACES3_BOUNDS(n) __launch_bounds__(n, POCEAN_FACES3_MINB * 256 / (n))
