@@ -56,12 +56,12 @@ def make_workload(name: str):
     return W.basin() if name == "basin" else W.zstar_box()
 
 
-# From one ncu capture of a step of this workload (all ten kernels; the profile summary
+# From one ncu capture of a step of this workload (all nine kernels; the profile summary
 # profiles/fct_and_remap_kernels_basin_512x512x50.md gives the command): DRAM bytes read + written per call, and
 # FP64 thread instructions (DFMA + DMUL + DADD) per call.
 NCU_PER_CALL = {
-    "basin_512x512x50_nt2": {"advect_fct": {"dram_bytes": 10275506400, "fp64_inst": 18034242543},
-                             "remap_columns": {"dram_bytes": 798768408, "fp64_inst": 2872665311}},
+    "basin_512x512x50_nt2": {"advect_fct": {"dram_bytes": 9517680608, "fp64_inst": 18348363343},
+                             "remap_columns": {"dram_bytes": 798247632, "fp64_inst": 2872665311}},
 }
 FP64_LANES_PER_SM, SMS = 64, 148
 
