@@ -83,6 +83,9 @@ def lib() -> ctypes.CDLL:
         L.oracle_limit_outflow.restype = i
         L.oracle_lagrangian_thickness.argtypes = [_D, _D, d, _D, d, i, i, i, _D]
         L.oracle_lagrangian_thickness.restype = ctypes.c_longlong
+        L.oracle_upwind_transport.argtypes = [_D, _D, _D, _D, _D, i, i, i, _D]
+        L.oracle_freshwater_volumes.argtypes = [_D, _D, _D, i, i, i, _D]
+        L.oracle_freshwater_volumes.restype = i
         L.oracle_num_threads.restype = i
         L.oracle_set_threads.argtypes = [i]
         _LIB = L
@@ -571,3 +574,56 @@ def lagrangian_thickness(h, divq, dt: float, area, tol: float = 1e-9):
         raise RuntimeError(f"layer {k} of cell (j={j}, i={i}) emptied in the Lagrangian step: h† = {v:.3e} m "
                            f"(reduce dt)")
     return out
+
+
+def upwind_transport_x(q_e, q_w, ut, L, Q_bt) -> np.ndarray:
+    """``upwind_transport_x`` (ale.py:233-251): donor-cell layer fluxes consistent with the free-surface flux."""
+    ut = _f64(ut)
+    n, a, b = ut.shape
+    out = np.empty_like(ut)
+    lib().oracle_upwind_transport(_p(_f64(q_e)), _p(_f64(q_w)), _p(ut), _p(_f64(np.broadcast_to(L, (a, b)))),
+                                  _p(_f64(np.broadcast_to(Q_bt, (a, b)))), n, a, b, _p(out))
+    return out
+
+
+DZ_FLOOR = 1e-6                        # core/vertical/ale.py:63
+
+
+def ale_layer_transport(h, u_old, v_old, u_new, v_new, wet_u, wet_v, wu, wv, Lu, Lv, Du, Dv, qe, qw, qn, qs, active,
+                        area, dx_t, dy_t, dt: float, theta: float, theta_bc: float, thickness_flux: str = "ppm",
+                        periodic=(False, False), fw=None) -> dict:
+    """``ALELayerTransport.__call__`` (core/components/layer_transport.py:111-156) without open faces, from the
+    restatements above: transport velocities, the PPM or donor-cell layer fluxes (v-faces on swapped axes), the
+    outflow limiter, h-dagger, the layer volumes h A, ok = active & V1 > 0 and, with freshwater, h_fw and V_fw.
+    ``qn``, ``qs`` are the v-face thicknesses in the swapped (N, nx, ny+1) layout the reference passes."""
+    if thickness_flux == "ppm" and any(periodic):
+        raise NotImplementedError("periodic PPM thickness flux (the reference pads by 4 cells)")
+    sw = lambda a: np.ascontiguousarray(np.swapaxes(a, 1, 2))                       # noqa: E731
+    utx, Qbx = transport_velocity(u_new, u_old, wet_u, wu, Lu, Du, theta, theta_bc)
+    uty, Qby = transport_velocity(v_new, v_old, wet_v, wv, Lv, Dv, theta, theta_bc)
+    if thickness_flux == "ppm":
+        Qx = ppm_transport_x(h, utx, Lu, Qbx, qe, qw, active, dt, dx_t)
+        Qy = sw(ppm_transport_x(sw(h), sw(uty), Lv.T, Qby.T, qn, qs, active.T, dt, dy_t.T))
+    else:
+        Qx = upwind_transport_x(qe, qw, utx, Lu, Qbx)
+        Qy = sw(upwind_transport_x(qn, qs, sw(uty), Lv.T, Qby.T))
+    Qx, Qy, n_lim = limit_outflow(h, Qx, Qy, area, dt, active, periodic=tuple(periodic))
+    divh = Qx[..., 1:] - Qx[..., :-1] + Qy[:, 1:, :] - Qy[:, :-1, :]
+    h_lag = lagrangian_thickness(h, divh, dt, area)
+    V0, V1 = h * area[None], h_lag * area[None]
+    ok = np.broadcast_to(active[None], V1.shape) & (V1 > 0)
+    out = dict(Qx=Qx, Qy=Qy, V0=V0, V1=V1, ok=ok, h_dagger=h_lag, n_limited=n_lim)
+    if fw is not None:
+        h_fw, _ = freshwater_volumes(h_lag, dt * fw, DZ_FLOOR)
+        out.update(h_fw=h_fw, V_fw=h_fw * area[None])
+    return out
+
+
+def freshwater_volumes(V, dV, floor):
+    """``freshwater_volumes`` (core/components/freshwater.py:31-58): (V_new, n_limited)."""
+    V = _f64(V)
+    n, ny, nx = V.shape
+    out = np.empty_like(V)
+    nl = lib().oracle_freshwater_volumes(_p(V), _p(_f64(dV)), _p(_f64(np.broadcast_to(floor, (ny, nx)))), n, ny, nx,
+                                         _p(out))
+    return out, int(nl)

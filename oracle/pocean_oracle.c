@@ -1559,9 +1559,74 @@ long long oracle_lagrangian_thickness(const double* h, const double* divq, doubl
             const i64 o = k * pc + c;
             const double v = h[o] - dt * divq[o] / (area[c] > 0 ? area[c] : 1.0);
             if (v < -tol && bad < 0) bad = o;
-            out[o] = (v >= 0.0 || isnan(v)) ? v : 0.0;                /* np.maximum(v, 0.0) */
+            out[o] = (v > 0.0 || isnan(v)) ? v : 0.0;                 /* np.maximum(v, 0.0): +0.0 for v = -0.0 */
         }
     return bad;
+}
+
+/*
+ * ale.py:233-251 `upwind_transport_x` on one face column (a, b) of nq layers: F_k = (L u_k) q_k(u_k) with q_e for
+ * u >= 0, q_w otherwise; R = Q_bt - sum_k F_k; the column's thicknesses on R's upwind side (the other side if that
+ * column is empty) share R in proportion.  Sums run k = 0 .. n-1 from 0.0, as numpy's first-axis reductions do.
+ */
+void oracle_upwind_transport(const double* q_e, const double* q_w, const double* ut, const double* L,
+                             const double* Q_bt, int n, int a, int b, double* out)
+{
+    const i64 pf = (i64)a * b;
+#pragma omp parallel for
+    for (i64 o = 0; o < pf; ++o) {
+        double S = 0.0;
+        for (int k = 0; k < n; ++k) {
+            const i64 x = k * pf + o;
+            const double F = (L[o] * ut[x]) * (ut[x] >= 0 ? q_e[x] : q_w[x]);
+            out[x] = F;
+            S += F;
+        }
+        const double R = Q_bt[o] - S;
+        const int pos = R >= 0;
+        double sq = 0.0;
+        for (int k = 0; k < n; ++k) sq += pos ? q_e[k * pf + o] : q_w[k * pf + o];
+        const int use_e = sq > 0 ? pos : !pos;
+        double tot = 0.0;
+        for (int k = 0; k < n; ++k) tot += use_e ? q_e[k * pf + o] : q_w[k * pf + o];
+        const double den = tot > 0 ? tot : 1.0;
+        for (int k = 0; k < n; ++k) {
+            const i64 x = k * pf + o;
+            out[x] = out[x] + R * (use_e ? q_e[x] : q_w[x]) / den;
+        }
+    }
+}
+
+static inline double np_min(double a, double b) { return (a < b || isnan(a)) ? a : b; }   /* numpy.minimum */
+static inline double np_max(double a, double b) { return (a > b || isnan(a)) ? a : b; }   /* numpy.maximum */
+
+/*
+ * core/components/freshwater.py:31-58 `freshwater_volumes`: dV (ny, nx) added to the top layer (k = n-1) of V
+ * (n, ny, nx); a removal that would take the top layer below floor (ny, nx) is taken from the layers below, top
+ * down, each kept at the floor, then down to zero.  Returns the number of such columns.
+ */
+int oracle_freshwater_volumes(const double* V, const double* dV, const double* floor_, int n, int ny, int nx,
+                              double* out)
+{
+    const i64 pc = (i64)ny * nx;
+    int spilled = 0;
+    for (i64 c = 0; c < pc; ++c) {
+        for (int k = 0; k < n; ++k) out[k * pc + c] = V[k * pc + c];
+        out[(n - 1) * pc + c] += dV[c];
+        if (!(dV[c] < 0 && out[(n - 1) * pc + c] < floor_[c])) continue;
+        ++spilled;
+        double deficit = -dV[c];
+        for (int pass = 0; pass < 2; ++pass) {
+            const double keep = pass == 0 ? floor_[c] : 0.0;
+            for (int k = n - 1; k >= 0; --k) {
+                const double col = pass == 0 && k == n - 1 ? V[k * pc + c] : out[k * pc + c];
+                const double take = np_min(deficit, np_max(col - keep, 0.0));
+                out[k * pc + c] = col - take;
+                deficit = deficit - take;
+            }
+        }
+    }
+    return spilled;
 }
 
 /* Threads available to the OpenMP loops (for reporting the CPU baseline's core count). */

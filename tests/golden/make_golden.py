@@ -486,6 +486,114 @@ def producer_cases():
     return out
 
 
+def layer_transport_cases():
+    """The donor-cell layer transport, the freshwater volumes, the Lagrangian thickness at a signed-zero tie and the
+    whole ALE layer-transport step (ALELayerTransport.__call__ without open faces; PPM and donor-cell thickness
+    fluxes, with and without freshwater, donor cell on a periodic x axis)."""
+    from types import SimpleNamespace as NS
+    from core.components.freshwater import freshwater_volumes
+    from core.components.layer_transport import ALELayerTransport
+    out = {}
+    rng = np.random.default_rng(71)
+    n, ny, nx = 6, 9, 14
+    H, active, h, dx, Lu = _producer_state(rng, n, ny, nx)
+    q_e, q_w = ale.face_transport_thickness(h, H, active, True)
+    ut = rng.normal(0.0, 0.4, (n, ny, nx + 1))
+    Q_bt = rng.normal(0.0, 1.0, (ny, nx + 1)) * 5e4
+    qe2, qw2 = q_e.copy(), q_w.copy()
+    qe2[:, 2, :6] = 0.0                                                   # one side empty: the other side takes R
+    qw2[:, 3, 4:9] = 0.0
+    qe2[:, 4, 1:3] = qw2[:, 4, 1:3] = 0.0                                 # both empty: R added to nothing
+    for name, (a_, b_) in (("upwind", (q_e, q_w)), ("upwind_empty", (qe2, qw2))):
+        out[name] = dict(q_e=a_, q_w=b_, ut=ut, L=Lu, Q_bt=Q_bt, Q=ale.upwind_transport_x(a_, b_, ut, Lu, Q_bt))
+    # freshwater volumes: thicknesses with the scalar floor (ALE), volumes with a per-column floor (sigma)
+    dt = 600.0
+    hz = np.where(active[None], np.nan_to_num(h), 0.0)
+    area = dx * rng.uniform(900.0, 1100.0, (ny, nx))
+    dh = rng.normal(0.0, 0.3, (ny, nx)) * 1e-3 * dt
+    dh[1, 2:8] = -hz[-1, 1, 2:8] - rng.uniform(0.0, 2.0, 6)                # evaporation beyond the top layer
+    dh[5, 3:6] = -hz[:, 5, 3:6].sum(0) - 1.0                               # more than the whole column
+    dh[6, 7] = -hz[-1, 6, 7]                                               # exactly the top layer
+    for name, (V, dv, fl) in (("fw_thickness", (hz, dh, ale.DZ_FLOOR)),
+                              ("fw_volume", (hz * area[None], dh * area, ale.DZ_FLOOR * area))):
+        Vn, nl = freshwater_volumes(V, dv, fl)
+        out[name] = dict(V=V, dV=dv, floor=np.broadcast_to(fl, (ny, nx)).copy(), V_new=Vn, n_limited=nl)
+    # Lagrangian thickness of a layer that is -0.0 with no divergence (numpy.maximum(-0.0, 0.0) is +0.0)
+    Aw = np.where(active, area, 0.0)
+    hn = hz.copy()
+    hn[2] = -0.0
+    div = rng.normal(0.0, 1.0, hz.shape) * 1e-3 * hz * area[None] / dt
+    div[2] = 0.0
+    out["lagrangian_negzero"] = dict(h=hn, divq=div, dt=dt, area=Aw, h_dag=ale.lagrangian_thickness(hn, div, dt, Aw))
+    # the whole ALE layer-transport step
+    Lv = rng.uniform(900.0, 1100.0, (ny + 1, nx))
+    dy = rng.uniform(900.0, 1100.0, (ny, nx))
+    eta, eta_new = rng.uniform(-0.3, 0.3, (ny, nx)), rng.uniform(-0.3, 0.3, (ny, nx))
+    u_old, u_new = rng.normal(0.0, 0.1, (n, ny, nx + 1)), rng.normal(0.0, 0.1, (n, ny, nx + 1))
+    v_old, v_new = rng.normal(0.0, 0.1, (n, ny + 1, nx)), rng.normal(0.0, 0.1, (n, ny + 1, nx))
+    wet_u = np.zeros((ny, nx + 1), bool)
+    wet_u[:, 1:-1] = active[:, 1:] & active[:, :-1]
+    wet_v = np.zeros((ny + 1, nx), bool)
+    wet_v[1:-1] = active[1:] & active[:-1]
+    u_old *= wet_u
+    u_new *= wet_u
+    v_old *= wet_v
+    v_new *= wet_v
+    Dc = hz.sum(0)                                                         # face depths of the columns' water
+    Du = np.zeros((ny, nx + 1))
+    Du[:, 1:-1] = np.minimum(Dc[:, 1:], Dc[:, :-1])
+    Du *= wet_u
+    Dv = np.zeros((ny + 1, nx))
+    Dv[1:-1] = np.minimum(Dc[1:], Dc[:-1])
+    Dv *= wet_v
+    qn, qs = ale.face_transport_thickness(hz.swapaxes(1, 2), H.T, active.T, True)
+    wu = face_fractions(0.5 * (q_e + q_w))
+    wv = face_fractions(0.5 * (qn + qs)).swapaxes(1, 2)
+    fw = rng.normal(0.0, 1.0, (ny, nx)) * 2e-6
+    for name, flux, per, with_fw, amp in (("lt_ppm", "ppm", (), False, 1.0), ("lt_upwind", "upwind", (), False, 1.0),
+                                          ("lt_ppm_fw", "ppm", (), True, 1.0),
+                                          ("lt_upwind_perx", "upwind", ("x",), False, 1.0),
+                                          ("lt_ppm_strong", "ppm", (), False, 6.0),
+                                          ("lt_upwind_strong", "upwind", (), False, 6.0)):
+        fs = NS(theta=0.6, active=active, Lu=Lu, Lv=Lv)
+        lt = ALELayerTransport(fs=fs, H=H, area=area, dt=dt, thickness_flux=flux, vi_geom={"dx_t": dx, "dy_t": dy},
+                               layer_volumes=lambda e, hh: hh * area[None], ob=None)
+        Lu_p, u_o, u_n, wet_up, Du_p, qe_p, qw_p, wu_p = Lu, u_old, u_new, wet_u, Du, q_e, q_w, wu
+        if per:
+            lt.per = Periodic(per)
+            Lu_p = Lu.copy()
+            Lu_p[:, -1] = Lu_p[:, 0]                                          # face nx is face 0
+            wrap = active[:, 0] & active[:, -1]
+            wet_up = wet_u.copy()
+            wet_up[:, 0] = wet_up[:, -1] = wrap
+            u_o, u_n = u_old.copy(), u_new.copy()
+            u_o[..., 0] = u_o[..., -1] = rng.normal(0.0, 0.1, (n, ny)) * wrap
+            u_n[..., 0] = u_n[..., -1] = rng.normal(0.0, 0.1, (n, ny)) * wrap
+            Du_p = Du.copy()
+            Du_p[:, 0] = Du_p[:, -1] = np.minimum(Dc[:, 0], Dc[:, -1]) * wrap
+            pe = np.concatenate([hz[..., -1:], hz], axis=-1)
+            pw = np.concatenate([hz, hz[..., :1]], axis=-1)
+            qe_p, qw_p = q_e.copy(), q_w.copy()
+            qe_p[..., 0] = qe_p[..., -1] = (pe[..., 0] * wrap)
+            qw_p[..., 0] = qw_p[..., -1] = (pw[..., -1] * wrap)
+            wu_p = face_fractions(0.5 * (qe_p + qw_p))
+            fs.Lu = Lu_p
+        u_o, u_n, v_o, v_n = u_o * amp, u_n * amp, v_old * amp, v_new * amp
+        st = NS(h=hz, u=u_o, v=v_o, eta=eta)
+        fluxes = NS(wet_u=wet_up, wet_v=wet_v, Du=Du_p, Dv=Dv, fw=fw if with_fw else None)
+        lf = lt(st, eta_new, u_n, v_n, fluxes, 0.5, (), wu_p, wv, qe_p, qw_p, qn, qs)
+        rec = dict(thickness_flux=flux, periodic=np.array(per, dtype=str), theta=0.6, theta_bc=0.5, dt=dt, H=H,
+                   area=area, active=active, Lu=Lu_p, Lv=Lv, dx_t=dx, dy_t=dy, h=hz, u=u_o, v=v_o, eta=eta,
+                   eta_new=eta_new, u_new=u_n, v_new=v_n, wet_u=wet_up, wet_v=wet_v, Du=Du_p, Dv=Dv, wu=wu_p,
+                   wv=wv, qe=qe_p, qw=qw_p, qn=qn, qs=qs, Qx=lf.Qx, Qy=lf.Qy, V0=lf.V0, V1=lf.V1, ok=lf.ok,
+                   h_dagger=lf.h_dagger, n_limited=lf.n_limited)
+        if with_fw:
+            rec.update(fw=fw, V_fw=lf.V_fw, h_fw=lf.h_fw)
+        out[name] = rec
+        print(name, "limited", lf.n_limited)
+    return out
+
+
 def save(name, cases):
     flat = {}
     for case, rec in cases.items():
@@ -498,8 +606,8 @@ def save(name, cases):
 
 if __name__ == "__main__":
     threads.set_threads(1)
-    which = sys.argv[2:] or ["fct", "rk3", "kernels", "remap", "neighbours", "producers"]
+    which = sys.argv[2:] or ["fct", "rk3", "kernels", "remap", "neighbours", "producers", "layer_transport"]
     makers = {"fct": fct_cases, "rk3": rk3_cases, "kernels": kernel_cases, "remap": remap_cases,
-              "neighbours": neighbour_cases, "producers": producer_cases}
+              "neighbours": neighbour_cases, "producers": producer_cases, "layer_transport": layer_transport_cases}
     for name in which:
         save(name, makers[name]())

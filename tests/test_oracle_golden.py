@@ -214,3 +214,48 @@ def test_oracle_lagrangian_thickness_matches_reference_bitwise(case):
             O.lagrangian_thickness(*args)
         return
     np.testing.assert_array_equal(O.lagrangian_thickness(*args), rec["h_dag"])
+
+
+LT = load_golden("layer_transport")
+
+
+@pytest.mark.parametrize("case", ["upwind", "upwind_empty"])
+def test_oracle_upwind_transport_matches_reference_bitwise(case):
+    rec = LT[case]
+    np.testing.assert_array_equal(O.upwind_transport_x(rec["q_e"], rec["q_w"], rec["ut"], rec["L"], rec["Q_bt"]),
+                                  rec["Q"])
+
+
+@pytest.mark.parametrize("case", ["fw_thickness", "fw_volume"])
+def test_oracle_freshwater_volumes_match_reference_bitwise(case):
+    rec = LT[case]
+    V, nl = O.freshwater_volumes(rec["V"], rec["dV"], rec["floor"])
+    np.testing.assert_array_equal(V, rec["V_new"])
+    assert nl == int(rec["n_limited"])
+
+
+def test_oracle_lagrangian_thickness_signed_zero_matches_reference():
+    rec = LT["lagrangian_negzero"]
+    out = O.lagrangian_thickness(rec["h"], rec["divq"], float(rec["dt"]), rec["area"])
+    np.testing.assert_array_equal(out, rec["h_dag"])
+    assert not np.signbit(out).any() and not np.signbit(rec["h_dag"]).any()
+
+
+def layer_transport_args(rec) -> dict:
+    return dict(h=rec["h"], u_old=rec["u"], v_old=rec["v"], u_new=rec["u_new"], v_new=rec["v_new"],
+                wet_u=rec["wet_u"], wet_v=rec["wet_v"], wu=rec["wu"], wv=rec["wv"], Lu=rec["Lu"], Lv=rec["Lv"],
+                Du=rec["Du"], Dv=rec["Dv"], qe=rec["qe"], qw=rec["qw"], qn=rec["qn"], qs=rec["qs"],
+                active=rec["active"], area=rec["area"], dx_t=rec["dx_t"], dy_t=rec["dy_t"], dt=float(rec["dt"]),
+                theta=float(rec["theta"]), theta_bc=float(rec["theta_bc"]),
+                thickness_flux=str(rec["thickness_flux"]),
+                periodic=("x" in list(rec["periodic"]), "y" in list(rec["periodic"])), fw=rec.get("fw"))
+
+
+@pytest.mark.parametrize("case", ["lt_ppm", "lt_upwind", "lt_ppm_fw", "lt_upwind_perx", "lt_ppm_strong",
+                                  "lt_upwind_strong"])
+def test_oracle_layer_transport_step_matches_reference_bitwise(case):
+    rec = LT[case]
+    out = O.ale_layer_transport(**layer_transport_args(rec))
+    for key in ("Qx", "Qy", "V0", "V1", "ok", "h_dagger") + (("h_fw", "V_fw") if "fw" in rec else ()):
+        np.testing.assert_array_equal(out[key], rec[key], err_msg=key)
+    assert out["n_limited"] == int(rec["n_limited"])
