@@ -236,6 +236,31 @@ int pocean_lagrangian_thickness_f64(const double* h, const double* divq, const d
                                     double dt, double tol, double* h_dag, unsigned long long* first_bad,
                                     void* stream);
 
+/* ale.py:233-251 upwind_transport_x, the donor-cell layer flux of ALELayerTransport (thickness_flux != "ppm"):
+ * Q_k = L u_k q_k(u_k) + R q_k(R) / sum_j q_j(R) with R = Q_bt - sum_k L u_k q_k(u_k), q = q_e for a non-negative
+ * argument, q_w otherwise (the other side where that column is empty).  q_e, q_w, ut, Q (nz, a, b); L, Q_bt (a, b).
+ * v-faces: the same call on swapped horizontal axes, as the reference makes it. */
+int pocean_upwind_transport_f64(const double* q_e, const double* q_w, const double* ut, const double* L,
+                                const double* Q_bt, int nz, int a, int b, double* Q, void* stream);
+
+/* core/components/freshwater.py:31-58 freshwater_volumes: dV (ny, nx) added to the top layer (k = nz-1) of V
+ * (nz, ny, nx); a removal that would take the top layer below the floor is taken from the layers below, top down,
+ * first keeping each at the floor, then down to zero.  floor: (ny, nx) or NULL for floor_value everywhere.
+ * *n_limited (DEVICE int, may be NULL; the caller zeroes it) is incremented for every such column.  V_new must not
+ * alias V. */
+int pocean_freshwater_volumes_f64(const double* V, const double* dV, const double* floor_, double floor_value,
+                                  int nz, int ny, int nx, double* V_new, int* n_limited, void* stream);
+
+/* Divergence of the layer fluxes, Qx[..., 1:] - Qx[..., :-1] + Qy[:, 1:, :] - Qy[:, :-1, :]
+ * (core/components/layer_transport.py:146): Qx (nz, ny, nx+1), Qy (nz, ny+1, nx) -> divq (nz, ny, nx). */
+int pocean_flux_divergence_f64(const double* Qx, const double* Qy, int nz, int ny, int nx, double* divq,
+                               void* stream);
+
+/* ALE layer volumes V = h A (core/dynamics/sigma_baroclinic.py:1812-1815) and, when ok is not NULL,
+ * ok = active & (V > 0) (layer_transport.py:149). */
+int pocean_layer_volumes_f64(const double* h, const double* area, const uint8_t* active, int nz, int ny, int nx,
+                             double* V, uint8_t* ok, void* stream);
+
 /*
  * Batched steps of many independent domains (no counterpart in the reference, which advances one model at a time):
  * one ALE tracer step = advect_fct of the stack C then the remap of the advected stack C_adv onto the target grid,

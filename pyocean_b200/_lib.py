@@ -51,6 +51,10 @@ SIGNATURES: dict[str, tuple] = {
     "pocean_limit_outflow_f64": (_I, [_P, _P, _P, _P, _P, _I, _I, _I, _D, _D, _I, _U, ctypes.POINTER(_I),
                                       ctypes.POINTER(_I), _P, _Z, _P]),
     "pocean_lagrangian_thickness_f64": (_I, [_P, _P, _P, _I, _I, _I, _D, _D, _P, _P, _P]),
+    "pocean_upwind_transport_f64": (_I, [_P, _P, _P, _P, _P, _I, _I, _I, _P, _P]),
+    "pocean_freshwater_volumes_f64": (_I, [_P, _P, _P, _D, _I, _I, _I, _P, _P, _P]),
+    "pocean_flux_divergence_f64": (_I, [_P, _P, _I, _I, _I, _P, _P]),
+    "pocean_layer_volumes_f64": (_I, [_P, _P, _P, _I, _I, _I, _P, _P, _P]),
     "pocean_batch_device_bytes": (_Z, [_I]),
     "pocean_batch_create": (_I, [_P, _I, _I, _P, _Z, ctypes.POINTER(_P), _P]),
     "pocean_batch_step": (_I, [_P, _I, _I, _I, _P]),

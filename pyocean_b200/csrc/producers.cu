@@ -566,7 +566,103 @@ __global__ void __launch_bounds__(256) lagrangian_kernel(const double* __restric
     const double A = __ldg(area + t % pc);
     const double v = __ldg(h + t) - dt * __ldg(divq + t) / (A > 0 ? A : 1.0);
     if (v < -tol) atomicMin(bad, (unsigned long long)t);
-    out[t] = (v >= 0.0 || isnan(v)) ? v : 0.0;
+    out[t] = (v > 0.0 || isnan(v)) ? v : 0.0;                         // numpy.maximum(v, 0.0): +0.0 for v = -0.0
+}
+
+// ale.py:233-251 `upwind_transport_x`: one face column (numpy semantics: sums over k from 0.0 in layer order).
+__global__ void __launch_bounds__(128) upwind_kernel(const double* __restrict__ q_e, const double* __restrict__ q_w,
+                                                     const double* __restrict__ ut, const double* __restrict__ L,
+                                                     const double* __restrict__ Q_bt, int n, i64 pf,
+                                                     double* __restrict__ out)
+{
+    const i64 o = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (o >= pf) return;
+    const double Lo = __ldg(L + o);
+    double S = 0.0;
+    for (int k = 0; k < n; ++k) {
+        const i64 x = k * pf + o;
+        const double u = __ldg(ut + x);
+        const double F = (Lo * u) * (u >= 0 ? __ldg(q_e + x) : __ldg(q_w + x));
+        out[x] = F;
+        S += F;
+    }
+    const double R = __ldg(Q_bt + o) - S;
+    const bool pos = R >= 0;
+    double sq = 0.0;
+    for (int k = 0; k < n; ++k) sq += pos ? __ldg(q_e + k * pf + o) : __ldg(q_w + k * pf + o);
+    const bool use_e = sq > 0 ? pos : !pos;                          // the other side if this column is empty
+    const double* q = use_e ? q_e : q_w;
+    double tot = 0.0;
+    for (int k = 0; k < n; ++k) tot += __ldg(q + k * pf + o);
+    const double den = tot > 0 ? tot : 1.0;
+    for (int k = 0; k < n; ++k) {
+        const i64 x = k * pf + o;
+        out[x] = out[x] + R * __ldg(q + x) / den;
+    }
+}
+
+__device__ __forceinline__ double np_min(double a, double b) { return (a < b || isnan(a)) ? a : b; }
+__device__ __forceinline__ double np_max(double a, double b) { return (a > b || isnan(a)) ? a : b; }
+
+// core/components/freshwater.py:31-58 `freshwater_volumes`: one column per thread.
+__global__ void __launch_bounds__(128) freshwater_kernel(const double* __restrict__ V, const double* __restrict__ dV,
+                                                         const double* __restrict__ floor_arr, double floor_value,
+                                                         int n, i64 pc, double* __restrict__ out,
+                                                         int* __restrict__ n_limited)
+{
+    const i64 c = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= pc) return;
+    const double d = __ldg(dV + c);
+    const double fl = floor_arr ? __ldg(floor_arr + c) : floor_value;
+    const i64 top = (i64)(n - 1) * pc + c;
+    const double vtop = __ldg(V + top);
+    const double top_new = vtop + d;
+    if (!(d < 0 && top_new < fl)) {
+        for (int k = 0; k < n - 1; ++k) out[k * pc + c] = __ldg(V + k * pc + c);
+        out[top] = top_new;
+        return;
+    }
+    if (n_limited) atomicAdd(n_limited, 1);
+    double deficit = -d;
+    for (int k = n - 1; k >= 0; --k) {                               // first keep the floor
+        const double col = __ldg(V + k * pc + c);
+        const double take = np_min(deficit, np_max(col - fl, 0.0));
+        out[k * pc + c] = col - take;
+        deficit = deficit - take;
+    }
+    for (int k = n - 1; k >= 0; --k) {                               // then down to zero
+        const double col = out[k * pc + c];
+        const double take = np_min(deficit, np_max(col - 0.0, 0.0));
+        out[k * pc + c] = col - take;
+        deficit = deficit - take;
+    }
+}
+
+// div Q of each cell-layer: Qx[..., 1:] - Qx[..., :-1] + Qy[:, 1:, :] - Qy[:, :-1, :] (layer_transport.py:146).
+__global__ void __launch_bounds__(256) divergence_kernel(const double* __restrict__ Qx, const double* __restrict__ Qy,
+                                                         int ny, int nx, i64 total, double* __restrict__ out)
+{
+    const i64 t = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= total) return;
+    const i64 pc = (i64)ny * nx;
+    const int k = (int)(t / pc);
+    const i64 c = t - k * pc;
+    const int j = (int)(c / nx), i = (int)(c - (i64)j * nx);
+    const i64 ox = ((i64)k * ny + j) * (nx + 1) + i, oy = ((i64)k * (ny + 1) + j) * nx + i;
+    out[t] = __ldg(Qx + ox + 1) - __ldg(Qx + ox) + __ldg(Qy + oy + nx) - __ldg(Qy + oy);
+}
+
+// Layer volumes h A of the ALE coordinate (sigma_baroclinic.py:1812-1815) and ok = active & V > 0.
+__global__ void __launch_bounds__(256) volumes_kernel(const double* __restrict__ h, const double* __restrict__ area,
+                                                      const uint8_t* __restrict__ active, i64 pc, i64 total,
+                                                      double* __restrict__ V, uint8_t* __restrict__ ok)
+{
+    const i64 t = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= total) return;
+    const i64 c = t % pc;
+    const double v = __ldg(h + t) * __ldg(area + c);
+    V[t] = v;
+    if (ok) ok[t] = __ldg(active + c) != 0 && v > 0.0;
 }
 
 static size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
@@ -789,5 +885,63 @@ extern "C" int pocean_lagrangian_thickness_f64(const double* h, const double* di
     const i64 pc = (i64)ny * nx, total = pc * nz;
     pr::lagrangian_kernel<<<(unsigned)((total + 255) / 256), 256, 0, st>>>(h, divq, area, pc, total, dt, tol, h_dag,
                                                                             first_bad);
+    return pocean_check_launch(fn);
+}
+
+extern "C" int pocean_upwind_transport_f64(const double* q_e, const double* q_w, const double* ut, const double* L,
+                                           const double* Q_bt, int nz, int a, int b, double* Q, void* stream)
+{
+    const char* fn = "pocean_upwind_transport_f64";
+    if (nz < 1 || a < 1 || b < 1) return pocean_fail(POCEAN_EINVAL, "%s: bad sizes", fn);
+    if (!q_e || !q_w || !ut || !L || !Q_bt || !Q) return pocean_fail(POCEAN_EINVAL, "%s: null pointer", fn);
+    int rc = pocean_check_device();
+    if (rc) return rc;
+    const i64 pf = (i64)a * b;
+    pr::upwind_kernel<<<(unsigned)((pf + 127) / 128), 128, 0, (cudaStream_t)stream>>>(q_e, q_w, ut, L, Q_bt, nz, pf,
+                                                                                        Q);
+    return pocean_check_launch(fn);
+}
+
+extern "C" int pocean_freshwater_volumes_f64(const double* V, const double* dV, const double* floor_,
+                                             double floor_value, int nz, int ny, int nx, double* V_new,
+                                             int* n_limited, void* stream)
+{
+    const char* fn = "pocean_freshwater_volumes_f64";
+    if (nz < 1 || ny < 1 || nx < 1) return pocean_fail(POCEAN_EINVAL, "%s: bad sizes", fn);
+    if (!V || !dV || !V_new) return pocean_fail(POCEAN_EINVAL, "%s: null pointer", fn);
+    if (V_new == V) return pocean_fail(POCEAN_EINVAL, "%s: V_new must not alias V", fn);
+    int rc = pocean_check_device();
+    if (rc) return rc;
+    const i64 pc = (i64)ny * nx;
+    pr::freshwater_kernel<<<(unsigned)((pc + 127) / 128), 128, 0, (cudaStream_t)stream>>>(V, dV, floor_, floor_value,
+                                                                                           nz, pc, V_new, n_limited);
+    return pocean_check_launch(fn);
+}
+
+extern "C" int pocean_flux_divergence_f64(const double* Qx, const double* Qy, int nz, int ny, int nx, double* divq,
+                                          void* stream)
+{
+    const char* fn = "pocean_flux_divergence_f64";
+    if (nz < 1 || ny < 1 || nx < 1) return pocean_fail(POCEAN_EINVAL, "%s: bad sizes", fn);
+    if (!Qx || !Qy || !divq) return pocean_fail(POCEAN_EINVAL, "%s: null pointer", fn);
+    int rc = pocean_check_device();
+    if (rc) return rc;
+    const i64 total = (i64)nz * ny * nx;
+    pr::divergence_kernel<<<(unsigned)((total + 255) / 256), 256, 0, (cudaStream_t)stream>>>(Qx, Qy, ny, nx, total,
+                                                                                              divq);
+    return pocean_check_launch(fn);
+}
+
+extern "C" int pocean_layer_volumes_f64(const double* h, const double* area, const uint8_t* active, int nz, int ny,
+                                        int nx, double* V, uint8_t* ok, void* stream)
+{
+    const char* fn = "pocean_layer_volumes_f64";
+    if (nz < 1 || ny < 1 || nx < 1) return pocean_fail(POCEAN_EINVAL, "%s: bad sizes", fn);
+    if (!h || !area || !V || (ok && !active)) return pocean_fail(POCEAN_EINVAL, "%s: null pointer", fn);
+    int rc = pocean_check_device();
+    if (rc) return rc;
+    const i64 pc = (i64)ny * nx, total = (i64)nz * pc;
+    pr::volumes_kernel<<<(unsigned)((total + 255) / 256), 256, 0, (cudaStream_t)stream>>>(h, area, active, pc, total,
+                                                                                           V, ok);
     return pocean_check_launch(fn);
 }

@@ -1,15 +1,18 @@
 """
 The producers of the tracer step's inputs, with the reference's interface (core/vertical/ale.py), on B200:
-``face_transport_thickness``, ``transport_velocity``, ``ppm_edges_x``, ``ppm_transport_x``, ``limit_outflow`` and
-``lagrangian_thickness``.  With CUDA tensors the fluxes, h-dagger and everything in between stay in HBM, so a model
-that keeps its state on the device runs the whole ALE tracer step (these, then ``TracerAdvection.advect_fct`` and
-the remap) without a host round trip.  For v-faces call them on swapped horizontal axes, as the reference does
+``face_transport_thickness``, ``transport_velocity``, ``ppm_edges_x``, ``ppm_transport_x``, ``upwind_transport_x``,
+``limit_outflow`` and ``lagrangian_thickness``; ``freshwater_volumes`` (core/components/freshwater.py); and the whole
+Lagrangian step of ``ALELayerTransport`` (core/components/layer_transport.py:98-160) built from them.  With CUDA
+tensors the fluxes, h-dagger and everything in between stay in HBM, so a model that keeps its state on the device
+runs the whole ALE tracer step (these, then ``TracerAdvection.advect_fct`` and the remap) without a host round
+trip.  For v-faces call them on swapped horizontal axes, as the reference does
 (non-contiguous arrays are made contiguous).  Results are the reference's, bit for bit.
 """
 from __future__ import annotations
 
 import ctypes
 import warnings
+from dataclasses import dataclass
 
 import numpy as np
 import torch
@@ -18,6 +21,7 @@ from . import _lib
 from ._device import Converter, shape_of
 
 H_PPM_MIN = 2e-10                      # core/vertical/ale.py:297
+DZ_FLOOR = 1e-6                        # core/vertical/ale.py:63
 
 
 def face_transport_thickness(h, H, active, clip: bool):
@@ -126,3 +130,122 @@ def lagrangian_thickness(h, divq, dt: float, area, tol: float = 1e-9):
         raise RuntimeError(f"layer {k} of cell (j={j}, i={i}) emptied in the Lagrangian step: h† = {v:.3e} m "
                            f"(reduce dt)")
     return cv.out(out)
+
+
+def upwind_transport_x(q_e, q_w, ut, L, Q_bt):
+    """Donor-cell layer fluxes through the u-faces consistent with the free-surface flux (ale.py:233-251)."""
+    n, a, b = shape_of(ut)
+    cv = Converter(q_e, q_w, ut, L, Q_bt)
+    qe, qw, u = cv.f64(q_e), cv.f64(q_w), cv.f64(ut)
+    Ld, Qd = cv.f64(L, (a, b)), cv.f64(Q_bt, (a, b))
+    out = cv.empty((n, a, b))
+    _lib.check(_lib.lib().pocean_upwind_transport_f64(qe.data_ptr(), qw.data_ptr(), u.data_ptr(), Ld.data_ptr(),
+                                                      Qd.data_ptr(), n, a, b, out.data_ptr(), cv.stream()),
+               "upwind_transport_x")
+    return cv.out(out)
+
+
+def freshwater_volumes(V, dV, floor):
+    """(V_new, n_limited): dV added to the top layer, a removal beyond the floor taken from the layers below
+    (core/components/freshwater.py:31-58).  ``floor`` a scalar or (ny, nx)."""
+    n, ny, nx = shape_of(V)
+    scalar = np.ndim(floor) == 0 and not isinstance(floor, torch.Tensor)
+    cv = Converter(V, dV, *(() if scalar else (floor,)))
+    Vd, dd = cv.f64(V), cv.f64(dV, (ny, nx))
+    fd = None if scalar else cv.f64(floor, (ny, nx))
+    out = cv.empty((n, ny, nx))
+    nl = torch.zeros(1, dtype=torch.int32, device=cv.device)
+    _lib.check(_lib.lib().pocean_freshwater_volumes_f64(Vd.data_ptr(), dd.data_ptr(),
+                                                        None if fd is None else fd.data_ptr(),
+                                                        float(floor) if scalar else 0.0, n, ny, nx, out.data_ptr(),
+                                                        nl.data_ptr(), cv.stream()), "freshwater_volumes")
+    return cv.out(out), int(nl.item())
+
+
+@dataclass
+class LayerFluxes:
+    """The record ``ALELayerTransport`` returns (layer_transport.py:30-41)."""
+    Qx: object
+    Qy: object
+    Fz: object
+    V0: object
+    V1: object
+    ok: object
+    h_dagger: object = None
+    n_limited: int = 0
+    V_fw: object = None
+    h_fw: object = None
+
+
+def _swap(t: torch.Tensor) -> torch.Tensor:
+    return t.transpose(-1, -2).contiguous()
+
+
+class ALELayerTransport:
+    """The Lagrangian layer-transport step of the ALE core on B200, with the reference component's constructor and
+    call (layer_transport.py:98-160): transport velocities, the PPM or donor-cell layer fluxes (v-faces on swapped
+    axes), the outflow limiter, h-dagger, the layer volumes h A, ``ok`` and, with ``fluxes.fw``, the freshwater
+    thickness and volumes.  Open faces (``open_`` not empty) and the periodic PPM flux (the reference pads by 4 cells)
+    raise ``NotImplementedError``.  The ALE layer volumes are h A (sigma_baroclinic.py:1812-1815): the
+    ``layer_volumes`` callable is kept for the interface and not called.  Arrays are NumPy (results come back as
+    NumPy) or CUDA tensors (everything stays in HBM)."""
+
+    def __init__(self, *, fs, H, area, dt: float, thickness_flux: str, vi_geom: dict, layer_volumes=None,
+                 ob=None) -> None:
+        if thickness_flux not in ("ppm", "upwind"):
+            raise ValueError(f"thickness_flux {thickness_flux!r}: use 'ppm' or 'upwind'")
+        self.fs, self.H, self.area, self.dt, self.thickness_flux = fs, H, area, float(dt), thickness_flux
+        self.vi_geom, self.layer_volumes, self.ob = vi_geom, layer_volumes, ob
+        self.per = None
+
+    def __call__(self, st, eta_new, u_new, v_new, fluxes, theta_bc: float, open_, wu, wv, qe, qw, qn,
+                 qs) -> LayerFluxes:
+        if open_:
+            raise NotImplementedError("open-boundary face transports are not on the GPU")
+        px, py = bool(getattr(self.per, "x", False)), bool(getattr(self.per, "y", False))
+        if self.thickness_flux == "ppm" and (px or py):
+            raise NotImplementedError("the periodic PPM thickness flux (the reference pads by 4 cells)")
+        fw = getattr(fluxes, "fw", None)
+        n, ny, nx = shape_of(st.h)
+        fs, dt, L = self.fs, self.dt, _lib.lib()
+        cv = Converter(st.h, st.u, st.v, u_new, v_new, wu, wv, qe, qw, qn, qs, self.area, *(() if fw is None else (fw,)))
+        h = cv.f64(st.h)
+        act = cv.u8(fs.active, (ny, nx))
+        area = cv.f64(self.area, (ny, nx))
+        tb = theta_bc
+        utx, Qbx = transport_velocity(cv.f64(u_new), cv.f64(st.u), cv.u8(fluxes.wet_u, (ny, nx + 1)), cv.f64(wu),
+                                      cv.f64(fs.Lu, (ny, nx + 1)), cv.f64(fluxes.Du, (ny, nx + 1)), fs.theta, tb)
+        uty, Qby = transport_velocity(cv.f64(v_new), cv.f64(st.v), cv.u8(fluxes.wet_v, (ny + 1, nx)), cv.f64(wv),
+                                      cv.f64(fs.Lv, (ny + 1, nx)), cv.f64(fluxes.Dv, (ny + 1, nx)), fs.theta, tb)
+        Lv_t, Qby_t, uty_t = _swap(cv.f64(fs.Lv, (ny + 1, nx))), _swap(Qby), _swap(uty)
+        qn_d, qs_d = cv.f64(qn), cv.f64(qs)
+        if self.thickness_flux == "ppm":
+            Qx = ppm_transport_x(h, utx, cv.f64(fs.Lu, (ny, nx + 1)), Qbx, cv.f64(qe), cv.f64(qw), act, dt,
+                                 cv.f64(self.vi_geom["dx_t"], (ny, nx)))
+            Qy = _swap(ppm_transport_x(_swap(h), uty_t, Lv_t, Qby_t, qn_d, qs_d, _swap(act), dt,
+                                       _swap(cv.f64(self.vi_geom["dy_t"], (ny, nx)))))
+        else:
+            Qx = upwind_transport_x(cv.f64(qe), cv.f64(qw), utx, cv.f64(fs.Lu, (ny, nx + 1)), Qbx)
+            Qy = _swap(upwind_transport_x(qn_d, qs_d, uty_t, Lv_t, Qby_t))
+        Qx, Qy, n_lim = limit_outflow(h, Qx, Qy, area, dt, act, periodic=(px, py))
+        divh = cv.empty((n, ny, nx))
+        _lib.check(L.pocean_flux_divergence_f64(Qx.data_ptr(), Qy.data_ptr(), n, ny, nx, divh.data_ptr(),
+                                                cv.stream()), "flux_divergence")
+        h_lag = lagrangian_thickness(h, divh, dt, area)
+        V0, V1 = cv.empty((n, ny, nx)), cv.empty((n, ny, nx))
+        ok = torch.empty((n, ny, nx), dtype=torch.uint8, device=cv.device)
+        for hh, V, o in ((h, V0, None), (h_lag, V1, ok)):
+            _lib.check(L.pocean_layer_volumes_f64(hh.data_ptr(), area.data_ptr(), act.data_ptr(), n, ny, nx,
+                                                  V.data_ptr(), None if o is None else o.data_ptr(), cv.stream()),
+                       "layer_volumes")
+        Fz = torch.zeros((n + 1, ny, nx), dtype=torch.float64, device=cv.device)
+        h_fw = V_fw = None
+        if fw is not None:
+            h_fw, _ = freshwater_volumes(h_lag, cv.f64(fw, (ny, nx)) * dt, DZ_FLOOR)
+            V_fw = cv.empty((n, ny, nx))
+            _lib.check(L.pocean_layer_volumes_f64(h_fw.data_ptr(), area.data_ptr(), act.data_ptr(), n, ny, nx,
+                                                  V_fw.data_ptr(), None, cv.stream()), "layer_volumes")
+        okb = ok.bool()
+        return LayerFluxes(cv.out(Qx), cv.out(Qy), cv.out(Fz), cv.out(V0), cv.out(V1),
+                           okb.cpu().numpy() if cv.numpy_out else okb, cv.out(h_lag), int(n_lim),
+                           None if V_fw is None else cv.out(V_fw), None if h_fw is None else cv.out(h_fw))

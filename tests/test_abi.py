@@ -125,6 +125,12 @@ def test_neighbour_argument_errors():
 
 def test_producer_argument_errors_and_workspaces():
     L = _lib.lib()
+    assert L.pocean_upwind_transport_f64(8, 8, 8, 8, 8, 0, 3, 4, 8, None) == 1
+    assert L.pocean_upwind_transport_f64(8, None, 8, 8, 8, 2, 3, 4, 8, None) == 1
+    assert L.pocean_freshwater_volumes_f64(8, 8, None, 1e-6, 2, 3, 4, 8, None, None) == 1   # V_new aliases V
+    assert L.pocean_freshwater_volumes_f64(8, None, None, 1e-6, 2, 3, 4, 16, None, None) == 1
+    assert L.pocean_flux_divergence_f64(8, None, 2, 3, 4, 8, None) == 1
+    assert L.pocean_layer_volumes_f64(8, 8, None, 2, 3, 4, 8, 8, None) == 1                 # ok without active
     assert L.pocean_ppm_transport_workspace_bytes(4, 8, 9, 20) >= 2 * 4 * 8 * 9 * 8 + 5 * 8 * 10 * 8
     assert L.pocean_limit_outflow_workspace_bytes(4, 8, 9) >= 3 * 4 * 8 * 9 * 8
     assert L.pocean_face_transport_thickness_f64(None, 8, 8, 2, 3, 4, 1, 8, 8, None) == 1
