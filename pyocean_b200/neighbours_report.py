@@ -8,7 +8,8 @@ Timing of the neighbours of the tracer step at the benchmark size (512 x 512 x 5
 * the velocity remap in fraction space of the u-faces (512 x 513 x 50);
 * the producers of the step's inputs on the u-faces: face transport thickness, transport velocity, PPM layer
   transport with the barotropic Newton correction, the outflow limiter's check (nothing to limit, its common case)
-  and the Lagrangian thickness.
+  and the Lagrangian thickness;
+* the whole layer-transport step (``producers.ALELayerTransport``) with the PPM and the donor-cell flux.
 
     python -m pyocean_b200.neighbours_report
 """
@@ -166,6 +167,7 @@ def neighbours_report(device=None) -> dict:
 
     t_ftt, t_tvel = _time(ftt), _time(tvel)
     t_ppm = _time(ppm, reps=5)
+    t_lt = _layer_transport_ms(w, dev, rng)
     peak = _hbm_peak()
     return dict(workload=w.name,
                 regrid_remap_zstar=dict(call_ms=t_fused, regrid_ms=t_regrid, regrid_then_remap_columns_ms=t_sep,
@@ -175,7 +177,57 @@ def neighbours_report(device=None) -> dict:
                                  frac_of_measured_hbm=diff_bytes / t_diff / 1e6 / peak, fields=nt),
                 remap_faces_u=dict(ms=t_faces, faces=n * ny * nf),
                 producers_u=dict(face_transport_thickness_ms=t_ftt, transport_velocity_ms=t_tvel,
-                                 ppm_transport_ms=t_ppm, faces=n * ny * nf))
+                                 ppm_transport_ms=t_ppm, faces=n * ny * nf),
+                layer_transport_step=t_lt)
+
+
+def _layer_transport_ms(w, dev, rng) -> dict:
+    """The whole ALE layer-transport step (``producers.ALELayerTransport``: both face axes, PPM or donor-cell
+    fluxes, limiter, h-dagger, volumes) on device tensors, warm, mean of a few calls."""
+    from types import SimpleNamespace as NS
+
+    from . import producers as P
+    n, ny, nx = w.h_src.shape
+    g = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)                       # noqa: E731
+    act = w.wet
+    h = np.where(act[None], w.h_src, 0.0)
+    H = h.sum(0)
+    wet_u = np.zeros((ny, nx + 1), bool)
+    wet_u[:, 1:-1] = act[:, 1:] & act[:, :-1]
+    wet_v = np.zeros((ny + 1, nx), bool)
+    wet_v[1:-1] = act[1:] & act[:-1]
+    Du, Dv = np.zeros((ny, nx + 1)), np.zeros((ny + 1, nx))
+    Du[:, 1:-1] = np.minimum(H[:, 1:], H[:, :-1])
+    Dv[1:-1] = np.minimum(H[1:], H[:-1])
+    hd, Hd = g(h), g(H)
+    qe, qw = P.face_transport_thickness(hd, Hd, g(act), True)
+    qn, qs = P.face_transport_thickness(hd.transpose(1, 2).contiguous(), Hd.T.contiguous(), g(act.T), True)
+    from .vertical import face_fractions
+    wu = face_fractions(0.5 * (qe + qw))
+    wv = face_fractions(0.5 * (qn + qs)).transpose(1, 2).contiguous()
+    u = [g(rng.normal(0.0, 0.2, (n, ny, nx + 1)) * wet_u) for _ in range(2)]
+    v = [g(rng.normal(0.0, 0.2, (n, ny + 1, nx)) * wet_v) for _ in range(2)]
+    area = g(np.full((ny, nx), 4e6))
+    fs = NS(theta=0.6, active=g(act), Lu=g(np.full((ny, nx + 1), 2000.0)), Lv=g(np.full((ny + 1, nx), 2000.0)))
+    geom = {"dx_t": g(np.full((ny, nx), 2000.0)), "dy_t": g(np.full((ny, nx), 2000.0))}
+    fl = NS(wet_u=g(wet_u), wet_v=g(wet_v), Du=g(Du), Dv=g(Dv), fw=None)
+    st = NS(h=hd, u=u[0], v=v[0], eta=None)
+    out = {}
+    for flux in ("ppm", "upwind"):
+        lt = P.ALELayerTransport(fs=fs, H=Hd, area=area, dt=300.0, thickness_flux=flux, vi_geom=geom)
+        run = lambda: lt(st, None, u[1], v[1], fl, 0.5, (), wu, wv, qe, qw, qn, qs)            # noqa: E731
+        run()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(3):
+            lf = run()
+        e1.record()
+        e1.synchronize()
+        out[flux + "_ms"] = e0.elapsed_time(e1) / 3
+        out[flux + "_n_limited"] = lf.n_limited
+    out["what"] = "ALELayerTransport on device tensors, both face axes, 512 x 512 x 50 basin layers, dt 300 s"
+    return out
 
 
 if __name__ == "__main__":
