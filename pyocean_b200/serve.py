@@ -216,10 +216,11 @@ class Server:
         j.dom = None
 
 
-def serve_report(n_jobs: int = 200, rate: float = 15.0, seed: int = 0, device=None, batched_f64: bool = False) -> dict:
+def serve_report(n_jobs: int = 200, rate: float = 15.0, seed: int = 0, device=None, batched_f64: bool = False,
+                 saturated: bool = True) -> dict:
     """Serves the seeded Poisson stream batched in mixed precision (the served form) and one job at a time with the
-    plain FP64 kernels, then both once more with every job arriving at once (their saturated throughput);
-    ``batched_f64`` adds the batched FP64 form.  Latencies in seconds."""
+    plain FP64 kernels, then (``saturated``) both once more with every job arriving at once (their saturated
+    throughput); ``batched_f64`` adds the batched FP64 form.  Latencies in seconds."""
     dev = torch.device("cuda", torch.cuda.current_device()) if device is None else torch.device(device)
     # warm-up: load the library and the kernels, fill the allocator's pools
     Server(dev).run(job_stream(8, seed=seed + 7, rate=1e9))
@@ -232,17 +233,21 @@ def serve_report(n_jobs: int = 200, rate: float = 15.0, seed: int = 0, device=No
     out["one_at_a_time_f64"] = Server(dev, mixed=False, batched=False).run(stream(rate))
     if batched_f64:
         out["batched_f64"] = Server(dev, mixed=False).run(stream(rate))
-    out["saturated_batched_mixed"] = Server(dev, mixed=True).run(stream(1e9))
-    out["saturated_one_at_a_time_f64"] = Server(dev, mixed=False, batched=False).run(stream(1e9))
     out["p99_ratio_plain_vs_served"] = out["one_at_a_time_f64"]["p99_s"] / out["batched_mixed"]["p99_s"]
-    out["saturated_throughput_ratio_served_vs_plain"] = (out["saturated_batched_mixed"]["throughput"] /
-                                                         out["saturated_one_at_a_time_f64"]["throughput"])
+    if saturated:
+        out["saturated_batched_mixed"] = Server(dev, mixed=True).run(stream(1e9))
+        out["saturated_one_at_a_time_f64"] = Server(dev, mixed=False, batched=False).run(stream(1e9))
+        out["saturated_throughput_ratio_served_vs_plain"] = (out["saturated_batched_mixed"]["throughput"] /
+                                                             out["saturated_one_at_a_time_f64"]["throughput"])
     return out
 
 
 if __name__ == "__main__":
     import json
     import sys
-    n = int(sys.argv[1]) if len(sys.argv) > 1 else 200
-    r = float(sys.argv[2]) if len(sys.argv) > 2 else 15.0
-    print(json.dumps(serve_report(n, r, batched_f64=True)))
+    # python -m pyocean_b200.serve [jobs] [rate] [--no-saturated] [--no-batched-f64]
+    pos = [x for x in sys.argv[1:] if not x.startswith("--")]
+    n = int(pos[0]) if pos else 200
+    r = float(pos[1]) if len(pos) > 1 else 15.0
+    print(json.dumps(serve_report(n, r, batched_f64="--no-batched-f64" not in sys.argv,
+                                  saturated="--no-saturated" not in sys.argv)))
