@@ -33,6 +33,29 @@ sys.path.insert(0, ROOT)
 import numpy as np  # noqa: E402
 
 
+def ranks_from_env() -> tuple[int, int, int]:
+    """(rank, world size, local rank) of this process as torchrun sets them (1 process: 0, 1, 0)."""
+    return (int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")),
+            int(os.environ.get("LOCAL_RANK", "0")))
+
+
+def max_over_ranks(x: float, device) -> float:
+    """The largest x over all ranks of the process group (the job's time is its slowest rank's); x itself without
+    a group.  ``device``: where the reduction tensor lives (CUDA for NCCL, CPU for gloo)."""
+    import torch
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return x
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_rate(units_per_rank: float, world: int, ms: float) -> float:
+    """Whole-job throughput of weak-scaled replicas: every rank's units over the slowest rank's time [units/s]."""
+    return units_per_rank * world / (ms / 1e3)
+
+
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -223,10 +246,7 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> dict | None:
     res = bufs[(args.warmup + args.steps) % 2]
     assert bool(torch.isfinite(res[:, :, w.wet]).all()), "non-finite tracer values after the timed steps"
 
-    if world > 1:
-        t = torch.tensor([ms], dtype=torch.float64, device=dev)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(ms, dev)
 
     # ---- the mixed-precision form of the same step (FP32 WENO weights, FP64 limiter / bookkeeping / remap)
     mixed_stepper = ALETracerStep(nt, n, ny, nx, w.dt, flags, w.remap_scheme, device=dev, mixed=True)
@@ -243,10 +263,7 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> dict | None:
     torch.cuda.synchronize()
     mixed_ms = m0.elapsed_time(m1)
     mixed_adv = float(np.mean([e[0].elapsed_time(e[1]) for e in mevs]))
-    if world > 1:
-        t = torch.tensor([mixed_ms], dtype=torch.float64, device=dev)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        mixed_ms = float(t.item())
+    mixed_ms = max_over_ranks(mixed_ms, dev)
     del mixed_stepper
 
     # ---- end to end through the public API, pinned host tensors, copies inside the timed region
@@ -276,13 +293,10 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> dict | None:
         e1.record(stream)
         torch.cuda.synchronize()
         e2e_ms = e0.elapsed_time(e1) / args.e2e_steps
-    if world > 1:
-        t = torch.tensor([e2e_ms], dtype=torch.float64, device=dev)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        e2e_ms = float(t.item())
+    e2e_ms = max_over_ranks(e2e_ms, dev)
 
     cells = w.tracer_cells
-    value = cells * args.steps * world / (ms / 1e3)
+    value = job_rate(cells * args.steps, world, ms)
     ab = W.algorithmic_bytes(w)
     pk = peaks()
     adv_avg, rem_avg = float(np.mean(adv_ms)), float(np.mean(rem_ms))
@@ -329,10 +343,10 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> dict | None:
                                "remap_columns": {"ms": rem_avg, "GB/s": rem_gbs, "bytes": ab["remap"]},
                                "step": {"ms": ms / args.steps,
                                         "GB/s": ab["step"] / (ms / args.steps / 1e3) / 1e9}}},
-        "e2e": {"value": cells * world / (e2e_ms / 1e3), "unit": "tracer cell-steps/s", "h2d_bytes_per_step": h2d,
+        "e2e": {"value": job_rate(cells, world, e2e_ms), "unit": "tracer cell-steps/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms,
                 "api": "TracerAdvection.advect_fct + remap_columns on pinned host tensors"},
-        "mixed": {"value": cells * args.steps * world / (mixed_ms / 1e3), "ms_per_step": mixed_ms / args.steps,
+        "mixed": {"value": job_rate(cells * args.steps, world, mixed_ms), "ms_per_step": mixed_ms / args.steps,
                   "advect_fct_ms": mixed_adv, "speedup_vs_f64": ms / mixed_ms,
                   "what": "pocean_advect_fct_mixed (FP32 WENO5 weights and face values, FP64 fluxes, limiter and "
                           "bookkeeping) + FP64 PPM_H4 remap, same workload"},
@@ -344,9 +358,7 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> dict | None:
 
 def main():
     args = parse()
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    rank, world, local_rank = ranks_from_env()
     if args.impl == "reference":
         if rank != 0:
             return
@@ -372,15 +384,16 @@ def main():
     line = run_ours(args, rank, world, local_rank)
     import torch
     torch.cuda.empty_cache()
-    if not args.no_neighbours:
+    # the single-GPU reports run on one GPU only (a scaling run holds its GPUs for the timed replicas alone)
+    if not args.no_neighbours and world == 1:
         from pyocean_b200.neighbours_report import neighbours_report
         line["neighbours"] = neighbours_report()
         torch.cuda.empty_cache()
-    if args.batched_steps > 0:
+    if args.batched_steps > 0 and world == 1:
         from pyocean_b200.batch_report import batched_report
         line["batched"] = batched_report(steps=args.batched_steps)
         torch.cuda.empty_cache()
-    if args.serve_jobs > 0:
+    if args.serve_jobs > 0 and world == 1:
         from pyocean_b200.serve import serve_report
         line["served"] = serve_report(n_jobs=args.serve_jobs, rate=args.serve_rate)
         torch.cuda.empty_cache()
