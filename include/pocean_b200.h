@@ -53,6 +53,13 @@ const char* pocean_last_error(void);
 /* Library version as MAJOR*10000 + MINOR*100 + PATCH. */
 int pocean_version(void);
 
+/* Utility (no counterpart in the reference): a stream-ordered strided 2-D copy, height rows of width bytes from
+ * src (row pitch spitch) to dst (row pitch dpitch), in any direction the pointers allow (host pinned <-> device,
+ * device <-> device).  The host-array paths of the Python layer use it to stream row blocks so that copies overlap
+ * the kernels of other blocks. */
+int pocean_memcpy2d_async(void* dst, size_t dpitch, const void* src, size_t spitch, size_t width, size_t height,
+                          void* stream);
+
 /*
  * Workspace (bytes) that pocean_advect_fct_f64 needs for this shape.
  */

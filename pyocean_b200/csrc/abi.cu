@@ -46,3 +46,20 @@ int pocean_check_device()
 extern "C" const char* pocean_last_error(void) { return g_last_error; }
 
 extern "C" int pocean_version(void) { return 100; }   // 0.1.0
+
+// A strided 2-D copy in either direction (host pinned <-> device, or device <-> device), stream-ordered: the
+// host-buffer paths of the Python layer use it to move row blocks of a (planes, rows, columns) array between a
+// strided host array and a dense device block, so copies of one block overlap work on another.
+extern "C" int pocean_memcpy2d_async(void* dst, size_t dpitch, const void* src, size_t spitch, size_t width,
+                                     size_t height, void* stream)
+{
+    if (!dst || !src) return pocean_fail(POCEAN_EINVAL, "pocean_memcpy2d_async: null pointer");
+    if (width > dpitch || width > spitch)
+        return pocean_fail(POCEAN_EINVAL, "pocean_memcpy2d_async: width %zu exceeds a pitch (%zu, %zu)", width, dpitch,
+                           spitch);
+    if (width == 0 || height == 0) return POCEAN_OK;
+    cudaError_t e = cudaMemcpy2DAsync(dst, dpitch, src, spitch, width, height, cudaMemcpyDefault,
+                                      (cudaStream_t)stream);
+    if (e != cudaSuccess) return pocean_fail(POCEAN_ECUDA, "pocean_memcpy2d_async: %s", cudaGetErrorString(e));
+    return POCEAN_OK;
+}

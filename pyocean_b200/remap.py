@@ -4,13 +4,16 @@ Conservative vertical remap with the reference's interface (core/vertical/remap.
 ``remap_columns(h_src, f_src, h_tgt, scheme, wet)`` is the drop-in for ``core.vertical.remap.remap_columns``: every
 wet column of f_src (N0, ny, nx) goes from thicknesses h_src to h_tgt (N1, ny, nx); dry columns are copied when
 N0 == N1, else NaN.  It also takes a stack of fields (nf, N0, ny, nx) remapped in one launch (the ALE step remaps
-every tracer of the stack with the same thicknesses).  ``remap_column`` is the single-column form.
+every tracer of the stack with the same thicknesses).  ``remap_column`` is the single-column form.  Pinned host
+tensors are remapped in row blocks with the copies overlapping the kernels (``_pipeline``).
 """
 from __future__ import annotations
 
 import numpy as np
+import torch
 
 from . import _lib
+from . import _pipeline as _pl
 from ._device import Converter, shape_of
 
 PCM, PLM, PPM_H4 = _lib.PCM, _lib.PLM, _lib.PPM_H4
@@ -29,6 +32,10 @@ def remap_columns(h_src, f_src, h_tgt, scheme: int, wet):
     n0, ny, nx = hs
     n1 = ht[0]
     nf = fs[0] if stacked else 1
+    if _pl.pinned(h_src, f_src, h_tgt) and _wet_pinned(wet, ny, nx) and \
+            all(a.dtype == torch.float64 for a in (h_src, f_src, h_tgt)) and \
+            8 * nf * (n0 + n1) * ny * nx >= _pl.MIN_BYTES and ny >= 8:
+        return _remap_pipelined(h_src, f_src, h_tgt, wet, n0, n1, ny, nx, nf, int(scheme), stacked)
     cv = Converter(h_src, f_src, h_tgt, wet)
     hsd, fsd, htd = cv.f64(h_src), cv.f64(f_src), cv.f64(h_tgt)
     wd = cv.u8(wet, (ny, nx))
@@ -37,6 +44,46 @@ def remap_columns(h_src, f_src, h_tgt, scheme: int, wet):
                                              ny, nx, nf, int(scheme), out.data_ptr(), cv.stream())
     _lib.check(rc, "remap_columns")
     return cv.out(out)
+
+
+def _wet_pinned(wet, ny: int, nx: int) -> bool:
+    return (isinstance(wet, torch.Tensor) and not wet.is_cuda and wet.is_pinned() and wet.is_contiguous() and
+            tuple(wet.shape) == (ny, nx) and wet.dtype in (torch.bool, torch.uint8))
+
+
+def _remap_pipelined(h_src, f_src, h_tgt, wet, n0, n1, ny, nx, nf, scheme, stacked):
+    """remap_columns of pinned host tensors in row blocks of columns: block b's thicknesses and fields go to the
+    device on one stream while block b-1 is remapped on another and block b-2's result comes back on a third."""
+    dev = _pl.device_now()
+    s_in, s_cmp, s_out = _pl.streams(dev)
+    s_in.wait_stream(torch.cuda.current_stream(dev))
+    out = torch.empty((nf, n1, ny, nx) if stacked else (n1, ny, nx), dtype=torch.float64, pin_memory=True)
+    L, row, keep = _lib.lib(), 8 * nx, []
+    for j0, j1 in _pl.row_blocks(ny, 4):
+        r = j1 - j0
+        with torch.cuda.stream(s_in):
+            hs = torch.empty((n0, r, nx), dtype=torch.float64, device=dev)
+            ht = torch.empty((n1, r, nx), dtype=torch.float64, device=dev)
+            fc = torch.empty((nf, n0, r, nx), dtype=torch.float64, device=dev)
+            wc = torch.empty((r, nx), dtype=torch.uint8, device=dev)
+        _pl.copy2d(hs.data_ptr(), r * row, h_src.data_ptr() + j0 * row, ny * row, r * row, n0, s_in)
+        _pl.copy2d(ht.data_ptr(), r * row, h_tgt.data_ptr() + j0 * row, ny * row, r * row, n1, s_in)
+        _pl.copy2d(fc.data_ptr(), r * row, f_src.data_ptr() + j0 * row, ny * row, r * row, nf * n0, s_in)
+        _pl.copy2d(wc.data_ptr(), r * nx, wet.data_ptr() + j0 * nx, ny * nx, r * nx, 1, s_in)
+        ev = torch.cuda.Event()
+        ev.record(s_in)
+        s_cmp.wait_event(ev)
+        with torch.cuda.stream(s_cmp):
+            oc = torch.empty((nf, n1, r, nx), dtype=torch.float64, device=dev)
+        _lib.check(L.pocean_remap_columns_f64(hs.data_ptr(), fc.data_ptr(), ht.data_ptr(), wc.data_ptr(), n0, n1, r,
+                                              nx, nf, scheme, oc.data_ptr(), s_cmp.cuda_stream), "remap_columns")
+        ev = torch.cuda.Event()
+        ev.record(s_cmp)
+        s_out.wait_event(ev)
+        _pl.copy2d(out.data_ptr() + j0 * row, ny * row, oc.data_ptr(), r * row, r * row, nf * n1, s_out)
+        keep += [hs, ht, fc, wc, oc]
+    s_out.synchronize()
+    return out
 
 
 def remap_column(h_src, u_src, h_tgt, scheme: int, u_tgt=None):

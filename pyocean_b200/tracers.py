@@ -17,6 +17,7 @@ import numpy as np
 import torch
 
 from . import _lib
+from . import _pipeline as _pl
 from ._device import Converter, shape_of
 from .periodic import NONE
 
@@ -83,6 +84,11 @@ class TracerAdvection:
         nt, n, ny, nx = self._shapes(C, Qx, Qy)
         if shape_of(V0) != (n, ny, nx) or shape_of(V1) != (n, ny, nx):
             raise ValueError(f"volume shape {shape_of(V0)}/{shape_of(V1)} vs tracer layers {(n, ny, nx)}")
+        if (nt >= 2 and (inflow is None or inflow is C) and _pl.pinned(C, V0, V1, Qx, Qy, ok)
+                and all(a.dtype == torch.float64 for a in (C, V0, V1, Qx, Qy))
+                and ok.dtype in (torch.bool, torch.uint8) and tuple(ok.shape) in ((n, ny, nx), (ny, nx))
+                and 8 * nt * n * ny * nx >= _pl.MIN_BYTES):
+            return self._advect_fct_pipelined(C, V0, V1, Qx, Qy, ok, unlimited, flux_face_i)
         cv = Converter(C, V0, V1, Qx, Qy, ok, inflow)
         # tracers.py:230-231: an inflow stack that *is* C means "no exterior values" (each stage its own)
         own = inflow is None or (inflow is C and (isinstance(C, torch.Tensor) or
@@ -118,6 +124,63 @@ class TracerAdvection:
         if flux_face_i is None:
             return cv.out(out)
         return cv.out(out), cv.out(fx)
+
+    def _advect_fct_pipelined(self, C, V0, V1, Qx, Qy, ok, unlimited: bool, flux_face_i):
+        """advect_fct of pinned host tensors, one tracer of the stack at a time: the geometry goes to the device
+        first, then tracer t's field on the copy-in stream while tracer t-1 steps on the compute stream and tracer
+        t-2's result comes back on the copy-out stream (each tracer's step is independent of the others')."""
+        nt, n, ny, nx = C.shape
+        dev = _pl.device_now()
+        s_in, s_cmp, s_out = _pl.streams(dev)
+        s_in.wait_stream(torch.cuda.current_stream(dev))
+        L = _lib.lib()
+        fn = L.pocean_advect_fct_mixed if self.precision == "mixed" else L.pocean_advect_fct_f64
+        flags = self._flags() | (_lib.FCT_UNLIMITED if unlimited else 0)
+        fi = 0
+        if flux_face_i is not None:
+            fi = int(flux_face_i)
+            if fi < 0:
+                fi += nx + 1
+        record = self.record_open_flux and not unlimited
+        with torch.cuda.stream(s_in):
+            V0d, V1d, Qxd, Qyd = (a.to(dev, non_blocking=True) for a in (V0, V1, Qx, Qy))
+            okd = ok.to(dev, non_blocking=True)
+            okd = (okd if okd.dtype == torch.uint8 else (okd != 0).to(torch.uint8)).expand((n, ny, nx)).contiguous()
+        out = torch.empty((nt, n, ny, nx), dtype=torch.float64, pin_memory=True)
+        fx = torch.empty((nt, n, ny), dtype=torch.float64, pin_memory=True) if flux_face_i is not None else None
+        nbytes = L.pocean_advect_fct_workspace_bytes(1, n, ny, nx)
+        with torch.cuda.stream(s_cmp):
+            ws = torch.empty(max(nbytes, 256), dtype=torch.uint8, device=dev)
+            of = torch.empty((nt,), dtype=torch.float64, device=dev) if record else None
+        keep = [V0d, V1d, Qxd, Qyd, okd]
+        for t in range(nt):
+            with torch.cuda.stream(s_in):
+                ct = C[t].to(dev, non_blocking=True)
+            ev = torch.cuda.Event()
+            ev.record(s_in)
+            s_cmp.wait_event(ev)
+            with torch.cuda.stream(s_cmp):
+                ot = torch.empty((1, n, ny, nx), dtype=torch.float64, device=dev)
+                ft = torch.empty((1, n, ny), dtype=torch.float64, device=dev) if fx is not None else None
+            rc = fn(ct.data_ptr(), V0d.data_ptr(), V1d.data_ptr(), Qxd.data_ptr(), Qyd.data_ptr(), okd.data_ptr(),
+                    None, 1, n, ny, nx, flags, float(self.dt), ot.data_ptr(), fi,
+                    None if ft is None else ft.data_ptr(), None if of is None else of.data_ptr() + 8 * t,
+                    ws.data_ptr(), nbytes, s_cmp.cuda_stream)
+            _lib.check(rc, "advect_fct")
+            ev = torch.cuda.Event()
+            ev.record(s_cmp)
+            s_out.wait_event(ev)
+            with torch.cuda.stream(s_out):
+                out[t].copy_(ot[0], non_blocking=True)
+                if ft is not None:
+                    fx[t].copy_(ft[0], non_blocking=True)
+            keep += [ct, ot, ft]
+        s_out.synchronize()
+        if record:
+            self.last_open_flux = of.cpu().numpy()
+        if flux_face_i is None:
+            return out
+        return out, fx
 
     # ------------------------------------------------------------------------------------------------ RK3
     def advect(self, C, V0, V1, Qx, Qy, Fz, ok, inflow=None, flux_face_i: int | None = None):

@@ -1,0 +1,55 @@
+"""Pinned host tensors take the overlapped-copy paths (row blocks for the remap, one tracer at a time for the FCT
+step); their results equal the device-tensor and NumPy paths bit for bit, side outputs included."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+import torch
+
+import pyocean_b200 as P
+from pyocean_b200 import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+
+def _pin(a) -> torch.Tensor:
+    return torch.from_numpy(np.ascontiguousarray(a)).pin_memory()
+
+
+def _dev(a) -> torch.Tensor:
+    return torch.from_numpy(np.ascontiguousarray(a)).to("cuda")
+
+
+def test_remap_of_pinned_host_tensors_equals_device_path():
+    w = W.basin(seed=3, nx=256, ny=200, n=40)
+    ref = P.remap_columns(_dev(w.h_src), _dev(w.C), _dev(w.h_tgt), 2, _dev(w.wet)).cpu()
+    out = P.remap_columns(_pin(w.h_src), _pin(w.C), _pin(w.h_tgt), 2, _pin(w.wet))
+    assert out.is_pinned() and torch.equal(out, ref)
+    one = P.remap_columns(_pin(w.h_src), _pin(w.C[0]), _pin(w.h_tgt), 2, _pin(w.wet))   # a single field
+    assert torch.equal(one, ref[0])
+    np.testing.assert_array_equal(P.remap_columns(w.h_src, w.C, w.h_tgt, 2, w.wet), ref.numpy())
+
+
+@pytest.mark.parametrize("mixed", [False, True])
+def test_fct_step_of_pinned_host_tensors_equals_device_path(mixed):
+    w = W.zstar_box(seed=5, nx=256, ny=192, n=30, nt=3)
+    w.periodic, w.open = (), ("west", "east")
+    kw = dict(scheme="weno5", time="ssprk3", dt=w.dt, ob=P.OpenEdges(w.open))
+
+    def run(conv, ok):
+        adv = P.TracerAdvection(**kw, precision="mixed" if mixed else "f64")
+        adv.record_open_flux = True
+        out, fx = adv.advect_fct(conv(w.C), conv(w.V0), conv(w.V1), conv(w.Qx), conv(w.Qy), ok, flux_face_i=-1)
+        return out, fx, adv.last_open_flux
+
+    ref = run(_dev, _dev(w.ok))
+    got = run(_pin, _pin(w.ok))
+    assert got[0].is_pinned()
+    assert torch.equal(got[0], ref[0].cpu()) and torch.equal(got[1], ref[1].cpu())
+    np.testing.assert_array_equal(got[2], ref[2])
+    got2 = run(_pin, _pin(w.ok[0]))                      # ok given per column (ny, nx), broadcast over the layers
+    assert torch.equal(got2[0], run(_dev, _dev(w.ok[0]))[0].cpu())
+    adv = P.TracerAdvection(**kw)
+    un = adv.advect_fct(_pin(w.C), _pin(w.V0), _pin(w.V1), _pin(w.Qx), _pin(w.Qy), _pin(w.ok), unlimited=True)
+    assert torch.equal(un, adv.advect_fct(_dev(w.C), _dev(w.V0), _dev(w.V1), _dev(w.Qx), _dev(w.Qy), _dev(w.ok),
+                                          unlimited=True).cpu())

@@ -151,6 +151,51 @@ def test_fct_pulse_stays_bounded_where_unlimited_overshoots():
     assert un.max() > 1 + 1e-3
 
 
+def _box_advection(w):
+    adv = P.TracerAdvection(scheme="weno5", time="ssprk3", dt=w.dt, ob=P.OpenEdges(()))
+    adv.per = P.Periodic(w.periodic)
+    return adv
+
+
+@pytest.mark.parametrize("js", [False, True])
+def test_constant_field_stays_constant(js):
+    # tests/test_sigma_ale.py:1328-1339: C = 1 with V1 = V0 - dt div Q stays 1 (atol 1e-12), FCT and plain RK3
+    from pyocean_b200 import workloads as W
+    w = W.zstar_box(seed=3, nx=48, ny=40, n=6, nt=2)
+    adv = _box_advection(w)
+    adv.tracer_scheme = "weno5js" if js else "weno5"
+    C = np.ones_like(w.C)
+    out = adv.advect_fct(C, w.V0, w.V1, w.Qx, w.Qy, w.ok)
+    np.testing.assert_allclose(out, 1.0, rtol=0, atol=1e-12)
+    Fz = np.zeros((w.C.shape[1] + 1,) + w.C.shape[2:])
+    out = adv.advect(C, w.V0, w.V1, w.Qx, w.Qy, Fz, w.ok)
+    np.testing.assert_allclose(out, 1.0, rtol=0, atol=1e-12)
+
+
+def test_each_tracer_of_a_stack_stays_within_its_own_bounds_and_content():
+    # tests/test_sigma_ale.py:1342-1360, 1375-1384: per-tracer bounds and conservation (rtol 1e-12) of a stack with
+    # very different ranges, over 10 FCT steps of a periodic box
+    from pyocean_b200 import workloads as W
+    w = W.zstar_box(seed=4, nx=64, ny=48, n=5, nt=3)
+    rng = np.random.default_rng(8)
+    C = np.empty_like(w.C)
+    C[0] = rng.uniform(0.0, 1.0, C[0].shape)                                    # passive in [0, 1]
+    C[1] = 30.0 + 10.0 * (rng.random(C[1].shape) > 0.5)                         # a two-valued field in {30, 40}
+    C[2] = 1e-3 * np.sin(np.arange(C.shape[-1]) / 3.0)[None, None]             # small signed values
+    adv = _box_advection(w)
+    lo, hi = C.reshape(3, -1).min(1), C.reshape(3, -1).max(1)
+    c = C
+    for _ in range(10):                         # each step takes the volumes V0 -> V1 = V0 - dt div Q
+        c1 = adv.advect_fct(c, w.V0, w.V1, w.Qx, w.Qy, w.ok)
+        np.testing.assert_allclose((c1 * w.V1[None]).reshape(3, -1).sum(1), (c * w.V0[None]).reshape(3, -1).sum(1),
+                                   rtol=1e-12)
+        for t in range(3):
+            tol = 1e-12 * max(abs(lo[t]), abs(hi[t]))
+            assert c1[t].min() >= lo[t] - tol and c1[t].max() <= hi[t] + tol, t
+        c = c1
+    assert np.all(np.isfinite(c))
+
+
 # ---------------------------------------------------------------- larger seeded cases against the oracle
 def _random_case(seed, nt, n, ny, nx, open_=(), periodic=(), inflow=False, land=0.1):
     rng = np.random.default_rng(seed)
