@@ -96,6 +96,17 @@ int pocean_advect_fct_mixed(const double* C, const double* V0, const double* V1,
                             int nx, unsigned flags, double dt, double* C_out, int face_i, double* fx_face,
                             double* open_flux, void* workspace, size_t workspace_bytes, void* stream);
 
+/* Layer-range FCT passes (no counterpart in the reference): part 0 runs the three RK stage passes of layers
+ * k0 .. k1-1, part 1 the Zalesak coefficient and final passes of those layers (their bounds read layers k0-1 and
+ * k1, so part 0 of those layers must have run before, in stream order).  Blocks of layers covering 0 .. nz-1, each
+ * part 1 after part 0 of the next block, give pocean_advect_fct_f64 (mixed = 0) or _mixed (mixed = 1) bit for bit.
+ * The host-array path of the Python layer uses it to overlap the upload of later layers with the passes of earlier
+ * ones.  Same arguments as pocean_advect_fct_f64 without the side outputs; the unlimited flag is refused. */
+int pocean_advect_fct_layers(int mixed, const double* C, const double* V0, const double* V1, const double* Qx,
+                             const double* Qy, const uint8_t* ok, const double* inflow, int nt, int nz, int ny,
+                             int nx, unsigned flags, double dt, double* C_out, void* workspace,
+                             size_t workspace_bytes, int k0, int k1, int part, void* stream);
+
 /*
  * The same FCT step as pocean_advect_fct_f64 for callers that cannot allocate device memory (a host model that
  * reaches the GPU only through this ABI with no device allocator of its own, or one whose device memory belongs

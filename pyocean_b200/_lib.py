@@ -23,6 +23,8 @@ ERRORS = {1: "invalid argument", 2: "workspace", 3: "CUDA error", 4: "unsupporte
 # Every symbol the header declares, with its ctypes signature.
 _P, _I, _U, _D, _Z = ctypes.c_void_p, ctypes.c_int, ctypes.c_uint, ctypes.c_double, ctypes.c_size_t
 SIGNATURES: dict[str, tuple] = {
+    "pocean_advect_fct_layers": (_I, [_I, _P, _P, _P, _P, _P, _P, _P, _I, _I, _I, _I, _U, _D, _P, _P, _Z, _I, _I, _I,
+                                      _P]),
     "pocean_memcpy2d_async": (_I, [_P, _Z, _P, _Z, _Z, _Z, _P]),
     "pocean_last_error": (ctypes.c_char_p, []),
     "pocean_version": (_I, []),

@@ -377,12 +377,12 @@ __device__ __forceinline__ void final_body(const StepArgs& a, int i, int j, int 
 // Single-domain launches of passes 4 and 5: a 32 x 8 tile of one layer per CTA.
 __global__ void COEFF_BOUNDS fct_coeff_kernel(StepArgs a)
 {
-    coeff_body(a, blockIdx.x * TI + threadIdx.x % TI, blockIdx.y * TJ + threadIdx.x / TI, blockIdx.z);
+    coeff_body(a, blockIdx.x * TI + threadIdx.x % TI, blockIdx.y * TJ + threadIdx.x / TI, a.k0 + blockIdx.z);
 }
 
 __global__ void FINAL_BOUNDS fct_final_kernel(StepArgs a)
 {
-    final_body(a, blockIdx.x * TI + threadIdx.x % TI, blockIdx.y * TJ + threadIdx.x / TI, blockIdx.z);
+    final_body(a, blockIdx.x * TI + threadIdx.x % TI, blockIdx.y * TJ + threadIdx.x / TI, a.k0 + blockIdx.z);
 }
 
 // Batched launches of passes 4 and 5: domain d owns CTAs off[d] .. off[d+1]-1, one 32 x 8 tile of one layer each.
@@ -634,11 +634,11 @@ static int common_checks(const char* fn, const void* C, const void* V0, const vo
 #endif
 
 template <bool ZV, bool MIX>
-static void launch_split(const StepArgs& a, int stage, cudaStream_t st)
+static void launch_split(const StepArgs& a, int stage, cudaStream_t st, int nlayers = -1)
 {
     constexpr int R = POCEAN_FACE_ROWS;
     const Shape& s = a.s;
-    const dim3 grid(ceil_div(s.nx, TI), ceil_div(s.ny, R), s.nt * s.n);
+    const dim3 grid(ceil_div(s.nx, TI), ceil_div(s.ny, R), s.nt * (nlayers < 0 ? s.n : nlayers));
     if (stage == 1) {
         fct_faces_kernel<1, ZV, MIX, R><<<grid, TI * R, 0, st>>>(a);
         fct_update_kernel<1, R><<<grid, TI * R, 0, st>>>(a);
@@ -798,5 +798,49 @@ extern "C" int pocean_advect_rk3_f64(const double* C, const double* V0, const do
     rk3_stage_kernel<1><<<grid, NTHREADS, 0, st>>>(a);
     rk3_stage_kernel<2><<<grid, NTHREADS, 0, st>>>(a);
     rk3_stage_kernel<3><<<grid, NTHREADS, 0, st>>>(a);
+    return pocean_check_launch(fn);
+}
+
+// Layer-range FCT passes (no counterpart in the reference; the host-array path of the Python layer streams layer
+// blocks through them).  part 0: the three stage passes of layers k0 .. k1-1 (they read only those layers);
+// part 1: the coefficient and final passes of those layers, whose bounds read layers k0-1 and k1, so part 0 of
+// the neighbouring layers must have run first on the same stream.  Parts 0 and 1 over blocks covering 0 .. nz-1
+// give the result of pocean_advect_fct_f64 / _mixed bit for bit.  The workspace is the whole step's
+// (pocean_advect_fct_workspace_bytes); the unlimited step and the side outputs are not offered here.
+extern "C" int pocean_advect_fct_layers(int mixed, const double* C, const double* V0, const double* V1,
+                                        const double* Qx, const double* Qy, const uint8_t* ok, const double* inflow,
+                                        int nt, int nz, int ny, int nx, unsigned flags, double dt, double* C_out,
+                                        void* workspace, size_t workspace_bytes, int k0, int k1, int part,
+                                        void* stream)
+{
+    const char* fn = "pocean_advect_fct_layers";
+    if (flags & POCEAN_FCT_UNLIMITED) return pocean_fail(POCEAN_EINVAL, "%s: the unlimited step is not offered", fn);
+    if (k0 < 0 || k1 > nz || k0 >= k1) return pocean_fail(POCEAN_EINVAL, "%s: layers %d .. %d of %d", fn, k0, k1, nz);
+    if (part != 0 && part != 1) return pocean_fail(POCEAN_EINVAL, "%s: part %d (0 or 1)", fn, part);
+    int rc = common_checks(fn, C, V0, V1, Qx, Qy, ok, C_out, nt, nz, ny, nx, flags, 0, nullptr, workspace,
+                           workspace_bytes, pocean_advect_fct_workspace_bytes(nt, nz, ny, nx));
+    if (rc) return rc;
+    cudaStream_t st = (cudaStream_t)stream;
+    StepArgs a{};
+    a.s = Shape{nt, nz, ny, nx};
+    a.flags = flags;
+    a.dt = dt;
+    a.C = C; a.V0 = V0; a.V1 = V1; a.Qx = Qx; a.Qy = Qy; a.Fz = nullptr; a.ok = ok; a.inflow = inflow;
+    carve_fct_workspace(a, workspace);
+    a.out = C_out;
+    a.k0 = k0;
+    const int nl = k1 - k0;
+    if (part == 0) {
+        const bool zv = !(flags & POCEAN_WENO_JS);
+        for (int stage = 1; stage <= 3; ++stage) {
+            if (zv && !mixed) launch_split<true, false>(a, stage, st, nl);
+            else if (!zv && !mixed) launch_split<false, false>(a, stage, st, nl);
+            else if (zv) launch_split<true, true>(a, stage, st, nl);
+            else launch_split<false, true>(a, stage, st, nl);
+        }
+    } else {
+        fct_coeff_kernel<<<dim3(ceil_div(nx, TI), ceil_div(ny, TJ), nl), NTHREADS, 0, st>>>(a);
+        fct_final_kernel<<<dim3(ceil_div(nx, TI), ceil_div(ny, TJ), nl), NTHREADS, 0, st>>>(a);
+    }
     return pocean_check_launch(fn);
 }

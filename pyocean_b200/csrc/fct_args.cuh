@@ -33,13 +33,14 @@ struct StepArgs {
     double* c2;
     double* Sx;                         // FCT: F0, then the antidiffusive flux A
     double* Sy;
-    double* Tx;                         // FCT: (F0 + F1)/6
+    double* Tx;                         // FCT: F1
     double* Ty;
     double* tef0;                       // RK3 TEF column accumulators (nt, n, ny)
     double* tef1;
     // outputs
     double* out;
     int face_i;
+    int k0;                             // first layer of a layer-range launch of the single-domain passes (else 0)
     double* fx_face;
 };
 

@@ -246,7 +246,7 @@ __device__ __forceinline__ void faces_body(const StepArgs& a, int t, int k, int 
 template <int STAGE, bool ZV, bool MIX, int TJR>
 __device__ __forceinline__ void faces_plane(const StepArgs& a)
 {
-    const int p = blockIdx.z, k = p / a.s.nt, t = p - k * a.s.nt;
+    const int p = a.k0 * a.s.nt + blockIdx.z, k = p / a.s.nt, t = p - k * a.s.nt;
     faces_body<STAGE, ZV, MIX>(a, t, k, blockIdx.x * TI + threadIdx.x % TI, blockIdx.y * TJR + threadIdx.x / TI);
 }
 
@@ -335,7 +335,7 @@ __device__ __forceinline__ void update_body(const StepArgs& a, int t, int k, int
 template <int STAGE, int TJR>
 __global__ void __launch_bounds__(TI * TJR) fct_update_kernel(StepArgs a)
 {
-    const int p = blockIdx.z, k = p / a.s.nt, t = p - k * a.s.nt;
+    const int p = a.k0 * a.s.nt + blockIdx.z, k = p / a.s.nt, t = p - k * a.s.nt;
     update_body<STAGE>(a, t, k, blockIdx.x * TI + threadIdx.x % TI, blockIdx.y * TJR + threadIdx.x / TI);
 }
 

@@ -59,7 +59,7 @@ def _remap_pipelined(h_src, f_src, h_tgt, wet, n0, n1, ny, nx, nf, scheme, stack
     s_in.wait_stream(torch.cuda.current_stream(dev))
     out = torch.empty((nf, n1, ny, nx) if stacked else (n1, ny, nx), dtype=torch.float64, pin_memory=True)
     L, row, keep = _lib.lib(), 8 * nx, []
-    for j0, j1 in _pl.row_blocks(ny, 4):
+    for j0, j1 in _pl.row_blocks(ny, _pl.REMAP_ROW_BLOCKS):
         r = j1 - j0
         with torch.cuda.stream(s_in):
             hs = torch.empty((n0, r, nx), dtype=torch.float64, device=dev)

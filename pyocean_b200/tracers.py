@@ -88,6 +88,8 @@ class TracerAdvection:
                 and all(a.dtype == torch.float64 for a in (C, V0, V1, Qx, Qy))
                 and ok.dtype in (torch.bool, torch.uint8) and tuple(ok.shape) in ((n, ny, nx), (ny, nx))
                 and 8 * nt * n * ny * nx >= _pl.MIN_BYTES):
+            if not unlimited and flux_face_i is None and not self.record_open_flux:
+                return self._advect_fct_layered(C, V0, V1, Qx, Qy, ok)
             return self._advect_fct_pipelined(C, V0, V1, Qx, Qy, ok, unlimited, flux_face_i)
         cv = Converter(C, V0, V1, Qx, Qy, ok, inflow)
         # tracers.py:230-231: an inflow stack that *is* C means "no exterior values" (each stage its own)
@@ -124,6 +126,70 @@ class TracerAdvection:
         if flux_face_i is None:
             return cv.out(out)
         return cv.out(out), cv.out(fx)
+
+    def _advect_fct_layered(self, C, V0, V1, Qx, Qy, ok):
+        """advect_fct of pinned host tensors in blocks of layers: block b's tracers and geometry go to the device on
+        the copy-in stream while the stage passes of block b-1 and the limiter passes of block b-2 run on the
+        compute stream (``pocean_advect_fct_layers``: a block's limiter reads the layers either side of it) and
+        finished blocks come back on the copy-out stream."""
+        nt, n, ny, nx = C.shape
+        dev = _pl.device_now()
+        s_in, s_cmp, s_out = _pl.streams(dev)
+        s_in.wait_stream(torch.cuda.current_stream(dev))
+        L = _lib.lib()
+        mixed = int(self.precision == "mixed")
+        flags = self._flags()
+        f64 = dict(dtype=torch.float64, device=dev)
+        with torch.cuda.stream(s_in):
+            Cd = torch.empty((nt, n, ny, nx), **f64)
+            V0d, V1d = torch.empty((n, ny, nx), **f64), torch.empty((n, ny, nx), **f64)
+            Qxd, Qyd = torch.empty((n, ny, nx + 1), **f64), torch.empty((n, ny + 1, nx), **f64)
+            if ok.dim() == 2:                       # per column: uploaded once, broadcast over the layers
+                okd = ok.to(dev, non_blocking=True)
+                okd = (okd if okd.dtype == torch.uint8 else (okd != 0).to(torch.uint8)).expand((n, ny, nx)).contiguous()
+            else:
+                okd = torch.empty((n, ny, nx), dtype=torch.uint8, device=dev)
+        nbytes = L.pocean_advect_fct_workspace_bytes(nt, n, ny, nx)
+        with torch.cuda.stream(s_cmp):
+            outd = torch.empty((nt, n, ny, nx), **f64)
+            ws = torch.empty(max(nbytes, 256), dtype=torch.uint8, device=dev)
+        out = torch.empty((nt, n, ny, nx), dtype=torch.float64, pin_memory=True)
+        pl, px, py = ny * nx, ny * (nx + 1), (ny + 1) * nx
+
+        def layers(k0, k1, part):
+            _lib.check(L.pocean_advect_fct_layers(mixed, Cd.data_ptr(), V0d.data_ptr(), V1d.data_ptr(),
+                                                  Qxd.data_ptr(), Qyd.data_ptr(), okd.data_ptr(), None, nt, n, ny,
+                                                  nx, flags, float(self.dt), outd.data_ptr(), ws.data_ptr(), nbytes,
+                                                  k0, k1, part, s_cmp.cuda_stream), "advect_fct")
+
+        def download(k0, k1):
+            ev = torch.cuda.Event()
+            ev.record(s_cmp)
+            s_out.wait_event(ev)
+            _pl.copy2d(out.data_ptr() + 8 * k0 * pl, 8 * n * pl, outd.data_ptr() + 8 * k0 * pl, 8 * n * pl,
+                       8 * (k1 - k0) * pl, nt, s_out)
+
+        blocks = _pl.row_blocks(n, _pl.FCT_LAYER_BLOCKS)
+        for b, (k0, k1) in enumerate(blocks):
+            nl = k1 - k0
+            _pl.copy2d(Cd.data_ptr() + 8 * k0 * pl, 8 * n * pl, C.data_ptr() + 8 * k0 * pl, 8 * n * pl, 8 * nl * pl,
+                       nt, s_in)
+            for dst, src, per in ((V0d, V0, pl), (V1d, V1, pl), (Qxd, Qx, px), (Qyd, Qy, py)):
+                _pl.copy2d(dst.data_ptr() + 8 * k0 * per, 8 * nl * per, src.data_ptr() + 8 * k0 * per, 8 * nl * per,
+                           8 * nl * per, 1, s_in)
+            if ok.dim() == 3:                       # bool or uint8 bytes, one per cell
+                _pl.copy2d(okd.data_ptr() + k0 * pl, nl * pl, ok.data_ptr() + k0 * pl, nl * pl, nl * pl, 1, s_in)
+            ev = torch.cuda.Event()
+            ev.record(s_in)
+            s_cmp.wait_event(ev)
+            layers(k0, k1, 0)
+            if b > 0:
+                layers(*blocks[b - 1], 1)
+                download(*blocks[b - 1])
+        layers(*blocks[-1], 1)
+        download(*blocks[-1])
+        s_out.synchronize()
+        return out
 
     def _advect_fct_pipelined(self, C, V0, V1, Qx, Qy, ok, unlimited: bool, flux_face_i):
         """advect_fct of pinned host tensors, one tracer of the stack at a time: the geometry goes to the device

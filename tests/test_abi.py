@@ -105,6 +105,16 @@ def test_batch_argument_errors():
     assert L.pocean_batch_step(None, 0, 2, 0, None) == 1
 
 
+def test_layer_range_fct_argument_errors():
+    L = _lib.lib()
+    ws = 256 * 1024 * 1024
+    call = lambda k0, k1, part, flags=0: L.pocean_advect_fct_layers(                           # noqa: E731
+        0, 8, 8, 8, 8, 8, 8, None, 1, 4, 3, 3, flags, 1.0, 8, 256, ws, k0, k1, part, None)
+    assert call(0, 5, 0) == 1 and call(2, 2, 0) == 1 and call(-1, 2, 1) == 1      # layer range
+    assert call(0, 4, 2) == 1                                                     # part
+    assert call(0, 4, 0, _lib.FCT_UNLIMITED) == 1                                 # unlimited refused
+
+
 def test_neighbour_argument_errors():
     L = _lib.lib()
     # unknown rule, too many layers, null pointers, bad scheme

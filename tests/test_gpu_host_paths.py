@@ -1,5 +1,6 @@
-"""Pinned host tensors take the overlapped-copy paths (row blocks for the remap, one tracer at a time for the FCT
-step); their results equal the device-tensor and NumPy paths bit for bit, side outputs included."""
+"""Pinned host tensors take the overlapped-copy paths (row blocks for the remap; layer blocks for the FCT step, or
+one tracer at a time when side outputs are asked for); their results equal the device-tensor and NumPy paths bit
+for bit, side outputs included."""
 from __future__ import annotations
 
 import numpy as np
@@ -53,3 +54,18 @@ def test_fct_step_of_pinned_host_tensors_equals_device_path(mixed):
     un = adv.advect_fct(_pin(w.C), _pin(w.V0), _pin(w.V1), _pin(w.Qx), _pin(w.Qy), _pin(w.ok), unlimited=True)
     assert torch.equal(un, adv.advect_fct(_dev(w.C), _dev(w.V0), _dev(w.V1), _dev(w.Qx), _dev(w.Qy), _dev(w.ok),
                                           unlimited=True).cpu())
+
+
+@pytest.mark.parametrize("mixed,js", [(False, False), (True, False), (False, True)])
+def test_fct_step_in_layer_blocks_equals_device_path(mixed, js):
+    w = W.basin(seed=9, nx=256, ny=160, n=40, nt=2)
+    kw = dict(scheme="weno5js" if js else "weno5", time="ssprk3", dt=w.dt, ob=P.OpenEdges(w.open),
+              precision="mixed" if mixed else "f64")
+    adv = P.TracerAdvection(**kw)
+    adv.per = P.Periodic(w.periodic)
+    ref = adv.advect_fct(_dev(w.C), _dev(w.V0), _dev(w.V1), _dev(w.Qx), _dev(w.Qy), _dev(w.ok)).cpu()
+    for ok in (w.ok, w.ok[0]):                            # per cell-layer, and per column broadcast over the layers
+        got = adv.advect_fct(_pin(w.C), _pin(w.V0), _pin(w.V1), _pin(w.Qx), _pin(w.Qy), _pin(ok))
+        want = ref if ok is w.ok else adv.advect_fct(_dev(w.C), _dev(w.V0), _dev(w.V1), _dev(w.Qx), _dev(w.Qy),
+                                                     _dev(ok)).cpu()
+        assert got.is_pinned() and torch.equal(got, want)
