@@ -15,8 +15,8 @@ from . import _lib
 
 _STREAMS: dict = {}
 MIN_BYTES = 32 << 20            # smaller calls run the one-shot path (their copies are short anyway)
-REMAP_ROW_BLOCKS = 8            # row blocks of the remap's host path (8 and 6 measured best)
-FCT_LAYER_BLOCKS = 6            # layer blocks of the FCT step's host path (at 512 x 512 x 50)
+REMAP_ROW_BLOCKS = 8            # row blocks of the remap's host path (swept at 512 x 512 x 50)
+FCT_LAYER_BLOCKS = 6            # layer blocks of the FCT step's host path (swept likewise)
 
 
 def streams(device: torch.device) -> tuple:
