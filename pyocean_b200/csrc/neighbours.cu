@@ -388,13 +388,20 @@ __device__ __forceinline__ void fraction_io(FractionIO<NF>& io, const double* hf
     io.S = ts > 0.0 ? ts : 1.0;
 }
 
+// Register budgets of the velocity remap as resident 128-thread CTAs per SM, one field per thread (NF = 1) or two:
+// fitted to 7 and 5 (u-faces of 512 x 512 x 50: 1.17 and 1.93 ms against 1.43 and 2.48 at ptxas's own choice of
+// 108 / 152 registers; 5 / 6 and 3 / 4 in between).
+#ifndef POCEAN_VREMAP1_CTAS
+#define POCEAN_VREMAP1_CTAS 7
+#endif
+#ifndef POCEAN_VREMAP2_CTAS
+#define POCEAN_VREMAP2_CTAS 5
+#endif
 // One thread per face column and field group (NF fields from NF * blockIdx.y).
 template <int NF>
-__global__ void __launch_bounds__(128) remap_faces_kernel(const double* __restrict__ vel,
-                                                          const double* __restrict__ hf_src,
-                                                          const double* __restrict__ hf_tgt,
-                                                          const double* __restrict__ w_tgt, int n, i64 plane,
-                                                          int field0, int scheme, double* __restrict__ out)
+__global__ void __launch_bounds__(128, NF == 1 ? POCEAN_VREMAP1_CTAS : POCEAN_VREMAP2_CTAS)
+remap_faces_kernel(const double* __restrict__ vel, const double* __restrict__ hf_src, const double* __restrict__ hf_tgt,
+                   const double* __restrict__ w_tgt, int n, i64 plane, int field0, int scheme, double* __restrict__ out)
 {
     const i64 c = (i64)blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= plane) return;
@@ -446,7 +453,17 @@ __global__ void __launch_bounds__(128) face_fractions_kernel(const double* __res
 // loads are issued together and the masks applied afterwards.
 constexpr int DTI = 32, DTJ = 4, DKL = 4;
 
-__global__ void __launch_bounds__(DTI * DTJ) diffuse_ale_kernel(const double* __restrict__ T,
+// Register budget of the diffusion as resident 128-thread CTAs per SM: fitted to 12 (T and S at 512 x 512 x 50:
+// 0.236 ms against 0.334 at ptxas's choice of 80 registers, 0.273 at 8 and 0.246 at 10).
+#ifndef POCEAN_DIFF_CTAS
+#define POCEAN_DIFF_CTAS 12
+#endif
+#if POCEAN_DIFF_CTAS > 0
+#define DIFF_BOUNDS __launch_bounds__(DTI * DTJ, POCEAN_DIFF_CTAS)
+#else
+#define DIFF_BOUNDS __launch_bounds__(DTI * DTJ)
+#endif
+__global__ void DIFF_BOUNDS diffuse_ale_kernel(const double* __restrict__ T,
                                                                 const double* __restrict__ Tw,
                                                                 const double* __restrict__ h,
                                                                 const uint8_t* __restrict__ act,

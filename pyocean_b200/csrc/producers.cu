@@ -261,8 +261,20 @@ __device__ __forceinline__ void column_flux(const PPMArgs& a, int j, int f, doub
     }
 }
 
+// Register budget of the PPM Newton passes as resident 128-thread CTAs per SM: fitted to 7 (the layer loops are
+// load-latency bound; 512 x 512 x 50 u-faces, 20 iterations: 3.98 ms against 5.00 at ptxas's choice of 79-94
+// registers, 4.29 at 8, 4.79 at 9, 5.26 at 12).
+#ifndef POCEAN_PPM_CTAS
+#define POCEAN_PPM_CTAS 7
+#endif
+#if POCEAN_PPM_CTAS > 0
+#define PPM_BOUNDS __launch_bounds__(128, POCEAN_PPM_CTAS)
+#else
+#define PPM_BOUNDS __launch_bounds__(128)
+#endif
+
 // The first pass of _ppm_transport_kernel: bracket, fluxes at du = 0.
-__global__ void __launch_bounds__(128) ppm_init_kernel(PPMArgs a)
+__global__ void PPM_BOUNDS ppm_init_kernel(PPMArgs a)
 {
     const int nx = a.nx, nf = nx + 1;
     const i64 o = (i64)blockIdx.x * blockDim.x + threadIdx.x;
@@ -287,7 +299,7 @@ __global__ void __launch_bounds__(128) ppm_init_kernel(PPMArgs a)
 }
 
 // Newton step `it` (0-based) with bracketing bisection; skipped when iteration it-1 left no face unconverged.
-__global__ void __launch_bounds__(128) ppm_iter_kernel(PPMArgs a, int it)
+__global__ void PPM_BOUNDS ppm_iter_kernel(PPMArgs a, int it)
 {
     if (it > 0 && *(volatile int*)(a.unconverged + it - 1) == 0) return;
     const int nf = a.nx + 1;
@@ -313,7 +325,7 @@ __global__ void __launch_bounds__(128) ppm_iter_kernel(PPMArgs a, int it)
 }
 
 // Final fluxes with the converged correction and the residual share (cnuity.F90 style, ale.py:718-740).
-__global__ void __launch_bounds__(128) ppm_final_kernel(PPMArgs a, double* __restrict__ out)
+__global__ void PPM_BOUNDS ppm_final_kernel(PPMArgs a, double* __restrict__ out)
 {
     const int nf = a.nx + 1;
     const i64 o = (i64)blockIdx.x * blockDim.x + threadIdx.x;
