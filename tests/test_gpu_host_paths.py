@@ -69,3 +69,25 @@ def test_fct_step_in_layer_blocks_equals_device_path(mixed, js):
         want = ref if ok is w.ok else adv.advect_fct(_dev(w.C), _dev(w.V0), _dev(w.V1), _dev(w.Qx), _dev(w.Qy),
                                                      _dev(ok)).cpu()
         assert got.is_pinned() and torch.equal(got, want)
+
+
+def test_remap_of_pinned_host_tensors_onto_a_different_layer_count():
+    w = W.basin(seed=4, nx=192, ny=256, n=30)
+    rng = np.random.default_rng(2)
+    h1 = rng.uniform(0.5, 2.0, (45,) + w.h_src.shape[1:])
+    h1 *= w.h_src.sum(0) / h1.sum(0)
+    ref = P.remap_columns(_dev(w.h_src), _dev(w.C), _dev(h1), 1, _dev(w.wet)).cpu()
+    got = P.remap_columns(_pin(w.h_src), _pin(w.C), _pin(h1), 1, _pin(w.wet))
+    assert got.shape == (2, 45) + w.h_src.shape[1:]
+    np.testing.assert_array_equal(got.numpy(), ref.numpy())            # dry columns are NaN when N1 != N0
+
+
+def test_fct_step_in_layer_blocks_on_a_periodic_box():
+    w = W.zstar_box(seed=6, nx=256, ny=256, n=24, nt=3)                  # periodic x, walls in y (36 MB stack)
+    from pyocean_b200 import _pipeline
+    assert w.C.nbytes >= _pipeline.MIN_BYTES                           # large enough for the overlapped path
+    adv = P.TracerAdvection(scheme="weno5", time="ssprk3", dt=w.dt)
+    adv.per = P.Periodic(w.periodic)
+    ref = adv.advect_fct(_dev(w.C), _dev(w.V0), _dev(w.V1), _dev(w.Qx), _dev(w.Qy), _dev(w.ok)).cpu()
+    got = adv.advect_fct(_pin(w.C), _pin(w.V0), _pin(w.V1), _pin(w.Qx), _pin(w.Qy), _pin(w.ok))
+    assert torch.equal(got, ref)
