@@ -9,7 +9,8 @@ Timing of the neighbours of the tracer step at the benchmark size (512 x 512 x 5
 * the producers of the step's inputs on the u-faces: face transport thickness, transport velocity, PPM layer
   transport with the barotropic Newton correction, the outflow limiter's check (nothing to limit, its common case)
   and the Lagrangian thickness;
-* the whole layer-transport step (``producers.ALELayerTransport``) with the PPM and the donor-cell flux.
+* the whole layer-transport step (``producers.ALELayerTransport``) with the PPM and the donor-cell flux;
+* the unlimited RK3 step ``TracerAdvection.advect`` with a vertical transport (the secondary path).
 
     python -m pyocean_b200.neighbours_report
 """
@@ -168,6 +169,7 @@ def neighbours_report(device=None) -> dict:
     t_ftt, t_tvel = _time(ftt), _time(tvel)
     t_ppm = _time(ppm, reps=5)
     t_lt = _layer_transport_ms(w, dev, rng)
+    t_rk3 = _advect_rk3_ms(w, dev)
     peak = _hbm_peak()
     return dict(workload=w.name,
                 regrid_remap_zstar=dict(call_ms=t_fused, regrid_ms=t_regrid, regrid_then_remap_columns_ms=t_sep,
@@ -178,7 +180,29 @@ def neighbours_report(device=None) -> dict:
                 remap_faces_u=dict(ms=t_faces, faces=n * ny * nf),
                 producers_u=dict(face_transport_thickness_ms=t_ftt, transport_velocity_ms=t_tvel,
                                  ppm_transport_ms=t_ppm, faces=n * ny * nf),
-                layer_transport_step=t_lt)
+                layer_transport_step=t_lt, advect_rk3=t_rk3)
+
+
+def _advect_rk3_ms(w, dev) -> dict:
+    """``TracerAdvection.advect`` (SSP-RK3 without limiter, WENO5 in x, y and z) of the basin's stack with a
+    vertical transport through the interfaces, on device tensors."""
+    from .step import ALETracerStep  # noqa: F401  (library loaded)
+    from .tracers import TracerAdvection
+    from .periodic import Periodic
+    nt, n, ny, nx = w.C.shape
+    g = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)                       # noqa: E731
+    rng = np.random.default_rng(4)
+    Fz = np.zeros((n + 1, ny, nx))
+    Fz[1:-1] = rng.normal(0.0, 1.0, (n - 1, ny, nx)) * 1e2 * w.wet
+    adv = TracerAdvection(scheme=w.scheme, time="ssprk3", dt=w.dt)
+    adv.per = Periodic(w.periodic)
+    args = [g(a) for a in (w.C, w.V0, w.V1, w.Qx, w.Qy, Fz, w.ok)]
+    out = adv.advect(*args)
+    torch.cuda.synchronize()
+    ms = _time(lambda: adv.advect(*args), reps=10)
+    return dict(ms=ms, cell_steps_per_s=w.tracer_cells / (ms / 1e3),
+                what="advect (RK3, no limiter, vertical WENO) of the 512 x 512 x 50 T/S stack", finite=bool(
+                    torch.isfinite(out).all()))
 
 
 def _layer_transport_ms(w, dev, rng) -> dict:
