@@ -16,6 +16,8 @@
 //   6. coeff  Zalesak R+ / R- per cell from the 7-point (x, y, k +- 1) bounds of C and c_L (tracers looped per
 //             thread: the stencil geometry is read once).
 //   7. final  face coefficients from R of both neighbours; C_out = safe(q0 - dt div(F_L + C A), V1).
+// The unlimited step (tracers.py:289-291) runs stages 1-2, then a face pass storing the RK3 flux
+// F_H = (F0 + F1)/6 + 2 F2/3 and a cell pass C_out = safe(q0 - dt div F_H, V1).
 // q0 = V0 C, Va, Vb and q1 are recomputed where needed instead of stored.  Planes run k-major (the tracers of one
 // layer follow each other) so a layer's geometry is re-read from L2.  Periodic axes wrap natively in every stencil
 // (the reference pads by TRACER_HALO = 13 cells and crops; with the dependency radius of the step, 10 cells, both
@@ -36,7 +38,6 @@ namespace po {
 
 constexpr int TI = 32;          // tile width (i, contiguous in memory)
 constexpr int TJ = 8;           // tile height (j)
-constexpr int HALO = 3;         // WENO5 stencil radius
 constexpr int NTHREADS = TI * TJ;
 
 // Launch bounds of the coefficient and final passes; POCEAN_*_CTAS (resident CTAs per SM) sets their register
@@ -55,104 +56,6 @@ constexpr int NTHREADS = TI * TJ;
 #else
 #define FINAL_BOUNDS __launch_bounds__(NTHREADS)
 #endif
-constexpr int SW = TI + 2 * HALO;   // shared tile row length
-constexpr int SH = TJ + 2 * HALO;   // shared tile rows
-
-// ---------------------------------------------------------------------------------------------------------------
-// Shared-memory tile of one (t, k) plane of a cell field with a HALO-cell border.  Out-of-domain cells (closed or
-// open edges) get value 0 and validity false, which is the reference's `0 <= i < n and ok[i]` rule; periodic axes
-// wrap.
-struct Tile {
-    double c[SH][SW];
-    uint8_t v[SH][SW];
-    double fx[TJ][TI + 1];      // x-face fluxes, face lf between local cells lf-1 and lf
-    double fy[TJ + 1][TI];      // y-face fluxes
-};
-
-__device__ __forceinline__ void load_tile(Tile& T, const double* __restrict__ cp, const uint8_t* __restrict__ okp,
-                                          const Shape& s, const Flags& fl, int j0, int i0)
-{
-    for (int idx = threadIdx.x; idx < SH * SW; idx += NTHREADS) {
-        const int lj = idx / SW, li = idx - lj * SW;
-        int gj = j0 + lj - HALO, gi = i0 + li - HALO;
-        bool in = true;
-        if (fl.per_x) gi = wrap(gi, s.nx); else in = in && (gi >= 0 && gi < s.nx);
-        if (fl.per_y) gj = wrap(gj, s.ny); else in = in && (gj >= 0 && gj < s.ny);
-        double val = 0.0;
-        uint8_t ok = 0;
-        if (in) {
-            const i64 o = (i64)gj * s.nx + gi;
-            val = cp[o];
-            ok = okp[o];
-        }
-        T.c[lj][li] = val;
-        T.v[lj][li] = ok;
-    }
-}
-
-// x-face flux Q c_face of global face gf (row gj) at tile position (lj, lf): WENO5 on interior faces, the upstream
-// value on open edges, 0 on closed edges (sigma_baroclinic.py:277-297).  `cg`/`eg`: the plane of c / ext.
-typedef double TileC[SW];      // one row of a shared halo tile of values
-typedef uint8_t TileV[SW];     // one row of validity flags
-
-__device__ __forceinline__ double xface_flux(const TileC* tc, const TileV* tv, int lj, int lf, int gj, int gf, int k,
-                                             const Shape& s, const Flags& fl, const double* __restrict__ Qx,
-                                             const double* __restrict__ cg, const double* __restrict__ eg)
-{
-    if (fl.per_x || (gf >= 1 && gf <= s.nx - 1)) {
-        const double q = Qx[s.qx(k, gj, gf == s.nx ? 0 : gf)];
-        if (q == 0.0) return 0.0;
-        return q * upwind_face_value(&tc[lj + HALO][lf], &tv[lj + HALO][lf], 1, q, fl.z);
-    }
-    const double q = Qx[s.qx(k, gj, gf)];
-    const i64 row = (i64)gj * s.nx;
-    if (gf == 0) return fl.open_w ? q * (q > 0.0 ? eg[row] : cg[row]) : 0.0;
-    return fl.open_e ? q * (q < 0.0 ? eg[row + s.nx - 1] : cg[row + s.nx - 1]) : 0.0;
-}
-
-__device__ __forceinline__ double yface_flux(const TileC* tc, const TileV* tv, int lf, int li, int gf, int gi, int k,
-                                             const Shape& s, const Flags& fl, const double* __restrict__ Qy,
-                                             const double* __restrict__ cg, const double* __restrict__ eg)
-{
-    if (fl.per_y || (gf >= 1 && gf <= s.ny - 1)) {
-        const double q = Qy[s.qy(k, gf == s.ny ? 0 : gf, gi)];
-        if (q == 0.0) return 0.0;
-        return q * upwind_face_value(&tc[lf][li + HALO], &tv[lf][li + HALO], SW, q, fl.z);
-    }
-    const double q = Qy[s.qy(k, gf, gi)];
-    if (gf == 0) return fl.open_s ? q * (q > 0.0 ? eg[gi] : cg[gi]) : 0.0;
-    const i64 o = (i64)(s.ny - 1) * s.nx + gi;
-    return fl.open_n ? q * (q < 0.0 ? eg[o] : cg[o]) : 0.0;
-}
-
-// All x- and y-face fluxes of the tile into T.fx / T.fy.  Thread (tx, ty) computes the west face of its cell and
-// the south face; threads 0..TJ+TI-1 also compute the east faces of the last column and the north faces of the
-// last row.  Faces outside the domain are skipped.
-__device__ __forceinline__ void tile_faces(const TileC* tc, const TileV* tv, double (*fx)[TI + 1],
-                                           double (*fy)[TI], const Shape& s, const Flags& fl, int k, int j0, int i0,
-                                           const double* __restrict__ Qx, const double* __restrict__ Qy,
-                                           const double* __restrict__ cg, const double* __restrict__ eg)
-{
-    const int tx = threadIdx.x % TI, ty = threadIdx.x / TI;
-    const int gi = i0 + tx, gj = j0 + ty;
-    if (gj < s.ny && gi <= s.nx) fx[ty][tx] = xface_flux(tc, tv, ty, tx, gj, gi, k, s, fl, Qx, cg, eg);
-    if (gi < s.nx && gj <= s.ny) fy[ty][tx] = yface_flux(tc, tv, ty, tx, gj, gi, k, s, fl, Qy, cg, eg);
-    const int e = threadIdx.x;
-    if (e < TJ) {
-        const int r = j0 + e, f = i0 + TI;
-        if (r < s.ny && f <= s.nx) fx[e][TI] = xface_flux(tc, tv, e, TI, r, f, k, s, fl, Qx, cg, eg);
-    } else if (e < TJ + TI) {
-        const int c = e - TJ, f = j0 + TJ, col = i0 + c;
-        if (col < s.nx && f <= s.ny) fy[TJ][c] = yface_flux(tc, tv, TJ, c, f, col, k, s, fl, Qy, cg, eg);
-    }
-}
-
-__device__ __forceinline__ void tile_faces(Tile& T, const Shape& s, const Flags& fl, int k, int j0, int i0,
-                                           const double* __restrict__ Qx, const double* __restrict__ Qy,
-                                           const double* __restrict__ cg, const double* __restrict__ eg)
-{
-    tile_faces(T.c, T.v, T.fx, T.fy, s, fl, k, j0, i0, Qx, Qy, cg, eg);
-}
 
 // ---------------------------------------------------------------------------------------------------------------
 // Donor-cell flux F_L of x-face gf (sigma_baroclinic.py:486-494; periodic: every face interior, face nx = face 0).
@@ -194,39 +97,6 @@ __device__ __forceinline__ double donor_y(const double* __restrict__ cp, const d
 
 namespace po {
 
-// Unlimited step (tracers.py:289-291, `unlimited=True`): C_out = safe(q0 - dt div F_H, V1) with the RK3 flux
-// F_H = (F0 + F1)/6 + 2 F2/3; S is read, not modified.
-__global__ void __launch_bounds__(NTHREADS) fct_unlimited_kernel(StepArgs a)
-{
-    __shared__ Tile T;
-    const Shape s = a.s;
-    const Flags fl(a.flags);
-    const int p = blockIdx.z, t = p / s.n, k = p - t * s.n;
-    const int i0 = blockIdx.x * TI, j0 = blockIdx.y * TJ;
-    const double* c2p = a.c2 + s.cell(t, k, 0, 0);
-    const double* e2p = a.inflow ? a.inflow + s.cell(t, k, 0, 0) : c2p;
-    load_tile(T, c2p, a.ok + s.geo(k, 0, 0), s, fl, j0, i0);
-    __syncthreads();
-    tile_faces(T, s, fl, k, j0, i0, a.Qx, a.Qy, c2p, e2p);
-    __syncthreads();
-
-    const int tx = threadIdx.x % TI, ty = threadIdx.x / TI;
-    const int gi = i0 + tx, gj = j0 + ty;
-    if (gi >= s.nx || gj >= s.ny) return;
-    const i64 w = s.ux(t, k, gj, gi), so = s.vy(t, k, gj, gi);
-    // S holds F0 and T holds F1: (F0 + F1)/6 formed here
-    const double fw = div6_exact(a.Sx[w] + a.Tx[w]) + div3_exact(2.0 * T.fx[ty][tx]);
-    const double fe = div6_exact(a.Sx[w + 1] + a.Tx[w + 1]) + div3_exact(2.0 * T.fx[ty][tx + 1]);
-    const double fs = div6_exact(a.Sy[so] + a.Ty[so]) + div3_exact(2.0 * T.fy[ty][tx]);
-    const double fn = div6_exact(a.Sy[so + s.nx] + a.Ty[so + s.nx]) + div3_exact(2.0 * T.fy[ty + 1][tx]);
-    if (a.fx_face != nullptr && gi == (a.face_i == s.nx ? s.nx - 1 : a.face_i))
-        a.fx_face[((i64)t * s.n + k) * s.ny + gj] = a.face_i == s.nx ? fe : fw;
-    const double d = fe - fw + fn - fs;
-    const i64 g = s.geo(k, gj, gi), ci = s.cell(t, k, gj, gi);
-    const double v1 = a.V1[g], c0 = a.C[ci];
-    const double q = a.V0[g] * c0 - a.dt * d;
-    a.out[ci] = v1 > 0 ? q / v1 : c0;
-}
 
 // Pass 4: Zalesak R+ / R- (sigma_baroclinic.py:407-432): bounds over the cell, its x / y neighbours and the layers
 // k +- 1 (ok cells), P from the antidiffusive fluxes of the cell's faces, Q from V1 and c_L.
@@ -728,7 +598,13 @@ static int advect_fct_impl(const char* fn, bool mixed, const double* C, const do
     stage_passes(1);
     stage_passes(2);
     if (flags & POCEAN_FCT_UNLIMITED) {
-        fct_unlimited_kernel<<<grid, NTHREADS, 0, st>>>(a);
+        constexpr int R = POCEAN_FACE_ROWS;
+        const dim3 g2(ceil_div(nx, TI), ceil_div(ny, R), nt * nz);
+        if (zv && !mixed) fct_faces_kernel<4, true, false, R><<<g2, TI * R, 0, st>>>(a);
+        else if (!zv && !mixed) fct_faces_kernel<4, false, false, R><<<g2, TI * R, 0, st>>>(a);
+        else if (zv) fct_faces_kernel<4, true, true, R><<<g2, TI * R, 0, st>>>(a);
+        else fct_faces_kernel<4, false, true, R><<<g2, TI * R, 0, st>>>(a);
+        fct_update_kernel<4, R><<<g2, TI * R, 0, st>>>(a);
         return pocean_check_launch(fn);
     }
     stage_passes(3);

@@ -158,8 +158,10 @@ __device__ __forceinline__ void put_face(double* S, double* T, int fo, double F,
         S[fo] = F;
     } else if (STAGE == 2) {
         T[fo] = F;
-    } else {
+    } else if (STAGE == 3) {
         S[fo] = (div6_exact(s0 + t0) + div3_exact(2.0 * F)) - FL;
+    } else {                     // the unlimited step: S <- the RK3 flux F_H = (F0 + F1)/6 + 2 F2/3
+        S[fo] = div6_exact(s0 + t0) + div3_exact(2.0 * F);
     }
 }
 
@@ -187,7 +189,7 @@ __device__ __forceinline__ void faces_body(const StepArgs& a, int t, int k, int 
     const int fxo = j * (s.nx + 1) + i, fyo = j * s.nx + i;
     const bool last_x = i == s.nx - 1, last_y = j == s.ny - 1;
     double sxw = 0.0, txw = 0.0, sys = 0.0, tys = 0.0, sxe = 0.0, txe = 0.0, syn = 0.0, tyn = 0.0;
-    if (STAGE == 3) {
+    if (STAGE >= 3) {
         sxw = P.sx[fxo]; txw = P.tx[fxo];
         sys = P.sy[fyo]; tys = P.ty[fyo];
         if (last_x) { sxe = P.sx[fxo + 1]; txe = P.tx[fxo + 1]; }
@@ -316,7 +318,7 @@ __global__ void FACES3_BOUNDS(TI * TJR) fct_faces3_batched(const BatchDomain* __
 }
 
 // Cell pass of stage STAGE = 1, 2 (sigma_baroclinic.py:452-468 `_fct_stage`); stage 3 has none (its face pass
-// writes c_L).
+// writes c_L); STAGE = 4 is the unlimited step's final update from the RK3 flux.
 template <int STAGE>
 __device__ __forceinline__ void update_body(const StepArgs& a, int t, int k, int i, int j)
 {
@@ -337,6 +339,12 @@ __device__ __forceinline__ void update_body(const StepArgs& a, int t, int k, int
         const double q = 0.75 * q0 + 0.25 * (q1 - a.dt * d);
         const double v = v0 + 0.5 * (v1 - v0);
         a.c2[cc] = v > 0.0 ? q / v : c0;
+    } else if (STAGE == 4) {     // the unlimited step (tracers.py:289-291): C_out = safe(q0 - dt div F_H, V1)
+        const double d = a.Sx[w + 1] - a.Sx[w] + a.Sy[so + s.nx] - a.Sy[so];
+        if (a.fx_face != nullptr && i == (a.face_i == s.nx ? s.nx - 1 : a.face_i))
+            a.fx_face[((i64)t * s.n + k) * s.ny + j] = a.face_i == s.nx ? a.Sx[w + 1] : a.Sx[w];
+        const double q = q0 - a.dt * d;
+        a.out[cc] = v1 > 0 ? q / v1 : c0;
     }
 }
 
