@@ -41,10 +41,11 @@ constexpr int TJ = 8;           // tile height (j)
 constexpr int NTHREADS = TI * TJ;
 
 // Launch bounds of the coefficient and final passes; POCEAN_*_CTAS (resident CTAs per SM) sets their register
-// budget when defined, else ptxas chooses.  The final pass is fitted to 3 CTAs (24 warps) per SM: 3 % faster than
-// ptxas's choice (112 registers, 2 CTAs) and than 2 or 4 CTAs, measured at 512 x 512 x 50.
+// budget when defined, else ptxas chooses.  The final pass is fitted to 4 CTAs (32 warps, 64 registers) per SM:
+// 1.5 % faster for the step than 3 CTAs, measured at 512 x 512 x 50; the coefficient pass keeps ptxas's choice
+// (5 CTAs, which spills, was slower).
 #ifndef POCEAN_FINAL_CTAS
-#define POCEAN_FINAL_CTAS 3
+#define POCEAN_FINAL_CTAS 4
 #endif
 #ifdef POCEAN_COEFF_CTAS
 #define COEFF_BOUNDS __launch_bounds__(NTHREADS, POCEAN_COEFF_CTAS)
@@ -111,7 +112,9 @@ __device__ __forceinline__ void coeff_body(const StepArgs& a, int i, int j, int 
     const int dk[7] = {0, 0, 0, 0, 0, -1, 1};
     const int dj[7] = {0, 0, 0, -1, 1, 0, 0};
     const int di[7] = {0, -1, 1, 0, 0, 0, 0};
-    const bool self_ok = a.ok[s.geo(k, j, i)];
+    // 32-bit offsets within a field (every field holds fewer than 2^31 entries)
+    const int pl = s.ny * s.nx, gc = k * pl + j * s.nx + i;
+    const bool self_ok = a.ok[gc];
     int nb[7];
 #pragma unroll
     for (int m = 0; m < 7; ++m) {
@@ -119,23 +122,25 @@ __device__ __forceinline__ void coeff_body(const StepArgs& a, int i, int j, int 
         bool in = kk >= 0 && kk < s.n;
         if (fl.per_y) jj = wrap(jj, s.ny); else in = in && jj >= 0 && jj < s.ny;
         if (fl.per_x) ii = wrap(ii, s.nx); else in = in && ii >= 0 && ii < s.nx;
-        nb[m] = (in && a.ok[s.geo(in ? kk : 0, in ? jj : 0, in ? ii : 0)]) ? (int)(((i64)kk * s.ny + jj) * s.nx + ii) : -1;
+        const int o = in ? kk * pl + jj * s.nx + ii : 0;
+        nb[m] = (in && a.ok[o]) ? o : -1;
     }
-    const double v1 = a.V1[s.geo(k, j, i)];
-    const i64 tstride = (i64)s.n * s.plane();
+    const double v1 = a.V1[gc];
+    const int tstride = s.n * pl;
     for (int t = 0; t < s.nt; ++t) {
-        const i64 ci = s.cell(t, k, j, i);
+        const i64 ci = plane_at(t, tstride) + gc;
         double rin = 0.0, rout = 0.0;
         if (self_ok) {
             // every load of the tracer first (independent, in flight together), then the bounds in stencil order
             double vc[7], vl[7];
 #pragma unroll
             for (int m = 0; m < 7; ++m) {
-                const i64 o = (i64)t * tstride + (nb[m] >= 0 ? nb[m] : nb[0]);
+                const i64 o = plane_at(t, tstride) + (nb[m] >= 0 ? nb[m] : nb[0]);
                 vc[m] = __ldg(a.C + o);
                 vl[m] = cL[o];
             }
-            const i64 w = s.ux(t, k, j, i), so = s.vy(t, k, j, i);
+            const int p = t * s.n + k;
+            const i64 w = plane_at(p, s.ny * (s.nx + 1)) + (j * (s.nx + 1) + i), so = plane_at(p, (s.ny + 1) * s.nx) + (j * s.nx + i);
             const double axw = a.Sx[w], axe = a.Sx[w + 1], ays = a.Sy[so], ayn = a.Sy[so + s.nx];
             double cmax = -INFINITY, cmin = INFINITY;
 #pragma unroll
@@ -210,17 +215,20 @@ __device__ __forceinline__ void final_body(const StepArgs& a, int i, int j, int 
     const int js = fl.per_y ? wrap(j - 1, s.ny) : j - 1, jn = fl.per_y ? wrap(j + 1, s.ny) : (j + 1 < s.ny ? j + 1 : -1);
     const bool in_w = fl.per_x || i >= 1, in_e = fl.per_x || i + 1 <= s.nx - 1;
     const bool in_s = fl.per_y || j >= 1, in_n = fl.per_y || j + 1 <= s.ny - 1;
-    const i64 g = s.geo(k, j, i);
+    // 32-bit offsets within a field (every field holds fewer than 2^31 entries)
+    const int pl = s.ny * s.nx, xpl = s.ny * (s.nx + 1), ypl = (s.ny + 1) * s.nx;
+    const int g = k * pl + j * s.nx + i, gx = k * xpl + j * (s.nx + 1) + i, gy = k * ypl + j * s.nx + i;
     const double v0 = __ldg(a.V0 + g), v1 = __ldg(a.V1 + g);
-    const double qw = __ldg(a.Qx + s.qx(k, j, i));
-    const double qe = __ldg(a.Qx + s.qx(k, j, (fl.per_x && i + 1 == s.nx) ? 0 : i + 1));
-    const double qs = __ldg(a.Qy + s.qy(k, j, i));
-    const double qn = __ldg(a.Qy + s.qy(k, (fl.per_y && j + 1 == s.ny) ? 0 : j + 1, i));
+    const double qw = __ldg(a.Qx + gx);
+    const double qe = __ldg(a.Qx + ((fl.per_x && i + 1 == s.nx) ? gx + 1 - s.nx : gx + 1));
+    const double qs = __ldg(a.Qy + gy);
+    const double qn = __ldg(a.Qy + ((fl.per_y && j + 1 == s.ny) ? gy - j * s.nx : gy + s.nx));
     const i64 row = (i64)j * s.nx;
     const i64 o_c = row + i, o_w = row + (iw >= 0 ? iw : i), o_e = row + (ie >= 0 ? ie : i);
     const i64 o_s = (i64)(js >= 0 ? js : j) * s.nx + i, o_n = (i64)(jn >= 0 ? jn : j) * s.nx + i;
     for (int t = 0; t < s.nt; ++t) {
-        const i64 pc = s.cell(t, k, 0, 0);
+        const int p = t * s.n + k;
+        const i64 pc = plane_at(p, pl);
         const double* C = a.C + pc;
         const double* Rp = a.c1 + pc;
         const double* Rm = a.c2 + pc;
@@ -228,7 +236,7 @@ __device__ __forceinline__ void final_body(const StepArgs& a, int i, int j, int 
                      cn = __ldg(C + o_n);
         const double rp0 = Rp[o_c], rpw = Rp[o_w], rpe = Rp[o_e], rps = Rp[o_s], rpn = Rp[o_n];
         const double rm0 = Rm[o_c], rmw = Rm[o_w], rme = Rm[o_e], rms = Rm[o_s], rmn = Rm[o_n];
-        const i64 w = s.ux(t, k, j, i), so = s.vy(t, k, j, i);
+        const i64 w = plane_at(p, xpl) + (gx - k * xpl), so = plane_at(p, ypl) + (gy - k * ypl);
         const double aw = a.Sx[w], ae = a.Sx[w + 1], as = a.Sy[so], an = a.Sy[so + s.nx];
         double ext_c = c0;
         if (a.inflow && ((!in_w && fl.open_w) || (!in_e && fl.open_e) || (!in_s && fl.open_s) ||
@@ -362,16 +370,18 @@ __device__ __forceinline__ double zface_flux(const StepArgs& a, const Shape& s, 
                                              int t, int kf, int j, int i)
 {
     if (a.Fz == nullptr || kf < 1 || kf > s.n - 1) return 0.0;
-    const double q = a.Fz[s.geo(kf, j, i)];
+    const int pl = s.ny * s.nx, ij = j * s.nx + i;            // 32-bit offsets within a field
+    const double q = a.Fz[kf * pl + ij];
     if (q == 0.0) return 0.0;
+    const double* ct = cin + plane_at(t, s.n * pl);
     double w[6];
     uint8_t v[6];
 #pragma unroll
     for (int m = 0; m < 6; ++m) {
         const int kk = kf - 3 + m;
         const bool in = kk >= 0 && kk < s.n;
-        w[m] = in ? cin[s.cell(t, kk, j, i)] : 0.0;
-        v[m] = in ? a.ok[s.geo(kk, j, i)] : 0;
+        w[m] = in ? ct[kk * pl + ij] : 0.0;
+        v[m] = in ? a.ok[kk * pl + ij] : 0;
     }
     return q * upwind_face_value(w, v, 1, q, fl.z);
 }
@@ -394,18 +404,19 @@ __device__ __forceinline__ void rk3_faces_body(const StepArgs& a, int t, int k, 
     const Shape s = a.s;
     const Flags fl(a.flags);
     if (i >= s.nx || j >= s.ny) return;
-    const i64 pc = s.cell(t, k, 0, 0);
+    const int pl = s.ny * s.nx, xpl = s.ny * (s.nx + 1), ypl = (s.ny + 1) * s.nx, p = t * s.n + k;
+    const i64 pc = plane_at(p, pl);
     const double* cin = rk3_stage_field<STAGE>(a);
     FacePlane P;
     P.c = cin + pc;
     P.e = a.inflow ? a.inflow + pc : P.c;
     P.c0 = P.c;
     P.e0 = P.e;
-    P.ok = a.ok + s.geo(k, 0, 0);
-    P.qx = a.Qx + s.qx(k, 0, 0);
-    P.qy = a.Qy + s.qy(k, 0, 0);
-    double* sx = a.Sx + s.ux(t, k, 0, 0);
-    double* sy = a.Sy + s.vy(t, k, 0, 0);
+    P.ok = a.ok + plane_at(k, pl);
+    P.qx = a.Qx + plane_at(k, xpl);
+    P.qy = a.Qy + plane_at(k, ypl);
+    double* sx = a.Sx + plane_at(p, xpl);
+    double* sy = a.Sy + plane_at(p, ypl);
     const int fxo = j * (s.nx + 1) + i, fyo = j * s.nx + i;
     double F, unused;
     x_face<ZV, false, false>(P, s, fl, j, i, F, unused);
@@ -426,18 +437,22 @@ __device__ __forceinline__ void rk3_faces_body(const StepArgs& a, int t, int k, 
 template <int STAGE, bool ZV, int TJR>
 __global__ void __launch_bounds__(TI * TJR, POCEAN_FACES12_MINB * 256 / (TI * TJR)) rk3_faces_kernel(StepArgs a)
 {
-    const int p = blockIdx.z, k = p / a.s.nt, t = p - k * a.s.nt;
+    int k, t;
+    split_plane(blockIdx.z, a.s.nt, a.tdiv, k, t);
     rk3_faces_body<STAGE, ZV>(a, t, k, blockIdx.x * TI + threadIdx.x % TI, blockIdx.y * TJR + threadIdx.x / TI);
 }
 
 template <int STAGE, int TJR>
 __global__ void __launch_bounds__(TI * TJR) rk3_update_kernel(StepArgs a)
 {
-    const int p = blockIdx.z, k = p / a.s.nt, t = p - k * a.s.nt;
+    int k, t;
+    split_plane(blockIdx.z, a.s.nt, a.tdiv, k, t);
     const int gi = blockIdx.x * TI + threadIdx.x % TI, gj = blockIdx.y * TJR + threadIdx.x / TI;
     const Shape s = a.s;
     if (gi >= s.nx || gj >= s.ny) return;
-    const i64 w = s.ux(t, k, gj, gi), so = s.vy(t, k, gj, gi), ci = s.cell(t, k, gj, gi);
+    const int pl = s.ny * s.nx, p = t * s.n + k, ij = gj * s.nx + gi;
+    const i64 w = plane_at(p, s.ny * (s.nx + 1)) + (gj * (s.nx + 1) + gi), so = plane_at(p, (s.ny + 1) * s.nx) + ij;
+    const i64 ci = plane_at(p, pl) + ij;
     if (a.fx_face != nullptr && gi == (a.face_i == s.nx ? s.nx - 1 : a.face_i)) {
         const double F = a.Sx[a.face_i == s.nx ? w + 1 : w];
         const i64 r = ((i64)t * s.n + k) * s.ny + gj;
@@ -446,9 +461,9 @@ __global__ void __launch_bounds__(TI * TJR) rk3_update_kernel(StepArgs a)
         else a.fx_face[r] = div6_exact(a.tef0[r] + a.tef1[r]) + div3_exact(2.0 * F);
     }
     const double fzb = a.Tx[ci];
-    const double fzt = k + 1 < s.n ? a.Tx[ci + s.plane()] : 0.0;      // the surface interface carries no flux
+    const double fzt = k + 1 < s.n ? a.Tx[ci + pl] : 0.0;      // the surface interface carries no flux
     const double r = -(a.Sx[w + 1] - a.Sx[w] + a.Sy[so + s.nx] - a.Sy[so] + fzt - fzb);
-    const i64 g = s.geo(k, gj, gi);
+    const int g = k * pl + ij;
     const double v0 = a.V0[g], v1 = a.V1[g], c0 = a.C[ci];
     const double q0 = v0 * c0, dv = v1 - v0;
     double q, v;
@@ -581,6 +596,7 @@ static int advect_fct_impl(const char* fn, bool mixed, const double* C, const do
     cudaStream_t st = (cudaStream_t)stream;
     StepArgs a{};
     a.s = Shape{nt, nz, ny, nx};
+    a.tdiv = plane_magic(nt);
     a.flags = flags;
     a.dt = dt;
     a.C = C; a.V0 = V0; a.V1 = V1; a.Qx = Qx; a.Qy = Qy; a.Fz = nullptr; a.ok = ok; a.inflow = inflow;
@@ -701,6 +717,7 @@ extern "C" int pocean_advect_rk3_f64(const double* C, const double* V0, const do
     cudaStream_t st = (cudaStream_t)stream;
     StepArgs a{};
     a.s = Shape{nt, nz, ny, nx};
+    a.tdiv = plane_magic(nt);
     a.flags = flags;
     a.dt = dt;
     a.C = C; a.V0 = V0; a.V1 = V1; a.Qx = Qx; a.Qy = Qy; a.Fz = Fz; a.ok = ok; a.inflow = inflow;
@@ -760,6 +777,7 @@ extern "C" int pocean_advect_fct_layers(int mixed, const double* C, const double
     cudaStream_t st = (cudaStream_t)stream;
     StepArgs a{};
     a.s = Shape{nt, nz, ny, nx};
+    a.tdiv = plane_magic(nt);
     a.flags = flags;
     a.dt = dt;
     a.C = C; a.V0 = V0; a.V1 = V1; a.Qx = Qx; a.Qy = Qy; a.Fz = nullptr; a.ok = ok; a.inflow = inflow;

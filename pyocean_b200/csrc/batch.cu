@@ -71,6 +71,7 @@ extern "C" int pocean_batch_create(const pocean_domain* domains, int ndom, int t
             BatchDomain& B = host[(size_t)parity * ndom + d];
             std::memset(&B, 0, sizeof(B));
             B.a.s = Shape{D.nt, D.nz, D.ny, D.nx};
+            B.a.tdiv = plane_magic(D.nt);
             B.a.flags = D.flags;
             B.a.dt = D.dt;
             B.a.C = parity == 0 ? D.C : D.C_next;

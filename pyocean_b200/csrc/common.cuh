@@ -7,6 +7,7 @@
 #include <cuda_runtime.h>
 
 #include "../../include/pocean_b200.h"
+#include "planediv.cuh"
 
 typedef long long i64;
 
@@ -31,6 +32,13 @@ struct Shape {
     __host__ __device__ i64 qx(int k, int j, int f) const { return ((i64)k * ny + j) * (nx + 1) + f; }
     __host__ __device__ i64 qy(int k, int f, int i) const { return ((i64)k * (ny + 1) + f) * nx + i; }
 };
+
+// Offset of plane p of a stack whose planes hold `elems` elements, as one 32 x 32 -> 64-bit product (p >= 0 and
+// elems < 2^31: the entry points bound every field by 2^31 entries).
+__host__ __device__ __forceinline__ i64 plane_at(int p, int elems)
+{
+    return (i64)((unsigned long long)(unsigned)p * (unsigned)elems);
+}
 
 // Periodic wrap of a cell index (any integer) onto 0..n-1.
 __host__ __device__ __forceinline__ int wrap(int i, int n) {

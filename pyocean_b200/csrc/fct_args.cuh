@@ -41,6 +41,7 @@ struct StepArgs {
     double* out;
     int face_i;
     int k0;                             // first layer of a layer-range launch of the single-domain passes (else 0)
+    unsigned tdiv;                      // plane_magic(s.nt): plane index -> layer without an integer division
     double* fx_face;
 };
 
@@ -55,6 +56,16 @@ struct BatchDomain {
     double* rout;
     int remap_scheme;
 };
+
+// Layer k and tracer t of plane p = k nt + t (planes run k-major).
+#ifndef POCEAN_PLANE_MAGIC
+#define POCEAN_PLANE_MAGIC 1
+#endif
+__device__ __forceinline__ void split_plane(int p, int nt, unsigned tdiv, int& k, int& t)
+{
+    k = POCEAN_PLANE_MAGIC ? plane_div(p, tdiv) : p / nt;
+    t = p - k * nt;
+}
 
 // CTA offsets of every batched pass: domain d owns CTAs off[d] .. off[d+1]-1 of the launch (ndom + 1 entries each).
 enum BatchPass { BP_PTILE = 0, BP_TILE = 1, BP_RPAIR = 2, BP_RREM = 3, BP_RALL = 4, BP_RGEN = 5, BP_COUNT = 6 };

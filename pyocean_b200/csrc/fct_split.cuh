@@ -173,19 +173,20 @@ __device__ __forceinline__ void faces_body(const StepArgs& a, int t, int k, int 
     const Shape s = a.s;
     const Flags fl(a.flags);
     if (i >= s.nx || j >= s.ny) return;
-    const i64 pc = s.cell(t, k, 0, 0);
+    const int pl = s.ny * s.nx, xpl = s.ny * (s.nx + 1), ypl = (s.ny + 1) * s.nx, p = t * s.n + k;
+    const i64 pc = plane_at(p, pl), pu = plane_at(p, xpl), pv = plane_at(p, ypl);
     FacePlane P;
     P.c = stage_field<STAGE>(a) + pc;
     P.e = a.inflow ? a.inflow + pc : P.c;
     P.c0 = a.C + pc;
     P.e0 = a.inflow ? a.inflow + pc : P.c0;
-    P.ok = a.ok + s.geo(k, 0, 0);
-    P.qx = a.Qx + s.qx(k, 0, 0);
-    P.qy = a.Qy + s.qy(k, 0, 0);
-    P.sx = a.Sx + s.ux(t, k, 0, 0);
-    P.sy = a.Sy + s.vy(t, k, 0, 0);
-    P.tx = a.Tx + s.ux(t, k, 0, 0);
-    P.ty = a.Ty + s.vy(t, k, 0, 0);
+    P.ok = a.ok + plane_at(k, pl);
+    P.qx = a.Qx + plane_at(k, xpl);
+    P.qy = a.Qy + plane_at(k, ypl);
+    P.sx = a.Sx + pu;
+    P.sy = a.Sy + pv;
+    P.tx = a.Tx + pu;
+    P.ty = a.Ty + pv;
     const int fxo = j * (s.nx + 1) + i, fyo = j * s.nx + i;
     const bool last_x = i == s.nx - 1, last_y = j == s.ny - 1;
     double sxw = 0.0, txw = 0.0, sys = 0.0, tys = 0.0, sxe = 0.0, txe = 0.0, syn = 0.0, tyn = 0.0;
@@ -225,11 +226,11 @@ __device__ __forceinline__ void faces_body(const StepArgs& a, int t, int k, int 
             ln = q * (q >= 0 ? c0 : __ldg(P.c0 + fyo + s.nx));
         }
         const double dl = le - lw + ln - ls;
-        const i64 g = s.geo(k, j, i);
+        const i64 g = plane_at(k, pl) + fyo;
         const double v0 = __ldg(a.V0 + g), v1 = __ldg(a.V1 + g);
         const double q0 = v0 * c0;
         const double q = 0.0 * q0 + 1.0 * (q0 - a.dt * dl);
-        a.q1[pc + j * s.nx + i] = v1 > 0 ? q / v1 : c0;
+        a.q1[pc + fyo] = v1 > 0 ? q / v1 : c0;
     }
 }
 
@@ -256,7 +257,8 @@ __device__ __forceinline__ void faces_body(const StepArgs& a, int t, int k, int 
 template <int STAGE, bool ZV, bool MIX, int TJR>
 __device__ __forceinline__ void faces_plane(const StepArgs& a)
 {
-    const int p = a.k0 * a.s.nt + blockIdx.z, k = p / a.s.nt, t = p - k * a.s.nt;
+    int k, t;
+    split_plane(a.k0 * a.s.nt + blockIdx.z, a.s.nt, a.tdiv, k, t);
     faces_body<STAGE, ZV, MIX>(a, t, k, blockIdx.x * TI + threadIdx.x % TI, blockIdx.y * TJR + threadIdx.x / TI);
 }
 
@@ -284,8 +286,7 @@ __device__ __forceinline__ int batched_plane_tile(const BatchDomain* __restrict_
     int local = blockIdx.x - __ldg(off + d);
     const int p = local / (tx * ty);
     local -= p * tx * ty;
-    k = p / s.nt;
-    t = p - k * s.nt;
+    split_plane(p, s.nt, doms[d].a.tdiv, k, t);
     const int by = local / tx, bx = local - by * tx;
     i = bx * TI + threadIdx.x % TI;
     j = by * TJR + threadIdx.x / TI;
@@ -324,7 +325,9 @@ __device__ __forceinline__ void update_body(const StepArgs& a, int t, int k, int
 {
     const Shape s = a.s;
     if (i >= s.nx || j >= s.ny) return;
-    const i64 w = s.ux(t, k, j, i), so = s.vy(t, k, j, i), g = s.geo(k, j, i), cc = s.cell(t, k, j, i);
+    const int pl = s.ny * s.nx, p = t * s.n + k, ij = j * s.nx + i;
+    const i64 w = plane_at(p, s.ny * (s.nx + 1)) + (j * (s.nx + 1) + i), so = plane_at(p, (s.ny + 1) * s.nx) + ij;
+    const i64 g = plane_at(k, pl) + ij, cc = plane_at(p, pl) + ij;
     const double v0 = __ldg(a.V0 + g), v1 = __ldg(a.V1 + g), c0 = __ldg(a.C + cc);
     const double q0 = v0 * c0;
     if (STAGE == 1) {
@@ -351,7 +354,8 @@ __device__ __forceinline__ void update_body(const StepArgs& a, int t, int k, int
 template <int STAGE, int TJR>
 __global__ void __launch_bounds__(TI * TJR) fct_update_kernel(StepArgs a)
 {
-    const int p = a.k0 * a.s.nt + blockIdx.z, k = p / a.s.nt, t = p - k * a.s.nt;
+    int k, t;
+    split_plane(a.k0 * a.s.nt + blockIdx.z, a.s.nt, a.tdiv, k, t);
     update_body<STAGE>(a, t, k, blockIdx.x * TI + threadIdx.x % TI, blockIdx.y * TJR + threadIdx.x / TI);
 }
 

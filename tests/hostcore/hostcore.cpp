@@ -1,11 +1,12 @@
-// Host build of device arithmetic of libpocean_b200 (test harness only): the exact constant divisions and the
-// one-pass column remap, compiled with g++ -ffp-contract=off so the tests can check them on the CPU against IEEE
+// Host build of device arithmetic of libpocean_b200 (test harness only): the exact constant divisions, the
+// plane-index division and the one-pass column remap, compiled with g++ -ffp-contract=off so the tests can check them on the CPU against IEEE
 // division and against the oracle.  Never linked into the product.
 #include <cmath>
 #include <cstdint>
 #include <cstring>
 
 #include "../../pyocean_b200/csrc/exactdiv.cuh"
+#include "../../pyocean_b200/csrc/planediv.cuh"
 #include "../../pyocean_b200/csrc/remap_core.cuh"
 
 namespace {
@@ -47,6 +48,19 @@ struct HostIO {
 }  // namespace
 
 extern "C" {
+
+// Mismatches of plane_div(p, plane_magic(nt)) against p / nt over every plane index 0 <= p < 65536, for the
+// divisors nts[0..n).
+long long check_plane_div(const int* nts, long long n)
+{
+    long long bad = 0;
+    for (long long q = 0; q < n; ++q) {
+        const int nt = nts[q];
+        const unsigned m = po::plane_magic(nt);
+        for (int p = 0; p < 65536; ++p) bad += po::plane_div(p, m) != p / nt;
+    }
+    return bad;
+}
 
 // Number of arguments x among n random bit patterns (every exponent) and n random values of ordinary magnitude
 // for which div3_exact / div6_exact differ from IEEE division; mismatch examples go to bad[0..1].

@@ -4,6 +4,7 @@ the host (g++ -ffp-contract=off, the IEEE-754 operations the GPU executes) —
 
 * the correctly rounded constant divisions (div3_exact / div6_exact) against IEEE division, on random bit
   patterns of every exponent, on ordinary magnitudes, and on the edge values of their guard;
+* the plane-index division by the tracer count (plane_div) against integer division, for every plane index;
 * the one-pass column remap (remap_column_stream) against the oracle's restatement of remap_column, bit for bit,
   on thousands of seeded columns with vanished source and target layers, both schemes' order reductions, totals
   that differ by round-off, n0 != n1, and one or two fields per sweep.
@@ -34,6 +35,8 @@ def hostcore(tmp_path_factory):
     L.check_exactdiv.argtypes = [ctypes.c_longlong, ctypes.c_ulonglong, D]
     L.check_exactdiv_list.restype = ctypes.c_longlong
     L.check_exactdiv_list.argtypes = [D, ctypes.c_longlong]
+    L.check_plane_div.restype = ctypes.c_longlong
+    L.check_plane_div.argtypes = [ctypes.POINTER(ctypes.c_int), ctypes.c_longlong]
     L.remap_stream_column.restype = ctypes.c_int
     L.remap_stream_column.argtypes = [D, D, ctypes.c_int, D, ctypes.c_int, ctypes.c_int, ctypes.c_int, D]
     L.remap_general_column.restype = ctypes.c_int
@@ -43,6 +46,13 @@ def hostcore(tmp_path_factory):
 
 def _p(a):
     return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def test_plane_division_equals_integer_division(hostcore):
+    # every divisor up to 2048, then a spread up to the largest tracer count the entry points accept (65535)
+    nts = list(range(1, 2049)) + list(range(2049, 65536, 97)) + [2 ** e + d for e in range(11, 16) for d in (-1, 0, 1)]
+    nts = np.array(sorted(set(n for n in nts if 1 <= n <= 65535)), dtype=np.int32)
+    assert hostcore.check_plane_div(nts.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), nts.size) == 0
 
 
 def test_exact_constant_division_equals_ieee_division(hostcore):
