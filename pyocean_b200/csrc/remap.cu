@@ -36,22 +36,36 @@ namespace po {
 namespace remap {
 
 // One column c of NF fields m0 .. m0+NF-1: f_src (nfields, n0, plane) -> out (nfields, n1, plane).
-template <int NF>
+template <int NF, typename IX>
 __device__ __forceinline__ void remap_stream_body(const double* __restrict__ h_src, const double* __restrict__ f_src,
                                                   const double* __restrict__ h_tgt, const uint8_t* __restrict__ wet,
                                                   int n0, int n1, i64 plane, int m0, int scheme,
                                                   double* __restrict__ out, i64 c)
 {
-    ColumnIO<NF> io;
-    io.h = h_src + c;
-    io.t = h_tgt + c;
-    io.plane = plane;
+    if (sizeof(IX) == 4) {
+        ColumnIO32<NF> io;
+        io.h = h_src;
+        io.t = h_tgt;
+        io.c = (int)c;
+        io.plane = (int)plane;
 #pragma unroll
-    for (int m = 0; m < NF; ++m) {
-        io.u[m] = f_src + (i64)(m0 + m) * n0 * plane + c;
-        io.o[m] = out + (i64)(m0 + m) * n1 * plane + c;
+        for (int m = 0; m < NF; ++m) {
+            io.u[m] = f_src + (i64)(m0 + m) * n0 * plane;
+            io.o[m] = out + (i64)(m0 + m) * n1 * plane;
+        }
+        remap_column_io<NF>(io, wet[c] != 0, n0, n1, scheme);
+    } else {
+        ColumnIO<NF> io;
+        io.h = h_src + c;
+        io.t = h_tgt + c;
+        io.plane = plane;
+#pragma unroll
+        for (int m = 0; m < NF; ++m) {
+            io.u[m] = f_src + (i64)(m0 + m) * n0 * plane + c;
+            io.o[m] = out + (i64)(m0 + m) * n1 * plane + c;
+        }
+        remap_column_io<NF>(io, wet[c] != 0, n0, n1, scheme);
     }
-    remap_column_io<NF>(io, wet[c] != 0, n0, n1, scheme);
 }
 
 template <int NMAX>
@@ -70,7 +84,7 @@ __device__ __forceinline__ void remap_general_body(const double* __restrict__ h_
     rc::remap_column_general<NMAX>(io, 0, n0, n1, scheme);
 }
 
-template <int NF>
+template <int NF, typename IX>
 __global__ void REMAP_BOUNDS remap_stream_kernel(const double* __restrict__ h_src,
                                                            const double* __restrict__ f_src,
                                                            const double* __restrict__ h_tgt,
@@ -79,7 +93,7 @@ __global__ void REMAP_BOUNDS remap_stream_kernel(const double* __restrict__ h_sr
 {
     const i64 c = (i64)blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= plane) return;
-    remap_stream_body<NF>(h_src, f_src, h_tgt, wet, n0, n1, plane, field0 + (int)blockIdx.y * NF, scheme, out, c);
+    remap_stream_body<NF, IX>(h_src, f_src, h_tgt, wet, n0, n1, plane, field0 + (int)blockIdx.y * NF, scheme, out, c);
 }
 
 template <int NMAX>
@@ -109,7 +123,8 @@ __global__ void REMAP_BOUNDS remap_stream_batched(const BatchDomain* __restrict_
     const i64 c = (i64)(local - g * cblocks) * 128 + threadIdx.x;
     if (c >= plane) return;
     const int m0 = NF == 2 ? 2 * g : (odd_only ? s.nt - 1 : g);
-    remap_stream_body<NF>(D.h_src, D.a.out, D.h_tgt, D.wet, s.n, s.n, plane, m0, D.remap_scheme, D.rout, c);
+    // the batch bounds every field by 2^31 entries
+    remap_stream_body<NF, int>(D.h_src, D.a.out, D.h_tgt, D.wet, s.n, s.n, plane, m0, D.remap_scheme, D.rout, c);
 }
 
 template <int NMAX>
@@ -184,12 +199,24 @@ extern "C" int pocean_remap_columns_f64(const double* h_src, const double* f_src
     const i64 plane = (i64)ny * nx;
     const unsigned gx = (unsigned)((plane + 127) / 128);
     const int pairs = nfields / 2;
-    if (pairs > 0)
-        remap::remap_stream_kernel<2><<<dim3(gx, pairs), 128, 0, st>>>(h_src, f_src, h_tgt, wet, n0, n1, plane, 0,
-                                                                       scheme, out);
-    if (nfields & 1)
-        remap::remap_stream_kernel<1><<<dim3(gx, 1), 128, 0, st>>>(h_src, f_src, h_tgt, wet, n0, n1, plane,
-                                                                   nfields - 1, scheme, out);
+    // 32-bit offsets within a field when every field (n0 or n1 layers of the plane) holds fewer than 2^31 entries
+    const bool small = (i64)(n0 > n1 ? n0 : n1) * plane < (1ll << 31);
+    if (pairs > 0) {
+        if (small)
+            remap::remap_stream_kernel<2, int><<<dim3(gx, pairs), 128, 0, st>>>(h_src, f_src, h_tgt, wet, n0, n1,
+                                                                                plane, 0, scheme, out);
+        else
+            remap::remap_stream_kernel<2, i64><<<dim3(gx, pairs), 128, 0, st>>>(h_src, f_src, h_tgt, wet, n0, n1,
+                                                                                plane, 0, scheme, out);
+    }
+    if (nfields & 1) {
+        if (small)
+            remap::remap_stream_kernel<1, int><<<dim3(gx, 1), 128, 0, st>>>(h_src, f_src, h_tgt, wet, n0, n1, plane,
+                                                                            nfields - 1, scheme, out);
+        else
+            remap::remap_stream_kernel<1, i64><<<dim3(gx, 1), 128, 0, st>>>(h_src, f_src, h_tgt, wet, n0, n1, plane,
+                                                                            nfields - 1, scheme, out);
+    }
     remap_general_launch(h_src, f_src, h_tgt, n0, n1, plane, nfields, scheme, out, st);
     return pocean_check_launch(fn);
 }

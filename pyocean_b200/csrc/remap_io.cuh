@@ -27,6 +27,21 @@ struct ColumnIO {
     __device__ __forceinline__ void put(int m, int k, double v) { o[m][k * plane] = v; }
 };
 
+// The same for fields of fewer than 2^31 entries: the arrays' bases are the same for every thread of a block (kept
+// in uniform registers), the column and layer enter as one 32-bit offset per access.
+template <int NF>
+struct ColumnIO32 {
+    const double* __restrict__ h;
+    const double* __restrict__ t;
+    const double* __restrict__ u[NF];
+    double* __restrict__ o[NF];
+    int c, plane;
+    __device__ __forceinline__ double hs(int k) const { return __ldg(h + (c + k * plane)); }
+    __device__ __forceinline__ double ht(int k) const { return __ldg(t + (c + k * plane)); }
+    __device__ __forceinline__ double f(int m, int k) const { return __ldg(u[m] + (c + k * plane)); }
+    __device__ __forceinline__ void put(int m, int k, double v) { o[m][c + k * plane] = v; }
+};
+
 // remap.py:400-415 for one column and NF fields: a column that is not wet is copied (n0 == n1) or NaN; a column
 // with a negative or NaN target thickness gets the sentinel (the general algorithm finishes it in a later launch);
 // otherwise the one-pass sweep, or the no-active-source rule.
