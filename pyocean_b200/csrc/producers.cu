@@ -97,17 +97,18 @@ __global__ void __launch_bounds__(128) transport_velocity_kernel(const double* _
     Qb[c] = __ldg(L + c) * __ldg(D + c) * s;
 }
 
-// The masked thickness the PPM kernels read: where(active, nan_to_num(h), 0) (ale.py:755).
+// The masked thickness the PPM kernels read: where(active, nan_to_num(h), 0) (ale.py:755).  Offsets are 32-bit:
+// the PPM entry points bound every field by 2^31 entries.
 struct Thick {
     const double* __restrict__ h;
     const uint8_t* __restrict__ act;
-    i64 pc;
+    int pc;
     int nx;
     __device__ __forceinline__ double at(int k, int j, int i) const
     {
-        return __ldg(act + (i64)j * nx + i) ? nan_to_num(__ldg(h + k * pc + (i64)j * nx + i)) : 0.0;
+        return __ldg(act + (j * nx + i)) ? nan_to_num(__ldg(h + (k * pc + j * nx + i))) : 0.0;
     }
-    __device__ __forceinline__ double m(int j, int i) const { return __ldg(act + (i64)j * nx + i) ? 1.0 : 0.0; }
+    __device__ __forceinline__ double m(int j, int i) const { return __ldg(act + (j * nx + i)) ? 1.0 : 0.0; }
 };
 
 // The limited slope of cell i (first loop of _ppm_edges_kernel).
@@ -149,7 +150,7 @@ __global__ void __launch_bounds__(128) ppm_edges_kernel(Thick T, int n, int ny, 
     const double curv = 3.0 * ((hw + he) - 2.0 * hc);
     const double dh = he - hw;
     const bool inside = curv > 0.0 && fabs(dh) < curv;
-    const i64 o = (i64)k * T.pc + (i64)j * nx + i;
+    const int o = k * T.pc + j * nx + i;
     if (inside && hc <= h_min) {
         h_w[o] = hc;
         h_e[o] = hc;
@@ -192,7 +193,7 @@ struct PPMArgs {
 struct FaceCells {
     double dxw, dxe;
     bool aw, ae;
-    i64 cw, ce;          // cell offsets (j, iw), (j, ie) in a plane
+    int cw, ce;          // cell offsets (j, iw), (j, ie) in a plane
 };
 
 __device__ __forceinline__ FaceCells face_cells(const PPMArgs& a, int j, int f)
@@ -200,8 +201,8 @@ __device__ __forceinline__ FaceCells face_cells(const PPMArgs& a, int j, int f)
     const int nx = a.nx;
     const int iw = f > 0 ? f - 1 : 0, ie = f < nx ? f : nx - 1;
     FaceCells c;
-    c.cw = (i64)j * nx + iw;
-    c.ce = (i64)j * nx + ie;
+    c.cw = j * nx + iw;
+    c.ce = j * nx + ie;
     c.dxw = __ldg(a.dx + c.cw);
     c.dxe = __ldg(a.dx + c.ce);
     c.aw = __ldg(a.T.act + c.cw) != 0;
@@ -209,11 +210,11 @@ __device__ __forceinline__ FaceCells face_cells(const PPMArgs& a, int j, int f)
     return c;
 }
 
-__device__ __forceinline__ void face_flux(const PPMArgs& a, const FaceCells& fc, int k, i64 of, double u, double L_f,
+__device__ __forceinline__ void face_flux(const PPMArgs& a, const FaceCells& fc, int k, int of, double u, double L_f,
                                           double& F, double& dF)
 {
-    const i64 pf = (i64)a.ny * (a.nx + 1);
-    const i64 ow = k * a.T.pc + fc.cw, oe = k * a.T.pc + fc.ce;
+    const int pf = a.ny * (a.nx + 1);
+    const int ow = k * a.T.pc + fc.cw, oe = k * a.T.pc + fc.ce;
     const double hw_ = fc.aw ? nan_to_num(__ldg(a.T.h + ow)) : 0.0, he_ = fc.ae ? nan_to_num(__ldg(a.T.h + oe)) : 0.0;
     const double wwW = __ldg(a.h_w + ow), eeW = __ldg(a.h_e + ow), wwE = __ldg(a.h_w + oe), eeE = __ldg(a.h_e + oe);
     const double qE = __ldg(a.q_e + k * pf + of), qW = __ldg(a.q_w + k * pf + of);
@@ -238,7 +239,7 @@ __device__ __forceinline__ void face_flux(const PPMArgs& a, const FaceCells& fc,
 __device__ __forceinline__ bool face_open(const PPMArgs& a, int j, int f)
 {
     const int iw = f > 0 ? f - 1 : 0, ie = f < a.nx ? f : a.nx - 1;
-    return __ldg(a.T.act + (i64)j * a.nx + iw) && __ldg(a.T.act + (i64)j * a.nx + ie);
+    return __ldg(a.T.act + (j * a.nx + iw)) && __ldg(a.T.act + (j * a.nx + ie));
 }
 
 // Sum over the layers of (F, dF) at velocities ut + du (shift) or ut itself (the first evaluation, as the reference
@@ -246,7 +247,7 @@ __device__ __forceinline__ bool face_open(const PPMArgs& a, int j, int f)
 __device__ __forceinline__ void column_flux(const PPMArgs& a, int j, int f, double du, bool shift, double& s,
                                             double& sd)
 {
-    const i64 pf = (i64)a.ny * (a.nx + 1), o = (i64)j * (a.nx + 1) + f;
+    const int pf = a.ny * (a.nx + 1), o = j * (a.nx + 1) + f;
     const double L_f = __ldg(a.L + o);
     s = 0.0;
     sd = 0.0;
@@ -277,12 +278,12 @@ __device__ __forceinline__ void column_flux(const PPMArgs& a, int j, int f, doub
 __global__ void PPM_BOUNDS ppm_init_kernel(PPMArgs a)
 {
     const int nx = a.nx, nf = nx + 1;
-    const i64 o = (i64)blockIdx.x * blockDim.x + threadIdx.x;
-    if (o >= (i64)a.ny * nf) return;
-    const int j = (int)(o / nf), f = (int)(o - (i64)j * nf);
+    const i64 ot = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (ot >= (i64)a.ny * nf) return;
+    const int o = (int)ot, j = o / nf, f = o - j * nf;
     const int iw = f > 0 ? f - 1 : 0, ie = f < nx ? f : nx - 1;
-    const i64 pf = (i64)a.ny * nf;
-    const double limw = 0.5 * __ldg(a.dx + (i64)j * nx + iw) / a.dt, lime = 0.5 * __ldg(a.dx + (i64)j * nx + ie) / a.dt;
+    const int pf = a.ny * nf;
+    const double limw = 0.5 * __ldg(a.dx + (j * nx + iw)) / a.dt, lime = 0.5 * __ldg(a.dx + (j * nx + ie)) / a.dt;
     double mnw = INFINITY, mxe = -INFINITY;
     for (int k = 0; k < a.n; ++k) {
         const double u = __ldg(a.ut + k * pf + o);
@@ -303,9 +304,9 @@ __global__ void PPM_BOUNDS ppm_iter_kernel(PPMArgs a, int it)
 {
     if (it > 0 && *(volatile int*)(a.unconverged + it - 1) == 0) return;
     const int nf = a.nx + 1;
-    const i64 o = (i64)blockIdx.x * blockDim.x + threadIdx.x;
-    if (o >= (i64)a.ny * nf) return;
-    const int j = (int)(o / nf), f = (int)(o - (i64)j * nf);
+    const i64 ot = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (ot >= (i64)a.ny * nf) return;
+    const int o = (int)ot, j = o / nf, f = o - j * nf;
     const double e = a.err[o], d = a.du[o];
     if (e > 0.0) a.hi[o] = d;
     if (e < 0.0) a.lo[o] = d;
@@ -328,10 +329,10 @@ __global__ void PPM_BOUNDS ppm_iter_kernel(PPMArgs a, int it)
 __global__ void PPM_BOUNDS ppm_final_kernel(PPMArgs a, double* __restrict__ out)
 {
     const int nf = a.nx + 1;
-    const i64 o = (i64)blockIdx.x * blockDim.x + threadIdx.x;
-    if (o >= (i64)a.ny * nf) return;
-    const int j = (int)(o / nf), f = (int)(o - (i64)j * nf);
-    const i64 pf = (i64)a.ny * nf;
+    const i64 ot = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (ot >= (i64)a.ny * nf) return;
+    const int o = (int)ot, j = o / nf, f = o - j * nf;
+    const int pf = a.ny * nf;
     if (!face_open(a, j, f)) {
         for (int k = 0; k < a.n; ++k) out[k * pf + o] = 0.0;
         return;
@@ -742,6 +743,8 @@ static int ppm_sizes(const char* fn, int nz, int ny, int nx)
 {
     if (nz < 1 || ny < 1 || nx < 1 || ny > 65535 || nz > 65535)
         return pocean_fail(POCEAN_EINVAL, "%s: bad sizes nz=%d ny=%d nx=%d", fn, nz, ny, nx);
+    if ((i64)nz * (ny + 1) * (nx + 1) >= (1ll << 31))
+        return pocean_fail(POCEAN_EINVAL, "%s: nz=%d ny=%d nx=%d exceeds 2^31 entries per field", fn, nz, ny, nx);
     return POCEAN_OK;
 }
 
@@ -754,7 +757,7 @@ extern "C" int pocean_ppm_edges_f64(const double* h, const uint8_t* active, int 
     if (!h || !active || !h_w || !h_e) return pocean_fail(POCEAN_EINVAL, "%s: null pointer", fn);
     rc = pocean_check_device();
     if (rc) return rc;
-    const pr::Thick T{h, active, (i64)ny * nx, nx};
+    const pr::Thick T{h, active, ny * nx, nx};
     pr::ppm_edges_kernel<<<dim3((unsigned)((nx + 127) / 128), ny, nz), 128, 0, (cudaStream_t)stream>>>(T, nz, ny, h_min,
                                                                                                       h_w, h_e);
     return pocean_check_launch(fn);
@@ -788,7 +791,7 @@ extern "C" int pocean_ppm_transport_f64(const double* h, const double* ut, const
     const size_t cells = pr::align256((size_t)nz * ny * nx * sizeof(double));
     const size_t faces = pr::align256((size_t)ny * (nx + 1) * sizeof(double));
     pr::PPMArgs a;
-    a.T = pr::Thick{h, active, (i64)ny * nx, nx};
+    a.T = pr::Thick{h, active, ny * nx, nx};
     double* h_w = (double*)w; w += cells;
     double* h_e = (double*)w; w += cells;
     a.h_w = h_w; a.h_e = h_e;

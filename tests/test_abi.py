@@ -146,6 +146,9 @@ def test_producer_argument_errors_and_workspaces():
     assert L.pocean_face_transport_thickness_f64(None, 8, 8, 2, 3, 4, 1, 8, 8, None) == 1
     assert L.pocean_ppm_transport_f64(8, 8, 8, 8, 8, 8, 8, 8, 2, 3, 4, 1.0, 20, 8, 256, 16, None) == 2
     assert L.pocean_ppm_transport_f64(8, 8, 8, 8, 8, 8, 8, 8, 2, 3, 4, 1.0, -1, 8, 256, 1 << 20, None) == 1
+    # the PPM kernels index a field with 32-bit offsets: fields of 2^31 entries or more are refused
+    assert L.pocean_ppm_edges_f64(8, 8, 512, 2047, 2047, 1e-10, 8, 8, None) == 1
+    assert L.pocean_ppm_transport_f64(8, 8, 8, 8, 8, 8, 8, 8, 512, 2047, 2047, 1.0, 20, 8, 256, 1 << 20, None) == 1
     nl, wn = ctypes.c_int(0), ctypes.c_int(0)
     assert L.pocean_limit_outflow_f64(8, 8, 8, 8, 8, 2, 3, 4, 1.0, 1e-10, 50, 0x1, ctypes.byref(nl), ctypes.byref(wn),
                                       256, 1 << 20, None) == 1                     # open flag
