@@ -89,6 +89,30 @@ def test_oracle_reconstruction_matches_reference_bitwise(case):
     np.testing.assert_array_equal(O.reconstruct(rec["h"], rec["u"], int(rec["scheme"])), rec["coef"])
 
 
+def test_oracle_plm_is_exact_for_a_linear_profile_interior():
+    # tests/test_vertical_remap.py:83-93: u = 2 + 3 z as cell means on a non-uniform grid
+    h = np.array([1.0, 0.5, 2.0, 1.0, 1.5])
+    z = np.concatenate([[0.0], np.cumsum(h)])
+    u = 2 + 3 * 0.5 * (z[1:] + z[:-1])
+    coef = O.reconstruct(h, u, O.PLM)
+    for k in (1, 2, 3):
+        np.testing.assert_allclose(coef[k, 0], 2 + 3 * z[k], rtol=1e-12)
+        np.testing.assert_allclose(coef[k, 0] + coef[k, 1], 2 + 3 * z[k + 1], rtol=1e-12)
+    np.testing.assert_allclose(coef[[0, 4], 1], 0.0)
+
+
+def test_oracle_ppm_is_exact_for_a_quadratic_interior():
+    # tests/test_vertical_remap.py:124-135: cell means of 1 + z + z^2 (monotonic, no limiter action)
+    h = np.array([1.0, 0.7, 1.3, 0.9, 1.1, 0.8, 1.2])
+    z = np.concatenate([[0.0], np.cumsum(h)]) + 1.0
+    F = lambda x: x + x ** 2 / 2 + x ** 3 / 3                                   # noqa: E731
+    u = (F(z[1:]) - F(z[:-1])) / h
+    coef = O.reconstruct(h, u, O.PPM_H4)
+    for k in range(2, 5):
+        np.testing.assert_allclose(coef[k, 0], 1 + z[k] + z[k] ** 2, rtol=1e-10)
+        np.testing.assert_allclose(coef[k].sum(), 1 + z[k + 1] + z[k + 1] ** 2, rtol=1e-10)
+
+
 def test_oracle_thread_count_does_not_change_results():
     rec = FCT["open4_inflow"]
     adv = _adv(rec)
