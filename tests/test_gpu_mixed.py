@@ -1,6 +1,6 @@
 """
 The mixed-precision FCT step (pocean_advect_fct_mixed: FP32 WENO5 weights and face values, FP64 fluxes, limiter
-and bookkeeping) against the FP64 reference arithmetic.  Its bar (the north star's): at most 1e-5 relative tracer
+and bookkeeping) against the FP64 reference arithmetic.  Its bar: at most 1e-5 relative tracer
 error, tracer content conserved to 1e-13 relative, and the FCT bounds kept.
 """
 from __future__ import annotations

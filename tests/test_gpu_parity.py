@@ -2,7 +2,7 @@
 Parity of the CUDA path (libpocean_b200.so through the pyocean_b200 drop-ins) with the reference.
 
 * Golden vectors produced by the reference itself (tests/golden/): every FCT, RK3 and remap case.  The bar is the
-  north-star tolerance, 1e-12 relative (with an absolute floor of 1e-12 x the field's magnitude for values that
+  required parity tolerance, 1e-12 relative (with an absolute floor of 1e-12 x the field's magnitude for values that
   cross zero); the FP64 kernels evaluate the reference's expressions in its order without FMA contraction, so the
   measured difference is 0 and a second test asserts bit-for-bit equality.
 * Larger seeded cases (ragged tile edges, periodic axes, open edges, inflow) against the CPU oracle.
@@ -20,7 +20,7 @@ from oracle import oracle as O
 
 pytestmark = pytest.mark.gpu
 
-RTOL = 1e-12          # north-star parity tolerance for the plain FP64 kernels
+RTOL = 1e-12          # required parity tolerance of the plain FP64 kernels against the reference
 
 FCT = load_golden("fct")
 RK3 = load_golden("rk3")
