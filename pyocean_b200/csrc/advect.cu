@@ -434,8 +434,13 @@ __device__ __forceinline__ void rk3_faces_body(const StepArgs& a, int t, int k, 
     }
 }
 
+// Register budget of the RK3 face passes as resident 256-thread blocks per SM: 6 (40 registers); 8 (32 registers,
+// which the FCT face passes prefer) is 1.4 % slower here.
+#ifndef POCEAN_RK3_FACES_MINB
+#define POCEAN_RK3_FACES_MINB 6
+#endif
 template <int STAGE, bool ZV, int TJR>
-__global__ void __launch_bounds__(TI * TJR, POCEAN_FACES12_MINB * 256 / (TI * TJR)) rk3_faces_kernel(StepArgs a)
+__global__ void __launch_bounds__(TI * TJR, POCEAN_RK3_FACES_MINB * 256 / (TI * TJR)) rk3_faces_kernel(StepArgs a)
 {
     int k, t;
     split_plane(blockIdx.z, a.s.nt, a.tdiv, k, t);

@@ -1,8 +1,9 @@
 // The three WENO passes of the FCT step split into a face pass and a cell pass each (included by advect.cu).
 //
 // Face pass of stage s: one thread per cell (t, k, j, i) computes the west x-face and the south y-face of its cell
-// (the last column / row also the east / north domain face) straight from global memory (the six-cell stencils
-// overlap between neighbouring threads and are served by L1), with no shared memory and no barrier, so the pass runs
+// (the last column / row also the east / north domain face) straight from global memory (the five upwind cells of
+// a face, loaded in upwind order, overlap between neighbouring threads and are served by L1), with no shared memory
+// and no barrier, so the pass runs
 // at high occupancy and the two independent WENO5 chains of a thread overlap.  Cell pass of stage s: the stage
 // update from the stored faces.  Faces per stage are stored once:
 //   stage 1: S <- F0;  stage 2: T <- F1;  stage 3: S <- A = ((F0 + F1)/6 + 2 F2/3) - F_L,
@@ -11,7 +12,8 @@
 // cell's east and north faces, so F_L is never stored.  The arithmetic of every face and
 // update is the reference's (weno.cuh; sigma_baroclinic.py:265-321, 452-511), so results equal the reference's bit
 // for bit.  Addresses are formed once per thread as plane pointers with 32-bit offsets; interior stencils (all six
-// cells inside the domain, the common case) load with fixed offsets, edge and periodic stencils take a guarded path.
+// candidate cells inside the domain, the common case) load without checks, edge and periodic stencils take a guarded
+// path.
 #pragma once
 
 namespace po {
@@ -23,44 +25,34 @@ __device__ __forceinline__ const double* stage_field(const StepArgs& a)
     return STAGE == 1 ? a.C : (STAGE == 2 ? a.c1 : a.c2);
 }
 
-// Six cells f-3 .. f+2 of a line with element stride ST (compile-time 1 for rows) or st (columns): values and the
-// reference's validity `0 <= g < n and ok[g]` (periodic lines wrap).
+// The five cells of the stencil of face f (between cells f-1 and f) in upwind order, as the reference passes them
+// to _wval (sigma_baroclinic.py:277-297): v1..v5 = cells f-3 .. f+1 when the transport is >= 0, f+2 .. f-2 when it
+// is negative, with their validity `0 <= g < n and ok[g]` (periodic lines wrap).  Loading in upwind order after the
+// transport's sign is known replaces the per-value selects of a six-cell stencil (the loads wait for the transport
+// anyway: faces with Q = 0 load nothing): 1.1 % of advect_fct at 512 x 512 x 50, and fewer live registers.
 template <int ST>
-__device__ __forceinline__ void line6(const double* __restrict__ c, const uint8_t* __restrict__ ok, int st, int n,
-                                      bool per, int f, double* w, bool* v)
+__device__ __forceinline__ void upwind5(const double* __restrict__ c, const uint8_t* __restrict__ ok, int st, int n,
+                                        bool per, int f, bool pos, double* w, bool* v)
 {
     const int stride = ST > 0 ? ST : st;
+    const int g0 = pos ? f - 3 : f + 2, dg = pos ? 1 : -1;
     if (f >= 3 && f + 2 < n) {
-        const double* pc = c + (f - 3) * stride;
-        const uint8_t* po = ok + (f - 3) * stride;
+        const int o0 = g0 * stride, d = dg * stride;
 #pragma unroll
-        for (int m = 0; m < 6; ++m) {
-            w[m] = __ldg(pc);
-            v[m] = __ldg(po) != 0;
-            pc += stride;
-            po += stride;
+        for (int m = 0; m < 5; ++m) {
+            w[m] = __ldg(c + (o0 + m * d));
+            v[m] = __ldg(ok + (o0 + m * d)) != 0;
         }
         return;
     }
 #pragma unroll
-    for (int m = 0; m < 6; ++m) {
-        int g = f - 3 + m;
+    for (int m = 0; m < 5; ++m) {
+        int g = g0 + m * dg;
         bool in = true;
         if (per) g = wrap(g, n); else in = g >= 0 && g < n;
         w[m] = in ? __ldg(c + g * stride) : 0.0;
         v[m] = in && __ldg(ok + (in ? g : 0) * stride) != 0;
     }
-}
-
-// Q times the upwind face value of the stencil (the reference's _wval on the upwind ordering, sigma_baroclinic.py
-// :204-233, 277-297).
-template <bool MIX>
-__device__ __forceinline__ double weno_flux(const double* w, const bool* v, double q, bool z)
-{
-    const bool pos = q >= 0.0;
-    return q * weno5_face<MIX>(pos ? w[0] : w[5], pos ? w[1] : w[4], pos ? w[2] : w[3], pos ? w[3] : w[2],
-                               pos ? w[4] : w[1], pos ? v[0] : v[5], pos ? v[1] : v[4], pos ? v[2] : v[3],
-                               pos ? v[3] : v[2], pos ? v[4] : v[1], z);
 }
 
 // One plane (t, k) of the step as pointers; element offsets below are 32-bit.
@@ -92,10 +84,10 @@ __device__ __forceinline__ void x_face(const FacePlane& P, const Shape& s, const
     FL = 0.0;
     if (interior) {
         if (q != 0.0) {
-            double w[6];
-            bool v[6];
-            line6<1>(P.c + row, P.ok + row, 1, s.nx, fl.per_x, f, w, v);
-            F = weno_flux<MIX>(w, v, q, ZV);
+            double w[5];
+            bool v[5];
+            upwind5<1>(P.c + row, P.ok + row, 1, s.nx, fl.per_x, f, q >= 0.0, w, v);
+            F = q * weno5_face<MIX>(w[0], w[1], w[2], w[3], w[4], v[0], v[1], v[2], v[3], v[4], ZV);
         }
         if (DONOR) {
             const int ff = f == s.nx ? 0 : f;
@@ -125,10 +117,10 @@ __device__ __forceinline__ void y_face(const FacePlane& P, const Shape& s, const
     FL = 0.0;
     if (interior) {
         if (q != 0.0) {
-            double w[6];
-            bool v[6];
-            line6<0>(P.c + i, P.ok + i, s.nx, s.ny, fl.per_y, f, w, v);
-            F = weno_flux<MIX>(w, v, q, ZV);
+            double w[5];
+            bool v[5];
+            upwind5<0>(P.c + i, P.ok + i, s.nx, s.ny, fl.per_y, f, q >= 0.0, w, v);
+            F = q * weno5_face<MIX>(w[0], w[1], w[2], w[3], w[4], v[0], v[1], v[2], v[3], v[4], ZV);
         }
         if (DONOR) {
             const int ff = f == s.ny ? 0 : f;
@@ -234,15 +226,16 @@ __device__ __forceinline__ void faces_body(const StepArgs& a, int t, int k, int 
     }
 }
 
-// Register budget of the face passes, as resident 256-thread blocks per SM (scaled for other block sizes): 6 for
-// all three stages (40 registers; stage 3 spills a few values to L1).  Measured at 512 x 512 x 50: 8.5 % faster
-// than ptxas's own choice (58 / 80 registers), whose lower occupancy left the FP64 chains and the stencil loads
-// exposed; for stage 3, 6 is 0.6 % faster than 5 and 5 than 4.
+// Register budget of the face passes, as resident 256-thread blocks per SM (scaled for other block sizes): 7 for
+// all three stages, which ptxas rounds to 32 registers and full occupancy (64 warps per SM; stages 1-2 and 3 spill
+// a few values to L1).  Measured at 512 x 512 x 50: 2.0 % faster for advect_fct than 6 (40 registers), and 1.0 %
+// faster than 32 registers for stages 1-2 with 40 for stage 3 or the reverse; 40 registers had been 8.5 % faster
+// than ptxas's own choice (58 / 80 registers), whose lower occupancy left the FP64 chains and the loads exposed.
 #ifndef POCEAN_FACES12_MINB
-#define POCEAN_FACES12_MINB 6
+#define POCEAN_FACES12_MINB 7
 #endif
 #ifndef POCEAN_FACES3_MINB
-#define POCEAN_FACES3_MINB 6
+#define POCEAN_FACES3_MINB 7
 #endif
 // The mixed-precision face passes (FP32 weights) hold fewer FP64 values: 7 blocks of 256 (1 % faster than 6; 5 and
 // 8 slower).
