@@ -83,8 +83,8 @@ def make_workload(name: str):
 # profiles/fct_and_remap_kernels_basin_512x512x50.md gives the command): DRAM bytes read + written per call, and
 # FP64 thread instructions (DFMA + DMUL + DADD) per call.
 NCU_PER_CALL = {
-    "basin_512x512x50_nt2": {"advect_fct": {"dram_bytes": 10093055000, "fp64_inst": 18348363343},
-                             "remap_columns": {"dram_bytes": 776360000, "fp64_inst": 2861834106}},
+    "basin_512x512x50_nt2": {"advect_fct": {"dram_bytes": 9536458544, "fp64_inst": 18348363343},
+                             "remap_columns": {"dram_bytes": 778050424, "fp64_inst": 2861834106}},
 }
 FP64_LANES_PER_SM, SMS = 64, 148
 
