@@ -374,16 +374,20 @@ __device__ __forceinline__ double zface_flux(const StepArgs& a, const Shape& s, 
     const double q = a.Fz[kf * pl + ij];
     if (q == 0.0) return 0.0;
     const double* ct = cin + plane_at(t, s.n * pl);
-    double w[6];
-    uint8_t v[6];
+    // the five upwind layers in upwind order, as the reference passes them to _wval: kf-3 .. kf+1 when q >= 0,
+    // kf+2 .. kf-2 when q < 0 (no per-value selects)
+    const bool pos = q >= 0.0;
+    const int k0 = pos ? kf - 3 : kf + 2, dk = pos ? 1 : -1;
+    double w[5];
+    bool v[5];
 #pragma unroll
-    for (int m = 0; m < 6; ++m) {
-        const int kk = kf - 3 + m;
+    for (int m = 0; m < 5; ++m) {
+        const int kk = k0 + m * dk;
         const bool in = kk >= 0 && kk < s.n;
         w[m] = in ? ct[kk * pl + ij] : 0.0;
-        v[m] = in ? a.ok[kk * pl + ij] : 0;
+        v[m] = in && a.ok[(in ? kk : 0) * pl + ij] != 0;
     }
-    return q * upwind_face_value(w, v, 1, q, fl.z);
+    return q * weno5_value(w[0], w[1], w[2], w[3], w[4], v[0], v[1], v[2], v[3], v[4], fl.z);
 }
 
 // The step as face and cell passes (the FCT stages' design): the face pass of stage s has one thread per cell

@@ -54,18 +54,6 @@ __device__ __forceinline__ double weno5_value(double v1, double v2, double v3, d
     return v3;
 }
 
-// Upwind WENO5 value of the face between cells f-1 and f from the six cells f-3 .. f+2 (w[0..5] with stride
-// `step`, validity v[..]).  The upwind ordering is selected per face without branching, so a warp whose faces
-// have transports of both signs runs one reconstruction, not two.
-__device__ __forceinline__ double upwind_face_value(const double* w, const uint8_t* v, int step, double q, bool z)
-{
-    const bool pos = q >= 0.0;
-    const double w0 = w[0], w1 = w[step], w2 = w[2 * step], w3 = w[3 * step], w4 = w[4 * step], w5 = w[5 * step];
-    const bool b0 = v[0], b1 = v[step], b2 = v[2 * step], b3 = v[3 * step], b4 = v[4 * step], b5 = v[5 * step];
-    return weno5_value(pos ? w0 : w5, pos ? w1 : w4, pos ? w2 : w3, pos ? w3 : w2, pos ? w4 : w1,
-                       pos ? b0 : b5, pos ? b1 : b4, pos ? b2 : b3, pos ? b3 : b2, pos ? b4 : b1, z);
-}
-
 // ---------------------------------------------------------------------------------------------------------------
 // Mixed-precision WENO5 face value: the smoothness indicators, the nonlinear weights and the weighted candidate
 // run in FP32 on the differences of the stencil from the upwind cell (formed in FP64, then rounded), normalised by
@@ -138,17 +126,6 @@ __device__ __forceinline__ double weno5_face(double v1, double v2, double v3, do
 {
     if (MIX) return weno5_value_mixed(v1, v2, v3, v4, v5, k1, k2, k3, k4, k5, z);
     return weno5_value(v1, v2, v3, v4, v5, k1, k2, k3, k4, k5, z);
-}
-
-// Upwind face value with the arithmetic selected at compile time (MIX: FP32 weights).
-template <bool MIX>
-__device__ __forceinline__ double upwind_face(const double* w, const uint8_t* v, int step, double q, bool z)
-{
-    const bool pos = q >= 0.0;
-    const double w0 = w[0], w1 = w[step], w2 = w[2 * step], w3 = w[3 * step], w4 = w[4 * step], w5 = w[5 * step];
-    const bool b0 = v[0], b1 = v[step], b2 = v[2 * step], b3 = v[3 * step], b4 = v[4 * step], b5 = v[5 * step];
-    return weno5_face<MIX>(pos ? w0 : w5, pos ? w1 : w4, pos ? w2 : w3, pos ? w3 : w2, pos ? w4 : w1,
-                           pos ? b0 : b5, pos ? b1 : b4, pos ? b2 : b3, pos ? b3 : b2, pos ? b4 : b1, z);
 }
 
 }  // namespace po
