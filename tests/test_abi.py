@@ -59,6 +59,10 @@ def test_argument_errors_are_reported_before_any_device_work():
     assert _fct_call(ws=None) == 2
     assert _fct_call(wsb=16) == 2
     assert _fct_call(ws=264) == 2                               # misaligned workspace
+    assert _fct_call(nt=2, nz=40000) == 1                       # nt * nz planes > 65535 (one launch's grid)
+    assert b"65535" in L.pocean_last_error()
+    assert _fct_call(nz=512, ny=2047, nx=2047) == 1             # a field of 2^31 entries (32-bit offsets)
+    assert b"2^31" in L.pocean_last_error()
     assert L.pocean_remap_columns_f64(1, 1, 1, 1, 300, 10, 2, 2, 1, 2, 1, None) == 1
     assert L.pocean_remap_columns_f64(1, 1, 1, 1, 10, 10, 2, 2, 1, 7, 1, None) == 1
     with pytest.raises(ValueError):
