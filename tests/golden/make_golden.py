@@ -154,7 +154,8 @@ def rk3_cases():
     specs = [("open_vert", 2, 6, 9, 13, ("west", "east", "south"), True, "weno5", ()),
              ("closed_js_vert", 1, 5, 8, 10, (), False, "weno5js", ()),
              ("periodic_x_novert", 2, 4, 10, 12, (), False, "weno5", ("x",)),
-             ("tef", 1, 4, 7, 9, ("east",), False, "weno5", ())]
+             ("tef", 1, 4, 7, 9, ("east",), False, "weno5", ()),
+             ("open_inflow_vert", 2, 5, 8, 11, ("west", "east", "south", "north"), True, "weno5", ())]
     for seed, (name, nt, n, ny, nx, open_, vert, scheme, per) in enumerate(specs):
         rng = np.random.default_rng(200 + seed)
         dt = 10.0
@@ -162,12 +163,15 @@ def rk3_cases():
         Fz = rng.normal(size=(n + 1, ny, nx)) * 1e2 if vert else np.zeros((n + 1, ny, nx))
         Fz[0] = Fz[-1] = 0.0
         C = rng.normal(10.0, 1.0, (nt, n, ny, nx))
+        inflow = rng.normal(11.0, 1.0, C.shape) if "inflow" in name else None
         adv = TracerAdvection(scheme=scheme, time="ssprk3", dt=dt, ob=_OB(open_))
         adv.per = Periodic(per)
         fi = 3 if name == "tef" else None
-        res = adv.advect(C, V0, V1, Qx, Qy, Fz, ok, inflow=None, flux_face_i=fi)
+        res = adv.advect(C, V0, V1, Qx, Qy, Fz, ok, inflow=inflow, flux_face_i=fi)
         rec = dict(C=C, V0=V0, V1=V1, Qx=Qx, Qy=Qy, Fz=Fz, ok=ok, dt=dt, scheme=scheme,
                    open=np.array(open_, dtype="U5"), periodic=np.array(per, dtype="U1"))
+        if inflow is not None:
+            rec["inflow"] = inflow
         if fi is None:
             rec["out"] = res
         else:

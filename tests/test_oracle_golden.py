@@ -43,7 +43,8 @@ def test_oracle_rk3_matches_reference_bitwise(case):
     rec = RK3[case]
     adv = _adv(rec)
     fi = int(rec["flux_face_i"]) if "flux_face_i" in rec else None
-    res = adv.advect(rec["C"], rec["V0"], rec["V1"], rec["Qx"], rec["Qy"], rec["Fz"], rec["ok"], flux_face_i=fi)
+    res = adv.advect(rec["C"], rec["V0"], rec["V1"], rec["Qx"], rec["Qy"], rec["Fz"], rec["ok"],
+                     inflow=rec.get("inflow"), flux_face_i=fi)
     out, fx = (res if fi is not None else (res, None))
     np.testing.assert_array_equal(out, rec["out"])
     if fi is not None:
