@@ -65,6 +65,8 @@ def parse():
     ap.add_argument("--workload", default="basin", choices=["basin", "zstar_box"])
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="budget of the CPU-baseline sample")
+    ap.add_argument("--ref-seconds", type=float, default=150.0,
+                    help="time budget of the timed steps of --impl reference (it stops early past it)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--batched-steps", type=int, default=50,
                     help="steps of the 64-uneven-domains batch report (0: skip)")
@@ -77,6 +79,16 @@ def parse():
 def make_workload(name: str):
     from pyocean_b200 import workloads as W
     return W.basin() if name == "basin" else W.zstar_box()
+
+
+def workload_config(w, world: int) -> dict:
+    """The ``config`` of both arms' JSON lines: the workload, its shape and the step's schemes."""
+    nt, n, ny, nx = w.C.shape
+    return {"workload": w.name, "nt": nt, "nz": n, "ny": ny, "nx": nx,
+            "remap": {0: "pcm", 1: "plm", 2: "ppm_h4"}[w.remap_scheme], "limiter": "fct",
+            "weno": "z" if w.scheme == "weno5" else "js",
+            "l2": "inputs larger than L2 (210 MB stack, 105 MB per geometry array); no flush",
+            "parallelism": f"replicas x{world}"}
 
 
 # From one ncu capture of a step of this workload (all nine kernels; the profile summary
@@ -110,23 +122,30 @@ def cpu_model() -> str:
 
 
 # ------------------------------------------------------------------------------------------------ CPU baseline
-def cpu_sample(w, budget_s: float) -> dict:
-    """The reference algorithm on the host (oracle/ C restatement, OpenMP over every core): whole steps of the same
-    workload until ~budget_s seconds have passed (at least one), timed with perf_counter."""
+def cpu_sample(w, budget_s: float, max_steps: int = 5, warmup: int = 0) -> dict:
+    """The reference algorithm on the host (oracle/ C restatement, OpenMP over every core): ``warmup`` untimed
+    steps, then whole steps of the same workload until ``max_steps`` steps or ~budget_s seconds have passed (at
+    least one), timed with perf_counter."""
     from oracle import oracle as O
     ncores = os.cpu_count() or 1
     O.set_threads(ncores)
     adv = O.TracerAdvection(scheme=w.scheme, time="ssprk3", dt=w.dt, ob=O.OpenEdges(w.open))
     adv.per = O.Periodic(w.periodic)
+
+    def step(C):
+        A = adv.advect_fct(C, w.V0, w.V1, w.Qx, w.Qy, w.ok)
+        return np.stack([O.remap_columns(w.h_src, A[m], w.h_tgt, w.remap_scheme, w.wet) for m in range(A.shape[0])])
+
     C = w.C
+    for _ in range(warmup):
+        C = step(C)
     steps, t_total = 0, 0.0
     while True:
         t0 = time.perf_counter()
-        A = adv.advect_fct(C, w.V0, w.V1, w.Qx, w.Qy, w.ok)
-        C = np.stack([O.remap_columns(w.h_src, A[m], w.h_tgt, w.remap_scheme, w.wet) for m in range(A.shape[0])])
+        C = step(C)
         t_total += time.perf_counter() - t0
         steps += 1
-        if t_total >= budget_s or steps >= 5:
+        if t_total >= budget_s or steps >= max_steps:
             break
     value = w.tracer_cells * steps / t_total
     return dict(value=value, unit="tracer cell-steps/s", cores=O.num_threads(), kind="port",
@@ -327,9 +346,7 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> dict | None:
         "vs_baseline": None,
         "dtype": "f64",
         "data": "synthetic (seeded basin: Gaussian-bump bathymetry, 15% land, T/S stratification, eddy flow)",
-        "config": {"workload": w.name, "nt": nt, "nz": n, "ny": ny, "nx": nx, "remap": "ppm_h4",
-                   "limiter": "fct", "weno": "z", "l2": "inputs larger than L2 (210 MB stack, 105 MB per "
-                   "geometry array); no flush", "parallelism": f"replicas x{world}"},
+        "config": workload_config(w, world),
         "roofline": {"bound": "hbm", "kernel": dominant[0], "achieved": dominant[1], "peak": pk["hbm_gbs"],
                      "unit": "GB/s", "frac": dominant[1] / pk["hbm_gbs"], "peak_source": pk["source"],
                      "traffic": ncu.get(dominant[0], {}).get("dram_bytes"),
@@ -363,13 +380,15 @@ def main():
         if rank != 0:
             return
         w = make_workload(args.workload)
-        s = cpu_sample(w, args.cpu_seconds)
+        # the arm's own steps: K whole steps after min(W, 1) untimed ones, cut short after --ref-seconds so that
+        # the run ends within a few minutes
+        s = cpu_sample(w, args.ref_seconds, max_steps=args.steps, warmup=min(args.warmup, 1))
         line = {"metric": "tracer cell-steps/s at 512^2x50 (advect_fct + PPM_H4 remap, FP64)", "value": s["value"],
-                "unit": "tracer cell-steps/s", "n_gpus": 0, "steps": s["steps"], "warmup": 0,
+                "unit": "tracer cell-steps/s", "n_gpus": world, "steps": s["steps"], "warmup": min(args.warmup, 1),
                 "ms_per_step": 1e3 * s["seconds"] / s["steps"], "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f64", "data": "synthetic (same seeded workload)", "impl": "reference",
-                "config": {"workload": w.name}, "cpu_baseline": {k: s[k] for k in
-                                                                 ("value", "unit", "cores", "kind", "sample")},
+                "config": workload_config(w, world), "cpu_baseline": {k: s[k] for k in
+                                                                      ("value", "unit", "cores", "kind", "sample")},
                 "e2e": {"value": s["value"], "unit": "tracer cell-steps/s", "h2d_bytes_per_step": 0,
                         "d2h_bytes_per_step": 0}}
         print(json.dumps(line))

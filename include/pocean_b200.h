@@ -113,9 +113,10 @@ int pocean_advect_fct_layers(int mixed, const double* C, const double* V0, const
  * to a pool that forbids side allocations).  No counterpart in the reference: it is an addition of this library.
  * It allocates nothing; its scratch is a fixed array of POCEAN_NOALLOC_SCRATCH_BYTES inside the library, held by
  * every GPU that loads it until the process exits.  Shapes whose pocean_advect_fct_workspace_bytes() exceeds that
- * size are rejected with POCEAN_EINVAL.  The first call on a device looks up the array's address; make it before
- * any stream capture.  All calls on a device share the array: calls that overlap on the GPU race, so order them
- * on one stream.
+ * size are rejected with POCEAN_EINVAL.  Every call looks up the array's address in the current context (so a
+ * device reset between calls is safe); the first call on a device loads the library's module there, so make it
+ * before any stream capture.  All calls on a device share the array: calls that overlap on the GPU race, so order
+ * them on one stream.
  */
 #define POCEAN_NOALLOC_SCRATCH_BYTES (64u << 20)
 int pocean_advect_fct_f64_noalloc(const double* C, const double* V0, const double* V1, const double* Qx,

@@ -11,42 +11,30 @@
 //   * size: POCEAN_NOALLOC_SCRATCH_BYTES (64 MiB).  Every GPU that loads this module holds the array until the
 //     process exits.  A shape whose workspace (pocean_advect_fct_workspace_bytes) exceeds it is rejected with
 //     POCEAN_EINVAL and a message; nothing is launched.
-//   * the first call on a device looks up the array's device address (cudaGetSymbolAddress, with that device
-//     current) and caches it; make that first call before any stream capture on the device.
+//   * every call looks up the array's device address on the current device (cudaGetSymbolAddress, a host-side
+//     table lookup once the module is loaded) and checks the result.  The address is not kept between calls: a
+//     module loaded again (after cudaDeviceReset, or in another context of the same device) may sit at another
+//     address, and a cached one would then point at unmapped memory.  The first call on a device loads the module
+//     there; make it before any stream capture on that device.
 //   * every call on a device uses the same array and it keeps the last call's contents.  The FCT passes write
 //     every scratch element before they read it, so nothing needs clearing between calls; but calls that overlap
 //     on the GPU (different streams, or different host threads, without ordering between them) race on the
 //     array and give wrong results.  Order them on one stream.
-#include <mutex>
-
 #include "common.cuh"
 
 static __device__ __align__(256) unsigned char g_fct_scratch[POCEAN_NOALLOC_SCRATCH_BYTES];
 
 namespace {
 
-constexpr int kMaxDevices = 64;
-std::mutex g_scratch_mutex;
-void* g_scratch_ptr[kMaxDevices] = {};
-
-// Device address of g_fct_scratch on the current device (looked up once per device).
+// Device address of g_fct_scratch in the current context of the current device.
 int scratch_for_current_device(void** out)
 {
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess) return pocean_fail(POCEAN_ECUDA, "cudaGetDevice: %s", cudaGetErrorString(e));
-    if (dev < 0 || dev >= kMaxDevices)
-        return pocean_fail(POCEAN_EDEVICE, "pocean_advect_fct_f64_noalloc: device %d beyond %d", dev, kMaxDevices);
-    std::lock_guard<std::mutex> lock(g_scratch_mutex);
-    if (g_scratch_ptr[dev] == nullptr) {
-        void* p = nullptr;
-        e = cudaGetSymbolAddress(&p, g_fct_scratch);
-        if (e != cudaSuccess || p == nullptr)
-            return pocean_fail(POCEAN_ECUDA, "pocean_advect_fct_f64_noalloc: cudaGetSymbolAddress: %s",
-                               cudaGetErrorString(e));
-        g_scratch_ptr[dev] = p;
-    }
-    *out = g_scratch_ptr[dev];
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_fct_scratch);
+    if (e != cudaSuccess || p == nullptr)
+        return pocean_fail(POCEAN_ECUDA, "pocean_advect_fct_f64_noalloc: cudaGetSymbolAddress: %s",
+                           cudaGetErrorString(e));
+    *out = p;
     return POCEAN_OK;
 }
 

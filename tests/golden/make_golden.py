@@ -1,9 +1,9 @@
 """
 Generate the golden vectors of tests/golden/ by running the reference pyOCEAN code itself.
 
-Run in a container that has the reference checkout (read-only) at REFERENCE (default ``/root/reference``)::
+Run where a checkout of the reference (read-only) is available, giving its path::
 
-    python tests/golden/make_golden.py [REFERENCE]
+    python tests/golden/make_golden.py REFERENCE [case-group ...]
 
 It imports the reference's own modules (``core.components.tracers``, ``core.dynamics.sigma_baroclinic``,
 ``core.vertical.remap``) with a stub ``xarray`` (the hot-path modules use it only in annotations and helpers that
@@ -18,7 +18,10 @@ import sys
 import types
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REFERENCE = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+if len(sys.argv) < 2 or not os.path.isdir(sys.argv[1]):
+    sys.exit("usage: python tests/golden/make_golden.py REFERENCE [case-group ...]  (REFERENCE: path of the "
+             "reference pyOCEAN checkout)")
+REFERENCE = sys.argv[1]
 
 os.environ.setdefault("NUMBA_CACHE_DIR", "/tmp/pocean_golden_numba_cache")
 os.environ["PYTHONDONTWRITEBYTECODE"] = "1"

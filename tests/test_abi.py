@@ -1,10 +1,17 @@
 """The C ABI (include/pocean_b200.h) without a GPU: the library loads, exports every declared symbol, sizes its
-workspaces and rejects bad arguments before touching a device."""
+workspaces and rejects bad arguments before touching a device.
+
+The argument-error tests hand the entry points made-up pointers (1, 8, 256 ...) that the argument checks must
+refuse before any launch.  They run only in a process that sees no GPU: where one is visible (a plain `pytest` on a
+GPU machine), `test_fake_pointer_checks_run_without_a_gpu` re-runs them in a child process with
+CUDA_VISIBLE_DEVICES set empty, so a regression in the checks can never launch a kernel on a made-up address."""
 from __future__ import annotations
 
 import ctypes
 import os
 import re
+import subprocess
+import sys
 
 import pytest
 
@@ -12,6 +19,26 @@ from conftest import ROOT
 from pyocean_b200 import _lib
 
 HEADER = os.path.join(ROOT, "include", "pocean_b200.h")
+
+
+def _gpu_visible() -> bool:
+    import torch
+    return torch.cuda.is_available()
+
+
+GPU_VISIBLE = _gpu_visible()
+# tests that pass made-up device pointers: only where no GPU is visible
+fake_pointers = pytest.mark.skipif(GPU_VISIBLE, reason="made-up pointers: run by "
+                                   "test_fake_pointer_checks_run_without_a_gpu in a child process without a GPU")
+
+
+@pytest.mark.skipif(not GPU_VISIBLE, reason="no GPU visible: the made-up-pointer tests run in this process")
+def test_fake_pointer_checks_run_without_a_gpu():
+    env = dict(os.environ, CUDA_VISIBLE_DEVICES="")
+    r = subprocess.run([sys.executable, "-m", "pytest", "-q", "-p", "no:cacheprovider", "-m", "not gpu",
+                        os.path.abspath(__file__)], cwd=ROOT, env=env, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stdout[-4000:] + r.stderr[-2000:]
+    assert " passed" in r.stdout and " failed" not in r.stdout, r.stdout[-2000:]
 
 
 def declared_functions() -> list[str]:
@@ -49,6 +76,7 @@ def _fct_call(**over):
     return L.pocean_advect_fct_f64(*args.values())
 
 
+@fake_pointers
 def test_argument_errors_are_reported_before_any_device_work():
     L = _lib.lib()
     assert _fct_call(nx=0) == 1
@@ -94,6 +122,7 @@ def test_batch_domain_struct_layout_matches_ctypes(tmp_path):
         assert int(got[n]) == getattr(_Domain, n).offset, n
 
 
+@fake_pointers
 def test_batch_argument_errors():
     L = _lib.lib()
     assert L.pocean_batch_device_bytes(0) == 0
@@ -109,6 +138,7 @@ def test_batch_argument_errors():
     assert L.pocean_batch_step(None, 0, 2, 0, None) == 1
 
 
+@fake_pointers
 def test_layer_range_fct_argument_errors():
     L = _lib.lib()
     ws = 256 * 1024 * 1024
@@ -119,6 +149,7 @@ def test_layer_range_fct_argument_errors():
     assert call(0, 4, 0, _lib.FCT_UNLIMITED) == 1                                 # unlimited refused
 
 
+@fake_pointers
 def test_neighbour_argument_errors():
     L = _lib.lib()
     # unknown rule, too many layers, null pointers, bad scheme
@@ -137,6 +168,7 @@ def test_neighbour_argument_errors():
     assert L.pocean_diffuse_ale_f64(8, 8, 8, 8, 8, 8, 8, 8, None, 1, 2, 3, 4, 0, 1.0, 1.0, 8, None) == 1
 
 
+@fake_pointers
 def test_producer_argument_errors_and_workspaces():
     L = _lib.lib()
     assert L.pocean_upwind_transport_f64(8, 8, 8, 8, 8, 0, 3, 4, 8, None) == 1
@@ -157,3 +189,17 @@ def test_producer_argument_errors_and_workspaces():
     assert L.pocean_limit_outflow_f64(8, 8, 8, 8, 8, 2, 3, 4, 1.0, 1e-10, 50, 0x1, ctypes.byref(nl), ctypes.byref(wn),
                                       256, 1 << 20, None) == 1                     # open flag
     assert L.pocean_lagrangian_thickness_f64(8, 8, 8, 2, 3, 4, 1.0, 1e-9, 8, None, None) == 1
+
+
+@fake_pointers
+def test_noalloc_refuses_shapes_beyond_its_scratch():
+    # the allocation-free FCT entry point refuses a shape whose scratch need exceeds its fixed array, before any
+    # device call
+    L = _lib.lib()
+    nt, n, ny, nx = 2, 50, 512, 512
+    assert L.pocean_advect_fct_workspace_bytes(nt, n, ny, nx) > (64 << 20)
+    p = ctypes.c_void_p(256)
+    rc = L.pocean_advect_fct_f64_noalloc(p, p, p, p, p, p, None, nt, n, ny, nx, 0, 1.0, p, 0, None, None, None)
+    assert rc == 1
+    assert b"scratch" in L.pocean_last_error()
+    assert L.pocean_advect_fct_f64_noalloc(p, p, p, p, p, p, None, 0, n, ny, nx, 0, 1.0, p, 0, None, None, None) == 1
