@@ -70,6 +70,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--batched-steps", type=int, default=50,
                     help="steps of the 64-uneven-domains batch report (0: skip)")
+    ap.add_argument("--mixed-steps", type=int, default=100,
+                    help="steps of the mixed-precision accuracy report at 1024x1024x75, 6 tracers (0: skip)")
     ap.add_argument("--serve-jobs", type=int, default=200, help="jobs of the served-stream report (0: skip)")
     ap.add_argument("--serve-rate", type=float, default=15.0, help="Poisson arrival rate of the served stream [1/s]")
     ap.add_argument("--no-neighbours", action="store_true", help="skip the regrid / diffusion / velocity-remap timings")
@@ -91,13 +93,14 @@ def workload_config(w, world: int) -> dict:
             "parallelism": f"replicas x{world}"}
 
 
-# From one ncu capture of a step of this workload (all nine kernels; the profile summary
-# profiles/fct_and_remap_kernels_basin_512x512x50.md gives the command): DRAM bytes read + written per call, and
-# FP64 thread instructions (DFMA + DMUL + DADD) per call.
+# From one ncu capture of a step of this workload with the current kernels (the seven advect_fct kernels and the
+# remap): DRAM bytes read + written per call, and FP64 thread instructions (DFMA + DMUL + DADD) per call.  The
+# line carries the capture's date beside them (NCU_CAPTURED); a kernel change needs a new capture.
 NCU_PER_CALL = {
     "basin_512x512x50_nt2": {"advect_fct": {"dram_bytes": 9536458544, "fp64_inst": 18348363343},
                              "remap_columns": {"dram_bytes": 778050424, "fp64_inst": 2861834106}},
 }
+NCU_CAPTURED = "2026-12-03, ncu --set full of one step of the basin 512x512x50 workload (kernels unchanged since)"
 FP64_LANES_PER_SM, SMS = 64, 148
 
 
@@ -351,6 +354,7 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> dict | None:
                      "unit": "GB/s", "frac": dominant[1] / pk["hbm_gbs"], "peak_source": pk["source"],
                      "traffic": ncu.get(dominant[0], {}).get("dram_bytes"),
                      "traffic_note": "ncu dram__bytes_read.sum + dram__bytes_write.sum summed over the call's kernels",
+                     "traffic_captured": NCU_CAPTURED,
                      "algorithmic_bytes_per_launch": dominant[3],
                      "avg_launch_ms": dominant[2],
                      "fp64_issue_bound": {"advect_fct": fp64_part("advect_fct", adv_avg),
@@ -411,6 +415,11 @@ def main():
     if args.batched_steps > 0 and world == 1:
         from pyocean_b200.batch_report import batched_report
         line["batched"] = batched_report(steps=args.batched_steps)
+        torch.cuda.empty_cache()
+    if args.mixed_steps > 0 and world == 1:
+        from pyocean_b200.accuracy import mixed_report
+        line["mixed_accuracy"] = mixed_report(steps=args.mixed_steps, nx=1024, ny=1024, n=75, nt=6,
+                                              yardsticks=("ale",))
         torch.cuda.empty_cache()
     if args.serve_jobs > 0 and world == 1:
         from pyocean_b200.serve import serve_report

@@ -280,6 +280,29 @@ int pocean_flux_divergence_f64(const double* Qx, const double* Qy, int nz, int n
 int pocean_layer_volumes_f64(const double* h, const double* area, const uint8_t* active, int nz, int ny, int nx,
                              double* V, uint8_t* ok, void* stream);
 
+/* Periodic halo of a producer's inputs (core/model/periodic.py:72-94 Periodic.pad / crop; used for the PPM layer
+ * flux on periodic axes, core/components/layer_transport.py:121-128).  src (nlead, ny + face_y, nx + face_x) of ny x nx
+ * cells (face_y / face_x = 1 for v- / u-faces); pad: dst with `halo` wrapped positions on each side of every periodic
+ * axis (py, px), faces wrapping on the unique faces 0 .. n-1; crop: the inverse, from a padded src to the unpadded
+ * dst. */
+int pocean_periodic_pad_f64(const double* src, int nlead, int ny, int nx, int face_y, int face_x, int py, int px,
+                            int halo, double* dst, void* stream);
+int pocean_periodic_pad_u8(const uint8_t* src, int nlead, int ny, int nx, int face_y, int face_x, int py, int px,
+                           int halo, uint8_t* dst, void* stream);
+int pocean_periodic_crop_f64(const double* src, int nlead, int ny, int nx, int face_y, int face_x, int py, int px,
+                             int halo, double* dst, void* stream);
+
+/* core/vertical/ale.py:841-861 open_face_transport as core/components/open_boundary.py:334-352
+ * open_face_transports applies it: the layer fluxes Q (n layers x m faces of one open edge) are replaced where the
+ * open face depth D > 0 by the Flather flux Q_bt split with the interior cells' thickness fractions,
+ * Q_k = w_k Q_bt + L h_k (theta_bc u'_k(new) + (1 - theta_bc) u'_k(old)).  Every array is addressed with its own
+ * (layer, face) element strides; Q_bt, L and D share col_stride. */
+int pocean_open_face_transport_f64(const double* h_int, long long h_stride_k, long long h_stride_m,
+                                   const double* u_new, const double* u_old, long long u_stride_k,
+                                   long long u_stride_m, const double* Q_bt, const double* L, const double* D,
+                                   long long col_stride, int n, int m, double theta_bc, double* Q,
+                                   long long Q_stride_k, long long Q_stride_m, void* stream);
+
 /*
  * Batched steps of many independent domains (no counterpart in the reference, which advances one model at a time):
  * one ALE tracer step = advect_fct of the stack C then the remap of the advected stack C_adv onto the target grid,

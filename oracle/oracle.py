@@ -589,24 +589,66 @@ def upwind_transport_x(q_e, q_w, ut, L, Q_bt) -> np.ndarray:
 DZ_FLOOR = 1e-6                        # core/vertical/ale.py:63
 
 
+def open_face_transport(h_int, u_new, u_old, Q_bt, L, theta: float, theta_bc=None):
+    """``open_face_transport`` (core/vertical/ale.py:841-861): the layer fluxes through the faces of one open edge,
+    the Flather flux Q_bt split with the interior thickness fractions; h_int, u_new, u_old (N, m), Q_bt, L (m,)."""
+    tot = h_int.sum(axis=0)
+    wet = tot > 0
+    w = np.where(wet[None], h_int / np.where(wet, tot, 1.0)[None], 0.0)
+    pn = u_new - (w * u_new).sum(axis=0)[None]
+    po = u_old - (w * u_old).sum(axis=0)[None]
+    tb = theta if theta_bc is None else theta_bc
+    Q = w * Q_bt[None] + L[None] * h_int * (tb * pn + (1.0 - tb) * po)
+    return np.where(wet[None], Q, 0.0)
+
+
+def open_face_transports(Qx, Qy, h, un, vn, u_new, v_new, open_, open_Du, open_Dv, open_Qu, open_Qv, Lu, Lv,
+                         theta: float, theta_bc: float) -> None:
+    """In place, the open faces of Qx / Qy where the open face depth is positive
+    (core/components/open_boundary.py:334-352)."""
+    for edge, Q, D, Qo, L, hc, vo, vn1 in (
+            ("west", Qx[..., 0], open_Du[:, 0], open_Qu[:, 0], Lu[:, 0], h[..., 0], un[..., 0], u_new[..., 0]),
+            ("east", Qx[..., -1], open_Du[:, -1], open_Qu[:, -1], Lu[:, -1], h[..., -1], un[..., -1],
+             u_new[..., -1]),
+            ("south", Qy[:, 0, :], open_Dv[0, :], open_Qv[0, :], Lv[0, :], h[:, 0, :], vn[:, 0, :], v_new[:, 0, :]),
+            ("north", Qy[:, -1, :], open_Dv[-1, :], open_Qv[-1, :], Lv[-1, :], h[:, -1, :], vn[:, -1, :],
+             v_new[:, -1, :])):
+        if edge in open_:
+            Q[...] = np.where((D > 0)[None], open_face_transport(hc, vn1, vo, Qo, L, theta, theta_bc), Q)
+
+
 def ale_layer_transport(h, u_old, v_old, u_new, v_new, wet_u, wet_v, wu, wv, Lu, Lv, Du, Dv, qe, qw, qn, qs, active,
                         area, dx_t, dy_t, dt: float, theta: float, theta_bc: float, thickness_flux: str = "ppm",
-                        periodic=(False, False), fw=None) -> dict:
-    """``ALELayerTransport.__call__`` (core/components/layer_transport.py:111-156) without open faces, from the
-    restatements above: transport velocities, the PPM or donor-cell layer fluxes (v-faces on swapped axes), the
-    outflow limiter, h-dagger, the layer volumes h A, ok = active & V1 > 0 and, with freshwater, h_fw and V_fw.
-    ``qn``, ``qs`` are the v-face thicknesses in the swapped (N, nx, ny+1) layout the reference passes."""
-    if thickness_flux == "ppm" and any(periodic):
-        raise NotImplementedError("periodic PPM thickness flux (the reference pads by 4 cells)")
+                        periodic=(False, False), fw=None, open_=(), open_Du=None, open_Dv=None, open_Qu=None,
+                        open_Qv=None) -> dict:
+    """``ALELayerTransport.__call__`` (core/components/layer_transport.py:111-156) from the restatements above:
+    transport velocities, the PPM or donor-cell layer fluxes (v-faces on swapped axes; the periodic PPM flux on
+    inputs padded by four wrapped positions and cropped, as the reference does), the open faces, the outflow
+    limiter, h-dagger, the layer volumes h A, ok = active & V1 > 0 and, with freshwater, h_fw and V_fw.  ``qn``,
+    ``qs`` are the v-face thicknesses in the swapped (N, nx, ny+1) layout the reference passes."""
     sw = lambda a: np.ascontiguousarray(np.swapaxes(a, 1, 2))                       # noqa: E731
     utx, Qbx = transport_velocity(u_new, u_old, wet_u, wu, Lu, Du, theta, theta_bc)
     uty, Qby = transport_velocity(v_new, v_old, wet_v, wv, Lv, Dv, theta, theta_bc)
     if thickness_flux == "ppm":
-        Qx = ppm_transport_x(h, utx, Lu, Qbx, qe, qw, active, dt, dx_t)
-        Qy = sw(ppm_transport_x(sw(h), sw(uty), Lv.T, Qby.T, qn, qs, active.T, dt, dy_t.T))
+        def both(h_, ux, uy, Lu_, Lv_, bx, by, e, w, n_, s_, a, dx, dy):
+            return (ppm_transport_x(h_, ux, Lu_, bx, e, w, a, dt, dx),
+                    sw(ppm_transport_x(sw(h_), sw(uy), np.ascontiguousarray(Lv_.T), np.ascontiguousarray(by.T),
+                                       sw(n_), sw(s_), np.ascontiguousarray(a.T), dt, np.ascontiguousarray(dy.T))))
+        if any(periodic):
+            per = Periodic(tuple(ax for ax, f in zip(("x", "y"), periodic) if f))
+            args = (h, utx, uty, Lu, Lv, Qbx, Qby, qe, qw, sw(qn), sw(qs), active, dx_t, dy_t)
+            kinds = ("c", "u", "v", "u", "v", "u", "v", "u", "u", "v", "v", "c", "c", "c")
+            Qx, Qy = both(*(np.ascontiguousarray(per.pad(a, k, 4)) for a, k in zip(args, kinds)))
+            Qx, Qy = per.crop(Qx, "u", 4), per.crop(Qy, "v", 4)
+        else:
+            Qx, Qy = both(h, utx, uty, Lu, Lv, Qbx, Qby, qe, qw, sw(qn), sw(qs), active, dx_t, dy_t)
     else:
         Qx = upwind_transport_x(qe, qw, utx, Lu, Qbx)
         Qy = sw(upwind_transport_x(qn, qs, sw(uty), Lv.T, Qby.T))
+    if open_:
+        Qx, Qy = np.array(Qx), np.array(Qy)
+        open_face_transports(Qx, Qy, h, u_old, v_old, u_new, v_new, tuple(open_), open_Du, open_Dv, open_Qu,
+                             open_Qv, Lu, Lv, theta, theta_bc)
     Qx, Qy, n_lim = limit_outflow(h, Qx, Qy, area, dt, active, periodic=tuple(periodic))
     divh = Qx[..., 1:] - Qx[..., :-1] + Qy[:, 1:, :] - Qy[:, :-1, :]
     h_lag = lagrangian_thickness(h, divh, dt, area)

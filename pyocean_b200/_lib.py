@@ -22,6 +22,7 @@ ERRORS = {1: "invalid argument", 2: "workspace", 3: "CUDA error", 4: "unsupporte
 
 # Every symbol the header declares, with its ctypes signature.
 _P, _I, _U, _D, _Z = ctypes.c_void_p, ctypes.c_int, ctypes.c_uint, ctypes.c_double, ctypes.c_size_t
+_L = ctypes.c_longlong
 SIGNATURES: dict[str, tuple] = {
     "pocean_advect_fct_layers": (_I, [_I, _P, _P, _P, _P, _P, _P, _P, _I, _I, _I, _I, _U, _D, _P, _P, _Z, _I, _I, _I,
                                       _P]),
@@ -58,6 +59,11 @@ SIGNATURES: dict[str, tuple] = {
     "pocean_freshwater_volumes_f64": (_I, [_P, _P, _P, _D, _I, _I, _I, _P, _P, _P]),
     "pocean_flux_divergence_f64": (_I, [_P, _P, _I, _I, _I, _P, _P]),
     "pocean_layer_volumes_f64": (_I, [_P, _P, _P, _I, _I, _I, _P, _P, _P]),
+    "pocean_periodic_pad_f64": (_I, [_P, _I, _I, _I, _I, _I, _I, _I, _I, _P, _P]),
+    "pocean_periodic_pad_u8": (_I, [_P, _I, _I, _I, _I, _I, _I, _I, _I, _P, _P]),
+    "pocean_periodic_crop_f64": (_I, [_P, _I, _I, _I, _I, _I, _I, _I, _I, _P, _P]),
+    "pocean_open_face_transport_f64": (_I, [_P, _L, _L, _P, _P, _L, _L, _P, _P, _P, _L, _I, _I, _D, _P, _L, _L,
+                                            _P]),
     "pocean_batch_device_bytes": (_Z, [_I]),
     "pocean_batch_create": (_I, [_P, _I, _I, _P, _Z, ctypes.POINTER(_P), _P]),
     "pocean_batch_step": (_I, [_P, _I, _I, _I, _P]),

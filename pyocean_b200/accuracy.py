@@ -1,15 +1,21 @@
 """
 Error of the mixed-precision step against the FP64 path (whose results equal the reference's bit for bit).
 
-``mixed_report`` runs the same sequence of ALE tracer steps (advect_fct + PPM_H4 remap of every tracer) twice on
-the GPU — FP64 and mixed (FP32 WENO5 weights and face values) — and reports per tracer the max and RMS error of the
-mixed result against the FP64 one (absolute and relative to the field's range), the undershoot / overshoot of the
-mixed result below / above the initial range, and the relative change of the tracer content through the advection
-(sum V1 c_new vs sum V0 c) and through the remap (column sums of h c), each taken over the whole run.
+``mixed_report`` runs the same sequence of steps several times on the GPU and reports, per tracer, the max and RMS
+error against the FP64 run (absolute and relative to the tracer's initial range), the undershoot / overshoot below
+/ above the initial range, and the relative change of the tracer content through the advection (sum V1 c_new vs
+sum V0 c) and through the remap (column sums of h c), each the largest over the run.  Two sequences:
 
-As a yardstick of how strongly the scheme itself amplifies tiny perturbations over the run (WENO weights and FCT
-switching at fronts are not smooth functions of the data), the FP64 path is also run from initial fields moved by
-one unit in the last place, and its difference to the unperturbed FP64 run is reported beside the mixed error.
+* ``advect``: advect_fct alone, step after step (the operator whose arithmetic the mixed form changes: FP32 WENO5
+  weights and face values);
+* ``ale``: the ALE tracer step, advect_fct then the PPM_H4 remap of every tracer from the Lagrangian thicknesses
+  back onto the target grid, step after step.
+
+The ALE sequence amplifies any perturbation of its state, whatever its source: the remap's limiters (CW84, the
+edge bounding and the discontinuity check) switch discontinuously at fronts, and the advection carries each switch
+on.  Two yardsticks measure that amplification with FP64 arithmetic only: the FP64 sequence started from initial
+fields moved by one unit in the last place (``f64_one_ulp``), and the FP64 sequence whose first step alone is the
+mixed one (``mixed_first_step_only``).  Their errors against the FP64 run are reported beside the mixed errors.
 """
 from __future__ import annotations
 
@@ -21,61 +27,92 @@ from . import workloads as W
 from .step import ALETracerStep
 
 
-def mixed_report(steps: int = 100, nx: int = 1024, ny: int = 1024, n: int = 75, nt: int = 6, seed: int = 0,
-                 device=None) -> dict:
-    dev = torch.device("cuda", torch.cuda.current_device()) if device is None else torch.device(device)
-    w = W.basin(seed=seed, nx=nx, ny=ny, n=n, nt=nt, passive="tophat")
+def _run(w, dev, steps: int, mixed_steps: int, remap: bool, ulp: bool):
+    """Final stack of `steps` steps (the first `mixed_steps` mixed, the rest FP64) and the largest relative content
+    changes through the advection and the remap."""
+    nt, n, ny, nx = w.C.shape
     g = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)                     # noqa: E731
     V0, V1, Qx, Qy = g(w.V0), g(w.V1), g(w.Qx), g(w.Qy)
     ok = g(w.ok.view(np.uint8))
     wet = g(w.wet.astype(np.uint8))
     hs, ht = g(w.h_src), g(w.h_tgt)
-    flags = 0
-    out = {}
-    lo = w.C.reshape(nt, -1).min(axis=1)
-    hi = w.C.reshape(nt, -1).max(axis=1)
-    for mode in ("f64", "mixed", "f64_ulp"):
-        mixed = mode == "mixed"
-        step = ALETracerStep(nt, n, ny, nx, w.dt, flags, w.remap_scheme, device=dev, mixed=mixed)
-        c = g(w.C if mode != "f64_ulp" else np.nextafter(w.C, np.inf))
-        nxt = torch.empty_like(c)
-        adv_err = np.zeros(nt)
-        rem_err = np.zeros(nt)
-        for _ in range(steps):
-            a = step.advect(c, V0, V1, Qx, Qy, ok)
-            before = (V0[None] * c).sum(dim=(1, 2, 3))
-            after = (V1[None] * a).sum(dim=(1, 2, 3))
-            adv_err = np.maximum(adv_err, (torch.abs(after - before) / torch.abs(before)).cpu().numpy())
-            step.remap(hs, a, ht, wet, nxt)
+    f64 = ALETracerStep(nt, n, ny, nx, w.dt, 0, w.remap_scheme, device=dev, mixed=False)
+    mix = ALETracerStep(nt, n, ny, nx, w.dt, 0, w.remap_scheme, device=dev, mixed=True) if mixed_steps else None
+    c = g(np.nextafter(w.C, np.inf) if ulp else w.C)
+    nxt = torch.empty_like(c)
+    adv_err = torch.zeros(nt, dtype=torch.float64, device=dev)
+    rem_err = torch.zeros(nt, dtype=torch.float64, device=dev)
+    for s in range(steps):
+        st = mix if s < mixed_steps else f64
+        a = st.advect(c, V0, V1, Qx, Qy, ok)
+        before = (V0[None] * c).sum(dim=(1, 2, 3))
+        after = (V1[None] * a).sum(dim=(1, 2, 3))
+        adv_err = torch.maximum(adv_err, (after - before).abs() / before.abs())
+        if remap:
+            st.remap(hs, a, ht, wet, nxt)
             cin = (hs[None] * a).sum(dim=(1, 2, 3))
             cout = (ht[None] * nxt).sum(dim=(1, 2, 3))
-            rem_err = np.maximum(rem_err, (torch.abs(cout - cin) / torch.abs(cin)).cpu().numpy())
-            c, nxt = nxt, c
-        out[mode] = (c.cpu().numpy(), adv_err, rem_err)
-        del step
-        torch.cuda.empty_cache()
-    ref, _, _ = out["f64"]
-    mix, adv_m, rem_m = out["mixed"]
-    ulp, _, _ = out["f64_ulp"]
-    _, adv_f, rem_f = out["f64"]
-    wetc = np.broadcast_to(w.wet[None], (n, ny, nx))
+            rem_err = torch.maximum(rem_err, (cout - cin).abs() / cin.abs())
+        else:
+            nxt.copy_(a)
+        c, nxt = nxt, c
+    del f64, mix
+    return c, adv_err.cpu().numpy(), rem_err.cpu().numpy()
+
+
+def mixed_report(steps: int = 100, nx: int = 1024, ny: int = 1024, n: int = 75, nt: int = 6, seed: int = 0,
+                 device=None, sequences=("advect", "ale"), yardsticks=("advect", "ale")) -> dict:
+    """The report of the module docstring; ``yardsticks``: the sequences that also run the two FP64 sensitivity
+    runs (reported as None elsewhere)."""
+    dev = torch.device("cuda", torch.cuda.current_device()) if device is None else torch.device(device)
+    w = W.basin(seed=seed, nx=nx, ny=ny, n=n, nt=nt, passive="tophat")
+    lo = w.C.reshape(nt, -1).min(axis=1)
+    hi = w.C.reshape(nt, -1).max(axis=1)
+    rng = np.where(hi > lo, hi - lo, 1.0)
+    wetc = torch.from_numpy(np.broadcast_to(w.wet[None], (n, ny, nx)).copy()).to(dev)
     names = ["T", "S"] + [f"passive{m - 1}" for m in range(2, nt)]
-    tracers = []
-    for m in range(nt):
-        d = (mix[m] - ref[m])[wetc]
-        rng = float(hi[m] - lo[m]) or 1.0
-        tracers.append(dict(
-            tracer=names[m], max_abs_err=float(np.abs(d).max()), rms_abs_err=float(np.sqrt(np.mean(d * d))),
-            max_rel_err=float(np.abs(d).max() / max(np.abs(ref[m][wetc]).max(), 1e-300)),
-            max_err_over_range=float(np.abs(d).max() / rng),
-            f64_one_ulp_max_abs_diff=float(np.abs((ulp[m] - ref[m])[wetc]).max()),
-            f64_one_ulp_rms_abs_diff=float(np.sqrt(np.mean((ulp[m] - ref[m])[wetc] ** 2))),
-            undershoot=float(max(0.0, lo[m] - mix[m][wetc].min())), overshoot=float(max(0.0, mix[m][wetc].max() - hi[m])),
-            f64_undershoot=float(max(0.0, lo[m] - ref[m][wetc].min())),
-            f64_overshoot=float(max(0.0, ref[m][wetc].max() - hi[m])),
-            content_change_advect_mixed=float(adv_m[m]), content_change_advect_f64=float(adv_f[m]),
-            content_change_remap_mixed=float(rem_m[m]), content_change_remap_f64=float(rem_f[m])))
-    return dict(workload=w.name, steps=steps, dtype="mixed (FP32 WENO5 weights/faces) vs f64", tracers=tracers)
+
+    def stats(d):
+        d = torch.where(wetc[None], d, torch.zeros_like(d))
+        mx = d.abs().amax(dim=(1, 2, 3)).cpu().numpy()
+        rms = torch.sqrt((d * d).sum(dim=(1, 2, 3)) / wetc.sum()).cpu().numpy()
+        return mx, rms
+
+    out = dict(workload=w.name, steps=steps, dtype="mixed (FP32 WENO5 weights / faces) against FP64",
+               sequences={})
+    for seq in sequences:
+        remap = seq == "ale"
+        ref, adv_f, rem_f = _run(w, dev, steps, 0, remap, False)
+        mix, adv_m, rem_m = _run(w, dev, steps, steps, remap, False)
+        mx, rms = stats(mix - ref)
+        cw = torch.where(wetc[None], mix, torch.full_like(mix, np.nan))
+        mn = torch.nan_to_num(cw, nan=np.inf).amin(dim=(1, 2, 3)).cpu().numpy()
+        mxv = torch.nan_to_num(cw, nan=-np.inf).amax(dim=(1, 2, 3)).cpu().numpy()
+        del mix, cw
+        ulp_mx = ulp_rms = one_mx = None
+        if seq in yardsticks:
+            ulp, _, _ = _run(w, dev, steps, 0, remap, True)
+            ulp_mx, ulp_rms = stats(ulp - ref)
+            del ulp
+            one, _, _ = _run(w, dev, steps, 1, remap, False)
+            one_mx, _ = stats(one - ref)
+            del one
+        del ref
+        torch.cuda.empty_cache()
+        tracers = []
+        for m in range(nt):
+            tracers.append(dict(
+                tracer=names[m], max_abs_err=float(mx[m]), rms_abs_err=float(rms[m]),
+                max_err_over_range=float(mx[m] / rng[m]), rms_err_over_range=float(rms[m] / rng[m]),
+                f64_one_ulp_max_over_range=None if ulp_mx is None else float(ulp_mx[m] / rng[m]),
+                f64_one_ulp_rms_over_range=None if ulp_rms is None else float(ulp_rms[m] / rng[m]),
+                mixed_first_step_only_max_over_range=None if one_mx is None else float(one_mx[m] / rng[m]),
+                undershoot=float(max(0.0, lo[m] - mn[m])), overshoot=float(max(0.0, mxv[m] - hi[m])),
+                content_change_advect_mixed=float(adv_m[m]), content_change_advect_f64=float(adv_f[m]),
+                content_change_remap_mixed=float(rem_m[m]) if remap else None,
+                content_change_remap_f64=float(rem_f[m]) if remap else None))
+        out["sequences"][seq] = tracers
+    return out
 
 
 if __name__ == "__main__":
@@ -83,4 +120,5 @@ if __name__ == "__main__":
     import sys
     _lib.lib()
     steps = int(sys.argv[1]) if len(sys.argv) > 1 else 100
-    print(json.dumps(mixed_report(steps=steps)))
+    size = [int(x) for x in sys.argv[2:5]] if len(sys.argv) > 4 else [1024, 1024, 75]
+    print(json.dumps(mixed_report(steps=steps, nx=size[0], ny=size[1], n=size[2])))

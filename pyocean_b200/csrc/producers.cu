@@ -983,3 +983,136 @@ extern "C" int pocean_layer_volumes_f64(const double* h, const double* area, con
                                                                                            V, ok);
     return pocean_check_launch(fn);
 }
+
+// ---------------------------------------------------------------------------------------------------------------
+// Periodic halo of a producer's inputs (core/model/periodic.py:72-94 `Periodic.pad` / `crop`).  The reference
+// reaches the wrap of its PPM layer flux by running the kernel on inputs extended by `halo` wrapped positions on
+// each periodic axis and cropping the result (core/components/layer_transport.py:121-128); these copies give the
+// CUDA kernels the same extended inputs, so the fluxes (and the Newton iteration's global stop test, which sees the
+// halo faces too) are the reference's bit for bit.
+namespace po {
+namespace pr {
+
+// dst (nlead, Yd, Xd) from src (nlead, Ys, Xs): position y of dst reads row (y - oy) mod ny of src when `wy` (the
+// wrapped axis of ny unique positions), else row y + oy; the same for x.
+template <typename T>
+__global__ void __launch_bounds__(256) window_kernel(const T* __restrict__ src, int Ys, int Xs, T* __restrict__ dst,
+                                                     int Yd, int Xd, i64 total, int oy, int ox, int wy, int wx,
+                                                     int ny, int nx)
+{
+    const i64 e = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= total) return;
+    const int x = (int)(e % Xd);
+    const i64 r = e / Xd;
+    const int y = (int)(r % Yd);
+    const i64 l = r / Yd;
+    const int sy = wy ? wrap(y - oy, ny) : y + oy;
+    const int sx = wx ? wrap(x - ox, nx) : x + ox;
+    dst[e] = src[(l * Ys + sy) * Xs + sx];
+}
+
+}  // namespace pr
+}  // namespace po
+
+template <typename T>
+static int periodic_window(const char* fn, const T* src, int nlead, int ny, int nx, int face_y, int face_x, int py,
+                           int px, int halo, T* dst, bool pad, void* stream)
+{
+    if (nlead < 1 || ny < 1 || nx < 1 || halo < 0 || (face_y & ~1) || (face_x & ~1))
+        return pocean_fail(POCEAN_EINVAL, "%s: bad sizes (nlead=%d ny=%d nx=%d halo=%d)", fn, nlead, ny, nx, halo);
+    if (!src || !dst) return pocean_fail(POCEAN_EINVAL, "%s: null pointer", fn);
+    int rc = pocean_check_device();
+    if (rc) return rc;
+    const int Yc = ny + face_y, Xc = nx + face_x;                               // the unpadded array
+    const int Yp = py ? ny + 2 * halo + face_y : Yc, Xp = px ? nx + 2 * halo + face_x : Xc;
+    const int Ys = pad ? Yc : Yp, Xs = pad ? Xc : Xp, Yd = pad ? Yp : Yc, Xd = pad ? Xp : Xc;
+    const i64 total = (i64)nlead * Yd * Xd;
+    pr::window_kernel<T><<<(unsigned)((total + 255) / 256), 256, 0, (cudaStream_t)stream>>>(
+        src, Ys, Xs, dst, Yd, Xd, total, py ? halo : 0, px ? halo : 0, pad && py, pad && px, ny, nx);
+    return pocean_check_launch(fn);
+}
+
+extern "C" int pocean_periodic_pad_f64(const double* src, int nlead, int ny, int nx, int face_y, int face_x, int py,
+                                       int px, int halo, double* dst, void* stream)
+{
+    return periodic_window("pocean_periodic_pad_f64", src, nlead, ny, nx, face_y, face_x, py, px, halo, dst, true,
+                           stream);
+}
+
+extern "C" int pocean_periodic_pad_u8(const uint8_t* src, int nlead, int ny, int nx, int face_y, int face_x, int py,
+                                      int px, int halo, uint8_t* dst, void* stream)
+{
+    return periodic_window("pocean_periodic_pad_u8", src, nlead, ny, nx, face_y, face_x, py, px, halo, dst, true,
+                           stream);
+}
+
+extern "C" int pocean_periodic_crop_f64(const double* src, int nlead, int ny, int nx, int face_y, int face_x, int py,
+                                        int px, int halo, double* dst, void* stream)
+{
+    return periodic_window("pocean_periodic_crop_f64", src, nlead, ny, nx, face_y, face_x, py, px, halo, dst, false,
+                           stream);
+}
+
+// ---------------------------------------------------------------------------------------------------------------
+// Layer fluxes through the faces of one open edge (core/vertical/ale.py:841-861 `open_face_transport`, as
+// core/components/open_boundary.py:334-352 `open_face_transports` applies it in place where the open face depth
+// D > 0): Q_k = w_k Q_bt + L h_k (theta_bc u'_k^new + (1 - theta_bc) u'_k^old), w_k = h_k / sum h, u' = u - sum w u;
+// 0 in a column without water.  One thread per face of the edge; the column sums run over k in order, as numpy's
+// reduction over the leading axis does.
+namespace po {
+namespace pr {
+
+__global__ void __launch_bounds__(128) open_face_kernel(const double* __restrict__ h, i64 hk, i64 hm,
+                                                        const double* __restrict__ un, const double* __restrict__ uo,
+                                                        i64 uk, i64 um, const double* __restrict__ Qbt,
+                                                        const double* __restrict__ L, const double* __restrict__ D,
+                                                        i64 qm, int n, int m, double tb, double* __restrict__ Q,
+                                                        i64 Qk, i64 Qm)
+{
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= m) return;
+    if (!(D[c * qm] > 0)) return;
+    const double* hc = h + c * hm;
+    double tot = 0.0;
+    for (int k = 0; k < n; ++k) tot += hc[k * hk];
+    const bool wet = tot > 0;
+    const double dn = wet ? tot : 1.0;
+    double sn = 0.0, so = 0.0;
+    for (int k = 0; k < n; ++k) {
+        const double w = wet ? hc[k * hk] / dn : 0.0;
+        sn += w * un[c * um + k * uk];
+    }
+    for (int k = 0; k < n; ++k) {
+        const double w = wet ? hc[k * hk] / dn : 0.0;
+        so += w * uo[c * um + k * uk];
+    }
+    const double qb = Qbt[c * qm], Lc = L[c * qm];
+    for (int k = 0; k < n; ++k) {
+        const double hk_ = hc[k * hk];
+        const double w = wet ? hk_ / dn : 0.0;
+        const double pn = un[c * um + k * uk] - sn;
+        const double po = uo[c * um + k * uk] - so;
+        const double q = w * qb + Lc * hk_ * (tb * pn + (1.0 - tb) * po);
+        Q[c * Qm + k * Qk] = wet ? q : 0.0;
+    }
+}
+
+}  // namespace pr
+}  // namespace po
+
+extern "C" int pocean_open_face_transport_f64(const double* h_int, long long h_stride_k, long long h_stride_m,
+                                              const double* u_new, const double* u_old, long long u_stride_k,
+                                              long long u_stride_m, const double* Q_bt, const double* L,
+                                              const double* D, long long col_stride, int n, int m, double theta_bc,
+                                              double* Q, long long Q_stride_k, long long Q_stride_m, void* stream)
+{
+    const char* fn = "pocean_open_face_transport_f64";
+    if (n < 1 || m < 1) return pocean_fail(POCEAN_EINVAL, "%s: bad sizes (n=%d m=%d)", fn, n, m);
+    if (!h_int || !u_new || !u_old || !Q_bt || !L || !D || !Q) return pocean_fail(POCEAN_EINVAL, "%s: null pointer", fn);
+    int rc = pocean_check_device();
+    if (rc) return rc;
+    pr::open_face_kernel<<<(unsigned)((m + 127) / 128), 128, 0, (cudaStream_t)stream>>>(
+        h_int, h_stride_k, h_stride_m, u_new, u_old, u_stride_k, u_stride_m, Q_bt, L, D, col_stride, n, m, theta_bc, Q,
+        Q_stride_k, Q_stride_m);
+    return pocean_check_launch(fn);
+}

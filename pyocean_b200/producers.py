@@ -181,12 +181,79 @@ def _swap(t: torch.Tensor) -> torch.Tensor:
     return t.transpose(-1, -2).contiguous()
 
 
+PPM_HALO = 4                           # core/components/layer_transport.py:122 (the PPM edges' stencil)
+
+
+def _face_kind(kind: str) -> tuple[int, int]:
+    """(face_y, face_x) of a staggering: 'c' cells, 'u' u-faces, 'v' v-faces."""
+    return (1 if kind == "v" else 0), (1 if kind == "u" else 0)
+
+
+def periodic_pad(t: torch.Tensor, kind: str, px: bool, py: bool, halo: int) -> torch.Tensor:
+    """``t`` (leading axes, then y, x) with ``halo`` wrapped positions on each side of the periodic axes, as
+    ``Periodic.pad`` (core/model/periodic.py:72-85): faces wrap on the unique faces 0 .. n-1."""
+    fy, fx = _face_kind(kind)
+    ny, nx = t.shape[-2] - fy, t.shape[-1] - fx
+    lead = int(np.prod(t.shape[:-2])) if t.dim() > 2 else 1
+    shape = tuple(t.shape[:-2]) + (ny + fy + (2 * halo if py else 0), nx + fx + (2 * halo if px else 0))
+    out = torch.empty(shape, dtype=t.dtype, device=t.device)
+    fn = _lib.lib().pocean_periodic_pad_u8 if t.dtype == torch.uint8 else _lib.lib().pocean_periodic_pad_f64
+    _lib.check(fn(t.contiguous().data_ptr(), lead, ny, nx, fy, fx, int(py), int(px), halo, out.data_ptr(),
+                  torch.cuda.current_stream(t.device).cuda_stream), "periodic_pad")
+    return out
+
+
+def periodic_crop(t: torch.Tensor, kind: str, px: bool, py: bool, halo: int) -> torch.Tensor:
+    """The interior positions of a padded ``t`` (``Periodic.crop``, core/model/periodic.py:87-93)."""
+    fy, fx = _face_kind(kind)
+    ny = t.shape[-2] - fy - (2 * halo if py else 0)
+    nx = t.shape[-1] - fx - (2 * halo if px else 0)
+    lead = int(np.prod(t.shape[:-2])) if t.dim() > 2 else 1
+    out = torch.empty(tuple(t.shape[:-2]) + (ny + fy, nx + fx), dtype=t.dtype, device=t.device)
+    _lib.check(_lib.lib().pocean_periodic_crop_f64(t.contiguous().data_ptr(), lead, ny, nx, fy, fx, int(py), int(px),
+                                                   halo, out.data_ptr(),
+                                                   torch.cuda.current_stream(t.device).cuda_stream), "periodic_crop")
+    return out
+
+
+def open_face_transports(Qx: torch.Tensor, Qy: torch.Tensor, h, un, vn, u_new, v_new, open_, open_Du, open_Dv,
+                         open_Qu, open_Qv, Lu, Lv, theta_bc: float) -> None:
+    """In place on device tensors: the layer fluxes through the open faces where the open face depth is positive,
+    the Flather flux split with the interior cells' thickness fractions (core/components/open_boundary.py:334-352,
+    core/vertical/ale.py:841-861).  h (N, ny, nx); un, u_new, Qx (N, ny, nx+1); vn, v_new, Qy (N, ny+1, nx);
+    open_D*, open_Q*, L* face arrays of one layer."""
+    n, ny, nx = h.shape
+    L_ = _lib.lib()
+    st = torch.cuda.current_stream(h.device).cuda_stream
+    hs, us_x, us_y = (ny * nx, nx), (ny * (nx + 1), nx + 1), ((ny + 1) * nx, nx)
+    for edge in open_:
+        if edge == "west" or edge == "east":
+            c = 0 if edge == "west" else -1
+            ch, cu = (0 if c == 0 else nx - 1), (0 if c == 0 else nx)
+            rc = L_.pocean_open_face_transport_f64(
+                h.data_ptr() + 8 * ch, hs[0], hs[1], u_new.data_ptr() + 8 * cu, un.data_ptr() + 8 * cu, us_x[0],
+                us_x[1], open_Qu.data_ptr() + 8 * cu, Lu.data_ptr() + 8 * cu, open_Du.data_ptr() + 8 * cu, nx + 1, n,
+                ny, float(theta_bc), Qx.data_ptr() + 8 * cu, us_x[0], us_x[1], st)
+        elif edge == "south" or edge == "north":
+            r = 0 if edge == "south" else 1
+            rh, rv = (0 if r == 0 else (ny - 1) * nx), (0 if r == 0 else ny * nx)
+            rc = L_.pocean_open_face_transport_f64(
+                h.data_ptr() + 8 * rh, hs[0], 1, v_new.data_ptr() + 8 * rv, vn.data_ptr() + 8 * rv, us_y[0], 1,
+                open_Qv.data_ptr() + 8 * rv, Lv.data_ptr() + 8 * rv, open_Dv.data_ptr() + 8 * rv, 1, n, nx,
+                float(theta_bc), Qy.data_ptr() + 8 * rv, us_y[0], 1, st)
+        else:
+            raise ValueError(f"unknown open edge {edge!r}")
+        _lib.check(rc, "open_face_transport")
+
+
 class ALELayerTransport:
     """The Lagrangian layer-transport step of the ALE core on B200, with the reference component's constructor and
     call (layer_transport.py:98-160): transport velocities, the PPM or donor-cell layer fluxes (v-faces on swapped
-    axes), the outflow limiter, h-dagger, the layer volumes h A, ``ok`` and, with ``fluxes.fw``, the freshwater
-    thickness and volumes.  Open faces (``open_`` not empty) and the periodic PPM flux (the reference pads by 4 cells)
-    raise ``NotImplementedError``.  The ALE layer volumes are h A (sigma_baroclinic.py:1812-1815): the
+    axes; on periodic axes the PPM flux runs on inputs padded by four wrapped positions and is cropped, as the
+    reference does), the open faces, the outflow limiter, h-dagger, the layer volumes h A, ``ok`` and, with
+    ``fluxes.fw``, the freshwater thickness and volumes.  Open faces (``open_`` not empty)     are written in place on the device from ``fluxes.open_Du`` / ``open_Dv`` / ``open_Qu`` / ``open_Qv`` (the open
+    boundary component's Flather split, core/components/open_boundary.py:334-352; ``theta_bc`` from ``ob`` when it
+    has one, else the call's).  The ALE layer volumes are h A (sigma_baroclinic.py:1812-1815): the
     ``layer_volumes`` callable is kept for the interface and not called.  Arrays are NumPy (results come back as
     NumPy) or CUDA tensors (everything stays in HBM)."""
 
@@ -200,11 +267,7 @@ class ALELayerTransport:
 
     def __call__(self, st, eta_new, u_new, v_new, fluxes, theta_bc: float, open_, wu, wv, qe, qw, qn,
                  qs) -> LayerFluxes:
-        if open_:
-            raise NotImplementedError("open-boundary face transports are not on the GPU")
         px, py = bool(getattr(self.per, "x", False)), bool(getattr(self.per, "y", False))
-        if self.thickness_flux == "ppm" and (px or py):
-            raise NotImplementedError("the periodic PPM thickness flux (the reference pads by 4 cells)")
         fw = getattr(fluxes, "fw", None)
         n, ny, nx = shape_of(st.h)
         fs, dt, L = self.fs, self.dt, _lib.lib()
@@ -220,13 +283,35 @@ class ALELayerTransport:
         Lv_t, Qby_t, uty_t = _swap(cv.f64(fs.Lv, (ny + 1, nx))), _swap(Qby), _swap(uty)
         qn_d, qs_d = cv.f64(qn), cv.f64(qs)
         if self.thickness_flux == "ppm":
-            Qx = ppm_transport_x(h, utx, cv.f64(fs.Lu, (ny, nx + 1)), Qbx, cv.f64(qe), cv.f64(qw), act, dt,
-                                 cv.f64(self.vi_geom["dx_t"], (ny, nx)))
-            Qy = _swap(ppm_transport_x(_swap(h), uty_t, Lv_t, Qby_t, qn_d, qs_d, _swap(act), dt,
-                                       _swap(cv.f64(self.vi_geom["dy_t"], (ny, nx)))))
+            Lu_d, dx_d, dy_d = cv.f64(fs.Lu, (ny, nx + 1)), cv.f64(self.vi_geom["dx_t"], (ny, nx)), cv.f64(
+                self.vi_geom["dy_t"], (ny, nx))
+            Lv_d, qe_d, qw_d = cv.f64(fs.Lv, (ny + 1, nx)), cv.f64(qe), cv.f64(qw)
+            if px or py:                               # pad-crop with the PPM halo (layer_transport.py:121-128)
+                pad = lambda t, k: periodic_pad(t, k, px, py, PPM_HALO)                   # noqa: E731
+                hp, uxp, uyp, Lup, Lvp = pad(h, "c"), pad(utx, "u"), pad(uty, "v"), pad(Lu_d, "u"), pad(Lv_d, "v")
+                bxp, byp, ep, wp = pad(Qbx, "u"), pad(Qby, "v"), pad(qe_d, "u"), pad(qw_d, "u")
+                np_, sp = pad(_swap(qn_d), "v"), pad(_swap(qs_d), "v")
+                ap, dxp, dyp = pad(act, "c"), pad(dx_d, "c"), pad(dy_d, "c")
+                Qx = periodic_crop(ppm_transport_x(hp, uxp, Lup, bxp, ep, wp, ap, dt, dxp), "u", px, py, PPM_HALO)
+                Qy = periodic_crop(_swap(ppm_transport_x(_swap(hp), _swap(uyp), _swap(Lvp), _swap(byp), _swap(np_),
+                                                         _swap(sp), _swap(ap), dt, _swap(dyp))), "v", px, py,
+                                   PPM_HALO)
+            else:
+                Qx = ppm_transport_x(h, utx, Lu_d, Qbx, qe_d, qw_d, act, dt, dx_d)
+                Qy = _swap(ppm_transport_x(_swap(h), uty_t, Lv_t, Qby_t, qn_d, qs_d, _swap(act), dt, _swap(dy_d)))
         else:
             Qx = upwind_transport_x(cv.f64(qe), cv.f64(qw), utx, cv.f64(fs.Lu, (ny, nx + 1)), Qbx)
             Qy = _swap(upwind_transport_x(qn_d, qs_d, uty_t, Lv_t, Qby_t))
+        if open_:                                      # old velocity unmasked: the wet flag is False at edges
+            if self.ob is None:
+                raise ValueError("open edges need the open-boundary component (ob) of the reference's interface")
+            tbc = getattr(self.ob, "theta_bc", None)
+            tb = fs.theta if tbc is None else tbc          # ale.py:859
+            Qx, Qy = Qx.clone(), Qy.clone()
+            open_face_transports(Qx, Qy, h, cv.f64(st.u), cv.f64(st.v), cv.f64(u_new), cv.f64(v_new), tuple(open_),
+                                 cv.f64(fluxes.open_Du, (ny, nx + 1)), cv.f64(fluxes.open_Dv, (ny + 1, nx)),
+                                 cv.f64(fluxes.open_Qu, (ny, nx + 1)), cv.f64(fluxes.open_Qv, (ny + 1, nx)),
+                                 cv.f64(fs.Lu, (ny, nx + 1)), cv.f64(fs.Lv, (ny + 1, nx)), tb)
         Qx, Qy, n_lim = limit_outflow(h, Qx, Qy, area, dt, act, periodic=(px, py))
         divh = cv.empty((n, ny, nx))
         _lib.check(L.pocean_flux_divergence_f64(Qx.data_ptr(), Qy.data_ptr(), n, ny, nx, divh.data_ptr(),

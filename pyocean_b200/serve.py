@@ -7,7 +7,10 @@ thicknesses, transports, workspace) resident in HBM and advances ALL admitted jo
 time (every pass one launch over all jobs, as in ``batch.DomainBatch``).  Between steps it admits the jobs that have
 arrived — in arrival order, while the HBM budget and the slot count allow — and retires the jobs that have run
 their steps, so a job that arrives while others run joins the next step instead of waiting for them (continuous
-batching, as LLM servers batch requests per decoding iteration).  The host only enqueues work: it runs at most
+batching, as LLM servers batch requests per decoding iteration).  Which admitted jobs a step advances is the
+policy's (``Server._select``): by default the oldest job plus the small jobs that fit beside it without slowing it
+by more than a quarter, so the long jobs of the tail keep close to their run-alone time while short jobs never wait
+behind them.  The host only enqueues work: it runs at most
 ``max_ahead`` iterations ahead of the GPU, so the device queue never drains while jobs are active.
 
 Per job the report has the latency from arrival to the completion of its last step on the device (CUDA event
@@ -89,9 +92,15 @@ def make_domain(job: Job, device) -> Domain:
 class Server:
     """Serves a job stream; ``run`` returns the per-job and aggregate report."""
 
+    POLICIES = ("oldest_first", "all")
+
     def __init__(self, device=None, mixed: bool = True, batched: bool = True, max_slots: int = 256,
                  hbm_budget: int | None = None, max_ahead: int = 3, max_steps_per_iter: int = 4,
-                 tile_rows: int = 8, remap_nf: int = 2, keep_results: bool = False) -> None:
+                 tile_rows: int = 8, remap_nf: int = 2, keep_results: bool = False, policy: str = "oldest_first",
+                 fill_cells: int = 4_000_000, share: float = 0.25) -> None:
+        if policy not in self.POLICIES:
+            raise ValueError(f"policy {policy!r}: use one of {self.POLICIES}")
+        self.policy, self.fill_cells, self.share = policy, int(fill_cells), float(share)
         self.device = torch.device("cuda", torch.cuda.current_device()) if device is None else torch.device(device)
         self.mixed, self.batched = bool(mixed), bool(batched)
         self.max_slots = 1 if not batched else int(max_slots)
@@ -114,6 +123,7 @@ class Server:
         peak_active = 0
         inflight: deque[torch.cuda.Event] = deque()
         plan = None
+        step_set = None
         plan_buf = torch.empty(_lib.lib().pocean_batch_device_bytes(self.max_slots), dtype=torch.uint8, device=dev)
         parity = 0
         iters = launches = 0
@@ -147,25 +157,28 @@ class Server:
                 if pending:
                     time.sleep(max(0.0, min(0.01, pending[0].arrival - (clock() - t0))))
                 continue
-            k = min(self.kmax, min(j.steps - j.done_steps for j in active))
+            if changed or step_set is None:
+                step_set = self._select(active)
+                plan = None             # built for the stepped jobs with their current orientation
+            k = min(self.kmax, min(j.steps - j.done_steps for j in step_set))
             if self.batched:
-                if changed or plan is None:
-                    plan = _Plan([j.dom.as_struct(swapped=bool(j.flip)) for j in active], self.tile_rows, dev,
+                if plan is None:
+                    plan = _Plan([j.dom.as_struct(swapped=bool(j.flip)) for j in step_set], self.tile_rows, dev,
                                  buf=plan_buf, stream=stream.cuda_stream)
                     parity = 0
                 for _ in range(k):
                     plan.step(parity, self.remap_nf, self.mixed, stream.cuda_stream)
                     parity ^= 1
-                launches += k * self._launches(active)
+                launches += k * self._launches(step_set)
             else:
-                for j in active:
+                for j in step_set:
                     for s in range(k):
                         sequential_step([j.dom], j.flip ^ (s & 1), mixed=self.mixed, stream=stream.cuda_stream)
-                launches += k * sum(7 + (j.nt >= 2) + (j.nt % 2) + 1 for j in active)
+                launches += k * sum(7 + (j.nt >= 2) + (j.nt % 2) + 1 for j in step_set)
             iters += 1
-            occupancy.append(len(active))
+            occupancy.append(len(step_set))
             done = []
-            for j in active:
+            for j in step_set:
                 j.done_steps += k
                 j.flip ^= k & 1
                 if j.done_steps == j.steps:
@@ -175,7 +188,7 @@ class Server:
                     self._retire(j, stream)
                     used -= j.nbytes
                 active = [j for j in active if j.done_steps < j.steps]
-                plan = None             # rebuilt before the next step with the survivors' current orientation
+                step_set = None         # chosen again (and its plan built) before the next step
             ev = torch.cuda.Event()
             ev.record(stream)
             inflight.append(ev)
@@ -197,6 +210,27 @@ class Server:
                     unit="tracer cell-steps/s", iterations=iters, gpu_launches=launches,
                     mean_active=float(np.mean(occupancy)) if occupancy else 0.0, peak_active=peak_active,
                     peak_hbm_bytes=peak_used, hbm_budget=self.hbm_budget)
+
+    def _select(self, active: list[Job]) -> list[Job]:
+        """The jobs the next steps advance.  ``all``: every admitted job (processor sharing).  ``oldest_first``: the
+        job that arrived first, plus the others in increasing remaining work while the combined step stays within
+        max(fill_cells, (1 + share) x the oldest job's step): the oldest job is never slowed by more than ``share``
+        (so a long job's latency stays close to running it alone), and small jobs fill the GPU beside it.  One job
+        at a time (not batched): the oldest alone."""
+        oldest = min(active, key=lambda j: (j.arrival, j.id))
+        if not self.batched:
+            return [oldest]
+        if self.policy == "all":
+            return list(active)
+        cells = lambda j: j.nt * j.nz * j.ny * j.nx                                     # noqa: E731
+        budget = max(self.fill_cells, (1.0 + self.share) * cells(oldest))
+        chosen, used = [oldest], cells(oldest)
+        for j in sorted((j for j in active if j is not oldest), key=lambda j: ((j.steps - j.done_steps) * cells(j),
+                                                                            j.arrival)):
+            if used + cells(j) <= budget:
+                chosen.append(j)
+                used += cells(j)
+        return chosen
 
     def _launches(self, active) -> int:
         if self.remap_nf == 2:
@@ -231,6 +265,7 @@ def serve_report(n_jobs: int = 200, rate: float = 15.0, seed: int = 0, device=No
                            "generated on the device per job"))
     out["batched_mixed"] = Server(dev, mixed=True).run(stream(rate))
     out["one_at_a_time_f64"] = Server(dev, mixed=False, batched=False).run(stream(rate))
+    out["batched_mixed_all_jobs_every_step"] = Server(dev, mixed=True, policy="all").run(stream(rate))
     if batched_f64:
         out["batched_f64"] = Server(dev, mixed=False).run(stream(rate))
     out["p99_ratio_plain_vs_served"] = out["one_at_a_time_f64"]["p99_s"] / out["batched_mixed"]["p99_s"]

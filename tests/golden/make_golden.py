@@ -601,6 +601,127 @@ def layer_transport_cases():
     return out
 
 
+def layer_transport_ext_cases():
+    """The whole ALE layer-transport step with the PPM thickness flux on a periodic x axis and on periodic x and y
+    axes (the reference pads its inputs by four wrapped cells and crops), and with open edges (the Flather split of
+    OpenBoundary.open_face_transports, PPM and donor cell)."""
+    from types import SimpleNamespace as NS
+    from core.components.layer_transport import ALELayerTransport
+    from core.components.open_boundary import OpenBoundary
+    out = {}
+    rng = np.random.default_rng(83)
+    n, ny, nx = 6, 11, 14
+    H, active, h, dx, Lu = _producer_state(rng, n, ny, nx)
+    hz = np.where(active[None], np.nan_to_num(h), 0.0)
+    dt = 600.0
+    area = dx * rng.uniform(900.0, 1100.0, (ny, nx))
+    Lv = rng.uniform(900.0, 1100.0, (ny + 1, nx))
+    dy = rng.uniform(900.0, 1100.0, (ny, nx))
+    eta, eta_new = rng.uniform(-0.3, 0.3, (ny, nx)), rng.uniform(-0.3, 0.3, (ny, nx))
+    Dc = hz.sum(0)
+    for name, flux, per, open_ in (("lt_ppm_perx", "ppm", ("x",), ()), ("lt_ppm_perxy", "ppm", ("x", "y"), ()),
+                                   ("lt_ppm_open", "ppm", (), ("west", "north")),
+                                   ("lt_upwind_open", "upwind", (), ("east", "south")),
+                                   ("lt_ppm_perx_open_sn", "ppm", ("x",), ("south", "north"))):
+        px, py = "x" in per, "y" in per
+        wrapx = active[:, 0] & active[:, -1]
+        wrapy = active[0, :] & active[-1, :]
+        wet_u = np.zeros((ny, nx + 1), bool)
+        wet_u[:, 1:-1] = active[:, 1:] & active[:, :-1]
+        wet_v = np.zeros((ny + 1, nx), bool)
+        wet_v[1:-1] = active[1:] & active[:-1]
+        if px:
+            wet_u[:, 0] = wet_u[:, -1] = wrapx
+        if py:
+            wet_v[0] = wet_v[-1] = wrapy
+        u_old, u_new = rng.normal(0.0, 0.1, (n, ny, nx + 1)), rng.normal(0.0, 0.1, (n, ny, nx + 1))
+        v_old, v_new = rng.normal(0.0, 0.1, (n, ny + 1, nx)), rng.normal(0.0, 0.1, (n, ny + 1, nx))
+        if px:
+            u_old[..., -1], u_new[..., -1] = u_old[..., 0], u_new[..., 0]
+        if py:
+            v_old[:, -1], v_new[:, -1] = v_old[:, 0], v_new[:, 0]
+        u_old *= wet_u
+        u_new *= wet_u
+        v_old *= wet_v
+        v_new *= wet_v
+        Du = np.zeros((ny, nx + 1))
+        Du[:, 1:-1] = np.minimum(Dc[:, 1:], Dc[:, :-1])
+        Dv = np.zeros((ny + 1, nx))
+        Dv[1:-1] = np.minimum(Dc[1:], Dc[:-1])
+        if px:
+            Du[:, 0] = Du[:, -1] = np.minimum(Dc[:, 0], Dc[:, -1])
+        if py:
+            Dv[0] = Dv[-1] = np.minimum(Dc[0], Dc[-1])
+        Du *= wet_u
+        Dv *= wet_v
+        Lu_p, Lv_p = Lu.copy(), Lv.copy()
+        if px:
+            Lu_p[:, -1] = Lu_p[:, 0]                                          # face nx is face 0
+        if py:
+            Lv_p[-1] = Lv_p[0]
+        q_e, q_w = ale.face_transport_thickness(hz, H, active, True)
+        qn, qs = ale.face_transport_thickness(hz.swapaxes(1, 2), H.T, active.T, True)
+        if px:
+            pe = np.concatenate([hz[..., -1:], hz], axis=-1)
+            pw = np.concatenate([hz, hz[..., :1]], axis=-1)
+            q_e[..., 0] = q_e[..., -1] = pe[..., 0] * wrapx
+            q_w[..., 0] = q_w[..., -1] = pw[..., -1] * wrapx
+        if py:
+            hzt = hz.swapaxes(1, 2)
+            pn = np.concatenate([hzt[..., -1:], hzt], axis=-1)
+            ps = np.concatenate([hzt, hzt[..., :1]], axis=-1)
+            qn[..., 0] = qn[..., -1] = pn[..., 0] * wrapy
+            qs[..., 0] = qs[..., -1] = ps[..., -1] * wrapy
+        qn, qs = np.ascontiguousarray(qn), np.ascontiguousarray(qs)
+        wu = face_fractions(0.5 * (q_e + q_w))
+        wv = face_fractions(0.5 * (qn + qs)).swapaxes(1, 2)
+        fs = NS(theta=0.6, active=active, Lu=Lu_p, Lv=Lv_p)
+        ob = None
+        fluxes = NS(wet_u=wet_u, wet_v=wet_v, Du=Du, Dv=Dv, fw=None)
+        rec_open = {}
+        if open_:
+            ob = OpenBoundary()
+            ob.open, ob.fs, ob.theta_bc = tuple(open_), fs, 0.5
+            # open face depths and Flather volume fluxes of the free surface on the edge faces
+            oDu, oDv = np.zeros((ny, nx + 1)), np.zeros((ny + 1, nx))
+            oQu, oQv = np.zeros((ny, nx + 1)), np.zeros((ny + 1, nx))
+            oDu[:, 0], oDu[:, -1] = Dc[:, 0] * active[:, 0], Dc[:, -1] * active[:, -1]
+            oDv[0], oDv[-1] = Dc[0] * active[0], Dc[-1] * active[-1]
+            oQu[:, [0, -1]] = rng.normal(0.0, 1.0, (ny, 2)) * 2e3 * (oDu[:, [0, -1]] > 0)
+            oQv[[0, -1]] = rng.normal(0.0, 1.0, (2, nx)) * 2e3 * (oDv[[0, -1]] > 0)
+            # interior-cell velocities on the open faces (the wet flag is False there)
+            for e in open_:
+                if e == "west":
+                    u_new[..., 0] = rng.normal(0.0, 0.1, (n, ny)) * active[:, 0]
+                    u_old[..., 0] = rng.normal(0.0, 0.1, (n, ny)) * active[:, 0]
+                elif e == "east":
+                    u_new[..., -1] = rng.normal(0.0, 0.1, (n, ny)) * active[:, -1]
+                    u_old[..., -1] = rng.normal(0.0, 0.1, (n, ny)) * active[:, -1]
+                elif e == "south":
+                    v_new[:, 0] = rng.normal(0.0, 0.1, (n, nx)) * active[0]
+                    v_old[:, 0] = rng.normal(0.0, 0.1, (n, nx)) * active[0]
+                else:
+                    v_new[:, -1] = rng.normal(0.0, 0.1, (n, nx)) * active[-1]
+                    v_old[:, -1] = rng.normal(0.0, 0.1, (n, nx)) * active[-1]
+            fluxes = NS(wet_u=wet_u, wet_v=wet_v, Du=Du, Dv=Dv, fw=None, open_Du=oDu, open_Dv=oDv, open_Qu=oQu,
+                        open_Qv=oQv)
+            rec_open = dict(open=np.array(open_, dtype=str), open_Du=oDu, open_Dv=oDv, open_Qu=oQu, open_Qv=oQv)
+        lt = ALELayerTransport(fs=fs, H=H, area=area, dt=dt, thickness_flux=flux, vi_geom={"dx_t": dx, "dy_t": dy},
+                               layer_volumes=lambda e, hh: hh * area[None], ob=ob)
+        if per:
+            lt.per = Periodic(per)
+        st = NS(h=hz, u=u_old, v=v_old, eta=eta)
+        lf = lt(st, eta_new, u_new, v_new, fluxes, 0.5, tuple(open_), wu, wv, q_e, q_w, qn, qs)
+        rec = dict(thickness_flux=flux, periodic=np.array(per, dtype=str), theta=0.6, theta_bc=0.5, dt=dt, H=H,
+                   area=area, active=active, Lu=Lu_p, Lv=Lv_p, dx_t=dx, dy_t=dy, h=hz, u=u_old, v=v_old, eta=eta,
+                   eta_new=eta_new, u_new=u_new, v_new=v_new, wet_u=wet_u, wet_v=wet_v, Du=Du, Dv=Dv, wu=wu,
+                   wv=wv, qe=q_e, qw=q_w, qn=qn, qs=qs, Qx=lf.Qx, Qy=lf.Qy, V0=lf.V0, V1=lf.V1, ok=lf.ok,
+                   h_dagger=lf.h_dagger, n_limited=lf.n_limited, **rec_open)
+        out[name] = rec
+        print(name, "limited", lf.n_limited)
+    return out
+
+
 def save(name, cases):
     flat = {}
     for case, rec in cases.items():
@@ -613,8 +734,10 @@ def save(name, cases):
 
 if __name__ == "__main__":
     threads.set_threads(1)
-    which = sys.argv[2:] or ["fct", "rk3", "kernels", "remap", "neighbours", "producers", "layer_transport"]
+    which = sys.argv[2:] or ["fct", "rk3", "kernels", "remap", "neighbours", "producers", "layer_transport",
+                             "layer_transport_ext"]
     makers = {"fct": fct_cases, "rk3": rk3_cases, "kernels": kernel_cases, "remap": remap_cases,
-              "neighbours": neighbour_cases, "producers": producer_cases, "layer_transport": layer_transport_cases}
+              "neighbours": neighbour_cases, "producers": producer_cases, "layer_transport": layer_transport_cases,
+              "layer_transport_ext": layer_transport_ext_cases}
     for name in which:
         save(name, makers[name]())

