@@ -7,8 +7,9 @@ PPM_H4 remap of both fields, on the 512 x 512 x 50 curvilinear basin (FP64, seed
 
 Metric: tracer cell-steps/s = nt * N * ny * nx * steps / time.  One "step" is one advect_fct + remap of the whole
 stack.  `value` is device-resident throughput (inputs already in HBM, CUDA events on the launching stream, max over
-ranks); `e2e` is the same step through the public drop-in API (TracerAdvection.advect_fct, remap_columns) with
-pinned host tensors, host<->device copies inside the timed region.  The stack (210 MB) and every geometry array
+ranks); `e2e` is the same step through the reference's two drop-in calls (TracerAdvection.advect_fct,
+remap_columns) with pinned host tensors, host<->device copies inside the timed region, and beside it (`one_call`)
+the repository's ``ale_tracer_step``, which keeps the advected stack on the device.  The stack (210 MB) and every geometry array
 (105 MB each) exceed the 126 MB L2, so no flush is needed between steps.
 
 Multi-GPU: the path does not shard (one domain per GPU, "replicas only"); under torchrun every rank runs its own
@@ -63,6 +64,8 @@ def parse():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="basin", choices=["basin", "zstar_box"])
+    ap.add_argument("--basin-size", type=int, nargs=3, default=[512, 512, 50], metavar=("NX", "NY", "NZ"),
+                    help="size of the basin workload (a smaller one for profiling captures)")
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="budget of the CPU-baseline sample")
     ap.add_argument("--ref-seconds", type=float, default=150.0,
@@ -78,9 +81,9 @@ def parse():
     return ap.parse_args()
 
 
-def make_workload(name: str):
+def make_workload(name: str, size=(512, 512, 50)):
     from pyocean_b200 import workloads as W
-    return W.basin() if name == "basin" else W.zstar_box()
+    return W.basin(nx=size[0], ny=size[1], n=size[2]) if name == "basin" else W.zstar_box()
 
 
 def workload_config(w, world: int) -> dict:
@@ -211,14 +214,14 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> dict | None:
 
     from pyocean_b200 import _lib
     from pyocean_b200.remap import remap_columns
-    from pyocean_b200.step import ALETracerStep
+    from pyocean_b200.step import ALETracerStep, ale_tracer_step
     from pyocean_b200.tracers import OpenEdges, TracerAdvection
     from pyocean_b200.periodic import Periodic
     from pyocean_b200 import workloads as W
 
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
-    w = make_workload(args.workload)
+    w = make_workload(args.workload, args.basin_size)
     nt, n, ny, nx = w.C.shape
     flags = (_lib.PERIODIC_X if "x" in w.periodic else 0) | (_lib.PERIODIC_Y if "y" in w.periodic else 0)
     g = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)                     # noqa: E731
@@ -295,27 +298,36 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> dict | None:
     hC, hV0, hV1, hQx, hQy, hok = pin(w.C), pin(w.V0), pin(w.V1), pin(w.Qx), pin(w.Qy), pin(w.ok)
     hhs, hht, hwet = pin(w.h_src), pin(w.h_tgt), pin(w.wet)
     h2d = sum(int(t.numel() * t.element_size()) for t in (hC, hV0, hV1, hQx, hQy, hok, hhs, hht, hwet))
-    h2d += int(hC.numel() * hC.element_size())            # the advected stack goes back in for the remap
-    d2h = 2 * int(hC.numel() * hC.element_size())
-    e2e_ms = float("nan")
-    if args.e2e_steps > 0:
-        # warm-up of the API path with the timed loop's own chaining: it fills the device and pinned-host caching
-        # allocators with every block the loop holds at once (a new 210 MB pinned block costs ~100 ms)
+    d2h = int(hC.numel() * hC.element_size())
+    stack = int(hC.numel() * hC.element_size())
+
+    def timed(step, n):
+        """Device time of n chained steps of `step` on the host arrays (after three untimed ones, which fill the
+        device and pinned-host caching allocators with every block the chain holds at once: a new 210 MB pinned
+        block costs ~100 ms)."""
         hc = hC
         for _ in range(3):
-            A = adv.advect_fct(hc, hV0, hV1, hQx, hQy, hok)
-            hc = remap_columns(hhs, A, hht, w.remap_scheme, hwet)
+            hc = step(hc)
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
         hc = hC
-        for _ in range(args.e2e_steps):
-            A = adv.advect_fct(hc, hV0, hV1, hQx, hQy, hok)
-            hc = remap_columns(hhs, A, hht, w.remap_scheme, hwet)
+        for _ in range(n):
+            hc = step(hc)
         e1.record(stream)
         torch.cuda.synchronize()
-        e2e_ms = e0.elapsed_time(e1) / args.e2e_steps
+        return e0.elapsed_time(e1) / n
+
+    e2e_ms = e2e_two_ms = float("nan")
+    if args.e2e_steps > 0:
+        # the step as one call (the advected stack stays on the device) ...
+        e2e_ms = timed(lambda c: ale_tracer_step(adv, c, hV0, hV1, hQx, hQy, hok, hhs, hht, w.remap_scheme, hwet),
+                       args.e2e_steps)
+        # ... and as the reference's two drop-in calls (the advected stack goes back to the host between them)
+        e2e_two_ms = timed(lambda c: remap_columns(hhs, adv.advect_fct(c, hV0, hV1, hQx, hQy, hok), hht,
+                                                   w.remap_scheme, hwet), args.e2e_steps)
     e2e_ms = max_over_ranks(e2e_ms, dev)
+    e2e_two_ms = max_over_ranks(e2e_two_ms, dev)
 
     cells = w.tracer_cells
     value = job_rate(cells * args.steps, world, ms)
@@ -364,9 +376,14 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> dict | None:
                                "remap_columns": {"ms": rem_avg, "GB/s": rem_gbs, "bytes": ab["remap"]},
                                "step": {"ms": ms / args.steps,
                                         "GB/s": ab["step"] / (ms / args.steps / 1e3) / 1e9}}},
-        "e2e": {"value": job_rate(cells, world, e2e_ms), "unit": "tracer cell-steps/s", "h2d_bytes_per_step": h2d,
-                "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms,
-                "api": "TracerAdvection.advect_fct + remap_columns on pinned host tensors"},
+        "e2e": {"value": job_rate(cells, world, e2e_two_ms), "unit": "tracer cell-steps/s",
+                "h2d_bytes_per_step": h2d + stack, "d2h_bytes_per_step": d2h + stack, "ms_per_step": e2e_two_ms,
+                "api": "TracerAdvection.advect_fct + remap_columns (the reference's two drop-in calls) on pinned "
+                       "host tensors",
+                "one_call": {"value": job_rate(cells, world, e2e_ms), "ms_per_step": e2e_ms,
+                             "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                             "api": "pyocean_b200.ale_tracer_step (advect_fct then remap_columns in one call, the "
+                                    "advected stack kept on the device) on pinned host tensors"}},
         "mixed": {"value": job_rate(cells * args.steps, world, mixed_ms), "ms_per_step": mixed_ms / args.steps,
                   "advect_fct_ms": mixed_adv, "speedup_vs_f64": ms / mixed_ms,
                   "what": "pocean_advect_fct_mixed (FP32 WENO5 weights and face values, FP64 fluxes, limiter and "
@@ -383,7 +400,7 @@ def main():
     if args.impl == "reference":
         if rank != 0:
             return
-        w = make_workload(args.workload)
+        w = make_workload(args.workload, args.basin_size)
         # the arm's own steps: K whole steps after min(W, 1) untimed ones, cut short after --ref-seconds so that
         # the run ends within a few minutes
         s = cpu_sample(w, args.ref_seconds, max_steps=args.steps, warmup=min(args.warmup, 1))
@@ -427,7 +444,7 @@ def main():
         torch.cuda.empty_cache()
     if rank == 0:
         if not args.no_cpu_baseline and world == 1:
-            s = cpu_sample(make_workload(args.workload), args.cpu_seconds)
+            s = cpu_sample(make_workload(args.workload, args.basin_size), args.cpu_seconds)
             line["cpu_baseline"] = {k: s[k] for k in ("value", "unit", "cores", "kind", "sample")}
         print(json.dumps(line))
     if world > 1:

@@ -41,6 +41,14 @@ extern "C" {
 #define POCEAN_PERIODIC_Y 0x20u
 #define POCEAN_WENO_JS 0x40u  /* WENO5-JS weights (tracer_scheme != "weno5"); default WENO5-Z */
 #define POCEAN_FCT_UNLIMITED 0x80u /* advect_fct only: no limiter, C_out = the SSP-RK3 result (tracers.py:289-291) */
+/* advect (pocean_advect_rk3_f64) only: the face schemes and the time stepping of the reference's NumPy RHS path
+ * (tracers.py:110-151, 303-330).  POCEAN_FACES_UP3: tracer_scheme "upwind3" (and any other non-WENO5 name),
+ * POCEAN_FACES_UP1: "upwind1" (_up3_faces, sigma_baroclinic.py:164-188); neither: the WENO5 faces.
+ * POCEAN_TIME_PC: tracer_time "pc", a centred half step (_centred_faces, sigma_baroclinic.py:632-652) and a full step
+ * from the start with the scheme's faces of the half-step tracer; fx_face is then the corrector's flux. */
+#define POCEAN_FACES_UP3 0x100u
+#define POCEAN_FACES_UP1 0x200u
+#define POCEAN_TIME_PC 0x400u
 
 /* Remap schemes (core/vertical/remap.py:40). */
 #define POCEAN_PCM 0
@@ -133,7 +141,9 @@ size_t pocean_advect_rk3_workspace_bytes(int nt, int nz, int ny, int nx);
  * One SSP-RK3 step without limiter, WENO5 faces in x, y and z (interface transports Fz (nz+1, ny, nx), or NULL
  * for none).  Replaces TracerAdvection.advect (core/components/tracers.py:342-375) with _advect_div and _rk_stage
  * (core/dynamics/sigma_baroclinic.py:324-364, 856-875).  fx_face: (nt, nz, ny) SSP-RK3 combination
- * (F(c0) + F(c1))/6 + 2F(c2)/3 of the x-face fluxes through column face_i, or NULL.
+ * (F(c0) + F(c1))/6 + 2F(c2)/3 of the x-face fluxes through column face_i, or NULL.  With POCEAN_FACES_UP3 /
+ * POCEAN_FACES_UP1 the faces of the reference's NumPy RHS (tracers.py:139-151), with POCEAN_TIME_PC the 'pc'
+ * predictor-corrector step (tracers.py:324-330).
  */
 int pocean_advect_rk3_f64(const double* C, const double* V0, const double* V1, const double* Qx,
                           const double* Qy, const double* Fz, const uint8_t* ok, const double* inflow, int nt,
@@ -180,7 +190,7 @@ int pocean_regrid_remap_f64(int rule, const double* H, const double* eta, const 
  * towards sigma (dsigma, nz, bed first) and fully sigma below d_sigma or where H <= 0.  Then the nfields stacked
  * fields are remapped onto h_new as pocean_regrid_remap_f64 does.  bad_columns (device int, may be NULL) counts the
  * wet columns with a non-finite density, or with H <= 0 when d_hybrid <= 0, for which the reference raises
- * ValueError.  nz <= 256.  The reference's finer-source initial regrid (n_out != nz) is not provided.
+ * ValueError.  nz <= 256.  (A target layer count other than the source's: pocean_regrid_columns_f64.)
  */
 int pocean_regrid_hybrid_remap_f64(const double* H, const double* eta, const double* h_src, const uint8_t* active,
                                    const double* rho, const double* rho_target, const double* dz_top,
@@ -279,6 +289,18 @@ int pocean_flux_divergence_f64(const double* Qx, const double* Qy, int nz, int n
  * ok = active & (V > 0) (layer_transport.py:149). */
 int pocean_layer_volumes_f64(const double* h, const double* area, const uint8_t* active, int nz, int ny, int nx,
                              double* V, uint8_t* ok, void* stream);
+
+/* core/vertical/regrid.py:309-395 regrid_columns itself: target interface heights zw (m+1, ny, nx), bed first, of
+ * every column that wet marks (NaN elsewhere) for rule code 0 (z*, dz_top m surface first), 1 (sigma, dsigma m bed
+ * first) or 2 (hybrid: the n source layers h and densities rho (n, ny, nx) bed first, rho_target m+1 surface
+ * first, dz_top and max_h_top m, with d_hybrid > 0 the shallow sigma window on dsigma; keep the isopycnal test,
+ * applied only when m == n).  m != n only for the hybrid rule (regrid_columns' n_out: a finer or coarser source,
+ * such as the data levels of an initial state).  H is read as numpy.nan_to_num(H).  n, m <= 256.  The reference's
+ * argument checks (finite H and D > 0 in wet columns, ...) are the caller's. */
+int pocean_regrid_columns_f64(int code, const double* H, const double* eta, const double* h, const double* rho,
+                              const uint8_t* wet, const double* dz_top, const double* dsigma, const double* rho_target,
+                              const double* max_h_top, double d_sigma, double d_hybrid, double h_min, int keep, int n,
+                              int m, int ny, int nx, double* zw, void* stream);
 
 /* Periodic halo of a producer's inputs (core/model/periodic.py:72-94 Periodic.pad / crop; used for the PPM layer
  * flux on periodic axes, core/components/layer_transport.py:121-128).  src (nlead, ny + face_y, nx + face_x) of ny x nx

@@ -10,8 +10,10 @@ order, no FMA contraction), loaded through ctypes.  This module restates the Pyt
 kernels with the reference's call signatures:
 
 * ``TracerAdvection`` — ``core/components/tracers.py:50-375`` (``advect_fct`` :208-254, the unlimited NumPy path
-  :256-301, ``advect`` :342-375, ``faces_h`` :166-176, ``upwind_faces_h`` :178-193, periodic pad/crop :80-102,
-  ``_open_inflow`` :65-78).
+  :256-301, ``advect`` :342-375 with the ``'pc'`` branch of ``advect_numpy`` :324-330, ``faces_h`` :166-176,
+  ``upwind_faces_h`` :178-193, the NumPy RHS with its face rules :110-151, ``flux_x`` :195-206, periodic pad/crop
+  :80-102, ``_open_inflow`` :65-78); the upwind-3/1 and centred face values of the NumPy path
+  (``sigma_baroclinic.py:164-199, 632-652``) are restated here in NumPy.
 * ``Periodic`` — ``core/model/periodic.py:31, 47-94`` (pad/crop with ``TRACER_HALO`` wrapped cells).
 * ``remap_column`` / ``remap_columns`` / ``reconstruct`` — ``core/vertical/remap.py:234-427``.
 * ``regrid`` / ``regrid_remap`` — the z* and sigma rules of ``core/vertical/regrid.py:44-98, 309-395`` as
@@ -70,6 +72,8 @@ def lib() -> ctypes.CDLL:
         L.oracle_regrid.restype = i
         L.oracle_regrid_hybrid.argtypes = [_D, _D, _D, _U8, _D, _D, _D, _D, _D, d, d, d, i, i, i, i, _D, _U8]
         L.oracle_regrid_hybrid.restype = i
+        L.oracle_regrid_columns.argtypes = [i, _D, _D, _D, _D, _D, _D, _D, _D, d, d, d, i, _U8, i, i, i, i, _D]
+        L.oracle_regrid_columns.restype = None
         L.oracle_diffuse_ale.argtypes = [_D, _D, _D, _U8, _D, _D, _U8, _U8, _D, d, d, i, i, i, _D]
         L.oracle_face_fractions.argtypes = [_D, i, i, i, _D]
         L.oracle_ftt.argtypes = [_D, _D, _U8, i, i, i, i, _D, _D]
@@ -192,6 +196,66 @@ def advect_div(c, Qx, Qy, Fz, ok, ext, open_w, open_e, open_s, open_n, z_variant
     return out
 
 
+def _cell_at(c, ok, s):
+    """Values and validity of cells m + s along the last axis, m = 0 .. n-1 (0 and invalid out of range), as the
+    reference's ``_shift`` (``sigma_baroclinic.py:191-199``)."""
+    n = c.shape[-1]
+    val = np.zeros_like(c)
+    valid = np.zeros(ok.shape, bool)
+    a, b = max(0, -s), min(n, n - s)
+    if a < b:
+        val[..., a:b] = c[..., a + s:b + s]
+        valid[..., a:b] = ok[..., a + s:b + s]
+    return val, valid
+
+
+def up3_faces(c, flux, ok, axis, order=3):
+    """``sigma_baroclinic.py:164-188``: face values on the interior faces f = 1 .. n-1 along ``axis`` (between cells
+    f-1 and f), upwind with respect to ``flux``: third order (-c[f-2] + 5 c[f-1] + 2 c[f]) / 6 for flux >= 0 and
+    (2 c[f-1] + 5 c[f] - c[f+1]) / 6 otherwise where the three stencil cells are ok, the upwind cell elsewhere
+    (everywhere for ``order`` 1); the two boundary faces 0."""
+    c = np.moveaxis(c, axis, -1)
+    ok = np.moveaxis(ok, axis, -1)
+    f = np.moveaxis(flux, axis, -1)
+    n = c.shape[-1]
+    cm2, km2 = _cell_at(c, ok, -2)
+    cm1, km1 = _cell_at(c, ok, -1)
+    k0 = ok
+    cp1, kp1 = _cell_at(c, ok, 1)
+    # indexed at cell m = f: lo = cell f-1, hi = cell f
+    lo, hi = cm1, c
+    if order == 1:
+        pos, neg = lo, hi
+    else:
+        pos = np.where(km2 & km1 & k0, (-cm2 + 5.0 * lo + 2.0 * hi) / 6.0, lo)
+        neg = np.where(km1 & k0 & kp1, (2.0 * lo + 5.0 * hi - cp1) / 6.0, hi)
+    face = np.zeros(f.shape)
+    face[..., 1:n] = np.where(f[..., 1:n] >= 0, pos[..., 1:n], neg[..., 1:n])
+    return np.moveaxis(face, -1, axis)
+
+
+def centred_faces(c, ok, axis, n_out=None):
+    """``sigma_baroclinic.py:632-652``: centred face values on the interior faces along ``axis``, sixth order
+    (37 (c[f-1] + c[f]) - 8 (c[f-2] + c[f+1]) + (c[f-3] + c[f+2])) / 60 where all six cells are ok, fourth order
+    (7 (c[f-1] + c[f]) - (c[f-2] + c[f+1])) / 12 where the inner four are, the mean of the two neighbours
+    elsewhere; ``n_out`` faces (default n + 1), 0 outside 1 .. n-1."""
+    c = np.moveaxis(c, axis, -1)
+    ok = np.moveaxis(ok, axis, -1)
+    n = c.shape[-1]
+    cell = {s: _cell_at(c, ok, s) for s in range(-3, 3)}
+    near = cell[-1][0] + cell[0][0]
+    mid = cell[-2][0] + cell[1][0]
+    far = cell[-3][0] + cell[2][0]
+    f6 = (37 * near - 8 * mid + far) / 60
+    f4 = (7 * near - mid) / 12
+    f2 = 0.5 * near
+    m6 = cell[-3][1] & cell[-2][1] & cell[-1][1] & cell[0][1] & cell[1][1] & cell[2][1]
+    m4 = cell[-2][1] & cell[-1][1] & cell[0][1] & cell[1][1]
+    face = np.zeros(c.shape[:-1] + (n + 1 if n_out is None else n_out,))
+    face[..., 1:n] = np.where(m6, f6, np.where(m4, f4, f2))[..., 1:n]
+    return np.moveaxis(face, -1, axis)
+
+
 def fct_coefficients(c0, cL, V1, Ax, Ay, ok, dt):
     """``sigma_baroclinic.py:407-449`` (``_fct_coeff_kernel``): Zalesak coefficients (Cx, Cy)."""
     c0, cL, V1, Ax, Ay = _f64(c0), _f64(cL), _f64(V1), _f64(Ax), _f64(Ay)
@@ -281,10 +345,59 @@ class TracerAdvection:
             fy[..., -1, :] = Qy[None, :, -1, :] * np.where(Qy[None, :, -1, :] < 0, ext[..., -1, :], c[..., -1, :])
         return fx, fy
 
-    # tracers.py:153-164 (WENO5 schemes only: the fused compiled kernel)
+    # tracers.py:110-115: the face values of the NumPy path (centred, or the upwind-3/1 schemes)
+    def faces(self, c, flux, ok, axis, centred=False):
+        if centred:
+            return centred_faces(c, ok, axis, n_out=flux.shape[axis])
+        if self.tracer_scheme.startswith("weno5"):
+            raise NotImplementedError("oracle: WENO5 faces are restated through the fused kernels only")
+        return up3_faces(c, flux, ok, axis, order=1 if self.tracer_scheme == "upwind1" else 3)
+
+    # tracers.py:117-137: upstream values on the open-edge faces (the exterior on inflow)
+    def open_faces(self, face, c, Q, axis, inflow=None):
+        if not self.ob.open:
+            return face
+        ext = c if inflow is None else inflow
+        face = np.array(face, copy=True)
+        lo, hi = ("west", "east") if axis == 3 else ("south", "north")
+        for edge, f_i, sgn in ((lo, 0, 1.0), (hi, -1, -1.0)):
+            if edge not in self.ob.open:
+                continue
+            q = np.take(Q, f_i, axis=axis - 1)
+            cf = np.take(c, f_i, axis=axis)
+            ef = np.take(ext, f_i, axis=axis)
+            idx = [slice(None)] * face.ndim
+            idx[axis] = f_i
+            face[tuple(idx)] = np.where(sgn * q > 0, ef, cf)
+        return face
+
+    # tracers.py:139-151: -div(Q c) with the NumPy faces (x, y, then z differences, the reference's order)
+    def rhs_numpy(self, c, Qx, Qy, Fz, ok, centred=False, inflow=None):
+        c = _f64(c)
+        Qx, Qy, Fz = _f64(Qx), _f64(Qy), _f64(Fz)
+        okb = np.broadcast_to(np.asarray(ok, bool), c.shape)
+        fx = Qx * self.open_faces(self.faces(c, np.broadcast_to(Qx, c.shape[:1] + Qx.shape), okb, 3, centred),
+                                  c, Qx, 3, inflow)
+        fy = Qy * self.open_faces(self.faces(c, np.broadcast_to(Qy, c.shape[:1] + Qy.shape), okb, 2, centred),
+                                  c, Qy, 2, inflow)
+        fz = np.zeros(c.shape[:1] + Fz.shape)
+        fz[:, :-1] = Fz[:-1] * self.faces(c, np.broadcast_to(Fz[:-1], c.shape), okb, 1, centred)
+        return -(fx[..., 1:] - fx[..., :-1] + fy[:, :, 1:, :] - fy[:, :, :-1, :] + fz[:, 1:] - fz[:, :-1])
+
+    # tracers.py:195-206: the x-face fluxes that ``rhs`` differences
+    def flux_x(self, c, Qx, Qy, ok, centred=False, inflow=None):
+        if not centred and self.tracer_scheme.startswith("weno5"):
+            return self.faces_h(c, Qx, Qy, np.broadcast_to(ok, np.shape(c)[1:]), inflow=inflow)[0]
+        c = _f64(c)
+        Qx = _f64(Qx)
+        okb = np.broadcast_to(np.asarray(ok, bool), c.shape)
+        return Qx * self.open_faces(self.faces(c, np.broadcast_to(Qx, c.shape[:1] + Qx.shape), okb, 3, centred),
+                                    c, Qx, 3, inflow)
+
+    # tracers.py:153-164: the fused compiled kernel for WENO5 upwind faces, else the NumPy path
     def rhs(self, c, Qx, Qy, Fz, ok, centred=False, inflow=None):
         if centred or not self.tracer_scheme.startswith("weno5"):
-            raise NotImplementedError("oracle: only the WENO5 upwind RHS (the compiled path) is restated")
+            return self.rhs_numpy(c, Qx, Qy, Fz, ok, centred, inflow)
         c = _f64(c)
         ext = c if inflow is None else inflow
         return advect_div(c, Qx, Qy, Fz, ok, ext, *self._open_flags(), self.tracer_scheme == "weno5",
@@ -350,12 +463,28 @@ class TracerAdvection:
         i = flux_face_i
         return out if i is None else (out, FHx[..., i])
 
-    # tracers.py:342-375 (SSP-RK3 with the fused WENO5 RHS)
+    # tracers.py:324-330: the 'pc' branch of advect_numpy (centred predictor to the half step, corrector from the
+    # step's start with the upwind faces of the half-step tracer)
+    def _advect_pc(self, C, V0, V1, Qx, Qy, Fz, ok, inflow, flux_face_i):
+        dt = self.dt
+        C = _f64(C)
+        V0, V1 = np.asarray(V0, float), np.asarray(V1, float)
+        dV = V1 - V0
+        safe = lambda q, v: np.where(v > 0, q / np.where(v > 0, v, 1.0), C)     # noqa: E731
+        q0 = V0 * C
+        Vh = V0 + 0.5 * dV
+        ch = safe(q0 + 0.5 * dt * self.rhs(C, Qx, Qy, Fz, ok, centred=True, inflow=inflow), Vh)
+        out = safe(q0 + dt * self.rhs(ch, Qx, Qy, Fz, ok, inflow=inflow), V1)
+        if flux_face_i is None:
+            return out
+        return out, self.flux_x(ch, Qx, Qy, ok, inflow=inflow)[..., flux_face_i]
+
+    # tracers.py:342-375 (SSP-RK3; the fused WENO5 RHS or the NumPy one), 'pc' as advect_numpy
     def advect(self, C, V0, V1, Qx, Qy, Fz, ok, inflow=None, flux_face_i=None):
         if self.per:
             return self._periodic(self.advect, C, V0, V1, Qx, Qy, Fz, ok, inflow, flux_face_i)
-        if self.tracer_time != "ssprk3":
-            raise NotImplementedError("oracle: only the SSP-RK3 time stepping is restated")
+        if self.tracer_time == "pc":
+            return self._advect_pc(C, V0, V1, Qx, Qy, Fz, ok, inflow, flux_face_i)
         dt = self.dt
         C = _f64(C)
         if np.shape(V0) != C.shape[1:] or np.shape(V1) != C.shape[1:]:
@@ -369,7 +498,7 @@ class TracerAdvection:
         _, c3 = _rk_stage(q0, q2, self.rhs(c2, Qx, Qy, Fz, ok, inflow=inflow), dt, V1, C, 3)
         if flux_face_i is None:
             return c3
-        fx = lambda c: self.faces_h(c, Qx, Qy, ok, inflow=inflow)[0][..., flux_face_i]       # noqa: E731
+        fx = lambda c: self.flux_x(c, Qx, Qy, ok, inflow=inflow)[..., flux_face_i]            # noqa: E731
         return c3, (fx(C) + fx(c1)) / 6.0 + 2.0 * fx(c2) / 3.0
 
 
@@ -439,6 +568,49 @@ def regrid_hybrid(H, eta, h_src, active, rho, params: dict):
                                      float(params.get("h_min", H_MIN)), int(bool(params.get("keep_isopycnal", True))),
                                      n, ny, nx, _p(h_new), _pu8(wet))
     return h_new, wet.view(bool), int(bad)
+
+
+def regrid_columns(rule: str, H, eta, h, rho, params: dict, wet, n_out=None):
+    """``regrid_columns`` (core/vertical/regrid.py:345-395): target interface heights zw (N+1, ny, nx), bed first,
+    N = n_out (default the source layer count; only the hybrid rule regrids a source of another count), NaN in the
+    columns that are not wet; ValueError where the reference raises."""
+    if rule not in ("zstar", "sigma", "hybrid"):
+        raise ValueError(f"unknown rule {rule!r}; use 'zstar', 'sigma' or 'hybrid'")
+    required = {"zstar": ("dz_top",), "sigma": ("dsigma",), "hybrid": ("dz_top", "rho_target")}[rule]
+    if rule == "hybrid" and float(params.get("d_hybrid", 0.0)) > 0.0:
+        required += ("dsigma",)
+    for key in required:
+        if key not in params:
+            raise ValueError(f"regrid_columns({rule!r}) needs params[{key!r}]")
+    if rule == "hybrid" and rho is None:
+        raise ValueError("regrid_columns('hybrid') needs the layer densities rho")
+    wet = np.asarray(wet, np.bool_)
+    H = np.asarray(H, float)
+    eta = np.asarray(eta, float)
+    Hw, Dw = H[wet], (H + eta)[wet]
+    if not (np.isfinite(Hw).all() and np.isfinite(Dw).all() and (Dw > 0).all()):
+        raise ValueError("wet columns need finite H and D = H + eta > 0")
+    if rule == "zstar" and not (Hw > 0).all():
+        raise ValueError("z* needs H > 0 in every wet column")
+    if rule == "hybrid" and float(params.get("d_hybrid", 0.0)) <= 0 and (Hw <= 0).any():
+        raise ValueError("hybrid needs H > 0 unless it has a shallow sigma zone (d_hybrid > 0)")
+    if rule == "hybrid" and not np.isfinite(np.asarray(rho, float)[:, wet]).all():
+        raise ValueError("non-finite density in a wet column")
+    h = _f64(h)
+    n_src, ny, nx = h.shape
+    m = n_src if n_out is None else int(n_out)
+    if m != n_src and rule != "hybrid":
+        raise ValueError("n_out != the source layer count is only for rule 'hybrid'")
+    f = lambda key, default: _f64(params.get(key, default))                        # noqa: E731
+    zw = np.full((m + 1, ny, nx), np.nan)
+    lib().oracle_regrid_columns({"zstar": 0, "sigma": 1, "hybrid": 2}[rule], _p(_f64(np.nan_to_num(H))),
+                                _p(_f64(eta)), _p(h), _p(h if rho is None else _f64(rho)),
+                                _p(f("dz_top", np.ones(m))), _p(f("dsigma", np.full(m, 1.0 / m))),
+                                _p(f("rho_target", np.zeros(m + 1))), _p(f("max_h_top", np.full(m, np.inf))),
+                                float(params.get("d_sigma", 0.0)), float(params.get("d_hybrid", 0.0)),
+                                float(params.get("h_min", H_MIN)), int(bool(params.get("keep_isopycnal", True))),
+                                _pu8(_u8(wet)), n_src, m, ny, nx, _p(zw))
+    return zw
 
 
 def regrid_remap(rule: str, H, eta, h_src, active, fields, coord, scheme: int, h_min: float = H_MIN):

@@ -908,13 +908,13 @@ static void keep_consistent(const double* h, const double* rho, int n, const dou
     }
 }
 
-/* regrid.py:204-252 `hycom1_column` with n == m (target grid = source layer count); zw bed first (n+1).
- * work: >= 8n+8 doubles, bwork >= 2n+2 bytes. */
+/* regrid.py:204-252 `hycom1_column`: n source layers (h_bed, rho_bed), m target layers (rho_target m+1, dz_top and
+ * max_h_top m, zw bed first m+1); the isopycnal test (keep) only when n == m.  work: >= 6n + m + 8 doubles, bwork
+ * >= 2n+2 bytes. */
 static void hycom1_column(double H, double eta, const double* h_bed, const double* rho_bed, const double* rho_target,
-                          const double* dz_top, const double* max_h_top, double h_min, int keep, int n, double* zw,
-                          double* work, uint8_t* bwork)
+                          const double* dz_top, const double* max_h_top, double h_min, int keep, int n, int m,
+                          double* zw, double* work, uint8_t* bwork)
 {
-    const int m = n;
     const double D = H + eta;
     double* h_top = work;
     double* rho_own = h_top + n;
@@ -941,7 +941,7 @@ static void hycom1_column(double H, double eta, const double* h_bed, const doubl
         for (int kk = 0; kk < k0; ++kk) rho[kk] = rho[k0];
     for (int k = n - 2; k >= 0; --k) rho[k] = pmin(rho[k], rho[k + 1]);
     p1m_h2_positions(h_top, rho, n, rho_target, m, x, e, xg);
-    if (keep) keep_consistent(h_top, rho_own, n, rho_target, 2.0 * h_min, x, xg, bwork, bwork + n + 1);
+    if (keep && n == m) keep_consistent(h_top, rho_own, n, rho_target, 2.0 * h_min, x, xg, bwork, bwork + n + 1);
     const double s = D / H;
     double nominal = 0.0;
     for (int k = 1; k <= m; ++k) {
@@ -1029,7 +1029,7 @@ int oracle_regrid_hybrid(const double* Hin, const double* eta, const double* h_s
         if (qq <= 0.0) {
             sigma_column(H, eta[c], dsigma, n, h_min, col);
         } else {
-            hycom1_column(H, eta[c], hb, rb, rho_target, dz_top, max_h_top, h_min, keep, n, col, work, bwork);
+            hycom1_column(H, eta[c], hb, rb, rho_target, dz_top, max_h_top, h_min, keep, n, n, col, work, bwork);
             if (qq < 1.0) {
                 sigma_column(H, eta[c], dsigma, n, h_min, sig);
                 zstar_column(H, eta[c], dz_top, n, h_min, work, zs);
@@ -1042,6 +1042,61 @@ int oracle_regrid_hybrid(const double* Hin, const double* eta, const double* h_s
         free(bwork);
     }
     return bad;
+}
+
+/*
+ * regrid.py:309-342 `_regrid_columns`: target interface heights zw (m+1, ny, nx), bed first, of every column wet[c]
+ * (the others are left as they are; the caller fills NaN).  code 0 z*, 1 sigma, 2 hybrid; h, rho (n, ny, nx) bed
+ * first (n = m unless hybrid); dz_top, max_h_top (m) surface first; dsigma (m) bed first; rho_target (m+1) surface
+ * first; H already numpy.nan_to_num'ed by the caller, as the reference passes it.
+ */
+void oracle_regrid_columns(int code, const double* H, const double* eta, const double* h, const double* rho,
+                           const double* dz_top, const double* dsigma, const double* rho_target,
+                           const double* max_h_top, double d_sigma, double d_hybrid, double h_min, int keep,
+                           const uint8_t* wet, int n, int m, int ny, int nx, double* zw)
+{
+    const i64 plane = (i64)ny * nx;
+    const int nn = n > m ? n : m;
+#pragma omp parallel for
+    for (i64 c = 0; c < plane; ++c) {
+        if (!wet[c]) continue;
+        double* buf = (double*)malloc((size_t)(14 * nn + 32) * sizeof(double));
+        uint8_t* bwork = (uint8_t*)malloc((size_t)(2 * n + 4));
+        double* hb = buf;                      /* n */
+        double* rb = hb + nn;                  /* n */
+        double* col = rb + nn;                 /* m+1 */
+        double* sig = col + nn + 1;            /* m+1 */
+        double* zs = sig + nn + 1;             /* m+1 */
+        double* hyb = zs + nn + 1;             /* m+1 */
+        double* work = hyb + nn + 1;           /* 6n + m + 8 */
+        const double Hc = H[c], ec = eta[c];
+        if (code == 0) {
+            zstar_column(Hc, ec, dz_top, m, h_min, work, col);
+        } else if (code == 1) {
+            sigma_column(Hc, ec, dsigma, m, h_min, col);
+        } else {
+            for (int k = 0; k < n; ++k) {
+                hb[k] = h[k * plane + c];
+                rb[k] = rho[k * plane + c];
+            }
+            double q = d_hybrid > 0.0 ? transition_weight(Hc + ec, d_sigma, d_hybrid) : 1.0;
+            if (d_hybrid > 0.0 && Hc <= 0.0) q = 0.0;
+            if (q <= 0.0) {
+                sigma_column(Hc, ec, dsigma, m, h_min, col);
+            } else {
+                hycom1_column(Hc, ec, hb, rb, rho_target, dz_top, max_h_top, h_min, keep, n, m, col, work, bwork);
+                if (q < 1.0) {
+                    sigma_column(Hc, ec, dsigma, m, h_min, sig);
+                    zstar_column(Hc, ec, dz_top, m, h_min, work, zs);
+                    for (int j = 0; j <= m; ++j) hyb[j] = col[j];
+                    window_shallow_sigma(hyb, sig, zs, Hc, Hc + ec, d_sigma, d_hybrid, h_min, m, col);
+                }
+            }
+        }
+        for (int k = 0; k <= m; ++k) zw[k * plane + c] = col[k];
+        free(buf);
+        free(bwork);
+    }
 }
 
 /* sigma_baroclinic.py:533-561 `_diffuse_ale_kernel` on one field (n, ny, nx); faces (ny, nx+1) / (ny+1, nx). */

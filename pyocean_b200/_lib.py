@@ -16,6 +16,9 @@ OPEN_W, OPEN_E, OPEN_S, OPEN_N = 0x1, 0x2, 0x4, 0x8
 PERIODIC_X, PERIODIC_Y = 0x10, 0x20
 WENO_JS = 0x40
 FCT_UNLIMITED = 0x80
+FACES_UP3 = 0x100
+FACES_UP1 = 0x200
+TIME_PC = 0x400
 PCM, PLM, PPM_H4 = 0, 1, 2
 REGRID_ZSTAR, REGRID_SIGMA = 0, 1
 ERRORS = {1: "invalid argument", 2: "workspace", 3: "CUDA error", 4: "unsupported device", 5: "step cannot proceed"}
@@ -59,6 +62,8 @@ SIGNATURES: dict[str, tuple] = {
     "pocean_freshwater_volumes_f64": (_I, [_P, _P, _P, _D, _I, _I, _I, _P, _P, _P]),
     "pocean_flux_divergence_f64": (_I, [_P, _P, _I, _I, _I, _P, _P]),
     "pocean_layer_volumes_f64": (_I, [_P, _P, _P, _I, _I, _I, _P, _P, _P]),
+    "pocean_regrid_columns_f64": (_I, [_I, _P, _P, _P, _P, _P, _P, _P, _P, _P, _D, _D, _D, _I, _I, _I, _I, _I, _P,
+                                       _P]),
     "pocean_periodic_pad_f64": (_I, [_P, _I, _I, _I, _I, _I, _I, _I, _I, _P, _P]),
     "pocean_periodic_pad_u8": (_I, [_P, _I, _I, _I, _I, _I, _I, _I, _I, _P, _P]),
     "pocean_periodic_crop_f64": (_I, [_P, _I, _I, _I, _I, _I, _I, _I, _I, _P, _P]),

@@ -390,19 +390,115 @@ __device__ __forceinline__ double zface_flux(const StepArgs& a, const Shape& s, 
     return q * weno5_value(w[0], w[1], w[2], w[3], w[4], v[0], v[1], v[2], v[3], v[4], fl.z);
 }
 
+// Face values of the reference's NumPy RHS (tracers.py:110-151), used by `advect` for the upwind-3 / upwind-1
+// schemes and by the centred predictor of the 'pc' time stepping: FS_UP3 and FS_UP1 (_up3_faces,
+// sigma_baroclinic.py:164-188), FS_CEN (_centred_faces, :632-652); FS_WENO is the fused WENO5 path above.  The
+// NumPy path multiplies every face value by its transport (no skip where Q = 0) and gives the closed boundary faces
+// the value 0, so the fluxes here are Q * value there too.
+enum FaceScheme { FS_WENO = 0, FS_UP3 = 1, FS_UP1 = 2, FS_CEN = 3 };
+
+// Cells f-3 .. f+2 around face f of a line of n cells (stride `st`), with validity `in range and ok`; out of range
+// 0 and invalid (the reference's _shift), periodic lines wrap.
+__device__ __forceinline__ void line6(const double* __restrict__ c, const uint8_t* __restrict__ ok, int st, int n,
+                                      bool per, int f, double* w, bool* v)
+{
+    if (f >= 3 && f + 2 < n) {
+#pragma unroll
+        for (int m = 0; m < 6; ++m) {
+            w[m] = __ldg(c + (f - 3 + m) * st);
+            v[m] = __ldg(ok + (f - 3 + m) * st) != 0;
+        }
+        return;
+    }
+#pragma unroll
+    for (int m = 0; m < 6; ++m) {
+        int g = f - 3 + m;
+        bool in = true;
+        if (per) g = wrap(g, n); else in = g >= 0 && g < n;
+        w[m] = in ? __ldg(c + g * st) : 0.0;
+        v[m] = in && __ldg(ok + (in ? g : 0) * st) != 0;
+    }
+}
+
+// The value on face f from its six cells w[0..5] = c[f-3 .. f+2] (the same expressions, in the same order, as the
+// NumPy functions named above; the divisions are IEEE divisions, as NumPy's).
+template <int FS>
+__device__ __forceinline__ double lin_face_value(const double* w, const bool* v, double q)
+{
+    const double lo = w[2], hi = w[3];
+    if (FS == FS_UP1) return q >= 0.0 ? lo : hi;
+    if (FS == FS_UP3) {
+        if (q >= 0.0) return (v[1] && v[2] && v[3]) ? (-w[1] + 5.0 * lo + 2.0 * hi) / 6.0 : lo;
+        return (v[2] && v[3] && v[4]) ? (2.0 * lo + 5.0 * hi - w[4]) / 6.0 : hi;
+    }
+    const double near = lo + hi, mid = w[1] + w[4];
+    if (v[0] && v[1] && v[2] && v[3] && v[4] && v[5]) return (37.0 * near - 8.0 * mid + (w[0] + w[5])) / 60.0;
+    if (v[1] && v[2] && v[3] && v[4]) return (7.0 * near - mid) / 12.0;
+    return 0.5 * near;
+}
+
+// x-face flux of the NumPy path through face f of row j (open edges: upstream, the exterior on inflow).
+template <int FS>
+__device__ __forceinline__ double x_face_lin(const FacePlane& P, const Shape& s, const Flags& fl, int j, int f)
+{
+    const int row = j * s.nx;
+    const double q = __ldg(P.qx + j * (s.nx + 1) + ((fl.per_x && f == s.nx) ? 0 : f));
+    if (fl.per_x || (f >= 1 && f <= s.nx - 1)) {
+        double w[6];
+        bool v[6];
+        line6(P.c + row, P.ok + row, 1, s.nx, fl.per_x, f, w, v);
+        return q * lin_face_value<FS>(w, v, q);
+    }
+    if (f == 0) return q * (fl.open_w ? (q > 0.0 ? P.e[row] : P.c[row]) : 0.0);
+    return q * (fl.open_e ? (q < 0.0 ? P.e[row + s.nx - 1] : P.c[row + s.nx - 1]) : 0.0);
+}
+
+template <int FS>
+__device__ __forceinline__ double y_face_lin(const FacePlane& P, const Shape& s, const Flags& fl, int f, int i)
+{
+    const double q = __ldg(P.qy + ((fl.per_y && f == s.ny) ? 0 : f) * s.nx + i);
+    if (fl.per_y || (f >= 1 && f <= s.ny - 1)) {
+        double w[6];
+        bool v[6];
+        line6(P.c + i, P.ok + i, s.nx, s.ny, fl.per_y, f, w, v);
+        return q * lin_face_value<FS>(w, v, q);
+    }
+    const int o = (s.ny - 1) * s.nx + i;
+    if (f == 0) return q * (fl.open_s ? (q > 0.0 ? P.e[i] : P.c[i]) : 0.0);
+    return q * (fl.open_n ? (q < 0.0 ? P.e[o] : P.c[o]) : 0.0);
+}
+
+// z-face flux of the NumPy path through interface kf of column (j, i): Fz[kf] * value on kf = 1 .. n-1, Fz[0] * 0
+// on the bed, 0 on the surface (tracers.py:148-150).
+template <int FS>
+__device__ __forceinline__ double zface_lin(const StepArgs& a, const Shape& s, const double* cin, int t, int kf,
+                                            int j, int i)
+{
+    if (a.Fz == nullptr || kf > s.n - 1) return 0.0;
+    const int pl = s.ny * s.nx, ij = j * s.nx + i;
+    const double q = a.Fz[kf * pl + ij];
+    if (kf == 0) return q * 0.0;
+    double w[6];
+    bool v[6];
+    line6(cin + plane_at(t, s.n * pl) + ij, a.ok + ij, pl, s.n, false, kf, w, v);
+    return q * lin_face_value<FS>(w, v, q);
+}
+
 // The step as face and cell passes (the FCT stages' design): the face pass of stage s has one thread per cell
 // compute the west x-face, the south y-face and the bottom z-face of its cell (the last column / row also the
 // east / north domain face) into Sx, Sy and the z-face stack; the cell pass forms -div F from the stored faces
 // (x, y, then z, the reference's order), updates the stage and keeps the TEF column.  Each face is computed once.
 // A single kernel per stage on shared-memory tiles, which computed every z-face twice (once for each of its two
 // cells), took 6.68 ms at 512 x 512 x 50 with a vertical transport; these passes take 3.86 ms, bit-identical.
+// Stages 1-3: SSP-RK3 (input C, c1, c2); 4: the 'pc' predictor (input C, centred faces, half step to c1); 5: the
+// 'pc' corrector (input c1, the scheme's faces, full step from C).
 template <int STAGE>
 __device__ __forceinline__ const double* rk3_stage_field(const StepArgs& a)
 {
-    return STAGE == 1 ? a.C : (STAGE == 2 ? a.c1 : a.c2);
+    return (STAGE == 1 || STAGE == 4) ? a.C : ((STAGE == 2 || STAGE == 5) ? a.c1 : a.c2);
 }
 
-template <int STAGE, bool ZV>
+template <int STAGE, bool ZV, int FS>
 __device__ __forceinline__ void rk3_faces_body(const StepArgs& a, int t, int k, int i, int j)
 {
     const Shape s = a.s;
@@ -422,6 +518,14 @@ __device__ __forceinline__ void rk3_faces_body(const StepArgs& a, int t, int k, 
     double* sx = a.Sx + plane_at(p, xpl);
     double* sy = a.Sy + plane_at(p, ypl);
     const int fxo = j * (s.nx + 1) + i, fyo = j * s.nx + i;
+    if (FS != FS_WENO) {
+        sx[fxo] = x_face_lin<FS>(P, s, fl, j, i);
+        sy[fyo] = y_face_lin<FS>(P, s, fl, j, i);
+        a.Tx[pc + fyo] = zface_lin<FS>(a, s, cin, t, k, j, i);
+        if (i == s.nx - 1) sx[fxo + 1] = x_face_lin<FS>(P, s, fl, j, s.nx);
+        if (j == s.ny - 1) sy[fyo + s.nx] = y_face_lin<FS>(P, s, fl, s.ny, i);
+        return;
+    }
     double F, unused;
     x_face<ZV, false, false>(P, s, fl, j, i, F, unused);
     sx[fxo] = F;
@@ -443,12 +547,13 @@ __device__ __forceinline__ void rk3_faces_body(const StepArgs& a, int t, int k, 
 #ifndef POCEAN_RK3_FACES_MINB
 #define POCEAN_RK3_FACES_MINB 6
 #endif
-template <int STAGE, bool ZV, int TJR>
+template <int STAGE, bool ZV, int FS, int TJR>
 __global__ void __launch_bounds__(TI * TJR, POCEAN_RK3_FACES_MINB * 256 / (TI * TJR)) rk3_faces_kernel(StepArgs a)
 {
     int k, t;
     split_plane(blockIdx.z, a.s.nt, a.tdiv, k, t);
-    rk3_faces_body<STAGE, ZV>(a, t, k, blockIdx.x * TI + threadIdx.x % TI, blockIdx.y * TJR + threadIdx.x / TI);
+    rk3_faces_body<STAGE, ZV, FS>(a, t, k, blockIdx.x * TI + threadIdx.x % TI,
+                                  blockIdx.y * TJR + threadIdx.x / TI);
 }
 
 template <int STAGE, int TJR>
@@ -467,7 +572,8 @@ __global__ void __launch_bounds__(TI * TJR) rk3_update_kernel(StepArgs a)
         const i64 r = ((i64)t * s.n + k) * s.ny + gj;
         if (STAGE == 1) a.tef0[r] = F;
         else if (STAGE == 2) a.tef1[r] = F;
-        else a.fx_face[r] = div6_exact(a.tef0[r] + a.tef1[r]) + div3_exact(2.0 * F);
+        else if (STAGE == 3) a.fx_face[r] = div6_exact(a.tef0[r] + a.tef1[r]) + div3_exact(2.0 * F);
+        else if (STAGE == 5) a.fx_face[r] = F;                    // 'pc': the corrector's flux F(c^{n+1/2})
     }
     const double fzb = a.Tx[ci];
     const double fzt = k + 1 < s.n ? a.Tx[ci + pl] : 0.0;      // the surface interface carries no flux
@@ -486,8 +592,15 @@ __global__ void __launch_bounds__(TI * TJR) rk3_update_kernel(StepArgs a)
         v = v0 + 0.5 * dv;
         a.q2[ci] = q;
         a.c2[ci] = v > 0 ? q / v : c0;
-    } else {
+    } else if (STAGE == 3) {
         q = div3_exact(q0) + 2.0 / 3.0 * (a.q2[ci] + a.dt * r);
+        a.out[ci] = v1 > 0 ? q / v1 : c0;
+    } else if (STAGE == 4) {                                     // tracers.py:327-328
+        q = q0 + 0.5 * a.dt * r;
+        v = v0 + 0.5 * dv;
+        a.c1[ci] = v > 0 ? q / v : c0;
+    } else {                                                     // tracers.py:329
+        q = q0 + a.dt * r;
         a.out[ci] = v1 > 0 ? q / v1 : c0;
     }
 }
@@ -550,13 +663,14 @@ extern "C" size_t pocean_advect_rk3_workspace_bytes(int nt, int nz, int ny, int 
 
 static int common_checks(const char* fn, const void* C, const void* V0, const void* V1, const void* Qx,
                          const void* Qy, const void* ok, const void* out, int nt, int nz, int ny, int nx,
-                         unsigned flags, int face_i, const void* fx_face, void* ws, size_t ws_bytes, size_t need)
+                         unsigned flags, int face_i, const void* fx_face, void* ws, size_t ws_bytes, size_t need,
+                         unsigned allowed = 0xFFu)
 {
     int rc = check_shape(fn, nt, nz, ny, nx);
     if (rc) return rc;
     if (!C || !V0 || !V1 || !Qx || !Qy || !ok || !out)
         return pocean_fail(POCEAN_EINVAL, "%s: null input or output pointer", fn);
-    if (flags & ~(unsigned)0xFF) return pocean_fail(POCEAN_EINVAL, "%s: unknown flag bits 0x%x", fn, flags);
+    if (flags & ~allowed) return pocean_fail(POCEAN_EINVAL, "%s: unknown flag bits 0x%x", fn, flags & ~allowed);
     if (fx_face && (face_i < 0 || face_i > nx))
         return pocean_fail(POCEAN_EINVAL, "%s: face_i=%d outside 0..nx=%d", fn, face_i, nx);
     if (!ws || ws_bytes < need)
@@ -713,6 +827,27 @@ extern "C" int pocean_advect_fct_mixed(const double* C, const double* V0, const 
                            dt, C_out, face_i, fx_face, open_flux, workspace, workspace_bytes, stream);
 }
 
+// The passes of `advect`: three SSP-RK3 stages, or the 'pc' predictor (centred faces) and corrector (the
+// scheme's faces).
+template <bool ZV, int FS>
+static void launch_rk3(const StepArgs& a, bool pc, dim3 grid, cudaStream_t st)
+{
+    constexpr int R = POCEAN_FACE_ROWS;
+    if (pc) {
+        rk3_faces_kernel<4, false, FS_CEN, R><<<grid, TI * R, 0, st>>>(a);
+        rk3_update_kernel<4, R><<<grid, TI * R, 0, st>>>(a);
+        rk3_faces_kernel<5, ZV, FS, R><<<grid, TI * R, 0, st>>>(a);
+        rk3_update_kernel<5, R><<<grid, TI * R, 0, st>>>(a);
+        return;
+    }
+    rk3_faces_kernel<1, ZV, FS, R><<<grid, TI * R, 0, st>>>(a);
+    rk3_update_kernel<1, R><<<grid, TI * R, 0, st>>>(a);
+    rk3_faces_kernel<2, ZV, FS, R><<<grid, TI * R, 0, st>>>(a);
+    rk3_update_kernel<2, R><<<grid, TI * R, 0, st>>>(a);
+    rk3_faces_kernel<3, ZV, FS, R><<<grid, TI * R, 0, st>>>(a);
+    rk3_update_kernel<3, R><<<grid, TI * R, 0, st>>>(a);
+}
+
 extern "C" int pocean_advect_rk3_f64(const double* C, const double* V0, const double* V1, const double* Qx,
                                      const double* Qy, const double* Fz, const uint8_t* ok, const double* inflow,
                                      int nt, int nz, int ny, int nx, unsigned flags, double dt, double* C_out,
@@ -720,8 +855,11 @@ extern "C" int pocean_advect_rk3_f64(const double* C, const double* V0, const do
                                      void* stream)
 {
     const char* fn = "pocean_advect_rk3_f64";
+    if ((flags & POCEAN_FACES_UP3) && (flags & POCEAN_FACES_UP1))
+        return pocean_fail(POCEAN_EINVAL, "%s: POCEAN_FACES_UP3 and POCEAN_FACES_UP1 are exclusive", fn);
     int rc = common_checks(fn, C, V0, V1, Qx, Qy, ok, C_out, nt, nz, ny, nx, flags, face_i, fx_face, workspace,
-                           workspace_bytes, pocean_advect_rk3_workspace_bytes(nt, nz, ny, nx));
+                           workspace_bytes, pocean_advect_rk3_workspace_bytes(nt, nz, ny, nx),
+                           0xFFu | POCEAN_FACES_UP3 | POCEAN_FACES_UP1 | POCEAN_TIME_PC);
     if (rc) return rc;
     cudaStream_t st = (cudaStream_t)stream;
     StepArgs a{};
@@ -743,24 +881,12 @@ extern "C" int pocean_advect_rk3_f64(const double* C, const double* V0, const do
     a.Tx = (double*)w; w += cells;                                       // z-faces (interface k of each cell)
     a.Sx = (double*)w; w += align_up((size_t)nt * nz * ny * (nx + 1) * sizeof(double));
     a.Sy = (double*)w;
-    constexpr int R = POCEAN_FACE_ROWS;
-    const dim3 grid(ceil_div(nx, TI), ceil_div(ny, R), nt * nz);
-    const bool zv = !(flags & POCEAN_WENO_JS);
-    if (zv) {
-        rk3_faces_kernel<1, true, R><<<grid, TI * R, 0, st>>>(a);
-        rk3_update_kernel<1, R><<<grid, TI * R, 0, st>>>(a);
-        rk3_faces_kernel<2, true, R><<<grid, TI * R, 0, st>>>(a);
-        rk3_update_kernel<2, R><<<grid, TI * R, 0, st>>>(a);
-        rk3_faces_kernel<3, true, R><<<grid, TI * R, 0, st>>>(a);
-        rk3_update_kernel<3, R><<<grid, TI * R, 0, st>>>(a);
-    } else {
-        rk3_faces_kernel<1, false, R><<<grid, TI * R, 0, st>>>(a);
-        rk3_update_kernel<1, R><<<grid, TI * R, 0, st>>>(a);
-        rk3_faces_kernel<2, false, R><<<grid, TI * R, 0, st>>>(a);
-        rk3_update_kernel<2, R><<<grid, TI * R, 0, st>>>(a);
-        rk3_faces_kernel<3, false, R><<<grid, TI * R, 0, st>>>(a);
-        rk3_update_kernel<3, R><<<grid, TI * R, 0, st>>>(a);
-    }
+    const dim3 grid(ceil_div(nx, TI), ceil_div(ny, POCEAN_FACE_ROWS), nt * nz);
+    const bool pc = flags & POCEAN_TIME_PC;
+    if (flags & POCEAN_FACES_UP3) launch_rk3<false, FS_UP3>(a, pc, grid, st);
+    else if (flags & POCEAN_FACES_UP1) launch_rk3<false, FS_UP1>(a, pc, grid, st);
+    else if (flags & POCEAN_WENO_JS) launch_rk3<false, FS_WENO>(a, pc, grid, st);
+    else launch_rk3<true, FS_WENO>(a, pc, grid, st);
     return pocean_check_launch(fn);
 }
 

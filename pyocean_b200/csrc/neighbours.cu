@@ -140,10 +140,11 @@ __device__ __forceinline__ double edge_weighted(double h0, double h1, double r0,
     return (r0 * h1 + r1 * h0) / (h0 + h1);
 }
 
-// regrid.py:100-154 `_p1m_h2_positions` with m == n.  u: the modified densities; I out: interface densities;
-// G out: cumulative thickness from the surface; x out: the interface depths.
+// regrid.py:100-154 `_p1m_h2_positions` for m target layers (m + 1 target densities).  u: the modified densities;
+// I out: interface densities; G out: cumulative thickness from the surface; x out: the m + 1 interface depths.
 __device__ __forceinline__ void p1m_h2_positions(const HybridColumn& col, const double* u,
-                                                 const double* __restrict__ targets, double* I, double* G, double* x)
+                                                 const double* __restrict__ targets, int m, double* I, double* G,
+                                                 double* x)
 {
     const int n = col.n;
     double hm = col.th(0), hc = hm;                   // sliding h[k-1], h[k], h[k+1]
@@ -183,8 +184,9 @@ __device__ __forceinline__ void p1m_h2_positions(const HybridColumn& col, const 
         hp = k + 2 < n ? col.th(k + 2) : hc;
     }
     I[n] = er_prev;
-    for (int k = 0; k <= n; ++k) x[k] = G[k];
-    for (int kk = 1; kk < n; ++kk) {
+    // the fallback where no cell matches (a non-finite density): the source grid, or uniform for another count
+    for (int k = 0; k <= m; ++k) x[k] = m == n ? G[k] : G[n] * (double)k / (double)m;
+    for (int kk = 1; kk < m; ++kk) {
         const double t = __ldg(targets + kk);
         int lo = 0, len = n + 1;                      // p = first index with I[p] >= t (n + 1 if none)
         while (len > 0) {
@@ -242,10 +244,11 @@ __device__ __forceinline__ void keep_consistent(const HybridColumn& col, const d
     }
 }
 
-// regrid.py:204-252 `hycom1_column` (m == n) into zw (bed first); A, B, G scratch of n+1 each.
+// regrid.py:204-252 `hycom1_column` for m target layers into zw (bed first, m+1); A, B, G scratch of
+// max(n, m) + 1 each.  The isopycnal test (`keep`) applies only when m == n, as in the reference.
 template <int NMAX>
 __device__ __forceinline__ void hycom1_column(double H, double eta, const HybridColumn& col, const HybridParams& P,
-                                              double* zw, double* A, double* B, double* G)
+                                              int m, double* zw, double* A, double* B, double* G)
 {
     const int n = col.n;
     const double D = H + eta;
@@ -266,22 +269,22 @@ __device__ __forceinline__ void hycom1_column(double H, double eta, const Hybrid
         for (int kk = 0; kk < k0; ++kk) A[kk] = A[k0];
     for (int k = n - 2; k >= 0; --k) A[k] = pmin(A[k], A[k + 1]);
     double* x = zw;                           // depths in zw's storage, reversed into A below
-    p1m_h2_positions(col, A, P.rho_target, B, G, x);
-    if (P.keep) keep_consistent<NMAX>(col, P.rho_target, 2.0 * P.h_min, G, x);
+    p1m_h2_positions(col, A, P.rho_target, m, B, G, x);
+    if (P.keep && m == n) keep_consistent<NMAX>(col, P.rho_target, 2.0 * P.h_min, G, x);
     const double s = D / H;
     double nominal = 0.0;
-    for (int k = 1; k <= n; ++k) {
+    for (int k = 1; k <= m; ++k) {
         nominal += __ldg(P.dz_top + k - 1) * s;
         x[k] = pmin(pmax(x[k], nominal), D);
     }
-    for (int k = 1; k < n; ++k) x[k] = pmin(x[k], x[k - 1] + __ldg(P.max_h_top + k - 1));
-    for (int k = 1; k <= n; ++k) x[k] = pmax(x[k], x[k - 1]);
-    x[n] = D;
-    for (int j = 0; j <= n; ++j) A[j] = eta - x[n - j];
+    for (int k = 1; k < m; ++k) x[k] = pmin(x[k], x[k - 1] + __ldg(P.max_h_top + k - 1));
+    for (int k = 1; k <= m; ++k) x[k] = pmax(x[k], x[k - 1]);
+    x[m] = D;
+    for (int j = 0; j <= m; ++j) A[j] = eta - x[m - j];
     A[0] = -H;
-    A[n] = eta;
-    enforce_min_thickness(A, n, P.h_min);
-    for (int j = 0; j <= n; ++j) zw[j] = A[j];
+    A[m] = eta;
+    enforce_min_thickness(A, m, P.h_min);
+    for (int j = 0; j <= m; ++j) zw[j] = A[j];
 }
 
 // regrid.py:255-260 `transition_weight`.
@@ -289,6 +292,35 @@ __device__ __forceinline__ double transition_weight(double D, double d_sigma, do
 {
     if (d_hybrid <= d_sigma) return D > d_sigma ? 1.0 : 0.0;
     return pmin(pmax((D - d_sigma) / (d_hybrid - d_sigma), 0.0), 1.0);
+}
+
+// The hybrid rule of `_regrid_columns` (regrid.py:322-340) for one wet column: sigma where the shallow-sigma weight
+// is 0 (or H <= 0 with a sigma zone), else hycom1_column, windowed towards sigma where 0 < q < 1; zw bed first (m+1).
+template <int NMAX>
+__device__ __forceinline__ void hybrid_column(double H, double et, const HybridColumn& hc, const HybridParams& P,
+                                              int m, double* col, double* A, double* B, double* G)
+{
+    const double q = P.d_hybrid > 0.0 ? transition_weight(H + et, P.d_sigma, P.d_hybrid) : 1.0;
+    const double qq = (P.d_hybrid > 0.0 && H <= 0.0) ? 0.0 : q;     // flooded land: sigma at any depth
+    if (qq <= 0.0) {
+        sigma_heights(H, et, P.dsigma, m, P.h_min, col);
+        return;
+    }
+    hycom1_column<NMAX>(H, et, hc, P, m, col, A, B, G);
+    if (qq < 1.0) {                                   // regrid.py:263-289 `window_shallow_sigma`
+        double* sig = A;
+        double* zs = B;
+        sigma_heights(H, et, P.dsigma, m, P.h_min, sig);
+        zstar_heights(H, et, P.dz_top, m, P.h_min, zs);   // surface first: bed-first interface j is zs[m - j]
+        for (int j = 0; j <= m; ++j) {
+            const double lo = qq * (-H) + (1.0 - qq) * sig[j];
+            const double hi = qq * zs[m - j] + (1.0 - qq) * sig[j];
+            col[j] = pmin(pmax(col[j], lo), hi);
+        }
+        col[0] = -H;
+        col[m] = sig[m];
+        enforce_min_thickness(col, m, P.h_min);
+    }
 }
 
 // One thread per column: the hybrid rule of `_regrid_columns` (code 2) with the wet mask and h_new of
@@ -318,29 +350,40 @@ __global__ void __launch_bounds__(128) regrid_hybrid_kernel(const double* __rest
     for (int k = 0; k < n; ++k) finite = finite && isfinite(__ldg(rho + k * plane + c));
     if ((!finite || (P.d_hybrid <= 0.0 && !(H > 0.0))) && bad) atomicAdd(bad, 1);
     double col[NMAX + 1], A[NMAX + 1], B[NMAX + 1], G[NMAX + 1];
-    const double q = P.d_hybrid > 0.0 ? transition_weight(H + et, P.d_sigma, P.d_hybrid) : 1.0;
-    const double qq = (P.d_hybrid > 0.0 && H <= 0.0) ? 0.0 : q;     // flooded land: sigma at any depth
-    if (qq <= 0.0) {
-        sigma_heights(H, et, P.dsigma, n, P.h_min, col);
-    } else {
-        const HybridColumn hc{h_src + c, rho + c, plane, n};
-        hycom1_column<NMAX>(H, et, hc, P, col, A, B, G);
-        if (qq < 1.0) {                               // regrid.py:263-289 `window_shallow_sigma`
-            double* sig = A;
-            double* zs = B;
-            sigma_heights(H, et, P.dsigma, n, P.h_min, sig);
-            zstar_heights(H, et, P.dz_top, n, P.h_min, zs);   // surface first: bed-first interface j is zs[n - j]
-            for (int j = 0; j <= n; ++j) {
-                const double lo = qq * (-H) + (1.0 - qq) * sig[j];
-                const double hi = qq * zs[n - j] + (1.0 - qq) * sig[j];
-                col[j] = pmin(pmax(col[j], lo), hi);
-            }
-            col[0] = -H;
-            col[n] = sig[n];
-            enforce_min_thickness(col, n, P.h_min);
-        }
-    }
+    const HybridColumn hc{h_src + c, rho + c, plane, n};
+    hybrid_column<NMAX>(H, et, hc, P, n, col, A, B, G);
     for (int k = 0; k < n; ++k) h_new[k * plane + c] = col[k + 1] - col[k];
+}
+
+// One thread per column: `_regrid_columns` (regrid.py:309-342) itself, target interface heights zw (m+1, bed first)
+// of every column that `wet` marks (the others NaN, as the reference leaves them); code 0 z*, 1 sigma, 2 hybrid on
+// the n source layers h, rho (m may differ from n only for the hybrid rule).
+template <int NMAX>
+__global__ void __launch_bounds__(128) regrid_columns_kernel(int code, const double* __restrict__ Hin,
+                                                             const double* __restrict__ eta,
+                                                             const double* __restrict__ h,
+                                                             const double* __restrict__ rho,
+                                                             const uint8_t* __restrict__ wet, HybridParams P, int n,
+                                                             int m, i64 plane, double* __restrict__ zw)
+{
+    const i64 c = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= plane) return;
+    if (!__ldg(wet + c)) {
+        for (int k = 0; k <= m; ++k) zw[k * plane + c] = nan("");
+        return;
+    }
+    const double H = nan_to_num(__ldg(Hin + c)), et = __ldg(eta + c);
+    double col[NMAX + 1], A[NMAX + 1], B[NMAX + 1], G[NMAX + 1];
+    if (code == 0) {
+        zstar_heights(H, et, P.dz_top, m, P.h_min, A);
+        for (int j = 0; j <= m; ++j) col[j] = A[m - j];
+    } else if (code == 1) {
+        sigma_heights(H, et, P.dsigma, m, P.h_min, col);
+    } else {
+        const HybridColumn hc{h + c, rho + c, plane, n};
+        hybrid_column<NMAX>(H, et, hc, P, m, col, A, B, G);
+    }
+    for (int k = 0; k <= m; ++k) zw[k * plane + c] = col[k];
 }
 
 // Column IO of the velocity remap in fraction space (vertical_coordinate.py:142-153): source thickness
@@ -660,5 +703,35 @@ extern "C" int pocean_diffuse_ale_f64(const double* T, const double* Tw, const d
     nb::diffuse_ale_kernel<<<grid, nb::DTI * nb::DTJ, 0, (cudaStream_t)stream>>>(
         T, Tw, h, act, cx, cy, okx, oky, V, nt, nz, ny, nx, (flags & POCEAN_PERIODIC_X) != 0,
         (flags & POCEAN_PERIODIC_Y) != 0, kh, dt, out);
+    return pocean_check_launch(fn);
+}
+
+extern "C" int pocean_regrid_columns_f64(int code, const double* H, const double* eta, const double* h,
+                                         const double* rho, const uint8_t* wet, const double* dz_top,
+                                         const double* dsigma, const double* rho_target, const double* max_h_top,
+                                         double d_sigma, double d_hybrid, double h_min, int keep, int n, int m,
+                                         int ny, int nx, double* zw, void* stream)
+{
+    const char* fn = "pocean_regrid_columns_f64";
+    if (code < 0 || code > 2) return pocean_fail(POCEAN_EINVAL, "%s: unknown rule %d", fn, code);
+    if (n < 1 || m < 1 || ny < 1 || nx < 1) return pocean_fail(POCEAN_EINVAL, "%s: bad sizes", fn);
+    if (n > 256 || m > 256) return pocean_fail(POCEAN_EINVAL, "%s: at most 256 layers (n=%d m=%d)", fn, n, m);
+    if (code != 2 && n != m)
+        return pocean_fail(POCEAN_EINVAL, "%s: a target layer count other than the source's is only for the hybrid "
+                           "rule", fn);
+    if (!H || !eta || !wet || !zw || (code == 0 && !dz_top) || (code == 1 && !dsigma) ||
+        (code == 2 && (!h || !rho || !dz_top || !rho_target || !max_h_top || (d_hybrid > 0.0 && !dsigma))))
+        return pocean_fail(POCEAN_EINVAL, "%s: null pointer", fn);
+    int rc = pocean_check_device();
+    if (rc) return rc;
+    nb::HybridParams P{rho_target, dz_top, max_h_top, dsigma, d_sigma, d_hybrid, h_min, keep};
+    const i64 plane = (i64)ny * nx;
+    const unsigned gx = (unsigned)((plane + 127) / 128);
+    const int nm = n > m ? n : m;
+    cudaStream_t st = (cudaStream_t)stream;
+    if (nm <= 64) nb::regrid_columns_kernel<64><<<gx, 128, 0, st>>>(code, H, eta, h, rho, wet, P, n, m, plane, zw);
+    else if (nm <= 128)
+        nb::regrid_columns_kernel<128><<<gx, 128, 0, st>>>(code, H, eta, h, rho, wet, P, n, m, plane, zw);
+    else nb::regrid_columns_kernel<256><<<gx, 128, 0, st>>>(code, H, eta, h, rho, wet, P, n, m, plane, zw);
     return pocean_check_launch(fn);
 }

@@ -51,9 +51,11 @@ def _wet_pinned(wet, ny: int, nx: int) -> bool:
             tuple(wet.shape) == (ny, nx) and wet.dtype in (torch.bool, torch.uint8))
 
 
-def _remap_pipelined(h_src, f_src, h_tgt, wet, n0, n1, ny, nx, nf, scheme, stacked):
+def _remap_pipelined(h_src, f_src, h_tgt, wet, n0, n1, ny, nx, nf, scheme, stacked, f_dev=None):
     """remap_columns of pinned host tensors in row blocks of columns: block b's thicknesses and fields go to the
-    device on one stream while block b-1 is remapped on another and block b-2's result comes back on a third."""
+    device on one stream while block b-1 is remapped on another and block b-2's result comes back on a third.
+    ``f_dev``: the fields are already on the device (nf, n0, ny, nx), made by work ordered on the compute stream;
+    their rows are copied there instead of uploaded (``f_src`` unused)."""
     dev = _pl.device_now()
     s_in, s_cmp, s_out = _pl.streams(dev)
     s_in.wait_stream(torch.cuda.current_stream(dev))
@@ -68,11 +70,15 @@ def _remap_pipelined(h_src, f_src, h_tgt, wet, n0, n1, ny, nx, nf, scheme, stack
             wc = torch.empty((r, nx), dtype=torch.uint8, device=dev)
         _pl.copy2d(hs.data_ptr(), r * row, h_src.data_ptr() + j0 * row, ny * row, r * row, n0, s_in)
         _pl.copy2d(ht.data_ptr(), r * row, h_tgt.data_ptr() + j0 * row, ny * row, r * row, n1, s_in)
-        _pl.copy2d(fc.data_ptr(), r * row, f_src.data_ptr() + j0 * row, ny * row, r * row, nf * n0, s_in)
+        if f_dev is None:
+            _pl.copy2d(fc.data_ptr(), r * row, f_src.data_ptr() + j0 * row, ny * row, r * row, nf * n0, s_in)
         _pl.copy2d(wc.data_ptr(), r * nx, wet.data_ptr() + j0 * nx, ny * nx, r * nx, 1, s_in)
         ev = torch.cuda.Event()
         ev.record(s_in)
         s_cmp.wait_event(ev)
+        if f_dev is not None:
+            fc.record_stream(s_cmp)
+            _pl.copy2d(fc.data_ptr(), r * row, f_dev.data_ptr() + j0 * row, ny * row, r * row, nf * n0, s_cmp)
         with torch.cuda.stream(s_cmp):
             oc = torch.empty((nf, n1, r, nx), dtype=torch.float64, device=dev)
         _lib.check(L.pocean_remap_columns_f64(hs.data_ptr(), fc.data_ptr(), ht.data_ptr(), wc.data_ptr(), n0, n1, r,
@@ -83,6 +89,8 @@ def _remap_pipelined(h_src, f_src, h_tgt, wet, n0, n1, ny, nx, nf, scheme, stack
         _pl.copy2d(out.data_ptr() + j0 * row, ny * row, oc.data_ptr(), r * row, r * row, nf * n1, s_out)
         keep += [hs, ht, fc, wc, oc]
     s_out.synchronize()
+    if f_dev is not None:
+        keep.append(f_dev)
     return out
 
 

@@ -57,3 +57,29 @@ class ALETracerStep:
     def step(self, C, V0, V1, Qx, Qy, ok, h_src, h_tgt, wet, out) -> torch.Tensor:
         """out = remap(advect_fct(C)); ``out`` must not alias ``C``."""
         return self.remap(h_src, self.advect(C, V0, V1, Qx, Qy, ok), h_tgt, wet, out)
+
+
+def ale_tracer_step(adv, C, V0, V1, Qx, Qy, ok, h_src, h_tgt, scheme: int, wet):
+    """One ALE tracer step as the reference's driver runs it (core/model/driver.py:888-985, phases 7 and 8):
+    ``adv.advect_fct`` of the stack (``adv`` a ``TracerAdvection``), then ``remap_columns`` of every member from
+    h_src onto h_tgt, in one call, so the advected stack never leaves the device.  Results equal the two calls made
+    one after the other, bit for bit.  Host arrays (NumPy, or pinned torch tensors: then the uploads of layer blocks,
+    the FCT passes, the uploads of the thicknesses' row blocks, the remap and the downloads overlap) give the
+    remapped stack on the host; CUDA tensors give a CUDA tensor."""
+    from . import _pipeline as _pl
+    from .remap import _remap_pipelined, _wet_pinned, remap_columns
+    nt, n, ny, nx = tuple(C.shape)
+    n1 = tuple(h_tgt.shape)[0]
+    if (nt >= 2 and _pl.pinned(C, V0, V1, Qx, Qy, ok, h_src, h_tgt) and _wet_pinned(wet, ny, nx)
+            and all(a.dtype == torch.float64 for a in (C, V0, V1, Qx, Qy, h_src, h_tgt))
+            and ok.dtype in (torch.bool, torch.uint8) and tuple(ok.shape) in ((n, ny, nx), (ny, nx))
+            and 8 * nt * n * ny * nx >= _pl.MIN_BYTES and ny >= 8 and not adv.record_open_flux):
+        A = adv._advect_fct_layered(C, V0, V1, Qx, Qy, ok, download=False)
+        return _remap_pipelined(h_src, None, h_tgt, wet, n, n1, ny, nx, nt, int(scheme), True, f_dev=A)
+    host = not (isinstance(C, torch.Tensor) and C.is_cuda)
+    if host:
+        from ._device import Converter
+        cv = Converter(C, V0, V1, Qx, Qy, ok, h_src, h_tgt, wet)
+        A = adv.advect_fct(cv.f64(C), cv.f64(V0), cv.f64(V1), cv.f64(Qx), cv.f64(Qy), cv.u8(ok, tuple(ok.shape)))
+        return cv.out(remap_columns(cv.f64(h_src), A, cv.f64(h_tgt), scheme, cv.u8(wet, (ny, nx))))
+    return remap_columns(h_src, adv.advect_fct(C, V0, V1, Qx, Qy, ok), h_tgt, scheme, wet)

@@ -6,10 +6,11 @@ model's periodic axes, and call ``advect_fct`` (ALE step with Zalesak FCT) or ``
 Arrays are NumPy (copied to the GPU and back) or CUDA torch tensors (used in place, results stay on the device).
 Inputs are never modified; results are new arrays, as in the reference.
 
-What the reference offers and this class does not: the ``'pc'`` predictor-corrector time stepping and the
-non-WENO face schemes of ``advect`` (``upwind3`` / ``upwind1`` / centred faces) — both run the reference's NumPy
-path, not its compiled hot path — raise ``NotImplementedError``.  ``advect_fct`` uses WENO5-Z for
-``scheme='weno5'`` and WENO5-JS otherwise, exactly as the reference's fused path does (tracers.py:176).
+``advect`` also covers what the reference runs through its NumPy RHS path (tracers.py:110-151, 303-330): the
+``upwind3`` / ``upwind1`` face schemes (any other non-WENO5 name is upwind-3, as there) and the ``'pc'``
+predictor-corrector time stepping (a centred half step, then a full step with the scheme's faces), in FP64 and
+bit for bit.  ``advect_fct`` uses WENO5-Z for ``scheme='weno5'`` and WENO5-JS otherwise, exactly as the reference's
+fused path does (tracers.py:176).
 """
 from __future__ import annotations
 
@@ -127,11 +128,13 @@ class TracerAdvection:
             return cv.out(out)
         return cv.out(out), cv.out(fx)
 
-    def _advect_fct_layered(self, C, V0, V1, Qx, Qy, ok):
+    def _advect_fct_layered(self, C, V0, V1, Qx, Qy, ok, download: bool = True):
         """advect_fct of pinned host tensors in blocks of layers: block b's tracers and geometry go to the device on
         the copy-in stream while the stage passes of block b-1 and the limiter passes of block b-2 run on the
         compute stream (``pocean_advect_fct_layers``: a block's limiter reads the layers either side of it) and
-        finished blocks come back on the copy-out stream."""
+        finished blocks come back on the copy-out stream.  ``download=False``: the advected stack stays on the
+        device and is returned as a tensor whose producing kernels are ordered on the compute stream
+        (``_pipeline.streams``), for a caller that goes on with it there."""
         nt, n, ny, nx = C.shape
         dev = _pl.device_now()
         s_in, s_cmp, s_out = _pl.streams(dev)
@@ -153,7 +156,9 @@ class TracerAdvection:
         with torch.cuda.stream(s_cmp):
             outd = torch.empty((nt, n, ny, nx), **f64)
             ws = torch.empty(max(nbytes, 256), dtype=torch.uint8, device=dev)
-        out = torch.empty((nt, n, ny, nx), dtype=torch.float64, pin_memory=True)
+        out = torch.empty((nt, n, ny, nx), dtype=torch.float64, pin_memory=True) if download else None
+        for t in (Cd, V0d, V1d, Qxd, Qyd, okd):     # made on the copy-in stream, read on the compute stream
+            t.record_stream(s_cmp)
         pl, px, py = ny * nx, ny * (nx + 1), (ny + 1) * nx
 
         def layers(k0, k1, part):
@@ -162,7 +167,9 @@ class TracerAdvection:
                                                   nx, flags, float(self.dt), outd.data_ptr(), ws.data_ptr(), nbytes,
                                                   k0, k1, part, s_cmp.cuda_stream), "advect_fct")
 
-        def download(k0, k1):
+        def fetch(k0, k1):
+            if not download:
+                return
             ev = torch.cuda.Event()
             ev.record(s_cmp)
             s_out.wait_event(ev)
@@ -185,9 +192,11 @@ class TracerAdvection:
             layers(k0, k1, 0)
             if b > 0:
                 layers(*blocks[b - 1], 1)
-                download(*blocks[b - 1])
+                fetch(*blocks[b - 1])
         layers(*blocks[-1], 1)
-        download(*blocks[-1])
+        fetch(*blocks[-1])
+        if not download:
+            return outd
         s_out.synchronize()
         return out
 
@@ -252,15 +261,12 @@ class TracerAdvection:
     def advect(self, C, V0, V1, Qx, Qy, Fz, ok, inflow=None, flux_face_i: int | None = None):
         """
         SSP-RK3 flux-form advection of the stack C with frozen Qx, Qy, Fz (N+1, ny, nx); layer volumes linear from
-        V0 to V1 (tracers.py:342-375).  ``flux_face_i``: also return (F(c0) + F(c1))/6 + 2F(c2)/3 through u-face
-        column i.
+        V0 to V1 (tracers.py:342-375); with ``time='pc'`` the predictor-corrector step (tracers.py:324-330).
+        ``flux_face_i``: also return (F(c0) + F(c1))/6 + 2F(c2)/3 through u-face column i ('pc': the corrector's
+        flux F(c^{n+1/2})).
         """
-        if self.tracer_time == "pc":
-            raise NotImplementedError("tracer_time='pc' runs the reference's NumPy path; not implemented on GPU")
         if self.precision != "f64":
             raise NotImplementedError("advect (no limiter) is available in FP64 only")
-        if not self.tracer_scheme.startswith("weno5"):
-            raise NotImplementedError(f"tracer_scheme={self.tracer_scheme!r}: only the WENO5 schemes are on GPU")
         nt, n, ny, nx = self._shapes(C, Qx, Qy)
         if shape_of(V0) != (n, ny, nx) or shape_of(V1) != (n, ny, nx):
             raise ValueError(f"_advect: volume shape {shape_of(V0)}/{shape_of(V1)} vs tracer layers {(n, ny, nx)}")
@@ -283,9 +289,16 @@ class TracerAdvection:
         L = _lib.lib()
         nbytes = L.pocean_advect_rk3_workspace_bytes(nt, n, ny, nx)
         ws = cv.workspace(nbytes)
+        # tracers.py:110-115, 153-156: non-WENO5 schemes take the NumPy path's upwind faces (order 1 for
+        # "upwind1", else 3); 'pc' (tracers.py:355-356) the predictor-corrector step
+        flags = self._flags()
+        if not self.tracer_scheme.startswith("weno5"):
+            flags |= _lib.FACES_UP1 if self.tracer_scheme == "upwind1" else _lib.FACES_UP3
+        if self.tracer_time == "pc":
+            flags |= _lib.TIME_PC
         rc = L.pocean_advect_rk3_f64(Cd.data_ptr(), V0d.data_ptr(), V1d.data_ptr(), Qxd.data_ptr(), Qyd.data_ptr(),
                                      None if Fzd is None else Fzd.data_ptr(), okd.data_ptr(),
-                                     None if infl is None else infl.data_ptr(), nt, n, ny, nx, self._flags(),
+                                     None if infl is None else infl.data_ptr(), nt, n, ny, nx, flags,
                                      float(self.dt), out.data_ptr(), fi, None if fx is None else fx.data_ptr(),
                                      ws.data_ptr(), nbytes, cv.stream())
         _lib.check(rc, "advect")

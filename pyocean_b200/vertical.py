@@ -149,6 +149,56 @@ class ALECoordinate:
         return remap_faces(vel, hf_src, hf_tgt, self.remap_code, w_tgt)
 
 
+def regrid_columns(rule: str, H, eta, h, rho, params: dict, wet, n_out: int | None = None):
+    """Target interface heights zw (N+1, ny, nx), bed first, of the rule 'zstar', 'sigma' or 'hybrid'
+    (core/vertical/regrid.py:345-395, same arguments): N = n_out, by default the source layer count; the hybrid
+    rule may regrid a source of another count (the data levels of an initial state).  NaN in the columns that are
+    not wet.  Raises ValueError where the reference does."""
+    if rule not in ("zstar", "sigma", "hybrid"):
+        raise ValueError(f"unknown rule {rule!r}; use 'zstar', 'sigma' or 'hybrid'")
+    required = {"zstar": ("dz_top",), "sigma": ("dsigma",), "hybrid": ("dz_top", "rho_target")}[rule]
+    if rule == "hybrid" and float(params.get("d_hybrid", 0.0)) > 0.0:
+        required += ("dsigma",)
+    for key in required:
+        if key not in params:
+            raise ValueError(f"regrid_columns({rule!r}) needs params[{key!r}]")
+    if rule == "hybrid" and rho is None:
+        raise ValueError("regrid_columns('hybrid') needs the layer densities rho")
+    n, ny, nx = shape_of(h)
+    m = n if n_out is None else int(n_out)
+    if m != n and rule != "hybrid":
+        raise ValueError("n_out != the source layer count is only for rule 'hybrid'")
+    cv = Converter(H, eta, h, wet, *(() if rho is None else (rho,)))
+    Hd, ed, hd, wd = cv.f64(H, (ny, nx)), cv.f64(eta, (ny, nx)), cv.f64(h), cv.u8(wet, (ny, nx))
+    w = wd.bool()
+    Hw, Dw = Hd[w], (Hd + ed)[w]
+    if not bool(torch.isfinite(Hw).all() & torch.isfinite(Dw).all() & (Dw > 0).all()):
+        raise ValueError("wet columns need finite H and D = H + eta > 0")
+    if rule == "zstar" and not bool((Hw > 0).all()):
+        raise ValueError("z* needs H > 0 in every wet column (cells that can dry: sigma, or hybrid with d_hybrid > 0)")
+    rd = None
+    if rule == "hybrid":
+        if float(params.get("d_hybrid", 0.0)) <= 0 and bool((Hw <= 0).any()):
+            raise ValueError("hybrid needs H > 0 unless it has a shallow sigma zone (d_hybrid > 0); columns with "
+                             "H <= 0 then stay sigma at any depth")
+        rd = cv.f64(rho, (n, ny, nx))
+        if not bool(torch.isfinite(rd[:, w]).all()):
+            raise ValueError("non-finite density in a wet column")
+    f = lambda key, default, size: cv.f64(np.asarray(params.get(key, default), float), (size,))   # noqa: E731
+    dz = f("dz_top", np.ones(m), m)
+    ds = f("dsigma", np.full(m, 1.0 / m), m)
+    rt = f("rho_target", np.zeros(m + 1), m + 1)
+    mx = f("max_h_top", np.full(m, np.inf), m)
+    zw = cv.empty((m + 1, ny, nx))
+    code = {"zstar": 0, "sigma": 1, "hybrid": 2}[rule]
+    _lib.check(_lib.lib().pocean_regrid_columns_f64(
+        code, Hd.data_ptr(), ed.data_ptr(), hd.data_ptr(), None if rd is None else rd.data_ptr(), wd.data_ptr(),
+        dz.data_ptr(), ds.data_ptr(), rt.data_ptr(), mx.data_ptr(), float(params.get("d_sigma", 0.0)),
+        float(params.get("d_hybrid", 0.0)), float(params.get("h_min", H_MIN)),
+        int(bool(params.get("keep_isopycnal", True))), n, m, ny, nx, zw.data_ptr(), cv.stream()), "regrid_columns")
+    return cv.out(zw)
+
+
 def remap_faces(vel, hf_src, hf_tgt, scheme: int, w_tgt=None):
     vs, hs = shape_of(vel), shape_of(hf_src)
     if len(hs) != 3 or vs[-3:] != hs or len(vs) not in (3, 4) or shape_of(hf_tgt) != hs:

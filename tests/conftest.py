@@ -38,3 +38,16 @@ def case_open(rec) -> tuple:
 
 def case_periodic(rec) -> tuple:
     return tuple(str(s) for s in rec["periodic"]) if "periodic" in rec else ()
+
+
+def regrid_columns_args(rec) -> tuple:
+    """The arguments of ``regrid_columns(rule, H, eta, h, rho, params, wet, n_out)`` of a golden case."""
+    rule = str(rec["rule"])
+    if rule == "hybrid":
+        params = dict(dz_top=rec["dz_top"], rho_target=rec["rho_target"], max_h_top=rec["max_h_top"],
+                      h_min=float(rec["h_min"]), keep_isopycnal=bool(rec["keep"]))
+        if float(rec["d_hybrid"]) > 0:
+            params.update(dsigma=rec["dsigma"], d_sigma=float(rec["d_sigma"]), d_hybrid=float(rec["d_hybrid"]))
+        return rule, rec["H"], rec["eta"], rec["h"], rec["rho"], params, rec["wet"], int(rec["n_out"])
+    params = {k: rec[k] for k in ("dz_top", "dsigma") if k in rec}
+    return rule, rec["H"], rec["eta"], rec["h"], None, params, rec["wet"], None

@@ -186,6 +186,46 @@ def rk3_cases():
     return out
 
 
+def rk3_ext_cases():
+    """``advect`` with the NumPy path's face schemes (upwind3, upwind1) and the 'pc' predictor-corrector time
+    stepping (tracers.py:110-151, 303-375)."""
+    out = {}
+    specs = [("up3_open_vert_inflow", 2, 6, 9, 13, ("west", "east", "south"), True, "upwind3", "ssprk3", ()),
+             ("up1_closed_vert", 1, 5, 8, 10, (), True, "upwind1", "ssprk3", ()),
+             ("up3_periodic_xy_tef", 2, 4, 10, 12, (), False, "upwind3", "ssprk3", ("x", "y")),
+             ("pc_weno5_open_vert", 2, 7, 9, 11, ("west", "north"), True, "weno5", "pc", ()),
+             ("pc_weno5js_periodic_x_tef", 1, 5, 8, 12, ("south",), True, "weno5js", "pc", ("x",)),
+             ("pc_up3_inflow_vert", 2, 6, 8, 11, ("west", "east", "south", "north"), True, "upwind3", "pc", ()),
+             ("pc_up1_novert_tef", 1, 4, 7, 9, ("east",), False, "upwind1", "pc", ())]
+    for seed, (name, nt, n, ny, nx, open_, vert, scheme, time, per) in enumerate(specs):
+        rng = np.random.default_rng(900 + seed)
+        dt = 10.0
+        V0, V1, Qx, Qy, ok = transports(rng, nt, n, ny, nx, dt, open_, periodic=per)
+        Fz = rng.normal(size=(n + 1, ny, nx)) * 1e2 if vert else np.zeros((n + 1, ny, nx))
+        Fz[0] = Fz[-1] = 0.0
+        C = rng.normal(10.0, 1.0, (nt, n, ny, nx))
+        inflow = rng.normal(11.0, 1.0, C.shape) if "inflow" in name else None
+        adv = TracerAdvection(scheme=scheme, time=time, dt=dt, ob=_OB(open_))
+        adv.per = Periodic(per)
+        fi = 4 if name.endswith("tef") else None
+        res = adv.advect(C, V0, V1, Qx, Qy, Fz, ok, inflow=inflow, flux_face_i=fi)
+        rec = dict(C=C, V0=V0, V1=V1, Qx=Qx, Qy=Qy, Fz=Fz, ok=ok, dt=dt, scheme=scheme, time=time,
+                   open=np.array(open_, dtype="U5"), periodic=np.array(per, dtype="U1"))
+        if inflow is not None:
+            rec["inflow"] = inflow
+        if fi is None:
+            rec["out"] = res
+        else:
+            rec["flux_face_i"] = fi
+            rec["out"], rec["fx_i"] = res
+        if not per:
+            # the NumPy RHS alone: centred (the predictor's) and with the scheme's own faces
+            rec["rhs_centred"] = adv.rhs(C, Qx, Qy, Fz, ok, centred=True, inflow=inflow)
+            rec["rhs"] = adv.rhs(C, Qx, Qy, Fz, ok, inflow=inflow)
+        out[name] = rec
+    return out
+
+
 def kernel_cases():
     """Single kernels: faces_h and the FCT coefficients (tests/test_sigma_ale.py:1396-1429 inputs)."""
     out = {}
@@ -601,6 +641,53 @@ def layer_transport_cases():
     return out
 
 
+def regrid_columns_cases():
+    """``regrid_columns`` itself (regrid.py:345-395): the z*, sigma and hybrid rules on a given wet mask (NaN in the
+    other columns), and the hybrid rule on a source of another layer count (``n_out``: the finer data levels of an
+    initial state, and a coarser source), with and without the shallow sigma window."""
+    out = {}
+    rng = np.random.default_rng(91)
+    ny, nx = 7, 9
+
+    class _EOS:
+        @staticmethod
+        def density(T, S):
+            return 1027.0 * (1.0 - 2e-4 * (T - 10.0) + 7.6e-4 * (S - 35.0))
+
+    H = rng.uniform(20.0, 400.0, (ny, nx))
+    H[1, 2] = 3.0                                                     # shallower than the sigma zone
+    eta = rng.uniform(-0.5, 0.5, (ny, nx))
+    wet = rng.random((ny, nx)) > 0.15
+    for name, n_src, m in (("rc_hybrid_fine", 40, 12), ("rc_hybrid_coarse", 8, 15), ("rc_hybrid_same", 12, 12)):
+        D = H + eta
+        # source layers: thicker towards the bed, a few nearly massless, T warm at the surface with a jump
+        w = rng.uniform(0.5, 1.5, (n_src, ny, nx))
+        w[rng.random((n_src, ny, nx)) < 0.08] = 1e-4
+        h = w / w.sum(0) * D[None]
+        z = np.cumsum(h, axis=0) - 0.5 * h                                  # height above the bed
+        T = 4.0 + 18.0 * np.clip(z / 300.0, 0, 1) + np.where(z > 0.6 * D[None], 2.0, 0.0)
+        S = 35.0 - 0.5 * np.clip(z / 300.0, 0, 1)
+        rho = _EOS.density(T, S)
+        rho_t = rg.target_densities(rho[::-1, 3, 3], m, n_light=2)
+        dz_top = np.concatenate([np.full(m // 2, 5.0), np.full(m - m // 2, 30.0)])
+        dsigma = np.full(m, 1.0 / m)
+        for variant, extra in (("", {}), ("_window", {"dsigma": dsigma, "d_sigma": 5.0, "d_hybrid": 60.0})):
+            params = {"dz_top": dz_top, "rho_target": rho_t, "max_h_top": np.full(m, 60.0), "h_min": 0.05, **extra}
+            zw = rg.regrid_columns("hybrid", H, eta, h, rho, params, wet, n_out=m)
+            out[name + variant] = dict(rule="hybrid", H=H, eta=eta, h=h, rho=rho, wet=wet, n_out=m,
+                                       dz_top=dz_top, rho_target=rho_t, max_h_top=params["max_h_top"],
+                                       dsigma=params.get("dsigma", np.full(m, 1.0 / m)),
+                                       d_sigma=params.get("d_sigma", 0.0), d_hybrid=params.get("d_hybrid", 0.0),
+                                       h_min=params["h_min"], keep=True, zw=zw)
+    n = 10
+    h = rng.uniform(1.0, 10.0, (n, ny, nx))
+    for rule, params in (("zstar", {"dz_top": rng.uniform(2.0, 20.0, n)}),
+                         ("sigma", {"dsigma": rng.dirichlet(np.ones(n))})):
+        zw = rg.regrid_columns(rule, H, eta, h, None, params, wet)
+        out["rc_" + rule] = dict(rule=rule, H=H, eta=eta, h=h, wet=wet, zw=zw, **params)
+    return out
+
+
 def layer_transport_ext_cases():
     """The whole ALE layer-transport step with the PPM thickness flux on a periodic x axis and on periodic x and y
     axes (the reference pads its inputs by four wrapped cells and crops), and with open edges (the Flather split of
@@ -734,10 +821,10 @@ def save(name, cases):
 
 if __name__ == "__main__":
     threads.set_threads(1)
-    which = sys.argv[2:] or ["fct", "rk3", "kernels", "remap", "neighbours", "producers", "layer_transport",
-                             "layer_transport_ext"]
-    makers = {"fct": fct_cases, "rk3": rk3_cases, "kernels": kernel_cases, "remap": remap_cases,
+    which = sys.argv[2:] or ["fct", "rk3", "rk3_ext", "kernels", "remap", "neighbours", "producers", "layer_transport",
+                             "layer_transport_ext", "regrid_columns"]
+    makers = {"fct": fct_cases, "rk3": rk3_cases, "rk3_ext": rk3_ext_cases, "kernels": kernel_cases, "remap": remap_cases,
               "neighbours": neighbour_cases, "producers": producer_cases, "layer_transport": layer_transport_cases,
-              "layer_transport_ext": layer_transport_ext_cases}
+              "layer_transport_ext": layer_transport_ext_cases, "regrid_columns": regrid_columns_cases}
     for name in which:
         save(name, makers[name]())

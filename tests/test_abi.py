@@ -82,7 +82,12 @@ def test_argument_errors_are_reported_before_any_device_work():
     assert _fct_call(nx=0) == 1
     assert b"sizes" in L.pocean_last_error()
     assert _fct_call(C=None) == 1
-    assert _fct_call(flags=0x100) == 1
+    assert _fct_call(flags=0x100) == 1                          # advect's face-scheme flags are not the FCT's
+    rk3 = lambda flags: L.pocean_advect_rk3_f64(1, 1, 1, 1, 1, None, 1, None, 1, 2, 3, 4, flags, 1.0, 1, 0,  # noqa
+                                                None, 256, 1 << 20, None)
+    assert rk3(_lib.FACES_UP3 | _lib.FACES_UP1) == 1
+    assert b"exclusive" in L.pocean_last_error()
+    assert rk3(0x800) == 1
     assert _fct_call(fx=8, face_i=5) == 1                       # face_i > nx
     assert _fct_call(ws=None) == 2
     assert _fct_call(wsb=16) == 2

@@ -91,3 +91,19 @@ def test_fct_step_in_layer_blocks_on_a_periodic_box():
     ref = adv.advect_fct(_dev(w.C), _dev(w.V0), _dev(w.V1), _dev(w.Qx), _dev(w.Qy), _dev(w.ok)).cpu()
     got = adv.advect_fct(_pin(w.C), _pin(w.V0), _pin(w.V1), _pin(w.Qx), _pin(w.Qy), _pin(w.ok))
     assert torch.equal(got, ref)
+
+
+@pytest.mark.parametrize("mixed", [False, True])
+def test_fused_ale_step_equals_advect_then_remap(mixed):
+    # ale_tracer_step: advect_fct then remap_columns in one call; pinned host tensors take the overlapped path
+    # whose advected stack never leaves the device, NumPy and device tensors the one-shot paths
+    w = W.basin(seed=8, nx=256, ny=200, n=40, nt=3)
+    adv = P.TracerAdvection(scheme="weno5", time="ssprk3", dt=w.dt, precision="mixed" if mixed else "f64")
+    args = (w.C, w.V0, w.V1, w.Qx, w.Qy, w.ok)
+    ref = P.remap_columns(_dev(w.h_src), adv.advect_fct(*(_dev(a) for a in args)), _dev(w.h_tgt), 2,
+                          _dev(w.wet)).cpu()
+    got = P.ale_tracer_step(adv, *(_pin(a) for a in args), _pin(w.h_src), _pin(w.h_tgt), 2, _pin(w.wet))
+    assert got.is_pinned() and torch.equal(got, ref)
+    dev = P.ale_tracer_step(adv, *(_dev(a) for a in args), _dev(w.h_src), _dev(w.h_tgt), 2, _dev(w.wet))
+    assert dev.is_cuda and torch.equal(dev.cpu(), ref)
+    np.testing.assert_array_equal(P.ale_tracer_step(adv, *args, w.h_src, w.h_tgt, 2, w.wet), ref.numpy())

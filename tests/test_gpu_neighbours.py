@@ -7,7 +7,8 @@ import numpy as np
 import pytest
 import torch
 
-from conftest import case_periodic, load_golden
+from conftest import case_periodic, load_golden, regrid_columns_args
+import pyocean_b200 as P
 from oracle import oracle as O
 from pyocean_b200 import ALECoordinate, Periodic, diffuse_ale, face_fractions, remap_faces
 from pyocean_b200 import workloads as W
@@ -187,3 +188,46 @@ def test_full_size_regrid_remap_and_diffusion_against_oracle():
     Tw = w.C[0] - 10.0
     out = diffuse_ale(w.C[0], Tw, h, act, cx, cy, okx, oky, w.V0, 100.0, 600.0)
     np.testing.assert_array_equal(out, O.diffuse_ale(w.C[0], Tw, h, act, cx, cy, okx, oky, w.V0, 100.0, 600.0))
+
+
+RC = load_golden("regrid_columns")
+
+
+@pytest.mark.parametrize("case", sorted(RC))
+def test_regrid_columns_matches_reference_bitwise(case):
+    rec = RC[case]
+    args = regrid_columns_args(rec)
+    zw = P.regrid_columns(*args)
+    np.testing.assert_array_equal(zw, rec["zw"])
+    dev = lambda a: None if a is None else torch.from_numpy(np.ascontiguousarray(a)).cuda()   # noqa: E731
+    rule, H, eta, h, rho, params, wet, n_out = args
+    zd = P.regrid_columns(rule, dev(H), dev(eta), dev(h), dev(rho), params, dev(wet), n_out)
+    assert zd.is_cuda
+    np.testing.assert_array_equal(zd.cpu().numpy(), rec["zw"])
+
+
+def test_regrid_columns_finer_source_against_oracle_and_errors():
+    rng = np.random.default_rng(17)
+    n, m, ny, nx = 90, 40, 96, 80
+    H = rng.uniform(3.0, 500.0, (ny, nx))
+    eta = rng.uniform(-0.4, 0.4, (ny, nx))
+    wet = rng.random((ny, nx)) > 0.1
+    D = H + eta
+    w = rng.uniform(0.3, 1.7, (n, ny, nx))
+    h = w / w.sum(0) * D[None]
+    z = np.cumsum(h, axis=0) - 0.5 * h
+    rho = 1030.0 - 6.0 * np.clip(z / 400.0, 0, 1) + rng.normal(0, 0.01, (n, ny, nx))
+    rho_t = np.linspace(rho.min() - 0.5, rho.max() + 0.1, m + 1)
+    params = dict(dz_top=np.full(m, 4.0), rho_target=rho_t, max_h_top=np.full(m, 50.0), h_min=0.05,
+                  dsigma=np.full(m, 1.0 / m), d_sigma=5.0, d_hybrid=50.0)
+    zw = P.regrid_columns("hybrid", H, eta, h, rho, params, wet, n_out=m)
+    np.testing.assert_array_equal(zw, O.regrid_columns("hybrid", H, eta, h, rho, params, wet, n_out=m))
+    assert zw.shape == (m + 1, ny, nx) and np.isnan(zw[:, ~wet]).all() and np.isfinite(zw[:, wet]).all()
+    with pytest.raises(ValueError, match="only for rule 'hybrid'"):
+        P.regrid_columns("zstar", H, eta, h, None, {"dz_top": np.ones(n)}, wet, n_out=m)
+    bad = rho.copy()
+    bad[3, 5, 5] = np.nan
+    wet2 = wet.copy()
+    wet2[5, 5] = True
+    with pytest.raises(ValueError, match="non-finite density"):
+        P.regrid_columns("hybrid", H, eta, h, bad, params, wet2, n_out=m)

@@ -24,6 +24,7 @@ RTOL = 1e-12          # required parity tolerance of the plain FP64 kernels agai
 
 FCT = load_golden("fct")
 RK3 = load_golden("rk3")
+RK3X = load_golden("rk3_ext")
 REM = load_golden("remap")
 
 
@@ -35,7 +36,8 @@ def close(got, ref, rtol=RTOL):
 
 
 def _adv(rec):
-    adv = P.TracerAdvection(scheme=str(rec["scheme"]), time="ssprk3", dt=float(rec["dt"]),
+    time = str(rec["time"]) if "time" in rec else "ssprk3"
+    adv = P.TracerAdvection(scheme=str(rec["scheme"]), time=time, dt=float(rec["dt"]),
                             ob=P.OpenEdges(case_open(rec)))
     adv.per = P.Periodic(case_periodic(rec))
     return adv
@@ -80,6 +82,20 @@ def test_advect_rk3_matches_reference_bitwise(case):
                      inflow=rec.get("inflow"), flux_face_i=fi)
     out, fx = (res if fi is not None else (res, None))
     close(out, rec["out"])
+    np.testing.assert_array_equal(out, rec["out"])
+    if fx is not None:
+        np.testing.assert_array_equal(fx, rec["fx_i"])
+
+
+@pytest.mark.parametrize("case", sorted(RK3X))
+def test_advect_numpy_path_schemes_match_reference_bitwise(case):
+    """upwind3 / upwind1 faces and the 'pc' predictor-corrector step (the reference's NumPy RHS path)."""
+    rec = RK3X[case]
+    adv = _adv(rec)
+    fi = int(rec["flux_face_i"]) if "flux_face_i" in rec else None
+    res = adv.advect(rec["C"], rec["V0"], rec["V1"], rec["Qx"], rec["Qy"], rec["Fz"], rec["ok"],
+                     inflow=rec.get("inflow"), flux_face_i=fi)
+    out, fx = (res if fi is not None else (res, None))
     np.testing.assert_array_equal(out, rec["out"])
     if fx is not None:
         np.testing.assert_array_equal(fx, rec["fx_i"])
@@ -259,6 +275,25 @@ def test_advect_fct_matches_oracle_on_ragged_tiles(seed, nt, n, ny, nx, open_, p
     Fz[0] = Fz[-1] = 0.0
     np.testing.assert_array_equal(gpu.advect(C, V0, V1, Qx, Qy, Fz, ok, inflow=infl),
                                   ref.advect(C, V0, V1, Qx, Qy, Fz, ok, inflow=infl))
+
+
+@pytest.mark.parametrize("seed,nt,n,ny,nx,open_,per,inflow", CASES)
+@pytest.mark.parametrize("scheme,time", [("upwind3", "ssprk3"), ("upwind1", "ssprk3"), ("weno5", "pc"),
+                                         ("upwind3", "pc")])
+def test_advect_numpy_path_schemes_match_oracle_on_ragged_tiles(seed, nt, n, ny, nx, open_, per, inflow, scheme,
+                                                                 time):
+    C, V0, V1, Qx, Qy, ok, dt, infl = _random_case(seed, nt, n, ny, nx, open_, per, inflow)
+    ref = O.TracerAdvection(scheme=scheme, time=time, dt=dt, ob=O.OpenEdges(open_))
+    ref.per = O.Periodic(per)
+    gpu = P.TracerAdvection(scheme=scheme, time=time, dt=dt, ob=P.OpenEdges(open_))
+    gpu.per = P.Periodic(per)
+    Fz = np.random.default_rng(seed + 50).normal(size=(n + 1, ny, nx)) * 1e2
+    Fz[0] = Fz[-1] = 0.0
+    fi = nx // 3
+    g_out, g_fx = gpu.advect(C, V0, V1, Qx, Qy, Fz, ok, inflow=infl, flux_face_i=fi)
+    r_out, r_fx = ref.advect(C, V0, V1, Qx, Qy, Fz, ok, inflow=infl, flux_face_i=fi)
+    np.testing.assert_array_equal(g_out, r_out)
+    np.testing.assert_array_equal(g_fx, r_fx)
 
 
 def test_torch_tensors_stay_on_the_device():

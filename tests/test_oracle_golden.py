@@ -7,17 +7,19 @@ from __future__ import annotations
 import numpy as np
 import pytest
 
-from conftest import case_open, case_periodic, load_golden
+from conftest import case_open, case_periodic, load_golden, regrid_columns_args
 from oracle import oracle as O
 
 FCT = load_golden("fct")
 RK3 = load_golden("rk3")
+RK3X = load_golden("rk3_ext")
 KER = load_golden("kernels")
 REM = load_golden("remap")
 
 
 def _adv(rec, cls=O.TracerAdvection):
-    adv = cls(scheme=str(rec["scheme"]), time="ssprk3", dt=float(rec["dt"]), ob=O.OpenEdges(case_open(rec)))
+    time = str(rec["time"]) if "time" in rec else "ssprk3"
+    adv = cls(scheme=str(rec["scheme"]), time=time, dt=float(rec["dt"]), ob=O.OpenEdges(case_open(rec)))
     adv.per = O.Periodic(case_periodic(rec))
     return adv
 
@@ -51,6 +53,25 @@ def test_oracle_rk3_matches_reference_bitwise(case):
         np.testing.assert_array_equal(fx, rec["fx_i"])
     if not case_periodic(rec):
         np.testing.assert_array_equal(adv.rhs(rec["C"], rec["Qx"], rec["Qy"], rec["Fz"], rec["ok"]), rec["rhs"])
+
+
+@pytest.mark.parametrize("case", sorted(RK3X))
+def test_oracle_rk3_ext_matches_reference_bitwise(case):
+    """The NumPy path's upwind-3/1 faces and the 'pc' time stepping."""
+    rec = RK3X[case]
+    adv = _adv(rec)
+    fi = int(rec["flux_face_i"]) if "flux_face_i" in rec else None
+    inflow = rec.get("inflow")
+    res = adv.advect(rec["C"], rec["V0"], rec["V1"], rec["Qx"], rec["Qy"], rec["Fz"], rec["ok"], inflow=inflow,
+                     flux_face_i=fi)
+    out, fx = (res if fi is not None else (res, None))
+    np.testing.assert_array_equal(out, rec["out"])
+    if fi is not None:
+        np.testing.assert_array_equal(fx, rec["fx_i"])
+    if "rhs" in rec:
+        args = (rec["C"], rec["Qx"], rec["Qy"], rec["Fz"], rec["ok"])
+        np.testing.assert_array_equal(adv.rhs(*args, centred=True, inflow=inflow), rec["rhs_centred"])
+        np.testing.assert_array_equal(adv.rhs(*args, inflow=inflow), rec["rhs"])
 
 
 @pytest.mark.parametrize("variant", ["z", "js"])
@@ -298,3 +319,21 @@ def test_oracle_layer_transport_periodic_ppm_and_open_edges_match_reference_bitw
     for key in ("Qx", "Qy", "V0", "V1", "ok", "h_dagger"):
         np.testing.assert_array_equal(out[key], rec[key], err_msg=key)
     assert out["n_limited"] == int(rec["n_limited"])
+
+
+RC = load_golden("regrid_columns")
+
+
+@pytest.mark.parametrize("case", sorted(RC))
+def test_oracle_regrid_columns_matches_reference_bitwise(case):
+    rec = RC[case]
+    zw = O.regrid_columns(*regrid_columns_args(rec))
+    np.testing.assert_array_equal(zw, rec["zw"])
+
+
+def test_oracle_regrid_columns_raises_where_the_reference_does():
+    rec = RC["rc_zstar"]
+    with pytest.raises(ValueError, match="only for rule 'hybrid'"):
+        O.regrid_columns("zstar", rec["H"], rec["eta"], rec["h"], None, {"dz_top": rec["dz_top"]}, rec["wet"], 5)
+    with pytest.raises(ValueError, match="needs params"):
+        O.regrid_columns("sigma", rec["H"], rec["eta"], rec["h"], None, {}, rec["wet"])
