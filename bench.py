@@ -92,7 +92,8 @@ def workload_config(w, world: int) -> dict:
     return {"workload": w.name, "nt": nt, "nz": n, "ny": ny, "nx": nx,
             "remap": {0: "pcm", 1: "plm", 2: "ppm_h4"}[w.remap_scheme], "limiter": "fct",
             "weno": "z" if w.scheme == "weno5" else "js",
-            "l2": "inputs larger than L2 (210 MB stack, 105 MB per geometry array); no flush",
+            "l2": (f"inputs larger than L2 ({w.C.nbytes / 1e6:.0f} MB stack, {w.V0.nbytes / 1e6:.0f} MB per geometry "
+                   "array); no flush" if w.C.nbytes > 126e6 else "inputs smaller than L2; no flush"),
             "parallelism": f"replicas x{world}"}
 
 
@@ -318,8 +319,24 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> dict | None:
         torch.cuda.synchronize()
         return e0.elapsed_time(e1) / n
 
+    def copy_gbs(src, dst, reps=5):
+        """Bandwidth of one plain stream-ordered copy of a pinned host block (either direction)."""
+        dst.copy_(src, non_blocking=True)
+        torch.cuda.synchronize()
+        c0, c1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        c0.record(stream)
+        for _ in range(reps):
+            dst.copy_(src, non_blocking=True)
+        c1.record(stream)
+        torch.cuda.synchronize()
+        return reps * src.numel() * src.element_size() / (c0.elapsed_time(c1) / 1e3) / 1e9
+
     e2e_ms = e2e_two_ms = float("nan")
+    h2d_gbs = d2h_gbs = float("nan")
     if args.e2e_steps > 0:
+        blk = torch.empty_like(hV0, device=dev)
+        h2d_gbs, d2h_gbs = copy_gbs(hV0, blk), copy_gbs(blk, hV0.clone().pin_memory())
+        del blk
         # the step as one call (the advected stack stays on the device) ...
         e2e_ms = timed(lambda c: ale_tracer_step(adv, c, hV0, hV1, hQx, hQy, hok, hhs, hht, w.remap_scheme, hwet),
                        args.e2e_steps)
@@ -383,7 +400,12 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> dict | None:
                 "one_call": {"value": job_rate(cells, world, e2e_ms), "ms_per_step": e2e_ms,
                              "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                              "api": "pyocean_b200.ale_tracer_step (advect_fct then remap_columns in one call, the "
-                                    "advected stack kept on the device) on pinned host tensors"}},
+                                    "advected stack kept on the device) on pinned host tensors",
+                             "copy_bound_ms": 1e3 * max(h2d / h2d_gbs, d2h / d2h_gbs) / 1e9},
+                "copy_bound_ms": 1e3 * max((h2d + stack) / h2d_gbs, (d2h + stack) / d2h_gbs) / 1e9,
+                "copy_gbs": {"h2d": h2d_gbs, "d2h": d2h_gbs,
+                             "what": "one plain pinned copy of a 105 MB block each way, timed alone; the bound is the "
+                                     "larger direction's bytes at that rate (the two directions overlap)"}},
         "mixed": {"value": job_rate(cells * args.steps, world, mixed_ms), "ms_per_step": mixed_ms / args.steps,
                   "advect_fct_ms": mixed_adv, "speedup_vs_f64": ms / mixed_ms,
                   "what": "pocean_advect_fct_mixed (FP32 WENO5 weights and face values, FP64 fluxes, limiter and "

@@ -13,9 +13,16 @@ sum V0 c) and through the remap (column sums of h c), each the largest over the 
 
 The ALE sequence amplifies any perturbation of its state, whatever its source: the remap's limiters (CW84, the
 edge bounding and the discontinuity check) switch discontinuously at fronts, and the advection carries each switch
-on.  Two yardsticks measure that amplification with FP64 arithmetic only: the FP64 sequence started from initial
-fields moved by one unit in the last place (``f64_one_ulp``), and the FP64 sequence whose first step alone is the
-mixed one (``mixed_first_step_only``).  Their errors against the FP64 run are reported beside the mixed errors.
+on.  Yardsticks measure that amplification with FP64 arithmetic only, each reported as its max error against the
+FP64 run (over the tracer's range):
+
+* ``f64_one_ulp``: the FP64 sequence started from initial fields moved up by one unit in the last place;
+* ``mixed_first_step_only``: the FP64 sequence whose first step alone is the mixed one;
+* ``f64_ulp_noise_every_step``: the FP64 sequence with every value moved by one unit in the last place, up or down
+  at random (seeded), after every step — a perturbation at every step, as the mixed arithmetic makes, but ~10^6
+  times smaller than its per-step error;
+* ``f64_rel_noise_every_step``: the same with every value multiplied by 1 + e u, u uniform in [-1, 1], for
+  e = 1e-13 and 1e-10 (the mixed form's per-step error is below ~1e-10 of the range).
 """
 from __future__ import annotations
 
@@ -27,9 +34,13 @@ from . import workloads as W
 from .step import ALETracerStep
 
 
-def _run(w, dev, steps: int, mixed_steps: int, remap: bool, ulp: bool):
+REL_NOISE = (1e-13, 1e-10)
+
+
+def _run(w, dev, steps: int, mixed_steps: int, remap: bool, ulp: bool, noise: float = 0.0):
     """Final stack of `steps` steps (the first `mixed_steps` mixed, the rest FP64) and the largest relative content
-    changes through the advection and the remap."""
+    changes through the advection and the remap; ``ulp``: start one ulp up; ``noise``: after every step, -1 moves
+    every value one ulp up or down at random, e > 0 multiplies it by 1 + e u (u uniform in [-1, 1])."""
     nt, n, ny, nx = w.C.shape
     g = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)                     # noqa: E731
     V0, V1, Qx, Qy = g(w.V0), g(w.V1), g(w.Qx), g(w.Qy)
@@ -40,6 +51,10 @@ def _run(w, dev, steps: int, mixed_steps: int, remap: bool, ulp: bool):
     mix = ALETracerStep(nt, n, ny, nx, w.dt, 0, w.remap_scheme, device=dev, mixed=True) if mixed_steps else None
     c = g(np.nextafter(w.C, np.inf) if ulp else w.C)
     nxt = torch.empty_like(c)
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(12345)
+    pinf = torch.full((), np.inf, dtype=torch.float64, device=dev)
+    ninf = -pinf
     adv_err = torch.zeros(nt, dtype=torch.float64, device=dev)
     rem_err = torch.zeros(nt, dtype=torch.float64, device=dev)
     for s in range(steps):
@@ -55,6 +70,13 @@ def _run(w, dev, steps: int, mixed_steps: int, remap: bool, ulp: bool):
             rem_err = torch.maximum(rem_err, (cout - cin).abs() / cin.abs())
         else:
             nxt.copy_(a)
+        if noise < 0:
+            up = torch.rand(nxt.shape, generator=gen, device=dev) < 0.5
+            nxt.copy_(torch.where(up, torch.nextafter(nxt, pinf), torch.nextafter(nxt, ninf)))
+        elif noise > 0:
+            u = torch.rand(nxt.shape, generator=gen, device=dev, dtype=torch.float64) * 2.0 - 1.0
+            nxt.mul_(1.0 + noise * u)
+            del u
         c, nxt = nxt, c
     del f64, mix
     return c, adv_err.cpu().numpy(), rem_err.cpu().numpy()
@@ -89,7 +111,8 @@ def mixed_report(steps: int = 100, nx: int = 1024, ny: int = 1024, n: int = 75, 
         mn = torch.nan_to_num(cw, nan=np.inf).amin(dim=(1, 2, 3)).cpu().numpy()
         mxv = torch.nan_to_num(cw, nan=-np.inf).amax(dim=(1, 2, 3)).cpu().numpy()
         del mix, cw
-        ulp_mx = ulp_rms = one_mx = None
+        ulp_mx = ulp_rms = one_mx = noise_mx = None
+        rel_mx = {}
         if seq in yardsticks:
             ulp, _, _ = _run(w, dev, steps, 0, remap, True)
             ulp_mx, ulp_rms = stats(ulp - ref)
@@ -97,6 +120,13 @@ def mixed_report(steps: int = 100, nx: int = 1024, ny: int = 1024, n: int = 75, 
             one, _, _ = _run(w, dev, steps, 1, remap, False)
             one_mx, _ = stats(one - ref)
             del one
+            nz, _, _ = _run(w, dev, steps, 0, remap, False, noise=-1.0)
+            noise_mx, _ = stats(nz - ref)
+            del nz
+            for e in REL_NOISE:
+                nz, _, _ = _run(w, dev, steps, 0, remap, False, noise=e)
+                rel_mx[e], _ = stats(nz - ref)
+                del nz
         del ref
         torch.cuda.empty_cache()
         tracers = []
@@ -107,6 +137,9 @@ def mixed_report(steps: int = 100, nx: int = 1024, ny: int = 1024, n: int = 75, 
                 f64_one_ulp_max_over_range=None if ulp_mx is None else float(ulp_mx[m] / rng[m]),
                 f64_one_ulp_rms_over_range=None if ulp_rms is None else float(ulp_rms[m] / rng[m]),
                 mixed_first_step_only_max_over_range=None if one_mx is None else float(one_mx[m] / rng[m]),
+                f64_ulp_noise_every_step_max_over_range=None if noise_mx is None else float(noise_mx[m] / rng[m]),
+                f64_rel_noise_every_step_max_over_range=(None if not rel_mx else
+                                                         {f"{e:.0e}": float(v[m] / rng[m]) for e, v in rel_mx.items()}),
                 undershoot=float(max(0.0, lo[m] - mn[m])), overshoot=float(max(0.0, mxv[m] - hi[m])),
                 content_change_advect_mixed=float(adv_m[m]), content_change_advect_f64=float(adv_f[m]),
                 content_change_remap_mixed=float(rem_m[m]) if remap else None,
@@ -119,6 +152,8 @@ if __name__ == "__main__":
     import json
     import sys
     _lib.lib()
+    # python -m pyocean_b200.accuracy [steps [nx ny nz [sequence ...]]]
     steps = int(sys.argv[1]) if len(sys.argv) > 1 else 100
     size = [int(x) for x in sys.argv[2:5]] if len(sys.argv) > 4 else [1024, 1024, 75]
-    print(json.dumps(mixed_report(steps=steps, nx=size[0], ny=size[1], n=size[2])))
+    seqs = tuple(sys.argv[5:]) or ("advect", "ale")
+    print(json.dumps(mixed_report(steps=steps, nx=size[0], ny=size[1], n=size[2], sequences=seqs, yardsticks=seqs)))

@@ -120,8 +120,9 @@ class _Plan:
 
     def __del__(self) -> None:
         h = getattr(self, "handle", None)
-        if h is not None and h.value:
-            _lib.lib().pocean_batch_destroy(h)
+        L = getattr(_lib, "_LIB", None)           # None once the interpreter is shutting down
+        if h is not None and h.value and L is not None:
+            L.pocean_batch_destroy(h)
             self.handle = None
 
 

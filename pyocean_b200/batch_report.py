@@ -98,7 +98,31 @@ def batched_report(steps: int = 50, seed: int = 0, ndom: int = 64, device=None, 
     return out
 
 
+def idle_report(seed: int = 0, ndom: int = 64, steps: int = 20, device=None) -> dict:
+    """Two plain warm-up steps and one more plain step of the batched FP64 step (launches 19-27 of the run: under
+    an ncu launch list, the sum of their durations against the step time of the replayed graph that follows bounds
+    what any scheduling of the same passes could save between them), then that graph's device time per step."""
+    dev = torch.device("cuda", torch.cuda.current_device()) if device is None else torch.device(device)
+    doms = [Domain.from_workload(w, dev) for w in W.uneven_domains(seed=seed, ndom=ndom)]
+    batch = DomainBatch(doms)
+    stream = torch.cuda.current_stream(dev)
+    batch.step(2)
+    torch.cuda.synchronize()
+    batch.step(1)
+    torch.cuda.synchronize()
+    g = batch.capture(steps)
+    g.replay()
+    graph_ms = min(_timed(g.replay, stream) for _ in range(3)) / steps
+    del g
+    return dict(workload=f"{ndom} uneven z* boxes (seed {seed})", graph_ms_per_step=graph_ms,
+                launches_per_step=batch.launches_per_step, tracer_cells_per_step=batch.cells)
+
+
 if __name__ == "__main__":
+    # python -m pyocean_b200.batch_report [steps]   |   python -m pyocean_b200.batch_report idle
     import json
     import sys
-    print(json.dumps(batched_report(steps=int(sys.argv[1]) if len(sys.argv) > 1 else 50)))
+    if len(sys.argv) > 1 and sys.argv[1] == "idle":
+        print(json.dumps(idle_report()))
+    else:
+        print(json.dumps(batched_report(steps=int(sys.argv[1]) if len(sys.argv) > 1 else 50)))

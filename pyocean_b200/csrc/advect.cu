@@ -57,6 +57,23 @@ constexpr int NTHREADS = TI * TJ;
 #else
 #define FINAL_BOUNDS __launch_bounds__(NTHREADS)
 #endif
+// The batched coefficient and final passes have budgets of their own (the domains of a batch usually carry one
+// tracer, so a thread's loop over the tracers runs once).  The batched coefficient pass at 6 CTAs per SM (40
+// registers, spilling to L1): the 64-domain batched step 40.92 ms against 42.99 ms at ptxas's choice (68 registers,
+// 3 CTAs), 41.14 / 41.16 ms at 4 / 5 CTAs; the batched final pass keeps the single-domain budget (5 CTAs: slower).
+#ifndef POCEAN_COEFF_BATCHED_CTAS
+#define POCEAN_COEFF_BATCHED_CTAS 6
+#endif
+#ifdef POCEAN_COEFF_BATCHED_CTAS
+#define COEFF_BATCHED_BOUNDS __launch_bounds__(NTHREADS, POCEAN_COEFF_BATCHED_CTAS)
+#else
+#define COEFF_BATCHED_BOUNDS COEFF_BOUNDS
+#endif
+#ifdef POCEAN_FINAL_BATCHED_CTAS
+#define FINAL_BATCHED_BOUNDS __launch_bounds__(NTHREADS, POCEAN_FINAL_BATCHED_CTAS)
+#else
+#define FINAL_BATCHED_BOUNDS FINAL_BOUNDS
+#endif
 
 // ---------------------------------------------------------------------------------------------------------------
 // Donor-cell flux F_L of x-face gf (sigma_baroclinic.py:486-494; periodic: every face interior, face nx = face 0).
@@ -278,7 +295,7 @@ __device__ __forceinline__ void batched_tile(const BatchDomain* __restrict__ dom
     j = by * TJ + threadIdx.x / TI;
 }
 
-__global__ void COEFF_BOUNDS fct_coeff_batched(const BatchDomain* __restrict__ doms,
+__global__ void COEFF_BATCHED_BOUNDS fct_coeff_batched(const BatchDomain* __restrict__ doms,
                                                                const int* __restrict__ off, int ndom)
 {
     int d, i, j, k;
@@ -288,7 +305,7 @@ __global__ void COEFF_BOUNDS fct_coeff_batched(const BatchDomain* __restrict__ d
     coeff_body(a, i, j, k);
 }
 
-__global__ void FINAL_BOUNDS fct_final_batched(const BatchDomain* __restrict__ doms,
+__global__ void FINAL_BATCHED_BOUNDS fct_final_batched(const BatchDomain* __restrict__ doms,
                                                                const int* __restrict__ off, int ndom)
 {
     int d, i, j, k;
