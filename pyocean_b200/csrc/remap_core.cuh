@@ -19,10 +19,6 @@
 
 #include "exactdiv.cuh"
 
-#ifndef POCEAN_REMAP_PREFETCH
-#define POCEAN_REMAP_PREFETCH 0
-#endif
-
 #ifdef __CUDACC__
 #define PO_HD __host__ __device__ __forceinline__
 #define PO_HDT __host__ __device__
@@ -337,11 +333,6 @@ PO_HDT void remap_column_stream(IO& io, int n0, int n1, int scheme, int n_active
     bool last_reached = n1 == 1;      // target n1-1 reached: a vanished last target takes that cell's polynomial
     bool last_set = false;
     double a = 0.0;
-#if POCEAN_REMAP_PREFETCH
-    // thickness of target j + 1, loaded before the sweep needs it (the sweep's advance to the next target would
-    // otherwise wait for that load)
-    double ht_next = n1 > 1 ? io.ht(1) : 0.0;
-#endif
 
     for (int i = 0; i < n0; ++i) {
         // ---- polynomial of cell i (slots: 1 = i-1, 2 = i, 3 = i+1, 4 = i+2, 5 = i+3)
@@ -411,12 +402,7 @@ PO_HDT void remap_column_stream(IO& io, int n0, int n1, int scheme, int n_active
                 if (hi_t <= b && jj < n1 - 1) {
                     ++jj;
                     tl = th;
-#if POCEAN_REMAP_PREFETCH
-                    th = th + ht_next;
-                    ht_next = jj + 1 < n1 ? io.ht(jj + 1) : 0.0;
-#else
                     th = th + io.ht(jj);
-#endif
                 } else {
                     break;
                 }

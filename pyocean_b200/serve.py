@@ -8,9 +8,11 @@ time (every pass one launch over all jobs, as in ``batch.DomainBatch``).  Betwee
 arrived — in arrival order, while the HBM budget and the slot count allow — and retires the jobs that have run
 their steps, so a job that arrives while others run joins the next step instead of waiting for them (continuous
 batching, as LLM servers batch requests per decoding iteration).  Which admitted jobs a step advances is the
-policy's (``Server._select``): by default the oldest job plus the small jobs that fit beside it without slowing it
-by more than a quarter, so the long jobs of the tail keep close to their run-alone time while short jobs never wait
-behind them.  The host only enqueues work: it runs at most
+policy's (``Server._select``).  By default (``adaptive``) it depends on the backlog: while the admitted jobs'
+remaining work is short (below ``backlog_cells`` tracer cell-steps, about half a second of GPU work), the oldest job
+plus the small jobs that fit beside it without slowing it by more than a quarter, so the long jobs of the tail keep
+close to their run-alone time while short jobs never wait behind them; once the backlog is longer, every admitted
+job, so the GPU runs the largest batches and the queue drains at the batched rate.  The host only enqueues work: it runs at most
 ``max_ahead`` iterations ahead of the GPU, so the device queue never drains while jobs are active.
 
 Per job the report has the latency from arrival to the completion of its last step on the device (CUDA event
@@ -92,15 +94,16 @@ def make_domain(job: Job, device) -> Domain:
 class Server:
     """Serves a job stream; ``run`` returns the per-job and aggregate report."""
 
-    POLICIES = ("oldest_first", "all")
+    POLICIES = ("adaptive", "oldest_first", "all")
 
     def __init__(self, device=None, mixed: bool = True, batched: bool = True, max_slots: int = 256,
                  hbm_budget: int | None = None, max_ahead: int = 3, max_steps_per_iter: int = 4,
-                 tile_rows: int = 8, remap_nf: int = 2, keep_results: bool = False, policy: str = "oldest_first",
-                 fill_cells: int = 4_000_000, share: float = 0.25) -> None:
+                 tile_rows: int = 8, remap_nf: int = 2, keep_results: bool = False, policy: str = "adaptive",
+                 fill_cells: int = 4_000_000, share: float = 0.25, backlog_cells: float = 2e9) -> None:
         if policy not in self.POLICIES:
             raise ValueError(f"policy {policy!r}: use one of {self.POLICIES}")
         self.policy, self.fill_cells, self.share = policy, int(fill_cells), float(share)
+        self.backlog_cells = float(backlog_cells)
         self.device = torch.device("cuda", torch.cuda.current_device()) if device is None else torch.device(device)
         self.mixed, self.batched = bool(mixed), bool(batched)
         self.max_slots = 1 if not batched else int(max_slots)
@@ -215,14 +218,16 @@ class Server:
         """The jobs the next steps advance.  ``all``: every admitted job (processor sharing).  ``oldest_first``: the
         job that arrived first, plus the others in increasing remaining work while the combined step stays within
         max(fill_cells, (1 + share) x the oldest job's step): the oldest job is never slowed by more than ``share``
-        (so a long job's latency stays close to running it alone), and small jobs fill the GPU beside it.  One job
-        at a time (not batched): the oldest alone."""
+        (so a long job's latency stays close to running it alone), and small jobs fill the GPU beside it.
+        ``adaptive``: ``all`` while the admitted jobs' remaining tracer cell-steps exceed ``backlog_cells``, else
+        ``oldest_first``.  One job at a time (not batched): the oldest alone."""
         oldest = min(active, key=lambda j: (j.arrival, j.id))
         if not self.batched:
             return [oldest]
-        if self.policy == "all":
-            return list(active)
         cells = lambda j: j.nt * j.nz * j.ny * j.nx                                     # noqa: E731
+        if self.policy == "all" or (self.policy == "adaptive" and
+                                    sum((j.steps - j.done_steps) * cells(j) for j in active) > self.backlog_cells):
+            return list(active)
         budget = max(self.fill_cells, (1.0 + self.share) * cells(oldest))
         chosen, used = [oldest], cells(oldest)
         for j in sorted((j for j in active if j is not oldest), key=lambda j: ((j.steps - j.done_steps) * cells(j),
@@ -266,6 +271,7 @@ def serve_report(n_jobs: int = 200, rate: float = 15.0, seed: int = 0, device=No
     out["batched_mixed"] = Server(dev, mixed=True).run(stream(rate))
     out["one_at_a_time_f64"] = Server(dev, mixed=False, batched=False).run(stream(rate))
     out["batched_mixed_all_jobs_every_step"] = Server(dev, mixed=True, policy="all").run(stream(rate))
+    out["batched_mixed_oldest_first"] = Server(dev, mixed=True, policy="oldest_first").run(stream(rate))
     if batched_f64:
         out["batched_f64"] = Server(dev, mixed=False).run(stream(rate))
     out["p99_ratio_plain_vs_served"] = out["one_at_a_time_f64"]["p99_s"] / out["batched_mixed"]["p99_s"]

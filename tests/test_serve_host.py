@@ -52,7 +52,7 @@ def test_device_generator_builds_a_consistent_zstar_box():
 
 def test_oldest_first_policy_keeps_the_oldest_job_and_fills_beside_it():
     from pyocean_b200.serve import Job, Server
-    srv = Server(device="cpu", hbm_budget=1 << 30, fill_cells=1_000_000, share=0.25)
+    srv = Server(device="cpu", hbm_budget=1 << 30, fill_cells=1_000_000, share=0.25, policy="oldest_first")
     big = Job(0, 0.0, 512, 512, 50, 2, 100, 1)                       # 26 M cells a step, arrived first
     mid = Job(1, 0.1, 256, 256, 50, 2, 50, 2)                        # 6.6 M cells: does not fit beside it
     small = [Job(2 + i, 0.2 + i, 64, 64, 20, 1, 20 + i, 3 + i) for i in range(4)]   # 82 k cells each
@@ -67,3 +67,16 @@ def test_oldest_first_policy_keeps_the_oldest_job_and_fills_beside_it():
     assert chosen[0] is small[0] and late not in chosen and len(chosen) == 4
     assert Server(device="cpu", hbm_budget=1 << 30, policy="all")._select([big, mid] + small) == [big, mid] + small
     assert Server(device="cpu", hbm_budget=1 << 30, batched=False)._select([mid, big]) == [big]
+
+
+def test_adaptive_policy_batches_everything_only_behind_a_long_backlog():
+    from pyocean_b200.serve import Job, Server
+    big = Job(0, 0.0, 512, 512, 50, 2, 100, 1)                       # 26 M cells x 100 steps = 2.6e9 cell-steps
+    mid = Job(1, 0.1, 256, 256, 50, 2, 50, 2)
+    small = [Job(2 + i, 0.2 + i, 64, 64, 20, 1, 20 + i, 3 + i) for i in range(4)]
+    srv = Server(device="cpu", hbm_budget=1 << 30, fill_cells=1_000_000, backlog_cells=2e9)
+    assert srv.policy == "adaptive"
+    assert srv._select([mid, big] + small) == [mid, big] + small     # backlog 2.9e9 > 2e9: every job
+    big.done_steps = 95                                              # backlog now ~0.5e9: oldest first again
+    chosen = srv._select([mid, big] + small)
+    assert chosen[0] is big and mid not in chosen and all(s in chosen for s in small)
