@@ -51,17 +51,18 @@ def _wet_pinned(wet, ny: int, nx: int) -> bool:
             tuple(wet.shape) == (ny, nx) and wet.dtype in (torch.bool, torch.uint8))
 
 
-def _remap_pipelined(h_src, f_src, h_tgt, wet, n0, n1, ny, nx, nf, scheme, stacked, f_dev=None):
+def _remap_pipelined(h_src, f_src, h_tgt, wet, n0, n1, ny, nx, nf, scheme, stacked, f_dev=None, blocks=None):
     """remap_columns of pinned host tensors in row blocks of columns: block b's thicknesses and fields go to the
     device on one stream while block b-1 is remapped on another and block b-2's result comes back on a third.
     ``f_dev``: the fields are already on the device (nf, n0, ny, nx), made by work ordered on the compute stream;
-    their rows are copied there instead of uploaded (``f_src`` unused)."""
+    their rows are copied there instead of uploaded (``f_src`` unused).  ``blocks``: (full blocks, tail), default
+    ``_pipeline.REMAP_BLOCKS``."""
     dev = _pl.device_now()
     s_in, s_cmp, s_out = _pl.streams(dev)
     s_in.wait_stream(torch.cuda.current_stream(dev))
     out = torch.empty((nf, n1, ny, nx) if stacked else (n1, ny, nx), dtype=torch.float64, pin_memory=True)
     L, row, keep = _lib.lib(), 8 * nx, []
-    for j0, j1 in _pl.row_blocks(ny, _pl.REMAP_ROW_BLOCKS):
+    for j0, j1 in _pl.row_blocks(ny, *(blocks or _pl.REMAP_BLOCKS)):
         r = j1 - j0
         with torch.cuda.stream(s_in):
             hs = torch.empty((n0, r, nx), dtype=torch.float64, device=dev)

@@ -74,8 +74,9 @@ def ale_tracer_step(adv, C, V0, V1, Qx, Qy, ok, h_src, h_tgt, scheme: int, wet):
             and all(a.dtype == torch.float64 for a in (C, V0, V1, Qx, Qy, h_src, h_tgt))
             and ok.dtype in (torch.bool, torch.uint8) and tuple(ok.shape) in ((n, ny, nx), (ny, nx))
             and 8 * nt * n * ny * nx >= _pl.MIN_BYTES and ny >= 8 and not adv.record_open_flux):
-        A = adv._advect_fct_layered(C, V0, V1, Qx, Qy, ok, download=False)
-        return _remap_pipelined(h_src, None, h_tgt, wet, n, n1, ny, nx, nt, int(scheme), True, f_dev=A)
+        A = adv._advect_fct_layered(C, V0, V1, Qx, Qy, ok, download=False, blocks=_pl.FUSED_FCT_BLOCKS)
+        return _remap_pipelined(h_src, None, h_tgt, wet, n, n1, ny, nx, nt, int(scheme), True, f_dev=A,
+                                blocks=_pl.FUSED_REMAP_BLOCKS)
     host = not (isinstance(C, torch.Tensor) and C.is_cuda)
     if host:
         from ._device import Converter

@@ -128,13 +128,14 @@ class TracerAdvection:
             return cv.out(out)
         return cv.out(out), cv.out(fx)
 
-    def _advect_fct_layered(self, C, V0, V1, Qx, Qy, ok, download: bool = True):
+    def _advect_fct_layered(self, C, V0, V1, Qx, Qy, ok, download: bool = True, blocks=None):
         """advect_fct of pinned host tensors in blocks of layers: block b's tracers and geometry go to the device on
         the copy-in stream while the stage passes of block b-1 and the limiter passes of block b-2 run on the
         compute stream (``pocean_advect_fct_layers``: a block's limiter reads the layers either side of it) and
         finished blocks come back on the copy-out stream.  ``download=False``: the advected stack stays on the
         device and is returned as a tensor whose producing kernels are ordered on the compute stream
-        (``_pipeline.streams``), for a caller that goes on with it there."""
+        (``_pipeline.streams``), for a caller that goes on with it there.  ``blocks``: (full blocks, tail), default
+        ``_pipeline.FCT_BLOCKS``."""
         nt, n, ny, nx = C.shape
         dev = _pl.device_now()
         s_in, s_cmp, s_out = _pl.streams(dev)
@@ -176,7 +177,7 @@ class TracerAdvection:
             _pl.copy2d(out.data_ptr() + 8 * k0 * pl, 8 * n * pl, outd.data_ptr() + 8 * k0 * pl, 8 * n * pl,
                        8 * (k1 - k0) * pl, nt, s_out)
 
-        blocks = _pl.row_blocks(n, _pl.FCT_LAYER_BLOCKS)
+        blocks = _pl.row_blocks(n, *(blocks or _pl.FCT_BLOCKS))
         for b, (k0, k1) in enumerate(blocks):
             nl = k1 - k0
             _pl.copy2d(Cd.data_ptr() + 8 * k0 * pl, 8 * n * pl, C.data_ptr() + 8 * k0 * pl, 8 * n * pl, 8 * nl * pl,
