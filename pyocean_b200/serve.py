@@ -256,10 +256,11 @@ class Server:
 
 
 def serve_report(n_jobs: int = 200, rate: float = 15.0, seed: int = 0, device=None, batched_f64: bool = False,
-                 saturated: bool = True) -> dict:
+                 saturated: bool = True, policies: bool = True) -> dict:
     """Serves the seeded Poisson stream batched in mixed precision (the served form) and one job at a time with the
     plain FP64 kernels, then (``saturated``) both once more with every job arriving at once (their saturated
-    throughput); ``batched_f64`` adds the batched FP64 form.  Latencies in seconds."""
+    throughput); ``batched_f64`` adds the batched FP64 form, ``policies`` the served form under the two fixed
+    step-set policies (``all``, ``oldest_first``) beside the default one.  Latencies in seconds."""
     dev = torch.device("cuda", torch.cuda.current_device()) if device is None else torch.device(device)
     # warm-up: load the library and the kernels, fill the allocator's pools
     Server(dev).run(job_stream(8, seed=seed + 7, rate=1e9))
@@ -270,8 +271,9 @@ def serve_report(n_jobs: int = 200, rate: float = 15.0, seed: int = 0, device=No
                            "generated on the device per job"))
     out["batched_mixed"] = Server(dev, mixed=True).run(stream(rate))
     out["one_at_a_time_f64"] = Server(dev, mixed=False, batched=False).run(stream(rate))
-    out["batched_mixed_all_jobs_every_step"] = Server(dev, mixed=True, policy="all").run(stream(rate))
-    out["batched_mixed_oldest_first"] = Server(dev, mixed=True, policy="oldest_first").run(stream(rate))
+    if policies:
+        out["batched_mixed_all_jobs_every_step"] = Server(dev, mixed=True, policy="all").run(stream(rate))
+        out["batched_mixed_oldest_first"] = Server(dev, mixed=True, policy="oldest_first").run(stream(rate))
     if batched_f64:
         out["batched_f64"] = Server(dev, mixed=False).run(stream(rate))
     out["p99_ratio_plain_vs_served"] = out["one_at_a_time_f64"]["p99_s"] / out["batched_mixed"]["p99_s"]
@@ -286,9 +288,10 @@ def serve_report(n_jobs: int = 200, rate: float = 15.0, seed: int = 0, device=No
 if __name__ == "__main__":
     import json
     import sys
-    # python -m pyocean_b200.serve [jobs] [rate] [--no-saturated] [--no-batched-f64]
+    # python -m pyocean_b200.serve [jobs] [rate] [--no-saturated] [--no-batched-f64] [--no-policies]
     pos = [x for x in sys.argv[1:] if not x.startswith("--")]
     n = int(pos[0]) if pos else 200
     r = float(pos[1]) if len(pos) > 1 else 15.0
     print(json.dumps(serve_report(n, r, batched_f64="--no-batched-f64" not in sys.argv,
-                                  saturated="--no-saturated" not in sys.argv)))
+                                  saturated="--no-saturated" not in sys.argv,
+                                  policies="--no-policies" not in sys.argv)))

@@ -189,6 +189,23 @@ def test_constant_field_stays_constant(js):
     np.testing.assert_allclose(out, 1.0, rtol=0, atol=1e-12)
 
 
+@pytest.mark.parametrize("scheme,time", [("upwind3", "ssprk3"), ("upwind1", "ssprk3"), ("weno5", "pc"),
+                                         ("upwind3", "pc")])
+def test_numpy_path_schemes_keep_a_constant_field_and_conserve(scheme, time):
+    # the same identity for advect's NumPy-path schemes (tracers.py:110-151, 324-330), and tracer content
+    # conservation (sum V1 c_new = sum V0 c on a periodic box, rtol 1e-12)
+    from pyocean_b200 import workloads as W
+    w = W.zstar_box(seed=3, nx=48, ny=40, n=6, nt=2)
+    adv = _box_advection(w)
+    adv.tracer_scheme, adv.tracer_time = scheme, time
+    Fz = np.zeros((w.C.shape[1] + 1,) + w.C.shape[2:])
+    out = adv.advect(np.ones_like(w.C), w.V0, w.V1, w.Qx, w.Qy, Fz, w.ok)
+    np.testing.assert_allclose(out, 1.0, rtol=0, atol=1e-12)
+    out = adv.advect(w.C, w.V0, w.V1, w.Qx, w.Qy, Fz, w.ok)
+    for t in range(w.C.shape[0]):
+        np.testing.assert_allclose((w.V1 * out[t]).sum(), (w.V0 * w.C[t]).sum(), rtol=1e-12)
+
+
 def test_each_tracer_of_a_stack_stays_within_its_own_bounds_and_content():
     # tests/test_sigma_ale.py:1342-1360, 1375-1384: per-tracer bounds and conservation (rtol 1e-12) of a stack with
     # very different ranges, over 10 FCT steps of a periodic box
