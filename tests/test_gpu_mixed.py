@@ -83,3 +83,28 @@ def test_mixed_matches_oracle_on_ragged_open_periodic_case():
     g = gpu.advect_fct(C, V0, V1, Qx, Qy, ok, inflow=infl)
     for m in range(2):
         assert _rel_err(g[m], r[m]) <= REL_ERR
+
+
+@pytest.mark.parametrize("scale", [1e-35, 1e12])
+@pytest.mark.parametrize("scheme", ["weno5", "weno5js"])
+def test_mixed_keeps_fp64_where_fp32_would_lose_the_stencil(scale, scheme):
+    # stencils whose variation FP32 cannot carry (below 1e-30, or above 1e8 for the absolute-epsilon forms) take the
+    # FP64 arithmetic: the mixed step of a field scaled to 1e-35 or 1e12 stays within the bar of the FP64 result
+    rng = np.random.default_rng(21)
+    n, ny, nx = 3, 29, 41
+    h = rng.uniform(1.0, 5.0, (n, ny, nx))
+    V0 = 1e6 * h
+    Qx = rng.uniform(-0.4, 0.4, (n, ny, nx + 1)) * 1e3 * np.concatenate([h[..., :1], h], -1)
+    Qy = rng.uniform(-0.4, 0.4, (n, ny + 1, nx)) * 1e3 * np.concatenate([h[:, :1], h], 1)
+    Qx[..., 0] = Qx[..., -1] = 0.0
+    Qy[:, 0] = Qy[:, -1] = 0.0
+    V1 = V0 - 30.0 * (Qx[..., 1:] - Qx[..., :-1] + Qy[:, 1:] - Qy[:, :-1])
+    ok = V1 > 0
+    C = scale * (1.0 + rng.normal(0, 0.3, (2, n, ny, nx)))
+    ref = O.TracerAdvection(scheme=scheme, time="ssprk3", dt=30.0)
+    gpu = P.TracerAdvection(scheme=scheme, time="ssprk3", dt=30.0, precision="mixed")
+    r = ref.advect_fct(C, V0, V1, Qx, Qy, ok)
+    g = gpu.advect_fct(C, V0, V1, Qx, Qy, ok)
+    assert np.all(np.isfinite(g))
+    for m in range(2):
+        assert _rel_err(g[m], r[m]) <= REL_ERR
