@@ -151,6 +151,31 @@ int pocean_advect_rk3_f64(const double* C, const double* V0, const double* V1, c
                           double* fx_face, void* workspace, size_t workspace_bytes, void* stream);
 
 /*
+ * The single-stage helpers of TracerAdvection (core/components/tracers.py:139-206), which the reference runs on the
+ * arrays it is given (a periodic caller pads them first, so the periodic flags are refused here); ext: the
+ * exterior values on open edges (the reference's `ext` / `inflow`), or NULL for the field's own.
+ * pocean_advect_faces_f64: the horizontal face fluxes fx (nt, nz, ny, nx+1), fy (nt, nz, ny+1, nx) of the stack c:
+ *   kind POCEAN_HELPER_SCHEME   the advect scheme's faces — WENO5-Z, or WENO5-JS with POCEAN_WENO_JS, as
+ *                               `faces_h` (_advect_faces_h, sigma_baroclinic.py:265-321); with POCEAN_FACES_UP3 /
+ *                               _UP1 the NumPy path's upwind faces times Q (`flux_x`, tracers.py:195-206);
+ *   kind POCEAN_HELPER_CENTRED  the centred faces times Q (`flux_x(centred=True)`, _centred_faces);
+ *   kind POCEAN_HELPER_DONOR    the donor-cell fluxes of `upwind_faces_h` (tracers.py:178-193).
+ * pocean_advect_rhs_f64: -div(Q c) (nt, nz, ny, nx) with the scheme's faces (`rhs`: _advect_div for WENO5,
+ *   sigma_baroclinic.py:324-364; the NumPy RHS for the upwind schemes) or centred faces (centred != 0,
+ *   `rhs(centred=True)`), Fz (nz+1, ny, nx) or NULL; workspace pocean_advect_rhs_workspace_bytes.
+ */
+#define POCEAN_HELPER_SCHEME 0
+#define POCEAN_HELPER_CENTRED 1
+#define POCEAN_HELPER_DONOR 2
+int pocean_advect_faces_f64(const double* c, const double* Qx, const double* Qy, const uint8_t* ok,
+                            const double* ext, int nt, int nz, int ny, int nx, unsigned flags, int kind, double* fx,
+                            double* fy, void* stream);
+size_t pocean_advect_rhs_workspace_bytes(int nt, int nz, int ny, int nx);
+int pocean_advect_rhs_f64(const double* c, const double* Qx, const double* Qy, const double* Fz, const uint8_t* ok,
+                          const double* ext, int nt, int nz, int ny, int nx, unsigned flags, int centred,
+                          double* rhs, void* workspace, size_t workspace_bytes, void* stream);
+
+/*
  * Conservative remap of nfields stacked fields f_src (nfields, n0, ny, nx) from thicknesses h_src (n0, ny, nx)
  * onto h_tgt (n1, ny, nx); out (nfields, n1, ny, nx).  wet (ny, nx): dry columns are copied when n0 == n1, else
  * NaN.  scheme: POCEAN_PCM / POCEAN_PLM / POCEAN_PPM_H4.  Replaces core.vertical.remap.remap_columns

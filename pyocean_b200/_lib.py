@@ -19,6 +19,7 @@ FCT_UNLIMITED = 0x80
 FACES_UP3 = 0x100
 FACES_UP1 = 0x200
 TIME_PC = 0x400
+HELPER_SCHEME, HELPER_CENTRED, HELPER_DONOR = 0, 1, 2
 PCM, PLM, PPM_H4 = 0, 1, 2
 REGRID_ZSTAR, REGRID_SIGMA = 0, 1
 ERRORS = {1: "invalid argument", 2: "workspace", 3: "CUDA error", 4: "unsupported device", 5: "step cannot proceed"}
@@ -30,6 +31,9 @@ SIGNATURES: dict[str, tuple] = {
     "pocean_advect_fct_layers": (_I, [_I, _P, _P, _P, _P, _P, _P, _P, _I, _I, _I, _I, _U, _D, _P, _P, _Z, _I, _I, _I,
                                       _P]),
     "pocean_memcpy2d_async": (_I, [_P, _Z, _P, _Z, _Z, _Z, _P]),
+    "pocean_advect_faces_f64": (_I, [_P, _P, _P, _P, _P, _I, _I, _I, _I, _U, _I, _P, _P, _P]),
+    "pocean_advect_rhs_workspace_bytes": (_Z, [_I, _I, _I, _I]),
+    "pocean_advect_rhs_f64": (_I, [_P, _P, _P, _P, _P, _P, _I, _I, _I, _I, _U, _I, _P, _P, _Z, _P]),
     "pocean_last_error": (ctypes.c_char_p, []),
     "pocean_version": (_I, []),
     "pocean_advect_fct_workspace_bytes": (_Z, [_I, _I, _I, _I]),

@@ -622,6 +622,89 @@ __global__ void __launch_bounds__(TI * TJR) rk3_update_kernel(StepArgs a)
     }
 }
 
+// ---------------------------------------------------------------------------------------------------------------
+// The single-stage helpers of TracerAdvection (tracers.py:139-206): the horizontal face fluxes of a field
+// (`faces_h`: the WENO5 faces of _advect_faces_h; `flux_x`: the faces `rhs` differences, WENO5, the NumPy path's
+// upwind-3 / upwind-1 or centred faces; `upwind_faces_h`: donor cell) and the RHS -div(Q c) itself (`rhs`,
+// `rhs_numpy`).  The reference runs them on the arrays it is given (a periodic caller pads them first), so they
+// take no periodic flag.
+
+// x- and y-face fluxes of plane (t, k) for cell (j, i): its west and south faces, plus the east / north domain
+// faces on the last column / row.  KIND: FS_WENO, FS_UP3, FS_UP1, FS_CEN, or FACES_DONOR.
+constexpr int FACES_DONOR = 4;
+
+template <int KIND, bool ZV>
+__device__ __forceinline__ double any_x_face(const FacePlane& P, const StepArgs& a, const Shape& s, const Flags& fl,
+                                             int k, int j, int f)
+{
+    if (KIND == FACES_DONOR) return donor_x(P.c, P.e, a.Qx, s, fl, k, j, f);
+    if (KIND == FS_WENO) {
+        double F, unused;
+        x_face<ZV, false, false>(P, s, fl, j, f, F, unused);
+        return F;
+    }
+    return x_face_lin<KIND>(P, s, fl, j, f);
+}
+
+template <int KIND, bool ZV>
+__device__ __forceinline__ double any_y_face(const FacePlane& P, const StepArgs& a, const Shape& s, const Flags& fl,
+                                             int k, int f, int i)
+{
+    if (KIND == FACES_DONOR) return donor_y(P.c, P.e, a.Qy, s, fl, k, f, i);
+    if (KIND == FS_WENO) {
+        double F, unused;
+        y_face<ZV, false, false>(P, s, fl, f, i, F, unused);
+        return F;
+    }
+    return y_face_lin<KIND>(P, s, fl, f, i);
+}
+
+template <int KIND, bool ZV>
+__global__ void __launch_bounds__(TI * TJ) helper_faces_kernel(StepArgs a, double* __restrict__ fx,
+                                                               double* __restrict__ fy)
+{
+    int k, t;
+    split_plane(blockIdx.z, a.s.nt, a.tdiv, k, t);
+    const Shape s = a.s;
+    const Flags fl(a.flags);
+    const int i = blockIdx.x * TI + threadIdx.x % TI, j = blockIdx.y * TJ + threadIdx.x / TI;
+    if (i >= s.nx || j >= s.ny) return;
+    const int pl = s.ny * s.nx, xpl = s.ny * (s.nx + 1), ypl = (s.ny + 1) * s.nx, p = t * s.n + k;
+    const i64 pc = plane_at(p, pl);
+    FacePlane P;
+    P.c = a.C + pc;
+    P.e = a.inflow ? a.inflow + pc : P.c;
+    P.c0 = P.c;
+    P.e0 = P.e;
+    P.ok = a.ok + plane_at(k, pl);
+    P.qx = a.Qx + plane_at(k, xpl);
+    P.qy = a.Qy + plane_at(k, ypl);
+    double* sx = fx + plane_at(p, xpl);
+    double* sy = fy + plane_at(p, ypl);
+    const int fxo = j * (s.nx + 1) + i, fyo = j * s.nx + i;
+    sx[fxo] = any_x_face<KIND, ZV>(P, a, s, fl, k, j, i);
+    sy[fyo] = any_y_face<KIND, ZV>(P, a, s, fl, k, j, i);
+    if (i == s.nx - 1) sx[fxo + 1] = any_x_face<KIND, ZV>(P, a, s, fl, k, j, s.nx);
+    if (j == s.ny - 1) sy[fyo + s.nx] = any_y_face<KIND, ZV>(P, a, s, fl, k, s.ny, i);
+}
+
+// -div(Q c) of cell (t, k, j, i) from the stored faces, x then y then z (the reference's order, tracers.py:151 and
+// sigma_baroclinic.py:357-362).
+__global__ void __launch_bounds__(TI * TJ) helper_rhs_kernel(StepArgs a, double* __restrict__ out)
+{
+    int k, t;
+    split_plane(blockIdx.z, a.s.nt, a.tdiv, k, t);
+    const Shape s = a.s;
+    const int gi = blockIdx.x * TI + threadIdx.x % TI, gj = blockIdx.y * TJ + threadIdx.x / TI;
+    if (gi >= s.nx || gj >= s.ny) return;
+    const int pl = s.ny * s.nx, p = t * s.n + k, ij = gj * s.nx + gi;
+    const i64 w = plane_at(p, s.ny * (s.nx + 1)) + (gj * (s.nx + 1) + gi), so = plane_at(p, (s.ny + 1) * s.nx) + ij;
+    const i64 ci = plane_at(p, pl) + ij;
+    const double fzb = a.Tx[ci];
+    const double fzt = k + 1 < s.n ? a.Tx[ci + pl] : 0.0;
+    out[ci] = -(a.Sx[w + 1] - a.Sx[w] + a.Sy[so + s.nx] - a.Sy[so] + fzt - fzb);
+}
+
 }  // namespace po
 
 // =================================================================================================================
@@ -904,6 +987,98 @@ extern "C" int pocean_advect_rk3_f64(const double* C, const double* V0, const do
     else if (flags & POCEAN_FACES_UP1) launch_rk3<false, FS_UP1>(a, pc, grid, st);
     else if (flags & POCEAN_WENO_JS) launch_rk3<false, FS_WENO>(a, pc, grid, st);
     else launch_rk3<true, FS_WENO>(a, pc, grid, st);
+    return pocean_check_launch(fn);
+}
+
+// The single-stage helpers (tracers.py:139-206).  kind 0: the advect scheme's faces (WENO5-Z / -JS, or with
+// POCEAN_FACES_UP3 / _UP1 the NumPy path's upwind faces); 1: centred faces; 2: donor cell (upwind_faces_h).
+static int helper_checks(const char* fn, const void* c, const void* Qx, const void* Qy, const void* ok, int nt,
+                         int nz, int ny, int nx, unsigned flags)
+{
+    int rc = check_shape(fn, nt, nz, ny, nx);
+    if (rc) return rc;
+    if (!c || !Qx || !Qy || !ok) return pocean_fail(POCEAN_EINVAL, "%s: null input pointer", fn);
+    const unsigned allowed = POCEAN_OPEN_W | POCEAN_OPEN_E | POCEAN_OPEN_S | POCEAN_OPEN_N | POCEAN_WENO_JS |
+                             POCEAN_FACES_UP3 | POCEAN_FACES_UP1;
+    if (flags & ~allowed)
+        return pocean_fail(POCEAN_EINVAL, "%s: flag bits 0x%x not taken (the helpers do not wrap periodic axes: "
+                           "the caller pads)", fn, flags & ~allowed);
+    if ((flags & POCEAN_FACES_UP3) && (flags & POCEAN_FACES_UP1))
+        return pocean_fail(POCEAN_EINVAL, "%s: POCEAN_FACES_UP3 and POCEAN_FACES_UP1 are exclusive", fn);
+    return POCEAN_OK;
+}
+
+extern "C" int pocean_advect_faces_f64(const double* c, const double* Qx, const double* Qy, const uint8_t* ok,
+                                       const double* ext, int nt, int nz, int ny, int nx, unsigned flags, int kind,
+                                       double* fx, double* fy, void* stream)
+{
+    const char* fn = "pocean_advect_faces_f64";
+    int rc = helper_checks(fn, c, Qx, Qy, ok, nt, nz, ny, nx, flags);
+    if (rc) return rc;
+    if (kind < 0 || kind > 2) return pocean_fail(POCEAN_EINVAL, "%s: kind %d (0, 1 or 2)", fn, kind);
+    if (!fx || !fy) return pocean_fail(POCEAN_EINVAL, "%s: null output pointer", fn);
+    rc = pocean_check_device();
+    if (rc) return rc;
+    StepArgs a{};
+    a.s = Shape{nt, nz, ny, nx};
+    a.tdiv = plane_magic(nt);
+    a.flags = flags;
+    a.C = c; a.Qx = Qx; a.Qy = Qy; a.ok = ok; a.inflow = ext;
+    const dim3 grid(ceil_div(nx, TI), ceil_div(ny, TJ), nt * nz);
+    cudaStream_t st = (cudaStream_t)stream;
+    if (kind == 2) helper_faces_kernel<FACES_DONOR, true><<<grid, NTHREADS, 0, st>>>(a, fx, fy);
+    else if (kind == 1) helper_faces_kernel<FS_CEN, true><<<grid, NTHREADS, 0, st>>>(a, fx, fy);
+    else if (flags & POCEAN_FACES_UP3) helper_faces_kernel<FS_UP3, true><<<grid, NTHREADS, 0, st>>>(a, fx, fy);
+    else if (flags & POCEAN_FACES_UP1) helper_faces_kernel<FS_UP1, true><<<grid, NTHREADS, 0, st>>>(a, fx, fy);
+    else if (flags & POCEAN_WENO_JS) helper_faces_kernel<FS_WENO, false><<<grid, NTHREADS, 0, st>>>(a, fx, fy);
+    else helper_faces_kernel<FS_WENO, true><<<grid, NTHREADS, 0, st>>>(a, fx, fy);
+    return pocean_check_launch(fn);
+}
+
+extern "C" size_t pocean_advect_rhs_workspace_bytes(int nt, int nz, int ny, int nx)
+{
+    if (nt < 1 || nz < 1 || ny < 1 || nx < 1) return 0;
+    const size_t cells = (size_t)nt * nz * ny * nx * sizeof(double);
+    const size_t xf = (size_t)nt * nz * ny * (nx + 1) * sizeof(double);
+    const size_t yf = (size_t)nt * nz * (ny + 1) * nx * sizeof(double);
+    return align_up(cells) + align_up(xf) + align_up(yf);
+}
+
+extern "C" int pocean_advect_rhs_f64(const double* c, const double* Qx, const double* Qy, const double* Fz,
+                                     const uint8_t* ok, const double* ext, int nt, int nz, int ny, int nx,
+                                     unsigned flags, int centred, double* rhs, void* workspace,
+                                     size_t workspace_bytes, void* stream)
+{
+    const char* fn = "pocean_advect_rhs_f64";
+    int rc = helper_checks(fn, c, Qx, Qy, ok, nt, nz, ny, nx, flags);
+    if (rc) return rc;
+    if (!rhs) return pocean_fail(POCEAN_EINVAL, "%s: null output pointer", fn);
+    const size_t need = pocean_advect_rhs_workspace_bytes(nt, nz, ny, nx);
+    if (!workspace || workspace_bytes < need)
+        return pocean_fail(POCEAN_EWORKSPACE, "%s: workspace of %zu bytes needed, %zu given", fn, need,
+                           workspace ? workspace_bytes : (size_t)0);
+    if (((uintptr_t)workspace & 255) != 0)
+        return pocean_fail(POCEAN_EWORKSPACE, "%s: workspace not 256-byte aligned", fn);
+    rc = pocean_check_device();
+    if (rc) return rc;
+    StepArgs a{};
+    a.s = Shape{nt, nz, ny, nx};
+    a.tdiv = plane_magic(nt);
+    a.flags = flags;
+    a.C = c; a.Qx = Qx; a.Qy = Qy; a.Fz = Fz; a.ok = ok; a.inflow = ext;
+    char* w = (char*)workspace;
+    a.Tx = (double*)w; w += align_up((size_t)nt * nz * ny * nx * sizeof(double));
+    a.Sx = (double*)w; w += align_up((size_t)nt * nz * ny * (nx + 1) * sizeof(double));
+    a.Sy = (double*)w;
+    constexpr int R = POCEAN_FACE_ROWS;
+    const dim3 grid(ceil_div(nx, TI), ceil_div(ny, R), nt * nz);
+    cudaStream_t st = (cudaStream_t)stream;
+    if (centred) rk3_faces_kernel<4, false, FS_CEN, R><<<grid, TI * R, 0, st>>>(a);
+    else if (flags & POCEAN_FACES_UP3) rk3_faces_kernel<1, false, FS_UP3, R><<<grid, TI * R, 0, st>>>(a);
+    else if (flags & POCEAN_FACES_UP1) rk3_faces_kernel<1, false, FS_UP1, R><<<grid, TI * R, 0, st>>>(a);
+    else if (flags & POCEAN_WENO_JS) rk3_faces_kernel<1, false, FS_WENO, R><<<grid, TI * R, 0, st>>>(a);
+    else rk3_faces_kernel<1, true, FS_WENO, R><<<grid, TI * R, 0, st>>>(a);
+    helper_rhs_kernel<<<dim3(ceil_div(nx, TI), ceil_div(ny, TJ), nt * nz), NTHREADS, 0, st>>>(a, rhs);
     return pocean_check_launch(fn);
 }
 

@@ -258,6 +258,81 @@ class TracerAdvection:
             return out
         return out, fx
 
+    # ------------------------------------------------------------------------------------------------ helpers
+    # The single-stage helpers (tracers.py:139-206), as the reference runs them: on the arrays given, with no
+    # periodic wrap (a periodic caller pads first), the open edges of ``ob`` and their exterior values.
+    def _helper_flags(self, scheme_faces: bool) -> int:
+        f = self._flags() & ~(_lib.PERIODIC_X | _lib.PERIODIC_Y)
+        if scheme_faces and not self.tracer_scheme.startswith("weno5"):
+            f |= _lib.FACES_UP1 if self.tracer_scheme == "upwind1" else _lib.FACES_UP3
+        return f
+
+    def _faces(self, c, Qx, Qy, ok, ext, kind: int, scheme_faces: bool):
+        nt, n, ny, nx = self._shapes(c, Qx, Qy)
+        cv = Converter(c, Qx, Qy, ok, ext)
+        cd = cv.f64(c)
+        ed = None if ext is None else cv.f64(ext, (nt, n, ny, nx))
+        fx, fy = cv.empty((nt, n, ny, nx + 1)), cv.empty((nt, n, ny + 1, nx))
+        okd = cv.u8(ok, (n, ny, nx)) if ok is not None else torch.ones((n, ny, nx), dtype=torch.uint8,
+                                                                        device=cv.device)
+        rc = _lib.lib().pocean_advect_faces_f64(cd.data_ptr(), cv.f64(Qx).data_ptr(), cv.f64(Qy).data_ptr(),
+                                                okd.data_ptr(), None if ed is None else ed.data_ptr(), nt, n, ny, nx,
+                                                self._helper_flags(scheme_faces), kind, fx.data_ptr(), fy.data_ptr(),
+                                                cv.stream())
+        _lib.check(rc, "faces")
+        return cv.out(fx), cv.out(fy)
+
+    def faces_h(self, c, Qx, Qy, ok, ext=None, inflow=None):
+        """WENO5 horizontal face fluxes (fx, fy) of the stack, the terms _advect_div differences
+        (tracers.py:166-176): WENO5-Z for scheme 'weno5', WENO5-JS otherwise; ``ext``: the exterior values on
+        inflow, else ``inflow``, else the stack's own."""
+        return self._faces(c, Qx, Qy, ok, inflow if ext is None else ext, _lib.HELPER_SCHEME, False)
+
+    def upwind_faces_h(self, c, Qx, Qy, inflow=None):
+        """Donor-cell face fluxes Q c_up (the FCT low-order flux; tracers.py:178-193)."""
+        return self._faces(c, Qx, Qy, None, inflow, _lib.HELPER_DONOR, False)
+
+    def flux_x(self, c, Qx, Qy, ok, centred: bool = False, inflow=None):
+        """x-face fluxes (ntr, N, ny, nx+1) of the faces ``rhs`` differences (tracers.py:195-206)."""
+        if not centred and self.tracer_scheme.startswith("weno5"):
+            return self.faces_h(c, Qx, Qy, ok, inflow=inflow)[0]
+        return self._faces(c, Qx, Qy, ok, inflow, _lib.HELPER_CENTRED if centred else _lib.HELPER_SCHEME, True)[0]
+
+    def rhs(self, c, Qx, Qy, Fz, ok, centred: bool = False, inflow=None):
+        """Advection RHS -div(Q c) of the stack (tracers.py:153-164): the fused WENO5 RHS, or the NumPy path's
+        faces for the upwind schemes and for ``centred``."""
+        nt, n, ny, nx = self._shapes(c, Qx, Qy)
+        if Fz is not None and shape_of(Fz) != (n + 1, ny, nx):
+            raise ValueError(f"Fz shape {shape_of(Fz)} vs {(n + 1, ny, nx)}")
+        cv = Converter(c, Qx, Qy, Fz, ok, inflow)
+        ed = None if inflow is None else cv.f64(inflow, (nt, n, ny, nx))
+        out = cv.empty((nt, n, ny, nx))
+        L = _lib.lib()
+        nbytes = L.pocean_advect_rhs_workspace_bytes(nt, n, ny, nx)
+        ws = cv.workspace(nbytes)
+        Fzd = None if Fz is None else cv.f64(Fz)
+        rc = L.pocean_advect_rhs_f64(cv.f64(c).data_ptr(), cv.f64(Qx).data_ptr(), cv.f64(Qy).data_ptr(),
+                                     None if Fzd is None else Fzd.data_ptr(), cv.u8(ok, (n, ny, nx)).data_ptr(),
+                                     None if ed is None else ed.data_ptr(), nt, n, ny, nx, self._helper_flags(True),
+                                     int(bool(centred)), out.data_ptr(), ws.data_ptr(), nbytes, cv.stream())
+        _lib.check(rc, "rhs")
+        return cv.out(out)
+
+    def rhs_numpy(self, c, Qx, Qy, Fz, ok, centred: bool = False, inflow=None):
+        """The reference's NumPy RHS (tracers.py:139-151); its values are those of ``rhs`` (the reference's fused
+        and NumPy RHS agree), so this is ``rhs``."""
+        return self.rhs(c, Qx, Qy, Fz, ok, centred, inflow)
+
+    def advect_numpy(self, C, V0, V1, Qx, Qy, Fz, ok, inflow=None, flux_face_i: int | None = None):
+        """The reference's NumPy form of ``advect`` (tracers.py:303-340), the same arithmetic as ``advect``."""
+        return self.advect(C, V0, V1, Qx, Qy, Fz, ok, inflow=inflow, flux_face_i=flux_face_i)
+
+    def advect_fct_numpy(self, C, V0, V1, Qx, Qy, ok, unlimited: bool = False, inflow=None,
+                         flux_face_i: int | None = None):
+        """The reference's NumPy form of ``advect_fct`` (tracers.py:256-301), which its fused path equals bit for
+        bit: ``advect_fct``."""
+        return self.advect_fct(C, V0, V1, Qx, Qy, ok, unlimited=unlimited, inflow=inflow, flux_face_i=flux_face_i)
+
     # ------------------------------------------------------------------------------------------------ RK3
     def advect(self, C, V0, V1, Qx, Qy, Fz, ok, inflow=None, flux_face_i: int | None = None):
         """

@@ -226,6 +226,39 @@ def rk3_ext_cases():
     return out
 
 
+def helper_cases():
+    """The single-stage helpers of TracerAdvection (tracers.py:139-206) on unpadded arrays: faces_h, upwind_faces_h,
+    flux_x (scheme and centred faces), rhs (fused WENO5 or the NumPy path; centred) and rhs_numpy."""
+    out = {}
+    specs = [("weno5_open_inflow_vert", 2, 5, 9, 12, ("west", "east", "south"), True, "weno5"),
+             ("weno5js_closed", 1, 4, 8, 10, (), False, "weno5js"),
+             ("up3_open_vert", 2, 5, 8, 11, ("west", "north"), True, "upwind3"),
+             ("up1_inflow", 1, 4, 7, 9, ("east", "south"), True, "upwind1")]
+    for seed, (name, nt, n, ny, nx, open_, vert, scheme) in enumerate(specs):
+        rng = np.random.default_rng(700 + seed)
+        dt = 10.0
+        V0, V1, Qx, Qy, ok = transports(rng, nt, n, ny, nx, dt, open_)
+        Fz = rng.normal(size=(n + 1, ny, nx)) * 1e2 if vert else np.zeros((n + 1, ny, nx))
+        Fz[0] = Fz[-1] = 0.0
+        C = rng.normal(10.0, 1.0, (nt, n, ny, nx))
+        inflow = rng.normal(11.0, 1.0, C.shape) if "inflow" in name else None
+        adv = TracerAdvection(scheme=scheme, time="ssprk3", dt=dt, ob=_OB(open_))
+        okc = np.ascontiguousarray(np.broadcast_to(ok, C.shape[1:]))
+        rec = dict(C=C, Qx=Qx, Qy=Qy, Fz=Fz, ok=ok, dt=dt, scheme=scheme, open=np.array(open_, dtype="U5"),
+                   periodic=np.array((), dtype="U1"))
+        if inflow is not None:
+            rec["inflow"] = inflow
+        rec["faces_h_x"], rec["faces_h_y"] = adv.faces_h(C, Qx, Qy, okc, inflow=inflow)
+        rec["upwind_x"], rec["upwind_y"] = adv.upwind_faces_h(C, Qx, Qy, inflow=inflow)
+        rec["flux_x"] = adv.flux_x(C, Qx, Qy, ok, inflow=inflow)
+        rec["flux_x_centred"] = adv.flux_x(C, Qx, Qy, ok, centred=True, inflow=inflow)
+        rec["rhs"] = adv.rhs(C, Qx, Qy, Fz, ok, inflow=inflow)
+        rec["rhs_centred"] = adv.rhs(C, Qx, Qy, Fz, ok, centred=True, inflow=inflow)
+        rec["rhs_numpy"] = adv.rhs_numpy(C, Qx, Qy, Fz, ok, inflow=inflow)
+        out[name] = rec
+    return out
+
+
 def kernel_cases():
     """Single kernels: faces_h and the FCT coefficients (tests/test_sigma_ale.py:1396-1429 inputs)."""
     out = {}
@@ -821,9 +854,11 @@ def save(name, cases):
 
 if __name__ == "__main__":
     threads.set_threads(1)
-    which = sys.argv[2:] or ["fct", "rk3", "rk3_ext", "kernels", "remap", "neighbours", "producers", "layer_transport",
+    which = sys.argv[2:] or ["fct", "rk3", "rk3_ext", "helpers", "kernels", "remap", "neighbours", "producers",
+                             "layer_transport",
                              "layer_transport_ext", "regrid_columns"]
-    makers = {"fct": fct_cases, "rk3": rk3_cases, "rk3_ext": rk3_ext_cases, "kernels": kernel_cases, "remap": remap_cases,
+    makers = {"fct": fct_cases, "rk3": rk3_cases, "rk3_ext": rk3_ext_cases, "helpers": helper_cases,
+              "kernels": kernel_cases, "remap": remap_cases,
               "neighbours": neighbour_cases, "producers": producer_cases, "layer_transport": layer_transport_cases,
               "layer_transport_ext": layer_transport_ext_cases, "regrid_columns": regrid_columns_cases}
     for name in which:

@@ -25,6 +25,7 @@ RTOL = 1e-12          # required parity tolerance of the plain FP64 kernels agai
 FCT = load_golden("fct")
 RK3 = load_golden("rk3")
 RK3X = load_golden("rk3_ext")
+HLP = load_golden("helpers")
 REM = load_golden("remap")
 
 
@@ -99,6 +100,25 @@ def test_advect_numpy_path_schemes_match_reference_bitwise(case):
     np.testing.assert_array_equal(out, rec["out"])
     if fx is not None:
         np.testing.assert_array_equal(fx, rec["fx_i"])
+
+
+@pytest.mark.parametrize("case", sorted(HLP))
+def test_single_stage_helpers_match_reference_bitwise(case):
+    """faces_h, upwind_faces_h, flux_x, rhs, rhs_numpy (tracers.py:139-206) on unpadded arrays."""
+    rec = HLP[case]
+    adv = _adv(rec)
+    C, Qx, Qy, Fz, ok, infl = rec["C"], rec["Qx"], rec["Qy"], rec["Fz"], rec["ok"], rec.get("inflow")
+    fx, fy = adv.faces_h(C, Qx, Qy, ok, inflow=infl)
+    np.testing.assert_array_equal(fx, rec["faces_h_x"])
+    np.testing.assert_array_equal(fy, rec["faces_h_y"])
+    ux, uy = adv.upwind_faces_h(C, Qx, Qy, inflow=infl)
+    np.testing.assert_array_equal(ux, rec["upwind_x"])
+    np.testing.assert_array_equal(uy, rec["upwind_y"])
+    np.testing.assert_array_equal(adv.flux_x(C, Qx, Qy, ok, inflow=infl), rec["flux_x"])
+    np.testing.assert_array_equal(adv.flux_x(C, Qx, Qy, ok, centred=True, inflow=infl), rec["flux_x_centred"])
+    np.testing.assert_array_equal(adv.rhs(C, Qx, Qy, Fz, ok, inflow=infl), rec["rhs"])
+    np.testing.assert_array_equal(adv.rhs(C, Qx, Qy, Fz, ok, centred=True, inflow=infl), rec["rhs_centred"])
+    np.testing.assert_array_equal(adv.rhs_numpy(C, Qx, Qy, Fz, ok, inflow=infl), rec["rhs_numpy"])
 
 
 @pytest.mark.parametrize("group", ["cols", "n0n1"])

@@ -13,6 +13,7 @@ from oracle import oracle as O
 FCT = load_golden("fct")
 RK3 = load_golden("rk3")
 RK3X = load_golden("rk3_ext")
+HLP = load_golden("helpers")
 KER = load_golden("kernels")
 REM = load_golden("remap")
 
@@ -72,6 +73,27 @@ def test_oracle_rk3_ext_matches_reference_bitwise(case):
         args = (rec["C"], rec["Qx"], rec["Qy"], rec["Fz"], rec["ok"])
         np.testing.assert_array_equal(adv.rhs(*args, centred=True, inflow=inflow), rec["rhs_centred"])
         np.testing.assert_array_equal(adv.rhs(*args, inflow=inflow), rec["rhs"])
+
+
+@pytest.mark.parametrize("case", sorted(HLP))
+def test_oracle_single_stage_helpers_match_reference_bitwise(case):
+    """faces_h, upwind_faces_h, flux_x, rhs (and rhs_numpy where the oracle restates its faces)."""
+    rec = HLP[case]
+    adv = _adv(rec)
+    C, Qx, Qy, Fz, ok, infl = rec["C"], rec["Qx"], rec["Qy"], rec["Fz"], rec["ok"], rec.get("inflow")
+    okc = np.ascontiguousarray(np.broadcast_to(ok, C.shape[1:]))
+    fx, fy = adv.faces_h(C, Qx, Qy, okc, inflow=infl)
+    np.testing.assert_array_equal(fx, rec["faces_h_x"])
+    np.testing.assert_array_equal(fy, rec["faces_h_y"])
+    ux, uy = adv.upwind_faces_h(C, Qx, Qy, inflow=infl)
+    np.testing.assert_array_equal(ux, rec["upwind_x"])
+    np.testing.assert_array_equal(uy, rec["upwind_y"])
+    np.testing.assert_array_equal(adv.flux_x(C, Qx, Qy, ok, inflow=infl), rec["flux_x"])
+    np.testing.assert_array_equal(adv.flux_x(C, Qx, Qy, ok, centred=True, inflow=infl), rec["flux_x_centred"])
+    np.testing.assert_array_equal(adv.rhs(C, Qx, Qy, Fz, ok, inflow=infl), rec["rhs"])
+    np.testing.assert_array_equal(adv.rhs(C, Qx, Qy, Fz, ok, centred=True, inflow=infl), rec["rhs_centred"])
+    if not str(rec["scheme"]).startswith("weno5"):
+        np.testing.assert_array_equal(adv.rhs_numpy(C, Qx, Qy, Fz, ok, inflow=infl), rec["rhs_numpy"])
 
 
 @pytest.mark.parametrize("variant", ["z", "js"])
