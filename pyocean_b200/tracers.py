@@ -34,6 +34,7 @@ class TracerAdvection:
     """SSP-RK3 WENO5 tracer advection (with Zalesak FCT in ``advect_fct``) on frozen transports, on B200."""
 
     name = "tracer_advection"
+    role = None                     # the model's Role enum; a drop-in copies the replaced component's
     reads = ("T", "tr", "Qx", "Qy", "Fz")
     writes = ("T", "tr")
     per = NONE
@@ -49,7 +50,15 @@ class TracerAdvection:
         self.record_open_flux = False
         self.last_open_flux: np.ndarray | None = None
 
-    # ------------------------------------------------------------------------------------------------ helpers
+    # ------------------------------------------------------------------------------------------------ component
+    def check(self, ctx) -> list:
+        """The model builder's consistency check (tracers.py:104-105): nothing to report."""
+        return []
+
+    def state_fields(self) -> dict:
+        """Restart state (tracers.py:107-108): none — the component keeps nothing from step to step."""
+        return {}
+
     def _flags(self) -> int:
         opn = tuple(getattr(self.ob, "open", ()) or ())
         f = 0
