@@ -198,7 +198,8 @@ def periodic_pad(t: torch.Tensor, kind: str, px: bool, py: bool, halo: int) -> t
     shape = tuple(t.shape[:-2]) + (ny + fy + (2 * halo if py else 0), nx + fx + (2 * halo if px else 0))
     out = torch.empty(shape, dtype=t.dtype, device=t.device)
     fn = _lib.lib().pocean_periodic_pad_u8 if t.dtype == torch.uint8 else _lib.lib().pocean_periodic_pad_f64
-    _lib.check(fn(t.contiguous().data_ptr(), lead, ny, nx, fy, fx, int(py), int(px), halo, out.data_ptr(),
+    src = t.contiguous()                      # held until the launch is enqueued
+    _lib.check(fn(src.data_ptr(), lead, ny, nx, fy, fx, int(py), int(px), halo, out.data_ptr(),
                   torch.cuda.current_stream(t.device).cuda_stream), "periodic_pad")
     return out
 
@@ -210,9 +211,10 @@ def periodic_crop(t: torch.Tensor, kind: str, px: bool, py: bool, halo: int) -> 
     nx = t.shape[-1] - fx - (2 * halo if px else 0)
     lead = int(np.prod(t.shape[:-2])) if t.dim() > 2 else 1
     out = torch.empty(tuple(t.shape[:-2]) + (ny + fy, nx + fx), dtype=t.dtype, device=t.device)
-    _lib.check(_lib.lib().pocean_periodic_crop_f64(t.contiguous().data_ptr(), lead, ny, nx, fy, fx, int(py), int(px),
-                                                   halo, out.data_ptr(),
-                                                   torch.cuda.current_stream(t.device).cuda_stream), "periodic_crop")
+    src = t.contiguous()                      # held until the launch is enqueued
+    _lib.check(_lib.lib().pocean_periodic_crop_f64(src.data_ptr(), lead, ny, nx, fy, fx, int(py), int(px), halo,
+                                                   out.data_ptr(), torch.cuda.current_stream(t.device).cuda_stream),
+               "periodic_crop")
     return out
 
 

@@ -279,13 +279,15 @@ class TracerAdvection:
     def _faces(self, c, Qx, Qy, ok, ext, kind: int, scheme_faces: bool):
         nt, n, ny, nx = self._shapes(c, Qx, Qy)
         cv = Converter(c, Qx, Qy, ok, ext)
-        cd = cv.f64(c)
+        # every device buffer is held by a name until the launch is enqueued (a temporary's memory could be handed
+        # to the next upload before the kernel reads it)
+        cd, Qxd, Qyd = cv.f64(c), cv.f64(Qx), cv.f64(Qy)
         ed = None if ext is None else cv.f64(ext, (nt, n, ny, nx))
         fx, fy = cv.empty((nt, n, ny, nx + 1)), cv.empty((nt, n, ny + 1, nx))
         okd = cv.u8(ok, (n, ny, nx)) if ok is not None else torch.ones((n, ny, nx), dtype=torch.uint8,
                                                                         device=cv.device)
-        rc = _lib.lib().pocean_advect_faces_f64(cd.data_ptr(), cv.f64(Qx).data_ptr(), cv.f64(Qy).data_ptr(),
-                                                okd.data_ptr(), None if ed is None else ed.data_ptr(), nt, n, ny, nx,
+        rc = _lib.lib().pocean_advect_faces_f64(cd.data_ptr(), Qxd.data_ptr(), Qyd.data_ptr(), okd.data_ptr(),
+                                                None if ed is None else ed.data_ptr(), nt, n, ny, nx,
                                                 self._helper_flags(scheme_faces), kind, fx.data_ptr(), fy.data_ptr(),
                                                 cv.stream())
         _lib.check(rc, "faces")
@@ -319,9 +321,10 @@ class TracerAdvection:
         L = _lib.lib()
         nbytes = L.pocean_advect_rhs_workspace_bytes(nt, n, ny, nx)
         ws = cv.workspace(nbytes)
+        cd, Qxd, Qyd, okd = cv.f64(c), cv.f64(Qx), cv.f64(Qy), cv.u8(ok, (n, ny, nx))
         Fzd = None if Fz is None else cv.f64(Fz)
-        rc = L.pocean_advect_rhs_f64(cv.f64(c).data_ptr(), cv.f64(Qx).data_ptr(), cv.f64(Qy).data_ptr(),
-                                     None if Fzd is None else Fzd.data_ptr(), cv.u8(ok, (n, ny, nx)).data_ptr(),
+        rc = L.pocean_advect_rhs_f64(cd.data_ptr(), Qxd.data_ptr(), Qyd.data_ptr(),
+                                     None if Fzd is None else Fzd.data_ptr(), okd.data_ptr(),
                                      None if ed is None else ed.data_ptr(), nt, n, ny, nx, self._helper_flags(True),
                                      int(bool(centred)), out.data_ptr(), ws.data_ptr(), nbytes, cv.stream())
         _lib.check(rc, "rhs")
