@@ -185,6 +185,14 @@ int pocean_remap_columns_f64(const double* h_src, const double* f_src, const dou
                              int n0, int n1, int ny, int nx, int nfields, int scheme, double* out, void* stream);
 
 /*
+ * reconstruct (core/vertical/remap.py:234-294) of ncols columns of n cells: h and u (n, ncols), coef (n, ncols, 3),
+ * the coefficients (c0, c1, c2) of p(xi) = c0 + c1 xi + c2 xi^2 in each cell with the reference's default
+ * negligible thicknesses (H_NEGLECT, H_NEGLECT_EDGE); the scheme as given (no reduction by active cells).
+ */
+int pocean_reconstruct_f64(const double* h, const double* u, int n, long long ncols, int scheme, double* coef,
+                           void* stream);
+
+/*
  * The neighbours of the tracer step.
  *
  * Regrid + remap (ALECoordinate.regrid_remap, core/components/vertical_coordinate.py:69-78, with the z* and sigma

@@ -31,6 +31,7 @@ SIGNATURES: dict[str, tuple] = {
     "pocean_advect_fct_layers": (_I, [_I, _P, _P, _P, _P, _P, _P, _P, _I, _I, _I, _I, _U, _D, _P, _P, _Z, _I, _I, _I,
                                       _P]),
     "pocean_memcpy2d_async": (_I, [_P, _Z, _P, _Z, _Z, _Z, _P]),
+    "pocean_reconstruct_f64": (_I, [_P, _P, _I, _L, _I, _P, _P]),
     "pocean_advect_faces_f64": (_I, [_P, _P, _P, _P, _P, _I, _I, _I, _I, _U, _I, _P, _P, _P]),
     "pocean_advect_rhs_workspace_bytes": (_Z, [_I, _I, _I, _I]),
     "pocean_advect_rhs_f64": (_I, [_P, _P, _P, _P, _P, _P, _I, _I, _I, _I, _U, _I, _P, _P, _Z, _P]),

@@ -143,6 +143,28 @@ __global__ void __launch_bounds__(128) remap_general_batched(const BatchDomain* 
     remap_general_body<NMAX>(D.h_src, D.a.out, D.h_tgt, s.n, s.n, plane, m, D.remap_scheme, D.rout, c);
 }
 
+// reconstruct (remap.py:234-294) of ncols columns of n cells: h, u (n, ncols), coef (n, ncols, 3); the scheme as
+// given (PCM below 3 cells, PLM below 4 for PPM_H4, as there).
+template <int NMAX>
+__global__ void __launch_bounds__(128) reconstruct_kernel(const double* __restrict__ h, const double* __restrict__ u,
+                                                          int n, i64 ncols, int scheme, double* __restrict__ coef)
+{
+    const i64 c = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= ncols) return;
+    double hh[NMAX], uu[NMAX], c0[NMAX], c1[NMAX], c2[NMAX], e0[NMAX], e1[NMAX];
+    for (int k = 0; k < n; ++k) {
+        hh[k] = __ldg(h + (k * ncols + c));
+        uu[k] = __ldg(u + (k * ncols + c));
+    }
+    rc::reconstruct_column(hh, uu, n, scheme, c0, c1, c2, e0, e1);
+    for (int k = 0; k < n; ++k) {
+        double* o = coef + 3 * (k * ncols + c);
+        o[0] = c0[k];
+        o[1] = c1[k];
+        o[2] = c2[k];
+    }
+}
+
 }  // namespace remap
 
 // nf_mode 2: field pairs (+ the odd field); nf_mode 1: every field on its own.  nmax: the batch's deepest column.
@@ -218,5 +240,26 @@ extern "C" int pocean_remap_columns_f64(const double* h_src, const double* f_src
                                                                             nfields - 1, scheme, out);
     }
     remap_general_launch(h_src, f_src, h_tgt, n0, n1, plane, nfields, scheme, out, st);
+    return pocean_check_launch(fn);
+}
+
+extern "C" int pocean_reconstruct_f64(const double* h, const double* u, int n, long long ncols, int scheme,
+                                      double* coef, void* stream)
+{
+    const char* fn = "pocean_reconstruct_f64";
+    if (n < 1 || ncols < 1)
+        return pocean_fail(POCEAN_EINVAL, "%s: sizes must be >= 1 (n=%d ncols=%lld)", fn, n, ncols);
+    if (n > 256) return pocean_fail(POCEAN_EINVAL, "%s: at most 256 cells per column (n=%d)", fn, n);
+    if (ncols > (1ll << 40)) return pocean_fail(POCEAN_EINVAL, "%s: ncols=%lld too large", fn, ncols);
+    if (scheme < POCEAN_PCM || scheme > POCEAN_PPM_H4)
+        return pocean_fail(POCEAN_EINVAL, "%s: unknown scheme %d", fn, scheme);
+    if (!h || !u || !coef) return pocean_fail(POCEAN_EINVAL, "%s: null pointer", fn);
+    int rc = pocean_check_device();
+    if (rc) return rc;
+    cudaStream_t st = (cudaStream_t)stream;
+    const unsigned g = (unsigned)((ncols + 127) / 128);
+    if (n <= 64) remap::reconstruct_kernel<64><<<g, 128, 0, st>>>(h, u, n, (i64)ncols, scheme, coef);
+    else if (n <= 128) remap::reconstruct_kernel<128><<<g, 128, 0, st>>>(h, u, n, (i64)ncols, scheme, coef);
+    else remap::reconstruct_kernel<256><<<g, 128, 0, st>>>(h, u, n, (i64)ncols, scheme, coef);
     return pocean_check_launch(fn);
 }

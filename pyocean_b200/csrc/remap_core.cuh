@@ -525,23 +525,12 @@ PO_HDT void remap_column_dry(IO& io, int n0, int n1)
     }
 }
 
-// ------------------------------------------------------------------------------------------------------------
-// The reference's array formulation of remap_column (remap.py:306-397) for one field, with the column held in
-// thread-local arrays of NMAX entries (n0, n1 <= NMAX).  Used for the columns outside the one-pass sweep's domain
-// (a negative or NaN target thickness); same arithmetic, same results.
-template <int NMAX, class IO>
-PO_HDT void remap_column_general(IO& io, int m, int n0, int n1, int scheme)
+// reconstruct (remap.py:234-294): the coefficients (c0, c1, c2) of p(xi) = c0 + c1 xi + c2 xi^2 in each of the n0
+// cells (PCM; PLM from 3 cells on; PPM_H4 from 4: H4 edges, end values, edge bounding, discontinuity check, CW84
+// limiter); e0, e1: scratch of n0 entries.
+PO_HD void reconstruct_column(const double* h, const double* u, int n0, int sch, double* c0, double* c1, double* c2,
+                               double* e0, double* e1)
 {
-    double h[NMAX], u[NMAX], c0[NMAX], c1[NMAX], c2[NMAX], e0[NMAX], e1[NMAX];
-    double t_edge[NMAX + 1], content[NMAX], piece[NMAX + 1];
-    int piece_j[NMAX + 1];
-    int n_active = 0;
-    for (int k = 0; k < n0; ++k) {
-        h[k] = io.hs(k);
-        u[k] = io.f(m, k);
-        if (h[k] > 0.0) ++n_active;
-    }
-    const int sch = effective_scheme(n_active, scheme);
     for (int k = 0; k < n0; ++k) { c0[k] = u[k]; c1[k] = 0.0; c2[k] = 0.0; }
     if (sch == PLM && n0 >= 3) {                           // remap.py:248-262 (e0 = slp, e1 = mslp)
         e0[0] = e0[n0 - 1] = e1[0] = e1[n0 - 1] = 0.0;
@@ -569,6 +558,26 @@ PO_HDT void remap_column_general(IO& io, int m, int n0, int n1, int scheme)
         for (int k = 0; k < n0 - 1; ++k) check_pair(e1[k], e0[k + 1], u[k], u[k + 1]);
         for (int k = 1; k < n0 - 1; ++k) ppm_coef(u[k - 1], u[k], u[k + 1], e0[k], e1[k], c0[k], c1[k], c2[k]);
     }
+}
+
+// ------------------------------------------------------------------------------------------------------------
+// The reference's array formulation of remap_column (remap.py:306-397) for one field, with the column held in
+// thread-local arrays of NMAX entries (n0, n1 <= NMAX).  Used for the columns outside the one-pass sweep's domain
+// (a negative or NaN target thickness); same arithmetic, same results.
+template <int NMAX, class IO>
+PO_HDT void remap_column_general(IO& io, int m, int n0, int n1, int scheme)
+{
+    double h[NMAX], u[NMAX], c0[NMAX], c1[NMAX], c2[NMAX], e0[NMAX], e1[NMAX];
+    double t_edge[NMAX + 1], content[NMAX], piece[NMAX + 1];
+    int piece_j[NMAX + 1];
+    int n_active = 0;
+    for (int k = 0; k < n0; ++k) {
+        h[k] = io.hs(k);
+        u[k] = io.f(m, k);
+        if (h[k] > 0.0) ++n_active;
+    }
+    const int sch = effective_scheme(n_active, scheme);
+    reconstruct_column(h, u, n0, sch, c0, c1, c2, e0, e1);
     t_edge[0] = 0.0;
     for (int j = 0; j < n1; ++j) {
         t_edge[j + 1] = t_edge[j] + io.ht(j);

@@ -4,8 +4,9 @@ Conservative vertical remap with the reference's interface (core/vertical/remap.
 ``remap_columns(h_src, f_src, h_tgt, scheme, wet)`` is the drop-in for ``core.vertical.remap.remap_columns``: every
 wet column of f_src (N0, ny, nx) goes from thicknesses h_src to h_tgt (N1, ny, nx); dry columns are copied when
 N0 == N1, else NaN.  It also takes a stack of fields (nf, N0, ny, nx) remapped in one launch (the ALE step remaps
-every tracer of the stack with the same thicknesses).  ``remap_column`` is the single-column form.  Pinned host
-tensors are remapped in row blocks with the copies overlapping the kernels (``_pipeline``).
+every tracer of the stack with the same thicknesses).  ``remap_column`` is the single-column form, ``reconstruct``
+the per-cell polynomials of one column or of many.  Pinned host tensors are remapped in row blocks with the copies
+overlapping the kernels (``_pipeline``).
 """
 from __future__ import annotations
 
@@ -19,6 +20,8 @@ from ._device import Converter, shape_of
 PCM, PLM, PPM_H4 = _lib.PCM, _lib.PLM, _lib.PPM_H4
 SCHEMES = {"pcm": PCM, "plm": PLM, "ppm_h4": PPM_H4}
 MAX_LAYERS = 256
+H_NEGLECT = 1e-30          # remap.py:42-43, the negligible thicknesses the kernels are built with
+H_NEGLECT_EDGE = 1e-10
 
 
 def remap_columns(h_src, f_src, h_tgt, scheme: int, wet):
@@ -104,4 +107,31 @@ def remap_column(h_src, u_src, h_tgt, scheme: int, u_tgt=None):
     res = np.asarray(res).reshape(n1)
     if u_tgt is not None:
         u_tgt[...] = res
+    return res
+
+
+def reconstruct(h, u, scheme: int, h_neglect: float = H_NEGLECT, h_neglect_edge: float = H_NEGLECT_EDGE,
+                coef=None):
+    """The polynomial p(xi) = c0 + c1 xi + c2 xi^2 of every cell (remap.py:234-294): h, u of one column (n,) or of
+    many (n, ...) give coef (n, 3) or (n, ..., 3); ``coef``, when given, is filled as the reference fills it.  The
+    kernels carry the reference's default negligible thicknesses; other values are refused."""
+    if h_neglect != H_NEGLECT or h_neglect_edge != H_NEGLECT_EDGE:
+        raise ValueError("reconstruct: only the default h_neglect / h_neglect_edge (remap.py:42-43) are built")
+    shp = tuple(shape_of(h))
+    if tuple(shape_of(u)) != shp or len(shp) < 1:
+        raise ValueError(f"reconstruct: h {shp} and u {tuple(shape_of(u))} must have the same shape (n, ...)")
+    n = shp[0]
+    ncols = int(np.prod(shp[1:])) if len(shp) > 1 else 1
+    if n > MAX_LAYERS:
+        raise ValueError(f"reconstruct: at most {MAX_LAYERS} cells per column, got {n}")
+    if int(scheme) not in (PCM, PLM, PPM_H4):
+        raise ValueError(f"reconstruct: unknown scheme {scheme}")
+    cv = Converter(h, u)
+    hd, ud = cv.f64(h), cv.f64(u)
+    out = cv.empty(shp + (3,))
+    _lib.check(_lib.lib().pocean_reconstruct_f64(hd.data_ptr(), ud.data_ptr(), n, ncols, int(scheme),
+                                                 out.data_ptr(), cv.stream()), "reconstruct")
+    res = cv.out(out)
+    if coef is not None:
+        coef[...] = res
     return res

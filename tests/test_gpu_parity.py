@@ -102,6 +102,32 @@ def test_advect_numpy_path_schemes_match_reference_bitwise(case):
         np.testing.assert_array_equal(fx, rec["fx_i"])
 
 
+@pytest.mark.parametrize("case", ["coef_plm", "coef_ppm_h4"])
+def test_reconstruct_matches_reference_bitwise(case):
+    rec = REM[case]
+    coef = np.empty((rec["h"].size, 3))
+    got = P.reconstruct(rec["h"], rec["u"], int(rec["scheme"]), P.remap.H_NEGLECT, P.remap.H_NEGLECT_EDGE, coef)
+    np.testing.assert_array_equal(got, rec["coef"])
+    np.testing.assert_array_equal(coef, rec["coef"])
+
+
+def test_reconstruct_of_many_columns_equals_the_oracle_column_by_column():
+    rng = np.random.default_rng(31)
+    n, ny, nx = 12, 5, 7
+    h = rng.uniform(0.0, 3.0, (n, ny, nx))
+    h[3, 1, 2] = 0.0
+    h[5:9, 2, 4] = 1e-12                                      # vanished layers inside a column
+    u = rng.normal(10.0, 2.0, (n, ny, nx))
+    for scheme in (P.PCM, P.PLM, P.PPM_H4):
+        got = P.reconstruct(h, u, scheme)
+        assert got.shape == (n, ny, nx, 3)
+        for j in range(ny):
+            for i in range(nx):
+                np.testing.assert_array_equal(got[:, j, i], O.reconstruct(h[:, j, i], u[:, j, i], scheme))
+    with pytest.raises(ValueError):
+        P.reconstruct(h, u, P.PPM_H4, h_neglect=1e-20)
+
+
 @pytest.mark.parametrize("case", sorted(HLP))
 def test_single_stage_helpers_match_reference_bitwise(case):
     """faces_h, upwind_faces_h, flux_x, rhs, rhs_numpy (tracers.py:139-206) on unpadded arrays."""
