@@ -439,3 +439,42 @@ def test_basin_five_full_size_steps_bitwise():
     from pyocean_b200 import workloads as W
     w = W.basin(seed=3)
     np.testing.assert_array_equal(_gpu_steps(w, 5), _oracle_steps(w, 5))
+
+
+@pytest.mark.parametrize("nt,n,ny,nx", [(1, 1, 1, 1), (2, 1, 1, 5), (1, 3, 5, 1), (2, 2, 2, 3), (1, 6, 1, 1)])
+@pytest.mark.parametrize("scheme,time", [("weno5", "ssprk3"), ("weno5js", "ssprk3"), ("upwind3", "ssprk3"),
+                                         ("upwind1", "ssprk3"), ("weno5", "pc"), ("upwind3", "pc")])
+def test_degenerate_shapes_match_the_oracle(nt, n, ny, nx, scheme, time):
+    # single cells, single rows and columns, single layers: every stencil reaches out of the domain
+    rng = np.random.default_rng(nt * 1000 + n * 100 + ny * 10 + nx)
+    open_ = ("west", "east", "south", "north")
+    h = rng.uniform(1.0, 5.0, (n, ny, nx))
+    V0 = 1e6 * h
+    Qx = rng.uniform(-0.3, 0.3, (n, ny, nx + 1)) * 1e3
+    Qy = rng.uniform(-0.3, 0.3, (n, ny + 1, nx)) * 1e3
+    V1 = V0 - 10.0 * (Qx[..., 1:] - Qx[..., :-1] + Qy[:, 1:] - Qy[:, :-1])
+    ok = V1 > 0
+    C = rng.normal(10.0, 1.0, (nt, n, ny, nx))
+    infl = rng.normal(11.0, 1.0, C.shape)
+    Fz = rng.normal(size=(n + 1, ny, nx)) * 1e2
+    Fz[0] = Fz[-1] = 0.0
+    ref = O.TracerAdvection(scheme=scheme, time=time, dt=10.0, ob=O.OpenEdges(open_))
+    gpu = P.TracerAdvection(scheme=scheme, time=time, dt=10.0, ob=P.OpenEdges(open_))
+    np.testing.assert_array_equal(gpu.advect(C, V0, V1, Qx, Qy, Fz, ok, inflow=infl),
+                                  ref.advect(C, V0, V1, Qx, Qy, Fz, ok, inflow=infl))
+    np.testing.assert_array_equal(gpu.rhs(C, Qx, Qy, Fz, ok, inflow=infl), ref.rhs(C, Qx, Qy, Fz, ok, inflow=infl))
+    np.testing.assert_array_equal(gpu.flux_x(C, Qx, Qy, ok, centred=True, inflow=infl),
+                                  ref.flux_x(C, Qx, Qy, ok, centred=True, inflow=infl))
+    if time == "ssprk3":
+        np.testing.assert_array_equal(gpu.advect_fct(C, V0, V1, Qx, Qy, ok, inflow=infl),
+                                      ref.advect_fct(C, V0, V1, Qx, Qy, ok, inflow=infl))
+        for a, b in zip(gpu.upwind_faces_h(C, Qx, Qy, inflow=infl), ref.upwind_faces_h(C, Qx, Qy, inflow=infl)):
+            np.testing.assert_array_equal(a, b)
+    for scheme_r in (P.PCM, P.PLM, P.PPM_H4):
+        h_tgt = rng.uniform(0.5, 2.0, (n, ny, nx))
+        h_tgt *= h.sum(0) / h_tgt.sum(0)
+        wet = np.ones((ny, nx), bool)
+        np.testing.assert_array_equal(P.remap_columns(h, C[0], h_tgt, scheme_r, wet),
+                                      O.remap_columns(h, C[0], h_tgt, scheme_r, wet))
+        np.testing.assert_array_equal(P.reconstruct(h, C[0], scheme_r)[:, 0, 0],
+                                      O.reconstruct(h[:, 0, 0], C[0][:, 0, 0], scheme_r))
