@@ -9,7 +9,8 @@ Timing of the neighbours of the tracer step at the benchmark size (512 x 512 x 5
 * the producers of the step's inputs on the u-faces: face transport thickness, transport velocity, PPM layer
   transport with the barotropic Newton correction, the outflow limiter's check (nothing to limit, its common case)
   and the Lagrangian thickness;
-* the whole layer-transport step (``producers.ALELayerTransport``) with the PPM and the donor-cell flux;
+* the whole layer-transport step (``producers.ALELayerTransport``) with the PPM and the donor-cell flux, and the
+  whole ALE tracer step on device tensors (layer transport, advect_fct, regrid and remap);
 * the unlimited RK3 step ``TracerAdvection.advect`` with a vertical transport (the secondary path).
 
     python -m pyocean_b200.neighbours_report
@@ -251,6 +252,42 @@ def _layer_transport_ms(w, dev, rng) -> dict:
         out[flux + "_ms"] = e0.elapsed_time(e1) / 3
         out[flux + "_n_limited"] = lf.n_limited
     out["what"] = "ALELayerTransport on device tensors, both face axes, 512 x 512 x 50 basin layers, dt 300 s"
+
+    # the whole ALE tracer step on the device: the layer transport (PPM), advect_fct of the T/S stack on its
+    # fluxes and volumes, then the z* regrid of the Lagrangian thicknesses and the PPM_H4 remap of the stack; no
+    # array leaves HBM between the three
+    from .tracers import TracerAdvection
+    L = _lib.lib()
+    nt = w.C.shape[0]
+    lt = P.ALELayerTransport(fs=fs, H=Hd, area=area, dt=300.0, thickness_flux="ppm", vi_geom=geom)
+    adv = TracerAdvection(scheme="weno5", time="ssprk3", dt=300.0)
+    C = g(w.C)
+    Hn, eta0, actd = g(np.where(act, H, np.nan)), g(np.zeros((ny, nx))), g(act.astype(np.uint8))
+    dz = g(np.full(n, 4000.0 / n))
+    h_new, wet_new, C_new = torch.empty_like(hd), torch.empty((ny, nx), dtype=torch.uint8, device=dev), torch.empty_like(C)
+
+    def whole():
+        lf = lt(st, None, u[1], v[1], fl, 0.5, (), wu, wv, qe, qw, qn, qs)
+        A = adv.advect_fct(C, lf.V0, lf.V1, lf.Qx, lf.Qy, lf.ok)
+        _lib.check(L.pocean_regrid_remap_f64(0, Hn.data_ptr(), eta0.data_ptr(), lf.h_dagger.data_ptr(),
+                                             actd.data_ptr(), dz.data_ptr(), 1e-3, A.data_ptr(), n, ny, nx, nt, 2,
+                                             h_new.data_ptr(), wet_new.data_ptr(), C_new.data_ptr(), None,
+                                             torch.cuda.current_stream(dev).cuda_stream), "regrid_remap")
+        return A
+
+    whole()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(3):
+        whole()
+    e1.record()
+    e1.synchronize()
+    ms = e0.elapsed_time(e1) / 3
+    out["whole_ale_step"] = dict(ms=ms, tracer_cell_steps_per_s=nt * n * ny * nx / (ms / 1e3),
+                                 finite=bool(torch.isfinite(C_new).all()),
+                                 what="layer transport (PPM) + advect_fct of T and S + z* regrid and PPM_H4 remap, "
+                                      "all on device tensors")
     return out
 
 
