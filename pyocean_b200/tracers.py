@@ -10,7 +10,12 @@ Inputs are never modified; results are new arrays, as in the reference.
 ``upwind3`` / ``upwind1`` face schemes (any other non-WENO5 name is upwind-3, as there) and the ``'pc'``
 predictor-corrector time stepping (a centred half step, then a full step with the scheme's faces), in FP64 and
 bit for bit.  ``advect_fct`` uses WENO5-Z for ``scheme='weno5'`` and WENO5-JS otherwise, exactly as the reference's
-fused path does (tracers.py:176).
+fused path does (tracers.py:176).  The single-stage helpers ``faces_h``, ``upwind_faces_h``, ``flux_x``, ``rhs``,
+``rhs_numpy`` and the NumPy-named step methods, which ``SigmaBaroclinic`` delegates to, are here too.
+
+Not provided: the per-axis face-value functions ``faces`` and ``open_faces`` (tracers.py:110-137), which the
+reference calls only from inside ``rhs_numpy`` and ``flux_x`` (and from two ``SigmaBaroclinic`` delegators that
+nothing calls); their results reach the caller through ``rhs``, ``rhs_numpy`` and ``flux_x``.
 """
 from __future__ import annotations
 
