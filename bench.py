@@ -66,7 +66,7 @@ def parse():
     ap.add_argument("--workload", default="basin", choices=["basin", "zstar_box"])
     ap.add_argument("--basin-size", type=int, nargs=3, default=[512, 512, 50], metavar=("NX", "NY", "NZ"),
                     help="size of the basin workload (a smaller one for profiling captures)")
-    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="budget of the CPU-baseline sample")
     ap.add_argument("--ref-seconds", type=float, default=150.0,
                     help="time budget of the timed steps of --impl reference (it stops early past it)")
@@ -305,11 +305,11 @@ def run_ours(args, rank: int, world: int, local_rank: int) -> dict | None:
     stack = int(hC.numel() * hC.element_size())
 
     def timed(step, n):
-        """Device time of n chained steps of `step` on the host arrays (after three untimed ones, which fill the
+        """Device time of n chained steps of `step` on the host arrays (after five untimed ones, which fill the
         device and pinned-host caching allocators with every block the chain holds at once: a new 210 MB pinned
         block costs ~100 ms)."""
         hc = hC
-        for _ in range(3):
+        for _ in range(5):
             hc = step(hc)
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
