@@ -185,18 +185,6 @@ int pocean_remap_columns_f64(const double* h_src, const double* f_src, const dou
                              int n0, int n1, int ny, int nx, int nfields, int scheme, double* out, void* stream);
 
 /*
- * The same remap in two passes, with the same results bit for bit: the first stores every cell's reconstruction
- * (two values per field and cell: PLM c0 and c1, PPM_H4 edge values after the limiter) in the caller's workspace,
- * the second integrates each column in one walk over its (source cell, target) pairs, so the columns of a warp
- * stay in step whatever their overlap pattern.  workspace_bytes >= pocean_remap_workspace_bytes(n0, ny, nx,
- * nfields, scheme) (0 for PCM: workspace may then be NULL), else POCEAN_EWORKSPACE.
- */
-size_t pocean_remap_workspace_bytes(int n0, int ny, int nx, int nfields, int scheme);
-int pocean_remap_columns_ws_f64(const double* h_src, const double* f_src, const double* h_tgt, const uint8_t* wet,
-                                int n0, int n1, int ny, int nx, int nfields, int scheme, double* out,
-                                void* workspace, size_t workspace_bytes, void* stream);
-
-/*
  * reconstruct (core/vertical/remap.py:234-294) of ncols columns of n cells: h and u (n, ncols), coef (n, ncols, 3),
  * the coefficients (c0, c1, c2) of p(xi) = c0 + c1 xi + c2 xi^2 in each cell with the reference's default
  * negligible thicknesses (H_NEGLECT, H_NEGLECT_EDGE); the scheme as given (no reduction by active cells).

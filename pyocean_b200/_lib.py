@@ -48,8 +48,6 @@ SIGNATURES: dict[str, tuple] = {
     "pocean_advect_rk3_f64": (_I, [_P, _P, _P, _P, _P, _P, _P, _P, _I, _I, _I, _I, _U, _D, _P, _I, _P, _P, _Z,
                                    _P]),
     "pocean_remap_columns_f64": (_I, [_P, _P, _P, _P, _I, _I, _I, _I, _I, _I, _P, _P]),
-    "pocean_remap_workspace_bytes": (_Z, [_I, _I, _I, _I, _I]),
-    "pocean_remap_columns_ws_f64": (_I, [_P, _P, _P, _P, _I, _I, _I, _I, _I, _I, _P, _P, _Z, _P]),
     "pocean_regrid_remap_f64": (_I, [_I, _P, _P, _P, _P, _P, _D, _P, _I, _I, _I, _I, _I, _P, _P, _P, _P, _P]),
     "pocean_regrid_hybrid_remap_f64": (_I, [_P, _P, _P, _P, _P, _P, _P, _P, _P, _D, _D, _D, _I, _P, _I, _I, _I, _I,
                                             _I, _P, _P, _P, _P, _P]),

@@ -31,15 +31,6 @@
 #define POCEAN_REMAP1_CTAS 7
 #endif
 #define REMAP_BOUNDS __launch_bounds__(128, NF == 1 ? POCEAN_REMAP1_CTAS : POCEAN_REMAP_CTAS)
-// Launch bounds of the two-pass form (resident CTAs of 128 threads per SM): the reconstruction pass and the walk.
-#ifndef POCEAN_REC_CTAS
-#define POCEAN_REC_CTAS 6
-#endif
-#ifndef POCEAN_EVENTS_CTAS
-#define POCEAN_EVENTS_CTAS 6
-#endif
-#define REC_BOUNDS __launch_bounds__(128, POCEAN_REC_CTAS)
-#define EVENTS_BOUNDS __launch_bounds__(128, POCEAN_EVENTS_CTAS)
 
 namespace po {
 namespace remap {
@@ -77,49 +68,6 @@ __device__ __forceinline__ void remap_stream_body(const double* __restrict__ h_s
     }
 }
 
-// The two-pass form for column c of NF fields m0 .. m0+NF-1 of nfields: PASS 0 stores the reconstruction into ws
-// (p of field m, layer k at ws[(m n0 + k) plane + c], q at ws[((nfields + m) n0 + k) plane + c]), PASS 1 reads it
-// back and integrates the column into out.
-template <int NF, typename IX, int PASS>
-__device__ __forceinline__ void remap_two_pass_body(const double* __restrict__ h_src,
-                                                    const double* __restrict__ f_src,
-                                                    const double* __restrict__ h_tgt,
-                                                    const uint8_t* __restrict__ wet, int n0, int n1, i64 plane,
-                                                    int nfields, int m0, int scheme, double* __restrict__ ws,
-                                                    double* __restrict__ out, i64 c)
-{
-    if (sizeof(IX) == 4) {
-        ColumnIO32<NF> io;
-        io.h = h_src;
-        io.t = h_tgt;
-        io.c = (int)c;
-        io.plane = (int)plane;
-#pragma unroll
-        for (int m = 0; m < NF; ++m) {
-            io.u[m] = f_src + (i64)(m0 + m) * n0 * plane;
-            io.o[m] = out + (i64)(m0 + m) * n1 * plane;
-            io.rp_[m] = ws + (i64)(m0 + m) * n0 * plane;
-            io.rq_[m] = ws + (i64)(nfields + m0 + m) * n0 * plane;
-        }
-        if (PASS == 0) reconstruct_column_io<NF>(io, wet[c] != 0, n0, scheme);
-        else remap_column_io<NF, true>(io, wet[c] != 0, n0, n1, scheme);
-    } else {
-        ColumnIO<NF> io;
-        io.h = h_src + c;
-        io.t = h_tgt + c;
-        io.plane = plane;
-#pragma unroll
-        for (int m = 0; m < NF; ++m) {
-            io.u[m] = f_src + (i64)(m0 + m) * n0 * plane + c;
-            io.o[m] = out + (i64)(m0 + m) * n1 * plane + c;
-            io.rp_[m] = ws + (i64)(m0 + m) * n0 * plane + c;
-            io.rq_[m] = ws + (i64)(nfields + m0 + m) * n0 * plane + c;
-        }
-        if (PASS == 0) reconstruct_column_io<NF>(io, wet[c] != 0, n0, scheme);
-        else remap_column_io<NF, true>(io, wet[c] != 0, n0, n1, scheme);
-    }
-}
-
 template <int NMAX>
 __device__ __forceinline__ void remap_general_body(const double* __restrict__ h_src, const double* __restrict__ f_src,
                                                    const double* __restrict__ h_tgt, int n0, int n1, i64 plane,
@@ -146,29 +94,6 @@ __global__ void REMAP_BOUNDS remap_stream_kernel(const double* __restrict__ h_sr
     const i64 c = (i64)blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= plane) return;
     remap_stream_body<NF, IX>(h_src, f_src, h_tgt, wet, n0, n1, plane, field0 + (int)blockIdx.y * NF, scheme, out, c);
-}
-
-template <int NF, typename IX>
-__global__ void REC_BOUNDS remap_rec_kernel(const double* __restrict__ h_src, const double* __restrict__ f_src,
-                                            const uint8_t* __restrict__ wet, int n0, i64 plane, int nfields,
-                                            int field0, int scheme, double* __restrict__ ws)
-{
-    const i64 c = (i64)blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= plane) return;
-    remap_two_pass_body<NF, IX, 0>(h_src, f_src, nullptr, wet, n0, 0, plane, nfields, field0 + (int)blockIdx.y * NF,
-                                   scheme, ws, nullptr, c);
-}
-
-template <int NF, typename IX>
-__global__ void EVENTS_BOUNDS remap_events_kernel(const double* __restrict__ h_src, const double* __restrict__ f_src,
-                                                  const double* __restrict__ h_tgt, const uint8_t* __restrict__ wet,
-                                                  int n0, int n1, i64 plane, int nfields, int field0, int scheme,
-                                                  double* __restrict__ ws, double* __restrict__ out)
-{
-    const i64 c = (i64)blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= plane) return;
-    remap_two_pass_body<NF, IX, 1>(h_src, f_src, h_tgt, wet, n0, n1, plane, nfields, field0 + (int)blockIdx.y * NF,
-                                   scheme, ws, out, c);
 }
 
 template <int NMAX>
@@ -276,10 +201,11 @@ void remap_general_launch(const double* h_src, const double* f_src, const double
 
 using namespace po;
 
-// Argument checks shared by the remap entry points.
-static int remap_check(const char* fn, const double* h_src, const double* f_src, const double* h_tgt,
-                       const uint8_t* wet, int n0, int n1, int ny, int nx, int nfields, int scheme, double* out)
+extern "C" int pocean_remap_columns_f64(const double* h_src, const double* f_src, const double* h_tgt,
+                                        const uint8_t* wet, int n0, int n1, int ny, int nx, int nfields, int scheme,
+                                        double* out, void* stream)
 {
+    const char* fn = "pocean_remap_columns_f64";
     if (n0 < 1 || n1 < 1 || ny < 1 || nx < 1 || nfields < 1)
         return pocean_fail(POCEAN_EINVAL, "%s: sizes must be >= 1 (n0=%d n1=%d ny=%d nx=%d nfields=%d)", fn, n0, n1,
                            ny, nx, nfields);
@@ -289,15 +215,7 @@ static int remap_check(const char* fn, const double* h_src, const double* f_src,
     if (scheme < POCEAN_PCM || scheme > POCEAN_PPM_H4)
         return pocean_fail(POCEAN_EINVAL, "%s: unknown scheme %d", fn, scheme);
     if (!h_src || !f_src || !h_tgt || !wet || !out) return pocean_fail(POCEAN_EINVAL, "%s: null pointer", fn);
-    return pocean_check_device();
-}
-
-extern "C" int pocean_remap_columns_f64(const double* h_src, const double* f_src, const double* h_tgt,
-                                        const uint8_t* wet, int n0, int n1, int ny, int nx, int nfields, int scheme,
-                                        double* out, void* stream)
-{
-    const char* fn = "pocean_remap_columns_f64";
-    int rc = remap_check(fn, h_src, f_src, h_tgt, wet, n0, n1, ny, nx, nfields, scheme, out);
+    int rc = pocean_check_device();
     if (rc) return rc;
     cudaStream_t st = (cudaStream_t)stream;
     const i64 plane = (i64)ny * nx;
@@ -320,67 +238,6 @@ extern "C" int pocean_remap_columns_f64(const double* h_src, const double* f_src
         else
             remap::remap_stream_kernel<1, i64><<<dim3(gx, 1), 128, 0, st>>>(h_src, f_src, h_tgt, wet, n0, n1, plane,
                                                                             nfields - 1, scheme, out);
-    }
-    remap_general_launch(h_src, f_src, h_tgt, n0, n1, plane, nfields, scheme, out, st);
-    return pocean_check_launch(fn);
-}
-
-extern "C" size_t pocean_remap_workspace_bytes(int n0, int ny, int nx, int nfields, int scheme)
-{
-    if (n0 < 1 || ny < 1 || nx < 1 || nfields < 1 || scheme == POCEAN_PCM) return 0;
-    return (size_t)2 * (size_t)nfields * (size_t)n0 * (size_t)ny * (size_t)nx * sizeof(double);
-}
-
-extern "C" int pocean_remap_columns_ws_f64(const double* h_src, const double* f_src, const double* h_tgt,
-                                           const uint8_t* wet, int n0, int n1, int ny, int nx, int nfields,
-                                           int scheme, double* out, void* ws, size_t ws_bytes, void* stream)
-{
-    const char* fn = "pocean_remap_columns_ws_f64";
-    int rc = remap_check(fn, h_src, f_src, h_tgt, wet, n0, n1, ny, nx, nfields, scheme, out);
-    if (rc) return rc;
-    const size_t need = pocean_remap_workspace_bytes(n0, ny, nx, nfields, scheme);
-    if (need && (!ws || ws_bytes < need))
-        return pocean_fail(POCEAN_EWORKSPACE, "%s: workspace of %zu bytes given, %zu needed", fn,
-                           ws ? ws_bytes : 0, need);
-    cudaStream_t st = (cudaStream_t)stream;
-    const i64 plane = (i64)ny * nx;
-    const unsigned gx = (unsigned)((plane + 127) / 128);
-    const int pairs = nfields / 2;
-    double* w = (double*)ws;
-    const bool small = (i64)(n0 > n1 ? n0 : n1) * plane < (1ll << 31);
-    if (scheme != POCEAN_PCM) {
-        if (pairs > 0) {
-            if (small)
-                remap::remap_rec_kernel<2, int><<<dim3(gx, pairs), 128, 0, st>>>(h_src, f_src, wet, n0, plane, nfields,
-                                                                                 0, scheme, w);
-            else
-                remap::remap_rec_kernel<2, i64><<<dim3(gx, pairs), 128, 0, st>>>(h_src, f_src, wet, n0, plane, nfields,
-                                                                                 0, scheme, w);
-        }
-        if (nfields & 1) {
-            if (small)
-                remap::remap_rec_kernel<1, int><<<dim3(gx, 1), 128, 0, st>>>(h_src, f_src, wet, n0, plane, nfields,
-                                                                             nfields - 1, scheme, w);
-            else
-                remap::remap_rec_kernel<1, i64><<<dim3(gx, 1), 128, 0, st>>>(h_src, f_src, wet, n0, plane, nfields,
-                                                                             nfields - 1, scheme, w);
-        }
-    }
-    if (pairs > 0) {
-        if (small)
-            remap::remap_events_kernel<2, int><<<dim3(gx, pairs), 128, 0, st>>>(h_src, f_src, h_tgt, wet, n0, n1,
-                                                                                plane, nfields, 0, scheme, w, out);
-        else
-            remap::remap_events_kernel<2, i64><<<dim3(gx, pairs), 128, 0, st>>>(h_src, f_src, h_tgt, wet, n0, n1,
-                                                                                plane, nfields, 0, scheme, w, out);
-    }
-    if (nfields & 1) {
-        if (small)
-            remap::remap_events_kernel<1, int><<<dim3(gx, 1), 128, 0, st>>>(h_src, f_src, h_tgt, wet, n0, n1, plane,
-                                                                            nfields, nfields - 1, scheme, w, out);
-        else
-            remap::remap_events_kernel<1, i64><<<dim3(gx, 1), 128, 0, st>>>(h_src, f_src, h_tgt, wet, n0, n1, plane,
-                                                                            nfields, nfields - 1, scheme, w, out);
     }
     remap_general_launch(h_src, f_src, h_tgt, n0, n1, plane, nfields, scheme, out, st);
     return pocean_check_launch(fn);

@@ -229,8 +229,8 @@ PO_HD void check_pair(double& er_k, double& el_k1, double u_k, double u_k1)
     }
 }
 
-// Colella & Woodward limiter of an interior cell (remap.py:265-290): its final left and right edge values.
-PO_HD void ppm_limit(double u_l, double u_c, double u_r, double& el, double& er)
+// Colella & Woodward limiter and PPM coefficients of an interior cell (remap.py:265-294).
+PO_HD void ppm_coef(double u_l, double u_c, double u_r, double el, double er, double& c0, double& c1, double& c2)
 {
     if ((u_r - u_c) * (u_c - u_l) <= 0.0) {
         el = u_c;
@@ -250,21 +250,9 @@ PO_HD void ppm_limit(double u_l, double u_c, double u_r, double& el, double& er)
         el = u_c;
         er = u_c;
     }
-}
-
-// PPM coefficients of a cell from its final edge values (remap.py:291-294).
-PO_HD void ppm_poly(double u_c, double el, double er, double& c0, double& c1, double& c2)
-{
     c0 = el;
     c1 = 4.0 * (u_c - el) + 2.0 * (u_c - er);
     c2 = 3.0 * ((er - u_c) + (el - u_c));
-}
-
-// Colella & Woodward limiter and PPM coefficients of an interior cell (remap.py:265-294).
-PO_HD void ppm_coef(double u_l, double u_c, double u_r, double el, double er, double& c0, double& c1, double& c2)
-{
-    ppm_limit(u_l, u_c, u_r, el, er);
-    ppm_poly(u_c, el, er, c0, c1, c2);
 }
 
 PO_HD double average(double c0, double c1, double c2, double xa, double xb)      // remap.py:297-303
@@ -277,17 +265,16 @@ PO_HD double average(double c0, double c1, double c2, double xa, double xb)     
 }
 
 // ------------------------------------------------------------------------------------------------------------
-// The reconstruction of a column's cells in one pass with a 6-cell register window (remap.py:234-294, cell by
-// cell, bottom-up): for each cell i in order, visit(i, h_i, u_i, rec, plm, p, q) with u_i[m] = f(m, i).  rec: cell i
-// is an interior cell of a PLM or PPM_H4 column; then (p[m], q[m]) = (c0, c1) of its PLM line (plm), or its PPM_H4
-// edge values (el, er) after the H4 edges, end values, edge bounding, discontinuity check and CW84 limiter.  Any
-// other cell is constant (c0 = u_i).  sch is the column's effective scheme.
+// One-pass column remap.  IO: hs(k), ht(k), f(m, k) loads and put(m, k, v) stores; NF fields share the
+// thickness work.  Preconditions: the column is wet, has n_active >= 1 source cells with h > 0 (the last one is
+// `last`), and every target thickness is >= 0 (the caller sends other columns to the general algorithm).
 //
 // Window: slot s holds source cell i - 2 + s (s = 0..5) while cell i is processed; out-of-range slots hold 0 and
 // are never read by the formulas (each use is guarded by its cell range).
-template <int NF, class IO, class Visit>
-PO_HDT void sweep_reconstruction(IO& io, int n0, int sch, Visit& visit)
+template <int NF, class IO>
+PO_HDT void remap_column_stream(IO& io, int n0, int n1, int scheme, int n_active, int last)
 {
+    const int sch = effective_scheme(n_active, scheme);
     const bool plm = sch == PLM && n0 >= 3;
     const bool ppm = sch == PPM_H4 && n0 >= 4;
 
@@ -337,12 +324,21 @@ PO_HDT void sweep_reconstruction(IO& io, int n0, int sch, Visit& visit)
         }
     }
 
-    for (int i = 0; i < n0; ++i) {
-        // ---- reconstruction of cell i (slots: 1 = i-1, 2 = i, 3 = i+1, 4 = i+2, 5 = i+3)
-        const bool rec = (plm || ppm) && i >= 1 && i <= n0 - 2;
-        double p[NF], q[NF], u[NF];
+    // target sweep state: current target j with edges t_lo = t_edge[j], t_hi = t_edge[j+1]; acc = its content
+    int j = 0;
+    double t_lo = 0.0, t_hi = 0.0 + io.ht(0);
+    double acc[NF], last_val[NF];
 #pragma unroll
-        for (int m = 0; m < NF; ++m) { p[m] = q[m] = 0.0; u[m] = wu[m][2]; }
+    for (int m = 0; m < NF; ++m) acc[m] = last_val[m] = 0.0;
+    bool last_reached = n1 == 1;      // target n1-1 reached: a vanished last target takes that cell's polynomial
+    bool last_set = false;
+    double a = 0.0;
+
+    for (int i = 0; i < n0; ++i) {
+        // ---- polynomial of cell i (slots: 1 = i-1, 2 = i, 3 = i+1, 4 = i+2, 5 = i+3)
+        double c0[NF], c1[NF], c2[NF];
+#pragma unroll
+        for (int m = 0; m < NF; ++m) { c0[m] = wu[m][2]; c1[m] = 0.0; c2[m] = 0.0; }
         if (plm) {
             const bool have_p2 = i + 2 <= n0 - 2;                        // slope of cell i+2 is formed
             const double r2 = have_p2 ? plm_ratio(wh[3], wh[4], wh[5]) : 0.0;
@@ -353,7 +349,7 @@ PO_HDT void sweep_reconstruction(IO& io, int n0, int sch, Visit& visit)
                 const double mslp_p1 = have_m1 ? plm_monotonized(wu[m][2], wu[m][3], wu[m][4], st_a[m], st_b[m],
                                                                  slp_p2)
                                                : 0.0;
-                if (rec) plm_coef(wu[m][2], wu[m][3], st_c[m], mslp_p1, st_b[m], p[m], q[m]);
+                if (i >= 1 && i <= n0 - 2) plm_coef(wu[m][2], wu[m][3], st_c[m], mslp_p1, st_b[m], c0[m], c1[m]);
                 st_a[m] = st_b[m];
                 st_b[m] = slp_p2;
                 st_c[m] = mslp_p1;
@@ -381,16 +377,110 @@ PO_HDT void sweep_reconstruction(IO& io, int n0, int sch, Visit& visit)
                     el_next = bound_edge(e_ip1, wu[m][2], wu[m][3], sl_n, -1.0);
                     check_pair(er, el_next, wu[m][2], wu[m][3]);
                 }
-                p[m] = st_a[m];
-                q[m] = er;
-                if (rec) ppm_limit(wu[m][1], wu[m][2], wu[m][3], p[m], q[m]);
+                if (i >= 1 && i <= n0 - 2) ppm_coef(wu[m][1], wu[m][2], wu[m][3], st_a[m], er, c0[m], c1[m], c2[m]);
                 st_a[m] = el_next;
                 st_b[m] = sl_n;
                 st_c[m] = e_ip2;
             }
         }
-        visit(i, wh[2], u, rec, plm, p, q);
 
+        // ---- integrate cell i over the targets it overlaps (remap.py:331-367)
+        const double hi = wh[2];
+        if (hi > 0.0) {
+            const double b = a + hi;
+            // pass 1: which targets the cell reaches, and the first thickest piece
+            int jj = j, jthick = -1;
+            double tl = t_lo, th = t_hi, thick = -1.0;
+            while (true) {
+                const double lo = pmax(a, tl);
+                const double hi_t = jj < n1 - 1 ? th : pmax(th, b);
+                const double L = pmin(b, hi_t) - lo;
+                if (L > 0.0 && L > thick) {
+                    thick = L;
+                    jthick = jj;
+                }
+                if (hi_t <= b && jj < n1 - 1) {
+                    ++jj;
+                    tl = th;
+                    th = th + io.ht(jj);
+                } else {
+                    break;
+                }
+            }
+            const int j_end = jj;
+            // pass 2: pieces in target order; every piece but the thickest is summed, the thickest gets the
+            // residual u h - sum (Hallberg); targets the sweep leaves behind are final and written
+            double s[NF], base_thick[NF];
+#pragma unroll
+            for (int m = 0; m < NF; ++m) s[m] = base_thick[m] = 0.0;
+            jj = j;
+            tl = t_lo;
+            th = t_hi;
+            while (true) {
+                const double lo = pmax(a, tl);
+                const double hi_t = jj < n1 - 1 ? th : pmax(th, b);
+                const double up = pmin(b, hi_t);
+                const double L = up - lo;
+                double content[NF];
+#pragma unroll
+                for (int m = 0; m < NF; ++m) content[m] = jj == j ? acc[m] : 0.0;
+                if (L > 0.0) {
+                    if (jj == jthick) {
+#pragma unroll
+                        for (int m = 0; m < NF; ++m) base_thick[m] = content[m];
+                    } else {
+                        const double xa = (lo - a) / hi, xb = (up - a) / hi;
+#pragma unroll
+                        for (int m = 0; m < NF; ++m) {
+                            const double piece = L * average(c0[m], c1[m], c2[m], xa, xb);
+                            s[m] += piece;
+                            content[m] += piece;
+                        }
+                    }
+                }
+                if (jj == j_end) {
+                    if (jj != jthick) {
+#pragma unroll
+                        for (int m = 0; m < NF; ++m) acc[m] = content[m];
+                    }
+                    break;
+                }
+                if (jj != jthick) {
+                    const double hgt = io.ht(jj);
+                    if (hgt > 0.0) {
+#pragma unroll
+                        for (int m = 0; m < NF; ++m) io.put(m, jj, content[m] / hgt);
+                    } else {                                   // vanished target: this cell's value at its position
+                        const double xi = (tl - a) / hi;
+#pragma unroll
+                        for (int m = 0; m < NF; ++m) io.put(m, jj, c0[m] + xi * (c1[m] + xi * c2[m]));
+                    }
+                }
+                ++jj;
+                tl = th;
+                th = th + io.ht(jj);
+            }
+            if (jthick >= 0) {
+                const double hgt = jthick < j_end ? io.ht(jthick) : 0.0;
+#pragma unroll
+                for (int m = 0; m < NF; ++m) {
+                    const double cth = base_thick[m] + (wu[m][2] * hi - s[m]);
+                    if (jthick < j_end) io.put(m, jthick, cth / hgt);     // a piece implies a positive thickness
+                    else acc[m] = cth;
+                }
+            }
+            if (j_end == n1 - 1) last_reached = true;
+            if (last_reached && !last_set) {                       // x = t_edge[n1-1] = tl when j_end = n1-1
+                const double xi = (tl - a) / hi;
+#pragma unroll
+                for (int m = 0; m < NF; ++m) last_val[m] = c0[m] + xi * (c1[m] + xi * c2[m]);
+                last_set = true;
+            }
+            j = j_end;
+            t_lo = tl;
+            t_hi = th;
+            a = b;
+        }
         // ---- slide the window
 #pragma unroll
         for (int s = 0; s < 5; ++s) {
@@ -403,31 +493,9 @@ PO_HDT void sweep_reconstruction(IO& io, int n0, int sch, Visit& visit)
 #pragma unroll
         for (int m = 0; m < NF; ++m) wu[m][5] = in ? io.f(m, i + 4) : 0.0;
     }
-}
 
-// The polynomial of a cell from what sweep_reconstruction gives for it.
-PO_HD void cell_poly(double u, bool rec, bool plm, double p, double q, double& c0, double& c1, double& c2)
-{
-    c0 = u;
-    c1 = 0.0;
-    c2 = 0.0;
-    if (rec) {
-        if (plm) {
-            c0 = p;
-            c1 = q;
-        } else {
-            ppm_poly(u, p, q, c0, c1, c2);
-        }
-    }
-}
-
-// The targets of a column once every source cell is integrated (remap.py:382-397): the current target j keeps its
-// content; targets above it were never reached: content 0, or (vanished) the value of the last source cell, except
-// a vanished last target reached by some cell.
-template <int NF, class IO>
-PO_HDT void finish_targets(IO& io, int n1, int j, const double (&acc)[NF], bool last_set,
-                           const double (&last_val)[NF], int last)
-{
+    // the current target keeps its content; targets above it were never reached: content 0, or (vanished) the
+    // value of the last source cell, except a vanished last target reached by some cell (remap.py:382-397)
     for (int jj = j; jj < n1; ++jj) {
         const double hgt = io.ht(jj);
 #pragma unroll
@@ -439,355 +507,6 @@ PO_HDT void finish_targets(IO& io, int n1, int j, const double (&acc)[NF], bool 
             io.put(m, jj, val);
         }
     }
-}
-
-// ------------------------------------------------------------------------------------------------------------
-// One-pass column remap.  IO: hs(k), ht(k), f(m, k) loads and put(m, k, v) stores; NF fields share the
-// thickness work.  Preconditions: the column is wet, has n_active >= 1 source cells with h > 0 (the last one is
-// `last`), and every target thickness is >= 0 (the caller sends other columns to the general algorithm).
-// Each cell, as sweep_reconstruction gives it, is integrated at once over the targets it overlaps (two passes over
-// those targets: the first finds the thickest piece, the second accumulates the others and gives the thickest the
-// residual, remap.py:359-366); finished targets are written as the sweep passes them.
-template <int NF, class IO>
-struct StreamIntegration {
-    IO& io;
-    int n1;
-    int j;                     // current target, edges t_lo = t_edge[j], t_hi = t_edge[j+1]; acc = its content
-    double t_lo, t_hi, a;
-    double acc[NF], last_val[NF];
-    bool last_reached;         // target n1-1 reached: a vanished last target takes that cell's polynomial
-    bool last_set;
-
-    PO_HD void operator()(int, double hi, const double (&u)[NF], bool rec, bool plm, const double (&p)[NF],
-                          const double (&q)[NF])
-    {
-        if (!(hi > 0.0)) return;
-        double c0[NF], c1[NF], c2[NF];
-#pragma unroll
-        for (int m = 0; m < NF; ++m) cell_poly(u[m], rec, plm, p[m], q[m], c0[m], c1[m], c2[m]);
-        const double b = a + hi;
-        // pass 1: which targets the cell reaches, and the first thickest piece (remap.py:331-367)
-        int jj = j, jthick = -1;
-        double tl = t_lo, th = t_hi, thick = -1.0;
-        while (true) {
-            const double lo = pmax(a, tl);
-            const double hi_t = jj < n1 - 1 ? th : pmax(th, b);
-            const double L = pmin(b, hi_t) - lo;
-            if (L > 0.0 && L > thick) {
-                thick = L;
-                jthick = jj;
-            }
-            if (hi_t <= b && jj < n1 - 1) {
-                ++jj;
-                tl = th;
-                th = th + io.ht(jj);
-            } else {
-                break;
-            }
-        }
-        const int j_end = jj;
-        // pass 2: pieces in target order; every piece but the thickest is summed, the thickest gets the residual
-        // u h - sum (Hallberg); targets the sweep leaves behind are final and written
-        double s[NF], base_thick[NF];
-#pragma unroll
-        for (int m = 0; m < NF; ++m) s[m] = base_thick[m] = 0.0;
-        jj = j;
-        tl = t_lo;
-        th = t_hi;
-        while (true) {
-            const double lo = pmax(a, tl);
-            const double hi_t = jj < n1 - 1 ? th : pmax(th, b);
-            const double up = pmin(b, hi_t);
-            const double L = up - lo;
-            double content[NF];
-#pragma unroll
-            for (int m = 0; m < NF; ++m) content[m] = jj == j ? acc[m] : 0.0;
-            if (L > 0.0) {
-                if (jj == jthick) {
-#pragma unroll
-                    for (int m = 0; m < NF; ++m) base_thick[m] = content[m];
-                } else {
-                    const double xa = (lo - a) / hi, xb = (up - a) / hi;
-#pragma unroll
-                    for (int m = 0; m < NF; ++m) {
-                        const double piece = L * average(c0[m], c1[m], c2[m], xa, xb);
-                        s[m] += piece;
-                        content[m] += piece;
-                    }
-                }
-            }
-            if (jj == j_end) {
-                if (jj != jthick) {
-#pragma unroll
-                    for (int m = 0; m < NF; ++m) acc[m] = content[m];
-                }
-                break;
-            }
-            if (jj != jthick) {
-                const double hgt = io.ht(jj);
-                if (hgt > 0.0) {
-#pragma unroll
-                    for (int m = 0; m < NF; ++m) io.put(m, jj, content[m] / hgt);
-                } else {                                   // vanished target: this cell's value at its position
-                    const double xi = (tl - a) / hi;
-#pragma unroll
-                    for (int m = 0; m < NF; ++m) io.put(m, jj, c0[m] + xi * (c1[m] + xi * c2[m]));
-                }
-            }
-            ++jj;
-            tl = th;
-            th = th + io.ht(jj);
-        }
-        if (jthick >= 0) {
-            const double hgt = jthick < j_end ? io.ht(jthick) : 0.0;
-#pragma unroll
-            for (int m = 0; m < NF; ++m) {
-                const double cth = base_thick[m] + (u[m] * hi - s[m]);
-                if (jthick < j_end) io.put(m, jthick, cth / hgt);     // a piece implies a positive thickness
-                else acc[m] = cth;
-            }
-        }
-        if (j_end == n1 - 1) last_reached = true;
-        if (last_reached && !last_set) {                       // x = t_edge[n1-1] = tl when j_end = n1-1
-            const double xi = (tl - a) / hi;
-#pragma unroll
-            for (int m = 0; m < NF; ++m) last_val[m] = c0[m] + xi * (c1[m] + xi * c2[m]);
-            last_set = true;
-        }
-        j = j_end;
-        t_lo = tl;
-        t_hi = th;
-        a = b;
-    }
-};
-
-template <int NF, class IO>
-PO_HDT void remap_column_stream(IO& io, int n0, int n1, int scheme, int n_active, int last)
-{
-    StreamIntegration<NF, IO> it{io, n1, 0, 0.0, 0.0 + io.ht(0), 0.0, {}, {}, n1 == 1, false};
-#pragma unroll
-    for (int m = 0; m < NF; ++m) it.acc[m] = it.last_val[m] = 0.0;
-    sweep_reconstruction<NF>(io, n0, effective_scheme(n_active, scheme), it);
-    finish_targets<NF>(io, n1, it.j, it.acc, it.last_set, it.last_val, last);
-}
-
-// ------------------------------------------------------------------------------------------------------------
-// The two-pass form of the same remap.  reconstruct_column_stream stores (p, q) of sweep_reconstruction for the
-// interior cells of a PLM / PPM_H4 column through io.rput(m, k, p, q) (nothing for a PCM column); then
-// remap_column_events integrates the column reading them back through io.rp(m, k), io.rq(m, k).  Preconditions
-// as for remap_column_stream.
-template <int NF, class IO>
-struct StoreReconstruction {
-    IO& io;
-    PO_HD void operator()(int i, double, const double (&)[NF], bool rec, bool, const double (&p)[NF],
-                          const double (&q)[NF])
-    {
-        if (!rec) return;
-#pragma unroll
-        for (int m = 0; m < NF; ++m) io.rput(m, i, p[m], q[m]);
-    }
-};
-
-template <int NF, class IO>
-PO_HDT void reconstruct_column_stream(IO& io, int n0, int scheme, int n_active)
-{
-    const int sch = effective_scheme(n_active, scheme);
-    if (!((sch == PLM && n0 >= 3) || (sch == PPM_H4 && n0 >= 4))) return;
-    StoreReconstruction<NF, IO> st{io};
-    sweep_reconstruction<NF>(io, n0, sch, st);
-}
-
-// The integration as one walk over the (source cell, target) pairs of the column in order, one pair per step:
-// every step takes at most one piece integral and writes at most one target, so the columns of a warp step in
-// lockstep whatever their overlap pattern (remap_column_stream runs a data-dependent number of target steps per
-// cell, twice).
-//
-// The piece of a cell that takes the Hallberg residual u h - (sum of the others) is the first of its longest pieces
-// (remap.py:359-366), known only when the cell ends.  So the walk holds the longest piece so far as the candidate,
-// its integral not taken; a longer piece deposes it, and the deposed piece's integral is taken (and its target,
-// which ended inside the cell, written) then.  A deposed piece added to the others' sum after two or more of them
-// would change the order of that sum against remap.py's (target order); the walk marks the cell and sums its pieces
-// again in target order when the cell ends.  With one other piece or none, the order cannot change the sum (one
-// addition commutes).  Results equal remap_column_stream's bit for bit.
-template <int NF, class IO>
-PO_HDT void remap_column_events(IO& io, int n0, int n1, int scheme, int n_active, int last)
-{
-    const int sch = effective_scheme(n_active, scheme);
-    const bool plm = sch == PLM && n0 >= 3;
-    const bool rec_col = plm || (sch == PPM_H4 && n0 >= 4);
-
-    // source cell i = [a, b], thickness hi, mean u, polynomial c0 + c1 x + c2 x^2 over x in [0, 1]
-    int i = 0;
-    double hi = io.hs(0);
-    while (!(hi > 0.0)) hi = io.hs(++i);                   // n_active >= 1
-    double a = 0.0, b = 0.0 + hi, u[NF], c0[NF], c1[NF], c2[NF];
-    {
-        const bool rec = rec_col && i >= 1 && i <= n0 - 2;
-#pragma unroll
-        for (int m = 0; m < NF; ++m) {
-            u[m] = io.f(m, i);
-            cell_poly(u[m], rec, plm, rec ? io.rp(m, i) : 0.0, rec ? io.rq(m, i) : 0.0, c0[m], c1[m], c2[m]);
-        }
-    }
-    // target j = [tl, th], thickness hj, content so far acc
-    int j = 0;
-    double hj = io.ht(0);
-    double tl = 0.0, th = 0.0 + hj;
-    double acc[NF], last_val[NF];
-#pragma unroll
-    for (int m = 0; m < NF; ++m) acc[m] = last_val[m] = 0.0;
-    bool last_reached = n1 == 1, last_set = false;
-    // the cell's pieces so far: candidate (target cand, length thick, [cand_lo, cand_up], its target's content
-    // before it base, thickness cand_h), the others' sum s (ns pieces); the cell's first target j0 = [tl0, th0]
-    int cand = -1, ns = 0, j0 = 0;
-    bool resum = false;
-    double thick = -1.0, cand_lo = 0.0, cand_up = 0.0, cand_h = 0.0, tl0 = tl, th0 = th;
-    double base[NF], s[NF];
-#pragma unroll
-    for (int m = 0; m < NF; ++m) base[m] = s[m] = 0.0;
-
-    while (true) {
-        const double lo = pmax(a, tl);
-        const double hi_t = j < n1 - 1 ? th : pmax(th, b);
-        const double up = pmin(b, hi_t);
-        const double L = up - lo;
-        const bool newc = L > 0.0 && L > thick;
-        // the one piece integral of this step: this piece, or the candidate it deposes
-        double pc[NF];
-#pragma unroll
-        for (int m = 0; m < NF; ++m) pc[m] = 0.0;
-        if (newc ? cand >= 0 : L > 0.0) {
-            const double plo = newc ? cand_lo : lo, pup = newc ? cand_up : up, pl = newc ? thick : L;
-            const double xa = (plo - a) / hi, xb = (pup - a) / hi;
-#pragma unroll
-            for (int m = 0; m < NF; ++m) pc[m] = pl * average(c0[m], c1[m], c2[m], xa, xb);
-        }
-        // the one target write of this step: wj from wv / wh, or (vanished) the polynomial at wx
-        int wj = -1;
-        bool wpoly = false;
-        double wh = 0.0, wx = 0.0, wv[NF];
-#pragma unroll
-        for (int m = 0; m < NF; ++m) wv[m] = 0.0;
-        if (newc) {
-            if (cand >= 0) {                               // deposed: an ordinary piece of its finished target
-                resum = resum || ns >= 2;
-#pragma unroll
-                for (int m = 0; m < NF; ++m) {
-                    s[m] += pc[m];
-                    wv[m] = base[m] + pc[m];
-                }
-                ++ns;
-                wj = cand;
-                wh = cand_h;
-            }
-            cand = j;
-            thick = L;
-            cand_lo = lo;
-            cand_up = up;
-            cand_h = hj;
-#pragma unroll
-            for (int m = 0; m < NF; ++m) base[m] = acc[m];
-        } else if (L > 0.0) {
-#pragma unroll
-            for (int m = 0; m < NF; ++m) {
-                s[m] += pc[m];
-                acc[m] += pc[m];
-            }
-            ++ns;
-        }
-        const bool target_ends = hi_t <= b && j < n1 - 1;
-        if (target_ends) {
-            if (j != cand) {
-                wj = j;
-                if (hj > 0.0) {
-                    wh = hj;
-#pragma unroll
-                    for (int m = 0; m < NF; ++m) wv[m] = acc[m];
-                } else {                                   // vanished target: this cell's value at its position
-                    wpoly = true;
-                    wx = (tl - a) / hi;
-                }
-            }
-        } else {                                           // the cell ends in target j
-            if (cand >= 0) {
-                if (resum) {                               // the others' sum in target order
-                    int jj = j0;
-                    double tl2 = tl0, th2 = th0;
-#pragma unroll
-                    for (int m = 0; m < NF; ++m) s[m] = 0.0;
-                    while (true) {
-                        const double lo2 = pmax(a, tl2);
-                        const double up2 = pmin(b, jj < n1 - 1 ? th2 : pmax(th2, b));
-                        const double L2 = up2 - lo2;
-                        if (L2 > 0.0 && jj != cand) {
-                            const double xa = (lo2 - a) / hi, xb = (up2 - a) / hi;
-#pragma unroll
-                            for (int m = 0; m < NF; ++m) s[m] += L2 * average(c0[m], c1[m], c2[m], xa, xb);
-                        }
-                        if (jj == j) break;
-                        ++jj;
-                        tl2 = th2;
-                        th2 = th2 + io.ht(jj);
-                    }
-                }
-                double cth[NF];
-#pragma unroll
-                for (int m = 0; m < NF; ++m) cth[m] = base[m] + (u[m] * hi - s[m]);
-                if (cand < j) {                            // a piece implies a positive thickness
-                    wj = cand;
-                    wh = cand_h;
-#pragma unroll
-                    for (int m = 0; m < NF; ++m) wv[m] = cth[m];
-                } else {
-#pragma unroll
-                    for (int m = 0; m < NF; ++m) acc[m] = cth[m];
-                }
-            }
-            if (j == n1 - 1) last_reached = true;
-            if (last_reached && !last_set) {               // x = t_edge[n1-1] = tl when j = n1-1
-                const double xi = (tl - a) / hi;
-#pragma unroll
-                for (int m = 0; m < NF; ++m) last_val[m] = c0[m] + xi * (c1[m] + xi * c2[m]);
-                last_set = true;
-            }
-        }
-        if (wj >= 0) {
-#pragma unroll
-            for (int m = 0; m < NF; ++m) io.put(m, wj, wpoly ? c0[m] + wx * (c1[m] + wx * c2[m]) : wv[m] / wh);
-        }
-        // ---- next pair: the next target of this cell, or the next source cell with h > 0
-        if (target_ends) {
-            ++j;
-            tl = th;
-            hj = io.ht(j);
-            th = th + hj;
-#pragma unroll
-            for (int m = 0; m < NF; ++m) acc[m] = 0.0;
-        } else {
-            a = b;
-            do {
-                ++i;
-                hi = i < n0 ? io.hs(i) : 1.0;
-            } while (i < n0 && !(hi > 0.0));
-            if (i >= n0) break;
-            b = a + hi;
-            const bool rec = rec_col && i >= 1 && i <= n0 - 2;
-#pragma unroll
-            for (int m = 0; m < NF; ++m) {
-                u[m] = io.f(m, i);
-                cell_poly(u[m], rec, plm, rec ? io.rp(m, i) : 0.0, rec ? io.rq(m, i) : 0.0, c0[m], c1[m], c2[m]);
-                s[m] = 0.0;
-            }
-            cand = -1;
-            thick = -1.0;
-            ns = 0;
-            resum = false;
-            j0 = j;
-            tl0 = tl;
-            th0 = th;
-        }
-    }
-    finish_targets<NF>(io, n1, j, acc, last_set, last_val, last);
 }
 
 // Column with no active source cell (remap.py:375-381): copied when n0 == n1, else every target takes the mean.

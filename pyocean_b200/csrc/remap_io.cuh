@@ -20,20 +20,11 @@ struct ColumnIO {
     const double* __restrict__ t;
     const double* __restrict__ u[NF];
     double* __restrict__ o[NF];
-    double* __restrict__ rp_[NF];     // stored reconstruction (the two-pass form): p and q of each field
-    double* __restrict__ rq_[NF];
     i64 plane;
     __device__ __forceinline__ double hs(int k) const { return __ldg(h + k * plane); }
     __device__ __forceinline__ double ht(int k) const { return __ldg(t + k * plane); }
     __device__ __forceinline__ double f(int m, int k) const { return __ldg(u[m] + k * plane); }
     __device__ __forceinline__ void put(int m, int k, double v) { o[m][k * plane] = v; }
-    __device__ __forceinline__ double rp(int m, int k) const { return __ldg(rp_[m] + k * plane); }
-    __device__ __forceinline__ double rq(int m, int k) const { return __ldg(rq_[m] + k * plane); }
-    __device__ __forceinline__ void rput(int m, int k, double p, double q)
-    {
-        rp_[m][k * plane] = p;
-        rq_[m][k * plane] = q;
-    }
 };
 
 // The same for fields of fewer than 2^31 entries: the arrays' bases are the same for every thread of a block (kept
@@ -44,26 +35,17 @@ struct ColumnIO32 {
     const double* __restrict__ t;
     const double* __restrict__ u[NF];
     double* __restrict__ o[NF];
-    double* __restrict__ rp_[NF];     // stored reconstruction (the two-pass form): p and q of each field
-    double* __restrict__ rq_[NF];
     int c, plane;
     __device__ __forceinline__ double hs(int k) const { return __ldg(h + (c + k * plane)); }
     __device__ __forceinline__ double ht(int k) const { return __ldg(t + (c + k * plane)); }
     __device__ __forceinline__ double f(int m, int k) const { return __ldg(u[m] + (c + k * plane)); }
     __device__ __forceinline__ void put(int m, int k, double v) { o[m][c + k * plane] = v; }
-    __device__ __forceinline__ double rp(int m, int k) const { return __ldg(rp_[m] + (c + k * plane)); }
-    __device__ __forceinline__ double rq(int m, int k) const { return __ldg(rq_[m] + (c + k * plane)); }
-    __device__ __forceinline__ void rput(int m, int k, double p, double q)
-    {
-        rp_[m][c + k * plane] = p;
-        rq_[m][c + k * plane] = q;
-    }
 };
 
 // remap.py:400-415 for one column and NF fields: a column that is not wet is copied (n0 == n1) or NaN; a column
 // with a negative or NaN target thickness gets the sentinel (the general algorithm finishes it in a later launch);
-// otherwise the one-pass sweep (EVENTS: the walk over the stored reconstruction), or the no-active-source rule.
-template <int NF, bool EVENTS = false, class IO>
+// otherwise the one-pass sweep, or the no-active-source rule.
+template <int NF, class IO>
 __device__ __forceinline__ void remap_column_io(IO& io, bool wet, int n0, int n1, int scheme)
 {
     if (!wet) {                                      // remap.py:405-408
@@ -83,19 +65,7 @@ __device__ __forceinline__ void remap_column_io(IO& io, bool wet, int n0, int n1
         return;
     }
     if (n_active == 0) rc::remap_column_dry<NF>(io, n0, n1);
-    else if constexpr (EVENTS) rc::remap_column_events<NF>(io, n0, n1, scheme, n_active, last);
     else rc::remap_column_stream<NF>(io, n0, n1, scheme, n_active, last);
-}
-
-// The first pass of the two-pass form: the stored reconstruction of a wet column with an active source cell (what
-// remap_column_events reads back; nothing for PCM).
-template <int NF, class IO>
-__device__ __forceinline__ void reconstruct_column_io(IO& io, bool wet, int n0, int scheme)
-{
-    if (!wet || scheme == rc::PCM) return;
-    int n_active = 0;
-    for (int k = 0; k < n0; ++k) n_active += io.hs(k) > 0.0;
-    if (n_active > 0) rc::reconstruct_column_stream<NF>(io, n0, scheme, n_active);
 }
 
 }  // namespace remap

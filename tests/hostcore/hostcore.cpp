@@ -39,19 +39,10 @@ struct HostIO {
     const double* ht_;
     const double* u[4];
     double* o[4];
-    double* rp_[4];
-    double* rq_[4];
     double hs(int k) const { return h[k]; }
     double ht(int k) const { return ht_[k]; }
     double f(int m, int k) const { return u[m][k]; }
     void put(int m, int k, double v) { o[m][k] = v; }
-    double rp(int m, int k) const { return rp_[m][k]; }
-    double rq(int m, int k) const { return rq_[m][k]; }
-    void rput(int m, int k, double p, double q)
-    {
-        rp_[m][k] = p;
-        rq_[m][k] = q;
-    }
 };
 
 }  // namespace
@@ -108,32 +99,9 @@ int remap_stream_column(const double* h_src, const double* f_src, int n0, const 
     for (int k = 0; k < n1; ++k)
         if (!(h_tgt[k] >= 0.0)) return 1;
     if (n_active == 0) return 1;
-    HostIO io{h_src, h_tgt, {f_src, f_src + n0, nullptr, nullptr}, {out, out + n1, nullptr, nullptr}, {}, {}};
+    HostIO io{h_src, h_tgt, {f_src, f_src + n0, nullptr, nullptr}, {out, out + n1, nullptr, nullptr}};
     if (nf == 1) po::rc::remap_column_stream<1>(io, n0, n1, scheme, n_active, last);
     else po::rc::remap_column_stream<2>(io, n0, n1, scheme, n_active, last);
-    return 0;
-}
-
-// The two-pass form of the same remap (the reconstruction stored per cell in rec (2, nf, n0), then the walk over
-// the (cell, target) pairs).  Returns as remap_stream_column.
-int remap_events_column(const double* h_src, const double* f_src, int n0, const double* h_tgt, int n1, int nf,
-                        int scheme, double* out, double* rec)
-{
-    int n_active = 0, last = -1;
-    for (int k = 0; k < n0; ++k)
-        if (h_src[k] > 0.0) { ++n_active; last = k; }
-    for (int k = 0; k < n1; ++k)
-        if (!(h_tgt[k] >= 0.0)) return 1;
-    if (n_active == 0) return 1;
-    HostIO io{h_src, h_tgt, {f_src, f_src + n0, nullptr, nullptr}, {out, out + n1, nullptr, nullptr},
-              {rec, rec + n0, nullptr, nullptr}, {rec + nf * n0, rec + nf * n0 + n0, nullptr, nullptr}};
-    if (nf == 1) {
-        po::rc::reconstruct_column_stream<1>(io, n0, scheme, n_active);
-        po::rc::remap_column_events<1>(io, n0, n1, scheme, n_active, last);
-    } else {
-        po::rc::reconstruct_column_stream<2>(io, n0, scheme, n_active);
-        po::rc::remap_column_events<2>(io, n0, n1, scheme, n_active, last);
-    }
     return 0;
 }
 

@@ -39,8 +39,6 @@ def hostcore(tmp_path_factory):
     L.check_plane_div.argtypes = [ctypes.POINTER(ctypes.c_int), ctypes.c_longlong]
     L.remap_stream_column.restype = ctypes.c_int
     L.remap_stream_column.argtypes = [D, D, ctypes.c_int, D, ctypes.c_int, ctypes.c_int, ctypes.c_int, D]
-    L.remap_events_column.restype = ctypes.c_int
-    L.remap_events_column.argtypes = [D, D, ctypes.c_int, D, ctypes.c_int, ctypes.c_int, ctypes.c_int, D, D]
     L.remap_general_column.restype = ctypes.c_int
     L.remap_general_column.argtypes = [D, D, ctypes.c_int, D, ctypes.c_int, ctypes.c_int, D]
     return L
@@ -116,46 +114,6 @@ def test_one_pass_remap_equals_reference_column_remap(hostcore, scheme):
                 np.testing.assert_array_equal(out[m], ref, err_msg=f"n0={n0} n1={n1} scheme={scheme} field={m}")
             checked += 1
     assert checked > 2500
-
-
-def _wide_cells(seed, count):
-    # few thick source cells over many targets of mixed thickness (vanished ones included): each cell spans many
-    # pieces, and its longest piece often comes after two or more shorter ones
-    rng = np.random.default_rng(seed)
-    for c in range(count):
-        n0 = int(rng.integers(1, 8))
-        n1 = int(rng.integers(2, 61))
-        h0 = rng.uniform(0.5, 20.0, n0)
-        if c % 3 == 1:
-            h0 = np.where(rng.random(n0) < 0.3, 0.0, h0)
-        h1 = rng.choice([0.0, 0.05, 0.1, 0.3, 1.0, 2.5], n1) * rng.uniform(0.5, 1.5, n1)
-        if c % 4 == 0:
-            h1 = np.round(h1, 1)                                # equal lengths: ties for the longest piece
-        if h1.sum() > 0:
-            h1 *= h0.sum() / h1.sum()
-        yield n0, n1, h0, rng.normal(15, 3, n0), h1
-
-
-@pytest.mark.parametrize("scheme", [O.PCM, O.PLM, O.PPM_H4])
-def test_two_pass_remap_equals_reference_column_remap(hostcore, scheme):
-    # the stored reconstruction + walk over (cell, target) pairs: bit for bit the reference's remap_column
-    checked = 0
-    cols = list(_columns(500 + scheme, 1500)) + list(_wide_cells(900 + scheme, 1500))
-    for n0, n1, h0, u0, h1 in cols:
-        u2 = np.stack([u0, u0 * 0.37 - 4.0])
-        for nf in (1, 2):
-            out = np.full((nf, n1), np.nan)
-            rec = np.full((2, nf, n0), np.nan)
-            rc = hostcore.remap_events_column(_p(h0), _p(np.ascontiguousarray(u2[:nf])), n0, _p(h1), n1, nf,
-                                              scheme, _p(out), _p(rec))
-            if rc:
-                assert h0.max() <= 0.0
-                continue
-            for m in range(nf):
-                ref = O.remap_column(h0, u2[m], h1, scheme)
-                np.testing.assert_array_equal(out[m], ref, err_msg=f"n0={n0} n1={n1} scheme={scheme} field={m}")
-            checked += 1
-    assert checked > 5000
 
 
 @pytest.mark.parametrize("scheme", [O.PCM, O.PLM, O.PPM_H4])
