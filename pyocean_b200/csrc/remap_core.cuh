@@ -49,6 +49,7 @@ PO_HD int effective_scheme(int n_active, int scheme)          // remap.py:46-53
 // Thickness factor h_c / (h_l + 2 h_c + h_r + h_neglect) of the PLM slope, shared by every field of a column.
 PO_HD double plm_ratio(double h_l, double h_c, double h_r) { return h_c / (h_l + 2.0 * h_c + h_r + H_NEGLECT); }
 
+// The PLM steps are written with selects instead of branches, as the PPM_H4 limiter steps below are (same values).
 PO_HD double plm_slope(double ratio, double u_l, double u_c, double u_r)   // remap.py:59-80
 {
     const double sigma_r = u_r - u_c;
@@ -56,14 +57,11 @@ PO_HD double plm_slope(double ratio, double u_l, double u_c, double u_r)   // re
     const double sigma_c = 2.0 * (u_r - u_l) * ratio;
     const double u_min = pmin(pmin(u_l, u_c), u_r);
     const double u_max = pmax(pmax(u_l, u_c), u_r);
-    double slope = 0.0;
-    if (sigma_l * sigma_r > 0.0) {
-        const double m = pmin(fabs(sigma_c), 2.0 * pmin(u_c - u_min, u_max - u_c));
-        slope = sigma_c >= 0.0 ? m : -m;
-    }
-    if (u_c - 0.5 * fabs(slope) < u_min || u_c + 0.5 * fabs(slope) > u_max) slope = slope * (1.0 - EPS);
-    if (fabs(slope) < 1e-140) slope = 0.0;
-    return slope;
+    const double m = pmin(fabs(sigma_c), 2.0 * pmin(u_c - u_min, u_max - u_c));
+    double slope = sigma_l * sigma_r > 0.0 ? (sigma_c >= 0.0 ? m : -m) : 0.0;
+    const bool shrink = (u_c - 0.5 * fabs(slope) < u_min) | (u_c + 0.5 * fabs(slope) > u_max);
+    slope = shrink ? slope * (1.0 - EPS) : slope;
+    return fabs(slope) < 1e-140 ? 0.0 : slope;
 }
 
 PO_HD double plm_monotonized(double u_l, double u_c, double u_r, double s_l, double s_c, double s_r)   // :83-97
@@ -72,16 +70,14 @@ PO_HD double plm_monotonized(double u_l, double u_c, double u_r, double s_l, dou
     const double e_r = u_l + 0.5 * s_l;
     const double e_l = u_r - 0.5 * s_r;
     double slp = fabs(s_c);
-    double edge = u_c - 0.5 * s_c;
-    if ((edge - e_r) * (u_c - edge) < 0.0) {
-        edge = 0.5 * (edge + e_r);
-        slp = pmin(slp, fabs(edge - u_c) * almost_two);
-    }
-    edge = u_c + 0.5 * s_c;
-    if ((edge - u_c) * (e_l - edge) < 0.0) {
-        edge = 0.5 * (edge + e_l);
-        slp = pmin(slp, fabs(edge - u_c) * almost_two);
-    }
+    const double edge_l = u_c - 0.5 * s_c;
+    const double mid_l = 0.5 * (edge_l + e_r);
+    const double slp_l = pmin(slp, fabs(mid_l - u_c) * almost_two);
+    slp = (edge_l - e_r) * (u_c - edge_l) < 0.0 ? slp_l : slp;
+    const double edge_r = u_c + 0.5 * s_c;
+    const double mid_r = 0.5 * (edge_r + e_l);
+    const double slp_r = pmin(slp, fabs(mid_r - u_c) * almost_two);
+    slp = (edge_r - u_c) * (e_l - edge_r) < 0.0 ? slp_r : slp;
     return s_c >= 0.0 ? slp : -slp;
 }
 
@@ -97,7 +93,7 @@ PO_HD void plm_coef(double u_c, double u_next, double mslp, double mslp_next, do
     const double edge = c1 + c0;
     const double am = fabs(mslp_next);
     const double e_r = u_next - 0.5 * (slp_next >= 0.0 ? am : -am);
-    if ((edge - u_c) * (e_r - edge) < 0.0) c1 = c1 * (1.0 - EPS);
+    c1 = (edge - u_c) * (e_r - edge) < 0.0 ? c1 * (1.0 - EPS) : c1;
 }
 
 // (C(0), C(dz1)) of the cubic whose means over the 4 end cells are u1..u4, thicknesses h1..h4 from the end
@@ -385,13 +381,15 @@ PO_HDT void remap_column_stream(IO& io, int n0, int n1, int scheme, int n_active
         const double hi = wh[2];
         if (hi > 0.0) {
             const double b = a + hi;
-            // pass 1: which targets the cell reaches, and the first thickest piece
+            // pass 1: which targets the cell reaches, and the first thickest piece.  The edges here are sums of
+            // non-negative thicknesses from +0 (never NaN: such columns go to the general algorithm, such source
+            // cells are skipped; never -0), so the native fmax / fmin give pmax / pmin's values bit for bit.
             int jj = j, jthick = -1;
             double tl = t_lo, th = t_hi, thick = -1.0;
             while (true) {
-                const double lo = pmax(a, tl);
-                const double hi_t = jj < n1 - 1 ? th : pmax(th, b);
-                const double L = pmin(b, hi_t) - lo;
+                const double lo = fmax(a, tl);
+                const double hi_t = jj < n1 - 1 ? th : fmax(th, b);
+                const double L = fmin(b, hi_t) - lo;
                 if (L > 0.0 && L > thick) {
                     thick = L;
                     jthick = jj;
@@ -414,9 +412,9 @@ PO_HDT void remap_column_stream(IO& io, int n0, int n1, int scheme, int n_active
             tl = t_lo;
             th = t_hi;
             while (true) {
-                const double lo = pmax(a, tl);
-                const double hi_t = jj < n1 - 1 ? th : pmax(th, b);
-                const double up = pmin(b, hi_t);
+                const double lo = fmax(a, tl);
+                const double hi_t = jj < n1 - 1 ? th : fmax(th, b);
+                const double up = fmin(b, hi_t);
                 const double L = up - lo;
                 double content[NF];
 #pragma unroll
