@@ -101,12 +101,12 @@ def workload_config(w, world: int) -> dict:
 # remap): DRAM bytes read + written per call, and FP64 thread instructions (DFMA + DMUL + DADD) per call.  The
 # line carries the capture's date beside them (NCU_CAPTURED); a kernel change needs a new capture.
 NCU_PER_CALL = {
-    "basin_512x512x50_nt2": {"advect_fct": {"dram_bytes": 9508593408, "fp64_inst": 18348363343},
-                             "remap_columns": {"dram_bytes": 775190528, "fp64_inst": 2861834106}},
+    "basin_512x512x50_nt2": {"advect_fct": {"dram_bytes": 9515066880, "fp64_inst": 18348363343},
+                             "remap_columns": {"dram_bytes": 793686784, "fp64_inst": 3091276864}},
 }
 NCU_CAPTURED = ("2026-12-04: DRAM bytes from a one-pass ncu capture (dram__bytes_read.sum, dram__bytes_write.sum) of "
-                "one step of the basin 512x512x50 workload; FP64 instruction counts from the full-set capture of "
-                "2026-12-03 (same kernels)")
+                "one step of the basin 512x512x50 workload; FP64 instruction counts of advect_fct from the full-set "
+                "capture of 2026-12-03 (same kernels), of the remap from a capture of its kernel on 2026-12-04")
 FP64_LANES_PER_SM, SMS = 64, 148
 
 
