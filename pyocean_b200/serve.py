@@ -9,8 +9,8 @@ arrived — in arrival order, while the HBM budget and the slot count allow — 
 their steps, so a job that arrives while others run joins the next step instead of waiting for them (continuous
 batching, as LLM servers batch requests per decoding iteration).  Which admitted jobs a step advances is the
 policy's (``Server._select``).  By default (``adaptive``) it depends on the backlog: while the admitted jobs'
-remaining work is short (below ``backlog_cells`` tracer cell-steps, about half a second of GPU work), the oldest job
-plus the small jobs that fit beside it without slowing it by more than a quarter, so the long jobs of the tail keep
+remaining work is short (below ``backlog_cells`` tracer cell-steps, about 1.5 s of GPU work), the oldest job plus
+the small jobs that fit beside it without slowing it by more than ``share`` (5 %), so the long jobs of the tail keep
 close to their run-alone time while short jobs never wait behind them; once the backlog is longer, every admitted
 job, so the GPU runs the largest batches and the queue drains at the batched rate.  The host only enqueues work: it runs at most
 ``max_ahead`` iterations ahead of the GPU, so the device queue never drains while jobs are active.
@@ -99,7 +99,7 @@ class Server:
     def __init__(self, device=None, mixed: bool = True, batched: bool = True, max_slots: int = 256,
                  hbm_budget: int | None = None, max_ahead: int = 3, max_steps_per_iter: int = 4,
                  tile_rows: int = 8, remap_nf: int = 2, keep_results: bool = False, policy: str = "adaptive",
-                 fill_cells: int = 4_000_000, share: float = 0.25, backlog_cells: float = 2e9) -> None:
+                 fill_cells: int = 4_000_000, share: float = 0.05, backlog_cells: float = 6e9) -> None:
         if policy not in self.POLICIES:
             raise ValueError(f"policy {policy!r}: use one of {self.POLICIES}")
         self.policy, self.fill_cells, self.share = policy, int(fill_cells), float(share)
