@@ -281,38 +281,22 @@ __global__ void FINAL_BOUNDS fct_final_kernel(StepArgs a)
 }
 
 // Batched launches of passes 4 and 5: domain d owns CTAs off[d] .. off[d+1]-1, one 32 x 8 tile of one layer each.
-__device__ __forceinline__ void batched_tile(const BatchDomain* __restrict__ doms, const int* __restrict__ off,
-                                             int ndom, int& d, int& i, int& j, int& k)
-{
-    d = find_domain(off, ndom, blockIdx.x);
-    const Shape s = doms[d].a.s;
-    const int tx = ceil_div(s.nx, TI), ty = ceil_div(s.ny, TJ);
-    int local = blockIdx.x - __ldg(off + d);
-    k = local / (tx * ty);
-    local -= k * tx * ty;
-    const int by = local / tx, bx = local - by * tx;
-    i = bx * TI + threadIdx.x % TI;
-    j = by * TJ + threadIdx.x / TI;
-}
-
 __global__ void COEFF_BATCHED_BOUNDS fct_coeff_batched(const BatchDomain* __restrict__ doms,
                                                                const int* __restrict__ off, int ndom)
 {
-    int d, i, j, k;
-    batched_tile(doms, off, ndom, d, i, j, k);
+    __shared__ BlockTile bt;
     __shared__ StepArgs sh;
-    const StepArgs& a = block_args(doms, d, sh);
-    coeff_body(a, i, j, k);
+    const StepArgs& a = block_tile<false, TJ>(doms, off, ndom, bt, sh);
+    coeff_body(a, bt.bx * TI + threadIdx.x % TI, bt.by * TJ + threadIdx.x / TI, bt.k);
 }
 
 __global__ void FINAL_BATCHED_BOUNDS fct_final_batched(const BatchDomain* __restrict__ doms,
                                                                const int* __restrict__ off, int ndom)
 {
-    int d, i, j, k;
-    batched_tile(doms, off, ndom, d, i, j, k);
+    __shared__ BlockTile bt;
     __shared__ StepArgs sh;
-    const StepArgs& a = block_args(doms, d, sh);
-    final_body(a, i, j, k);
+    const StepArgs& a = block_tile<false, TJ>(doms, off, ndom, bt, sh);
+    final_body(a, bt.bx * TI + threadIdx.x % TI, bt.by * TJ + threadIdx.x / TI, bt.k);
 }
 
 // Effective flux F_L + C A of the step through u-face column face_i, (nt, n, ny) (tracers.py:251-254).

@@ -261,34 +261,50 @@ __global__ void FACES3_BOUNDS(TI * TJR) fct_faces3_kernel(StepArgs a)
     faces_plane<3, ZV, MIX, TJR>(a);
 }
 
-// Domain, plane and cell of a thread of a batched stage pass: domain d owns CTAs off[d] .. off[d+1]-1, each one
-// 32 x TJR tile of one (t, k) plane (k-major).
-template <int TJR>
-__device__ __forceinline__ int batched_plane_tile(const BatchDomain* __restrict__ doms, const int* __restrict__ off,
-                                                  int ndom, int& t, int& k, int& i, int& j)
+// Where a batched CTA works (domain d owns CTAs off[d] .. off[d+1]-1): its domain d, tracer t and layer k, and its
+// 32 x TJR tile (bx, by).  The first thread of
+// the CTA works it out (a binary search over the domains' CTA offsets and two integer divisions, the same for every
+// thread of the CTA) and shares it, with the domain's argument block, through shared memory: done by every thread,
+// that set-up cost the batched cell passes as many instructions again as their own work.
+struct BlockTile {
+    int d, t, k, bx, by;
+};
+
+// The CTA's tile (bt) and its domain's argument block (sh), both in shared memory.  PLANES: the CTA's index counts
+// 32 x TJR tiles of the (t, k) planes (k-major: the stage passes); else tiles of the layers (t = 0: the coefficient
+// and final passes).  Call before any thread returns: it contains block barriers.
+template <bool PLANES, int TJR>
+__device__ __forceinline__ const StepArgs& block_tile(const BatchDomain* __restrict__ doms, const int* __restrict__ off,
+                                                      int ndom, BlockTile& bt, StepArgs& sh)
 {
-    const int d = find_domain(off, ndom, blockIdx.x);
-    const Shape s = doms[d].a.s;
-    const int tx = ceil_div(s.nx, TI), ty = ceil_div(s.ny, TJR);
-    int local = blockIdx.x - __ldg(off + d);
-    const int p = local / (tx * ty);
-    local -= p * tx * ty;
-    split_plane(p, s.nt, doms[d].a.tdiv, k, t);
-    const int by = local / tx, bx = local - by * tx;
-    i = bx * TI + threadIdx.x % TI;
-    j = by * TJR + threadIdx.x / TI;
-    return d;
+    if (threadIdx.x == 0) {
+        const int d = find_domain(off, ndom, blockIdx.x);
+        const Shape s = doms[d].a.s;
+        const int tx = ceil_div(s.nx, TI), ty = ceil_div(s.ny, TJR);
+        int local = blockIdx.x - __ldg(off + d);
+        const int p = local / (tx * ty);
+        local -= p * tx * ty;
+        int t = 0, k = p;
+        if (PLANES) split_plane(p, s.nt, doms[d].a.tdiv, k, t);
+        const int by = local / tx;
+        bt.d = d;
+        bt.t = t;
+        bt.k = k;
+        bt.by = by;
+        bt.bx = local - by * tx;
+    }
+    __syncthreads();
+    return block_args(doms, bt.d, sh);
 }
 
 template <int STAGE, bool ZV, bool MIX, int TJR>
 __device__ __forceinline__ void faces_batched_body(const BatchDomain* __restrict__ doms, const int* __restrict__ off,
                                                    int ndom)
 {
-    int t, k, i, j;
-    const int d = batched_plane_tile<TJR>(doms, off, ndom, t, k, i, j);
+    __shared__ BlockTile bt;
     __shared__ StepArgs sh;
-    const StepArgs& a = block_args(doms, d, sh);
-    faces_body<STAGE, ZV, MIX>(a, t, k, i, j);
+    const StepArgs& a = block_tile<true, TJR>(doms, off, ndom, bt, sh);
+    faces_body<STAGE, ZV, MIX>(a, bt.t, bt.k, bt.bx * TI + threadIdx.x % TI, bt.by * TJR + threadIdx.x / TI);
 }
 
 template <int STAGE, bool ZV, bool MIX, int TJR>
@@ -350,11 +366,10 @@ template <int STAGE, int TJR>
 __global__ void __launch_bounds__(TI * TJR) fct_update_batched(const BatchDomain* __restrict__ doms,
                                                                const int* __restrict__ off, int ndom)
 {
-    int t, k, i, j;
-    const int d = batched_plane_tile<TJR>(doms, off, ndom, t, k, i, j);
+    __shared__ BlockTile bt;
     __shared__ StepArgs sh;
-    const StepArgs& a = block_args(doms, d, sh);
-    update_body<STAGE>(a, t, k, i, j);
+    const StepArgs& a = block_tile<true, TJR>(doms, off, ndom, bt, sh);
+    update_body<STAGE>(a, bt.t, bt.k, bt.bx * TI + threadIdx.x % TI, bt.by * TJR + threadIdx.x / TI);
 }
 
 }  // namespace po
