@@ -7,7 +7,8 @@ the host (g++ -ffp-contract=off, the IEEE-754 operations the GPU executes) —
 * the plane-index division by the tracer count (plane_div) against integer division, for every plane index;
 * the one-pass column remap (remap_column_stream) against the oracle's restatement of remap_column, bit for bit,
   on thousands of seeded columns with vanished source and target layers, both schemes' order reductions, totals
-  that differ by round-off, n0 != n1, and one or two fields per sweep.
+  that differ by round-off, n0 != n1, one or two fields per sweep, and thick source cells spanning many targets
+  (the thickest piece after shorter ones, ties for it); the array formulation on the same columns.
 """
 from __future__ import annotations
 
@@ -114,6 +115,46 @@ def test_one_pass_remap_equals_reference_column_remap(hostcore, scheme):
                 np.testing.assert_array_equal(out[m], ref, err_msg=f"n0={n0} n1={n1} scheme={scheme} field={m}")
             checked += 1
     assert checked > 2500
+
+
+def _wide_cells(seed, count):
+    # few thick source cells over many targets of mixed thickness (vanished ones included): each cell spans many
+    # pieces, its longest piece often follows shorter ones, and rounded thicknesses make ties for the longest
+    rng = np.random.default_rng(seed)
+    for c in range(count):
+        n0 = int(rng.integers(1, 8))
+        n1 = int(rng.integers(2, 61))
+        h0 = rng.uniform(0.5, 20.0, n0)
+        if c % 3 == 1:
+            h0 = np.where(rng.random(n0) < 0.3, 0.0, h0)
+        h1 = rng.choice([0.0, 0.05, 0.1, 0.3, 1.0, 2.5], n1) * rng.uniform(0.5, 1.5, n1)
+        if c % 4 == 0:
+            h1 = np.round(h1, 1)
+        if h1.sum() > 0:
+            h1 *= h0.sum() / h1.sum()
+        yield n0, n1, h0, rng.normal(15, 3, n0), h1
+
+
+@pytest.mark.parametrize("scheme", [O.PCM, O.PLM, O.PPM_H4])
+def test_one_pass_remap_on_cells_spanning_many_targets(hostcore, scheme):
+    checked = 0
+    for n0, n1, h0, u0, h1 in _wide_cells(900 + scheme, 1500):
+        u2 = np.stack([u0, u0 * 0.37 - 4.0])
+        for nf in (1, 2):
+            out = np.full((nf, n1), np.nan)
+            rc = hostcore.remap_stream_column(_p(h0), _p(np.ascontiguousarray(u2[:nf])), n0, _p(h1), n1, nf,
+                                              scheme, _p(out))
+            if rc:
+                assert h0.max() <= 0.0
+                continue
+            for m in range(nf):
+                ref = O.remap_column(h0, u2[m], h1, scheme)
+                np.testing.assert_array_equal(out[m], ref, err_msg=f"n0={n0} n1={n1} scheme={scheme} field={m}")
+            out1 = np.full(n1, np.nan)
+            assert hostcore.remap_general_column(_p(h0), _p(u0), n0, _p(h1), n1, scheme, _p(out1)) == 0
+            np.testing.assert_array_equal(out1, O.remap_column(h0, u0, h1, scheme))
+            checked += 1
+    assert checked > 2000
 
 
 @pytest.mark.parametrize("scheme", [O.PCM, O.PLM, O.PPM_H4])
